@@ -1,0 +1,165 @@
+/*
+ * uaamg.h -- C ABI of the B200 UAAMG-PCG library (libuaamg_b200.so).
+ *
+ * Drop-in boundary for the reference's SIMD_UAAMG pressure solver.  Every
+ * entry point names the reference interface it replaces (paths inside the
+ * reference project).  The reference passes OpenVDB grids by shared_ptr; this
+ * ABI passes the same content as a flattened leaf list (uaamg_leaf_grid,
+ * identical to an OpenVDB LeafNode<T,3> payload: origin, 512-bit value mask,
+ * 512 values with offset 64x+8y+z).
+ *
+ * Conventions
+ *  - Status codes, never exceptions: UAAMG_SUCCESS (0) and UAAMG_FAILED (1)
+ *    are the reference's PoissonSolver::SUCCESS / FAILED
+ *    (SIMD_UAAMG/simd_vdb_poisson.h:149-152); negative values are errors,
+ *    described by uaamg_last_error() (thread-local).
+ *  - Vectors (pressure, right-hand side) are "leaf-dense": float[leaf][512]
+ *    over the handle's DOF leaves (uaamg_poisson_dof_topology), zero at
+ *    voxels that are not degrees of freedom.  This is the buffer layout of
+ *    the grid LaplacianWithLevel::getZeroVectorGrid() returns.
+ *  - Functions without a suffix take HOST pointers and copy to and from the
+ *    device inside the call.  *_device functions take device pointers and
+ *    return after enqueueing on the handle's stream.
+ *  - One handle per host thread (the reference object is not re-entrant either).
+ */
+#ifndef UAAMG_H
+#define UAAMG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UAAMG_SUCCESS 0
+#define UAAMG_FAILED 1
+#define UAAMG_ERR_INVALID_ARGUMENT (-1)
+#define UAAMG_ERR_CUDA (-2)
+#define UAAMG_ERR_OUT_OF_MEMORY (-3)
+#define UAAMG_ERR_DOMAIN_TOO_LARGE (-4)
+#define UAAMG_ERR_NO_DEVICE (-5)
+
+/* PoissonSolver::SmootherOption (SIMD_UAAMG/simd_vdb_poisson.h:143-148) */
+#define UAAMG_SMOOTHER_SCHEDULED_RELAXED_JACOBI 0
+#define UAAMG_SMOOTHER_WEIGHTED_JACOBI 1
+#define UAAMG_SMOOTHER_RED_BLACK_GAUSS_SEIDEL 2
+#define UAAMG_SMOOTHER_SPAI0 3
+
+/* LaplacianApplySIMD::WorkingMode (SIMD_UAAMG/simd_vdb_poisson.cpp:685-692) */
+#define UAAMG_MODE_WEIGHTED_JACOBI 0
+#define UAAMG_MODE_RESIDUAL 1
+#define UAAMG_MODE_LAPLACIAN 2
+#define UAAMG_MODE_RED_GS 3
+#define UAAMG_MODE_BLACK_GS 4
+#define UAAMG_MODE_SPAI0 5
+
+/* A flattened openvdb::FloatGrid (components = 1) or Vec3fGrid (components = 3).
+ * origins and masks are host memory; values are host memory unless
+ * values_on_device != 0.  masks may be NULL (all voxels active). */
+typedef struct uaamg_leaf_grid {
+    int64_t leaf_count;
+    const int32_t* origins;   /* [leaf_count][3], multiples of 8 */
+    const uint64_t* masks;    /* [leaf_count][8] or NULL */
+    const float* values;      /* [leaf_count][512][components] */
+    int32_t components;       /* 1 or 3 */
+    int32_t values_on_device; /* 0: host pointer, 1: device pointer */
+    float background[3];      /* tree background per component */
+} uaamg_leaf_grid;
+
+typedef struct uaamg_poisson uaamg_poisson;
+
+/* Build the level-0 matrix and the multigrid hierarchy.
+ * Replaces LaplacianWithLevel::createPressurePoissonLaplacian(liquid_phi,
+ * face_weights, dt) (SIMD_UAAMG/simd_vdb_poisson.h:54-57, .cpp:95-99) followed
+ * by PoissonSolver::PoissonSolver(level0) (simd_vdb_poisson.h:153-160, which
+ * runs constructMultigridHierarchy, .cpp:1813-1842).  dx is the voxel size of
+ * liquid_phi (the reference reads liquid_phi->voxelSize()[0]). */
+int uaamg_poisson_create(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights,
+                         float dt, float dx, uaamg_poisson** out);
+/* ~PoissonSolver / ~LaplacianWithLevel */
+int uaamg_poisson_destroy(uaamg_poisson* h);
+
+/* Public fields of PoissonSolver (simd_vdb_poisson.h:165-169):
+ * mSmoother, mMaxIteration (100), mRelativeTolerance (1e-7). */
+int uaamg_poisson_set_smoother(uaamg_poisson* h, int smoother);
+int uaamg_poisson_set_max_iterations(uaamg_poisson* h, int max_iterations);
+int uaamg_poisson_set_relative_tolerance(uaamg_poisson* h, float relative_tolerance);
+/* mIterationTaken (simd_vdb_poisson.h:165) of the last solve */
+int uaamg_poisson_iterations(const uaamg_poisson* h);
+/* |r|_inf at the end of the last solve (the reference prints it per iteration,
+ * simd_vdb_poisson.cpp:2194) */
+float uaamg_poisson_final_residual(const uaamg_poisson* h);
+
+/* mMultigridHierarchy.size() and per level mNumDof / leaf count */
+int uaamg_poisson_num_levels(const uaamg_poisson* h);
+int64_t uaamg_poisson_num_dof(const uaamg_poisson* h, int level);
+int64_t uaamg_poisson_leaf_count(const uaamg_poisson* h, int level);
+/* Topology of a level's DOF grid (mDofIndex tree without empty leaves, in
+ * OpenVDB tree order): origins [n][3], masks [n][8] (host memory). */
+int uaamg_poisson_dof_topology(const uaamg_poisson* h, int level, int32_t* origins, uint64_t* masks);
+/* Every voxel's DOF index (mDofIndex values, setDofIndex .cpp:637-671), -1 off DOF. */
+int uaamg_poisson_dof_index(const uaamg_poisson* h, int level, int32_t* out);
+
+/* LaplacianWithLevel::createPressurePoissonRightHandSide(face_weights, vx, vy,
+ * vz, solid_velocity, dt) (simd_vdb_poisson.h:59-65, .cpp:101-127).
+ * rhs_out: host float[leaf][512] over the level-0 DOF leaves. */
+int uaamg_poisson_build_rhs(uaamg_poisson* h, const uaamg_leaf_grid* face_weights,
+                            const uaamg_leaf_grid* vx, const uaamg_leaf_grid* vy,
+                            const uaamg_leaf_grid* vz, const uaamg_leaf_grid* solid_velocity,
+                            float dt, float* rhs_out);
+int uaamg_poisson_build_rhs_device(uaamg_poisson* h, const uaamg_leaf_grid* face_weights,
+                                   const uaamg_leaf_grid* vx, const uaamg_leaf_grid* vy,
+                                   const uaamg_leaf_grid* vz, const uaamg_leaf_grid* solid_velocity,
+                                   float dt, float* d_rhs_out);
+
+/* PoissonSolver::solveMultigridPCG(in_out_pressure, rhs) (simd_vdb_poisson.h:162,
+ * .cpp:2155-2226).  pressure holds the initial guess on entry. Returns
+ * UAAMG_SUCCESS / UAAMG_FAILED (or an error); *iterations = mIterationTaken. */
+int uaamg_poisson_solve_pcg(uaamg_poisson* h, float* pressure, const float* rhs, int* iterations);
+int uaamg_poisson_solve_pcg_device(uaamg_poisson* h, float* d_pressure, const float* d_rhs,
+                                   int* iterations);
+/* PoissonSolver::solvePureMultigrid (simd_vdb_poisson.h:163, .cpp:2228-2267) */
+int uaamg_poisson_solve_mg(uaamg_poisson* h, float* pressure, const float* rhs, int* iterations);
+int uaamg_poisson_solve_mg_device(uaamg_poisson* h, float* d_pressure, const float* d_rhs,
+                                  int* iterations);
+
+/* Per-level operators, public methods of LaplacianWithLevel
+ * (simd_vdb_poisson.h:90-115).  Host pointers, level-dense vectors.
+ *   mode: UAAMG_MODE_*; weight: Jacobi weight; w_sor: SOR weight of GS modes.
+ * residualApply / laplacianApply / weightedJacobiApply / spai0Apply and one
+ * red or black Gauss-Seidel pass (.cpp:1347-1433). */
+int uaamg_poisson_level_apply(uaamg_poisson* h, int level, int mode, float weight, float w_sor,
+                              const float* lhs, const float* rhs, float* out);
+/* setGridToResultAfterFirstJacobi / ...FirstSPAI0 / ...FirstRBGS<true> (.cpp:1435-1582).
+ * kind: 0 Jacobi (uses weight), 1 SPAI0, 2 red-black Gauss-Seidel (uses w_sor). */
+int uaamg_poisson_level_first_sweep(uaamg_poisson* h, int level, int kind, float weight,
+                                    float w_sor, const float* rhs, float* out);
+/* restriction (fine level -> level+1) and prolongation<true> (level+1 -> level),
+ * .cpp:1624-1754. prolongation adds alpha*coarse into fine (in/out). */
+int uaamg_poisson_level_restrict(uaamg_poisson* h, int fine_level, const float* fine, float* coarse);
+int uaamg_poisson_level_prolongate(uaamg_poisson* h, int fine_level, const float* coarse,
+                                   float* fine, float alpha);
+/* Effective level coefficients after trimDefaultNodes (.cpp:1756-1811): diag,
+ * minus-x/y/z face entries ([n][512]) and per-leaf trimmed flags
+ * (bit0 diag, bit1 x, bit2 y, bit3 z). */
+int uaamg_poisson_level_coefficients(const uaamg_poisson* h, int level, float* diag, float* cx,
+                                     float* cy, float* cz, uint8_t* flags);
+/* Coarsest-level solve (Eigen CG, 10 iterations, zero guess: .cpp:2114-2152). */
+int uaamg_poisson_coarsest_solve(uaamg_poisson* h, const float* rhs, float* out);
+/* One preconditioner application z = M^-1 r (muCyclePreconditioner<2,true>(z, r, 0, 3)). */
+int uaamg_poisson_precondition(uaamg_poisson* h, const float* r, float* z);
+
+/* Stream (cudaStream_t as void*) used by *_device calls; NULL = the handle's own stream. */
+int uaamg_poisson_set_stream(uaamg_poisson* h, void* stream);
+/* Use the CUDA-graph PCG (1, default) or the host-driven loop (0). */
+int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph);
+/* Kernels launched by the last solve (including those inside the graph). */
+int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h);
+
+const char* uaamg_last_error(void);
+int uaamg_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

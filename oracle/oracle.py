@@ -1,0 +1,210 @@
+"""ctypes binding of the CPU oracle (liboracle.so built from poisson_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference arm of bench.py, never by the uaamg_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+SMOOTHERS = {"scheduled_jacobi": 0, "weighted_jacobi": 1, "rbgs": 2, "spai0": 3}
+MODES = {"jacobi": 0, "residual": 1, "laplacian": 2, "red_gs": 3, "black_gs": 4, "spai0": 5}
+
+f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    path = os.path.join(_HERE, "liboracle.so")
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return path
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        vp = C.c_void_p
+        L.orc_poisson_create.restype = vp
+        L.orc_poisson_create.argtypes = [C.c_int64, i32p, u64p, f32p, C.c_float,
+                                         C.c_int64, i32p, f32p, f32p, C.c_float, C.c_float, C.c_int]
+        L.orc_poisson_free.argtypes = [vp]
+        for fn in ("orc_num_levels",):
+            getattr(L, fn).argtypes = [vp]
+        L.orc_level_leaf_count.argtypes = [vp, C.c_int]
+        L.orc_level_ndof.argtypes = [vp, C.c_int]
+        L.orc_level_topology.argtypes = [vp, C.c_int, i32p, u64p]
+        L.orc_level_coefficients.argtypes = [vp, C.c_int, f32p, f32p, f32p, f32p, u8p]
+        L.orc_level_defaults.argtypes = [vp, C.c_int, f32p]
+        g = [C.c_int64, i32p, f32p]
+        L.orc_build_rhs.argtypes = [vp, *g, f32p, *g, C.c_float, *g, C.c_float, *g, C.c_float,
+                                    *g, f32p, f32p]
+        L.orc_apply.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_float, f32p, f32p, f32p]
+        L.orc_first_jacobi.argtypes = [vp, C.c_int, C.c_float, f32p, f32p]
+        L.orc_first_spai0.argtypes = [vp, C.c_int, f32p, f32p]
+        L.orc_first_rbgs.argtypes = [vp, C.c_int, C.c_int, C.c_float, f32p, f32p]
+        L.orc_restrict.argtypes = [vp, C.c_int, f32p, f32p]
+        L.orc_prolongate.argtypes = [vp, C.c_int, f32p, f32p, C.c_float]
+        L.orc_coarsest_solve.argtypes = [vp, f32p, f32p]
+        L.orc_precondition.argtypes = [vp, C.c_int, f32p, f32p]
+        sig = [vp, f32p, f32p, C.c_float, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
+        L.orc_solve_pcg.argtypes = sig
+        L.orc_solve_mg.argtypes = sig
+        L.orc_abs_max.argtypes = [vp, C.c_int, f32p]
+        L.orc_abs_max.restype = C.c_float
+        L.orc_dot.argtypes = [vp, C.c_int, f32p, f32p]
+        L.orc_dot.restype = C.c_float
+        L.orc_triplets.argtypes = [vp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_triplets.restype = C.c_int64
+        L.orc_dof_index.argtypes = [vp, C.c_int, i32p]
+        L.orc_set_threads.argtypes = [C.c_int]
+        _LIB = L
+    return _LIB
+
+
+def _grid_args(g):
+    return (g.leaf_count, g.origins, np.ascontiguousarray(g.values.reshape(-1), dtype=np.float32))
+
+
+class OraclePoisson:
+    """Oracle hierarchy for one Poisson system (level 0 + coarse levels)."""
+
+    def __init__(self, phi, face_weights, dt, dx, hierarchy=True):
+        L = lib()
+        self._h = L.orc_poisson_create(phi.leaf_count, phi.origins, phi.masks,
+                                       np.ascontiguousarray(phi.values.reshape(-1)),
+                                       float(phi.background[0]), *_grid_args(face_weights),
+                                       face_weights.background, float(dt), float(dx),
+                                       1 if hierarchy else 0)
+        self.num_levels = L.orc_num_levels(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_poisson_free(self._h)
+            self._h = None
+
+    def leaf_count(self, level=0):
+        return lib().orc_level_leaf_count(self._h, level)
+
+    def ndof(self, level=0):
+        return lib().orc_level_ndof(self._h, level)
+
+    def topology(self, level=0):
+        n = self.leaf_count(level)
+        o = np.zeros((n, 3), np.int32); m = np.zeros((n, 8), np.uint64)
+        lib().orc_level_topology(self._h, level, o, m)
+        return o, m
+
+    def coefficients(self, level=0):
+        n = self.leaf_count(level)
+        arr = [np.zeros((n, 512), np.float32) for _ in range(4)]
+        flags = np.zeros(n, np.uint8)
+        lib().orc_level_coefficients(self._h, level, *arr, flags)
+        return arr, flags
+
+    def defaults(self, level=0):
+        d = np.zeros(4, np.float32)
+        lib().orc_level_defaults(self._h, level, d)
+        return d
+
+    def zeros(self, level=0):
+        return np.zeros((self.leaf_count(level), 512), np.float32)
+
+    def build_rhs(self, face_weights, vx, vy, vz, solid_velocity):
+        out = self.zeros(0)
+        lib().orc_build_rhs(self._h, *_grid_args(face_weights), face_weights.background,
+                            *_grid_args(vx), float(vx.background[0]),
+                            *_grid_args(vy), float(vy.background[0]),
+                            *_grid_args(vz), float(vz.background[0]),
+                            *_grid_args(solid_velocity), solid_velocity.background, out)
+        return out
+
+    def apply(self, level, mode, lhs, rhs=None, weight=6.0 / 7.0, w_sor=1.2):
+        out = self.zeros(level)
+        rhs = lhs if rhs is None else rhs
+        lib().orc_apply(self._h, level, MODES[mode], weight, w_sor,
+                        np.ascontiguousarray(lhs, np.float32), np.ascontiguousarray(rhs, np.float32), out)
+        return out
+
+    def first_jacobi(self, level, rhs, weight):
+        out = self.zeros(level)
+        lib().orc_first_jacobi(self._h, level, weight, np.ascontiguousarray(rhs, np.float32), out)
+        return out
+
+    def first_spai0(self, level, rhs):
+        out = self.zeros(level)
+        lib().orc_first_spai0(self._h, level, np.ascontiguousarray(rhs, np.float32), out)
+        return out
+
+    def first_rbgs(self, level, rhs, red_first=True, w_sor=1.2):
+        out = self.zeros(level)
+        lib().orc_first_rbgs(self._h, level, 1 if red_first else 0, w_sor,
+                             np.ascontiguousarray(rhs, np.float32), out)
+        return out
+
+    def restrict(self, fine_level, fine):
+        out = self.zeros(fine_level + 1)
+        lib().orc_restrict(self._h, fine_level, np.ascontiguousarray(fine, np.float32), out)
+        return out
+
+    def prolongate(self, fine_level, coarse, fine, alpha=1.0):
+        out = np.array(fine, dtype=np.float32, copy=True)
+        lib().orc_prolongate(self._h, fine_level, np.ascontiguousarray(coarse, np.float32), out, alpha)
+        return out
+
+    def coarsest_solve(self, rhs):
+        out = self.zeros(self.num_levels - 1)
+        lib().orc_coarsest_solve(self._h, np.ascontiguousarray(rhs, np.float32), out)
+        return out
+
+    def precondition(self, r, smoother="scheduled_jacobi"):
+        z = self.zeros(0)
+        lib().orc_precondition(self._h, SMOOTHERS[smoother], np.ascontiguousarray(r, np.float32), z)
+        return z
+
+    def _solve(self, fn, x, b, tol, max_iter, smoother):
+        x = np.array(x, dtype=np.float32, copy=True)
+        it = C.c_int(0); res = C.c_float(0)
+        st = fn(self._h, x, np.ascontiguousarray(b, np.float32), float(tol), int(max_iter),
+                SMOOTHERS[smoother], C.byref(it), C.byref(res))
+        return x, int(st), int(it.value), float(res.value)
+
+    def solve_pcg(self, x, b, tol=1e-7, max_iter=100, smoother="scheduled_jacobi"):
+        return self._solve(lib().orc_solve_pcg, x, b, tol, max_iter, smoother)
+
+    def solve_mg(self, x, b, tol=1e-7, max_iter=100, smoother="scheduled_jacobi"):
+        return self._solve(lib().orc_solve_mg, x, b, tol, max_iter, smoother)
+
+    def abs_max(self, v, level=0):
+        return float(lib().orc_abs_max(self._h, level, np.ascontiguousarray(v, np.float32)))
+
+    def dot(self, a, b, level=0):
+        return float(lib().orc_dot(self._h, level, np.ascontiguousarray(a, np.float32),
+                                   np.ascontiguousarray(b, np.float32)))
+
+    def triplets(self, level):
+        n = lib().orc_triplets(self._h, level, None, None, None)
+        r = np.zeros(n, np.int32); c = np.zeros(n, np.int32); v = np.zeros(n, np.float32)
+        lib().orc_triplets(self._h, level, r.ctypes.data, c.ctypes.data, v.ctypes.data)
+        return r, c, v
+
+    def dof_index(self, level=0):
+        out = np.zeros((self.leaf_count(level), 512), np.int32)
+        lib().orc_dof_index(self._h, level, out)
+        return out
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))

@@ -1,0 +1,105 @@
+"""ctypes loader for libuaamg_b200.so (the C ABI declared in include/uaamg.h).
+
+There is no CPU fallback: importing the solver classes without the built CUDA
+library raises, so a missing extension can never silently turn into a
+different code path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libuaamg_b200.so")
+
+UAAMG_SUCCESS = 0
+UAAMG_FAILED = 1
+
+
+class UaamgError(RuntimeError):
+    pass
+
+
+class LeafGridC(C.Structure):
+    _fields_ = [
+        ("leaf_count", C.c_int64),
+        ("origins", C.c_void_p),
+        ("masks", C.c_void_p),
+        ("values", C.c_void_p),
+        ("components", C.c_int32),
+        ("values_on_device", C.c_int32),
+        ("background", C.c_float * 3),
+    ]
+
+
+_lib = None
+
+# (name, restype, argtypes) of every exported entry point in include/uaamg.h
+vp, i32, i64, f32 = C.c_void_p, C.c_int, C.c_int64, C.c_float
+pLG = C.POINTER(LeafGridC)
+EXPORTS = [
+    ("uaamg_poisson_create", i32, [pLG, pLG, f32, f32, C.POINTER(vp)]),
+    ("uaamg_poisson_destroy", i32, [vp]),
+    ("uaamg_poisson_set_smoother", i32, [vp, i32]),
+    ("uaamg_poisson_set_max_iterations", i32, [vp, i32]),
+    ("uaamg_poisson_set_relative_tolerance", i32, [vp, f32]),
+    ("uaamg_poisson_iterations", i32, [vp]),
+    ("uaamg_poisson_final_residual", f32, [vp]),
+    ("uaamg_poisson_num_levels", i32, [vp]),
+    ("uaamg_poisson_num_dof", i64, [vp, i32]),
+    ("uaamg_poisson_leaf_count", i64, [vp, i32]),
+    ("uaamg_poisson_dof_topology", i32, [vp, i32, vp, vp]),
+    ("uaamg_poisson_dof_index", i32, [vp, i32, vp]),
+    ("uaamg_poisson_build_rhs", i32, [vp, pLG, pLG, pLG, pLG, pLG, f32, vp]),
+    ("uaamg_poisson_build_rhs_device", i32, [vp, pLG, pLG, pLG, pLG, pLG, f32, vp]),
+    ("uaamg_poisson_solve_pcg", i32, [vp, vp, vp, C.POINTER(C.c_int)]),
+    ("uaamg_poisson_solve_pcg_device", i32, [vp, vp, vp, C.POINTER(C.c_int)]),
+    ("uaamg_poisson_solve_mg", i32, [vp, vp, vp, C.POINTER(C.c_int)]),
+    ("uaamg_poisson_solve_mg_device", i32, [vp, vp, vp, C.POINTER(C.c_int)]),
+    ("uaamg_poisson_level_apply", i32, [vp, i32, i32, f32, f32, vp, vp, vp]),
+    ("uaamg_poisson_level_first_sweep", i32, [vp, i32, i32, f32, f32, vp, vp]),
+    ("uaamg_poisson_level_restrict", i32, [vp, i32, vp, vp]),
+    ("uaamg_poisson_level_prolongate", i32, [vp, i32, vp, vp, f32]),
+    ("uaamg_poisson_level_coefficients", i32, [vp, i32, vp, vp, vp, vp, vp]),
+    ("uaamg_poisson_coarsest_solve", i32, [vp, vp, vp]),
+    ("uaamg_poisson_precondition", i32, [vp, vp, vp]),
+    ("uaamg_poisson_set_stream", i32, [vp, vp]),
+    ("uaamg_poisson_set_graph_mode", i32, [vp, i32]),
+    ("uaamg_poisson_kernel_launches", i64, [vp]),
+    ("uaamg_last_error", C.c_char_p, []),
+    ("uaamg_device_count", i32, []),
+]
+
+
+def lib():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise UaamgError(f"CUDA library not built: {LIB_PATH} (run __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in EXPORTS:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str) -> int:
+    if rc < 0:
+        msg = lib().uaamg_last_error().decode(errors="replace")
+        raise UaamgError(f"{what} failed ({rc}): {msg}")
+    return rc
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array (host) or a torch tensor (host or device)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    return a.data_ptr()

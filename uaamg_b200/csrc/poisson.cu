@@ -1,0 +1,1393 @@
+// poisson.cu -- host side of the B200 UAAMG-PCG pressure solver and its C ABI.
+//
+// What runs where
+//  * host (C++): leaf ordering, DOF-leaf compaction, neighbour / child tables
+//    and the coarse-level masks (bit operations on 64-byte masks; O(leaves)),
+//    then one upload of all tables.
+//  * device: every numeric step -- level-0 coefficients, Galerkin coarsening,
+//    trimming, SPAI0, the coarsest explicit matrix, right-hand side, and the
+//    whole PCG: the W-cycle preconditioner and the CG vector steps keep all
+//    scalars in device memory, and the iteration runs as a CUDA graph with a
+//    conditional WHILE node, so a solve is a single graph launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/uaamg.h"
+#include "common.cuh"
+#include "poisson_build.cuh"
+#include "poisson_kernels.cuh"
+
+using namespace uaamg;
+
+// ---------------------------------------------------------------------------
+// errors
+static thread_local std::string g_last_error;
+static void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+struct UaamgError {
+    int code;
+};
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            throw UaamgError{e_ == cudaErrorMemoryAllocation ? UAAMG_ERR_OUT_OF_MEMORY : UAAMG_ERR_CUDA}; \
+        }                                                                                         \
+    } while (0)
+#define CHECK_LAUNCH() CK(cudaGetLastError())
+
+// ---------------------------------------------------------------------------
+// host-side topology helpers
+namespace {
+
+struct VdbKey {
+    int32_t k[5];
+};
+// OpenVDB tree order of a leaf origin (5-4-3 tree): RootNode std::map keyed by
+// the 4096^3 tile origin (compared x, y, z), then the child offsets of the two
+// internal node levels.  Same leaf order as LeafManager, hence the same DOF
+// numbering as setDofIndex.
+static inline VdbKey vdb_key(const int32_t* o) {
+    VdbKey r;
+    r.k[0] = o[0] & ~4095;
+    r.k[1] = o[1] & ~4095;
+    r.k[2] = o[2] & ~4095;
+    r.k[3] = (((o[0] & 4095) >> 7) << 10) | (((o[1] & 4095) >> 7) << 5) | ((o[2] & 4095) >> 7);
+    r.k[4] = (((o[0] & 127) >> 3) << 8) | (((o[1] & 127) >> 3) << 4) | ((o[2] & 127) >> 3);
+    return r;
+}
+static inline bool key_less(const VdbKey& a, const VdbKey& b) {
+    for (int c = 0; c < 5; ++c) {
+        if (a.k[c] != b.k[c]) return a.k[c] < b.k[c];
+    }
+    return false;
+}
+
+struct HostMap {  // dense leaf-index volume over the bounding box
+    int lo[3] = {0, 0, 0}, dim[3] = {0, 0, 0};
+    std::vector<int32_t> idx;
+    void build(int64_t n, const int32_t* org, int pad = 0) {
+        idx.clear();
+        if (n <= 0) { dim[0] = dim[1] = dim[2] = 0; return; }
+        int mn[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, mx[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+        for (int64_t i = 0; i < n; ++i)
+            for (int c = 0; c < 3; ++c) {
+                int v = org[3 * i + c] >> 3;
+                mn[c] = std::min(mn[c], v);
+                mx[c] = std::max(mx[c], v);
+            }
+        int64_t tot = 1;
+        for (int c = 0; c < 3; ++c) {
+            lo[c] = mn[c] - pad;
+            dim[c] = mx[c] - mn[c] + 1 + 2 * pad;
+            tot *= dim[c];
+        }
+        if (tot > (int64_t(1) << 31)) {
+            set_error("leaf bounding box too large for the dense leaf map (%lld cells)", (long long)tot);
+            throw UaamgError{UAAMG_ERR_DOMAIN_TOO_LARGE};
+        }
+        idx.assign((size_t)tot, -1);
+        for (int64_t i = 0; i < n; ++i) idx[cell(org[3 * i] >> 3, org[3 * i + 1] >> 3, org[3 * i + 2] >> 3)] = (int32_t)i;
+    }
+    inline int64_t cell(int a, int b, int c) const {
+        return ((int64_t)(a - lo[0]) * dim[1] + (b - lo[1])) * dim[2] + (c - lo[2]);
+    }
+    inline int32_t find_leaf(int lx, int ly, int lz) const {  // leaf coordinates (origin >> 3)
+        if (idx.empty()) return -1;
+        int a = lx - lo[0], b = ly - lo[1], c = lz - lo[2];
+        if ((unsigned)a >= (unsigned)dim[0] || (unsigned)b >= (unsigned)dim[1] || (unsigned)c >= (unsigned)dim[2]) return -1;
+        return idx[((int64_t)a * dim[1] + b) * dim[2] + c];
+    }
+};
+
+struct HostLevel {
+    int nl = 0;
+    int64_t ndof = 0;
+    std::vector<int32_t> org;     // [nl][3]
+    std::vector<uint64_t> mask;   // [nl][8]
+    std::vector<int32_t> nbr;     // [nl][6]
+    std::vector<int32_t> child;   // [nl][8]
+    std::vector<int32_t> parent;  // [nl]
+    std::vector<uint8_t> octant;  // [nl]
+    std::vector<int32_t> dof_base;
+    HostMap map;
+    float dt = 0, dx = 0;
+};
+
+static void finalize_host_level(HostLevel& L) {
+    L.map.build(L.nl, L.org.data());
+    L.nbr.assign((size_t)L.nl * 6, -1);
+    for (int i = 0; i < L.nl; ++i) {
+        const int32_t* o = &L.org[3 * i];
+        for (int d = 0; d < 6; ++d) {
+            int p[3] = {o[0] >> 3, o[1] >> 3, o[2] >> 3};
+            p[d >> 1] += (d & 1) ? 1 : -1;
+            L.nbr[6 * i + d] = L.map.find_leaf(p[0], p[1], p[2]);
+        }
+    }
+    L.dof_base.resize(L.nl);
+    int64_t acc = 0;
+    for (int i = 0; i < L.nl; ++i) {
+        L.dof_base[i] = (int32_t)acc;
+        for (int w = 0; w < 8; ++w) acc += __builtin_popcountll(L.mask[8 * i + w]);
+    }
+    L.ndof = acc;
+}
+
+// coarse level topology from the fine level (TouchCoarseLeafReducer,
+// SIMD_UAAMG_Ops.h:4-38, and the coarse DOF rule of initializeFromFineLevel,
+// simd_vdb_poisson.cpp:283-311: a coarse voxel is a DOF if any of its 2x2x2
+// fine voxels is).
+static void coarsen_topology(HostLevel& F, HostLevel& C) {
+    C.dt = F.dt;
+    C.dx = 2.0f * F.dx;
+    std::vector<std::pair<VdbKey, int>> keys(F.nl);
+    std::vector<int32_t> corg((size_t)F.nl * 3);
+    for (int i = 0; i < F.nl; ++i) {
+        for (int c = 0; c < 3; ++c) corg[3 * i + c] = (F.org[3 * i + c] / 2) & ~7;
+        keys[i] = {vdb_key(&corg[3 * i]), i};
+    }
+    std::sort(keys.begin(), keys.end(), [](const std::pair<VdbKey, int>& a, const std::pair<VdbKey, int>& b) {
+        return key_less(a.first, b.first);
+    });
+    std::vector<int32_t> uorg;
+    for (int i = 0; i < F.nl; ++i) {
+        if (i > 0 && !key_less(keys[i - 1].first, keys[i].first)) continue;
+        const int32_t* o = &corg[3 * keys[i].second];
+        uorg.insert(uorg.end(), o, o + 3);
+    }
+    int nu = (int)(uorg.size() / 3);
+    std::vector<uint64_t> cmask((size_t)nu * 8, 0);
+    std::vector<int32_t> child((size_t)nu * 8, -1);
+    for (int i = 0; i < nu; ++i) {
+        for (int a = 0; a < 8; ++a) {
+            int fo[3] = {2 * uorg[3 * i] + ((a >> 2) & 1) * 8, 2 * uorg[3 * i + 1] + ((a >> 1) & 1) * 8,
+                         2 * uorg[3 * i + 2] + (a & 1) * 8};
+            int fl = F.map.find_leaf(fo[0] >> 3, fo[1] >> 3, fo[2] >> 3);
+            child[8 * i + a] = fl;
+            if (fl < 0) continue;
+            const int ox = (a >> 2) & 1, oy = (a >> 1) & 1, oz = a & 1;
+            // fine word x holds the (y,z) plane; OR pairs of planes, then pairs in y and z
+            for (int px = 0; px < 4; ++px) {
+                uint64_t p = F.mask[8 * fl + 2 * px] | F.mask[8 * fl + 2 * px + 1];
+                p |= (p >> 1);  // z pairs (bit z and z+1 of a row)
+                p |= (p >> 8);  // y pairs
+                uint64_t& w = cmask[8 * i + ox * 4 + px];
+                for (int yy = 0; yy < 4; ++yy)
+                    for (int zz = 0; zz < 4; ++zz)
+                        if ((p >> (16 * yy + 2 * zz)) & 1ull) w |= 1ull << ((oy * 4 + yy) * 8 + oz * 4 + zz);
+            }
+        }
+    }
+    // drop leaves without DOF
+    C.org.clear(); C.mask.clear(); C.child.clear();
+    for (int i = 0; i < nu; ++i) {
+        uint64_t any = 0;
+        for (int w = 0; w < 8; ++w) any |= cmask[8 * i + w];
+        if (!any) continue;
+        C.org.insert(C.org.end(), &uorg[3 * i], &uorg[3 * i] + 3);
+        C.mask.insert(C.mask.end(), &cmask[8 * i], &cmask[8 * i] + 8);
+        C.child.insert(C.child.end(), &child[8 * i], &child[8 * i] + 8);
+    }
+    C.nl = (int)(C.org.size() / 3);
+    finalize_host_level(C);
+    F.parent.assign(F.nl, -1);
+    F.octant.assign(F.nl, 0);
+    for (int i = 0; i < C.nl; ++i)
+        for (int a = 0; a < 8; ++a) {
+            int fl = C.child[8 * i + a];
+            if (fl >= 0) { F.parent[fl] = i; F.octant[fl] = (uint8_t)a; }
+        }
+}
+
+// ---------------------------------------------------------------------------
+struct DevGrid {  // device copy of an input grid + its leaf map
+    DGrid g{};
+    void* mem = nullptr;
+};
+
+}  // namespace
+
+struct LevelDev {
+    DLevel L{};
+    float* lhs = nullptr;
+    float* rhs = nullptr;
+    float* tmp = nullptr;
+    float* spai0 = nullptr;
+    uint32_t* flags = nullptr;
+    int* spai0_ready = nullptr;
+    int* dof_base = nullptr;
+    int* org = nullptr;
+    float w_sor = 1.2f;
+    float dt = 0, dx = 0;
+};
+
+struct uaamg_poisson {
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaStream_t body_stream = nullptr;
+    std::vector<HostLevel> host;
+    std::vector<LevelDev> lv;
+    int nlev = 0;
+    // hierarchy memory (one allocation)
+    char* dmem = nullptr;
+    size_t dmem_bytes = 0;
+    // coarsest
+    DCoarsest C{};
+    // PCG
+    float *x = nullptr, *b = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
+    double* partials = nullptr;
+    PcgState* st = nullptr;
+    PcgState* st_host = nullptr;  // pinned
+    float* scalar_dev = nullptr;
+    float* scalar_host = nullptr;  // pinned
+    // options
+    int smoother = UAAMG_SMOOTHER_SCHEDULED_RELAXED_JACOBI;
+    int max_iter = 100;
+    float rel_tol = 1e-7f;
+    int use_graph = 1;
+    // graph
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    int graph_key = -1;
+    int64_t body_launches = 0, setup_launches = 0, finish_launches = 0;
+    int64_t launches = 0;
+    int64_t last_launches = 0;
+    int iterations = 0;
+    float final_residual = 0.f;
+    bool spai0_built = false;
+    float dt = 0, dx = 0;
+};
+
+namespace {
+
+template <typename T>
+static T* carve(char*& cur, size_t count) {
+    size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(cur);
+    cur += bytes;
+    return p;
+}
+static size_t carve_size(size_t count, size_t elem) { return (count * elem + 255) & ~size_t(255); }
+
+static void upload_grid(uaamg_poisson* h, const uaamg_leaf_grid* gr, DevGrid& dg, HostMap& map,
+                        std::vector<void*>& tofree) {
+    map.build(gr->leaf_count, gr->origins);
+    dg.g = DGrid{};
+    dg.g.comps = gr->components;
+    dg.g.bg0 = gr->background[0];
+    dg.g.bg1 = gr->components > 1 ? gr->background[1] : 0.f;
+    dg.g.bg2 = gr->components > 2 ? gr->background[2] : 0.f;
+    if (gr->leaf_count == 0) return;
+    size_t mapn = map.idx.size();
+    size_t vbytes = (size_t)gr->leaf_count * UAAMG_LEAF * gr->components * sizeof(float);
+    size_t total = carve_size(mapn, 4) + (gr->values_on_device ? 0 : carve_size(vbytes, 1));
+    void* mem = nullptr;
+    CK(cudaMallocAsync(&mem, total, h->stream));
+    tofree.push_back(mem);
+    char* cur = (char*)mem;
+    int* dmap = carve<int>(cur, mapn);
+    CK(cudaMemcpyAsync(dmap, map.idx.data(), mapn * 4, cudaMemcpyHostToDevice, h->stream));
+    const float* vals = gr->values;
+    if (!gr->values_on_device) {
+        float* dv = carve<float>(cur, vbytes / 4);
+        CK(cudaMemcpyAsync(dv, gr->values, vbytes, cudaMemcpyHostToDevice, h->stream));
+        vals = dv;
+    }
+    dg.g.val = vals;
+    dg.g.map = dmap;
+    dg.g.lo0 = map.lo[0]; dg.g.lo1 = map.lo[1]; dg.g.lo2 = map.lo[2];
+    dg.g.d0 = map.dim[0]; dg.g.d1 = map.dim[1]; dg.g.d2 = map.dim[2];
+}
+
+static void check_grid(const uaamg_leaf_grid* g, int comps, const char* name) {
+    if (!g) { set_error("%s is NULL", name); throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT}; }
+    if (g->components != comps) {
+        set_error("%s must have %d component(s), got %d", name, comps, g->components);
+        throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT};
+    }
+    if (g->leaf_count < 0 || (g->leaf_count > 0 && (!g->origins || !g->values))) {
+        set_error("%s has no origins/values", name);
+        throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT};
+    }
+    for (int64_t i = 0; i < 3 * g->leaf_count; ++i)
+        if (g->origins[i] & 7) {
+            set_error("%s: leaf origins must be multiples of 8", name);
+            throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT};
+        }
+}
+
+static LevelOut level_out(LevelDev& d) {
+    LevelOut O;
+    O.diag = const_cast<float*>(d.L.diag);
+    O.cx = const_cast<float*>(d.L.cx);
+    O.cy = const_cast<float*>(d.L.cy);
+    O.cz = const_cast<float*>(d.L.cz);
+    O.invdiag = const_cast<float*>(d.L.invdiag);
+    O.flags = d.flags;
+    // trimDefaultNodes (simd_vdb_poisson.cpp:1756-1770)
+    float term = -d.dt / (d.dx * d.dx);
+    float diagonalTerm = -6.0f * term;
+    O.def_diag = diagonalTerm;
+    O.def_face = term;
+    O.eps_diag = fabsf(diagonalTerm * 1e-5f);
+    O.eps_face = fabsf(term * 1e-5f);
+    O.inv_bg = 1.0f / d.L.def_diag;
+    O.def_invdiag = d.L.def_invdiag;
+    return O;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// hierarchy construction
+static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const uaamg_leaf_grid* fw, float dt,
+                            float dx) {
+    check_grid(phi, 1, "liquid_phi");
+    check_grid(fw, 3, "face_weights");
+    if (!(dx > 0.f)) { set_error("dx must be positive"); throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT}; }
+    h->dt = dt;
+    h->dx = dx;
+    cudaStream_t s = h->stream;
+    std::vector<void*> tofree;
+    const int64_t nphi = phi->leaf_count;
+    h->host.clear();
+    h->host.reserve(32);  // references into it are held while levels are appended
+    h->host.emplace_back();
+    HostLevel& L0 = h->host[0];
+    L0.dt = dt;
+    L0.dx = dx;
+    if (nphi > 0) {
+        // ---- inputs to the device
+        HostMap phimap, fwmap;
+        DevGrid dphi, dfw;
+        upload_grid(h, phi, dphi, phimap, tofree);
+        upload_grid(h, fw, dfw, fwmap, tofree);
+        size_t extra = carve_size((size_t)nphi * 8, 8) * 2 + carve_size((size_t)nphi * 3, 4);
+        void* mem = nullptr;
+        CK(cudaMallocAsync(&mem, extra, s));
+        tofree.push_back(mem);
+        char* cur = (char*)mem;
+        uint64_t* dphimask = carve<uint64_t>(cur, (size_t)nphi * 8);
+        uint64_t* ddofmask = carve<uint64_t>(cur, (size_t)nphi * 8);
+        int* dphiorg = carve<int>(cur, (size_t)nphi * 3);
+        CK(cudaMemcpyAsync(dphiorg, phi->origins, (size_t)nphi * 12, cudaMemcpyHostToDevice, s));
+        const uint64_t* pm = nullptr;
+        if (phi->masks) {
+            CK(cudaMemcpyAsync(dphimask, phi->masks, (size_t)nphi * 64, cudaMemcpyHostToDevice, s));
+            pm = dphimask;
+        }
+        const float dtOverDxSqr = dt / (dx * dx);
+        k_finest_mask<<<(unsigned)nphi, 128, 0, s>>>(dphi.g, pm, dphiorg, dfw.g, dtOverDxSqr, ddofmask);
+        CHECK_LAUNCH();
+        std::vector<uint64_t> dofmask((size_t)nphi * 8);
+        CK(cudaMemcpyAsync(dofmask.data(), ddofmask, (size_t)nphi * 64, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        // ---- level-0 DOF leaves in tree order
+        std::vector<std::pair<VdbKey, int>> keys;
+        keys.reserve(nphi);
+        for (int64_t i = 0; i < nphi; ++i) {
+            uint64_t any = 0;
+            for (int w = 0; w < 8; ++w) any |= dofmask[8 * i + w];
+            if (any) keys.push_back({vdb_key(&phi->origins[3 * i]), (int)i});
+        }
+        std::sort(keys.begin(), keys.end(), [](const std::pair<VdbKey, int>& a, const std::pair<VdbKey, int>& b) {
+            return key_less(a.first, b.first);
+        });
+        std::vector<int32_t> src(keys.size());
+        for (size_t i = 0; i < keys.size(); ++i) {
+            int sidx = keys[i].second;
+            src[i] = sidx;
+            L0.org.insert(L0.org.end(), &phi->origins[3 * sidx], &phi->origins[3 * sidx] + 3);
+            L0.mask.insert(L0.mask.end(), &dofmask[8 * (size_t)sidx], &dofmask[8 * (size_t)sidx] + 8);
+        }
+        L0.nl = (int)keys.size();
+        finalize_host_level(L0);
+        // ---- coarse topology: constructMultigridHierarchy (.cpp:1813-1842)
+        while (h->host.back().ndof > 4000 && h->host.size() < 32) {
+            h->host.emplace_back();
+            HostLevel& F = h->host[h->host.size() - 2];
+            HostLevel& C = h->host.back();
+            coarsen_topology(F, C);
+        }
+        const int nlev = (int)h->host.size();
+        // ---- device memory for the whole hierarchy
+        size_t bytes = 0;
+        for (int l = 0; l < nlev; ++l) {
+            const HostLevel& H = h->host[l];
+            size_t n = (size_t)H.nl;
+            bytes += carve_size(n * 8, 8) + carve_size(n * 6, 4) + carve_size(n * 8, 4) + carve_size(n, 4) +
+                     carve_size(n, 1) + carve_size(n, 4) + carve_size(n * 3, 4) + carve_size(n, 4) + carve_size(1, 4);
+            bytes += 10 * carve_size(n * UAAMG_LEAF, 4);  // diag cx cy cz invdiag spai0 lhs rhs tmp (+1 spare)
+        }
+        const HostLevel& HC = h->host.back();
+        size_t nc = (size_t)HC.ndof;
+        if (nc > (size_t)CG_THREADS * CG_ROWS) {
+            set_error("coarsening stalled: %zu DOF on the coarsest level (max %d)", nc, CG_THREADS * CG_ROWS);
+            throw UaamgError{UAAMG_ERR_DOMAIN_TOO_LARGE};
+        }
+        bytes += carve_size(nc, 4) * 3 + carve_size(nc * 6, 4) * 2;
+        size_t n0 = (size_t)L0.nl * UAAMG_LEAF;
+        bytes += 6 * carve_size(n0, 4);  // x b r z p q
+        bytes += carve_size(std::max<size_t>((size_t)L0.nl, 1) + 64, 8);
+        bytes += carve_size(sizeof(PcgState), 1) + carve_size(64, 4) + carve_size(src.size(), 4);
+        CK(cudaMalloc(&h->dmem, bytes));
+        h->dmem_bytes = bytes;
+        CK(cudaMemsetAsync(h->dmem, 0, bytes, s));
+        char* cur2 = h->dmem;
+        // topology staging (pinned) so the uploads are plain DMA
+        std::vector<std::pair<void*, std::pair<const void*, size_t>>> ups;
+        h->lv.assign(nlev, LevelDev());
+        for (int l = 0; l < nlev; ++l) {
+            HostLevel& H = h->host[l];
+            LevelDev& D = h->lv[l];
+            size_t n = (size_t)H.nl;
+            D.dt = H.dt;
+            D.dx = H.dx;
+            uint64_t* m = carve<uint64_t>(cur2, n * 8);
+            int* nb = carve<int>(cur2, n * 6);
+            int* ch = carve<int>(cur2, n * 8);
+            int* par = carve<int>(cur2, n);
+            uint8_t* oc = carve<uint8_t>(cur2, n);
+            D.dof_base = carve<int>(cur2, n);
+            D.org = carve<int>(cur2, n * 3);
+            D.flags = carve<uint32_t>(cur2, n);
+            D.spai0_ready = carve<int>(cur2, 1);
+            float* dg = carve<float>(cur2, n * UAAMG_LEAF);
+            float* cx = carve<float>(cur2, n * UAAMG_LEAF);
+            float* cy = carve<float>(cur2, n * UAAMG_LEAF);
+            float* cz = carve<float>(cur2, n * UAAMG_LEAF);
+            float* iv = carve<float>(cur2, n * UAAMG_LEAF);
+            D.spai0 = carve<float>(cur2, n * UAAMG_LEAF);
+            D.lhs = carve<float>(cur2, n * UAAMG_LEAF);
+            D.rhs = carve<float>(cur2, n * UAAMG_LEAF);
+            D.tmp = carve<float>(cur2, n * UAAMG_LEAF);
+            carve<float>(cur2, n * UAAMG_LEAF);
+            ups.push_back({m, {H.mask.data(), n * 64}});
+            ups.push_back({nb, {H.nbr.data(), n * 24}});
+            if (!H.child.empty()) ups.push_back({ch, {H.child.data(), n * 32}});
+            if (!H.parent.empty()) ups.push_back({par, {H.parent.data(), n * 4}});
+            if (!H.octant.empty()) ups.push_back({oc, {H.octant.data(), n}});
+            ups.push_back({D.dof_base, {H.dof_base.data(), n * 4}});
+            ups.push_back({D.org, {H.org.data(), n * 12}});
+            const float t = H.dt / (H.dx * H.dx);  // LaplacianApplySIMD ctor (.cpp:1045-1065)
+            DLevel& L = D.L;
+            L.nl = (int)n;
+            L.mask = m; L.nbr = nb; L.child = ch; L.parent = par; L.octant = oc;
+            L.diag = dg; L.cx = cx; L.cy = cy; L.cz = cz; L.invdiag = iv; L.spai0 = D.spai0; L.flags = D.flags;
+            L.def_face = -t;
+            L.def_diag = 6.f * t;
+            L.def_invdiag = 1.0f / (6.f * t);
+            L.def_spai0 = 1.0f / (7.f * t);
+        }
+        h->C.n = (int)nc;
+        int* dslot = carve<int>(cur2, nc);
+        float* cdiag = carve<float>(cur2, nc);
+        float* cinvd = carve<float>(cur2, nc);
+        int* ccol = carve<int>(cur2, nc * 6);
+        float* cval = carve<float>(cur2, nc * 6);
+        h->C.dof_slot = dslot; h->C.diag = cdiag; h->C.invd = cinvd; h->C.col = ccol; h->C.val = cval;
+        h->x = carve<float>(cur2, n0);
+        h->b = carve<float>(cur2, n0);
+        h->r = carve<float>(cur2, n0);
+        h->z = carve<float>(cur2, n0);
+        h->p = carve<float>(cur2, n0);
+        h->q = carve<float>(cur2, n0);
+        h->partials = carve<double>(cur2, std::max<size_t>((size_t)L0.nl, 1) + 64);
+        h->st = reinterpret_cast<PcgState*>(carve<char>(cur2, sizeof(PcgState)));
+        h->scalar_dev = carve<float>(cur2, 64);
+        int* dsrc = carve<int>(cur2, src.size());
+        ups.push_back({dsrc, {src.data(), src.size() * 4}});
+        // one pinned staging buffer for all tables
+        size_t tot = 0;
+        for (auto& u : ups) tot += (u.second.second + 15) & ~size_t(15);
+        char* pin = nullptr;
+        CK(cudaMallocHost(&pin, std::max<size_t>(tot, 16)));
+        size_t o = 0;
+        for (auto& u : ups) {
+            memcpy(pin + o, u.second.first, u.second.second);
+            CK(cudaMemcpyAsync(u.first, pin + o, u.second.second, cudaMemcpyHostToDevice, s));
+            o += (u.second.second + 15) & ~size_t(15);
+        }
+        // ---- numeric construction on the device
+        if (L0.nl > 0) {
+            LevelDev& D0 = h->lv[0];
+            k_finest_coef<<<(unsigned)L0.nl, 128, 0, s>>>(dphi.g, dphiorg, dfw.g, dtOverDxSqr, dsrc, D0.L.mask,
+                                                          level_out(D0));
+            CHECK_LAUNCH();
+        }
+        for (int l = 1; l < nlev; ++l) {
+            LevelDev& D = h->lv[l];
+            if (D.L.nl == 0) continue;
+            k_coarsen<<<(unsigned)D.L.nl, 128, 0, s>>>(h->lv[l - 1].L, D.L.child, D.L.mask, level_out(D));
+            CHECK_LAUNCH();
+        }
+        if (h->lv[nlev - 1].L.nl > 0) {
+            LevelDev& D = h->lv[nlev - 1];
+            k_coarsest_ell<<<(unsigned)D.L.nl, 128, 0, s>>>(D.L, D.dof_base, dslot, cdiag, cinvd, ccol, cval);
+            CHECK_LAUNCH();
+        }
+        for (void* pmem : tofree) CK(cudaFreeAsync(pmem, s));
+        tofree.clear();
+        CK(cudaStreamSynchronize(s));
+        cudaFreeHost(pin);
+        h->nlev = nlev;
+    } else {
+        h->nlev = 1;
+        h->lv.assign(1, LevelDev());
+    }
+}
+
+static void ensure_spai0(uaamg_poisson* h) {
+    if (h->spai0_built) return;
+    for (int l = 0; l < h->nlev; ++l) {
+        LevelDev& D = h->lv[l];
+        if (D.L.nl == 0) continue;
+        float bg = D.L.def_diag;  // mDiagonal->background()
+        float defaultSPAI0Val = 6.0f / (7.f * bg);
+        k_spai0<<<(unsigned)D.L.nl, 128, 0, h->stream>>>(D.L, D.spai0, D.flags, defaultSPAI0Val,
+                                                         fabsf(defaultSPAI0Val * 1e-5f));
+        CHECK_LAUNCH();
+    }
+    h->spai0_built = true;
+}
+
+// ---------------------------------------------------------------------------
+// kernel enqueue helpers
+namespace {
+
+struct Enq {
+    uaamg_poisson* h;
+    cudaStream_t s;
+    int64_t count = 0;
+
+    template <int MODE, class Src>
+    void sweep(int l, const Src& src, const float* b, float* out, float w, DotOut dot = DotOut{nullptr, nullptr, nullptr},
+               bool mark_spai0 = false) {
+        LevelDev& D = h->lv[l];
+        float ws = D.w_sor;
+        k_sweep<MODE, Src><<<(unsigned)D.L.nl, 128, 0, s>>>(D.L, src, b, out, w, ws, 1.0f - ws, dot,
+                                                             mark_spai0 ? D.spai0_ready : nullptr);
+        CHECK_LAUNCH();
+        count++;
+    }
+    void restrict_resid(int l, const float* x, const float* b) {
+        LevelDev& D = h->lv[l];
+        k_restrict<true><<<(unsigned)D.L.nl, 128, 0, s>>>(D.L, x, b, h->lv[l + 1].rhs);
+        CHECK_LAUNCH();
+        count++;
+    }
+    void coarsest(const float* rhs, float* out) {
+        if (h->C.n == 0) return;
+        k_coarsest_cg<<<1, CG_THREADS, 0, s>>>(h->C, rhs, out);
+        CHECK_LAUNCH();
+        count++;
+    }
+};
+
+static float sched_weight_precond(int n, int it) {
+    // muCyclePreconditioner's get_scheduled_weight (simd_vdb_poisson.cpp:1848-1866)
+    if (it >= n) return 6.0f / 7.0f;
+    if (n == 1) return 6.0f / 7.0f;
+    if (n == 2) { const float w[2] = {1.7319f, 0.5695f}; return w[it]; }
+    const float w[3] = {2.2473f, 0.8571f, 0.5296f};
+    return w[it];
+}
+static float sched_weight_iter(int n, int it) {
+    // muCycleIterative's get_scheduled_weight (simd_vdb_poisson.cpp:1983-2000)
+    if (it >= n) return 6.0f / 7.0f;
+    if (n == 2) { const float w[2] = {1.7319f, 0.5695f}; return w[it]; }
+    if (n >= 3) { const float w[3] = {2.2473f, 0.8571f, 0.5296f}; return w[it]; }
+    return 6.0f / 7.0f;
+}
+
+}  // namespace
+
+// The materialised z.r for a one-level hierarchy (the coarsest solve is the
+// whole preconditioner, so no sweep is available to carry the dot).
+__global__ void __launch_bounds__(128) k_dot_rho(DLevel L, const float* z, const float* r, double* partials,
+                                                 PcgState* st) {
+    __shared__ double shd[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    float4 a = ld4(z, leaf, t), c = ld4(r, leaf, t);
+    unsigned m = mask4(L.mask, leaf, t);
+    double s = 0;
+    if (m & 1) s += (double)a.x * c.x;
+    if (m & 2) s += (double)a.y * c.y;
+    if (m & 4) s += (double)a.z * c.z;
+    if (m & 8) s += (double)a.w * c.w;
+    double part = block_sum128(s, shd);
+    if (publish_partial(part, partials, &st->ticket[0], &last)) {
+        double tot = gather_sum(partials, shd);
+        if (t == 0) {
+            float rho_new = (float)tot;
+            st->rho_new = rho_new;
+            st->beta = st->first ? 0.f : __fdiv_rn(rho_new, st->rho);
+            st->rho = rho_new;
+            st->ticket[0] = 0;
+        }
+    }
+}
+
+// muCyclePreconditioner<2, skip_first> (simd_vdb_poisson.cpp:1844-1977) at
+// level l: lhs <- M^-1 rhs.  Fusions (bit-identical to the unfused sequence):
+// first sweep from zero + second sweep; residual + restriction;
+// prolongation-add + first post-smoothing sweep; z.r into the last level-0
+// sweep.  The W-cycle's second visit of the coarsest level re-solves the same
+// system from a zero guess, so it is skipped.
+static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool skip_first, DotOut dot) {
+    uaamg_poisson* h = E.h;
+    LevelDev& D = h->lv[l];
+    const int n = 3;
+    const int sm = h->smoother;
+    if (l == h->nlev - 1) {
+        E.coarsest(rhs, lhs);
+        if (dot.r) {
+            k_dot_rho<<<(unsigned)D.L.nl, 128, 0, E.s>>>(D.L, lhs, dot.r, dot.partials, dot.st);
+            CHECK_LAUNCH();
+            E.count++;
+        }
+        return;
+    }
+    float* T = D.tmp;
+    LevelDev& P = h->lv[l + 1];
+    auto wpre = [&](int i) { return sm == UAAMG_SMOOTHER_WEIGHTED_JACOBI ? 6.0f / 7.0f : sched_weight_precond(n, i); };
+    float* cur = nullptr;
+    if (sm == UAAMG_SMOOTHER_RED_BLACK_GAUSS_SEIDEL) {
+        int i0 = 0;
+        if (skip_first) {
+            E.sweep<M_BLACK>(l, SrcFirstRbgs{rhs, D.w_sor, 1}, rhs, lhs, 0.f);
+            i0 = 1;
+        }
+        for (int i = i0; i < n; ++i) {
+            E.sweep<M_RED>(l, SrcPlain{lhs}, rhs, lhs, 0.f);
+            E.sweep<M_BLACK>(l, SrcPlain{lhs}, rhs, lhs, 0.f);
+        }
+        cur = lhs;
+        E.restrict_resid(l, cur, rhs);
+        enqueue_precond(E, l + 1, P.lhs, P.rhs, true, DotOut{nullptr, nullptr, nullptr});
+        if (l + 1 != h->nlev - 1) enqueue_precond(E, l + 1, P.lhs, P.rhs, false, DotOut{nullptr, nullptr, nullptr});
+        // post: (black, red) x n; the first black pass adds the prolongation,
+        // writes T; the last red pass writes back into lhs
+        E.sweep<M_BLACK>(l, SrcProlong{lhs, P.lhs, 1.0f}, rhs, T, 0.f);
+        for (int i = 0; i < n; ++i) {
+            if (i > 0) E.sweep<M_BLACK>(l, SrcPlain{T}, rhs, T, 0.f);
+            if (i < n - 1) E.sweep<M_RED>(l, SrcPlain{T}, rhs, T, 0.f);
+            else E.sweep<M_RED>(l, SrcPlain{T}, rhs, lhs, 0.f, dot);
+        }
+        return;
+    }
+    const bool spai = (sm == UAAMG_SMOOTHER_SPAI0);
+    // pre-smoothing, ends in T
+    if (skip_first) {
+        if (spai) E.sweep<M_SPAI0>(l, SrcFirstSpai0{rhs, D.spai0_ready}, rhs, lhs, 0.f);
+        else E.sweep<M_JACOBI>(l, SrcFirstJacobi{rhs, wpre(0)}, rhs, lhs, wpre(1));
+        if (spai) E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f, DotOut{nullptr, nullptr, nullptr}, true);
+        else E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(2));
+    } else {
+        if (spai) {
+            E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f, DotOut{nullptr, nullptr, nullptr}, true);
+            E.sweep<M_SPAI0>(l, SrcPlain{T}, rhs, lhs, 0.f);
+            E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f);
+        } else {
+            E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(0));
+            E.sweep<M_JACOBI>(l, SrcPlain{T}, rhs, lhs, wpre(1));
+            E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(2));
+        }
+    }
+    cur = T;
+    E.restrict_resid(l, cur, rhs);
+    enqueue_precond(E, l + 1, P.lhs, P.rhs, true, DotOut{nullptr, nullptr, nullptr});
+    if (l + 1 != h->nlev - 1) enqueue_precond(E, l + 1, P.lhs, P.rhs, false, DotOut{nullptr, nullptr, nullptr});
+    // post-smoothing with reversed weights: T(+P x_c) -> lhs -> T -> lhs
+    if (spai) {
+        E.sweep<M_SPAI0>(l, SrcProlong{T, P.lhs, 1.0f}, rhs, lhs, 0.f);
+        E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f);
+        E.sweep<M_SPAI0>(l, SrcPlain{T}, rhs, lhs, 0.f, dot);
+    } else {
+        E.sweep<M_JACOBI>(l, SrcProlong{T, P.lhs, 1.0f}, rhs, lhs, wpre(2));
+        E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(1));
+        E.sweep<M_JACOBI>(l, SrcPlain{T}, rhs, lhs, wpre(0), dot);
+    }
+}
+
+// muCycleIterative<2> (simd_vdb_poisson.cpp:1979-2110): the MG-as-solver
+// cycle; coarse levels start from whatever their lhs holds, as in the reference.
+static void enqueue_mg_cycle(Enq& E, int l, float* lhs, const float* rhs) {
+    uaamg_poisson* h = E.h;
+    LevelDev& D = h->lv[l];
+    const int n = 3;
+    const int sm = h->smoother;
+    float* T = D.tmp;
+    auto w = [&](int i) { return sm == UAAMG_SMOOTHER_WEIGHTED_JACOBI ? 6.0f / 7.0f : sched_weight_iter(n, i); };
+    if (sm == UAAMG_SMOOTHER_RED_BLACK_GAUSS_SEIDEL) D.w_sor = 1.0f;
+    auto smooth = [&](int i, int red_first, float*& cur, float*& oth) {
+        if (sm == UAAMG_SMOOTHER_RED_BLACK_GAUSS_SEIDEL) {
+            if (red_first) { E.sweep<M_RED>(l, SrcPlain{cur}, rhs, cur, 0.f); E.sweep<M_BLACK>(l, SrcPlain{cur}, rhs, cur, 0.f); }
+            else { E.sweep<M_BLACK>(l, SrcPlain{cur}, rhs, cur, 0.f); E.sweep<M_RED>(l, SrcPlain{cur}, rhs, cur, 0.f); }
+        } else if (sm == UAAMG_SMOOTHER_SPAI0) {
+            E.sweep<M_SPAI0>(l, SrcPlain{cur}, rhs, oth, 0.f, DotOut{nullptr, nullptr, nullptr}, true);
+            std::swap(cur, oth);
+        } else {
+            E.sweep<M_JACOBI>(l, SrcPlain{cur}, rhs, oth, w(i));
+            std::swap(cur, oth);
+        }
+    };
+    float* cur = lhs;
+    float* oth = T;
+    if (l == h->nlev - 1) {
+        for (int i = 0; i < 10 * n; ++i) smooth(i, 1, cur, oth);
+        if (cur != lhs) { CK(cudaMemcpyAsync(lhs, cur, (size_t)D.L.nl * UAAMG_LEAF * 4, cudaMemcpyDeviceToDevice, E.s)); }
+        return;
+    }
+    for (int i = 0; i < n; ++i) smooth(i, 1, cur, oth);
+    LevelDev& P = h->lv[l + 1];
+    E.restrict_resid(l, cur, rhs);
+    for (int mu = 0; mu < 2; ++mu) enqueue_mg_cycle(E, l + 1, P.lhs, P.rhs);
+    // prolongation (alpha 0.5) + post-smoothing
+    if (sm == UAAMG_SMOOTHER_RED_BLACK_GAUSS_SEIDEL) {
+        k_materialize<SrcProlong><<<(unsigned)D.L.nl, 128, 0, E.s>>>(D.L, SrcProlong{cur, P.lhs, 0.5f}, oth);
+        CHECK_LAUNCH();
+        E.count++;
+        std::swap(cur, oth);
+        for (int i = 0; i < n; ++i) smooth(n - 1 - i, 0, cur, oth);
+    } else {
+        if (sm == UAAMG_SMOOTHER_SPAI0) E.sweep<M_SPAI0>(l, SrcProlong{cur, P.lhs, 0.5f}, rhs, oth, 0.f);
+        else E.sweep<M_JACOBI>(l, SrcProlong{cur, P.lhs, 0.5f}, rhs, oth, w(n - 1));
+        std::swap(cur, oth);
+        for (int i = 1; i < n; ++i) smooth(n - 1 - i, 0, cur, oth);
+    }
+    if (cur != lhs) CK(cudaMemcpyAsync(lhs, cur, (size_t)D.L.nl * UAAMG_LEAF * 4, cudaMemcpyDeviceToDevice, E.s));
+}
+
+// ---------------------------------------------------------------------------
+// PCG (PoissonSolver::solveMultigridPCG, simd_vdb_poisson.cpp:2155-2226), loop
+// rotated so that the convergence test ends the iteration:
+//   setup:  r = b - A x, nu0, numax                        [k_pcg_init]
+//   while running:
+//     z = M^-1 r, rho_new = z.r, beta, rho                 [W-cycle]
+//     x += alpha_prev p (not in the first pass); p = z + beta p
+//     q = A p, sigma, alpha = rho / sigma
+//     r -= alpha q, nu, convergence / divergence test
+//   finish: x += alpha p when converged or out of iterations
+static void enqueue_setup(Enq& E, cudaGraphConditionalHandle cond, int use_cond) {
+    uaamg_poisson* h = E.h;
+    LevelDev& D0 = h->lv[0];
+    const size_t n0 = (size_t)D0.L.nl * UAAMG_LEAF;
+    CK(cudaMemsetAsync(h->p, 0, n0 * 4, E.s));
+    k_mask_vec<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->x);
+    CHECK_LAUNCH();
+    k_mask_vec<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->b);
+    CHECK_LAUNCH();
+    k_pcg_init<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->x, h->b, h->r, h->partials, h->st, cond, use_cond);
+    CHECK_LAUNCH();
+    E.count += 3;
+}
+static void enqueue_body(Enq& E, cudaGraphConditionalHandle cond, int use_cond) {
+    uaamg_poisson* h = E.h;
+    LevelDev& D0 = h->lv[0];
+    enqueue_precond(E, 0, h->z, h->r, true, DotOut{h->r, h->partials, h->st});
+    k_pcg_update_p<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->z, h->p, h->x, h->st);
+    CHECK_LAUNCH();
+    k_pcg_Ap<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->p, h->q, h->partials, h->st);
+    CHECK_LAUNCH();
+    k_pcg_update_r<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->q, h->r, h->partials, h->st, cond, use_cond);
+    CHECK_LAUNCH();
+    E.count += 3;
+}
+static void enqueue_finish(Enq& E) {
+    uaamg_poisson* h = E.h;
+    LevelDev& D0 = h->lv[0];
+    k_pcg_finish<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->p, h->x, h->st);
+    CHECK_LAUNCH();
+    E.count += 1;
+}
+
+static int graph_key(const uaamg_poisson* h) {
+    int k = h->smoother;
+    for (int l = 0; l < h->nlev; ++l) k = k * 3 + (h->lv[l].w_sor == 1.2f ? 0 : 1);
+    return k;
+}
+
+static void destroy_graph(uaamg_poisson* h) {
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+    h->graph_key = -1;
+}
+
+static void build_graph(uaamg_poisson* h) {
+    destroy_graph(h);
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    Enq E{h, h->stream};
+    CK(cudaStreamBeginCaptureToGraph(h->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+        enqueue_setup(E, cond, 1);
+        h->setup_launches = E.count;
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        cudaGraph_t cg = nullptr;
+        CK(cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &cg, &deps, &ndeps));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t wnode;
+        CK(cudaGraphAddNode(&wnode, cg, deps, ndeps, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamUpdateCaptureDependencies(h->stream, &wnode, 1, cudaStreamSetCaptureDependencies));
+        Enq B{h, h->body_stream};
+        CK(cudaStreamBeginCaptureToGraph(h->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        enqueue_body(B, cond, 1);
+        cudaGraph_t bodyout = nullptr;
+        CK(cudaStreamEndCapture(h->body_stream, &bodyout));
+        h->body_launches = B.count;
+        Enq F{h, h->stream};
+        enqueue_finish(F);
+        h->finish_launches = F.count;
+    } catch (...) {
+        cudaGraph_t dummy = nullptr;
+        cudaStreamEndCapture(h->stream, &dummy);
+        cudaStreamEndCapture(h->body_stream, &dummy);
+        cudaGraphDestroy(g);
+        throw;
+    }
+    cudaGraph_t out = nullptr;
+    CK(cudaStreamEndCapture(h->stream, &out));
+    CK(cudaGraphInstantiate(&h->graph_exec, g, 0));
+    h->graph = g;
+    h->graph_key = graph_key(h);
+}
+
+static void init_state(uaamg_poisson* h) {
+    PcgState s;
+    memset(&s, 0, sizeof(s));
+    s.tol = h->rel_tol;
+    s.max_iter = h->max_iter;
+    *h->st_host = s;
+    CK(cudaMemcpyAsync(h->st, h->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, h->stream));
+}
+
+// x, b (h->x, h->b) already on the device; returns status
+static int run_pcg(uaamg_poisson* h) {
+    if (h->lv[0].L.nl == 0 || h->lv[0].L.nl == 0) {
+        h->iterations = 0;
+        h->final_residual = 0.f;
+        return UAAMG_SUCCESS;
+    }
+    if (h->smoother == UAAMG_SMOOTHER_SPAI0) ensure_spai0(h);
+    init_state(h);
+    int64_t launches = 0;
+    if (h->use_graph) {
+        if (!h->graph_exec || h->graph_key != graph_key(h)) build_graph(h);
+        CK(cudaGraphLaunch(h->graph_exec, h->stream));
+        CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        int iters_run = h->st_host->iter;  // body executions
+        launches = h->setup_launches + (int64_t)iters_run * h->body_launches + h->finish_launches;
+    } else {
+        Enq E{h, h->stream};
+        enqueue_setup(E, 0, 0);
+        CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        while (h->st_host->status == PCG_RUNNING) {
+            enqueue_body(E, 0, 0);
+            CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+        enqueue_finish(E);
+        CK(cudaStreamSynchronize(h->stream));
+        launches = E.count;
+    }
+    h->last_launches = launches;
+    h->launches += launches;
+    const PcgState& s = *h->st_host;
+    h->iterations = s.iterations_taken;
+    h->final_residual = s.nu;
+    return (s.status == PCG_SUCCESS) ? UAAMG_SUCCESS : UAAMG_FAILED;
+}
+
+// PoissonSolver::solvePureMultigrid (simd_vdb_poisson.cpp:2228-2267)
+static int run_mg(uaamg_poisson* h) {
+    LevelDev& D0 = h->lv[0];
+    if (D0.L.nl == 0) { h->iterations = 0; h->final_residual = 0.f; return UAAMG_SUCCESS; }
+    if (h->smoother == UAAMG_SMOOTHER_SPAI0) ensure_spai0(h);
+    Enq E{h, h->stream};
+    k_mask_vec<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->x);
+    k_mask_vec<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->b);
+    E.count += 2;
+    auto resid_norm = [&]() {
+        E.sweep<M_RESIDUAL>(0, SrcPlain{h->x}, h->b, h->r, 0.f);
+        k_absmax<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->r, h->partials, &h->st->ticket[4], h->scalar_dev);
+        CHECK_LAUNCH();
+        E.count++;
+        CK(cudaMemcpyAsync(h->scalar_host, h->scalar_dev, 4, cudaMemcpyDeviceToHost, E.s));
+        CK(cudaStreamSynchronize(E.s));
+        return h->scalar_host[0];
+    };
+    init_state(h);
+    float nu = resid_norm();
+    const float numax = h->rel_tol * nu;
+    int it = 0, status = UAAMG_FAILED;
+    if (nu <= numax) {
+        status = UAAMG_SUCCESS;
+    } else {
+        float nu_old = nu;
+        for (; it < h->max_iter; ++it) {
+            enqueue_mg_cycle(E, 0, h->x, h->b);
+            nu_old = nu;
+            nu = resid_norm();
+            if (nu <= numax) { status = UAAMG_SUCCESS; break; }
+            if (nu > nu_old && it > 8) { status = UAAMG_FAILED; break; }
+        }
+    }
+    h->iterations = it;
+    h->final_residual = nu;
+    h->last_launches = E.count;
+    h->launches += E.count;
+    return status;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+#define ABI_BEGIN try {
+#define ABI_END                                            \
+    }                                                      \
+    catch (const UaamgError& e) { return e.code; }         \
+    catch (const std::bad_alloc&) {                        \
+        set_error("host out of memory");                   \
+        return UAAMG_ERR_OUT_OF_MEMORY;                    \
+    }                                                      \
+    catch (...) {                                          \
+        set_error("unexpected exception");                 \
+        return UAAMG_ERR_CUDA;                             \
+    }
+
+static void require(bool c, const char* msg) {
+    if (!c) { set_error("%s", msg); throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT}; }
+}
+static size_t vec_bytes(const uaamg_poisson* h, int level) { return (size_t)h->lv[level].L.nl * UAAMG_LEAF * 4; }
+
+extern "C" {
+
+const char* uaamg_last_error(void) { return g_last_error.c_str(); }
+
+int uaamg_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+int uaamg_poisson_create(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights, float dt, float dx,
+                         uaamg_poisson** out) {
+    if (!out) { set_error("out is NULL"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_error("no CUDA device");
+        return UAAMG_ERR_NO_DEVICE;
+    }
+    uaamg_poisson* h = new (std::nothrow) uaamg_poisson();
+    if (!h) { set_error("host out of memory"); return UAAMG_ERR_OUT_OF_MEMORY; }
+    try {
+        CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking));
+        h->stream = h->own_stream;
+        CK(cudaMallocHost(&h->st_host, sizeof(PcgState)));
+        CK(cudaMallocHost(&h->scalar_host, 64));
+        build_hierarchy(h, liquid_phi, face_weights, dt, dx);
+    } catch (const UaamgError& e) {
+        uaamg_poisson_destroy(h);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        uaamg_poisson_destroy(h);
+        set_error("host out of memory");
+        return UAAMG_ERR_OUT_OF_MEMORY;
+    }
+    *out = h;
+    return UAAMG_SUCCESS;
+}
+
+int uaamg_poisson_destroy(uaamg_poisson* h) {
+    if (!h) return UAAMG_SUCCESS;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    destroy_graph(h);
+    if (h->dmem) cudaFree(h->dmem);
+    if (h->st_host) cudaFreeHost(h->st_host);
+    if (h->scalar_host) cudaFreeHost(h->scalar_host);
+    if (h->body_stream) cudaStreamDestroy(h->body_stream);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return UAAMG_SUCCESS;
+}
+
+int uaamg_poisson_set_smoother(uaamg_poisson* h, int smoother) {
+    if (!h || smoother < 0 || smoother > 3) { set_error("invalid smoother"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    h->smoother = smoother;
+    return UAAMG_SUCCESS;
+}
+int uaamg_poisson_set_max_iterations(uaamg_poisson* h, int m) {
+    if (!h) { set_error("NULL handle"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    h->max_iter = m;
+    return UAAMG_SUCCESS;
+}
+int uaamg_poisson_set_relative_tolerance(uaamg_poisson* h, float t) {
+    if (!h) { set_error("NULL handle"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    h->rel_tol = t;
+    return UAAMG_SUCCESS;
+}
+int uaamg_poisson_iterations(const uaamg_poisson* h) { return h ? h->iterations : 0; }
+float uaamg_poisson_final_residual(const uaamg_poisson* h) { return h ? h->final_residual : 0.f; }
+int uaamg_poisson_num_levels(const uaamg_poisson* h) { return h ? h->nlev : 0; }
+int64_t uaamg_poisson_num_dof(const uaamg_poisson* h, int level) {
+    if (!h || level < 0 || level >= (int)h->host.size()) return -1;
+    return h->host[level].ndof;
+}
+int64_t uaamg_poisson_leaf_count(const uaamg_poisson* h, int level) {
+    if (!h || level < 0 || level >= (int)h->host.size()) return -1;
+    return h->host[level].nl;
+}
+int uaamg_poisson_dof_topology(const uaamg_poisson* h, int level, int32_t* origins, uint64_t* masks) {
+    if (!h || level < 0 || level >= (int)h->host.size()) { set_error("invalid level"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    const HostLevel& H = h->host[level];
+    if (origins && H.nl) memcpy(origins, H.org.data(), (size_t)H.nl * 12);
+    if (masks && H.nl) memcpy(masks, H.mask.data(), (size_t)H.nl * 64);
+    return UAAMG_SUCCESS;
+}
+int uaamg_poisson_dof_index(const uaamg_poisson* h, int level, int32_t* out) {
+    if (!h || !out || level < 0 || level >= (int)h->host.size()) { set_error("invalid argument"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    const HostLevel& H = h->host[level];
+    for (int i = 0; i < H.nl; ++i) {
+        int32_t d = H.dof_base[i];
+        for (int off = 0; off < UAAMG_LEAF; ++off)
+            out[(size_t)i * UAAMG_LEAF + off] = ((H.mask[8 * i + (off >> 6)] >> (off & 63)) & 1ull) ? d++ : -1;
+    }
+    return UAAMG_SUCCESS;
+}
+
+static int build_rhs_impl(uaamg_poisson* h, const uaamg_leaf_grid* fw, const uaamg_leaf_grid* vx,
+                          const uaamg_leaf_grid* vy, const uaamg_leaf_grid* vz, const uaamg_leaf_grid* sv, float dt,
+                          float* d_out) {
+    (void)dt;  // the reference's BuildPoissonRhs carries dt but does not use it (.cpp:84-86)
+    check_grid(fw, 3, "face_weights");
+    check_grid(vx, 1, "vx");
+    check_grid(vy, 1, "vy");
+    check_grid(vz, 1, "vz");
+    check_grid(sv, 3, "solid_velocity");
+    LevelDev& D0 = h->lv[0];
+    if (D0.L.nl == 0) return UAAMG_SUCCESS;
+    std::vector<void*> tofree;
+    HostMap m0, m1, m2, m3, m4;
+    DevGrid g0, g1, g2, g3, g4;
+    upload_grid(h, fw, g0, m0, tofree);
+    upload_grid(h, vx, g1, m1, tofree);
+    upload_grid(h, vy, g2, m2, tofree);
+    upload_grid(h, vz, g3, m3, tofree);
+    upload_grid(h, sv, g4, m4, tofree);
+    float invdx = 1.0f / D0.dx;
+    k_build_rhs<<<(unsigned)D0.L.nl, 128, 0, h->stream>>>(D0.L.mask, D0.org, g0.g, g1.g, g2.g, g3.g, g4.g, invdx, d_out);
+    CHECK_LAUNCH();
+    for (void* p : tofree) CK(cudaFreeAsync(p, h->stream));
+    return UAAMG_SUCCESS;
+}
+
+int uaamg_poisson_build_rhs(uaamg_poisson* h, const uaamg_leaf_grid* fw, const uaamg_leaf_grid* vx,
+                            const uaamg_leaf_grid* vy, const uaamg_leaf_grid* vz, const uaamg_leaf_grid* sv, float dt,
+                            float* rhs_out) {
+    ABI_BEGIN
+    require(h && rhs_out, "NULL argument");
+    int rc = build_rhs_impl(h, fw, vx, vy, vz, sv, dt, h->b);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(rhs_out, h->b, vec_bytes(h, 0), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+int uaamg_poisson_build_rhs_device(uaamg_poisson* h, const uaamg_leaf_grid* fw, const uaamg_leaf_grid* vx,
+                                   const uaamg_leaf_grid* vy, const uaamg_leaf_grid* vz, const uaamg_leaf_grid* sv,
+                                   float dt, float* d_rhs_out) {
+    ABI_BEGIN
+    require(h && d_rhs_out, "NULL argument");
+    return build_rhs_impl(h, fw, vx, vy, vz, sv, dt, d_rhs_out);
+    ABI_END
+}
+
+int uaamg_poisson_solve_pcg(uaamg_poisson* h, float* pressure, const float* rhs, int* iterations) {
+    ABI_BEGIN
+    require(h && pressure && rhs, "NULL argument");
+    size_t nb = vec_bytes(h, 0);
+    if (nb) {
+        CK(cudaMemcpyAsync(h->x, pressure, nb, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->b, rhs, nb, cudaMemcpyHostToDevice, h->stream));
+    }
+    int st = run_pcg(h);
+    if (nb) {
+        CK(cudaMemcpyAsync(pressure, h->x, nb, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (iterations) *iterations = h->iterations;
+    return st;
+    ABI_END
+}
+int uaamg_poisson_solve_pcg_device(uaamg_poisson* h, float* d_pressure, const float* d_rhs, int* iterations) {
+    ABI_BEGIN
+    require(h && d_pressure && d_rhs, "NULL argument");
+    size_t nb = vec_bytes(h, 0);
+    if (nb) {
+        if (d_pressure != h->x) CK(cudaMemcpyAsync(h->x, d_pressure, nb, cudaMemcpyDeviceToDevice, h->stream));
+        if (d_rhs != h->b) CK(cudaMemcpyAsync(h->b, d_rhs, nb, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    int st = run_pcg(h);
+    if (nb && d_pressure != h->x) {
+        CK(cudaMemcpyAsync(d_pressure, h->x, nb, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (iterations) *iterations = h->iterations;
+    return st;
+    ABI_END
+}
+int uaamg_poisson_solve_mg(uaamg_poisson* h, float* pressure, const float* rhs, int* iterations) {
+    ABI_BEGIN
+    require(h && pressure && rhs, "NULL argument");
+    size_t nb = vec_bytes(h, 0);
+    if (nb) {
+        CK(cudaMemcpyAsync(h->x, pressure, nb, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->b, rhs, nb, cudaMemcpyHostToDevice, h->stream));
+    }
+    int st = run_mg(h);
+    if (nb) {
+        CK(cudaMemcpyAsync(pressure, h->x, nb, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (iterations) *iterations = h->iterations;
+    return st;
+    ABI_END
+}
+int uaamg_poisson_solve_mg_device(uaamg_poisson* h, float* d_pressure, const float* d_rhs, int* iterations) {
+    ABI_BEGIN
+    require(h && d_pressure && d_rhs, "NULL argument");
+    size_t nb = vec_bytes(h, 0);
+    if (nb) {
+        CK(cudaMemcpyAsync(h->x, d_pressure, nb, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->b, d_rhs, nb, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    int st = run_mg(h);
+    if (nb) {
+        CK(cudaMemcpyAsync(d_pressure, h->x, nb, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (iterations) *iterations = h->iterations;
+    return st;
+    ABI_END
+}
+
+// ---- per-level operators (host pointers); scratch = the level's lhs/rhs/tmp
+// buffers are NOT used so the multigrid state is not disturbed
+struct Scratch {
+    float* a = nullptr;
+    float* b = nullptr;
+    float* c = nullptr;
+    cudaStream_t s;
+    Scratch(size_t bytes, cudaStream_t st) : s(st) {
+        CK(cudaMallocAsync(&a, std::max<size_t>(bytes, 16) * 3, s));
+        b = a + std::max<size_t>(bytes, 16) / 4;
+        c = b + std::max<size_t>(bytes, 16) / 4;
+    }
+    ~Scratch() { cudaFreeAsync(a, s); }
+};
+
+static void check_level(const uaamg_poisson* h, int level) {
+    require(h != nullptr, "NULL handle");
+    require(level >= 0 && level < h->nlev, "invalid level");
+}
+
+int uaamg_poisson_level_apply(uaamg_poisson* h, int level, int mode, float weight, float w_sor, const float* lhs,
+                              const float* rhs, float* out) {
+    ABI_BEGIN
+    check_level(h, level);
+    require(lhs && out && mode >= 0 && mode <= 5, "invalid argument");
+    if (mode == UAAMG_MODE_SPAI0) ensure_spai0(h);
+    size_t nb = vec_bytes(h, level);
+    if (!nb) return UAAMG_SUCCESS;
+    Scratch S(nb, h->stream);
+    CK(cudaMemcpyAsync(S.a, lhs, nb, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(S.b, rhs ? rhs : lhs, nb, cudaMemcpyHostToDevice, h->stream));
+    LevelDev& D = h->lv[level];
+    float save = D.w_sor;
+    D.w_sor = w_sor;
+    Enq E{h, h->stream};
+    switch (mode) {
+        case UAAMG_MODE_WEIGHTED_JACOBI: E.sweep<M_JACOBI>(level, SrcPlain{S.a}, S.b, S.c, weight); break;
+        case UAAMG_MODE_RESIDUAL: E.sweep<M_RESIDUAL>(level, SrcPlain{S.a}, S.b, S.c, weight); break;
+        case UAAMG_MODE_LAPLACIAN: E.sweep<M_LAPLACIAN>(level, SrcPlain{S.a}, S.b, S.c, weight); break;
+        case UAAMG_MODE_RED_GS: E.sweep<M_RED>(level, SrcPlain{S.a}, S.b, S.a, weight); break;
+        case UAAMG_MODE_BLACK_GS: E.sweep<M_BLACK>(level, SrcPlain{S.a}, S.b, S.a, weight); break;
+        default: E.sweep<M_SPAI0>(level, SrcPlain{S.a}, S.b, S.c, weight, DotOut{nullptr, nullptr, nullptr}, true); break;
+    }
+    D.w_sor = save;
+    float* res = (mode == UAAMG_MODE_RED_GS || mode == UAAMG_MODE_BLACK_GS) ? S.a : S.c;
+    CK(cudaMemcpyAsync(out, res, nb, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_poisson_level_first_sweep(uaamg_poisson* h, int level, int kind, float weight, float w_sor, const float* rhs,
+                                    float* out) {
+    ABI_BEGIN
+    check_level(h, level);
+    require(rhs && out && kind >= 0 && kind <= 2, "invalid argument");
+    if (kind == 1) ensure_spai0(h);
+    size_t nb = vec_bytes(h, level);
+    if (!nb) return UAAMG_SUCCESS;
+    Scratch S(nb, h->stream);
+    CK(cudaMemcpyAsync(S.b, rhs, nb, cudaMemcpyHostToDevice, h->stream));
+    LevelDev& D = h->lv[level];
+    cudaStream_t s = h->stream;
+    if (kind == 0) {
+        k_materialize<SrcFirstJacobi><<<(unsigned)D.L.nl, 128, 0, s>>>(D.L, SrcFirstJacobi{S.b, weight}, S.c);
+    } else if (kind == 1) {
+        k_materialize<SrcFirstSpai0><<<(unsigned)D.L.nl, 128, 0, s>>>(D.L, SrcFirstSpai0{S.b, D.spai0_ready}, S.c);
+    } else {
+        float save = D.w_sor;
+        D.w_sor = w_sor;
+        Enq E{h, s};
+        E.sweep<M_BLACK>(level, SrcFirstRbgs{S.b, w_sor, 1}, S.b, S.c, 0.f);
+        D.w_sor = save;
+    }
+    CHECK_LAUNCH();
+    CK(cudaMemcpyAsync(out, S.c, nb, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_poisson_level_restrict(uaamg_poisson* h, int fine_level, const float* fine, float* coarse) {
+    ABI_BEGIN
+    check_level(h, fine_level);
+    require(fine_level + 1 < h->nlev && fine && coarse, "invalid argument");
+    size_t nf = vec_bytes(h, fine_level), nc = vec_bytes(h, fine_level + 1);
+    Scratch S(std::max(nf, nc), h->stream);
+    CK(cudaMemcpyAsync(S.a, fine, nf, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(S.c, 0, nc, h->stream));
+    LevelDev& D = h->lv[fine_level];
+    k_restrict<false><<<(unsigned)D.L.nl, 128, 0, h->stream>>>(D.L, S.a, nullptr, S.c);
+    CHECK_LAUNCH();
+    CK(cudaMemcpyAsync(coarse, S.c, nc, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_poisson_level_prolongate(uaamg_poisson* h, int fine_level, const float* coarse, float* fine, float alpha) {
+    ABI_BEGIN
+    check_level(h, fine_level);
+    require(fine_level + 1 < h->nlev && fine && coarse, "invalid argument");
+    size_t nf = vec_bytes(h, fine_level), nc = vec_bytes(h, fine_level + 1);
+    Scratch S(std::max(nf, nc), h->stream);
+    CK(cudaMemcpyAsync(S.a, fine, nf, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(S.b, coarse, nc, cudaMemcpyHostToDevice, h->stream));
+    LevelDev& D = h->lv[fine_level];
+    k_materialize<SrcProlong><<<(unsigned)D.L.nl, 128, 0, h->stream>>>(D.L, SrcProlong{S.a, S.b, alpha}, S.c);
+    CHECK_LAUNCH();
+    CK(cudaMemcpyAsync(fine, S.c, nf, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_poisson_level_coefficients(const uaamg_poisson* h, int level, float* diag, float* cx, float* cy, float* cz,
+                                     uint8_t* flags) {
+    ABI_BEGIN
+    check_level(h, level);
+    const LevelDev& D = h->lv[level];
+    size_t nb = (size_t)D.L.nl * UAAMG_LEAF * 4;
+    if (!nb) return UAAMG_SUCCESS;
+    if (diag) CK(cudaMemcpyAsync(diag, D.L.diag, nb, cudaMemcpyDeviceToHost, h->stream));
+    if (cx) CK(cudaMemcpyAsync(cx, D.L.cx, nb, cudaMemcpyDeviceToHost, h->stream));
+    if (cy) CK(cudaMemcpyAsync(cy, D.L.cy, nb, cudaMemcpyDeviceToHost, h->stream));
+    if (cz) CK(cudaMemcpyAsync(cz, D.L.cz, nb, cudaMemcpyDeviceToHost, h->stream));
+    std::vector<uint32_t> f(D.L.nl);
+    CK(cudaMemcpyAsync(f.data(), D.flags, (size_t)D.L.nl * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (flags)
+        for (int i = 0; i < D.L.nl; ++i) flags[i] = (uint8_t)(f[i] & 15u);
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_poisson_coarsest_solve(uaamg_poisson* h, const float* rhs, float* out) {
+    ABI_BEGIN
+    require(h && rhs && out, "NULL argument");
+    int l = h->nlev - 1;
+    size_t nb = vec_bytes(h, l);
+    if (!nb) return UAAMG_SUCCESS;
+    Scratch S(nb, h->stream);
+    CK(cudaMemcpyAsync(S.a, rhs, nb, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(S.c, 0, nb, h->stream));
+    Enq E{h, h->stream};
+    E.coarsest(S.a, S.c);
+    CK(cudaMemcpyAsync(out, S.c, nb, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_poisson_precondition(uaamg_poisson* h, const float* r, float* z) {
+    ABI_BEGIN
+    require(h && r && z, "NULL argument");
+    size_t nb = vec_bytes(h, 0);
+    if (!nb) return UAAMG_SUCCESS;
+    if (h->smoother == UAAMG_SMOOTHER_SPAI0) ensure_spai0(h);
+    Scratch S(nb, h->stream);
+    CK(cudaMemcpyAsync(S.b, r, nb, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(S.a, 0, nb, h->stream));
+    Enq E{h, h->stream};
+    enqueue_precond(E, 0, S.a, S.b, true, DotOut{nullptr, nullptr, nullptr});
+    CK(cudaMemcpyAsync(z, S.a, nb, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_poisson_set_stream(uaamg_poisson* h, void* stream) {
+    if (!h) { set_error("NULL handle"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->own_stream;
+    if (s != h->stream) {
+        cudaStreamSynchronize(h->stream);
+        h->stream = s;
+    }
+    return UAAMG_SUCCESS;
+}
+int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph) {
+    if (!h) { set_error("NULL handle"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    h->use_graph = use_graph ? 1 : 0;
+    return UAAMG_SUCCESS;
+}
+int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h) { return h ? h->last_launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,734 @@
+// poisson_kernels.cuh -- sm_100a kernels of the pressure-Poisson UAAMG-PCG.
+//
+// Arithmetic follows LaplacianApplySIMD::LightWeightApplier::operator()
+// (SIMD_UAAMG/simd_vdb_poisson.cpp:755-1031) operation by operation with
+// round-to-nearest intrinsics, so every per-voxel result is bit-identical to
+// the reference's AVX2 lanes; the library is built with --fmad=false so the
+// compiler cannot contract what the reference keeps separate.
+//
+// One CTA of 128 threads per 8^3 leaf; thread t owns voxels 4t..4t+3
+// (x = t>>4, y = (t>>1)&7, z = 4*(t&1)+j), i.e. one 16-byte float4 of each
+// leaf-dense array, so a warp reads 512 contiguous bytes per array.  The +-z
+// neighbours inside a leaf come from the partner thread (t^1) by shuffle,
+// +-x/+-y neighbours from the L1-resident own or neighbour leaf.
+#pragma once
+#include "common.cuh"
+
+namespace uaamg {
+
+#define FULLMASK 0xffffffffu
+
+// ---------------------------------------------------------------------------
+// lhs sources: what the stencil reads as "x" at any voxel.  Besides a stored
+// vector they compute, on the fly, the result of a pass the reference stores
+// and immediately re-reads (first sweep from zero, prolongation-add), which
+// removes a kernel launch and a full pass per use.
+struct SrcPlain {
+    const float* x;
+    __device__ __forceinline__ float4 get4(const DLevel&, int leaf, int t) const { return ld4(x, leaf, t); }
+    __device__ __forceinline__ float get1(const DLevel&, int leaf, int off) const {
+        return x[(long long)leaf * UAAMG_LEAF + off];
+    }
+};
+
+// setGridToResultAfterFirstJacobi (.cpp:1435-1479): x1 = w * (invdiag * b)
+struct SrcFirstJacobi {
+    const float* b;
+    float w;
+    __device__ __forceinline__ float4 get4(const DLevel& L, int leaf, int t) const {
+        float4 bb = ld4(b, leaf, t);
+        float4 iv = (L.flags[leaf] & TRIM_DIAG) ? f4splat(L.def_invdiag) : ld4(L.invdiag, leaf, t);
+        return make_float4(__fmul_rn(w, __fmul_rn(iv.x, bb.x)), __fmul_rn(w, __fmul_rn(iv.y, bb.y)),
+                           __fmul_rn(w, __fmul_rn(iv.z, bb.z)), __fmul_rn(w, __fmul_rn(iv.w, bb.w)));
+    }
+    __device__ __forceinline__ float get1(const DLevel& L, int leaf, int off) const {
+        long long i = (long long)leaf * UAAMG_LEAF + off;
+        float iv = (L.flags[leaf] & TRIM_DIAG) ? L.def_invdiag : L.invdiag[i];
+        return __fmul_rn(w, __fmul_rn(iv, b[i]));
+    }
+};
+
+// setGridToResultAfterFirstSPAI0 (.cpp:1481-1517): x1 = spai0 * b.  Before the
+// level's first spai0Apply the reference's SPAI0 grid is still empty, so the
+// default is used everywhere (`ready` is the device flag that tracks it).
+struct SrcFirstSpai0 {
+    const float* b;
+    const int* ready;
+    __device__ __forceinline__ float4 get4(const DLevel& L, int leaf, int t) const {
+        float4 bb = ld4(b, leaf, t);
+        float4 s = (!*ready || (L.flags[leaf] & TRIM_SPAI0)) ? f4splat(L.def_spai0) : ld4(L.spai0, leaf, t);
+        return make_float4(__fmul_rn(s.x, bb.x), __fmul_rn(s.y, bb.y), __fmul_rn(s.z, bb.z), __fmul_rn(s.w, bb.w));
+    }
+    __device__ __forceinline__ float get1(const DLevel& L, int leaf, int off) const {
+        long long i = (long long)leaf * UAAMG_LEAF + off;
+        float s = (!*ready || (L.flags[leaf] & TRIM_SPAI0)) ? L.def_spai0 : L.spai0[i];
+        return __fmul_rn(s, b[i]);
+    }
+};
+
+// setGridToResultAfterFirstRBGS<redFirst> red part (.cpp:1519-1566):
+// updated colour = w_sor * (invdiag * b), other colour = 0
+struct SrcFirstRbgs {
+    const float* b;
+    float wsor;
+    int red_first;
+    __device__ __forceinline__ float one(const DLevel& L, int leaf, int off, float bv, float iv) const {
+        int par = ((off >> 6) + (off >> 3) + off) & 1;  // (x+y+z) & 1, 0 = red
+        int upd = red_first ? (par == 0) : (par == 1);
+        return upd ? __fmul_rn(wsor, __fmul_rn(iv, bv)) : 0.f;
+    }
+    __device__ __forceinline__ float4 get4(const DLevel& L, int leaf, int t) const {
+        float4 bb = ld4(b, leaf, t);
+        float4 iv = (L.flags[leaf] & TRIM_DIAG) ? f4splat(L.def_invdiag) : ld4(L.invdiag, leaf, t);
+        int o = 4 * t;
+        return make_float4(one(L, leaf, o, bb.x, iv.x), one(L, leaf, o + 1, bb.y, iv.y),
+                           one(L, leaf, o + 2, bb.z, iv.z), one(L, leaf, o + 3, bb.w, iv.w));
+    }
+    __device__ __forceinline__ float get1(const DLevel& L, int leaf, int off) const {
+        long long i = (long long)leaf * UAAMG_LEAF + off;
+        float iv = (L.flags[leaf] & TRIM_DIAG) ? L.def_invdiag : L.invdiag[i];
+        return one(L, leaf, off, b[i], iv);
+    }
+};
+
+// prolongation<inplace_add=true> (.cpp:1686-1754): active fine voxels get
+// x + alpha * x_coarse(parent voxel)
+struct SrcProlong {
+    const float* x;
+    const float* xc;  // coarse-level vector
+    float alpha;
+    __device__ __forceinline__ float4 get4(const DLevel& L, int leaf, int t) const {
+        float4 v = ld4(x, leaf, t);
+        unsigned m = mask4(L.mask, leaf, t);
+        if (!m) return v;
+        int P = L.parent[leaf];
+        int o = L.octant[leaf];
+        int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
+        int coff = (((o >> 2) & 1) * 4 + (X >> 1)) * 64 + (((o >> 1) & 1) * 4 + (Y >> 1)) * 8 + (o & 1) * 4 + 2 * zh;
+        float2 c = *reinterpret_cast<const float2*>(xc + (long long)P * UAAMG_LEAF + coff);
+        float c0 = __fmul_rn(alpha, c.x), c1 = __fmul_rn(alpha, c.y);
+        if (m & 1) v.x = __fadd_rn(v.x, c0);
+        if (m & 2) v.y = __fadd_rn(v.y, c0);
+        if (m & 4) v.z = __fadd_rn(v.z, c1);
+        if (m & 8) v.w = __fadd_rn(v.w, c1);
+        return v;
+    }
+    __device__ __forceinline__ float get1(const DLevel& L, int leaf, int off) const {
+        float v = x[(long long)leaf * UAAMG_LEAF + off];
+        if (!((L.mask[(long long)leaf * 8 + (off >> 6)] >> (off & 63)) & 1ull)) return v;
+        int P = L.parent[leaf];
+        int o = L.octant[leaf];
+        int X = off >> 6, Y = (off >> 3) & 7, Z = off & 7;
+        int coff = (((o >> 2) & 1) * 4 + (X >> 1)) * 64 + (((o >> 1) & 1) * 4 + (Y >> 1)) * 8 + (o & 1) * 4 + (Z >> 1);
+        return __fadd_rn(v, __fmul_rn(alpha, xc[(long long)P * UAAMG_LEAF + coff]));
+    }
+};
+
+// p_new = z + beta * p (levelXPlusAlphaY), read on the fly
+// ---------------------------------------------------------------------------
+// The 6-neighbour off-diagonal sum of one float4 (4 z-consecutive voxels):
+// off = ((x+ c_x+ + x- c_x-) + (y+ c_y+ + y- c_y-)) + (z+ c_z+ + z- c_z-)
+// with c_k- this voxel's minus-face entry and c_k+ the +k neighbour's.
+template <class Src>
+__device__ __forceinline__ void stencil4(const DLevel& L, int leaf, int t, const Src& src, float4& xc,
+                                         float4& off) {
+    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
+    const unsigned fl = L.flags[leaf];
+    const int* nb = L.nbr + (long long)leaf * 6;
+    const float df = L.def_face;
+    const float4 dfv = f4splat(df);
+    xc = src.get4(L, leaf, t);
+    float4 xp, xm, yp, ym, cxp, cyp;
+    if (X < 7) {
+        xp = src.get4(L, leaf, t + 16);
+        cxp = (fl & TRIM_X) ? dfv : ld4(L.cx, leaf, t + 16);
+    } else {
+        int n = nb[1];
+        if (n >= 0) {
+            xp = src.get4(L, n, t - 112);
+            cxp = (L.flags[n] & TRIM_X) ? dfv : ld4(L.cx, n, t - 112);
+        } else {
+            xp = f4zero();
+            cxp = dfv;
+        }
+    }
+    if (X > 0) {
+        xm = src.get4(L, leaf, t - 16);
+    } else {
+        int n = nb[0];
+        xm = (n >= 0) ? src.get4(L, n, t + 112) : f4zero();
+    }
+    if (Y < 7) {
+        yp = src.get4(L, leaf, t + 2);
+        cyp = (fl & TRIM_Y) ? dfv : ld4(L.cy, leaf, t + 2);
+    } else {
+        int n = nb[3];
+        if (n >= 0) {
+            yp = src.get4(L, n, t - 14);
+            cyp = (L.flags[n] & TRIM_Y) ? dfv : ld4(L.cy, n, t - 14);
+        } else {
+            yp = f4zero();
+            cyp = dfv;
+        }
+    }
+    if (Y > 0) {
+        ym = src.get4(L, leaf, t - 2);
+    } else {
+        int n = nb[2];
+        ym = (n >= 0) ? src.get4(L, n, t + 14) : f4zero();
+    }
+    const float4 cxm = (fl & TRIM_X) ? dfv : ld4(L.cx, leaf, t);
+    const float4 cym = (fl & TRIM_Y) ? dfv : ld4(L.cy, leaf, t);
+    const float4 czo = (fl & TRIM_Z) ? dfv : ld4(L.cz, leaf, t);
+    const float px = __shfl_xor_sync(FULLMASK, xc.x, 1);
+    const float pw = __shfl_xor_sync(FULLMASK, xc.w, 1);
+    const float pcz = __shfl_xor_sync(FULLMASK, czo.x, 1);
+    const int base = 4 * t;
+    float zp3, zm0, czp3;
+    if (zh == 0) {
+        zp3 = px;
+        czp3 = pcz;
+        int n = nb[4];
+        zm0 = (n >= 0) ? src.get1(L, n, base + 7) : 0.f;
+    } else {
+        zm0 = pw;
+        int n = nb[5];
+        if (n >= 0) {
+            zp3 = src.get1(L, n, base - 4);
+            czp3 = (L.flags[n] & TRIM_Z) ? df : L.cz[(long long)n * UAAMG_LEAF + base - 4];
+        } else {
+            zp3 = 0.f;
+            czp3 = df;
+        }
+    }
+    const float zp[4] = {xc.y, xc.z, xc.w, zp3};
+    const float zm[4] = {zm0, xc.x, xc.y, xc.z};
+    const float czp[4] = {czo.y, czo.z, czo.w, czp3};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float f1 = __fmul_rn(f4get(xp, j), f4get(cxp, j));
+        float f2 = __fmul_rn(f4get(xm, j), f4get(cxm, j));
+        float f3 = __fmul_rn(f4get(yp, j), f4get(cyp, j));
+        float f4 = __fmul_rn(f4get(ym, j), f4get(cym, j));
+        float f5 = __fmul_rn(zp[j], czp[j]);
+        float f6 = __fmul_rn(zm[j], f4get(czo, j));
+        f1 = __fadd_rn(f1, f2);
+        f3 = __fadd_rn(f3, f4);
+        f5 = __fadd_rn(f5, f6);
+        f1 = __fadd_rn(f1, f3);
+        f1 = __fadd_rn(f1, f5);
+        f4set(off, j, f1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// deterministic block reductions (128 threads) and last-block finalisation
+__device__ __forceinline__ double block_sum128(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULLMASK, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double r = 0;
+    if (threadIdx.x == 0) r = ((sh[0] + sh[1]) + sh[2]) + sh[3];
+    __syncthreads();
+    return r;  // valid in thread 0
+}
+__device__ __forceinline__ float nanmax(float a, float b) {
+    if (isnan(a) || isnan(b)) return __int_as_float(0x7fc00000);
+    return fmaxf(a, b);
+}
+__device__ __forceinline__ float block_max128(float v, float* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(FULLMASK, v, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float r = 0;
+    if (threadIdx.x == 0) r = nanmax(nanmax(sh[0], sh[1]), nanmax(sh[2], sh[3]));
+    __syncthreads();
+    return r;
+}
+// |v| with non-finite values propagated (grid_abs_max_op, openvdb_grid_math_op.h:4-43)
+__device__ __forceinline__ float absprop(float v) { return isfinite(v) ? fabsf(v) : (isnan(v) ? v : INFINITY); }
+
+// Writes this block's partial; returns true in every thread of the last block.
+__device__ __forceinline__ bool publish_partial(double part, double* partials, unsigned* ticket, bool* sh_last) {
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = part;
+        __threadfence();
+        unsigned tk = atomicAdd(ticket, 1u);
+        *sh_last = (tk == gridDim.x - 1);
+    }
+    __syncthreads();
+    return *sh_last;
+}
+// Sum of all partials in a fixed order (last block only), valid in thread 0.
+__device__ __forceinline__ double gather_sum(const double* partials, double* sh) {
+    double acc = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) acc += __ldcg(partials + i);
+    return block_sum128(acc, sh);
+}
+__device__ __forceinline__ float gather_max(const double* partials, float* sh) {
+    float acc = 0.f;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) acc = nanmax(acc, (float)__ldcg(partials + i));
+    return block_max128(acc, sh);
+}
+
+// ---------------------------------------------------------------------------
+// One sweep of the applier in any mode.  out may alias the stored lhs only for
+// the Gauss-Seidel modes with SrcPlain (in-place red/black passes).
+enum { M_JACOBI = 0, M_RESIDUAL = 1, M_LAPLACIAN = 2, M_RED = 3, M_BLACK = 4, M_SPAI0 = 5 };
+
+struct DotOut {            // optional fused z.r for the PCG (rho_new, beta)
+    const float* r;        // second operand; nullptr = no dot
+    double* partials;
+    PcgState* st;
+};
+
+template <int MODE, class Src>
+__device__ __forceinline__ float4 sweep_value(const DLevel& L, int leaf, int t, const Src& src, const float* b,
+                                              float w, float wsor, float one_minus_wsor, float4& xc, unsigned& m) {
+    float4 off;
+    stencil4(L, leaf, t, src, xc, off);
+    m = mask4(L.mask, leaf, t);
+    const unsigned fl = L.flags[leaf];
+    float4 res = f4zero();
+    if (MODE == M_RED || MODE == M_BLACK) {
+        const float4 bb = ld4(b, leaf, t);
+        const float4 iv = (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : ld4(L.invdiag, leaf, t);
+        const int X = t >> 4, Y = (t >> 1) & 7;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int par = (X + Y + j) & 1;  // z = 4*zh + j has the parity of j
+            bool upd = (MODE == M_RED) ? (par == 0) : (par == 1);
+            float r = __fsub_rn(f4get(bb, j), f4get(off, j));
+            r = __fmul_rn(r, f4get(iv, j));
+            r = __fmul_rn(r, wsor);
+            float v = __fmaf_rn(f4get(xc, j), one_minus_wsor, r);
+            f4set(res, j, upd ? v : f4get(xc, j));
+        }
+    } else {
+        const float4 dg = (fl & TRIM_DIAG) ? f4splat(L.def_diag) : ld4(L.diag, leaf, t);
+        if (MODE == M_LAPLACIAN) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) f4set(res, j, __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+        } else {
+            const float4 bb = ld4(b, leaf, t);
+            if (MODE == M_RESIDUAL) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    f4set(res, j, __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j))));
+            } else if (MODE == M_JACOBI) {
+                const float4 iv = (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : ld4(L.invdiag, leaf, t);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+                    r = __fmul_rn(r, f4get(iv, j));
+                    f4set(res, j, __fmaf_rn(w, r, f4get(xc, j)));
+                }
+            } else {  // SPAI0
+                const float4 sp = (fl & TRIM_SPAI0) ? f4splat(L.def_spai0) : ld4(L.spai0, leaf, t);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+                    f4set(res, j, __fmaf_rn(f4get(sp, j), r, f4get(xc, j)));
+                }
+            }
+        }
+    }
+    if (!(m & 1)) res.x = 0.f;
+    if (!(m & 2)) res.y = 0.f;
+    if (!(m & 4)) res.z = 0.f;
+    if (!(m & 8)) res.w = 0.f;
+    return res;
+}
+
+template <int MODE, class Src>
+__global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b, float* out, float w, float wsor,
+                                               float one_minus_wsor, DotOut dot, int* spai0_ready) {
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    float4 xc;
+    unsigned m;
+    float4 res = sweep_value<MODE>(L, leaf, t, src, b, w, wsor, one_minus_wsor, xc, m);
+    st4(out, leaf, t, res);
+    if (MODE == M_SPAI0 && spai0_ready && leaf == 0 && t == 0) *spai0_ready = 1;
+    if (dot.r) {  // rho_new = z . r (levelDot), then beta and rho (PCG lines 13-15)
+        __shared__ double shd[4];
+        __shared__ bool last;
+        float4 rr = ld4(dot.r, leaf, t);
+        double s = (double)res.x * rr.x + (double)res.y * rr.y + (double)res.z * rr.z + (double)res.w * rr.w;
+        double part = block_sum128(s, shd);
+        if (publish_partial(part, dot.partials, &dot.st->ticket[0], &last)) {
+            double tot = gather_sum(dot.partials, shd);
+            if (t == 0) {
+                PcgState* st = dot.st;
+                float rho_new = (float)tot;
+                st->rho_new = rho_new;
+                st->beta = st->first ? 0.f : __fdiv_rn(rho_new, st->rho);
+                st->rho = rho_new;
+                st->ticket[0] = 0;
+            }
+        }
+    }
+}
+
+// out = value of a source (materialise a first sweep or a prolongation)
+template <class Src>
+__global__ void __launch_bounds__(128) k_materialize(DLevel L, Src src, float* out) {
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    float4 v = src.get4(L, leaf, t);
+    unsigned m = mask4(L.mask, leaf, t);
+    if (!(m & 1)) v.x = 0.f;
+    if (!(m & 2)) v.y = 0.f;
+    if (!(m & 4)) v.z = 0.f;
+    if (!(m & 8)) v.w = 0.f;
+    st4(out, leaf, t, v);
+}
+
+// residual (RESID) or plain values, restricted to the parent level:
+// coarse = 0.125 * sum of the active fine values of the 2x2x2 block (.cpp:1624-1684)
+template <bool RESID>
+__global__ void __launch_bounds__(128) k_restrict(DLevel L, const float* x, const float* b, float* coarse) {
+    __shared__ float rs[UAAMG_LEAF];
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    float4 r;
+    if (RESID) {
+        float4 xc;
+        unsigned m;
+        r = sweep_value<M_RESIDUAL>(L, leaf, t, SrcPlain{x}, b, 0.f, 0.f, 0.f, xc, m);
+    } else {
+        r = ld4(x, leaf, t);
+    }
+    reinterpret_cast<float4*>(rs)[t] = r;
+    __syncthreads();
+    if (t < 64) {
+        const int i = t >> 4, j = (t >> 2) & 3, k = t & 3;
+        const uint64_t* mk = L.mask + (long long)leaf * 8;
+        float s = 0.f;
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    int fo = ((2 * i + ii) << 6) | ((2 * j + jj) << 3) | (2 * k + kk);
+                    if ((mk[fo >> 6] >> (fo & 63)) & 1ull) s = __fadd_rn(s, rs[fo]);
+                }
+        const int o = L.octant[leaf];
+        const int coff = ((((o >> 2) & 1) * 4 + i) << 6) | ((((o >> 1) & 1) * 4 + j) << 3) | ((o & 1) * 4 + k);
+        coarse[(long long)L.parent[leaf] * UAAMG_LEAF + coff] = __fmul_rn(s, 0.125f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// PCG vector kernels (PoissonSolver::solveMultigridPCG, .cpp:2155-2226)
+__global__ void __launch_bounds__(128) k_mask_vec(DLevel L, float* v) {
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    unsigned m = mask4(L.mask, leaf, t);
+    if (m == 0xF) return;
+    float4 a = ld4(v, leaf, t);
+    if (!(m & 1)) a.x = 0.f;
+    if (!(m & 2)) a.y = 0.f;
+    if (!(m & 4)) a.z = 0.f;
+    if (!(m & 8)) a.w = 0.f;
+    st4(v, leaf, t, a);
+}
+
+__device__ __forceinline__ void set_cond(cudaGraphConditionalHandle h, int use, unsigned v) {
+    if (use) cudaGraphSetConditional(h, v);
+}
+
+// lines 2-3: r = b - A x; nu = |r|_inf; numax = tol * nu
+__global__ void __launch_bounds__(128) k_pcg_init(DLevel L, const float* x, const float* b, float* r,
+                                                  double* partials, PcgState* st,
+                                                  cudaGraphConditionalHandle cond, int use_cond) {
+    __shared__ float shf[4];
+    __shared__ double shd[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    float4 xc;
+    unsigned m;
+    float4 res = sweep_value<M_RESIDUAL>(L, leaf, t, SrcPlain{x}, b, 0.f, 0.f, 0.f, xc, m);
+    st4(r, leaf, t, res);
+    float a = nanmax(nanmax(absprop(res.x), absprop(res.y)), nanmax(absprop(res.z), absprop(res.w)));
+    float part = block_max128(a, shf);
+    (void)shd;
+    if (publish_partial((double)part, partials, &st->ticket[1], &last)) {
+        float nu = gather_max(partials, shf);
+        if (t == 0) {
+            st->nu = nu;
+            st->nu_old = nu;
+            st->numax = __fmul_rn(st->tol, nu);
+            st->iter = 0;
+            st->first = 1;
+            st->iterations_taken = 0;
+            st->alpha = 0.f;
+            st->beta = 0.f;
+            int status = PCG_RUNNING;
+            if (nu <= st->numax) status = PCG_SUCCESS;
+            else if (st->max_iter <= 0) status = PCG_FAILED_DIVERGED;  // no iteration: x untouched
+            st->status = status;
+            st->ticket[1] = 0;
+            set_cond(cond, use_cond, status == PCG_RUNNING ? 1u : 0u);
+        }
+    }
+}
+
+// x += alpha_prev * p_prev (line 16, skipped in the first iteration); p = z + beta p (line 16)
+__global__ void __launch_bounds__(128) k_pcg_update_p(DLevel L, const float* z, float* p, float* x,
+                                                      const PcgState* st) {
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    const float beta = st->beta, alpha = st->alpha;
+    const int first = st->first;
+    float4 zz = ld4(z, leaf, t), pp = ld4(p, leaf, t);
+    if (!first) {
+        float4 xx = ld4(x, leaf, t);
+        xx.x = __fmaf_rn(alpha, pp.x, xx.x);
+        xx.y = __fmaf_rn(alpha, pp.y, xx.y);
+        xx.z = __fmaf_rn(alpha, pp.z, xx.z);
+        xx.w = __fmaf_rn(alpha, pp.w, xx.w);
+        st4(x, leaf, t, xx);
+    }
+    pp.x = __fmaf_rn(beta, pp.x, zz.x);
+    pp.y = __fmaf_rn(beta, pp.y, zz.y);
+    pp.z = __fmaf_rn(beta, pp.z, zz.z);
+    pp.w = __fmaf_rn(beta, pp.w, zz.w);
+    st4(p, leaf, t, pp);
+}
+
+// lines 6-7: q = A p; sigma = p.q; alpha = rho / sigma
+__global__ void __launch_bounds__(128) k_pcg_Ap(DLevel L, const float* p, float* q, double* partials, PcgState* st) {
+    __shared__ double shd[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    float4 xc;
+    unsigned m;
+    float4 res = sweep_value<M_LAPLACIAN>(L, leaf, t, SrcPlain{p}, nullptr, 0.f, 0.f, 0.f, xc, m);
+    st4(q, leaf, t, res);
+    double s = (double)xc.x * res.x + (double)xc.y * res.y + (double)xc.z * res.z + (double)xc.w * res.w;
+    double part = block_sum128(s, shd);
+    if (publish_partial(part, partials, &st->ticket[2], &last)) {
+        double tot = gather_sum(partials, shd);
+        if (t == 0) {
+            float sigma = (float)tot;
+            st->sigma = sigma;
+            st->alpha = __fdiv_rn(st->rho, sigma);
+            st->first = 0;
+            st->ticket[2] = 0;
+        }
+    }
+}
+
+// lines 8-12: r -= alpha q; nu = |r|_inf; convergence / divergence test
+__global__ void __launch_bounds__(128) k_pcg_update_r(DLevel L, const float* q, float* r, double* partials,
+                                                      PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
+    __shared__ float shf[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    const float na = -st->alpha;
+    float4 qq = ld4(q, leaf, t), rr = ld4(r, leaf, t);
+    rr.x = __fmaf_rn(na, qq.x, rr.x);
+    rr.y = __fmaf_rn(na, qq.y, rr.y);
+    rr.z = __fmaf_rn(na, qq.z, rr.z);
+    rr.w = __fmaf_rn(na, qq.w, rr.w);
+    st4(r, leaf, t, rr);
+    float a = nanmax(nanmax(absprop(rr.x), absprop(rr.y)), nanmax(absprop(rr.z), absprop(rr.w)));
+    float part = block_max128(a, shf);
+    if (publish_partial((double)part, partials, &st->ticket[3], &last)) {
+        float nu = gather_max(partials, shf);
+        if (t == 0) {
+            const int k = st->iter;
+            st->nu_old = st->nu;
+            st->nu = nu;
+            int status = PCG_RUNNING;
+            if (nu <= st->numax) {
+                status = PCG_SUCCESS;
+                st->iterations_taken = k;
+            } else if (nu > st->nu_old && k > 3) {
+                status = PCG_FAILED_DIVERGED;
+                st->iterations_taken = k;
+            } else if (k + 1 >= st->max_iter) {
+                status = PCG_FAILED_MAXITER;
+                st->iterations_taken = st->max_iter;
+            }
+            st->iter = k + 1;
+            st->status = status;
+            st->ticket[3] = 0;
+            set_cond(cond, use_cond, status == PCG_RUNNING ? 1u : 0u);
+        }
+    }
+}
+
+// line 10 on success, and line 16 of the last iteration when max_iter is reached
+__global__ void __launch_bounds__(128) k_pcg_finish(DLevel L, const float* p, float* x, const PcgState* st) {
+    const int s = st->status;
+    if (s != PCG_SUCCESS && s != PCG_FAILED_MAXITER) return;
+    if (st->iterations_taken == 0 && st->iter == 0) return;  // converged before the loop
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    const float alpha = st->alpha;
+    float4 pp = ld4(p, leaf, t), xx = ld4(x, leaf, t);
+    xx.x = __fmaf_rn(alpha, pp.x, xx.x);
+    xx.y = __fmaf_rn(alpha, pp.y, xx.y);
+    xx.z = __fmaf_rn(alpha, pp.z, xx.z);
+    xx.w = __fmaf_rn(alpha, pp.w, xx.w);
+    st4(x, leaf, t, xx);
+}
+
+// |v|_inf over a level (levelAbsMax), result in out[0]
+__global__ void __launch_bounds__(128) k_absmax(DLevel L, const float* v, double* partials, unsigned* ticket,
+                                                float* out) {
+    __shared__ float shf[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    float4 a = ld4(v, leaf, t);
+    unsigned m = mask4(L.mask, leaf, t);
+    float mx = 0.f;
+    if (m & 1) mx = nanmax(mx, absprop(a.x));
+    if (m & 2) mx = nanmax(mx, absprop(a.y));
+    if (m & 4) mx = nanmax(mx, absprop(a.z));
+    if (m & 8) mx = nanmax(mx, absprop(a.w));
+    float part = block_max128(mx, shf);
+    if (publish_partial((double)part, partials, ticket, &last)) {
+        float r = gather_max(partials, shf);
+        if (t == 0) {
+            *out = r;
+            *ticket = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coarsest level: restatement of Eigen::ConjugateGradient<SparseMatrix<float>>
+// (diagonal preconditioner, tolerance FLT_EPSILON, maxIterations 10, zero
+// guess), one CTA, rows in DOF order with up to six off-diagonal entries.
+struct DCoarsest {
+    int n;
+    const int* dof_slot;   // [n] leaf*512 + offset
+    const float* diag;     // [n]
+    const float* invd;     // [n] 1/diag (1 where diag == 0)
+    const int* col;        // [n][6] (-1 = none)
+    const float* val;      // [n][6]
+};
+
+#define CG_THREADS 512
+#define CG_ROWS 8  // CG_THREADS * CG_ROWS >= 4096 >= coarsest DOF count
+
+__device__ __forceinline__ double cg_block_sum(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULLMASK, v, o);
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        double s = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(FULLMASK, s, o);
+        if (threadIdx.x == 0) sh[32] = s;
+    }
+    __syncthreads();
+    double r = sh[32];
+    __syncthreads();
+    return r;
+}
+__device__ __forceinline__ double2 cg_block_sum2(double a, double b, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(FULLMASK, a, o);
+        b += __shfl_down_sync(FULLMASK, b, o);
+    }
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sh[w] = a; sh[32 + w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        double s = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+        double u = (threadIdx.x < nw) ? sh[32 + threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_down_sync(FULLMASK, s, o);
+            u += __shfl_down_sync(FULLMASK, u, o);
+        }
+        if (threadIdx.x == 0) { sh[64] = s; sh[65] = u; }
+    }
+    __syncthreads();
+    double2 r = make_double2(sh[64], sh[65]);
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(CG_THREADS) k_coarsest_cg(DCoarsest C, const float* rhs, float* out) {
+    __shared__ float ps[CG_THREADS * CG_ROWS];
+    __shared__ double sh[72];
+    const int tid = threadIdx.x, n = C.n;
+    float x[CG_ROWS], r[CG_ROWS], p[CG_ROWS], z[CG_ROWS], tq[CG_ROWS];
+    double bb = 0;
+#pragma unroll
+    for (int k = 0; k < CG_ROWS; ++k) {
+        int i = tid + k * CG_THREADS;
+        x[k] = 0.f;
+        r[k] = (i < n) ? rhs[C.dof_slot[i]] : 0.f;
+        bb += (double)r[k] * r[k];
+    }
+    const float rhsNorm2 = (float)cg_block_sum(bb, sh);
+    bool done = (rhsNorm2 == 0.f);
+    float threshold = fmaxf(__fmul_rn(__fmul_rn(FLT_EPSILON, FLT_EPSILON), rhsNorm2), FLT_MIN);
+    if (!done && rhsNorm2 < threshold) done = true;  // residualNorm2 == rhsNorm2 for x = 0
+    if (!done) {
+        double an = 0;
+#pragma unroll
+        for (int k = 0; k < CG_ROWS; ++k) {
+            int i = tid + k * CG_THREADS;
+            p[k] = (i < n) ? __fmul_rn(C.invd[i], r[k]) : 0.f;
+            an += (double)r[k] * p[k];
+        }
+        float absNew = (float)cg_block_sum(an, sh);
+        for (int it = 0; it < 10; ++it) {
+#pragma unroll
+            for (int k = 0; k < CG_ROWS; ++k) ps[tid + k * CG_THREADS] = p[k];
+            __syncthreads();
+            double pt = 0;
+#pragma unroll
+            for (int k = 0; k < CG_ROWS; ++k) {
+                int i = tid + k * CG_THREADS;
+                float s = 0.f;
+                if (i < n) {
+                    s = __fmul_rn(C.diag[i], p[k]);
+#pragma unroll
+                    for (int e = 0; e < 6; ++e) {
+                        int c = C.col[i * 6 + e];
+                        if (c >= 0) s = __fadd_rn(s, __fmul_rn(C.val[i * 6 + e], ps[c]));
+                    }
+                }
+                tq[k] = s;
+                pt += (double)p[k] * s;
+            }
+            const float alpha = __fdiv_rn(absNew, (float)cg_block_sum(pt, sh));
+            double rr = 0;
+#pragma unroll
+            for (int k = 0; k < CG_ROWS; ++k) {
+                x[k] = __fmaf_rn(alpha, p[k], x[k]);
+                r[k] = __fmaf_rn(-alpha, tq[k], r[k]);
+                rr += (double)r[k] * r[k];
+            }
+            double rz = 0;
+#pragma unroll
+            for (int k = 0; k < CG_ROWS; ++k) {
+                int i = tid + k * CG_THREADS;
+                z[k] = (i < n) ? __fmul_rn(C.invd[i], r[k]) : 0.f;
+                rz += (double)r[k] * z[k];
+            }
+            double2 s2 = cg_block_sum2(rr, rz, sh);
+            if ((float)s2.x < threshold) break;
+            const float absOld = absNew;
+            absNew = (float)s2.y;
+            const float beta = __fdiv_rn(absNew, absOld);
+#pragma unroll
+            for (int k = 0; k < CG_ROWS; ++k) p[k] = __fmaf_rn(beta, p[k], z[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < CG_ROWS; ++k) {
+        int i = tid + k * CG_THREADS;
+        if (i < n) out[C.dof_slot[i]] = x[k];
+    }
+}
+
+}  // namespace uaamg

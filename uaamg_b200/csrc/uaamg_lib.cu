@@ -1,0 +1,2 @@
+// uaamg_lib.cu -- single translation unit of libuaamg_b200.so
+#include "poisson.cu"

@@ -1,0 +1,247 @@
+"""Python mirror of the reference's pressure-solver interface over the C ABI.
+
+Names, argument meaning and status codes follow SIMD_UAAMG/simd_vdb_poisson.h:
+``LaplacianWithLevel.createPressurePoissonLaplacian`` (h:54-57),
+``createPressurePoissonRightHandSide`` (h:59-65), ``getZeroVectorGrid`` (h:98),
+``PoissonSolver`` with ``mMaxIteration``/``mRelativeTolerance``/``mSmoother``/
+``mIterationTaken`` and ``solveMultigridPCG``/``solvePureMultigrid`` returning
+``SUCCESS`` (0) / ``FAILED`` (1) (h:141-169).  Grids are ``LeafGrid`` objects
+(flattened OpenVDB leaves); vectors are leaf-dense float32 [leaves, 512] arrays
+(numpy on the host, or torch CUDA tensors for the ``*_device`` path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+
+import numpy as np
+
+from . import _lib
+from .grids import LeafGrid
+
+
+def _as_c(grid: LeafGrid, keep: list) -> _lib.LeafGridC:
+    g = _lib.LeafGridC()
+    g.leaf_count = grid.leaf_count
+    org = np.ascontiguousarray(grid.origins, dtype=np.int32)
+    keep.append(org)
+    g.origins = org.ctypes.data if grid.leaf_count else None
+    if grid.masks is not None and grid.leaf_count:
+        m = np.ascontiguousarray(grid.masks, dtype=np.uint64)
+        keep.append(m)
+        g.masks = m.ctypes.data
+    else:
+        g.masks = None
+    vals = grid.values
+    if isinstance(vals, np.ndarray):
+        v = np.ascontiguousarray(vals, dtype=np.float32)
+        keep.append(v)
+        g.values = v.ctypes.data if grid.leaf_count else None
+        g.values_on_device = 0
+    else:  # torch tensor
+        keep.append(vals)
+        g.values = vals.data_ptr() if grid.leaf_count else None
+        g.values_on_device = 1 if vals.is_cuda else 0
+    g.components = grid.components
+    bg = np.zeros(3, np.float32)
+    bg[: grid.background.size] = grid.background
+    for i in range(3):
+        g.background[i] = float(bg[i])
+    return g
+
+
+class LaplacianWithLevel:
+    """The pressure Poisson operator with its multigrid hierarchy on the GPU."""
+
+    def __init__(self, handle: int, dt: float, dx: float):
+        self._h = handle
+        self.mDt = dt
+        self.mDxThisLevel = dx
+        self.mLevel = 0
+
+    @staticmethod
+    def createPressurePoissonLaplacian(liquid_phi: LeafGrid, face_weights: LeafGrid, dt: float,
+                                       dx: float) -> "LaplacianWithLevel":
+        L = _lib.lib()
+        keep: list = []
+        a = _as_c(liquid_phi, keep)
+        b = _as_c(face_weights, keep)
+        h = C.c_void_p()
+        _lib.check(L.uaamg_poisson_create(C.byref(a), C.byref(b), float(dt), float(dx), C.byref(h)),
+                   "uaamg_poisson_create")
+        return LaplacianWithLevel(h.value, dt, dx)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().uaamg_poisson_destroy(h)
+            self._h = None
+
+    # --- topology / sizes
+    @property
+    def mNumDof(self) -> int:
+        return int(_lib.lib().uaamg_poisson_num_dof(self._h, 0))
+
+    def num_levels(self) -> int:
+        return int(_lib.lib().uaamg_poisson_num_levels(self._h))
+
+    def num_dof(self, level: int = 0) -> int:
+        return int(_lib.lib().uaamg_poisson_num_dof(self._h, level))
+
+    def leaf_count(self, level: int = 0) -> int:
+        return int(_lib.lib().uaamg_poisson_leaf_count(self._h, level))
+
+    def dof_topology(self, level: int = 0):
+        n = self.leaf_count(level)
+        o = np.zeros((n, 3), np.int32)
+        m = np.zeros((n, 8), np.uint64)
+        _lib.check(_lib.lib().uaamg_poisson_dof_topology(self._h, level, o.ctypes.data, m.ctypes.data),
+                   "dof_topology")
+        return o, m
+
+    def dof_index(self, level: int = 0) -> np.ndarray:
+        out = np.zeros((self.leaf_count(level), 512), np.int32)
+        _lib.check(_lib.lib().uaamg_poisson_dof_index(self._h, level, out.ctypes.data), "dof_index")
+        return out
+
+    def getZeroVectorGrid(self, level: int = 0) -> np.ndarray:
+        return np.zeros((self.leaf_count(level), 512), np.float32)
+
+    # --- right-hand side
+    def createPressurePoissonRightHandSide(self, face_weights, vx, vy, vz, solid_velocity, dt,
+                                           out=None):
+        keep: list = []
+        gs = [_as_c(g, keep) for g in (face_weights, vx, vy, vz, solid_velocity)]
+        L = _lib.lib()
+        if out is not None and not isinstance(out, np.ndarray):
+            _lib.check(L.uaamg_poisson_build_rhs_device(self._h, *[C.byref(g) for g in gs], float(dt),
+                                                        out.data_ptr()), "build_rhs_device")
+            return out
+        rhs = self.getZeroVectorGrid() if out is None else out
+        _lib.check(L.uaamg_poisson_build_rhs(self._h, *[C.byref(g) for g in gs], float(dt), rhs.ctypes.data),
+                   "build_rhs")
+        return rhs
+
+    # --- per-level operators (public methods of the reference class)
+    def apply(self, level, mode, lhs, rhs=None, weight=6.0 / 7.0, w_sor=1.2):
+        modes = {"jacobi": 0, "residual": 1, "laplacian": 2, "red_gs": 3, "black_gs": 4, "spai0": 5}
+        out = np.zeros_like(lhs, dtype=np.float32)
+        lhs = np.ascontiguousarray(lhs, np.float32)
+        rhs = lhs if rhs is None else np.ascontiguousarray(rhs, np.float32)
+        _lib.check(_lib.lib().uaamg_poisson_level_apply(self._h, level, modes[mode], weight, w_sor,
+                                                        lhs.ctypes.data, rhs.ctypes.data, out.ctypes.data),
+                   "level_apply")
+        return out
+
+    def residualApply(self, lhs, rhs, level=0):
+        return self.apply(level, "residual", lhs, rhs)
+
+    def laplacianApply(self, lhs, level=0):
+        return self.apply(level, "laplacian", lhs)
+
+    def weightedJacobiApply(self, lhs, rhs, weight=6.0 / 7.0, level=0):
+        return self.apply(level, "jacobi", lhs, rhs, weight=weight)
+
+    def first_sweep(self, level, kind, rhs, weight=6.0 / 7.0, w_sor=1.2):
+        kinds = {"jacobi": 0, "spai0": 1, "rbgs": 2}
+        out = np.zeros_like(rhs, dtype=np.float32)
+        rhs = np.ascontiguousarray(rhs, np.float32)
+        _lib.check(_lib.lib().uaamg_poisson_level_first_sweep(self._h, level, kinds[kind], weight, w_sor,
+                                                              rhs.ctypes.data, out.ctypes.data), "first_sweep")
+        return out
+
+    def restriction(self, fine, fine_level=0):
+        out = np.zeros((self.leaf_count(fine_level + 1), 512), np.float32)
+        fine = np.ascontiguousarray(fine, np.float32)
+        _lib.check(_lib.lib().uaamg_poisson_level_restrict(self._h, fine_level, fine.ctypes.data,
+                                                           out.ctypes.data), "restrict")
+        return out
+
+    def prolongation(self, coarse, fine, fine_level=0, alpha=1.0):
+        out = np.array(fine, dtype=np.float32, copy=True)
+        coarse = np.ascontiguousarray(coarse, np.float32)
+        _lib.check(_lib.lib().uaamg_poisson_level_prolongate(self._h, fine_level, coarse.ctypes.data,
+                                                             out.ctypes.data, alpha), "prolongate")
+        return out
+
+    def coefficients(self, level=0):
+        n = self.leaf_count(level)
+        arr = [np.zeros((n, 512), np.float32) for _ in range(4)]
+        flags = np.zeros(n, np.uint8)
+        _lib.check(_lib.lib().uaamg_poisson_level_coefficients(self._h, level, *[a.ctypes.data for a in arr],
+                                                                flags.ctypes.data), "coefficients")
+        return arr, flags
+
+    def coarsest_solve(self, rhs):
+        out = np.zeros_like(rhs, dtype=np.float32)
+        rhs = np.ascontiguousarray(rhs, np.float32)
+        _lib.check(_lib.lib().uaamg_poisson_coarsest_solve(self._h, rhs.ctypes.data, out.ctypes.data),
+                   "coarsest_solve")
+        return out
+
+
+class PoissonSolver:
+    """PCG with the unsmoothed-aggregation mu-cycle (mu = 2) as preconditioner."""
+
+    class SmootherOption(enum.IntEnum):
+        ScheduledRelaxedJacobi = 0
+        WeightedJacobi = 1
+        RedBlackGaussSeidel = 2
+        SPAI0 = 3
+
+    SUCCESS = 0
+    FAILED = 1
+
+    def __init__(self, level0: LaplacianWithLevel):
+        self.mMultigridHierarchy = level0
+        self.mIterationTaken = 0
+        self.mMaxIteration = 100
+        self.mRelativeTolerance = 1e-7
+        self.mSmoother = PoissonSolver.SmootherOption.ScheduledRelaxedJacobi
+        self.use_graph = True
+
+    def _configure(self):
+        L = _lib.lib()
+        h = self.mMultigridHierarchy._h
+        _lib.check(L.uaamg_poisson_set_smoother(h, int(self.mSmoother)), "set_smoother")
+        _lib.check(L.uaamg_poisson_set_max_iterations(h, int(self.mMaxIteration)), "set_max_iterations")
+        _lib.check(L.uaamg_poisson_set_relative_tolerance(h, float(self.mRelativeTolerance)), "set_tolerance")
+        _lib.check(L.uaamg_poisson_set_graph_mode(h, 1 if self.use_graph else 0), "set_graph_mode")
+        return L, h
+
+    def _solve(self, host_fn, dev_fn, pressure, rhs) -> int:
+        L, h = self._configure()
+        it = C.c_int(0)
+        if isinstance(pressure, np.ndarray):
+            assert pressure.dtype == np.float32 and pressure.flags["C_CONTIGUOUS"]
+            rhs = np.ascontiguousarray(rhs, np.float32)
+            rc = getattr(L, host_fn)(h, pressure.ctypes.data, rhs.ctypes.data, C.byref(it))
+        else:
+            rc = getattr(L, dev_fn)(h, pressure.data_ptr(), rhs.data_ptr(), C.byref(it))
+        _lib.check(rc, host_fn)
+        self.mIterationTaken = int(it.value)
+        return int(rc)
+
+    def solveMultigridPCG(self, in_out_pressure, in_rhs) -> int:
+        return self._solve("uaamg_poisson_solve_pcg", "uaamg_poisson_solve_pcg_device", in_out_pressure, in_rhs)
+
+    def solvePureMultigrid(self, in_out_pressure, in_rhs) -> int:
+        return self._solve("uaamg_poisson_solve_mg", "uaamg_poisson_solve_mg_device", in_out_pressure, in_rhs)
+
+    def precondition(self, r: np.ndarray) -> np.ndarray:
+        L, h = self._configure()
+        z = np.zeros_like(r, dtype=np.float32)
+        r = np.ascontiguousarray(r, np.float32)
+        _lib.check(L.uaamg_poisson_precondition(h, r.ctypes.data, z.ctypes.data), "precondition")
+        return z
+
+    @property
+    def final_residual(self) -> float:
+        return float(_lib.lib().uaamg_poisson_final_residual(self.mMultigridHierarchy._h))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(_lib.lib().uaamg_poisson_kernel_launches(self.mMultigridHierarchy._h))
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        _lib.check(_lib.lib().uaamg_poisson_set_stream(self.mMultigridHierarchy._h, stream_ptr), "set_stream")
