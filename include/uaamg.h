@@ -149,11 +149,19 @@ int uaamg_poisson_coarsest_solve(uaamg_poisson* h, const float* rhs, float* out)
 /* One preconditioner application z = M^-1 r (muCyclePreconditioner<2,true>(z, r, 0, 3)). */
 int uaamg_poisson_precondition(uaamg_poisson* h, const float* r, float* z);
 
+/* Diagnostics: one PCG solve (device pointers) driven from the host with a
+ * CUDA event pair around every kernel; returns per kernel class its total
+ * device time and launch count.  names: max_classes * 64 chars.  No
+ * counterpart in the reference (it keeps wall-clock timers, singletons/Timer.h). */
+int uaamg_poisson_profile_pcg(uaamg_poisson* h, float* d_pressure, const float* d_rhs, int max_classes,
+                              char* names, double* total_ms, int64_t* counts, int* nclasses);
+
 /* Stream (cudaStream_t as void*) used by *_device calls; NULL = the handle's own stream. */
 int uaamg_poisson_set_stream(uaamg_poisson* h, void* stream);
 /* Use the CUDA-graph PCG (1, default) or the host-driven loop (0). */
 int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph);
-/* Kernels launched by the last solve (including those inside the graph). */
+/* Kernels launched through this handle since it was created: hierarchy build,
+ * right-hand side and every solve (kernels inside the solve graph included). */
 int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h);
 
 const char* uaamg_last_error(void);

@@ -1,0 +1,85 @@
+"""CPU checks of the drop-in boundary: the CUDA library loads, exports every
+entry point declared in include/uaamg.h, and its host-side argument checks
+answer without a GPU (no compute calls)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for fn in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(uaamg_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope="module")
+def cuda_lib():
+    from uaamg_b200 import build
+    build.build()
+    from uaamg_b200 import _lib
+    return _lib.lib()
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "uaamg_poisson_create" in names and "uaamg_poisson_solve_pcg" in names
+    assert len(names) >= 25
+
+
+def test_library_exports_every_declared_symbol(cuda_lib):
+    from uaamg_b200 import _lib
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT\s+(uaamg_\w+)", out))
+    missing = [n for n in declared_functions() if n not in exported]
+    assert not missing, missing
+    for n in declared_functions():
+        assert hasattr(cuda_lib, n)
+
+
+def test_python_binding_covers_header():
+    from uaamg_b200 import _lib
+    bound = {name for name, _, _ in _lib.EXPORTS}
+    assert set(declared_functions()) <= bound
+
+
+def test_create_without_device_reports_error(cuda_lib):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    from uaamg_b200 import _lib
+    g = _lib.LeafGridC()
+    h = C.c_void_p()
+    rc = cuda_lib.uaamg_poisson_create(C.byref(g), C.byref(g), 1.0, 0.1, C.byref(h))
+    assert rc == -5  # UAAMG_ERR_NO_DEVICE
+    assert b"device" in cuda_lib.uaamg_last_error()
+    assert cuda_lib.uaamg_device_count() == 0
+
+
+def test_null_arguments_are_rejected(cuda_lib):
+    assert cuda_lib.uaamg_poisson_create(None, None, 1.0, 0.1, None) == -1
+    assert cuda_lib.uaamg_poisson_set_smoother(None, 0) == -1
+    assert cuda_lib.uaamg_poisson_destroy(None) == 0
+
+
+def test_cpp_facade_compiles():
+    """The header-only C++ facade (reference class names over the C ABI)."""
+    src = os.path.join(ROOT, "include", "uaamg_simd.hpp")
+    if not os.path.exists(src):
+        pytest.skip("no C++ facade")
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-x", "c++", "-I", os.path.join(ROOT, "include"), src],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -65,6 +65,7 @@ EXPORTS = [
     ("uaamg_poisson_level_coefficients", i32, [vp, i32, vp, vp, vp, vp, vp]),
     ("uaamg_poisson_coarsest_solve", i32, [vp, vp, vp]),
     ("uaamg_poisson_precondition", i32, [vp, vp, vp]),
+    ("uaamg_poisson_profile_pcg", i32, [vp, vp, vp, i32, vp, vp, vp, C.POINTER(C.c_int)]),
     ("uaamg_poisson_set_stream", i32, [vp, vp]),
     ("uaamg_poisson_set_graph_mode", i32, [vp, i32]),
     ("uaamg_poisson_kernel_launches", i64, [vp]),

@@ -26,6 +26,7 @@
 #include "common.cuh"
 #include "poisson_build.cuh"
 #include "poisson_kernels.cuh"
+#include "resources.cuh"
 
 using namespace uaamg;
 
@@ -240,6 +241,11 @@ struct LevelDev {
 };
 
 struct uaamg_poisson {
+    DeviceCtx* ctx = nullptr;
+    void* pin_state = nullptr;  // pinned block holding st_host and scalar_host
+    size_t pin_state_cap = 0;
+    void* pin_stage = nullptr;  // pinned staging of the topology upload
+    size_t pin_stage_cap = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t body_stream = nullptr;
@@ -300,7 +306,7 @@ static void upload_grid(uaamg_poisson* h, const uaamg_leaf_grid* gr, DevGrid& dg
     size_t vbytes = (size_t)gr->leaf_count * UAAMG_LEAF * gr->components * sizeof(float);
     size_t total = carve_size(mapn, 4) + (gr->values_on_device ? 0 : carve_size(vbytes, 1));
     void* mem = nullptr;
-    CK(cudaMallocAsync(&mem, total, h->stream));
+    CK(ctx_dev_alloc(h->ctx, &mem, total, h->stream));
     tofree.push_back(mem);
     char* cur = (char*)mem;
     int* dmap = carve<int>(cur, mapn);
@@ -382,7 +388,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         upload_grid(h, fw, dfw, fwmap, tofree);
         size_t extra = carve_size((size_t)nphi * 8, 8) * 2 + carve_size((size_t)nphi * 3, 4);
         void* mem = nullptr;
-        CK(cudaMallocAsync(&mem, extra, s));
+        CK(ctx_dev_alloc(h->ctx, &mem, extra, s));
         tofree.push_back(mem);
         char* cur = (char*)mem;
         uint64_t* dphimask = carve<uint64_t>(cur, (size_t)nphi * 8);
@@ -397,6 +403,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         const float dtOverDxSqr = dt / (dx * dx);
         k_finest_mask<<<(unsigned)nphi, 128, 0, s>>>(dphi.g, pm, dphiorg, dfw.g, dtOverDxSqr, ddofmask);
         CHECK_LAUNCH();
+        h->launches++;
         std::vector<uint64_t> dofmask((size_t)nphi * 8);
         CK(cudaMemcpyAsync(dofmask.data(), ddofmask, (size_t)nphi * 64, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
@@ -439,8 +446,8 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         }
         const HostLevel& HC = h->host.back();
         size_t nc = (size_t)HC.ndof;
-        if (nc > (size_t)CG_THREADS * CG_ROWS) {
-            set_error("coarsening stalled: %zu DOF on the coarsest level (max %d)", nc, CG_THREADS * CG_ROWS);
+        if (nc > (size_t)CG_THREADS * CG_MAX_ROWS) {
+            set_error("coarsening stalled: %zu DOF on the coarsest level (max %d)", nc, CG_THREADS * CG_MAX_ROWS);
             throw UaamgError{UAAMG_ERR_DOMAIN_TOO_LARGE};
         }
         bytes += carve_size(nc, 4) * 3 + carve_size(nc * 6, 4) * 2;
@@ -448,7 +455,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         bytes += 6 * carve_size(n0, 4);  // x b r z p q
         bytes += carve_size(std::max<size_t>((size_t)L0.nl, 1) + 64, 8);
         bytes += carve_size(sizeof(PcgState), 1) + carve_size(64, 4) + carve_size(src.size(), 4);
-        CK(cudaMalloc(&h->dmem, bytes));
+        CK(ctx_dev_alloc(h->ctx, (void**)&h->dmem, bytes, s));
         h->dmem_bytes = bytes;
         CK(cudaMemsetAsync(h->dmem, 0, bytes, s));
         char* cur2 = h->dmem;
@@ -518,8 +525,9 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         // one pinned staging buffer for all tables
         size_t tot = 0;
         for (auto& u : ups) tot += (u.second.second + 15) & ~size_t(15);
-        char* pin = nullptr;
-        CK(cudaMallocHost(&pin, std::max<size_t>(tot, 16)));
+        // kept by the handle until destroy, so create() need not wait for the DMA
+        CK(ctx_pinned_acquire(h->ctx, std::max<size_t>(tot, 16), &h->pin_stage, &h->pin_stage_cap));
+        char* pin = (char*)h->pin_stage;
         size_t o = 0;
         for (auto& u : ups) {
             memcpy(pin + o, u.second.first, u.second.second);
@@ -532,22 +540,23 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             k_finest_coef<<<(unsigned)L0.nl, 128, 0, s>>>(dphi.g, dphiorg, dfw.g, dtOverDxSqr, dsrc, D0.L.mask,
                                                           level_out(D0));
             CHECK_LAUNCH();
+            h->launches++;
         }
         for (int l = 1; l < nlev; ++l) {
             LevelDev& D = h->lv[l];
             if (D.L.nl == 0) continue;
             k_coarsen<<<(unsigned)D.L.nl, 128, 0, s>>>(h->lv[l - 1].L, D.L.child, D.L.mask, level_out(D));
             CHECK_LAUNCH();
+            h->launches++;
         }
         if (h->lv[nlev - 1].L.nl > 0) {
             LevelDev& D = h->lv[nlev - 1];
             k_coarsest_ell<<<(unsigned)D.L.nl, 128, 0, s>>>(D.L, D.dof_base, dslot, cdiag, cinvd, ccol, cval);
             CHECK_LAUNCH();
+            h->launches++;
         }
         for (void* pmem : tofree) CK(cudaFreeAsync(pmem, s));
         tofree.clear();
-        CK(cudaStreamSynchronize(s));
-        cudaFreeHost(pin);
         h->nlev = nlev;
     } else {
         h->nlev = 1;
@@ -565,6 +574,7 @@ static void ensure_spai0(uaamg_poisson* h) {
         k_spai0<<<(unsigned)D.L.nl, 128, 0, h->stream>>>(D.L, D.spai0, D.flags, defaultSPAI0Val,
                                                          fabsf(defaultSPAI0Val * 1e-5f));
         CHECK_LAUNCH();
+        h->launches++;
     }
     h->spai0_built = true;
 }
@@ -573,31 +583,86 @@ static void ensure_spai0(uaamg_poisson* h) {
 // kernel enqueue helpers
 namespace {
 
+// Launch with programmatic stream serialisation (PDL); the kernels start with
+// griddepcontrol.wait, so ordering is preserved while launch latency overlaps.
+static bool g_use_pdl = true;
+template <typename... KArgs, typename... Args>
+static void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = g_use_pdl ? 1 : 0;
+    CK(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+}
+
+// Optional per-kernel timing (diagnostics): a CUDA event pair around every launch.
+struct ProfRec {
+    std::string label;
+    cudaEvent_t a, b;
+};
+
+template <class Src> struct SrcName { static const char* get() { return ""; } };
+template <> struct SrcName<SrcFirstJacobi> { static const char* get() { return "+first"; } };
+template <> struct SrcName<SrcFirstSpai0> { static const char* get() { return "+first"; } };
+template <> struct SrcName<SrcFirstRbgs> { static const char* get() { return "+first"; } };
+template <> struct SrcName<SrcProlong> { static const char* get() { return "+prolong"; } };
+static const char* mode_name(int m) {
+    static const char* n[] = {"jacobi", "residual", "laplacian", "red_gs", "black_gs", "spai0"};
+    return n[m];
+}
+
 struct Enq {
     uaamg_poisson* h;
     cudaStream_t s;
     int64_t count = 0;
+    std::vector<ProfRec>* prof = nullptr;
+
+    void pb(const std::string& label) {
+        if (!prof) return;
+        ProfRec r;
+        r.label = label;
+        CK(cudaEventCreate(&r.a));
+        CK(cudaEventCreate(&r.b));
+        CK(cudaEventRecord(r.a, s));
+        prof->push_back(r);
+    }
+    void pe() {
+        if (!prof) return;
+        CK(cudaEventRecord(prof->back().b, s));
+    }
 
     template <int MODE, class Src>
     void sweep(int l, const Src& src, const float* b, float* out, float w, DotOut dot = DotOut{nullptr, nullptr, nullptr},
                bool mark_spai0 = false) {
         LevelDev& D = h->lv[l];
         float ws = D.w_sor;
-        k_sweep<MODE, Src><<<(unsigned)D.L.nl, 128, 0, s>>>(D.L, src, b, out, w, ws, 1.0f - ws, dot,
-                                                             mark_spai0 ? D.spai0_ready : nullptr);
-        CHECK_LAUNCH();
+        if (prof) pb("L" + std::to_string(l) + " " + mode_name(MODE) + SrcName<Src>::get() + (dot.r ? "+dot" : ""));
+        launch(k_sweep<MODE, Src>, (unsigned)D.L.nl, 128, s, D.L, src, b, out, w, ws, 1.0f - ws, dot,
+               mark_spai0 ? D.spai0_ready : nullptr);
+        pe();
         count++;
     }
     void restrict_resid(int l, const float* x, const float* b) {
         LevelDev& D = h->lv[l];
-        k_restrict<true><<<(unsigned)D.L.nl, 128, 0, s>>>(D.L, x, b, h->lv[l + 1].rhs);
-        CHECK_LAUNCH();
+        if (prof) pb("L" + std::to_string(l) + " residual+restrict");
+        launch(k_restrict<true>, (unsigned)D.L.nl, 128, s, D.L, x, b, h->lv[l + 1].rhs);
+        pe();
         count++;
     }
     void coarsest(const float* rhs, float* out) {
         if (h->C.n == 0) return;
-        k_coarsest_cg<<<1, CG_THREADS, 0, s>>>(h->C, rhs, out);
-        CHECK_LAUNCH();
+        pb("coarsest cg");
+        const int n = h->C.n;
+        if (n <= CG_THREADS) launch(k_coarsest_cg<1>, 1, CG_THREADS, s, h->C, rhs, out);
+        else if (n <= 2 * CG_THREADS) launch(k_coarsest_cg<2>, 1, CG_THREADS, s, h->C, rhs, out);
+        else launch(k_coarsest_cg<4>, 1, CG_THREADS, s, h->C, rhs, out);
+        pe();
         count++;
     }
 };
@@ -624,6 +689,8 @@ static float sched_weight_iter(int n, int it) {
 // whole preconditioner, so no sweep is available to carry the dot).
 __global__ void __launch_bounds__(128) k_dot_rho(DLevel L, const float* z, const float* r, double* partials,
                                                  PcgState* st) {
+    griddep_wait();
+    griddep_launch();
     __shared__ double shd[4];
     __shared__ bool last;
     const int leaf = blockIdx.x, t = threadIdx.x;
@@ -661,8 +728,9 @@ static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool sk
     if (l == h->nlev - 1) {
         E.coarsest(rhs, lhs);
         if (dot.r) {
-            k_dot_rho<<<(unsigned)D.L.nl, 128, 0, E.s>>>(D.L, lhs, dot.r, dot.partials, dot.st);
-            CHECK_LAUNCH();
+            E.pb("L0 dot");
+            launch(k_dot_rho, (unsigned)D.L.nl, 128, E.s, D.L, (const float*)lhs, dot.r, dot.partials, dot.st);
+            E.pe();
             E.count++;
         }
         return;
@@ -764,8 +832,7 @@ static void enqueue_mg_cycle(Enq& E, int l, float* lhs, const float* rhs) {
     for (int mu = 0; mu < 2; ++mu) enqueue_mg_cycle(E, l + 1, P.lhs, P.rhs);
     // prolongation (alpha 0.5) + post-smoothing
     if (sm == UAAMG_SMOOTHER_RED_BLACK_GAUSS_SEIDEL) {
-        k_materialize<SrcProlong><<<(unsigned)D.L.nl, 128, 0, E.s>>>(D.L, SrcProlong{cur, P.lhs, 0.5f}, oth);
-        CHECK_LAUNCH();
+        launch(k_materialize<SrcProlong>, (unsigned)D.L.nl, 128, E.s, D.L, SrcProlong{cur, P.lhs, 0.5f}, oth);
         E.count++;
         std::swap(cur, oth);
         for (int i = 0; i < n; ++i) smooth(n - 1 - i, 0, cur, oth);
@@ -793,31 +860,38 @@ static void enqueue_setup(Enq& E, cudaGraphConditionalHandle cond, int use_cond)
     LevelDev& D0 = h->lv[0];
     const size_t n0 = (size_t)D0.L.nl * UAAMG_LEAF;
     CK(cudaMemsetAsync(h->p, 0, n0 * 4, E.s));
-    k_mask_vec<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->x);
-    CHECK_LAUNCH();
-    k_mask_vec<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->b);
-    CHECK_LAUNCH();
-    k_pcg_init<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->x, h->b, h->r, h->partials, h->st, cond, use_cond);
-    CHECK_LAUNCH();
+    E.pb("L0 mask inputs");
+    launch(k_mask_vec, (unsigned)D0.L.nl, 128, E.s, D0.L, h->x);
+    launch(k_mask_vec, (unsigned)D0.L.nl, 128, E.s, D0.L, h->b);
+    E.pe();
+    E.pb("L0 pcg init (residual+absmax)");
+    launch(k_pcg_init, (unsigned)D0.L.nl, 128, E.s, D0.L, (const float*)h->x, (const float*)h->b, h->r, h->partials,
+           h->st, cond, use_cond);
+    E.pe();
     E.count += 3;
 }
 static void enqueue_body(Enq& E, cudaGraphConditionalHandle cond, int use_cond) {
     uaamg_poisson* h = E.h;
     LevelDev& D0 = h->lv[0];
     enqueue_precond(E, 0, h->z, h->r, true, DotOut{h->r, h->partials, h->st});
-    k_pcg_update_p<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->z, h->p, h->x, h->st);
-    CHECK_LAUNCH();
-    k_pcg_Ap<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->p, h->q, h->partials, h->st);
-    CHECK_LAUNCH();
-    k_pcg_update_r<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->q, h->r, h->partials, h->st, cond, use_cond);
-    CHECK_LAUNCH();
+    E.pb("L0 pcg x,p update");
+    launch(k_pcg_update_p, (unsigned)D0.L.nl, 128, E.s, D0.L, (const float*)h->z, h->p, h->x, (const PcgState*)h->st);
+    E.pe();
+    E.pb("L0 pcg Ap+dot");
+    launch(k_pcg_Ap, (unsigned)D0.L.nl, 128, E.s, D0.L, (const float*)h->p, h->q, h->partials, h->st);
+    E.pe();
+    E.pb("L0 pcg r update+absmax");
+    launch(k_pcg_update_r, (unsigned)D0.L.nl, 128, E.s, D0.L, (const float*)h->q, h->r, h->partials, h->st, cond,
+           use_cond);
+    E.pe();
     E.count += 3;
 }
 static void enqueue_finish(Enq& E) {
     uaamg_poisson* h = E.h;
     LevelDev& D0 = h->lv[0];
-    k_pcg_finish<<<(unsigned)D0.L.nl, 128, 0, E.s>>>(D0.L, h->p, h->x, h->st);
-    CHECK_LAUNCH();
+    E.pb("L0 pcg finish");
+    launch(k_pcg_finish, (unsigned)D0.L.nl, 128, E.s, D0.L, (const float*)h->p, h->x, (const PcgState*)h->st);
+    E.pe();
     E.count += 1;
 }
 
@@ -1004,6 +1078,10 @@ int uaamg_device_count(void) {
 
 int uaamg_poisson_create(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights, float dt, float dx,
                          uaamg_poisson** out) {
+    {
+        const char* e = getenv("UAAMG_PDL");
+        g_use_pdl = !(e && e[0] == '0');
+    }
     if (!out) { set_error("out is NULL"); return UAAMG_ERR_INVALID_ARGUMENT; }
     *out = nullptr;
     int ndev = 0;
@@ -1014,11 +1092,15 @@ int uaamg_poisson_create(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_gri
     uaamg_poisson* h = new (std::nothrow) uaamg_poisson();
     if (!h) { set_error("host out of memory"); return UAAMG_ERR_OUT_OF_MEMORY; }
     try {
-        CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
-        CK(cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking));
+        cudaError_t ce = cudaSuccess;
+        h->ctx = device_ctx(&ce);
+        CK(ce);
+        CK(ctx_stream_acquire(h->ctx, &h->own_stream));
+        CK(ctx_stream_acquire(h->ctx, &h->body_stream));
         h->stream = h->own_stream;
-        CK(cudaMallocHost(&h->st_host, sizeof(PcgState)));
-        CK(cudaMallocHost(&h->scalar_host, 64));
+        CK(ctx_pinned_acquire(h->ctx, sizeof(PcgState) + 256, &h->pin_state, &h->pin_state_cap));
+        h->st_host = reinterpret_cast<PcgState*>(h->pin_state);
+        h->scalar_host = reinterpret_cast<float*>((char*)h->pin_state + ((sizeof(PcgState) + 63) & ~size_t(63)));
         build_hierarchy(h, liquid_phi, face_weights, dt, dx);
     } catch (const UaamgError& e) {
         uaamg_poisson_destroy(h);
@@ -1036,11 +1118,14 @@ int uaamg_poisson_destroy(uaamg_poisson* h) {
     if (!h) return UAAMG_SUCCESS;
     if (h->stream) cudaStreamSynchronize(h->stream);
     destroy_graph(h);
-    if (h->dmem) cudaFree(h->dmem);
-    if (h->st_host) cudaFreeHost(h->st_host);
-    if (h->scalar_host) cudaFreeHost(h->scalar_host);
-    if (h->body_stream) cudaStreamDestroy(h->body_stream);
-    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    if (h->ctx) {
+        if (h->dmem) cudaFreeAsync(h->dmem, h->stream);
+        if (h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
+        ctx_pinned_release(h->ctx, h->pin_state, h->pin_state_cap);
+        ctx_pinned_release(h->ctx, h->pin_stage, h->pin_stage_cap);
+        ctx_stream_release(h->ctx, h->body_stream);
+        ctx_stream_release(h->ctx, h->own_stream);
+    }
     delete h;
     return UAAMG_SUCCESS;
 }
@@ -1111,6 +1196,7 @@ static int build_rhs_impl(uaamg_poisson* h, const uaamg_leaf_grid* fw, const uaa
     float invdx = 1.0f / D0.dx;
     k_build_rhs<<<(unsigned)D0.L.nl, 128, 0, h->stream>>>(D0.L.mask, D0.org, g0.g, g1.g, g2.g, g3.g, g4.g, invdx, d_out);
     CHECK_LAUNCH();
+    h->launches++;
     for (void* p : tofree) CK(cudaFreeAsync(p, h->stream));
     return UAAMG_SUCCESS;
 }
@@ -1213,7 +1299,10 @@ struct Scratch {
     float* c = nullptr;
     cudaStream_t s;
     Scratch(size_t bytes, cudaStream_t st) : s(st) {
-        CK(cudaMallocAsync(&a, std::max<size_t>(bytes, 16) * 3, s));
+        cudaError_t ce = cudaSuccess;
+        DeviceCtx* dc = device_ctx(&ce);
+        CK(ce);
+        CK(ctx_dev_alloc(dc, (void**)&a, std::max<size_t>(bytes, 16) * 3, s));
         b = a + std::max<size_t>(bytes, 16) / 4;
         c = b + std::max<size_t>(bytes, 16) / 4;
     }
@@ -1374,6 +1463,56 @@ int uaamg_poisson_precondition(uaamg_poisson* h, const float* r, float* z) {
     ABI_END
 }
 
+int uaamg_poisson_profile_pcg(uaamg_poisson* h, float* d_pressure, const float* d_rhs, int max_classes, char* names,
+                              double* total_ms, int64_t* counts, int* nclasses) {
+    ABI_BEGIN
+    require(h && d_pressure && d_rhs && names && total_ms && counts && nclasses, "NULL argument");
+    size_t nb = vec_bytes(h, 0);
+    *nclasses = 0;
+    if (!nb) return UAAMG_SUCCESS;
+    if (h->smoother == UAAMG_SMOOTHER_SPAI0) ensure_spai0(h);
+    CK(cudaMemcpyAsync(h->x, d_pressure, nb, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->b, d_rhs, nb, cudaMemcpyDeviceToDevice, h->stream));
+    init_state(h);
+    std::vector<ProfRec> prof;
+    Enq E{h, h->stream};
+    E.prof = &prof;
+    enqueue_setup(E, 0, 0);
+    CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    while (h->st_host->status == PCG_RUNNING) {
+        enqueue_body(E, 0, 0);
+        CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    enqueue_finish(E);
+    CK(cudaStreamSynchronize(h->stream));
+    h->launches += E.count;
+    h->iterations = h->st_host->iterations_taken;
+    std::vector<std::string> lab;
+    for (auto& r : prof) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, r.a, r.b));
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+        int k = (int)(std::find(lab.begin(), lab.end(), r.label) - lab.begin());
+        if (k == (int)lab.size()) {
+            if (k >= max_classes) continue;
+            lab.push_back(r.label);
+            total_ms[k] = 0;
+            counts[k] = 0;
+            snprintf(names + 64 * k, 64, "%s", r.label.c_str());
+        }
+        total_ms[k] += ms;
+        counts[k] += 1;
+    }
+    *nclasses = (int)lab.size();
+    CK(cudaMemcpyAsync(d_pressure, h->x, nb, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return h->st_host->status == PCG_SUCCESS ? UAAMG_SUCCESS : UAAMG_FAILED;
+    ABI_END
+}
+
 int uaamg_poisson_set_stream(uaamg_poisson* h, void* stream) {
     if (!h) { set_error("NULL handle"); return UAAMG_ERR_INVALID_ARGUMENT; }
     cudaStream_t s = stream ? (cudaStream_t)stream : h->own_stream;
@@ -1388,6 +1527,6 @@ int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph) {
     h->use_graph = use_graph ? 1 : 0;
     return UAAMG_SUCCESS;
 }
-int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h) { return h ? h->last_launches : 0; }
+int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h) { return h ? h->launches : 0; }
 
 }  // extern "C"

@@ -18,6 +18,14 @@ namespace uaamg {
 
 #define FULLMASK 0xffffffffu
 
+// Programmatic dependent launch: every solve kernel is launched with
+// programmatic stream serialisation, waits for its predecessor's memory
+// before touching anything (griddepcontrol.wait), and lets its successor
+// start launching right away, which hides the kernel-to-kernel launch gap of
+// the many small coarse-level kernels.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // lhs sources: what the stencil reads as "x" at any voxel.  Besides a stored
 // vector they compute, on the fly, the result of a pass the reference stores
@@ -124,7 +132,6 @@ struct SrcProlong {
     }
 };
 
-// p_new = z + beta * p (levelXPlusAlphaY), read on the fly
 // ---------------------------------------------------------------------------
 // The 6-neighbour off-diagonal sum of one float4 (4 z-consecutive voxels):
 // off = ((x+ c_x+ + x- c_x-) + (y+ c_y+ + y- c_y-)) + (z+ c_z+ + z- c_z-)
@@ -345,6 +352,8 @@ __device__ __forceinline__ float4 sweep_value(const DLevel& L, int leaf, int t, 
 template <int MODE, class Src>
 __global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b, float* out, float w, float wsor,
                                                float one_minus_wsor, DotOut dot, int* spai0_ready) {
+    griddep_wait();
+    griddep_launch();
     const int leaf = blockIdx.x, t = threadIdx.x;
     float4 xc;
     unsigned m;
@@ -374,6 +383,8 @@ __global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b
 // out = value of a source (materialise a first sweep or a prolongation)
 template <class Src>
 __global__ void __launch_bounds__(128) k_materialize(DLevel L, Src src, float* out) {
+    griddep_wait();
+    griddep_launch();
     const int leaf = blockIdx.x, t = threadIdx.x;
     float4 v = src.get4(L, leaf, t);
     unsigned m = mask4(L.mask, leaf, t);
@@ -388,6 +399,8 @@ __global__ void __launch_bounds__(128) k_materialize(DLevel L, Src src, float* o
 // coarse = 0.125 * sum of the active fine values of the 2x2x2 block (.cpp:1624-1684)
 template <bool RESID>
 __global__ void __launch_bounds__(128) k_restrict(DLevel L, const float* x, const float* b, float* coarse) {
+    griddep_wait();
+    griddep_launch();
     __shared__ float rs[UAAMG_LEAF];
     const int leaf = blockIdx.x, t = threadIdx.x;
     float4 r;
@@ -422,6 +435,8 @@ __global__ void __launch_bounds__(128) k_restrict(DLevel L, const float* x, cons
 // ---------------------------------------------------------------------------
 // PCG vector kernels (PoissonSolver::solveMultigridPCG, .cpp:2155-2226)
 __global__ void __launch_bounds__(128) k_mask_vec(DLevel L, float* v) {
+    griddep_wait();
+    griddep_launch();
     const int leaf = blockIdx.x, t = threadIdx.x;
     unsigned m = mask4(L.mask, leaf, t);
     if (m == 0xF) return;
@@ -441,6 +456,8 @@ __device__ __forceinline__ void set_cond(cudaGraphConditionalHandle h, int use, 
 __global__ void __launch_bounds__(128) k_pcg_init(DLevel L, const float* x, const float* b, float* r,
                                                   double* partials, PcgState* st,
                                                   cudaGraphConditionalHandle cond, int use_cond) {
+    griddep_wait();
+    griddep_launch();
     __shared__ float shf[4];
     __shared__ double shd[4];
     __shared__ bool last;
@@ -476,6 +493,8 @@ __global__ void __launch_bounds__(128) k_pcg_init(DLevel L, const float* x, cons
 // x += alpha_prev * p_prev (line 16, skipped in the first iteration); p = z + beta p (line 16)
 __global__ void __launch_bounds__(128) k_pcg_update_p(DLevel L, const float* z, float* p, float* x,
                                                       const PcgState* st) {
+    griddep_wait();
+    griddep_launch();
     const int leaf = blockIdx.x, t = threadIdx.x;
     const float beta = st->beta, alpha = st->alpha;
     const int first = st->first;
@@ -497,6 +516,8 @@ __global__ void __launch_bounds__(128) k_pcg_update_p(DLevel L, const float* z, 
 
 // lines 6-7: q = A p; sigma = p.q; alpha = rho / sigma
 __global__ void __launch_bounds__(128) k_pcg_Ap(DLevel L, const float* p, float* q, double* partials, PcgState* st) {
+    griddep_wait();
+    griddep_launch();
     __shared__ double shd[4];
     __shared__ bool last;
     const int leaf = blockIdx.x, t = threadIdx.x;
@@ -521,6 +542,8 @@ __global__ void __launch_bounds__(128) k_pcg_Ap(DLevel L, const float* p, float*
 // lines 8-12: r -= alpha q; nu = |r|_inf; convergence / divergence test
 __global__ void __launch_bounds__(128) k_pcg_update_r(DLevel L, const float* q, float* r, double* partials,
                                                       PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
+    griddep_wait();
+    griddep_launch();
     __shared__ float shf[4];
     __shared__ bool last;
     const int leaf = blockIdx.x, t = threadIdx.x;
@@ -560,6 +583,8 @@ __global__ void __launch_bounds__(128) k_pcg_update_r(DLevel L, const float* q, 
 
 // line 10 on success, and line 16 of the last iteration when max_iter is reached
 __global__ void __launch_bounds__(128) k_pcg_finish(DLevel L, const float* p, float* x, const PcgState* st) {
+    griddep_wait();
+    griddep_launch();
     const int s = st->status;
     if (s != PCG_SUCCESS && s != PCG_FAILED_MAXITER) return;
     if (st->iterations_taken == 0 && st->iter == 0) return;  // converged before the loop
@@ -576,6 +601,8 @@ __global__ void __launch_bounds__(128) k_pcg_finish(DLevel L, const float* p, fl
 // |v|_inf over a level (levelAbsMax), result in out[0]
 __global__ void __launch_bounds__(128) k_absmax(DLevel L, const float* v, double* partials, unsigned* ticket,
                                                 float* out) {
+    griddep_wait();
+    griddep_launch();
     __shared__ float shf[4];
     __shared__ bool last;
     const int leaf = blockIdx.x, t = threadIdx.x;
@@ -609,124 +636,122 @@ struct DCoarsest {
     const float* val;      // [n][6]
 };
 
-#define CG_THREADS 512
-#define CG_ROWS 8  // CG_THREADS * CG_ROWS >= 4096 >= coarsest DOF count
+#define CG_THREADS 1024
+#define CG_MAX_ROWS 4  // CG_THREADS * CG_MAX_ROWS = 4096 > coarsest DOF count (<= 4000)
 
-__device__ __forceinline__ double cg_block_sum(double v, double* sh) {
+// Block reductions in one barrier: warps reduce with shfl_down, lane 0 of each
+// warp publishes, every warp reduces the 32 partials the same way and
+// broadcasts lane 0, so all threads hold bit-identical scalars (the CG's
+// control flow depends on them).
+__device__ __forceinline__ float cg_warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULLMASK, v, o);
-    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if ((threadIdx.x & 31) == 0) sh[w] = v;
-    __syncthreads();
-    if (w == 0) {
-        double s = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(FULLMASK, s, o);
-        if (threadIdx.x == 0) sh[32] = s;
-    }
-    __syncthreads();
-    double r = sh[32];
-    __syncthreads();
-    return r;
+    return __shfl_sync(FULLMASK, v, 0);
 }
-__device__ __forceinline__ double2 cg_block_sum2(double a, double b, double* sh) {
+__device__ __forceinline__ float cg_block_sum(float v, float* buf) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v = cg_warp_sum(v);
+    if (lane == 0) buf[w] = v;
+    __syncthreads();
+    return cg_warp_sum(buf[lane]);
+}
+__device__ __forceinline__ float2 cg_block_sum2(float a, float b, float* buf) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_down_sync(FULLMASK, a, o);
         b += __shfl_down_sync(FULLMASK, b, o);
     }
-    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if ((threadIdx.x & 31) == 0) { sh[w] = a; sh[32 + w] = b; }
+    if (lane == 0) { buf[w] = a; buf[32 + w] = b; }
     __syncthreads();
-    if (w == 0) {
-        double s = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
-        double u = (threadIdx.x < nw) ? sh[32 + threadIdx.x] : 0.0;
+    float x = buf[lane], y = buf[32 + lane];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            s += __shfl_down_sync(FULLMASK, s, o);
-            u += __shfl_down_sync(FULLMASK, u, o);
-        }
-        if (threadIdx.x == 0) { sh[64] = s; sh[65] = u; }
+    for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_down_sync(FULLMASK, x, o);
+        y += __shfl_down_sync(FULLMASK, y, o);
     }
-    __syncthreads();
-    double2 r = make_double2(sh[64], sh[65]);
-    __syncthreads();
-    return r;
+    return make_float2(__shfl_sync(FULLMASK, x, 0), __shfl_sync(FULLMASK, y, 0));
 }
 
-__global__ void __launch_bounds__(CG_THREADS) k_coarsest_cg(DCoarsest C, const float* rhs, float* out) {
-    __shared__ float ps[CG_THREADS * CG_ROWS];
-    __shared__ double sh[72];
+// ROWS rows per thread (row i = tid + k * CG_THREADS); the matrix rows stay in
+// registers for the whole solve.  Three barriers per CG iteration.
+template <int ROWS>
+__global__ void __launch_bounds__(CG_THREADS, 1) k_coarsest_cg(DCoarsest C, const float* rhs, float* out) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ float ps[CG_THREADS * ROWS];
+    __shared__ float red[3][64];  // rotating reduction buffers (no reuse within 2 barriers)
     const int tid = threadIdx.x, n = C.n;
-    float x[CG_ROWS], r[CG_ROWS], p[CG_ROWS], z[CG_ROWS], tq[CG_ROWS];
-    double bb = 0;
+    float x[ROWS], r[ROWS], p[ROWS], z[ROWS], dg[ROWS], iv[ROWS], val[ROWS][6];
+    int col[ROWS][6];
+    float bb = 0.f;
 #pragma unroll
-    for (int k = 0; k < CG_ROWS; ++k) {
-        int i = tid + k * CG_THREADS;
+    for (int k = 0; k < ROWS; ++k) {
+        const int i = tid + k * CG_THREADS;
+        const bool ok = i < n;
         x[k] = 0.f;
-        r[k] = (i < n) ? rhs[C.dof_slot[i]] : 0.f;
-        bb += (double)r[k] * r[k];
-    }
-    const float rhsNorm2 = (float)cg_block_sum(bb, sh);
-    bool done = (rhsNorm2 == 0.f);
-    float threshold = fmaxf(__fmul_rn(__fmul_rn(FLT_EPSILON, FLT_EPSILON), rhsNorm2), FLT_MIN);
-    if (!done && rhsNorm2 < threshold) done = true;  // residualNorm2 == rhsNorm2 for x = 0
-    if (!done) {
-        double an = 0;
+        r[k] = ok ? rhs[C.dof_slot[i]] : 0.f;
+        dg[k] = ok ? C.diag[i] : 0.f;
+        iv[k] = ok ? C.invd[i] : 0.f;
 #pragma unroll
-        for (int k = 0; k < CG_ROWS; ++k) {
-            int i = tid + k * CG_THREADS;
-            p[k] = (i < n) ? __fmul_rn(C.invd[i], r[k]) : 0.f;
-            an += (double)r[k] * p[k];
+        for (int e = 0; e < 6; ++e) {
+            col[k][e] = ok ? C.col[i * 6 + e] : -1;
+            val[k][e] = ok ? C.val[i * 6 + e] : 0.f;
         }
-        float absNew = (float)cg_block_sum(an, sh);
+        bb = __fadd_rn(bb, __fmul_rn(r[k], r[k]));
+    }
+    int rb = 0;
+    const float rhsNorm2 = cg_block_sum(bb, red[rb]);
+    rb = rb == 2 ? 0 : rb + 1;
+    const float threshold = fmaxf(__fmul_rn(__fmul_rn(FLT_EPSILON, FLT_EPSILON), rhsNorm2), FLT_MIN);
+    // rhsNorm2 == 0 -> x = 0; residualNorm2 (== rhsNorm2 for x = 0) < threshold -> x = 0
+    if (rhsNorm2 != 0.f && !(rhsNorm2 < threshold)) {
+        float an = 0.f;
+#pragma unroll
+        for (int k = 0; k < ROWS; ++k) {
+            p[k] = __fmul_rn(iv[k], r[k]);
+            an = __fadd_rn(an, __fmul_rn(r[k], p[k]));
+        }
+        float absNew = cg_block_sum(an, red[rb]);
+        rb = rb == 2 ? 0 : rb + 1;
         for (int it = 0; it < 10; ++it) {
 #pragma unroll
-            for (int k = 0; k < CG_ROWS; ++k) ps[tid + k * CG_THREADS] = p[k];
+            for (int k = 0; k < ROWS; ++k) ps[tid + k * CG_THREADS] = p[k];
             __syncthreads();
-            double pt = 0;
+            float pt = 0.f, tq[ROWS];
 #pragma unroll
-            for (int k = 0; k < CG_ROWS; ++k) {
-                int i = tid + k * CG_THREADS;
-                float s = 0.f;
-                if (i < n) {
-                    s = __fmul_rn(C.diag[i], p[k]);
+            for (int k = 0; k < ROWS; ++k) {
+                float s = __fmul_rn(dg[k], p[k]);
 #pragma unroll
-                    for (int e = 0; e < 6; ++e) {
-                        int c = C.col[i * 6 + e];
-                        if (c >= 0) s = __fadd_rn(s, __fmul_rn(C.val[i * 6 + e], ps[c]));
-                    }
-                }
+                for (int e = 0; e < 6; ++e)
+                    if (col[k][e] >= 0) s = __fadd_rn(s, __fmul_rn(val[k][e], ps[col[k][e]]));
                 tq[k] = s;
-                pt += (double)p[k] * s;
+                pt = __fadd_rn(pt, __fmul_rn(p[k], s));
             }
-            const float alpha = __fdiv_rn(absNew, (float)cg_block_sum(pt, sh));
-            double rr = 0;
+            const float alpha = __fdiv_rn(absNew, cg_block_sum(pt, red[rb]));
+            rb = rb == 2 ? 0 : rb + 1;
+            float rr = 0.f, rz = 0.f;
 #pragma unroll
-            for (int k = 0; k < CG_ROWS; ++k) {
+            for (int k = 0; k < ROWS; ++k) {
                 x[k] = __fmaf_rn(alpha, p[k], x[k]);
                 r[k] = __fmaf_rn(-alpha, tq[k], r[k]);
-                rr += (double)r[k] * r[k];
+                z[k] = __fmul_rn(iv[k], r[k]);
+                rr = __fadd_rn(rr, __fmul_rn(r[k], r[k]));
+                rz = __fadd_rn(rz, __fmul_rn(r[k], z[k]));
             }
-            double rz = 0;
-#pragma unroll
-            for (int k = 0; k < CG_ROWS; ++k) {
-                int i = tid + k * CG_THREADS;
-                z[k] = (i < n) ? __fmul_rn(C.invd[i], r[k]) : 0.f;
-                rz += (double)r[k] * z[k];
-            }
-            double2 s2 = cg_block_sum2(rr, rz, sh);
-            if ((float)s2.x < threshold) break;
+            const float2 s2 = cg_block_sum2(rr, rz, red[rb]);
+            rb = rb == 2 ? 0 : rb + 1;
+            if (s2.x < threshold) break;
             const float absOld = absNew;
-            absNew = (float)s2.y;
+            absNew = s2.y;
             const float beta = __fdiv_rn(absNew, absOld);
 #pragma unroll
-            for (int k = 0; k < CG_ROWS; ++k) p[k] = __fmaf_rn(beta, p[k], z[k]);
+            for (int k = 0; k < ROWS; ++k) p[k] = __fmaf_rn(beta, p[k], z[k]);
         }
     }
 #pragma unroll
-    for (int k = 0; k < CG_ROWS; ++k) {
-        int i = tid + k * CG_THREADS;
+    for (int k = 0; k < ROWS; ++k) {
+        const int i = tid + k * CG_THREADS;
         if (i < n) out[C.dof_slot[i]] = x[k];
     }
 }

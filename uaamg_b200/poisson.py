@@ -235,6 +235,25 @@ class PoissonSolver:
         _lib.check(L.uaamg_poisson_precondition(h, r.ctypes.data, z.ctypes.data), "precondition")
         return z
 
+    def profile_pcg(self, d_pressure, d_rhs, max_classes: int = 64):
+        """One solve with CUDA events around every kernel (device tensors).
+        Returns {kernel class: (total ms, launches)}."""
+        L, h = self._configure()
+        names = C.create_string_buffer(64 * max_classes)
+        ms = np.zeros(max_classes, np.float64)
+        cnt = np.zeros(max_classes, np.int64)
+        nc = C.c_int(0)
+        rc = L.uaamg_poisson_profile_pcg(h, d_pressure.data_ptr(), d_rhs.data_ptr(), max_classes,
+                                         C.addressof(names), ms.ctypes.data, cnt.ctypes.data, C.byref(nc))
+        _lib.check(rc, "profile_pcg")
+        self.mIterationTaken = int(L.uaamg_poisson_iterations(h))
+        raw = names.raw
+        out = {}
+        for k in range(nc.value):
+            nm = raw[64 * k: 64 * k + 64].split(b"\0", 1)[0].decode()
+            out[nm] = (float(ms[k]), int(cnt[k]))
+        return out
+
     @property
     def final_residual(self) -> float:
         return float(_lib.lib().uaamg_poisson_final_residual(self.mMultigridHierarchy._h))
