@@ -123,6 +123,15 @@ int uaamg_poisson_solve_mg(uaamg_poisson* h, float* pressure, const float* rhs, 
 int uaamg_poisson_solve_mg_device(uaamg_poisson* h, float* d_pressure, const float* d_rhs,
                                   int* iterations);
 
+/* r = b - A x over level 0 and |r|_inf: LaplacianWithLevel::residualApply
+ * (simd_vdb_poisson.cpp:1347-1357) followed by PoissonSolver::levelAbsMax
+ * (.cpp:2270-2276, grid_abs_max_op, openvdb_grid_math_op.h:4-43).  Device
+ * pointers; d_r: float[leaf][512], d_norm: one float.  Uses the handle's
+ * reduction scratch (one partial per leaf), so calls on one handle must not
+ * overlap; returns after enqueueing on the handle's stream. */
+int uaamg_poisson_residual_norm_device(uaamg_poisson* h, const float* d_x, const float* d_b, float* d_r,
+                                       float* d_norm);
+
 /* Per-level operators, public methods of LaplacianWithLevel
  * (simd_vdb_poisson.h:90-115).  Host pointers, level-dense vectors.
  *   mode: UAAMG_MODE_*; weight: Jacobi weight; w_sor: SOR weight of GS modes.

@@ -337,3 +337,19 @@ def test_full_size_plain_poisson(gpu):
     bv = np.zeros(n); bv[idx[m]] = rhs[m]
     assert np.abs(bv - A @ pv).max() <= 1e-5 * np.abs(bv).max()
     assert s.kernel_launches > 0
+
+
+def test_residual_norm_device(scene64, gpu):
+    torch = gpu
+    sc, lap, ref = scene64
+    rhs = ref.build_rhs(sc.face_weights, sc.vx, sc.vy, sc.vz, sc.solid_velocity)
+    x = rand_vec(ref, 0, 80)
+    dx, db = torch.from_numpy(x).cuda(), torch.from_numpy(rhs).cuda()
+    dr = torch.empty_like(db)
+    dn = torch.empty(1, device="cuda")
+    lap.set_stream(torch.cuda.current_stream().cuda_stream)
+    lap.residual_norm_device(dx, db, dr, dn)
+    torch.cuda.synchronize()
+    r = ref.apply(0, "residual", x, rhs)
+    assert np.array_equal(dr.cpu().numpy(), r)
+    assert float(dn.item()) == ref.abs_max(r)

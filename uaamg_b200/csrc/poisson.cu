@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1459,6 +1460,22 @@ int uaamg_poisson_precondition(uaamg_poisson* h, const float* r, float* z) {
     enqueue_precond(E, 0, S.a, S.b, true, DotOut{nullptr, nullptr, nullptr});
     CK(cudaMemcpyAsync(z, S.a, nb, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_poisson_residual_norm_device(uaamg_poisson* h, const float* d_x, const float* d_b, float* d_r,
+                                       float* d_norm) {
+    ABI_BEGIN
+    require(h && d_x && d_b && d_r && d_norm, "NULL argument");
+    LevelDev& D0 = h->lv[0];
+    if (D0.L.nl == 0) {
+        CK(cudaMemsetAsync(d_norm, 0, sizeof(float), h->stream));
+        return UAAMG_SUCCESS;
+    }
+    launch(k_residual_absmax, (unsigned)D0.L.nl, 128, h->stream, D0.L, d_x, d_b, d_r, h->partials,
+           &h->st->ticket[5], d_norm);
+    h->launches++;
     return UAAMG_SUCCESS;
     ABI_END
 }

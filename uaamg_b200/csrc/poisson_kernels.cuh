@@ -598,6 +598,29 @@ __global__ void __launch_bounds__(128) k_pcg_finish(DLevel L, const float* p, fl
     st4(x, leaf, t, xx);
 }
 
+// r = b - A x and |r|_inf (residualApply + levelAbsMax), result in out[0]
+__global__ void __launch_bounds__(128) k_residual_absmax(DLevel L, const float* x, const float* b, float* r,
+                                                         double* partials, unsigned* ticket, float* out) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ float shf[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    float4 xc;
+    unsigned m;
+    float4 res = sweep_value<M_RESIDUAL>(L, leaf, t, SrcPlain{x}, b, 0.f, 0.f, 0.f, xc, m);
+    st4(r, leaf, t, res);
+    float a = nanmax(nanmax(absprop(res.x), absprop(res.y)), nanmax(absprop(res.z), absprop(res.w)));
+    float part = block_max128(a, shf);
+    if (publish_partial((double)part, partials, ticket, &last)) {
+        float nu = gather_max(partials, shf);
+        if (t == 0) {
+            *out = nu;
+            *ticket = 0;
+        }
+    }
+}
+
 // |v|_inf over a level (levelAbsMax), result in out[0]
 __global__ void __launch_bounds__(128) k_absmax(DLevel L, const float* v, double* partials, unsigned* ticket,
                                                 float* out) {

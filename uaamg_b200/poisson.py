@@ -122,6 +122,15 @@ class LaplacianWithLevel:
                    "build_rhs")
         return rhs
 
+    def residual_norm_device(self, d_x, d_b, d_r, d_norm) -> None:
+        """r = b - A x and |r|_inf into device tensors (enqueued on the handle's stream)."""
+        _lib.check(_lib.lib().uaamg_poisson_residual_norm_device(self._h, d_x.data_ptr(), d_b.data_ptr(),
+                                                                 d_r.data_ptr(), d_norm.data_ptr()),
+                   "residual_norm_device")
+
+    def set_stream(self, stream_ptr) -> None:
+        _lib.check(_lib.lib().uaamg_poisson_set_stream(self._h, stream_ptr), "set_stream")
+
     # --- per-level operators (public methods of the reference class)
     def apply(self, level, mode, lhs, rhs=None, weight=6.0 / 7.0, w_sor=1.2):
         modes = {"jacobi": 0, "residual": 1, "laplacian": 2, "red_gs": 3, "black_gs": 4, "spai0": 5}
