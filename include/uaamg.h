@@ -132,6 +132,24 @@ int uaamg_poisson_solve_mg_device(uaamg_poisson* h, float* d_pressure, const flo
 int uaamg_poisson_residual_norm_device(uaamg_poisson* h, const float* d_x, const float* d_b, float* d_r,
                                        float* d_norm);
 
+/* Allocation-free variant of uaamg_poisson_residual_norm_device, same inputs,
+ * outputs and results.  No counterpart in the reference.  For callers that
+ * must not allocate GPU memory while they run, e.g. a simulation loop that
+ * reserves its whole device budget up front (an allocation can synchronise the
+ * device, take milliseconds, or fail once the budget is spent) or a host
+ * application that owns the device heap through its own allocator.  The
+ * reduction scratch is a fixed array inside the library (2 MiB per device,
+ * kept until the process exits) instead of memory allocated per handle;
+ * nothing is allocated by the call.  Limit: level 0 may hold at most 262144
+ * leaves (134 M voxels); larger levels are rejected with
+ * UAAMG_ERR_INVALID_ARGUMENT.  The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture.  All calls on a device share the one
+ * array, so calls whose kernels overlap on the GPU (different streams or
+ * handles) race and must be serialised by the caller. */
+int uaamg_poisson_residual_norm_noalloc(uaamg_poisson* h, const float* d_x, const float* d_b, float* d_r,
+                                        float* d_norm);
+
 /* Per-level operators, public methods of LaplacianWithLevel
  * (simd_vdb_poisson.h:90-115).  Host pointers, level-dense vectors.
  *   mode: UAAMG_MODE_*; weight: Jacobi weight; w_sor: SOR weight of GS modes.

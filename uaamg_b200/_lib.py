@@ -59,6 +59,7 @@ EXPORTS = [
     ("uaamg_poisson_solve_mg", i32, [vp, vp, vp, C.POINTER(C.c_int)]),
     ("uaamg_poisson_solve_mg_device", i32, [vp, vp, vp, C.POINTER(C.c_int)]),
     ("uaamg_poisson_residual_norm_device", i32, [vp, vp, vp, vp, vp]),
+    ("uaamg_poisson_residual_norm_noalloc", i32, [vp, vp, vp, vp, vp]),
     ("uaamg_poisson_level_apply", i32, [vp, i32, i32, f32, f32, vp, vp, vp]),
     ("uaamg_poisson_level_first_sweep", i32, [vp, i32, i32, f32, f32, vp, vp]),
     ("uaamg_poisson_level_restrict", i32, [vp, i32, vp, vp]),

@@ -1480,6 +1480,61 @@ int uaamg_poisson_residual_norm_device(uaamg_poisson* h, const float* d_x, const
     ABI_END
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of uaamg_poisson_residual_norm_device.  Its reduction
+// scratch (one double per level-0 leaf, then the finishing ticket) lives in
+// this file-scope array, which every GPU that loads the library holds until
+// the process exits; the call itself allocates nothing.
+#define UAAMG_NOALLOC_MAX_LEAVES 262144
+static __device__ __align__(256) unsigned char g_noalloc_scratch[(UAAMG_NOALLOC_MAX_LEAVES + 32) * sizeof(double)];
+
+// Device address of g_noalloc_scratch on each device, resolved once per device
+// (host code may not use the symbol itself: it names a host-side stand-in).
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_addr[64] = {nullptr};
+
+static void* noalloc_scratch_on_current_device() {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_error("device index %d out of range", dev);
+        throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT};
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[dev] = p;
+    }
+    return g_noalloc_addr[dev];
+}
+
+int uaamg_poisson_residual_norm_noalloc(uaamg_poisson* h, const float* d_x, const float* d_b, float* d_r,
+                                        float* d_norm) {
+    ABI_BEGIN
+    require(h && d_x && d_b && d_r && d_norm, "NULL argument");
+    LevelDev& D0 = h->lv[0];
+    if (D0.L.nl > UAAMG_NOALLOC_MAX_LEAVES) {
+        set_error("uaamg_poisson_residual_norm_noalloc: level 0 has %d leaves, the allocation-free variant "
+                  "handles at most %d (use uaamg_poisson_residual_norm_device)",
+                  D0.L.nl, UAAMG_NOALLOC_MAX_LEAVES);
+        return UAAMG_ERR_INVALID_ARGUMENT;
+    }
+    char* scratch = (char*)noalloc_scratch_on_current_device();
+    double* partials = reinterpret_cast<double*>(scratch);
+    unsigned* ticket = reinterpret_cast<unsigned*>(scratch + (size_t)UAAMG_NOALLOC_MAX_LEAVES * sizeof(double));
+    if (D0.L.nl == 0) {
+        CK(cudaMemsetAsync(d_norm, 0, sizeof(float), h->stream));
+        return UAAMG_SUCCESS;
+    }
+    // the array keeps the previous call's contents: the ticket must start at zero
+    CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned), h->stream));
+    launch(k_residual_absmax, (unsigned)D0.L.nl, 128, h->stream, D0.L, d_x, d_b, d_r, partials, ticket, d_norm);
+    h->launches++;
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
 int uaamg_poisson_profile_pcg(uaamg_poisson* h, float* d_pressure, const float* d_rhs, int max_classes, char* names,
                               double* total_ms, int64_t* counts, int* nclasses) {
     ABI_BEGIN
