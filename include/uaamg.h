@@ -185,7 +185,9 @@ int uaamg_poisson_profile_pcg(uaamg_poisson* h, float* d_pressure, const float* 
 
 /* Stream (cudaStream_t as void*) used by *_device calls; NULL = the handle's own stream. */
 int uaamg_poisson_set_stream(uaamg_poisson* h, void* stream);
-/* Use the CUDA-graph PCG (1, default) or the host-driven loop (0). */
+/* PCG driver: 1 (default) host-driven loop for a handle's first solve and the
+ * CUDA-graph solve (conditional WHILE node) from the second solve on; 2 the
+ * graph always; 0 the host-driven loop always. */
 int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph);
 /* Kernels launched through this handle since it was created: hierarchy build,
  * right-hand side and every solve (kernels inside the solve graph included). */

@@ -50,6 +50,7 @@ struct PcgState {
     float rho, rho_new, sigma, alpha, beta, nu, nu_old, numax;
     float tol;
     int iter, status, max_iter, first, iterations_taken;
+    int error;  // set by a kernel whose bounded wait timed out
     unsigned int ticket[8];
 };
 

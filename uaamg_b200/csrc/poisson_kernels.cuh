@@ -433,6 +433,335 @@ __global__ void __launch_bounds__(128) k_restrict(DLevel L, const float* x, cons
 }
 
 // ---------------------------------------------------------------------------
+// Bulk-async staged sweeps.  One CTA per leaf: thread 0 issues
+// cp.async.bulk copies (2 KB each) of the leaf's vectors and of the
+// coefficient arrays that are stored for it (trimmed leaves hold the default
+// and are not read) into shared memory, completing on an mbarrier; while they
+// are in flight the boundary threads load the halo values of the six
+// neighbour leaves; the stencil then reads the leaf from shared memory.
+// Same arithmetic as sweep_value, so results are bit-identical.
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~2^22 polls (each try_wait blocks briefly).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+    for (int i = 0; i < (1 << 22); ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// What a staged sweep needs in shared memory.
+struct Staged {
+    float* x;
+    float* b;
+    float* d;   // diag
+    float* i;   // 1/diag or spai0
+    float* cx;
+    float* cy;
+    float* cz;
+};
+
+// Issue the bulk copies of one leaf (thread 0) and return the byte count.
+template <int MODE>
+__device__ __forceinline__ unsigned stage_issue(const DLevel& L, int leaf, unsigned fl, const float* x, const float* b,
+                                                const Staged& S, uint64_t* bar) {
+    const bool need_b = (MODE != M_LAPLACIAN);
+    const bool need_d = (MODE != M_RED && MODE != M_BLACK) && !(fl & TRIM_DIAG);
+    const bool need_i = (MODE == M_JACOBI || MODE == M_RED || MODE == M_BLACK) ? !(fl & TRIM_DIAG)
+                        : (MODE == M_SPAI0 ? !(fl & TRIM_SPAI0) : false);
+    unsigned bytes = 2048u;
+    bytes += need_b ? 2048u : 0u;
+    bytes += need_d ? 2048u : 0u;
+    bytes += need_i ? 2048u : 0u;
+    bytes += (fl & TRIM_X) ? 0u : 2048u;
+    bytes += (fl & TRIM_Y) ? 0u : 2048u;
+    bytes += (fl & TRIM_Z) ? 0u : 2048u;
+    mbar_expect_tx(bar, bytes);
+    const long long o = (long long)leaf * UAAMG_LEAF;
+    bulk_g2s(S.x, x + o, 2048u, bar);
+    if (need_b) bulk_g2s(S.b, b + o, 2048u, bar);
+    if (need_d) bulk_g2s(S.d, L.diag + o, 2048u, bar);
+    if (need_i) bulk_g2s(S.i, (MODE == M_SPAI0 ? L.spai0 : L.invdiag) + o, 2048u, bar);
+    if (!(fl & TRIM_X)) bulk_g2s(S.cx, L.cx + o, 2048u, bar);
+    if (!(fl & TRIM_Y)) bulk_g2s(S.cy, L.cy + o, 2048u, bar);
+    if (!(fl & TRIM_Z)) bulk_g2s(S.cz, L.cz + o, 2048u, bar);
+    return bytes;
+}
+
+__device__ __forceinline__ float4 s4(const float* s, int t) { return reinterpret_cast<const float4*>(s)[t]; }
+
+// Staged stencil: own-leaf values from shared memory, halo values (already
+// loaded into registers by the caller) for the neighbour leaves.
+template <int MODE>
+__device__ __forceinline__ float4 staged_value(const DLevel& L, int leaf, int t, unsigned fl, const Staged& S,
+                                               const float4& hxp, const float4& hxm, const float4& hyp,
+                                               const float4& hym, const float4& hcxp, const float4& hcyp, float hz,
+                                               float hcz, float w, float wsor, float one_minus_wsor, float4& xc,
+                                               unsigned& m) {
+    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
+    const float df = L.def_face;
+    const float4 dfv = f4splat(df);
+    xc = s4(S.x, t);
+    const float4 xp = (X < 7) ? s4(S.x, t + 16) : hxp;
+    const float4 xm = (X > 0) ? s4(S.x, t - 16) : hxm;
+    const float4 yp = (Y < 7) ? s4(S.x, t + 2) : hyp;
+    const float4 ym = (Y > 0) ? s4(S.x, t - 2) : hym;
+    const float4 cxp = (X < 7) ? ((fl & TRIM_X) ? dfv : s4(S.cx, t + 16)) : hcxp;
+    const float4 cyp = (Y < 7) ? ((fl & TRIM_Y) ? dfv : s4(S.cy, t + 2)) : hcyp;
+    const float4 cxm = (fl & TRIM_X) ? dfv : s4(S.cx, t);
+    const float4 cym = (fl & TRIM_Y) ? dfv : s4(S.cy, t);
+    const float4 czo = (fl & TRIM_Z) ? dfv : s4(S.cz, t);
+    // z neighbours inside the leaf from shared memory, across the leaf face from the halo
+    float zp3, zm0, czp3;
+    if (zh == 0) {
+        zp3 = S.x[4 * t + 4];
+        czp3 = (fl & TRIM_Z) ? df : S.cz[4 * t + 4];
+        zm0 = hz;
+    } else {
+        zm0 = S.x[4 * t - 1];
+        zp3 = hz;
+        czp3 = hcz;
+    }
+    const float zp[4] = {xc.y, xc.z, xc.w, zp3};
+    const float zm[4] = {zm0, xc.x, xc.y, xc.z};
+    const float czp[4] = {czo.y, czo.z, czo.w, czp3};
+    float4 off;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float f1 = __fmul_rn(f4get(xp, j), f4get(cxp, j));
+        float f2 = __fmul_rn(f4get(xm, j), f4get(cxm, j));
+        float f3 = __fmul_rn(f4get(yp, j), f4get(cyp, j));
+        float f4 = __fmul_rn(f4get(ym, j), f4get(cym, j));
+        float f5 = __fmul_rn(zp[j], czp[j]);
+        float f6 = __fmul_rn(zm[j], f4get(czo, j));
+        f1 = __fadd_rn(f1, f2);
+        f3 = __fadd_rn(f3, f4);
+        f5 = __fadd_rn(f5, f6);
+        f1 = __fadd_rn(f1, f3);
+        f1 = __fadd_rn(f1, f5);
+        f4set(off, j, f1);
+    }
+    m = mask4(L.mask, leaf, t);
+    float4 res = f4zero();
+    if (MODE == M_RED || MODE == M_BLACK) {
+        const float4 bb = s4(S.b, t);
+        const float4 iv = (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : s4(S.i, t);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int par = (X + Y + j) & 1;
+            bool upd = (MODE == M_RED) ? (par == 0) : (par == 1);
+            float r = __fsub_rn(f4get(bb, j), f4get(off, j));
+            r = __fmul_rn(r, f4get(iv, j));
+            r = __fmul_rn(r, wsor);
+            float v = __fmaf_rn(f4get(xc, j), one_minus_wsor, r);
+            f4set(res, j, upd ? v : f4get(xc, j));
+        }
+    } else {
+        const float4 dg = (fl & TRIM_DIAG) ? f4splat(L.def_diag) : s4(S.d, t);
+        if (MODE == M_LAPLACIAN) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) f4set(res, j, __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+        } else {
+            const float4 bb = s4(S.b, t);
+            if (MODE == M_RESIDUAL) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    f4set(res, j, __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j))));
+            } else if (MODE == M_JACOBI) {
+                const float4 iv = (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : s4(S.i, t);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+                    r = __fmul_rn(r, f4get(iv, j));
+                    f4set(res, j, __fmaf_rn(w, r, f4get(xc, j)));
+                }
+            } else {  // SPAI0
+                const float4 sp = (fl & TRIM_SPAI0) ? f4splat(L.def_spai0) : s4(S.i, t);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+                    f4set(res, j, __fmaf_rn(f4get(sp, j), r, f4get(xc, j)));
+                }
+            }
+        }
+    }
+    if (!(m & 1)) res.x = 0.f;
+    if (!(m & 2)) res.y = 0.f;
+    if (!(m & 4)) res.z = 0.f;
+    if (!(m & 8)) res.w = 0.f;
+    return res;
+}
+
+// Halo loads of one thread (issued while the bulk copies are in flight).
+__device__ __forceinline__ void staged_halo(const DLevel& L, int leaf, int t, const float* x, float4& hxp, float4& hxm,
+                                            float4& hyp, float4& hym, float4& hcxp, float4& hcyp, float& hz, float& hcz) {
+    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
+    const int* nb = L.nbr + (long long)leaf * 6;
+    const float df = L.def_face;
+    hxp = hxm = hyp = hym = f4zero();
+    hcxp = hcyp = f4splat(df);
+    hz = 0.f;
+    hcz = df;
+    if (X == 7) {
+        int n = nb[1];
+        if (n >= 0) {
+            hxp = ld4(x, n, t - 112);
+            if (!(L.flags[n] & TRIM_X)) hcxp = ld4(L.cx, n, t - 112);
+        }
+    }
+    if (X == 0) {
+        int n = nb[0];
+        if (n >= 0) hxm = ld4(x, n, t + 112);
+    }
+    if (Y == 7) {
+        int n = nb[3];
+        if (n >= 0) {
+            hyp = ld4(x, n, t - 14);
+            if (!(L.flags[n] & TRIM_Y)) hcyp = ld4(L.cy, n, t - 14);
+        }
+    }
+    if (Y == 0) {
+        int n = nb[2];
+        if (n >= 0) hym = ld4(x, n, t + 14);
+    }
+    if (zh == 0) {
+        int n = nb[4];
+        if (n >= 0) hz = x[(long long)n * UAAMG_LEAF + 4 * t + 7];
+    } else {
+        int n = nb[5];
+        if (n >= 0) {
+            hz = x[(long long)n * UAAMG_LEAF + 4 * t - 4];
+            if (!(L.flags[n] & TRIM_Z)) hcz = L.cz[(long long)n * UAAMG_LEAF + 4 * t - 4];
+        }
+    }
+}
+
+#define STAGED_SMEM_DECL                                                         \
+    __shared__ __align__(128) float sm_x[UAAMG_LEAF], sm_b[UAAMG_LEAF], sm_d[UAAMG_LEAF], \
+        sm_i[UAAMG_LEAF], sm_cx[UAAMG_LEAF], sm_cy[UAAMG_LEAF], sm_cz[UAAMG_LEAF];      \
+    __shared__ __align__(8) uint64_t sm_bar;                                     \
+    const Staged S{sm_x, sm_b, sm_d, sm_i, sm_cx, sm_cy, sm_cz};
+
+// Stage + halo + wait; false if the wait timed out (error flagged).
+template <int MODE>
+__device__ __forceinline__ bool staged_prologue(const DLevel& L, int leaf, int t, const float* x, const float* b,
+                                                const Staged& S, uint64_t* bar, unsigned& fl, float4& hxp,
+                                                float4& hxm, float4& hyp, float4& hym, float4& hcxp, float4& hcyp,
+                                                float& hz, float& hcz, int* err) {
+    fl = L.flags[leaf];
+    if (t == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (t == 0) stage_issue<MODE>(L, leaf, fl, x, b, S, bar);
+    staged_halo(L, leaf, t, x, hxp, hxm, hyp, hym, hcxp, hcyp, hz, hcz);
+    // every thread of the CTA agrees on the outcome, so no thread leaves a
+    // later barrier short-handed
+    const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0) != 0;
+    if (!ok) {
+        if (t == 0 && err) atomicExch(err, 1);
+        mbar_wait_bounded(bar, 0);  // let the copies in flight land before the CTA exits
+    }
+    return ok;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_sweep_staged(DLevel L, const float* x, const float* b, float* out, float w,
+                                                      float wsor, float one_minus_wsor, DotOut dot, int* err) {
+    griddep_wait();
+    griddep_launch();
+    STAGED_SMEM_DECL
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    unsigned fl;
+    float4 hxp, hxm, hyp, hym, hcxp, hcyp;
+    float hz, hcz;
+    const bool ok = staged_prologue<MODE>(L, leaf, t, x, b, S, &sm_bar, fl, hxp, hxm, hyp, hym, hcxp, hcyp, hz, hcz, err);
+    float4 xc, res = f4zero();
+    unsigned m;
+    if (ok) {
+        res = staged_value<MODE>(L, leaf, t, fl, S, hxp, hxm, hyp, hym, hcxp, hcyp, hz, hcz, w, wsor,
+                                 one_minus_wsor, xc, m);
+        st4(out, leaf, t, res);
+    }
+    if (dot.r) {  // rho_new = z . r, then beta and rho (PCG lines 13-15)
+        __shared__ double shd[4];
+        __shared__ bool last;
+        float4 rr = ok ? s4(S.b, t) : f4zero();  // b of this sweep is r
+        double s = (double)res.x * rr.x + (double)res.y * rr.y + (double)res.z * rr.z + (double)res.w * rr.w;
+        double part = block_sum128(s, shd);
+        if (publish_partial(part, dot.partials, &dot.st->ticket[0], &last)) {
+            double tot = gather_sum(dot.partials, shd);
+            if (t == 0) {
+                PcgState* st = dot.st;
+                float rho_new = (float)tot;
+                st->rho_new = rho_new;
+                st->beta = st->first ? 0.f : __fdiv_rn(rho_new, st->rho);
+                st->rho = rho_new;
+                st->ticket[0] = 0;
+            }
+        }
+    }
+}
+
+// residual + restriction with the fine leaf staged
+__global__ void __launch_bounds__(128) k_restrict_staged(DLevel L, const float* x, const float* b, float* coarse,
+                                                         int* err) {
+    griddep_wait();
+    griddep_launch();
+    STAGED_SMEM_DECL
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    unsigned fl;
+    float4 hxp, hxm, hyp, hym, hcxp, hcyp;
+    float hz, hcz;
+    const bool ok =
+        staged_prologue<M_RESIDUAL>(L, leaf, t, x, b, S, &sm_bar, fl, hxp, hxm, hyp, hym, hcxp, hcyp, hz, hcz, err);
+    if (!ok) return;
+    float4 xc;
+    unsigned m;
+    float4 r = staged_value<M_RESIDUAL>(L, leaf, t, fl, S, hxp, hxm, hyp, hym, hcxp, hcyp, hz, hcz, 0.f, 0.f, 0.f, xc, m);
+    __syncthreads();  // every thread has read sm_x before it is reused for the residuals
+    reinterpret_cast<float4*>(sm_x)[t] = r;
+    __syncthreads();
+    if (t < 64) {
+        const int i = t >> 4, j = (t >> 2) & 3, k = t & 3;
+        const uint64_t* mk = L.mask + (long long)leaf * 8;
+        float s = 0.f;
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    int fo = ((2 * i + ii) << 6) | ((2 * j + jj) << 3) | (2 * k + kk);
+                    if ((mk[fo >> 6] >> (fo & 63)) & 1ull) s = __fadd_rn(s, sm_x[fo]);
+                }
+        const int o = L.octant[leaf];
+        const int coff = ((((o >> 2) & 1) * 4 + i) << 6) | ((((o >> 1) & 1) * 4 + j) << 3) | ((o & 1) * 4 + k);
+        coarse[(long long)L.parent[leaf] * UAAMG_LEAF + coff] = __fmul_rn(s, 0.125f);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // PCG vector kernels (PoissonSolver::solveMultigridPCG, .cpp:2155-2226)
 __global__ void __launch_bounds__(128) k_mask_vec(DLevel L, float* v) {
     griddep_wait();
@@ -699,11 +1028,8 @@ __device__ __forceinline__ float2 cg_block_sum2(float a, float b, float* buf) {
 // ROWS rows per thread (row i = tid + k * CG_THREADS); the matrix rows stay in
 // registers for the whole solve.  Three barriers per CG iteration.
 template <int ROWS>
-__global__ void __launch_bounds__(CG_THREADS, 1) k_coarsest_cg(DCoarsest C, const float* rhs, float* out) {
-    griddep_wait();
-    griddep_launch();
-    __shared__ float ps[CG_THREADS * ROWS];
-    __shared__ float red[3][64];  // rotating reduction buffers (no reuse within 2 barriers)
+__device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float* rhs, float* out, float* ps,
+                                                 float (*red)[64]) {
     const int tid = threadIdx.x, n = C.n;
     float x[ROWS], r[ROWS], p[ROWS], z[ROWS], dg[ROWS], iv[ROWS], val[ROWS][6];
     int col[ROWS][6];
@@ -776,6 +1102,151 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_coarsest_cg(DCoarsest C, cons
     for (int k = 0; k < ROWS; ++k) {
         const int i = tid + k * CG_THREADS;
         if (i < n) out[C.dof_slot[i]] = x[k];
+    }
+}
+
+template <int ROWS>
+__global__ void __launch_bounds__(CG_THREADS, 1) k_coarsest_cg(DCoarsest C, const float* rhs, float* out) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ float ps[CG_THREADS * ROWS];
+    __shared__ float red[3][64];  // rotating reduction buffers (no reuse within 2 barriers)
+    coarsest_cg_body<ROWS>(C, rhs, out, ps, red);
+}
+
+// ---------------------------------------------------------------------------
+// Bottom of the W-cycle in one launch.  The coarse levels hold few leaves
+// (tens), so each of their sweeps is a kernel of a few microseconds that is
+// nearly all launch and memory latency.  k_bottom runs a whole recorded visit
+// of such a level -- its sweeps, residual + restriction, the recursive visits
+// below it and the coarsest CG -- as a list of steps inside one thread-block
+// cluster, with a cluster barrier between steps.  Each step runs exactly the
+// device code of the standalone kernel, so results are bit-identical.
+enum { B_SWEEP = 0, B_RESTRICT = 1, B_COARSEST = 2 };
+enum { S_PLAIN = 0, S_FIRST_JACOBI = 1, S_FIRST_SPAI0 = 2, S_FIRST_RBGS = 3, S_PROLONG = 4 };
+
+struct BStep {
+    int op, level, mode, src;
+    const float* x;    // lhs (plain / prolong) or rhs (first-sweep sources)
+    const float* xc;   // coarse vector (prolong)
+    const float* b;
+    float* out;
+    const int* ready;  // SPAI0 first-sweep flag
+    int* mark;         // set by SPAI0 sweeps
+    float w, wsor, one_minus_wsor, alpha;
+    int red_first;
+};
+#define BOTTOM_MAX_LEVELS 32
+struct BLevels {
+    DLevel L[BOTTOM_MAX_LEVELS];
+    DCoarsest C;
+};
+#define BOTTOM_THREADS 1024
+#define BOTTOM_SLOTS (BOTTOM_THREADS / 128)
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void slot_barrier(int slot) {
+    asm volatile("bar.sync %0, 128;" ::"r"(slot + 1) : "memory");
+}
+
+template <int MODE, class Src>
+__device__ __forceinline__ void bottom_sweep_leaf(const DLevel& L, int leaf, int t, const Src& src, const BStep& st) {
+    float4 xc;
+    unsigned m;
+    float4 res = sweep_value<MODE>(L, leaf, t, src, st.b, st.w, st.wsor, st.one_minus_wsor, xc, m);
+    st4(st.out, leaf, t, res);
+    if (MODE == M_SPAI0 && st.mark && leaf == 0 && t == 0) *st.mark = 1;
+}
+
+__device__ __noinline__ void bottom_sweep_dispatch(const DLevel& L, int leaf, int t, const BStep& st) {
+    switch (st.src * 8 + st.mode) {
+        case S_PLAIN * 8 + M_JACOBI: bottom_sweep_leaf<M_JACOBI>(L, leaf, t, SrcPlain{st.x}, st); break;
+        case S_FIRST_JACOBI * 8 + M_JACOBI: bottom_sweep_leaf<M_JACOBI>(L, leaf, t, SrcFirstJacobi{st.x, st.alpha}, st); break;
+        case S_PROLONG * 8 + M_JACOBI: bottom_sweep_leaf<M_JACOBI>(L, leaf, t, SrcProlong{st.x, st.xc, st.alpha}, st); break;
+        case S_PLAIN * 8 + M_SPAI0: bottom_sweep_leaf<M_SPAI0>(L, leaf, t, SrcPlain{st.x}, st); break;
+        case S_FIRST_SPAI0 * 8 + M_SPAI0: bottom_sweep_leaf<M_SPAI0>(L, leaf, t, SrcFirstSpai0{st.x, st.ready}, st); break;
+        case S_PROLONG * 8 + M_SPAI0: bottom_sweep_leaf<M_SPAI0>(L, leaf, t, SrcProlong{st.x, st.xc, st.alpha}, st); break;
+        case S_PLAIN * 8 + M_RED: bottom_sweep_leaf<M_RED>(L, leaf, t, SrcPlain{st.x}, st); break;
+        case S_PLAIN * 8 + M_BLACK: bottom_sweep_leaf<M_BLACK>(L, leaf, t, SrcPlain{st.x}, st); break;
+        case S_FIRST_RBGS * 8 + M_BLACK:
+            bottom_sweep_leaf<M_BLACK>(L, leaf, t, SrcFirstRbgs{st.x, st.wsor, st.red_first}, st);
+            break;
+        case S_PROLONG * 8 + M_BLACK: bottom_sweep_leaf<M_BLACK>(L, leaf, t, SrcProlong{st.x, st.xc, st.alpha}, st); break;
+        default: break;
+    }
+}
+
+// residual + restriction of one fine leaf by one 128-thread slot
+__device__ __noinline__ void bottom_restrict_leaf(const DLevel& L, int leaf, int t, const BStep& st, float* rs, int slot) {
+    float4 xc;
+    unsigned m;
+    float4 r = sweep_value<M_RESIDUAL>(L, leaf, t, SrcPlain{st.x}, st.b, 0.f, 0.f, 0.f, xc, m);
+    reinterpret_cast<float4*>(rs)[t] = r;
+    slot_barrier(slot);
+    if (t < 64) {
+        const int i = t >> 4, j = (t >> 2) & 3, k = t & 3;
+        const uint64_t* mk = L.mask + (long long)leaf * 8;
+        float s = 0.f;
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    int fo = ((2 * i + ii) << 6) | ((2 * j + jj) << 3) | (2 * k + kk);
+                    if ((mk[fo >> 6] >> (fo & 63)) & 1ull) s = __fadd_rn(s, rs[fo]);
+                }
+        const int o = L.octant[leaf];
+        const int coff = ((((o >> 2) & 1) * 4 + i) << 6) | ((((o >> 1) & 1) * 4 + j) << 3) | ((o & 1) * 4 + k);
+        st.out[(long long)L.parent[leaf] * UAAMG_LEAF + coff] = __fmul_rn(s, 0.125f);
+    }
+    slot_barrier(slot);
+}
+
+__global__ void __launch_bounds__(BOTTOM_THREADS, 1) k_bottom(const BStep* steps, int nsteps, const BLevels* lv) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ float rs[BOTTOM_SLOTS][UAAMG_LEAF];
+    __shared__ float ps[CG_THREADS * CG_MAX_ROWS];
+    __shared__ float red[3][64];
+    __shared__ BStep sst;
+    __shared__ DLevel sl;
+    const int slot = threadIdx.x >> 7, t = threadIdx.x & 127;
+    const int cta = (int)cluster_rank(), ncta = (int)cluster_size();
+    for (int s = 0; s < nsteps; ++s) {
+        if (threadIdx.x == 0) {
+            sst = steps[s];
+            if (sst.op != B_COARSEST) sl = lv->L[sst.level];
+        }
+        __syncthreads();
+        const BStep st = sst;
+        if (st.op == B_COARSEST) {
+            if (cta == 0) {
+                const int n = lv->C.n;
+                if (n <= CG_THREADS) coarsest_cg_body<1>(lv->C, st.b, st.out, ps, red);
+                else if (n <= 2 * CG_THREADS) coarsest_cg_body<2>(lv->C, st.b, st.out, ps, red);
+                else coarsest_cg_body<4>(lv->C, st.b, st.out, ps, red);
+            }
+        } else {
+            const DLevel& L = sl;
+            for (int leaf = cta * BOTTOM_SLOTS + slot; leaf < L.nl; leaf += ncta * BOTTOM_SLOTS) {
+                if (st.op == B_SWEEP) bottom_sweep_dispatch(L, leaf, t, st);
+                else bottom_restrict_leaf(L, leaf, t, st, rs[slot], slot);
+            }
+        }
+        cluster_sync_all();
     }
 }
 

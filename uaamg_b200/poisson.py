@@ -215,7 +215,9 @@ class PoissonSolver:
         _lib.check(L.uaamg_poisson_set_smoother(h, int(self.mSmoother)), "set_smoother")
         _lib.check(L.uaamg_poisson_set_max_iterations(h, int(self.mMaxIteration)), "set_max_iterations")
         _lib.check(L.uaamg_poisson_set_relative_tolerance(h, float(self.mRelativeTolerance)), "set_tolerance")
-        _lib.check(L.uaamg_poisson_set_graph_mode(h, 1 if self.use_graph else 0), "set_graph_mode")
+        mode = self.use_graph if isinstance(self.use_graph, int) and not isinstance(self.use_graph, bool) \
+            else (1 if self.use_graph else 0)
+        _lib.check(L.uaamg_poisson_set_graph_mode(h, mode), "set_graph_mode")
         return L, h
 
     def _solve(self, host_fn, dev_fn, pressure, rhs) -> int:
