@@ -1,4 +1,5 @@
-"""ctypes binding of the CPU oracle (liboracle.so built from poisson_oracle.c).
+"""ctypes binding of the CPU oracle (liboracle.so built from poisson_oracle.c and
+viscosity_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 cpu_baseline / reference arm of bench.py, never by the uaamg_b200 package.
@@ -70,6 +71,35 @@ def lib():
         L.orc_triplets.restype = C.c_int64
         L.orc_dof_index.argtypes = [vp, C.c_int, i32p]
         L.orc_set_threads.argtypes = [C.c_int]
+        # variational viscosity
+        L.orc_visc_create.restype = vp
+        L.orc_visc_create.argtypes = [C.c_int64, i32p, u64p, f32p, C.c_float,
+                                      C.c_int64, i32p, f32p, C.c_float,
+                                      C.c_int64, i32p, f32p, C.c_float,
+                                      C.c_float, C.c_float, C.c_float, C.c_int]
+        L.orc_visc_free.argtypes = [vp]
+        L.orc_visc_num_levels.argtypes = [vp]
+        for fn in ("orc_visc_leaf_count", "orc_visc_ndof"):
+            getattr(L, fn).argtypes = [vp, C.c_int]
+        L.orc_visc_topology.argtypes = [vp, C.c_int, i32p, u64p]
+        L.orc_visc_coefficients.argtypes = [vp, C.c_int, f32p, C.c_void_p]
+        L.orc_visc_defaults.argtypes = [vp, C.c_int, f32p]
+        L.orc_visc_dof_index.argtypes = [vp, C.c_int, i32p]
+        L.orc_visc_triplets.argtypes = [vp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_visc_triplets.restype = C.c_int64
+        L.orc_visc_build_rhs.argtypes = [vp, *g, C.c_float, *g, C.c_float, *g, C.c_float, *g, f32p, f32p]
+        L.orc_visc_apply.argtypes = [vp, C.c_int, C.c_int, C.c_int, f32p, f32p, f32p]
+        L.orc_visc_rbgs.argtypes = [vp, C.c_int, C.c_int, f32p, f32p]
+        L.orc_visc_restrict.argtypes = [vp, C.c_int, f32p, f32p]
+        L.orc_visc_prolongate.argtypes = [vp, C.c_int, f32p, f32p]
+        L.orc_visc_coarsest_solve.argtypes = [vp, f32p, f32p]
+        L.orc_visc_precondition.argtypes = [vp, f32p, f32p]
+        L.orc_visc_pcg.argtypes = [vp, f32p, f32p, C.c_float, C.c_int, C.POINTER(C.c_int),
+                                   C.POINTER(C.c_float)]
+        L.orc_visc_abs_max.argtypes = [vp, C.c_int, f32p]
+        L.orc_visc_abs_max.restype = C.c_float
+        L.orc_visc_dot.argtypes = [vp, C.c_int, f32p, f32p]
+        L.orc_visc_dot.restype = C.c_float
         _LIB = L
     return _LIB
 
@@ -204,6 +234,130 @@ class OraclePoisson:
         out = np.zeros((self.leaf_count(level), 512), np.int32)
         lib().orc_dof_index(self._h, level, out)
         return out
+
+
+VMODES = {"normal": 0, "residual": 1, "jacobi": 2, "red_gs": 3, "black_gs": 4}
+VARRAYS = ("diag", "invdiag", "neg_x", "neg_y", "neg_z", "T00", "T01", "T10", "T11")
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class OracleViscosity:
+    """Oracle hierarchy for one variational viscosity system.  Vectors are
+    float32 [3, leaf, 512] over a level's leaf set (0 at non-DOF voxels)."""
+
+    def __init__(self, liquid_phi, solid_phi, viscosity, dt, rho, dx, hierarchy=True):
+        L = lib()
+        self._h = L.orc_visc_create(
+            liquid_phi.leaf_count, liquid_phi.origins, liquid_phi.masks, _f32(liquid_phi.values.reshape(-1)),
+            float(liquid_phi.background[0]),
+            *_grid_args(solid_phi), float(solid_phi.background[0]),
+            *_grid_args(viscosity), float(viscosity.background[0]),
+            float(dt), float(rho), float(dx), 1 if hierarchy else 0)
+        self.num_levels = L.orc_visc_num_levels(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_visc_free(self._h)
+            self._h = None
+
+    def leaf_count(self, level=0):
+        return lib().orc_visc_leaf_count(self._h, level)
+
+    def ndof(self, level=0):
+        return lib().orc_visc_ndof(self._h, level)
+
+    def zeros(self, level=0):
+        return np.zeros((3, self.leaf_count(level), 512), np.float32)
+
+    def topology(self, level=0):
+        n = self.leaf_count(level)
+        o = np.zeros((n, 3), np.int32)
+        m = np.zeros((3, n, 8), np.uint64)
+        lib().orc_visc_topology(self._h, level, o, m)
+        return o, m
+
+    def coefficients(self, level=0):
+        """([3, 9, leaf, 512] effective values, [leaf] trimmed bits)."""
+        n = self.leaf_count(level)
+        coef = np.zeros((3, 9, n, 512), np.float32)
+        trim = np.zeros(max(n, 1), np.uint32)
+        lib().orc_visc_coefficients(self._h, level, coef, trim.ctypes.data)
+        return coef, trim[:n]
+
+    def defaults(self, level=0):
+        d = np.zeros(27, np.float32)
+        lib().orc_visc_defaults(self._h, level, d)
+        return d.reshape(3, 9)
+
+    def dof_index(self, level=0):
+        out = np.zeros((3, self.leaf_count(level), 512), np.int32)
+        lib().orc_visc_dof_index(self._h, level, out)
+        return out
+
+    def triplets(self, level):
+        n = lib().orc_visc_triplets(self._h, level, None, None, None)
+        r = np.zeros(n, np.int32); c = np.zeros(n, np.int32); v = np.zeros(n, np.float32)
+        lib().orc_visc_triplets(self._h, level, r.ctypes.data, c.ctypes.data, v.ctypes.data)
+        return r, c, v
+
+    def build_rhs(self, u, v, w, solid_velocity):
+        out = self.zeros(0)
+        lib().orc_visc_build_rhs(self._h, *_grid_args(u), float(u.background[0]),
+                                 *_grid_args(v), float(v.background[0]),
+                                 *_grid_args(w), float(w.background[0]),
+                                 *_grid_args(solid_velocity), _f32(solid_velocity.background), out)
+        return out
+
+    def apply(self, level, mode, lhs, rhs=None, channel=0):
+        """normal/residual/jacobi: returns a new vector; red_gs/black_gs:
+        returns a copy of lhs with channel ``channel`` updated."""
+        rhs = lhs if rhs is None else rhs
+        if mode in ("red_gs", "black_gs"):
+            out = np.array(lhs, dtype=np.float32, copy=True)
+        else:
+            out = self.zeros(level)
+        lib().orc_visc_apply(self._h, level, VMODES[mode], int(channel), _f32(lhs), _f32(rhs), out)
+        return out
+
+    def rbgs(self, level, lhs, rhs, order="xyz"):
+        out = np.array(lhs, dtype=np.float32, copy=True)
+        lib().orc_visc_rbgs(self._h, level, 0 if order == "xyz" else 1, out, _f32(rhs))
+        return out
+
+    def restrict(self, fine_level, fine):
+        out = self.zeros(fine_level + 1)
+        lib().orc_visc_restrict(self._h, fine_level, _f32(fine), out)
+        return out
+
+    def prolongate(self, fine_level, coarse, fine):
+        out = np.array(fine, dtype=np.float32, copy=True)
+        lib().orc_visc_prolongate(self._h, fine_level, _f32(coarse), out)
+        return out
+
+    def coarsest_solve(self, rhs):
+        out = self.zeros(self.num_levels - 1)
+        lib().orc_visc_coarsest_solve(self._h, _f32(rhs), out)
+        return out
+
+    def precondition(self, r):
+        z = self.zeros(0)
+        lib().orc_visc_precondition(self._h, _f32(r), z)
+        return z
+
+    def solve_pcg(self, x, b, tol=1e-6, max_iter=100):
+        x = np.array(x, dtype=np.float32, copy=True)
+        it = C.c_int(0); res = C.c_float(0)
+        st = lib().orc_visc_pcg(self._h, x, _f32(b), float(tol), int(max_iter), C.byref(it), C.byref(res))
+        return x, int(st), int(it.value), float(res.value)
+
+    def abs_max(self, v, level=0):
+        return float(lib().orc_visc_abs_max(self._h, level, _f32(v)))
+
+    def dot(self, a, b, level=0):
+        return float(lib().orc_visc_dot(self._h, level, _f32(a), _f32(b)))
 
 
 def set_threads(n: int) -> None:

@@ -106,6 +106,80 @@ void orc_dof_index(const orc_poisson* h, int level, int32_t* out);
 
 void orc_set_threads(int n);
 
+/* ======================================================================== */
+/* Variational viscosity (SIMD_UAAMG/simd_viscosity3d.cpp).
+ *
+ * A level is stored over one leaf set: the leaves of the union of the three
+ * channels' DOF masks dilated by 2 (level 0) or 3 (coarse levels) voxels, in
+ * OpenVDB tree order (the reference's coefficient pattern,
+ * simd_viscosity3d.cpp:881-899 and :1353-1362).  Vectors are
+ * [3 channels][leaf][512] floats over that set, 0 at non-DOF voxels.
+ * Coefficients are [3 channels][9 arrays][leaf][512]: diag, invdiag, neg_x,
+ * neg_y, neg_z, T00, T01, T10, T11 (T = m_cross_channel[channel][j][k]). */
+typedef struct orc_visc orc_visc;
+
+enum { ORC_VA_DIAG = 0, ORC_VA_INVDIAG = 1, ORC_VA_NEGX = 2, ORC_VA_NEGY = 3, ORC_VA_NEGZ = 4,
+       ORC_VA_T00 = 5, ORC_VA_T01 = 6, ORC_VA_T10 = 7, ORC_VA_T11 = 8, ORC_VA_COUNT = 9 };
+/* L_with_level::working_mode (simd_viscosity3d.h:14) */
+enum { ORC_VMODE_NORMAL = 0, ORC_VMODE_RESIDUAL = 1, ORC_VMODE_JACOBI = 2,
+       ORC_VMODE_RED_GS = 3, ORC_VMODE_BLACK_GS = 4 };
+
+/* simd_viscosity3d ctor (simd_viscosity3d.cpp:3621-3658) minus the rhs:
+ * level 0 from the viscosity, liquid SDF and solid SDF grids, coarse levels
+ * while ndof > 4000 (if build_hierarchy), level-0 trimming, coarsest matrix.
+ * All grids share one index space (voxel centre i at world i*dx). */
+orc_visc* orc_visc_create(
+    int64_t liq_n, const int32_t* liq_origins, const uint64_t* liq_masks,
+    const float* liq_values, float liq_background,
+    int64_t sol_n, const int32_t* sol_origins, const float* sol_values, float sol_background,
+    int64_t mu_n, const int32_t* mu_origins, const float* mu_values, float mu_background,
+    float dt, float rho, float dx, int build_hierarchy);
+void orc_visc_free(orc_visc* h);
+
+int  orc_visc_num_levels(const orc_visc* h);
+int  orc_visc_leaf_count(const orc_visc* h, int level);
+int  orc_visc_ndof(const orc_visc* h, int level);
+/* origins [nl][3], DOF masks [3][nl][8] */
+void orc_visc_topology(const orc_visc* h, int level, int32_t* origins, uint64_t* dof_masks);
+/* effective coefficients [3][9][nl][512] and per-leaf trimmed bits
+ * (bit 9*channel+array) */
+void orc_visc_coefficients(const orc_visc* h, int level, float* coef, uint32_t* trim);
+void orc_visc_defaults(const orc_visc* h, int level, float* out27);
+/* DOF index [3][nl][512], -1 at non-DOF voxels */
+void orc_visc_dof_index(const orc_visc* h, int level, int32_t* out);
+/* explicit matrix triplets (explicit_matrix_reducer :2415-2642); NULL to count */
+int64_t orc_visc_triplets(const orc_visc* h, int level, int32_t* rows, int32_t* cols, float* vals);
+
+/* L_with_level::build_rhs (:2005-2087): velocity channels are scalar grids,
+ * solid velocity a vec3 grid (n may be 0).  rhs_out [3][nl][512]. */
+void orc_visc_build_rhs(const orc_visc* h,
+    int64_t u_n, const int32_t* u_origins, const float* u_values, float u_bg,
+    int64_t v_n, const int32_t* v_origins, const float* v_values, float v_bg,
+    int64_t w_n, const int32_t* w_origins, const float* w_values, float w_bg,
+    int64_t sv_n, const int32_t* sv_origins, const float* sv_values, const float* sv_bg3,
+    float* rhs_out);
+
+/* One light_weight_applier pass (:2849-3603).  NORMAL/RESIDUAL/JACOBI write
+ * all three channels of out; RED_GS/BLACK_GS update channel `channel` of
+ * `out` in place (out holds the current iterate). */
+void orc_visc_apply(orc_visc* h, int level, int mode, int channel,
+                    const float* lhs, const float* rhs, float* out);
+/* XYZ_RBGS_apply (order 0) / ZYX_RBGS_apply (order 1), in place. */
+void orc_visc_rbgs(orc_visc* h, int level, int order, float* lhs, const float* rhs);
+void orc_visc_restrict(const orc_visc* h, int fine_level, const float* fine, float* coarse);
+/* prolongation<true>: fine += P coarse */
+void orc_visc_prolongate(const orc_visc* h, int fine_level, const float* coarse, float* fine);
+void orc_visc_coarsest_solve(orc_visc* h, const float* rhs, float* out);
+/* out = mucycle(0, r, mu=2, for_precon=true, level 0, n=2) */
+void orc_visc_precondition(orc_visc* h, const float* r, float* out);
+/* simd_viscosity3d::pcg_solve (:3691-3754) on x in place.  Returns 0 when
+ * the stopping test held, 1 when it stopped at max_iter-1; *iterations is
+ * m_iteration (the 0-based index of the last iteration run). */
+int orc_visc_pcg(orc_visc* h, float* x, const float* b, float tol, int max_iter,
+                 int* iterations, float* final_abs_res);
+float orc_visc_abs_max(const orc_visc* h, int level, const float* v);
+float orc_visc_dot(const orc_visc* h, int level, const float* a, const float* b);
+
 #ifdef __cplusplus
 }
 #endif

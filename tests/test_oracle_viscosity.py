@@ -1,0 +1,346 @@
+"""CPU checks of the viscosity oracle (restatement of
+SIMD_UAAMG/simd_viscosity3d.cpp).
+
+The reference cannot run here, so the oracle is checked against
+  * a dense numpy restatement of the level-0 construction (tests/visc_dense.py),
+    bit for bit,
+  * the assembled FP64 matrix (symmetry, apply modes, red-black Gauss-Seidel),
+  * the Galerkin identity of its coarsening, A_c = 1/8 P^T A P with P the
+    per-channel piecewise-constant prolongation (rap_factor 0.125,
+    simd_viscosity3d.cpp:1136),
+  * R = P^T / 8 and prolongation = P (:2353-2413, :2659-2729),
+  * an FP64 sparse direct solve of the same system,
+  * known values of the cube volume fraction (volume_fractions.cpp:102-120),
+  * and its own golden fixture (tests/golden/make_golden_viscosity.py).
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from oracle.oracle import OracleViscosity
+from uaamg_b200 import scenes
+from uaamg_b200.grids import LeafGrid, dense_to_leaves
+
+from . import visc_dense
+
+
+def vscene(n=16, spheres=(((0.5, 0.7, 0.5), 0.15),), slab=0.4, seed=1, mu=1e3):
+    return scenes.viscosity_box_scene(n, slab, list(spheres), seed, mu)
+
+
+def build(s, hierarchy=True):
+    return OracleViscosity(s.liquid_phi, s.solid_phi, s.viscosity, s.dt, s.rho, s.dx, hierarchy)
+
+
+def matrix(o, level):
+    r, c, v = o.triplets(level)
+    n = o.ndof(level)
+    return sp.csr_matrix((v.astype(np.float64), (r, c)), shape=(n, n))
+
+
+def to_vec(o, level, x):
+    idx = o.dof_index(level)
+    out = np.zeros(o.ndof(level))
+    m = idx >= 0
+    out[idx[m]] = x[m]
+    return out
+
+
+def from_vec(o, level, v):
+    idx = o.dof_index(level)
+    out = np.zeros(idx.shape, np.float32)
+    m = idx >= 0
+    out[m] = v[idx[m]]
+    return out
+
+
+def prolongation(o, fine_level):
+    """P: fine DOF (c, g) -> coarse DOF (c, g >> 1)."""
+    fi, ci = o.dof_index(fine_level), o.dof_index(fine_level + 1)
+    fo, _ = o.topology(fine_level)
+    co, _ = o.topology(fine_level + 1)
+    cmap = {tuple(x): k for k, x in enumerate(co)}
+    off = np.arange(512)
+    xyz = np.stack([off >> 6, (off >> 3) & 7, off & 7], 1)
+    rows, cols = [], []
+    for c in range(3):
+        for li in range(fo.shape[0]):
+            offs = np.nonzero(fi[c, li] >= 0)[0]
+            if offs.size == 0:
+                continue
+            G = (fo[li][None, :] + xyz[offs]) >> 1
+            for gg, fo_ in zip(G, offs):
+                k = cmap[tuple((gg >> 3) << 3)]
+                rows.append(fi[c, li, fo_])
+                cols.append(ci[c, k, ((gg[0] & 7) << 6) | ((gg[1] & 7) << 3) | (gg[2] & 7)])
+    return sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(o.ndof(fine_level), o.ndof(fine_level + 1)))
+
+
+# ---------------------------------------------------------------------------
+def test_cube_fraction_known_values():
+    f32 = np.float32
+    # plane phi = z - 1/2 through the unit cube: half full
+    lo, hi = f32(-0.5), f32(0.5)
+    v = visc_dense.cube_fraction(*(np.array([x], f32) for x in (lo, lo, lo, lo, hi, hi, hi, hi)))
+    assert abs(float(v[0]) - 0.5) < 1e-6
+    allneg = visc_dense.cube_fraction(*(np.array([-1.0], f32),) * 8)
+    allpos = visc_dense.cube_fraction(*(np.array([1.0], f32),) * 8)
+    assert float(allneg[0]) == 1.0 and float(allpos[0]) == 0.0
+    # one corner inside: tetrahedron-ish sliver, strictly between 0 and 1/8
+    one = visc_dense.cube_fraction(*(np.array([x], f32) for x in (-0.2, 1, 1, 1, 1, 1, 1, 1)))
+    assert 0.0 < float(one[0]) < 0.125
+
+
+@pytest.mark.parametrize("n,spheres,slab", [
+    (16, (((0.5, 0.7, 0.5), 0.15),), 0.4),
+    (24, (((0.3, 0.5, 0.6), 0.2), ((0.7, 0.3, 0.3), 0.12)), None),
+])
+def test_level0_matches_dense_restatement(n, spheres, slab):
+    s = vscene(n, spheres, slab)
+    o = build(s, hierarchy=False)
+    box = visc_dense.Box(-16, n + 32)
+    ref = visc_dense.level0(s, box)
+    org, dofm = o.topology(0)
+    nb = box.size // 8
+    # leaf set = coefficient pattern leaves
+    blocks = {tuple(b * 8 + box.lo) for b in np.argwhere(ref["pattern"])}
+    assert blocks == {tuple(x) for x in org}
+    coef, trim = o.coefficients(0)
+    defaults = o.defaults(0)
+    off = np.arange(512)
+    lx, ly, lz = off >> 6, (off >> 3) & 7, off & 7
+    bits = ((dofm[..., None] >> np.arange(64, dtype=np.uint64)) & np.uint64(1)).reshape(3, -1, 512).astype(bool)
+    for li, o3 in enumerate(org):
+        g = o3 - box.lo
+        sl = (g[0] + lx, g[1] + ly, g[2] + lz)
+        for c in range(3):
+            assert np.array_equal(bits[c, li], ref["dof"][c][sl]), (li, c)
+            for a in range(9):
+                want = ref["coef"][c, a][sl]
+                got = coef[c, a, li]
+                if trim[li] >> (c * 9 + a) & 1:
+                    d = defaults[c, a]
+                    assert np.all(got == d)
+                else:
+                    assert np.array_equal(got, want), (li, c, a)
+    assert o.ndof(0) == sum(int(d.sum()) for d in ref["dof"])
+
+
+def test_operator_symmetric_and_apply_modes_match_matrix():
+    s = vscene(16)
+    o = build(s)
+    rng = np.random.default_rng(3)
+    for level in range(o.num_levels):
+        A = matrix(o, level)
+        assert abs(A - A.T).max() == 0.0
+        n = o.ndof(level)
+        x = rng.standard_normal(n).astype(np.float32)
+        b = rng.standard_normal(n).astype(np.float32)
+        X, B = from_vec(o, level, x), from_vec(o, level, b)
+        Ax = A @ x.astype(np.float64)
+        scale = np.abs(A).max() * np.abs(x).max()
+        y = to_vec(o, level, o.apply(level, "normal", X))
+        assert np.abs(y - Ax).max() <= 1e-5 * scale
+        r = to_vec(o, level, o.apply(level, "residual", X, B))
+        assert np.abs(r - (b - Ax)).max() <= 1e-5 * scale
+        D = A.diagonal()
+        j = to_vec(o, level, o.apply(level, "jacobi", X, B))
+        assert np.allclose(j, x + (b - Ax) / D, rtol=1e-4, atol=1e-4 * np.abs(x).max())
+        # non-DOF voxels stay zero
+        out = o.apply(level, "normal", X)
+        assert np.all(out[o.dof_index(level) < 0] == 0)
+
+
+def test_red_black_gauss_seidel_matches_matrix():
+    s = vscene(16)
+    o = build(s)
+    A = matrix(o, 0)
+    n = o.ndof(0)
+    idx = o.dof_index(0)
+    org, _ = o.topology(0)
+    off = np.arange(512)
+    xyz = np.stack([off >> 6, (off >> 3) & 7, off & 7], 1)
+    ch = np.zeros(n, int)
+    col = np.zeros(n, int)
+    for c in range(3):
+        for li in range(org.shape[0]):
+            offs = np.nonzero(idx[c, li] >= 0)[0]
+            ch[idx[c, li, offs]] = c
+            col[idx[c, li, offs]] = (org[li][None, :] + xyz[offs]).sum(1) % 2
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal(n).astype(np.float32)
+    b = rng.standard_normal(n).astype(np.float32)
+    D = A.diagonal()
+
+    def gs(xv, c, color):
+        sel = (ch == c) & (col == color)
+        y = xv.copy()
+        y[sel] = (b[sel] - (A @ xv - D * xv)[sel]) / D[sel]
+        return y
+
+    X, B = from_vec(o, 0, x), from_vec(o, 0, b)
+    ref = x.astype(np.float64)
+    for c in range(3):
+        for color, mode in ((0, "red_gs"), (1, "black_gs")):
+            X = o.apply(0, mode, X, B, channel=c)
+            ref = gs(ref, c, color)
+            got = to_vec(o, 0, X)
+            assert np.abs(got - ref).max() <= 1e-4 * np.abs(ref).max()
+    # XYZ = red/black per channel in order; ZYX = black/red from channel 2
+    Xa = o.rbgs(0, from_vec(o, 0, x), B, "xyz")
+    Xb = from_vec(o, 0, x)
+    for c in range(3):
+        Xb = o.apply(0, "red_gs", Xb, B, channel=c)
+        Xb = o.apply(0, "black_gs", Xb, B, channel=c)
+    assert np.array_equal(Xa, Xb)
+    Xa = o.rbgs(0, from_vec(o, 0, x), B, "zyx")
+    Xb = from_vec(o, 0, x)
+    for c in (2, 1, 0):
+        Xb = o.apply(0, "black_gs", Xb, B, channel=c)
+        Xb = o.apply(0, "red_gs", Xb, B, channel=c)
+    assert np.array_equal(Xa, Xb)
+
+
+def test_coarsening_is_galerkin_and_transfers_are_adjoint():
+    s = vscene(24, spheres=(((0.5, 0.6, 0.5), 0.2),), slab=0.3)
+    o = build(s)
+    assert o.num_levels >= 2
+    rng = np.random.default_rng(5)
+    for fl in range(o.num_levels - 1):
+        A, Ac = matrix(o, fl), matrix(o, fl + 1)
+        P = prolongation(o, fl)
+        G = 0.125 * (P.T @ A @ P)
+        assert abs(G - Ac).max() <= 2e-6 * abs(Ac).max()
+        f = rng.standard_normal(o.ndof(fl)).astype(np.float32)
+        r = to_vec(o, fl + 1, o.restrict(fl, from_vec(o, fl, f)))
+        assert np.allclose(r, 0.125 * (P.T @ f.astype(np.float64)), rtol=1e-5, atol=1e-6)
+        cvec = rng.standard_normal(o.ndof(fl + 1)).astype(np.float32)
+        base = rng.standard_normal(o.ndof(fl)).astype(np.float32)
+        p = to_vec(o, fl, o.prolongate(fl, from_vec(o, fl + 1, cvec), from_vec(o, fl, base)))
+        assert np.allclose(p, base + P @ cvec, rtol=1e-6, atol=1e-6)
+
+
+def test_dof_numbering_channel_major_tree_order():
+    s = vscene(16)
+    o = build(s)
+    idx = o.dof_index(0)
+    n = o.ndof(0)
+    v = idx[idx >= 0]
+    assert np.array_equal(np.sort(v), np.arange(n))
+    # channel c numbers follow channel c-1, leaves in order, voxels in offset order
+    flat = idx.reshape(3, -1)
+    last = -1
+    for c in range(3):
+        vals = flat[c][flat[c] >= 0]
+        assert np.all(np.diff(vals) == 1) and vals[0] == last + 1
+        last = vals[-1]
+
+
+def test_pcg_converges_to_direct_solution():
+    """Liquid touching the walls (no floating drop): PCG reaches 1e-6 in a
+    handful of iterations and agrees with an FP64 sparse direct solve."""
+    s = vscene(24, spheres=(), slab=0.45)
+    o = build(s)
+    b = o.build_rhs(s.u, s.v, s.w, s.solid_velocity)
+    x, st, it, res = o.solve_pcg(np.zeros_like(b), b, 1e-6, 100)
+    assert st == 0 and it < 20
+    A = matrix(o, 0).tocsc()
+    xd = spla.spsolve(A, to_vec(o, 0, b))
+    xv = to_vec(o, 0, x)
+    assert np.abs(xv - xd).max() <= 1e-4 * np.abs(xd).max()
+    r = o.apply(0, "residual", x, b)
+    assert o.abs_max(r) <= 1e-5 * o.abs_max(b)  # true residual, float32 drift
+
+
+def test_pcg_floating_drop_stops_at_iteration_cap():
+    """A floating drop adds near-rigid modes that the unsmoothed aggregation
+    does not capture; from a zero guess the reference's loop runs to its cap
+    and returns after iteration max_iter-1 (simd_viscosity3d.cpp:3724)."""
+    s = vscene(16)
+    o = build(s)
+    b = o.build_rhs(s.u, s.v, s.w, s.solid_velocity)
+    x, st, it, res = o.solve_pcg(np.zeros_like(b), b, 1e-6, 12)
+    assert st == 1 and it == 11
+    assert res < o.abs_max(b)
+
+
+def test_rhs_without_solid_velocity_is_u_times_face_volume():
+    s = vscene(16)
+    o = build(s)
+    rhs = o.build_rhs(s.u, s.v, s.w, s.solid_velocity)
+    ref = visc_dense.level0(s, visc_dense.Box(-16, 48))
+    org, _ = o.topology(0)
+    idx = o.dof_index(0)
+    off = np.arange(512)
+    lx, ly, lz = off >> 6, (off >> 3) & 7, off & 7
+    vel = [visc_dense.dense(g, visc_dense.Box(-16, 48))[0] for g in (s.u, s.v, s.w)]
+    for li, o3 in enumerate(org):
+        gg = o3 + 16
+        sl = (gg[0] + lx, gg[1] + ly, gg[2] + lz)
+        for c in range(3):
+            fv = ref["face_vol"][c][sl]
+            fv = np.where(fv < np.float32(0.1), np.float32(0.1), fv)
+            want = np.where(idx[c, li] >= 0, vel[c][sl] * fv, 0).astype(np.float32)
+            assert np.array_equal(rhs[c, li], want)
+
+
+def test_rhs_solid_velocity_equals_matrix_coupling():
+    """With a moving solid, the rhs gains -sum_j A_ij u_j over the solid faces
+    j coupled to DOF i.  Check against a dense operator built with every face
+    (DOF or solid) as an unknown: for a solid velocity field that is constant
+    per channel, the contribution of the solid faces equals the rhs change."""
+    s = vscene(16, spheres=(), slab=0.5)
+    o = build(s)
+    base = o.build_rhs(s.u, s.v, s.w, s.solid_velocity)
+    sv = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512, 3), np.float32),
+                  background=np.array([0.25, -0.5, 0.75], np.float32))
+    moved = o.build_rhs(s.u, s.v, s.w, sv)
+    diff = moved - base
+    idx = o.dof_index(0)
+    assert np.all(diff[idx < 0] == 0)
+    assert np.abs(diff).max() > 0
+    # linear in the solid velocity
+    sv2 = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512, 3), np.float32),
+                   background=np.array([0.5, -1.0, 1.5], np.float32))
+    diff2 = o.build_rhs(s.u, s.v, s.w, sv2) - base
+    assert np.allclose(diff2, 2 * diff, rtol=1e-5, atol=1e-3 * np.abs(diff).max())
+
+
+def test_single_level_and_empty_liquid():
+    s = vscene(8, spheres=(((0.5, 0.5, 0.5), 0.3),), slab=None)
+    o = build(s)
+    assert o.num_levels == 1
+    b = o.build_rhs(s.u, s.v, s.w, s.solid_velocity)
+    x, st, it, res = o.solve_pcg(np.zeros_like(b), b, 1e-6, 100)
+    assert st == 0
+    # no liquid: no DOFs at all
+    e = vscene(8, spheres=(), slab=-1.0)
+    oe = build(e)
+    assert oe.ndof(0) == 0
+    be = oe.build_rhs(e.u, e.v, e.w, e.solid_velocity)
+    xe, st, it, res = oe.solve_pcg(np.zeros_like(be), be, 1e-6, 100)
+    assert st == 0 and it == 0
+
+
+def test_golden_fixture():
+    import os
+    from tests.golden.make_golden_viscosity import FILE, golden_scene, warm_start
+    g = np.load(FILE)
+    sc = golden_scene()
+    o = OracleViscosity(sc.liquid_phi, sc.solid_phi, sc.viscosity, sc.dt, sc.rho, sc.dx)
+    assert o.num_levels == int(g["levels"])
+    for l in range(o.num_levels):
+        org, masks = o.topology(l)
+        coef, trim = o.coefficients(l)
+        assert np.array_equal(org, g[f"l{l}_origins"])
+        assert np.array_equal(masks, g[f"l{l}_dof"])
+        assert np.array_equal(coef, g[f"l{l}_coef"])
+        assert np.array_equal(trim, g[f"l{l}_trim"])
+    rhs = o.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    assert np.array_equal(rhs, g["rhs"])
+    x0 = warm_start(o, sc)
+    assert np.array_equal(x0, g["x0"])
+    x, st, it, _ = o.solve_pcg(x0, rhs, 1e-6, 100)
+    assert it == int(g["pcg_iters"]) and st == int(g["pcg_status"])
+    assert np.array_equal(x, g["pcg_x"])

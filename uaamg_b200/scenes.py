@@ -117,3 +117,71 @@ def random_balls_scene(seed: int, sides=(32, 64, 96, 128, 192)) -> PoissonScene:
         r = float(np.exp(np.log(0.05) + (np.log(0.3) - np.log(0.05)) * u[2 + 4 * s]))
         spheres.append(((float(u[3 + 4 * s]), float(u[4 + 4 * s]), float(u[5 + 4 * s])), r))
     return sdf_box_scene(n, None, spheres, seed, 1.0, name=f"balls{k} {n}^3 seed{seed}")
+
+
+@dataclass
+class ViscosityScene:
+    name: str
+    n: int
+    dx: float
+    dt: float
+    rho: float
+    liquid_phi: LeafGrid
+    solid_phi: LeafGrid
+    viscosity: LeafGrid
+    u: LeafGrid
+    v: LeafGrid
+    w: LeafGrid
+    solid_velocity: LeafGrid
+
+
+def viscosity_box_scene(n: int, slab_height: float | None, spheres, seed: int, mu: float = 1e3,
+                        dt: float = 1.0 / 240.0, rho: float = 1.0, name: str = "viscosity") -> ViscosityScene:
+    """Viscosity inputs in the convention of simd_viscosity3d's call site
+    (FLIP_vdb.cpp:3170-3204): every grid shares one index space, voxel i of
+    the n^3 box centred at world (i + 1/2) dx.
+
+    * liquid SDF: {y < slab_height} U spheres, all n^3 voxels active,
+      background 3 dx (air);
+    * solid SDF on the box plus one leaf of margin: distance to the nearest
+      domain wall minus dx/4, so that the faces on the walls sample < 0 (solid,
+      like the Poisson workload's zero wall fractions) and the first interior
+      faces do not; background -3 dx (solid);
+    * constant dynamic viscosity ``mu`` (a grid with no leaves);
+    * face velocities U[-1, 1] from ``seed`` on the (n+1)^3 face lattice of
+      each channel, zero solid velocity."""
+    dx = 1.0 / n
+    c = (np.arange(n, dtype=np.float64) + 0.5) * dx
+    X, Y, Z = np.meshgrid(c, c, c, indexing="ij")
+    phi = np.full((n, n, n), np.inf, dtype=np.float64)
+    if slab_height is not None:
+        phi = np.minimum(phi, Y - slab_height)
+    for cen, r in spheres:
+        phi = np.minimum(phi, np.sqrt((X - cen[0]) ** 2 + (Y - cen[1]) ** 2 + (Z - cen[2]) ** 2) - r)
+    phi = np.minimum(phi, 3.0 * 4 * n * dx)
+    liquid = dense_to_leaves(phi.astype(np.float32), background=3.0 * dx)
+    m = n + 16
+    cs = (np.arange(m, dtype=np.float64) - 8 + 0.5) * dx
+    SX, SY, SZ = np.meshgrid(cs, cs, cs, indexing="ij")
+    wall = np.minimum.reduce([SX, 1.0 - SX, SY, 1.0 - SY, SZ, 1.0 - SZ]) - 0.25 * dx
+    solid = dense_to_leaves(wall.astype(np.float32), origin=(-8, -8, -8), background=-3.0 * dx)
+    visc = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512), np.float32),
+                    background=np.float32(mu))
+    f = n + 1
+    vel = uniform(seed, 3 * f * f * f, -1.0, 1.0).reshape(3, f, f, f)
+    u = dense_to_leaves(vel[0], background=0.0)
+    v = dense_to_leaves(vel[1], background=0.0)
+    w = dense_to_leaves(vel[2], background=0.0)
+    sv = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512, 3), np.float32),
+                  background=np.zeros(3, np.float32))
+    return ViscosityScene(name=name, n=n, dx=dx, dt=dt, rho=rho, liquid_phi=liquid, solid_phi=solid,
+                          viscosity=visc, u=u, v=v, w=w, solid_velocity=sv)
+
+
+def plain_viscosity_scene(n: int = 128, seed: int = 1, mu: float = 1e3) -> ViscosityScene:
+    """Plain variational viscosity workload: the Poisson geometry at n^3
+    (128^3; liquid y < 0.4 plus a sphere of radius 0.15 at (0.5, 0.7, 0.5)),
+    walls solid, face velocities U[-1,1] from seed 1, mu = 1e3, dt = 1/240,
+    rho = 1."""
+    return viscosity_box_scene(n, 0.4, [((0.5, 0.7, 0.5), 0.15)], seed, mu,
+                               name=f"slab0.4+sphere0.15 {n}^3 mu{mu:g} seed{seed}")
