@@ -193,6 +193,108 @@ int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph);
  * right-hand side and every solve (kernels inside the solve graph included). */
 int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h);
 
+/* ======================================================================== */
+/* Variational viscosity: simd_viscosity3d / L_with_level
+ * (SIMD_UAAMG/simd_viscosity3d.h:12-320, simd_viscosity3d.cpp).
+ *
+ * Vectors are leaf-dense over the handle's level-0 leaf set, three channels:
+ * float[3][leaf][512] (channel c = face velocity component c), zero at every
+ * voxel that is not a DOF of that channel (uaamg_viscosity_topology gives the
+ * leaves and the per-channel DOF masks).  All input grids share one index
+ * space: voxel centre i at world i*dx, face channel c of voxel g at g - e_c/2
+ * (the transforms of L_with_level::initialize_transforms, .cpp:80-148). */
+typedef struct uaamg_viscosity uaamg_viscosity;
+
+/* L_with_level apply modes (working_mode, simd_viscosity3d.h:14) */
+#define UAAMG_VMODE_NORMAL 0
+#define UAAMG_VMODE_RESIDUAL 1
+#define UAAMG_VMODE_JACOBI 2
+#define UAAMG_VMODE_RED_GS 3
+#define UAAMG_VMODE_BLACK_GS 4
+
+/* Level 0 and the multigrid hierarchy: replaces
+ * L_with_level::create_viscosity_matrix(viscosity, liquid_sdf, solid_sdf, dt,
+ * rho) (.cpp:14-50) and the hierarchy part of the simd_viscosity3d
+ * constructor (.cpp:3621-3658: coarse levels while ndof > 4000, level-0
+ * trimming, coarsest explicit solver).  dx is the voxel size of liquid_sdf.
+ * viscosity may have no leaves (constant: its background), as at the call
+ * site FLIP_vdb.cpp:3173-3182. */
+int uaamg_viscosity_create(const uaamg_leaf_grid* viscosity, const uaamg_leaf_grid* liquid_sdf,
+                           const uaamg_leaf_grid* solid_sdf, float dt, float rho, float dx,
+                           uaamg_viscosity** out);
+int uaamg_viscosity_destroy(uaamg_viscosity* h);
+/* simd_viscosity3d::m_max_iter (100) */
+int uaamg_viscosity_set_max_iterations(uaamg_viscosity* h, int max_iterations);
+/* simd_viscosity3d::m_iteration of the last solve: the 0-based index of the
+ * iteration in which pcg_solve returned */
+int uaamg_viscosity_iterations(const uaamg_viscosity* h);
+float uaamg_viscosity_final_residual(const uaamg_viscosity* h);
+/* m_matrix_levels.size() and per level m_ndof / leaf count */
+int uaamg_viscosity_num_levels(const uaamg_viscosity* h);
+int64_t uaamg_viscosity_num_dof(const uaamg_viscosity* h, int level);
+int64_t uaamg_viscosity_leaf_count(const uaamg_viscosity* h, int level);
+/* Leaf set of a level (the coefficient pattern leaves, OpenVDB tree order):
+ * origins [n][3] and the DOF masks of m_velocity_DOF, [3][n][8] (host memory). */
+int uaamg_viscosity_topology(const uaamg_viscosity* h, int level, int32_t* origins, uint64_t* dof_masks);
+/* DOF indices of m_velocity_DOF (set_dof, .cpp:500-538), [3][n][512], -1 off DOF. */
+int uaamg_viscosity_dof_index(const uaamg_viscosity* h, int level, int32_t* out);
+
+/* L_with_level::build_rhs(velocity, solid_velocity) (.cpp:2005-2087), the
+ * m_rhs of the simd_viscosity3d constructor.  u, v, w: the three channels of
+ * the packed3grids velocity; solid_velocity: a vec3 grid (may be NULL or have
+ * no leaves). */
+int uaamg_viscosity_build_rhs(uaamg_viscosity* h, const uaamg_leaf_grid* u, const uaamg_leaf_grid* v,
+                              const uaamg_leaf_grid* w, const uaamg_leaf_grid* solid_velocity, float* rhs_out);
+int uaamg_viscosity_build_rhs_device(uaamg_viscosity* h, const uaamg_leaf_grid* u, const uaamg_leaf_grid* v,
+                                     const uaamg_leaf_grid* w, const uaamg_leaf_grid* solid_velocity,
+                                     float* d_rhs_out);
+/* The velocity at every DOF: the warm start the call site writes into the
+ * result before pcg_solve (FLIP_vdb.cpp:3188-3198). */
+int uaamg_viscosity_gather_velocity(uaamg_viscosity* h, const uaamg_leaf_grid* u, const uaamg_leaf_grid* v,
+                                    const uaamg_leaf_grid* w, float* out);
+int uaamg_viscosity_gather_velocity_device(uaamg_viscosity* h, const uaamg_leaf_grid* u,
+                                           const uaamg_leaf_grid* v, const uaamg_leaf_grid* w, float* d_out);
+
+/* simd_viscosity3d::pcg_solve(in_lhs, tolerance) (.cpp:3691-3754) with m_rhs =
+ * rhs.  velocity holds the initial guess on entry.  Returns UAAMG_SUCCESS when
+ * |r|_inf <= tolerance * |r0|_inf held, UAAMG_FAILED when the loop returned at
+ * iteration max_iterations - 1 (the reference returns void in both cases and
+ * never reports divergence); *iterations = m_iteration. */
+int uaamg_viscosity_solve_pcg(uaamg_viscosity* h, float* velocity, const float* rhs, float tolerance,
+                              int* iterations);
+int uaamg_viscosity_solve_pcg_device(uaamg_viscosity* h, float* d_velocity, const float* d_rhs,
+                                     float tolerance, int* iterations);
+
+/* Level operations (host pointers), for parity checks against the reference's
+ * L_with_level members: one light_weight_applier pass (L_apply,
+ * residual_apply, Jacobi_apply, and the RED_GS/BLACK_GS passes of one channel
+ * in place, .cpp:2187-2302); XYZ_RBGS_apply (order 0) / ZYX_RBGS_apply
+ * (order 1); restriction (.cpp:2353-2413); prolongation<true> (fine += P
+ * coarse, .cpp:2659-2729); the coefficients [3][9][n][512] (diag, invdiag,
+ * neg_x, neg_y, neg_z, cross T00, T01, T10, T11 of m_cross_channel[c]) and the
+ * level-0 trimmed-leaf bits (bit 9*c+a, trim_default_nodes .cpp:1692-1721);
+ * solve_exact on the coarsest level (.cpp:2652-2657); one mucycle as the
+ * preconditioner (z = mucycle(0, r, 2, true, 0, 2), .cpp:3837-3884). */
+int uaamg_viscosity_level_apply(uaamg_viscosity* h, int level, int mode, int channel, const float* lhs,
+                                const float* rhs, float* out);
+int uaamg_viscosity_level_rbgs(uaamg_viscosity* h, int level, int order, float* lhs, const float* rhs);
+int uaamg_viscosity_level_restrict(uaamg_viscosity* h, int fine_level, const float* fine, float* coarse);
+int uaamg_viscosity_level_prolongate(uaamg_viscosity* h, int fine_level, const float* coarse, float* fine);
+int uaamg_viscosity_level_coefficients(const uaamg_viscosity* h, int level, float* coef, uint32_t* trim);
+int uaamg_viscosity_coarsest_solve(uaamg_viscosity* h, const float* rhs, float* out);
+int uaamg_viscosity_precondition(uaamg_viscosity* h, const float* r, float* z);
+
+/* Diagnostics: one host-driven solve with a CUDA event pair around every
+ * kernel, per kernel class total device time and launch count (no
+ * counterpart in the reference). */
+int uaamg_viscosity_profile_pcg(uaamg_viscosity* h, float* d_velocity, const float* d_rhs, float tolerance,
+                                int max_classes, char* names, double* total_ms, int64_t* counts,
+                                int* nclasses);
+int uaamg_viscosity_set_stream(uaamg_viscosity* h, void* stream);
+/* 1 (default): host-driven first solve, CUDA graph afterwards; 2 graph always; 0 never. */
+int uaamg_viscosity_set_graph_mode(uaamg_viscosity* h, int use_graph);
+int64_t uaamg_viscosity_kernel_launches(const uaamg_viscosity* h);
+
 const char* uaamg_last_error(void);
 int uaamg_device_count(void);
 

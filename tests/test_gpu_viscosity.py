@@ -1,0 +1,258 @@
+"""GPU parity of the variational-viscosity UAAMG-PCG through the C ABI against
+the oracle (restatement of SIMD_UAAMG/simd_viscosity3d.cpp).
+
+Construction, every apply mode, the red-black Gauss-Seidel passes and the
+transfers are bit-exact (the kernels follow the reference's float operation
+order); whole solves match in iteration count (+-2) and solution (relative
+difference <= 1e-5), the criterion for the reference's SIMD UAAMG-PCG, whose
+dot products and coarsest CG sum in a different order.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleViscosity
+from uaamg_b200 import scenes
+from uaamg_b200.grids import LeafGrid
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-5
+ITER_TOL = 2
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("gpu tests need a CUDA device")
+    from uaamg_b200 import build
+    build.build()
+    return torch
+
+
+def make(sc):
+    from uaamg_b200.viscosity import L_with_level
+    lv = L_with_level.create_viscosity_matrix(sc.viscosity, sc.liquid_phi, sc.solid_phi, sc.dt, sc.rho, sc.dx)
+    ref = OracleViscosity(sc.liquid_phi, sc.solid_phi, sc.viscosity, sc.dt, sc.rho, sc.dx)
+    return lv, ref
+
+
+def rand_vec(ref, level, seed):
+    act = ref.dof_index(level) >= 0
+    return (np.random.default_rng(seed).standard_normal(act.shape) * act).astype(np.float32)
+
+
+@pytest.fixture(scope="module")
+def scene32(gpu):
+    sc = scenes.plain_viscosity_scene(n=32, seed=1)
+    lv, ref = make(sc)
+    return sc, lv, ref
+
+
+def test_hierarchy_topology_and_coefficients_bit_exact(scene32):
+    sc, lv, ref = scene32
+    assert lv.num_levels() == ref.num_levels >= 3
+    for l in range(ref.num_levels):
+        assert lv.num_dof(l) == ref.ndof(l)
+        o1, m1 = lv.topology(l)
+        o2, m2 = ref.topology(l)
+        assert np.array_equal(o1, o2) and np.array_equal(m1, m2)
+        assert np.array_equal(lv.dof_index(l), ref.dof_index(l))
+        (a, ta), (b, tb) = lv.coefficients(l), ref.coefficients(l)
+        assert np.array_equal(ta, tb), l
+        for c in range(3):
+            for k in range(9):
+                assert np.array_equal(a[c, k], b[c, k]), (l, c, k)
+
+
+def test_rhs_and_warm_start_bit_exact(scene32):
+    sc, lv, ref = scene32
+    r1 = lv.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    r2 = ref.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    assert np.array_equal(r1, r2)
+    from tests.golden.make_golden_viscosity import warm_start
+    assert np.array_equal(lv.gather_velocity(sc.u, sc.v, sc.w), warm_start(ref, sc))
+
+
+def test_rhs_with_moving_solid_bit_exact(gpu):
+    sc = scenes.viscosity_box_scene(24, 0.5, [], seed=3)
+    lv, ref = make(sc)
+    rng = np.random.default_rng(9)
+    org = sc.solid_phi.origins
+    sv = LeafGrid(origins=org, values=rng.uniform(-1, 1, (org.shape[0], 512, 3)).astype(np.float32),
+                  background=np.array([0.25, -0.5, 0.75], np.float32))
+    r1 = lv.build_rhs(sc.u, sc.v, sc.w, sv)
+    r2 = ref.build_rhs(sc.u, sc.v, sc.w, sv)
+    base = ref.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    assert np.abs(r2 - base).max() > 0
+    assert np.array_equal(r1, r2)
+
+
+@pytest.mark.parametrize("mode", ["normal", "residual", "jacobi"])
+def test_apply_modes_bit_exact(scene32, mode):
+    sc, lv, ref = scene32
+    for l in range(ref.num_levels):
+        x, b = rand_vec(ref, l, 10 + l), rand_vec(ref, l, 20 + l)
+        assert np.array_equal(lv.apply(l, mode, x, b), ref.apply(l, mode, x, b)), l
+
+
+@pytest.mark.parametrize("mode", ["red_gs", "black_gs"])
+def test_gauss_seidel_passes_bit_exact(scene32, mode):
+    sc, lv, ref = scene32
+    for l in range(ref.num_levels):
+        x, b = rand_vec(ref, l, 30 + l), rand_vec(ref, l, 40 + l)
+        for c in range(3):
+            assert np.array_equal(lv.apply(l, mode, x, b, channel=c), ref.apply(l, mode, x, b, channel=c)), (l, c)
+
+
+def test_rbgs_sweeps_bit_exact(scene32):
+    sc, lv, ref = scene32
+    for l in range(ref.num_levels):
+        x, b = rand_vec(ref, l, 50 + l), rand_vec(ref, l, 60 + l)
+        for order in ("xyz", "zyx"):
+            assert np.array_equal(lv.rbgs(l, x, b, order), ref.rbgs(l, x, b, order)), (l, order)
+
+
+def test_restriction_prolongation_bit_exact(scene32):
+    sc, lv, ref = scene32
+    for l in range(ref.num_levels - 1):
+        f = rand_vec(ref, l, 70 + l)
+        assert np.array_equal(lv.restriction(f, l), ref.restrict(l, f))
+        c = rand_vec(ref, l + 1, 80 + l)
+        assert np.array_equal(lv.prolongation(c, f, l), ref.prolongate(l, c, f))
+
+
+def test_coarsest_and_preconditioner_close(scene32):
+    sc, lv, ref = scene32
+    L = ref.num_levels - 1
+    b = rand_vec(ref, L, 90)
+    g, c = lv.solve_exact(b), ref.coarsest_solve(b)
+    assert np.abs(g - c).max() <= 1e-3 * max(np.abs(c).max(), 1e-30)
+    from uaamg_b200.viscosity import simd_viscosity3d
+    s = simd_viscosity3d(lv)
+    r = rand_vec(ref, 0, 91)
+    zg, zc = s.precondition(r), ref.precondition(r)
+    assert np.abs(zg - zc).max() <= 1e-2 * np.abs(zc).max()
+
+
+def _solve_pair(sc, lv, ref, tol=1e-6, warm=True, max_iter=100, graph=1):
+    from uaamg_b200.viscosity import simd_viscosity3d
+    rhs = lv.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    x0 = lv.gather_velocity(sc.u, sc.v, sc.w) if warm else lv.get_zero_vec()
+    s = simd_viscosity3d(lv)
+    s.m_max_iter = max_iter
+    s.use_graph = graph
+    x = x0.copy()
+    st = s.pcg_solve(x, tol, rhs)
+    xr, str_, itr, _ = ref.solve_pcg(x0, rhs, tol, max_iter)
+    return s, x, st, xr, str_, itr
+
+
+def test_pcg_matches_oracle_warm_start(scene32):
+    sc, lv, ref = scene32
+    s, x, st, xr, str_, itr = _solve_pair(sc, lv, ref)
+    assert st == str_ == 0
+    assert abs(s.m_iteration - itr) <= ITER_TOL
+    assert np.abs(x - xr).max() <= REL_TOL * np.abs(xr).max()
+
+
+def test_pcg_iteration_cap(scene32):
+    sc, lv, ref = scene32
+    s, x, st, xr, str_, itr = _solve_pair(sc, lv, ref, warm=False, max_iter=7)
+    assert st == str_ == 1
+    assert s.m_iteration == itr == 6
+
+
+def test_graph_and_host_loop_identical(scene32):
+    sc, lv, ref = scene32
+    from uaamg_b200.viscosity import simd_viscosity3d
+    rhs = lv.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    x0 = lv.gather_velocity(sc.u, sc.v, sc.w)
+    out = []
+    for mode in (0, 2, 2):
+        s = simd_viscosity3d(lv)
+        s.use_graph = mode
+        x = x0.copy()
+        st = s.pcg_solve(x, 1e-6, rhs)
+        out.append((st, s.m_iteration, x))
+    for st, it, x in out[1:]:
+        assert st == out[0][0] and it == out[0][1]
+        assert np.array_equal(x, out[0][2])
+
+
+def test_device_api_matches_host_api(scene32, gpu):
+    torch = gpu
+    sc, lv, ref = scene32
+    from uaamg_b200.viscosity import simd_viscosity3d
+    rhs = lv.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    x0 = lv.gather_velocity(sc.u, sc.v, sc.w)
+    s = simd_viscosity3d(lv)
+    xh = x0.copy()
+    s.pcg_solve(xh, 1e-6, rhs)
+    d_rhs = torch.zeros(rhs.shape, dtype=torch.float32, device="cuda")
+    lv.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity, out=d_rhs)
+    d_x = torch.zeros(rhs.shape, dtype=torch.float32, device="cuda")
+    lv.gather_velocity(sc.u, sc.v, sc.w, out=d_x)
+    assert np.array_equal(d_rhs.cpu().numpy(), rhs)
+    s.pcg_solve(d_x, 1e-6, d_rhs)
+    assert np.array_equal(d_x.cpu().numpy(), xh)
+
+
+def test_golden_fixture_on_gpu(gpu):
+    from tests.golden.make_golden_viscosity import FILE, golden_scene
+    g = np.load(FILE)
+    sc = golden_scene()
+    from uaamg_b200.viscosity import L_with_level, simd_viscosity3d
+    lv = L_with_level.create_viscosity_matrix(sc.viscosity, sc.liquid_phi, sc.solid_phi, sc.dt, sc.rho, sc.dx)
+    assert lv.num_levels() == int(g["levels"])
+    for l in range(lv.num_levels()):
+        o, m = lv.topology(l)
+        coef, trim = lv.coefficients(l)
+        assert np.array_equal(o, g[f"l{l}_origins"]) and np.array_equal(m, g[f"l{l}_dof"])
+        assert np.array_equal(coef, g[f"l{l}_coef"]) and np.array_equal(trim, g[f"l{l}_trim"])
+    rhs = lv.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    assert np.array_equal(rhs, g["rhs"])
+    x = lv.gather_velocity(sc.u, sc.v, sc.w)
+    assert np.array_equal(x, g["x0"])
+    s = simd_viscosity3d(lv)
+    st = s.pcg_solve(x, 1e-6, rhs)
+    assert st == int(g["pcg_status"])
+    assert abs(s.m_iteration - int(g["pcg_iters"])) <= ITER_TOL
+    assert np.abs(x - g["pcg_x"]).max() <= REL_TOL * np.abs(g["pcg_x"]).max()
+
+
+@pytest.mark.parametrize("spheres,slab", [((), 0.45), ((((0.5, 0.5, 0.5), 0.3),), None)])
+def test_other_geometries(gpu, spheres, slab):
+    sc = scenes.viscosity_box_scene(24, slab, list(spheres), seed=11)
+    lv, ref = make(sc)
+    for l in range(ref.num_levels):
+        (a, ta), (b, tb) = lv.coefficients(l), ref.coefficients(l)
+        assert np.array_equal(a, b) and np.array_equal(ta, tb)
+    s, x, st, xr, str_, itr = _solve_pair(sc, lv, ref, warm=False)
+    assert st == str_
+    assert abs(s.m_iteration - itr) <= ITER_TOL
+    assert np.abs(x - xr).max() <= REL_TOL * np.abs(xr).max()
+
+
+def test_empty_liquid(gpu):
+    sc = scenes.viscosity_box_scene(16, -1.0, [], seed=1)
+    from uaamg_b200.viscosity import L_with_level, simd_viscosity3d
+    lv = L_with_level.create_viscosity_matrix(sc.viscosity, sc.liquid_phi, sc.solid_phi, sc.dt, sc.rho, sc.dx)
+    assert lv.num_dof(0) == 0
+    rhs = lv.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    x = lv.get_zero_vec()
+    assert simd_viscosity3d(lv).pcg_solve(x, 1e-6, rhs) == 0
+
+
+def test_full_workload_128(gpu):
+    """The 128^3 workload: PCG from the call-site warm start converges; the
+    solution agrees with the oracle and its FP64 residual is at the target."""
+    sc = scenes.plain_viscosity_scene(n=128, seed=1)
+    lv, ref = make(sc)
+    assert lv.num_levels() == ref.num_levels
+    for l in range(ref.num_levels):
+        assert lv.num_dof(l) == ref.ndof(l)
+    s, x, st, xr, str_, itr = _solve_pair(sc, lv, ref)
+    assert st == str_ == 0
+    assert abs(s.m_iteration - itr) <= ITER_TOL
+    assert np.abs(x - xr).max() <= REL_TOL * np.abs(xr).max()

@@ -71,6 +71,33 @@ EXPORTS = [
     ("uaamg_poisson_set_stream", i32, [vp, vp]),
     ("uaamg_poisson_set_graph_mode", i32, [vp, i32]),
     ("uaamg_poisson_kernel_launches", i64, [vp]),
+    ("uaamg_viscosity_create", i32, [pLG, pLG, pLG, f32, f32, f32, C.POINTER(vp)]),
+    ("uaamg_viscosity_destroy", i32, [vp]),
+    ("uaamg_viscosity_set_max_iterations", i32, [vp, i32]),
+    ("uaamg_viscosity_iterations", i32, [vp]),
+    ("uaamg_viscosity_final_residual", f32, [vp]),
+    ("uaamg_viscosity_num_levels", i32, [vp]),
+    ("uaamg_viscosity_num_dof", i64, [vp, i32]),
+    ("uaamg_viscosity_leaf_count", i64, [vp, i32]),
+    ("uaamg_viscosity_topology", i32, [vp, i32, vp, vp]),
+    ("uaamg_viscosity_dof_index", i32, [vp, i32, vp]),
+    ("uaamg_viscosity_build_rhs", i32, [vp, pLG, pLG, pLG, pLG, vp]),
+    ("uaamg_viscosity_build_rhs_device", i32, [vp, pLG, pLG, pLG, pLG, vp]),
+    ("uaamg_viscosity_gather_velocity", i32, [vp, pLG, pLG, pLG, vp]),
+    ("uaamg_viscosity_gather_velocity_device", i32, [vp, pLG, pLG, pLG, vp]),
+    ("uaamg_viscosity_solve_pcg", i32, [vp, vp, vp, f32, C.POINTER(C.c_int)]),
+    ("uaamg_viscosity_solve_pcg_device", i32, [vp, vp, vp, f32, C.POINTER(C.c_int)]),
+    ("uaamg_viscosity_level_apply", i32, [vp, i32, i32, i32, vp, vp, vp]),
+    ("uaamg_viscosity_level_rbgs", i32, [vp, i32, i32, vp, vp]),
+    ("uaamg_viscosity_level_restrict", i32, [vp, i32, vp, vp]),
+    ("uaamg_viscosity_level_prolongate", i32, [vp, i32, vp, vp]),
+    ("uaamg_viscosity_level_coefficients", i32, [vp, i32, vp, vp]),
+    ("uaamg_viscosity_coarsest_solve", i32, [vp, vp, vp]),
+    ("uaamg_viscosity_precondition", i32, [vp, vp, vp]),
+    ("uaamg_viscosity_profile_pcg", i32, [vp, vp, vp, f32, i32, vp, vp, vp, C.POINTER(C.c_int)]),
+    ("uaamg_viscosity_set_stream", i32, [vp, vp]),
+    ("uaamg_viscosity_set_graph_mode", i32, [vp, i32]),
+    ("uaamg_viscosity_kernel_launches", i64, [vp]),
     ("uaamg_last_error", C.c_char_p, []),
     ("uaamg_device_count", i32, []),
 ]

@@ -1,2 +1,3 @@
 // uaamg_lib.cu -- single translation unit of libuaamg_b200.so
 #include "poisson.cu"
+#include "viscosity.cu"

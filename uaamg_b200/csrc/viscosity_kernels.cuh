@@ -1,0 +1,661 @@
+// viscosity_kernels.cuh -- sm_100a kernels of the variational-viscosity
+// UAAMG-PCG (the solve phase).
+//
+// Arithmetic follows L_with_level::light_weight_applier::component_operator<c>
+// (SIMD_UAAMG/simd_viscosity3d.cpp:2849-3603) operation by operation with
+// round-to-nearest intrinsics (the library is built with --fmad=false), so the
+// per-voxel results are bit-identical to the reference's AVX2 lanes.
+//
+// Layout of a level (one leaf set for all three velocity channels: the leaves
+// of the union of the channel DOF masks dilated by the coefficient pattern):
+//   dof   uint64 [3][nl][8]     per-channel DOF masks (word x = plane x)
+//   nb    int32  [nl][27]       3x3x3 neighbour leaves, (dx+1)*9+(dy+1)*3+dz+1
+//   coef  float  [27][nl][512]  array (c*9 + a): diag, invdiag, neg_x, neg_y,
+//                               neg_z, T00, T01, T10, T11 of channel c
+//   vectors float [3][nl][512], zero at every non-DOF voxel
+// One CTA of 128 threads per (leaf, channel); thread t owns voxels 4t..4t+3
+// (x = t>>4, y = (t>>1)&7, z = 4*(t&1)+j): one float4 of every array.
+#pragma once
+#include "common.cuh"
+#include "poisson_kernels.cuh"
+
+namespace uaamg {
+
+#define VNA 9
+enum { VA_DIAG = 0, VA_INV = 1, VA_NEGX = 2, VA_NEGY = 3, VA_NEGZ = 4, VA_T00 = 5, VA_T01 = 6, VA_T10 = 7,
+       VA_T11 = 8 };
+enum { VM_NORMAL = 0, VM_RESIDUAL = 1, VM_JACOBI = 2, VM_RED = 3, VM_BLACK = 4 };
+
+struct VLevel {
+    int nl;
+    const uint64_t* dof;          // [3][nl][8]
+    const int* nb;                // [nl][27]
+    const float* coef;            // [27][nl][512]
+    const uint32_t* trim;         // [nl] bit (c*9+a): leaf holds the default
+    const int* parent;            // [nl] coarse leaf, -1 if none
+    const unsigned char* octant;  // [nl] position in the parent: x<<2 | y<<1 | z
+    const int* child;             // [nl][8] fine leaf per octant, -1 if none
+    float app[27];                // light_weight_applier defaults (missing leaf)
+};
+
+__device__ __forceinline__ unsigned vmask4(const VLevel& L, int c, int leaf, int t) {
+    return (unsigned)((L.dof[((long long)c * L.nl + leaf) * 8 + (t >> 4)] >> ((t & 15) * 4)) & 0xFull);
+}
+__device__ __forceinline__ bool vdof_bit(const VLevel& L, int c, int leaf, int off) {
+    return (L.dof[((long long)c * L.nl + leaf) * 8 + (off >> 6)] >> (off & 63)) & 1ull;
+}
+__device__ __forceinline__ int vnb_index(int X, int Y, int Z) {
+    const int a = X < 0 ? 0 : (X > 7 ? 2 : 1), b = Y < 0 ? 0 : (Y > 7 ? 2 : 1), c = Z < 0 ? 0 : (Z > 7 ? 2 : 1);
+    return a * 9 + b * 3 + c;
+}
+__device__ __forceinline__ int voff3(int X, int Y, int Z) { return ((X & 7) << 6) | ((Y & 7) << 3) | (Z & 7); }
+
+// Values of a [nl][512] array at the thread's four voxels shifted by
+// (dx, dy, dz), dz in {-1, 0, 1}; leaves that do not exist read `fill`, and
+// leaves whose trim bit is set (trim != nullptr) read `def`.
+__device__ __forceinline__ float vload1(const float* arr, const int* nbrow, const uint32_t* trim, uint32_t bit,
+                                        int X, int Y, int Z, float fill, float def) {
+    const int lf = nbrow[vnb_index(X, Y, Z)];
+    if (lf < 0) return fill;
+    if (trim && (trim[lf] & bit)) return def;
+    return arr[(long long)lf * UAAMG_LEAF + voff3(X, Y, Z)];
+}
+__device__ __forceinline__ float4 vload4(const float* arr, const int* nbrow, const uint32_t* trim, uint32_t bit,
+                                         int x, int y, int z0, int dx, int dy, int dz, float fill, float def) {
+    const int X = x + dx, Y = y + dy;
+    const int lf = nbrow[vnb_index(X, Y, z0)];
+    float4 a;
+    if (lf < 0) a = f4splat(fill);
+    else if (trim && (trim[lf] & bit)) a = f4splat(def);
+    else a = reinterpret_cast<const float4*>(arr)[((long long)lf * UAAMG_LEAF + voff3(X, Y, z0)) >> 2];
+    if (dz == 0) return a;
+    if (dz > 0) {
+        const float n = vload1(arr, nbrow, trim, bit, X, Y, z0 + 4, fill, def);
+        return make_float4(a.y, a.z, a.w, n);
+    }
+    const float p = vload1(arr, nbrow, trim, bit, X, Y, z0 - 1, fill, def);
+    return make_float4(p, a.x, a.y, a.z);
+}
+
+struct VArr {  // one coefficient array of a level with its trim bit and applier default
+    const float* a;
+    uint32_t bit;
+    float def;
+};
+__device__ __forceinline__ VArr varr(const VLevel& L, int c, int a) {
+    VArr r;
+    r.a = L.coef + (long long)(c * VNA + a) * L.nl * UAAMG_LEAF;
+    r.bit = 1u << (c * VNA + a);
+    r.def = L.app[c * VNA + a];
+    return r;
+}
+__device__ __forceinline__ float4 cload4(const VArr& A, const VLevel& L, const int* nbrow, int x, int y, int z0, int dx,
+                                         int dy, int dz) {
+    return vload4(A.a, nbrow, L.trim, A.bit, x, y, z0, dx, dy, dz, A.def, A.def);
+}
+__device__ __forceinline__ float4 uload4(const float* v, const VLevel& L, int c, const int* nbrow, int x, int y, int z0,
+                                         int dx, int dy, int dz) {
+    return vload4(v + (long long)c * L.nl * UAAMG_LEAF, nbrow, nullptr, 0u, x, y, z0, dx, dy, dz, 0.f, 0.f);
+}
+
+// Off-diagonal sum of channel c at the thread's four voxels (faced_result[1]
+// after the cross terms, :3084-3490) and the centre value.
+__device__ __forceinline__ float4 voffdiag(const VLevel& L, int c, int leaf, int t, const float* x, float4& xc) {
+    const int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    const int* nbrow = L.nb + (long long)leaf * 27;
+    const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
+    int e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0};
+    e0[d0] = 1;
+    e1[d1] = 1;
+    e2[d2] = 1;
+    xc = uload4(x, L, c, nbrow, X, Y, Z0, 0, 0, 0);
+    // same channel, absolute axes x, y, z: u(g+e)*neg(g+e) and u(g-e)*neg(g)
+    float4 fr[6];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int px = ax == 0, py = ax == 1, pz = ax == 2;
+        const VArr W = varr(L, c, VA_NEGX + ax);
+        const float4 up = uload4(x, L, c, nbrow, X, Y, Z0, px, py, pz);
+        const float4 wp = cload4(W, L, nbrow, X, Y, Z0, px, py, pz);
+        const float4 um = uload4(x, L, c, nbrow, X, Y, Z0, -px, -py, -pz);
+        const float4 wm = cload4(W, L, nbrow, X, Y, Z0, 0, 0, 0);
+        fr[2 * ax] = make_float4(__fmul_rn(up.x, wp.x), __fmul_rn(up.y, wp.y), __fmul_rn(up.z, wp.z),
+                                 __fmul_rn(up.w, wp.w));
+        fr[2 * ax + 1] = make_float4(__fmul_rn(um.x, wm.x), __fmul_rn(um.y, wm.y), __fmul_rn(um.z, wm.z),
+                                     __fmul_rn(um.w, wm.w));
+    }
+    // Td2 (m_cross_channel[d2], channel d1 velocities) and Td1
+    // (m_cross_channel[d1], channel d2 velocities)
+    const float4 u1_g = uload4(x, L, d1, nbrow, X, Y, Z0, 0, 0, 0);
+    const float4 u1_p1 = uload4(x, L, d1, nbrow, X, Y, Z0, e1[0], e1[1], e1[2]);
+    const float4 u1_m0 = uload4(x, L, d1, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 u1_m0p1 = uload4(x, L, d1, nbrow, X, Y, Z0, e1[0] - e0[0], e1[1] - e0[1], e1[2] - e0[2]);
+    const float4 u2_g = uload4(x, L, d2, nbrow, X, Y, Z0, 0, 0, 0);
+    const float4 u2_m0 = uload4(x, L, d2, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 u2_p2 = uload4(x, L, d2, nbrow, X, Y, Z0, e2[0], e2[1], e2[2]);
+    const float4 u2_m0p2 = uload4(x, L, d2, nbrow, X, Y, Z0, e2[0] - e0[0], e2[1] - e0[1], e2[2] - e0[2]);
+    const float4 a00 = cload4(varr(L, d2, VA_T00), L, nbrow, X, Y, Z0, 0, 0, 0);
+    const float4 a01 = cload4(varr(L, d2, VA_T01), L, nbrow, X, Y, Z0, 0, 0, 0);
+    const float4 a10 = cload4(varr(L, d2, VA_T10), L, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 a11 = cload4(varr(L, d2, VA_T11), L, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 b00 = cload4(varr(L, d1, VA_T00), L, nbrow, X, Y, Z0, 0, 0, 0);
+    const float4 b01 = cload4(varr(L, d1, VA_T01), L, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 b10 = cload4(varr(L, d1, VA_T10), L, nbrow, X, Y, Z0, 0, 0, 0);
+    const float4 b11 = cload4(varr(L, d1, VA_T11), L, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    float4 off;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float f1 = __fadd_rn(f4get(fr[0], j), f4get(fr[1], j));
+        float f3 = __fadd_rn(f4get(fr[2], j), f4get(fr[3], j));
+        float f5 = __fadd_rn(f4get(fr[4], j), f4get(fr[5], j));
+        f1 = __fadd_rn(f1, f3);
+        f1 = __fadd_rn(f1, f5);
+        const float R0 = __fmul_rn(f4get(u1_g, j), f4get(a00, j));
+        const float R1 = __fmul_rn(f4get(a01, j), f4get(u1_p1, j));
+        const float R2 = __fmul_rn(f4get(a10, j), f4get(u1_m0, j));
+        const float R3 = __fmul_rn(f4get(a11, j), f4get(u1_m0p1, j));
+        const float Q0 = __fmul_rn(f4get(b00, j), f4get(u2_g, j));
+        const float Q1 = __fmul_rn(f4get(b01, j), f4get(u2_m0, j));
+        const float Q2 = __fmul_rn(f4get(b10, j), f4get(u2_p2, j));
+        const float Q3 = __fmul_rn(f4get(b11, j), f4get(u2_m0p2, j));
+        const float td2 = __fadd_rn(__fadd_rn(R0, R1), __fadd_rn(R2, R3));
+        const float td1 = __fadd_rn(__fadd_rn(Q0, Q1), __fadd_rn(Q2, Q3));
+        f1 = __fadd_rn(f1, td2);
+        f1 = __fadd_rn(f1, td1);
+        f4set(off, j, f1);
+    }
+    return off;
+}
+
+// One applier pass for channel c at the thread's voxels; m = DOF bits.
+template <int MODE>
+__device__ __forceinline__ float4 vapply_value(const VLevel& L, int c, int leaf, int t, const float* x,
+                                               const float* b, float w, unsigned m, float4& xc) {
+    const float4 off = voffdiag(L, c, leaf, t, x, xc);
+    const int* nbrow = L.nb + (long long)leaf * 27;
+    const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
+    float4 res = xc;
+    if (MODE == VM_RED || MODE == VM_BLACK) {
+        const float4 bb = uload4(b, L, c, nbrow, X, Y, Z0, 0, 0, 0);
+        const float4 iv = cload4(varr(L, c, VA_INV), L, nbrow, X, Y, Z0, 0, 0, 0);
+        const float one_minus_w = __fsub_rn(1.0f, w);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int par = (X + Y + Z0 + j) & 1;
+            const bool upd = (MODE == VM_RED) ? (par == 0) : (par == 1);
+            float r = __fsub_rn(f4get(bb, j), f4get(off, j));
+            r = __fmul_rn(r, f4get(iv, j));
+            r = __fmul_rn(r, w);
+            const float v = __fmaf_rn(f4get(xc, j), one_minus_w, r);
+            f4set(res, j, upd ? v : f4get(xc, j));
+        }
+    } else {
+        const float4 dg = cload4(varr(L, c, VA_DIAG), L, nbrow, X, Y, Z0, 0, 0, 0);
+        if (MODE == VM_NORMAL) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) f4set(res, j, __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+        } else {
+            const float4 bb = uload4(b, L, c, nbrow, X, Y, Z0, 0, 0, 0);
+            if (MODE == VM_RESIDUAL) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    f4set(res, j, __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j))));
+            } else {  // JACOBI
+                const float4 iv = cload4(varr(L, c, VA_INV), L, nbrow, X, Y, Z0, 0, 0, 0);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+                    r = __fmul_rn(r, f4get(iv, j));
+                    f4set(res, j, __fmaf_rn(w, r, f4get(xc, j)));
+                }
+            }
+        }
+    }
+    if (!(m & 1)) res.x = 0.f;
+    if (!(m & 2)) res.y = 0.f;
+    if (!(m & 4)) res.z = 0.f;
+    if (!(m & 8)) res.w = 0.f;
+    return res;
+}
+
+// grid (nl, channels): NORMAL / RESIDUAL / JACOBI write all channels of out
+// (blockIdx.y = channel); RED / BLACK update channel c0 of x in place.
+// Voxel groups without DOFs are not written: every vector holds zeros there.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_vapply(VLevel L, int c0, const float* x, const float* b, float* out,
+                                                float w) {
+    griddep_wait();
+    griddep_launch();
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    const int c = (MODE == VM_RED || MODE == VM_BLACK) ? c0 : (int)blockIdx.y;
+    const unsigned m = vmask4(L, c, leaf, t);
+    if (!m) return;
+    float4 xc;
+    const float4 res = vapply_value<MODE>(L, c, leaf, t, x, b, w, m, xc);
+    reinterpret_cast<float4*>(out + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
+}
+
+// restriction (:2353-2413), grid (coarse nl, 3): coarse = (sum of the DOF
+// children) * 0.125 * 0.5 * 2, zero at coarse non-DOF voxels
+__global__ void __launch_bounds__(128) k_vrestrict(VLevel F, VLevel C, const float* fine, float* coarse) {
+    griddep_wait();
+    griddep_launch();
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const unsigned m = vmask4(C, c, leaf, t);
+    const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
+    float4 res = f4zero();
+    if (m) {
+        const int q = ((X >= 4) << 2) | ((Y >= 4) << 1) | (Z0 >= 4);
+        const int fl = C.child[leaf * 8 + q];
+        if (fl >= 0) {
+            const float* fv = fine + ((long long)c * F.nl + fl) * UAAMG_LEAF;
+            const uint64_t* fm = F.dof + ((long long)c * F.nl + fl) * 8;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (!(m >> j & 1)) continue;
+                const int base = voff3(2 * X, 2 * Y, 2 * (Z0 + j));
+                float s = 0.f;
+#pragma unroll
+                for (int a = 0; a < 2; ++a)
+#pragma unroll
+                    for (int bq = 0; bq < 2; ++bq)
+#pragma unroll
+                        for (int k = 0; k < 2; ++k) {
+                            const int fo = base + 64 * a + 8 * bq + k;
+                            if ((fm[fo >> 6] >> (fo & 63)) & 1ull) s = __fadd_rn(s, fv[fo]);
+                        }
+                f4set(res, j, __fmul_rn(__fmul_rn(__fmul_rn(s, 0.125f), 0.5f), 2.0f));
+            }
+        }
+    }
+    reinterpret_cast<float4*>(coarse + (long long)c * C.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
+}
+
+// prolongation<true> (:2659-2729), grid (fine nl, 3): fine += coarse parent
+__global__ void __launch_bounds__(128) k_vprolong(VLevel F, VLevel C, const float* coarse, float* fine) {
+    griddep_wait();
+    griddep_launch();
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const unsigned m = vmask4(F, c, leaf, t);
+    if (!m) return;
+    const int P = F.parent[leaf];
+    if (P < 0) return;
+    const int oc = F.octant[leaf];
+    const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
+    const int cx = ((oc >> 2) & 1) * 4 + (X >> 1), cy = ((oc >> 1) & 1) * 4 + (Y >> 1);
+    const float* cv = coarse + ((long long)c * C.nl + P) * UAAMG_LEAF;
+    float4* fp = reinterpret_cast<float4*>(fine + (long long)c * F.nl * UAAMG_LEAF) + (long long)leaf * UAAMG_LEAF4 + t;
+    float4 v = *fp;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (!(m >> j & 1)) continue;
+        const int cz = (oc & 1) * 4 + ((Z0 + j) >> 1);
+        f4set(v, j, __fadd_rn(f4get(v, j), cv[(cx << 6) | (cy << 3) | cz]));
+    }
+    *fp = v;
+}
+
+// zero every non-DOF voxel of a 3-channel vector (inputs from callers)
+__global__ void __launch_bounds__(128) k_vmask(VLevel L, float* v) {
+    griddep_wait();
+    griddep_launch();
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const unsigned m = vmask4(L, c, leaf, t);
+    float4* p = reinterpret_cast<float4*>(v + (long long)c * L.nl * UAAMG_LEAF) + (long long)leaf * UAAMG_LEAF4 + t;
+    if (m == 0xF) return;
+    float4 a = *p;
+    if (!(m & 1)) a.x = 0.f;
+    if (!(m & 2)) a.y = 0.f;
+    if (!(m & 4)) a.z = 0.f;
+    if (!(m & 8)) a.w = 0.f;
+    *p = a;
+}
+
+// ---------------------------------------------------------------------------
+// PCG of simd_viscosity3d::pcg_solve (:3691-3754) with device-resident scalars.
+// Reductions: per-block partials (FP64 for dots), the last block to arrive
+// combines them in block order, so results do not depend on scheduling.
+__device__ __forceinline__ bool vpublish(double part, double* partials, unsigned* ticket, bool* sh_last) {
+    const unsigned bid = blockIdx.x + blockIdx.y * gridDim.x, nb = gridDim.x * gridDim.y;
+    if (threadIdx.x == 0) {
+        partials[bid] = part;
+        __threadfence();
+        const unsigned tk = atomicAdd(ticket, 1u);
+        *sh_last = (tk == nb - 1);
+    }
+    __syncthreads();
+    return *sh_last;
+}
+__device__ __forceinline__ double vgather_sum(const double* partials, double* sh) {
+    const int nb = gridDim.x * gridDim.y;
+    double acc = 0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += __ldcg(partials + i);
+    return block_sum128(acc, sh);
+}
+__device__ __forceinline__ float vgather_max(const double* partials, float* sh) {
+    const int nb = gridDim.x * gridDim.y;
+    float acc = 0.f;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) acc = nanmax(acc, (float)__ldcg(partials + i));
+    return block_max128(acc, sh);
+}
+__device__ __forceinline__ float vabs4(float4 v, unsigned m) {
+    float a = 0.f;
+    if (m & 1) a = nanmax(a, absprop(v.x));
+    if (m & 2) a = nanmax(a, absprop(v.y));
+    if (m & 4) a = nanmax(a, absprop(v.z));
+    if (m & 8) a = nanmax(a, absprop(v.w));
+    return a;
+}
+
+// lines 2-3: r = b - A x; nu = |r|_inf; numax = tol * nu
+__global__ void __launch_bounds__(128) k_vpcg_init(VLevel L, const float* x, const float* b, float* r,
+                                                   double* partials, PcgState* st, cudaGraphConditionalHandle cond,
+                                                   int use_cond) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ float shf[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const unsigned m = vmask4(L, c, leaf, t);
+    float a = 0.f;
+    if (m) {
+        float4 xc;
+        const float4 res = vapply_value<VM_RESIDUAL>(L, c, leaf, t, x, b, 1.f, m, xc);
+        reinterpret_cast<float4*>(r + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
+        a = vabs4(res, m);
+    }
+    const float part = block_max128(a, shf);
+    if (vpublish((double)part, partials, &st->ticket[1], &last)) {
+        const float nu = vgather_max(partials, shf);
+        if (t == 0) {
+            st->nu = nu;
+            st->numax = __fmul_rn(st->tol, nu);
+            st->iter = 0;
+            st->first = 1;
+            st->iterations_taken = 0;
+            st->alpha = 0.f;
+            st->beta = 0.f;
+            int status = PCG_RUNNING;
+            if (nu <= st->numax) status = PCG_SUCCESS;
+            else if (st->max_iter <= 0) status = PCG_FAILED_MAXITER;  // loop never runs: x untouched
+            st->status = status;
+            st->ticket[1] = 0;
+            set_cond(cond, use_cond, status == PCG_RUNNING ? 1u : 0u);
+        }
+    }
+}
+
+// line 13 tail: rho_new = z.r; first iteration: rho = rho_new (line 4),
+// later: beta = rho_new / rho, rho = rho_new (lines 14-15)
+__global__ void __launch_bounds__(128) k_vpcg_rho(VLevel L, const float* z, const float* r, double* partials,
+                                                  PcgState* st) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ double shd[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const long long i = (long long)c * L.nl * UAAMG_LEAF4 + (long long)leaf * UAAMG_LEAF4 + t;
+    const float4 zz = reinterpret_cast<const float4*>(z)[i], rr = reinterpret_cast<const float4*>(r)[i];
+    const double s = ((double)zz.x * rr.x + (double)zz.y * rr.y) + ((double)zz.z * rr.z + (double)zz.w * rr.w);
+    const double part = block_sum128(s, shd);
+    if (vpublish(part, partials, &st->ticket[2], &last)) {
+        const double tot = vgather_sum(partials, shd);
+        if (t == 0) {
+            const float rho_new = (float)tot;
+            if (st->first) {
+                st->beta = 0.f;
+            } else {
+                st->beta = __fdiv_rn(rho_new, st->rho);
+            }
+            st->rho = rho_new;
+            st->ticket[2] = 0;
+        }
+    }
+}
+
+// line 16: x += alpha p (not in the first iteration); p = z + beta p
+__global__ void __launch_bounds__(128) k_vpcg_update_p(VLevel L, const float* z, float* p, float* x,
+                                                       const PcgState* st) {
+    griddep_wait();
+    griddep_launch();
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const long long i = (long long)c * L.nl * UAAMG_LEAF4 + (long long)leaf * UAAMG_LEAF4 + t;
+    const float beta = st->beta, alpha = st->alpha;
+    float4 pp = reinterpret_cast<float4*>(p)[i];
+    const float4 zz = reinterpret_cast<const float4*>(z)[i];
+    if (!st->first) {
+        float4 xx = reinterpret_cast<float4*>(x)[i];
+        xx.x = __fadd_rn(xx.x, __fmul_rn(alpha, pp.x));
+        xx.y = __fadd_rn(xx.y, __fmul_rn(alpha, pp.y));
+        xx.z = __fadd_rn(xx.z, __fmul_rn(alpha, pp.z));
+        xx.w = __fadd_rn(xx.w, __fmul_rn(alpha, pp.w));
+        reinterpret_cast<float4*>(x)[i] = xx;
+    }
+    pp.x = __fadd_rn(zz.x, __fmul_rn(beta, pp.x));
+    pp.y = __fadd_rn(zz.y, __fmul_rn(beta, pp.y));
+    pp.z = __fadd_rn(zz.z, __fmul_rn(beta, pp.z));
+    pp.w = __fadd_rn(zz.w, __fmul_rn(beta, pp.w));
+    reinterpret_cast<float4*>(p)[i] = pp;
+}
+
+// lines 6-7: q = A p; sigma = p.q; alpha = rho / sigma
+__global__ void __launch_bounds__(128) k_vpcg_Ap(VLevel L, const float* p, float* q, double* partials, PcgState* st) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ double shd[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const unsigned m = vmask4(L, c, leaf, t);
+    double s = 0.0;
+    if (m) {
+        float4 xc;
+        const float4 res = vapply_value<VM_NORMAL>(L, c, leaf, t, p, nullptr, 1.f, m, xc);
+        reinterpret_cast<float4*>(q + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
+        s = ((double)xc.x * res.x + (double)xc.y * res.y) + ((double)xc.z * res.z + (double)xc.w * res.w);
+    }
+    const double part = block_sum128(s, shd);
+    if (vpublish(part, partials, &st->ticket[3], &last)) {
+        const double tot = vgather_sum(partials, shd);
+        if (t == 0) {
+            const float sigma = (float)tot;
+            st->sigma = sigma;
+            st->alpha = __fdiv_rn(st->rho, sigma);
+            st->first = 0;
+            st->ticket[3] = 0;
+        }
+    }
+}
+
+// lines 8-9: r -= alpha q; nu = |r|_inf; stop when nu <= numax or at the
+// last allowed iteration (no divergence test in this solver)
+__global__ void __launch_bounds__(128) k_vpcg_update_r(VLevel L, const float* q, float* r, double* partials,
+                                                       PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ float shf[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const unsigned m = vmask4(L, c, leaf, t);
+    const long long i = (long long)c * L.nl * UAAMG_LEAF4 + (long long)leaf * UAAMG_LEAF4 + t;
+    const float na = -st->alpha;
+    float a = 0.f;
+    if (m) {
+        const float4 qq = reinterpret_cast<const float4*>(q)[i];
+        float4 rr = reinterpret_cast<float4*>(r)[i];
+        rr.x = __fadd_rn(rr.x, __fmul_rn(na, qq.x));
+        rr.y = __fadd_rn(rr.y, __fmul_rn(na, qq.y));
+        rr.z = __fadd_rn(rr.z, __fmul_rn(na, qq.z));
+        rr.w = __fadd_rn(rr.w, __fmul_rn(na, qq.w));
+        reinterpret_cast<float4*>(r)[i] = rr;
+        a = vabs4(rr, m);
+    }
+    const float part = block_max128(a, shf);
+    if (vpublish((double)part, partials, &st->ticket[4], &last)) {
+        const float nu = vgather_max(partials, shf);
+        if (t == 0) {
+            const int k = st->iter;
+            st->nu = nu;
+            int status = PCG_RUNNING;
+            if (nu <= st->numax) {
+                status = PCG_SUCCESS;
+                st->iterations_taken = k;
+            } else if (k == st->max_iter - 1) {
+                status = PCG_FAILED_MAXITER;
+                st->iterations_taken = k;
+            }
+            st->iter = k + 1;
+            st->status = status;
+            st->ticket[4] = 0;
+            set_cond(cond, use_cond, status == PCG_RUNNING ? 1u : 0u);
+        }
+    }
+}
+
+// line 10: x += alpha p after the stopping iteration
+__global__ void __launch_bounds__(128) k_vpcg_finish(VLevel L, const float* p, float* x, const PcgState* st) {
+    griddep_wait();
+    griddep_launch();
+    if (st->iter == 0) return;  // stopped before the loop
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const long long i = (long long)c * L.nl * UAAMG_LEAF4 + (long long)leaf * UAAMG_LEAF4 + t;
+    const float alpha = st->alpha;
+    const float4 pp = reinterpret_cast<const float4*>(p)[i];
+    float4 xx = reinterpret_cast<float4*>(x)[i];
+    xx.x = __fadd_rn(xx.x, __fmul_rn(alpha, pp.x));
+    xx.y = __fadd_rn(xx.y, __fmul_rn(alpha, pp.y));
+    xx.z = __fadd_rn(xx.z, __fmul_rn(alpha, pp.z));
+    xx.w = __fadd_rn(xx.w, __fmul_rn(alpha, pp.w));
+    reinterpret_cast<float4*>(x)[i] = xx;
+}
+
+// |v|_inf (lv_abs_max) or v.w (lv_dot) over a level, result in out[0]
+__global__ void __launch_bounds__(128) k_vreduce(VLevel L, const float* v, const float* w, double* partials,
+                                                 unsigned* ticket, float* out) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ float shf[4];
+    __shared__ double shd[4];
+    __shared__ bool last;
+    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    const unsigned m = vmask4(L, c, leaf, t);
+    const long long i = (long long)c * L.nl * UAAMG_LEAF4 + (long long)leaf * UAAMG_LEAF4 + t;
+    const float4 a = reinterpret_cast<const float4*>(v)[i];
+    if (w) {
+        const float4 bb = reinterpret_cast<const float4*>(w)[i];
+        double s = 0.0;
+        if (m & 1) s += (double)a.x * bb.x;
+        if (m & 2) s += (double)a.y * bb.y;
+        if (m & 4) s += (double)a.z * bb.z;
+        if (m & 8) s += (double)a.w * bb.w;
+        const double part = block_sum128(s, shd);
+        if (vpublish(part, partials, ticket, &last)) {
+            const double tot = vgather_sum(partials, shd);
+            if (t == 0) { *out = (float)tot; *ticket = 0; }
+        }
+    } else {
+        const float part = block_max128(vabs4(a, m), shf);
+        if (vpublish((double)part, partials, ticket, &last)) {
+            const float mx = vgather_max(partials, shf);
+            if (t == 0) { *out = mx; *ticket = 0; }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coarsest level: Eigen::ConjugateGradient<RowMajor, Upper|Lower> with the
+// diagonal preconditioner, tolerance FLT_EPSILON, maxIterations 10, zero guess
+// (construct_exact_solver / solve_exact, :2645-2657), one CTA.  The explicit
+// matrix rows (explicit_matrix_reducer, :2415-2605) are stored as an ELL of
+// width 15 with columns ascending, the order of a RowMajor row after
+// setFromTriplets.
+#define VCG_W 15
+struct DCoarsestV {
+    int n;
+    const long long* slot;  // [n] c*nl*512 + leaf*512 + offset
+    const float* invd;      // [n] 1/diag (1 where diag == 0)
+    const int* col;         // [n][15] (-1 = padding)
+    const float* val;       // [n][15]
+};
+
+template <int ROWS>
+__global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, const float* rhs, float* out) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ float ps[CG_THREADS * ROWS];
+    __shared__ float red[3][64];
+    const int tid = threadIdx.x, n = C.n;
+    float x[ROWS], r[ROWS], p[ROWS], z[ROWS], iv[ROWS];
+    float bb = 0.f;
+#pragma unroll
+    for (int k = 0; k < ROWS; ++k) {
+        const int i = tid + k * CG_THREADS;
+        const bool ok = i < n;
+        x[k] = 0.f;
+        r[k] = ok ? rhs[C.slot[i]] : 0.f;
+        iv[k] = ok ? C.invd[i] : 0.f;
+        p[k] = 0.f;
+        bb = __fadd_rn(bb, __fmul_rn(r[k], r[k]));
+    }
+    int rb = 0;
+    const float rhsNorm2 = cg_block_sum(bb, red[rb]);
+    rb = rb == 2 ? 0 : rb + 1;
+    const float threshold = fmaxf(__fmul_rn(__fmul_rn(FLT_EPSILON, FLT_EPSILON), rhsNorm2), FLT_MIN);
+    if (rhsNorm2 != 0.f && !(rhsNorm2 < threshold)) {
+        float an = 0.f;
+#pragma unroll
+        for (int k = 0; k < ROWS; ++k) {
+            p[k] = __fmul_rn(iv[k], r[k]);
+            an = __fadd_rn(an, __fmul_rn(r[k], p[k]));
+        }
+        float absNew = cg_block_sum(an, red[rb]);
+        rb = rb == 2 ? 0 : rb + 1;
+        for (int it = 0; it < 10; ++it) {
+#pragma unroll
+            for (int k = 0; k < ROWS; ++k) ps[tid + k * CG_THREADS] = p[k];
+            __syncthreads();
+            float pt = 0.f, tq[ROWS];
+#pragma unroll
+            for (int k = 0; k < ROWS; ++k) {
+                const int i = tid + k * CG_THREADS;
+                float s = 0.f;
+                if (i < n) {
+                    const int* cr = C.col + (long long)i * VCG_W;
+                    const float* vr = C.val + (long long)i * VCG_W;
+#pragma unroll
+                    for (int e = 0; e < VCG_W; ++e) {
+                        const int cc = __ldg(cr + e);
+                        if (cc >= 0) s = __fadd_rn(s, __fmul_rn(__ldg(vr + e), ps[cc]));
+                    }
+                }
+                tq[k] = s;
+                pt = __fadd_rn(pt, __fmul_rn(p[k], s));
+            }
+            const float alpha = __fdiv_rn(absNew, cg_block_sum(pt, red[rb]));
+            rb = rb == 2 ? 0 : rb + 1;
+            float rr = 0.f, rz = 0.f;
+#pragma unroll
+            for (int k = 0; k < ROWS; ++k) {
+                x[k] = __fmaf_rn(alpha, p[k], x[k]);
+                r[k] = __fmaf_rn(-alpha, tq[k], r[k]);
+                z[k] = __fmul_rn(iv[k], r[k]);
+                rr = __fadd_rn(rr, __fmul_rn(r[k], r[k]));
+                rz = __fadd_rn(rz, __fmul_rn(r[k], z[k]));
+            }
+            const float2 s2 = cg_block_sum2(rr, rz, red[rb]);
+            rb = rb == 2 ? 0 : rb + 1;
+            if (s2.x < threshold) break;
+            const float absOld = absNew;
+            absNew = s2.y;
+            const float beta = __fdiv_rn(absNew, absOld);
+#pragma unroll
+            for (int k = 0; k < ROWS; ++k) p[k] = __fmaf_rn(beta, p[k], z[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < ROWS; ++k) {
+        const int i = tid + k * CG_THREADS;
+        if (i < n) out[C.slot[i]] = x[k];
+    }
+}
+
+}  // namespace uaamg
