@@ -611,19 +611,26 @@ static void venqueue_body(VEnq& E, cudaGraphConditionalHandle cond, int use_cond
     const VLevelDev& D = h->lv[0];
     const dim3 g((unsigned)D.L.nl, 3);
     enqueue_mucycle(E, 0, h->z, h->r, true);
-    if (E.prof) E.pb("L0 pcg rho");
-    launch2(k_vpcg_rho, g, 128, E.s, D.L, (const float*)h->z, (const float*)h->r, h->partials, h->st);
+    const dim3 gd((unsigned)((3 * D.L.nl + 3) / 4));
+    float* part = reinterpret_cast<float*>(h->partials);
+    if (E.prof) E.pb("L0 pcg rho (z.r)");
+    launch2(k_vdot_leaf, gd, 128, E.s, D.L, (const float*)h->z, (const float*)h->r, part);
+    launch2(k_vdot_final, dim3(1), 32, E.s, D.L.nl, (const float*)part, h->st, 0);
     E.pe();
     if (E.prof) E.pb("L0 pcg x,p update");
     launch2(k_vpcg_update_p, g, 128, E.s, D.L, (const float*)h->z, h->p, h->x, (const PcgState*)h->st);
     E.pe();
-    if (E.prof) E.pb("L0 pcg Ap+dot");
-    launch2(k_vpcg_Ap, g, 128, E.s, D.L, (const float*)h->p, h->q, h->partials, h->st);
+    if (E.prof) E.pb("L0 pcg Ap");
+    launch2(k_vpcg_Ap, g, 128, E.s, D.L, (const float*)h->p, h->q);
+    E.pe();
+    if (E.prof) E.pb("L0 pcg sigma (p.q)");
+    launch2(k_vdot_leaf, gd, 128, E.s, D.L, (const float*)h->p, (const float*)h->q, part);
+    launch2(k_vdot_final, dim3(1), 32, E.s, D.L.nl, (const float*)part, h->st, 1);
     E.pe();
     if (E.prof) E.pb("L0 pcg r update+absmax");
     launch2(k_vpcg_update_r, g, 128, E.s, D.L, (const float*)h->q, h->r, h->partials, h->st, cond, use_cond);
     E.pe();
-    E.count += 4;
+    E.count += 7;
 }
 static void venqueue_finish(VEnq& E) {
     uaamg_viscosity* h = E.h;

@@ -329,9 +329,15 @@ __global__ void __launch_bounds__(128) k_vcoef0(VLevel L, const int* org, VolFie
             }
             val[VA_DIAG] = diag;
             val[VA_INV] = diag != 0.f ? __fdiv_rn(1.0f, diag) : 0.f;
-            val[VA_NEGX + d0] = negv[0];
-            val[VA_NEGX + d1] = negv[1];
-            val[VA_NEGX + d2] = negv[2];
+            // negv[k] is the entry along axis d_k; store by absolute axis with
+            // static indices only
+            if (c == 0) {
+                val[VA_NEGX] = negv[0]; val[VA_NEGY] = negv[1]; val[VA_NEGZ] = negv[2];
+            } else if (c == 1) {
+                val[VA_NEGY] = negv[0]; val[VA_NEGZ] = negv[1]; val[VA_NEGX] = negv[2];
+            } else {
+                val[VA_NEGZ] = negv[0]; val[VA_NEGX] = negv[1]; val[VA_NEGY] = negv[2];
+            }
         } else {
             val[VA_DIAG] = ddiag;  // setValueOff keeps the default
             val[VA_INV] = 0.f;
@@ -421,18 +427,26 @@ __global__ void __launch_bounds__(128) k_vcoarse_coef(VLevel F, VLevel C, float*
             }
             val[VA_DIAG] = __fmul_rn(rap, nd);
             val[VA_INV] = nd != 0.f ? __fdiv_rn(1.0f, __fmul_rn(rap, nd)) : 0.f;
+            float ng[3];  // along d_k
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 int l[3] = {X, Y, lz};
                 l[d[k]] -= 1;
-                val[VA_NEGX + d[k]] = vdof_at(C, nbrow, c, l[0], l[1], l[2]) ? __fmul_rn(rap, nn[k]) : 0.f;
+                ng[k] = vdof_at(C, nbrow, c, l[0], l[1], l[2]) ? __fmul_rn(rap, nn[k]) : 0.f;
+            }
+            if (c == 0) {
+                val[VA_NEGX] = ng[0]; val[VA_NEGY] = ng[1]; val[VA_NEGZ] = ng[2];
+            } else if (c == 1) {
+                val[VA_NEGY] = ng[0]; val[VA_NEGZ] = ng[1]; val[VA_NEGX] = ng[2];
+            } else {
+                val[VA_NEGZ] = ng[0]; val[VA_NEGX] = ng[1]; val[VA_NEGY] = ng[2];
             }
         } else {
             val[VA_DIAG] = val[VA_INV] = 0.f;
             val[VA_NEGX] = val[VA_NEGY] = val[VA_NEGZ] = 0.f;
         }
-#pragma unroll 1
-        for (int tt = 0; tt < 4; ++tt) {
+#pragma unroll
+        for (int tt = 0; tt < 4; ++tt) {  // unrolled: val[] takes static indices only
             float s = 0.f;
             if (fl >= 0) {
                 const float* T0 = F.coef + (long long)(c * VNA + VA_T00) * F.nl * UAAMG_LEAF + (long long)fl * UAAMG_LEAF;

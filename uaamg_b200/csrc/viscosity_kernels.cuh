@@ -385,30 +385,73 @@ __global__ void __launch_bounds__(128) k_vpcg_init(VLevel L, const float* x, con
     }
 }
 
-// line 13 tail: rho_new = z.r; first iteration: rho = rho_new (line 4),
-// later: beta = rho_new / rho, rho = rho_new (lines 14-15)
-__global__ void __launch_bounds__(128) k_vpcg_rho(VLevel L, const float* z, const float* r, double* partials,
-                                                  PcgState* st) {
+// lv_dot (:3769-3780) with grid_dot_op (openvdb_grid_math_op.h:45-75): float
+// accumulation of a*b over the DOF voxels of a leaf in offset order, then of
+// the leaf partials in leaf order per channel, then of the three channel
+// sums.  (TBB may split the reference's sum anywhere; this is the serial
+// schedule, so the PCG follows the reference's float rounding.)
+// Stage 1: one warp per (channel, leaf) item; lane 0 adds the products in order.
+__global__ void __launch_bounds__(128) k_vdot_leaf(VLevel L, const float* a, const float* b, float* part) {
     griddep_wait();
     griddep_launch();
-    __shared__ double shd[4];
-    __shared__ bool last;
-    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
-    const long long i = (long long)c * L.nl * UAAMG_LEAF4 + (long long)leaf * UAAMG_LEAF4 + t;
-    const float4 zz = reinterpret_cast<const float4*>(z)[i], rr = reinterpret_cast<const float4*>(r)[i];
-    const double s = ((double)zz.x * rr.x + (double)zz.y * rr.y) + ((double)zz.z * rr.z + (double)zz.w * rr.w);
-    const double part = block_sum128(s, shd);
-    if (vpublish(part, partials, &st->ticket[2], &last)) {
-        const double tot = vgather_sum(partials, shd);
-        if (t == 0) {
-            const float rho_new = (float)tot;
-            if (st->first) {
-                st->beta = 0.f;
-            } else {
-                st->beta = __fdiv_rn(rho_new, st->rho);
+    __shared__ float prod[4][UAAMG_LEAF];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long item = (long long)blockIdx.x * 4 + w;  // c * nl + leaf
+    if (item >= 3LL * L.nl) return;
+    const float* pa = a + item * UAAMG_LEAF;
+    const float* pb = b + item * UAAMG_LEAF;
+    const uint64_t* m = L.dof + item * 8;
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) any |= (m[q] != 0ull);
+    if (!any) {
+        if (lane == 0) part[item] = 0.f;
+        return;
+    }
+#pragma unroll 4
+    for (int k = lane; k < UAAMG_LEAF; k += 32) prod[w][k] = __fmul_rn(pa[k], pb[k]);
+    __syncwarp();
+    if (lane == 0) {
+        float acc = 0.f;
+        for (int q = 0; q < 8; ++q) {
+            uint64_t word = m[q];
+            while (word) {
+                const int bit = __ffsll((long long)word) - 1;
+                acc = __fadd_rn(acc, prod[w][q * 64 + bit]);
+                word &= word - 1;
             }
-            st->rho = rho_new;
-            st->ticket[2] = 0;
+        }
+        part[item] = acc;
+    }
+}
+// Stage 2 (one block): per-channel sums in leaf order, then the PCG scalar.
+// which = 0: rho_new = z.r (line 13; first iteration: rho = rho_new, beta = 0,
+// later beta = rho_new / rho, rho = rho_new); which = 1: sigma = p.q,
+// alpha = rho / sigma (lines 6-7).
+__global__ void __launch_bounds__(32) k_vdot_final(int nl, const float* part, PcgState* st, int which) {
+    griddep_wait();
+    griddep_launch();
+    __shared__ float cs[3];
+    const int t = threadIdx.x;
+    if (t < 3) {
+        const float* p = part + (long long)t * nl;
+        float acc = 0.f;
+        for (int i = 0; i < nl; ++i) acc = __fadd_rn(acc, p[i]);
+        cs[t] = acc;
+    }
+    __syncthreads();
+    if (t == 0) {
+        float r = 0.f;
+        r = __fadd_rn(r, cs[0]);
+        r = __fadd_rn(r, cs[1]);
+        r = __fadd_rn(r, cs[2]);
+        if (which == 0) {
+            st->beta = st->first ? 0.f : __fdiv_rn(r, st->rho);
+            st->rho = r;
+        } else {
+            st->sigma = r;
+            st->alpha = __fdiv_rn(st->rho, r);
+            st->first = 0;
         }
     }
 }
@@ -438,32 +481,16 @@ __global__ void __launch_bounds__(128) k_vpcg_update_p(VLevel L, const float* z,
     reinterpret_cast<float4*>(p)[i] = pp;
 }
 
-// lines 6-7: q = A p; sigma = p.q; alpha = rho / sigma
-__global__ void __launch_bounds__(128) k_vpcg_Ap(VLevel L, const float* p, float* q, double* partials, PcgState* st) {
+// line 6: q = A p (sigma and alpha follow in k_vdot_leaf / k_vdot_final)
+__global__ void __launch_bounds__(128) k_vpcg_Ap(VLevel L, const float* p, float* q) {
     griddep_wait();
     griddep_launch();
-    __shared__ double shd[4];
-    __shared__ bool last;
     const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
     const unsigned m = vmask4(L, c, leaf, t);
-    double s = 0.0;
-    if (m) {
-        float4 xc;
-        const float4 res = vapply_value<VM_NORMAL>(L, c, leaf, t, p, nullptr, 1.f, m, xc);
-        reinterpret_cast<float4*>(q + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
-        s = ((double)xc.x * res.x + (double)xc.y * res.y) + ((double)xc.z * res.z + (double)xc.w * res.w);
-    }
-    const double part = block_sum128(s, shd);
-    if (vpublish(part, partials, &st->ticket[3], &last)) {
-        const double tot = vgather_sum(partials, shd);
-        if (t == 0) {
-            const float sigma = (float)tot;
-            st->sigma = sigma;
-            st->alpha = __fdiv_rn(st->rho, sigma);
-            st->first = 0;
-            st->ticket[3] = 0;
-        }
-    }
+    if (!m) return;
+    float4 xc;
+    const float4 res = vapply_value<VM_NORMAL>(L, c, leaf, t, p, nullptr, 1.f, m, xc);
+    reinterpret_cast<float4*>(q + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
 }
 
 // lines 8-9: r -= alpha q; nu = |r|_inf; stop when nu <= numax or at the

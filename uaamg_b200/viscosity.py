@@ -52,7 +52,10 @@ class L_with_level:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            _lib.lib().uaamg_viscosity_destroy(h)
+            try:
+                _lib.lib().uaamg_viscosity_destroy(h)
+            except Exception:  # interpreter shutdown: module globals already gone
+                pass
             self._h = None
 
     # --- sizes and topology
