@@ -1,17 +1,23 @@
 #!/usr/bin/env python
-"""UAAMG-PCG benchmark: ms per pressure solve on the plain Poisson workload.
+"""UAAMG-PCG benchmark: ms per solve.
 
-Workload (one "step" = one solve, as in FLIP_vdb's solve_pressure_simd,
-FLIP_vdb.cpp:3118-3168): 128^3 voxels, dx = 1/128, liquid = {y < 0.4} U
-sphere(r 0.15 at (0.5, 0.7, 0.5)), walls solid, face velocities U[-1,1]
-(seed 0), dt = 1; build the level-0 matrix and the multigrid hierarchy, build
-the right-hand side, and run UAAMG-PCG to 1e-7 relative inf-norm residual.
+Headline workload (one "step" = one viscosity solve as at FLIP_vdb's call site,
+FLIP_vdb.cpp:3170-3208): the 128^3 domain, dx = 1/128, liquid = {y < 0.4} U
+sphere(r 0.15 at (0.5, 0.7, 0.5)), domain walls solid, face velocities
+U[-1,1] (seed 1), constant viscosity 1e3, dt = 1/240, rho = 1; build the
+level-0 viscosity matrix and the multigrid hierarchy, the right-hand side and
+the warm start (velocity at the DOFs), and run UAAMG-PCG to 1e-6 relative
+inf-norm residual (simd_viscosity3d::pcg_solve).
+
+Secondary (the "poisson" object of the same line): the plain pressure Poisson
+solve on the same geometry (face velocities seed 0, dt = 1) to 1e-7, as at
+FLIP_vdb.cpp:3118-3168.
 
   value      device-resident inputs (torch CUDA tensors) through the C ABI
   e2e        the same step through the host-pointer C ABI from pinned host
              memory, host<->device copies inside the timed region
   cpu_baseline / --impl reference
-             the CPU restatement of the reference's SIMD solver (oracle/),
+             the CPU restatement of the reference's SIMD solvers (oracle/),
              OpenMP over all host cores, on a bounded sample of solves
 
 Multi-GPU: every rank solves its own independent instances (replicas; no
@@ -35,7 +41,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "UAAMG-PCG ms/solve to 1e-7 rel-res (plain vs batched/mixed), p99 served latency"
 UNIT = "ms/solve"
-WORKLOAD = "plain pressure Poisson 128^3, liquid y<0.4 + sphere r0.15, walls solid, U[-1,1] face velocities seed 0"
+WORKLOAD = ("plain variational viscosity 128^3, liquid y<0.4 + sphere r0.15, walls solid, U[-1,1] face velocities "
+            "seed 1, mu 1e3, dt 1/240, rho 1, rel-res 1e-6, warm start = velocity")
+POISSON_WORKLOAD = "plain pressure Poisson 128^3, liquid y<0.4 + sphere r0.15, walls solid, U[-1,1] face velocities seed 0"
 
 
 def _peaks():
@@ -122,8 +130,12 @@ def _dist():
     return rank, ws, local, dist
 
 
+def _threads() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
 def cpu_solve_once(sc, threads: int):
-    """One full solve with the CPU restatement (build + rhs + PCG); seconds."""
+    """One full Poisson solve with the CPU restatement (build + rhs + PCG); seconds."""
     from oracle.oracle import OraclePoisson, set_threads
     set_threads(threads)
     t0 = time.perf_counter()
@@ -134,18 +146,48 @@ def cpu_solve_once(sc, threads: int):
     return dt, it, st
 
 
-def cpu_baseline(sc, budget_s: float = 12.0, min_samples: int = 3, max_samples: int = 30):
-    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    cpu_solve_once(sc, threads)  # warm-up
+def _visc_warm_start(o, sc):
+    """The velocity at every DOF (FLIP_vdb.cpp:3188-3198), from the oracle's topology."""
+    org, _ = o.topology(0)
+    idx = o.dof_index(0)
+    out = o.zeros(0)
+    for c, g in enumerate((sc.u, sc.v, sc.w)):
+        lut = {tuple(x): i for i, x in enumerate(g.origins)}
+        for li in range(org.shape[0]):
+            j = lut.get(tuple(org[li]))
+            if j is None:
+                continue
+            m = idx[c, li] >= 0
+            out[c, li, m] = g.values[j].reshape(512)[m]
+    return out
+
+
+def cpu_visc_solve_once(sc, threads: int):
+    """One full viscosity solve with the CPU restatement (build + rhs + warm
+    start + PCG); seconds."""
+    from oracle.oracle import OracleViscosity, set_threads
+    set_threads(threads)
+    t0 = time.perf_counter()
+    o = OracleViscosity(sc.liquid_phi, sc.solid_phi, sc.viscosity, sc.dt, sc.rho, sc.dx)
+    rhs = o.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+    x0 = _visc_warm_start(o, sc)
+    x, st, it, _ = o.solve_pcg(x0, rhs, 1e-6, 100)
+    dt = time.perf_counter() - t0
+    return dt, it, st
+
+
+def cpu_baseline(fn, sc, what: str, budget_s: float = 12.0, min_samples: int = 3, max_samples: int = 30):
+    threads = _threads()
+    fn(sc, threads)  # warm-up
     times, iters = [], []
     t0 = time.perf_counter()
     while len(times) < max_samples and (len(times) < min_samples or time.perf_counter() - t0 < budget_s):
-        dt, it, _ = cpu_solve_once(sc, threads)
+        dt, it, _ = fn(sc, threads)
         times.append(dt)
         iters.append(it)
     return {"value": round(statistics.median(times) * 1e3, 3), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{len(times)} full solves (build+rhs+PCG) of the same 128^3 workload, median; "
-                      f"oracle/poisson_oracle.c, OpenMP, {threads} threads; iterations {iters[0]}"}
+            "sample": f"{len(times)} full solves of the same 128^3 workload, median; {what}, OpenMP, "
+                      f"{threads} threads; iterations {iters[0]}"}
 
 
 def run_reference(args, rank, ws):
@@ -153,13 +195,13 @@ def run_reference(args, rank, ws):
     if rank != 0:
         return
     from uaamg_b200 import scenes
-    sc = scenes.plain_poisson_scene(n=args.n, seed=0)
-    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    sc = scenes.plain_viscosity_scene(n=args.n, seed=1)
+    threads = _threads()
     for _ in range(args.warmup):
-        cpu_solve_once(sc, threads)
+        cpu_visc_solve_once(sc, threads)
     times, iters = [], []
     for _ in range(args.steps):
-        dt, it, _ = cpu_solve_once(sc, threads)
+        dt, it, _ = cpu_visc_solve_once(sc, threads)
         times.append(dt)
         iters.append(it)
     ms = sum(times) / len(times) * 1e3
@@ -168,8 +210,8 @@ def run_reference(args, rank, ws):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "n": args.n, "iterations": iters[0]},
             "cpu_baseline": {"value": round(ms, 3), "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} full solves (build+rhs+PCG), mean; CPU restatement "
-                                       f"oracle/poisson_oracle.c (the reference needs OpenVDB/TBB/Eigen, absent)"},
+                             "sample": f"{args.steps} full solves (build+rhs+warm start+PCG), mean; CPU restatement "
+                                       f"oracle/viscosity_oracle.c (the reference needs OpenVDB/TBB/Eigen, absent)"},
             "e2e": {"value": round(ms, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -184,6 +226,33 @@ def _pinned(a: np.ndarray):
     return t
 
 
+def _grid_bytes(*gs) -> int:
+    return int(sum(_gbytes(g) + (g.masks.nbytes if g.masks is not None else 0) for g in gs))
+
+
+# algorithmic bytes of one pass per DOF it updates (canonical model: every array
+# read or written once at 4 B, halos excluded): GS colour pass of one channel =
+# half of the 44 B two-colour channel sweep; residual 44 B and A.x 40 B per
+# channel DOF; restriction 4.5 B and prolong-add 8.5 B per fine DOF
+def _visc_pass_bytes(label: str, ndof_level: list[int], ndof_c: list[list[int]]) -> float | None:
+    parts = label.split()
+    if not parts or not parts[0].startswith("L") or not parts[0][1:].isdigit():
+        return None
+    lv = int(parts[0][1:])
+    if len(parts) >= 3 and parts[1] in ("red_gs", "black_gs"):
+        c = int(parts[2][1:])
+        return 22.0 * ndof_c[lv][c]
+    if parts[1] == "residual":
+        return 44.0 * ndof_level[lv]
+    if parts[1] == "normal":
+        return 40.0 * ndof_level[lv]
+    if parts[1] == "restrict":
+        return 4.5 * ndof_level[lv]
+    if parts[1] == "prolong":
+        return 8.5 * ndof_level[lv]
+    return None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -192,10 +261,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-poisson", action="store_true", help="skip the secondary Poisson measurement")
     ap.add_argument("--no-graph", action="store_true", help="host-driven PCG loop instead of the CUDA graph")
-    ap.add_argument("--profile", choices=["solve", "sweep"], default=None,
-                    help="short fixed sequence for ncu: 'solve' = build + 2 graph solves, "
-                         "'sweep' = build + 3 level-0 Jacobi sweeps")
+    ap.add_argument("--profile", choices=["solve", "sweep", "vsolve"], default=None,
+                    help="short fixed sequence for ncu: 'vsolve' = viscosity build + 2 solves, "
+                         "'solve' = Poisson build + 2 graph solves, 'sweep' = Poisson build + 3 level-0 sweeps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -213,8 +283,8 @@ def main():
     from uaamg_b200 import scenes
     from uaamg_b200.grids import LeafGrid
     from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver
+    from uaamg_b200.viscosity import L_with_level, simd_viscosity3d
 
-    sc = scenes.plain_poisson_scene(n=args.n, seed=0)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
 
@@ -230,12 +300,33 @@ def main():
         d._pin = t
         return d
 
-    dgr = {k: on_device(getattr(sc, k)) for k in ("phi", "face_weights", "vx", "vy", "vz", "solid_velocity")}
+    vsc = scenes.plain_viscosity_scene(n=args.n, seed=1)
+    vkeys = ("liquid_phi", "solid_phi", "viscosity", "u", "v", "w", "solid_velocity")
+    vdg = {k: on_device(getattr(vsc, k)) for k in vkeys}
+
+    if args.profile == "vsolve":
+        lv = L_with_level.create_viscosity_matrix(vdg["viscosity"], vdg["liquid_phi"], vdg["solid_phi"], vsc.dt,
+                                                  vsc.rho, vsc.dx)
+        rhs = torch.empty((3, lv.leaf_count(0), 512), dtype=torch.float32, device=dev)
+        lv.build_rhs(vdg["u"], vdg["v"], vdg["w"], vdg["solid_velocity"], out=rhs)
+        x0 = torch.empty_like(rhs)
+        lv.gather_velocity(vdg["u"], vdg["v"], vdg["w"], out=x0)
+        s = simd_viscosity3d(lv)
+        s.use_graph = 0 if args.no_graph else 1
+        for _ in range(2):
+            x = x0.clone()
+            st = s.pcg_solve(x, 1e-6, rhs)
+        print(json.dumps({"profile": "vsolve", "status": st, "iterations": s.m_iteration}))
+        return
+
+    psc = scenes.plain_poisson_scene(n=args.n, seed=0)
+    pkeys = ("phi", "face_weights", "vx", "vy", "vz", "solid_velocity")
+    pdg = {k: on_device(getattr(psc, k)) for k in pkeys}
     if args.profile:
-        lap = LaplacianWithLevel.createPressurePoissonLaplacian(dgr["phi"], dgr["face_weights"], sc.dt, sc.dx)
+        lap = LaplacianWithLevel.createPressurePoissonLaplacian(pdg["phi"], pdg["face_weights"], psc.dt, psc.dx)
         rhs = torch.empty((lap.leaf_count(0), 512), dtype=torch.float32, device=dev)
-        lap.createPressurePoissonRightHandSide(dgr["face_weights"], dgr["vx"], dgr["vy"], dgr["vz"],
-                                              dgr["solid_velocity"], sc.dt, out=rhs)
+        lap.createPressurePoissonRightHandSide(pdg["face_weights"], pdg["vx"], pdg["vy"], pdg["vz"],
+                                              pdg["solid_velocity"], psc.dt, out=rhs)
         if args.profile == "solve":
             solver = PoissonSolver(lap)
             solver.use_graph = not args.no_graph
@@ -250,46 +341,10 @@ def main():
                 x = lap.apply(0, "jacobi", x, b, weight=0.8571)
             print(json.dumps({"profile": "sweep", "leaves": lap.leaf_count(0)}))
         return
-    hgr = {k: pinned(getattr(sc, k)) for k in ("phi", "face_weights", "vx", "vy", "vz", "solid_velocity")}
+
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    stats = {"launches": 0, "iters": [], "status": []}
-
-    def step_device():
-        lap = LaplacianWithLevel.createPressurePoissonLaplacian(dgr["phi"], dgr["face_weights"], sc.dt, sc.dx)
-        solver = PoissonSolver(lap)
-        solver.set_stream(stream.cuda_stream)
-        rhs = torch.empty((lap.leaf_count(0), 512), dtype=torch.float32, device=dev)
-        lap.createPressurePoissonRightHandSide(dgr["face_weights"], dgr["vx"], dgr["vy"], dgr["vz"],
-                                              dgr["solid_velocity"], sc.dt, out=rhs)
-        p = torch.zeros_like(rhs)
-        st = solver.solveMultigridPCG(p, rhs)
-        stats["launches"] += solver.kernel_launches
-        stats["iters"].append(solver.mIterationTaken)
-        stats["status"].append(st)
-        return lap, p
-
-    host_p = {}
-
-    def step_host():
-        lap = LaplacianWithLevel.createPressurePoissonLaplacian(hgr["phi"], hgr["face_weights"], sc.dt, sc.dx)
-        solver = PoissonSolver(lap)
-        n = lap.leaf_count(0)
-        if "rhs" not in host_p or host_p["rhs"].shape[0] != n:
-            host_p["rhs_t"] = torch.empty((n, 512), dtype=torch.float32).pin_memory()
-            host_p["p_t"] = torch.empty((n, 512), dtype=torch.float32).pin_memory()
-            host_p["rhs"] = host_p["rhs_t"].numpy()
-            host_p["p"] = host_p["p_t"].numpy()
-        lap.createPressurePoissonRightHandSide(hgr["face_weights"], hgr["vx"], hgr["vy"], hgr["vz"],
-                                              hgr["solid_velocity"], sc.dt, out=host_p["rhs"])
-        host_p["p"][:] = 0.0
-        st = solver.solveMultigridPCG(host_p["p"], host_p["rhs"])
-        stats["launches"] += solver.kernel_launches
-        return lap, st
-
-    def timed(fn, steps, warmup):
-        for _ in range(warmup):
-            fn()
+    def timed(fn, steps):
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
@@ -308,95 +363,194 @@ def main():
             dist.barrier()
         return total
 
-    # ---- headline: device-resident inputs
-    clk = ClockSampler(local)
-    stats.update(launches=0, iters=[], status=[])
-    for _ in range(args.warmup):
-        step_device()
-    stats.update(launches=0, iters=[], status=[])
-    clk.start()
-    t_dev = timed(step_device, args.steps, 0)
-    clocks = clk.stop()
-    launches = stats["launches"]
-    iters = list(stats["iters"])
-    statuses = list(stats["status"])
-    # ---- e2e through the host-pointer C ABI
-    for _ in range(args.warmup):
-        step_host()
-    t_host = timed(step_host, args.steps, 0)
-
-    if dist is not None:
-        tt = torch.tensor([t_dev, t_host], dtype=torch.float64, device=dev)
+    def max_over_ranks(*vals):
+        if dist is None:
+            return vals
+        tt = torch.tensor(vals, dtype=torch.float64, device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev, t_host = float(tt[0]), float(tt[1])
-    total_solves = args.steps * ws
-    value = t_dev / total_solves
-    e2e = t_host / total_solves
+        return tuple(float(v) for v in tt)
 
-    # ---- per-kernel device times (event pairs, host-driven loop) for the roofline
-    lap, p = step_device()
-    solver = PoissonSolver(lap)
-    solver.set_stream(stream.cuda_stream)
-    rhs = torch.empty((lap.leaf_count(0), 512), dtype=torch.float32, device=dev)
-    lap.createPressurePoissonRightHandSide(dgr["face_weights"], dgr["vx"], dgr["vy"], dgr["vz"],
-                                          dgr["solid_velocity"], sc.dt, out=rhs)
-    prof = solver.profile_pcg(torch.zeros_like(rhs), rhs)
-    levels = lap.num_levels()
-    vec_bytes = 4 * 512 * lap.leaf_count(0)
-    ndof = [lap.num_dof(l) for l in range(levels)]
-    # algorithmic bytes of a level-0 Jacobi sweep: x, b, out for every DOF plus
-    # diag, 1/diag, c_x, c_y, c_z for DOF in leaves whose array is stored
-    # (trimmed leaves hold the default and are not read), 4 B each
-    (diag, cx, cy, cz), flags = lap.coefficients(0)
-    _, masks = lap.dof_topology(0)
-    from uaamg_b200.grids import unpack_masks
-    per_leaf = unpack_masks(masks).sum(axis=1)
-    stored = lambda bit: int(per_leaf[(flags & bit) == 0].sum())
-    jac_bytes = 4 * (3 * ndof[0] + 2 * stored(1) + stored(2) + stored(4) + stored(8))
-    # the level-0 plain Jacobi sweep (staged or not); the fused variants move
-    # the same bytes plus small extras and are reported in kernel_profile_ms
-    tags = [k for k in prof if k.startswith("L0 jacobi") and "+" not in k]
-    tag = tags[0] if tags else "L0 jacobi"
-    t_ms, cnt = prof.get(tag, (0.0, 0))
-    achieved = jac_bytes / (t_ms / cnt * 1e-3) / 1e9 if cnt else None
-    peak, peak_kind = _peaks()
-    traffic = _traffic_from_profile("k_sweep_staged<0>")
+    # ================= headline: variational viscosity =================
+    vstats = {"launches": 0, "iters": [], "status": []}
+
+    def vstep_device():
+        lv = L_with_level.create_viscosity_matrix(vdg["viscosity"], vdg["liquid_phi"], vdg["solid_phi"], vsc.dt,
+                                                  vsc.rho, vsc.dx)
+        lv.set_stream(stream.cuda_stream)
+        n = lv.leaf_count(0)
+        rhs = torch.empty((3, n, 512), dtype=torch.float32, device=dev)
+        lv.build_rhs(vdg["u"], vdg["v"], vdg["w"], vdg["solid_velocity"], out=rhs)
+        x = torch.empty_like(rhs)
+        lv.gather_velocity(vdg["u"], vdg["v"], vdg["w"], out=x)
+        s = simd_viscosity3d(lv)
+        st = s.pcg_solve(x, 1e-6, rhs)
+        vstats["launches"] += s.kernel_launches
+        vstats["iters"].append(s.m_iteration)
+        vstats["status"].append(st)
+        return lv, x
+
+    vhg = {k: pinned(getattr(vsc, k)) for k in vkeys}
+    vhost = {}
+
+    def vstep_host():
+        lv = L_with_level.create_viscosity_matrix(vhg["viscosity"], vhg["liquid_phi"], vhg["solid_phi"], vsc.dt,
+                                                  vsc.rho, vsc.dx)
+        n = lv.leaf_count(0)
+        if vhost.get("n") != n:
+            vhost["rhs_t"] = torch.empty((3, n, 512), dtype=torch.float32).pin_memory()
+            vhost["x_t"] = torch.empty((3, n, 512), dtype=torch.float32).pin_memory()
+            vhost["rhs"], vhost["x"], vhost["n"] = vhost["rhs_t"].numpy(), vhost["x_t"].numpy(), n
+        lv.build_rhs(vhg["u"], vhg["v"], vhg["w"], vhg["solid_velocity"], out=vhost["rhs"])
+        lv.gather_velocity(vhg["u"], vhg["v"], vhg["w"], out=vhost["x"])
+        s = simd_viscosity3d(lv)
+        st = s.pcg_solve(vhost["x"], 1e-6, vhost["rhs"])
+        vstats["launches"] += s.kernel_launches
+        return lv, st
+
+    for _ in range(args.warmup):
+        vstep_device()
+    vstats.update(launches=0, iters=[], status=[])
+    clk = ClockSampler(local)
+    clk.start()
+    t_dev = timed(vstep_device, args.steps)
+    clocks = clk.stop()
+    launches = vstats["launches"]
+    viters, vstatus = list(vstats["iters"]), list(vstats["status"])
+    for _ in range(args.warmup):
+        vstep_host()
+    t_host = timed(vstep_host, args.steps)
+    t_dev, t_host = max_over_ranks(t_dev, t_host)
+    total = args.steps * ws
+    value, e2e = t_dev / total, t_host / total
+
+    # per-kernel device times (event pairs, host-driven loop) for the roofline
+    lv, _ = vstep_device()
+    n0 = lv.leaf_count(0)
+    rhs = torch.empty((3, n0, 512), dtype=torch.float32, device=dev)
+    lv.build_rhs(vdg["u"], vdg["v"], vdg["w"], vdg["solid_velocity"], out=rhs)
+    x0 = torch.empty_like(rhs)
+    lv.gather_velocity(vdg["u"], vdg["v"], vdg["w"], out=x0)
+    s = simd_viscosity3d(lv)
+    prof = s.profile_pcg(x0.clone(), rhs, 1e-6)
+    levels = lv.num_levels()
+    ndof = [lv.num_dof(l) for l in range(levels)]
+    ndof_c = []
+    for l in range(levels):
+        _, m = lv.topology(l)
+        ndof_c.append([int(sum(bin(int(w)).count("1") for w in m[c].reshape(-1))) for c in range(3)])
     dominant = max(prof.items(), key=lambda kv: kv[1][0])
-    cpu = None
+    dom_bytes = _visc_pass_bytes(dominant[0], ndof, ndof_c)
+    # the level-0 red-black passes: the bandwidth-heavy kernels of the cycle
+    l0 = [(k, v) for k, v in prof.items() if k.startswith("L0 red_gs") or k.startswith("L0 black_gs")]
+    l0_bytes = sum(_visc_pass_bytes(k, ndof, ndof_c) * v[1] for k, v in l0)
+    l0_ms = sum(v[0] for k, v in l0)
+    peak, peak_kind = _peaks()
+    t_ms, cnt = dominant[1]
+    achieved = dom_bytes / (t_ms / cnt * 1e-3) / 1e9 if (dom_bytes and cnt) else None
+    traffic = _traffic_from_profile("k_vapply<3>")
+    vec_bytes = 3 * 4 * 512 * n0
+    vcpu = None
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
-        cpu = cpu_baseline(sc)
+        vcpu = cpu_baseline(cpu_visc_solve_once, vsc, "oracle/viscosity_oracle.c (build+rhs+warm start+PCG)",
+                            budget_s=20.0, min_samples=2, max_samples=10)
+
+    # ================= secondary: plain pressure Poisson =================
+    poisson = None
+    if not args.no_poisson:
+        pstats = {"launches": 0, "iters": [], "status": []}
+
+        def pstep_device():
+            lap = LaplacianWithLevel.createPressurePoissonLaplacian(pdg["phi"], pdg["face_weights"], psc.dt, psc.dx)
+            solver = PoissonSolver(lap)
+            solver.set_stream(stream.cuda_stream)
+            rhs = torch.empty((lap.leaf_count(0), 512), dtype=torch.float32, device=dev)
+            lap.createPressurePoissonRightHandSide(pdg["face_weights"], pdg["vx"], pdg["vy"], pdg["vz"],
+                                                  pdg["solid_velocity"], psc.dt, out=rhs)
+            p = torch.zeros_like(rhs)
+            st = solver.solveMultigridPCG(p, rhs)
+            pstats["launches"] += solver.kernel_launches
+            pstats["iters"].append(solver.mIterationTaken)
+            pstats["status"].append(st)
+            return lap
+
+        phg = {k: pinned(getattr(psc, k)) for k in pkeys}
+        phost = {}
+
+        def pstep_host():
+            lap = LaplacianWithLevel.createPressurePoissonLaplacian(phg["phi"], phg["face_weights"], psc.dt, psc.dx)
+            solver = PoissonSolver(lap)
+            n = lap.leaf_count(0)
+            if phost.get("n") != n:
+                phost["rhs_t"] = torch.empty((n, 512), dtype=torch.float32).pin_memory()
+                phost["p_t"] = torch.empty((n, 512), dtype=torch.float32).pin_memory()
+                phost["rhs"], phost["p"], phost["n"] = phost["rhs_t"].numpy(), phost["p_t"].numpy(), n
+            lap.createPressurePoissonRightHandSide(phg["face_weights"], phg["vx"], phg["vy"], phg["vz"],
+                                                  phg["solid_velocity"], psc.dt, out=phost["rhs"])
+            phost["p"][:] = 0.0
+            st = solver.solveMultigridPCG(phost["p"], phost["rhs"])
+            pstats["launches"] += solver.kernel_launches
+            return lap, st
+
+        for _ in range(args.warmup):
+            pstep_device()
+        pstats.update(launches=0, iters=[], status=[])
+        tp_dev = timed(pstep_device, args.steps)
+        plaunch = pstats["launches"]
+        piters, pstatus = list(pstats["iters"]), list(pstats["status"])
+        for _ in range(args.warmup):
+            pstep_host()
+        tp_host = timed(pstep_host, args.steps)
+        tp_dev, tp_host = max_over_ranks(tp_dev, tp_host)
+        lap = pstep_device()
+        pvec = 4 * 512 * lap.leaf_count(0)
+        pndof = [lap.num_dof(l) for l in range(lap.num_levels())]
+        poisson = {"workload": POISSON_WORKLOAD, "value": round(tp_dev / total, 4), "unit": UNIT,
+                   "e2e": {"value": round(tp_host / total, 4), "unit": UNIT,
+                           "h2d_bytes_per_step": int(_grid_bytes(psc.phi, psc.face_weights, psc.face_weights, psc.vx,
+                                                                 psc.vy, psc.vz) + 2 * pvec),
+                           "d2h_bytes_per_step": int(2 * pvec)},
+                   "ndof": pndof, "pcg_iterations": piters[0],
+                   "status": "SUCCESS" if all(x == 0 for x in pstatus) else "FAILED",
+                   "gpu_launches": int(plaunch)}
+        launches += plaunch
+        if rank == 0 and not args.no_cpu_baseline and ws == 1:
+            poisson["cpu_baseline"] = cpu_baseline(cpu_solve_once, psc, "oracle/poisson_oracle.c (build+rhs+PCG)")
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t_dev / args.steps, 4), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": args.n, "ndof": ndof, "levels": levels,
-                       "pcg_iterations": iters[0], "status": "SUCCESS" if all(s == 0 for s in statuses) else "FAILED",
-                       "step": "create matrix+hierarchy, rhs, UAAMG-PCG (device-resident inputs)",
+            "config": {"workload": WORKLOAD, "n": args.n, "ndof": ndof, "ndof_per_channel_l0": ndof_c[0],
+                       "levels": levels, "pcg_iterations": viters[0],
+                       "status": "SUCCESS" if all(x == 0 for x in vstatus) else "FAILED",
+                       "step": "create viscosity matrix+hierarchy, rhs, warm start, UAAMG-PCG "
+                               "(device-resident inputs)",
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"replicas x{ws}", "solves_per_s": round(1e3 / value, 2),
-                       "voxel_updates_per_s": round(ndof[0] * iters[0] * 1e3 / value, 1)},
+                       "dof_updates_per_s": round(ndof[0] * (viters[0] + 1) * 1e3 / value, 1)},
             "e2e": {"value": round(e2e, 4), "unit": UNIT,
-                    # create: phi (+mask) and face weights; rhs: face weights and
-                    # three velocity channels; solve: pressure guess and rhs
-                    "h2d_bytes_per_step": int(_gbytes(sc.phi) + sc.phi.masks.nbytes + 2 * _gbytes(sc.face_weights)
-                                              + sum(_gbytes(getattr(sc, k)) for k in ("vx", "vy", "vz"))
-                                              + 2 * vec_bytes),
-                    # rhs returned to the caller, solved pressure
-                    "d2h_bytes_per_step": int(2 * vec_bytes)},
+                    # create: viscosity, liquid SDF (+mask), solid SDF; rhs and warm
+                    # start: three velocity channels each; solve: x and rhs
+                    "h2d_bytes_per_step": int(_grid_bytes(vsc.viscosity, vsc.liquid_phi, vsc.solid_phi)
+                                              + 2 * _grid_bytes(vsc.u, vsc.v, vsc.w) + 2 * vec_bytes),
+                    # rhs and warm start returned to the caller, solved velocity
+                    "d2h_bytes_per_step": int(3 * vec_bytes)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": f"level-0 Jacobi sweep ({tag})",
+            "roofline": {"bound": "hbm", "kernel": dominant[0],
                          "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / peak, 4) if achieved else None,
-                         "traffic": traffic, "algorithmic_bytes": jac_bytes,
-                         "avg_launch_us": round(t_ms / cnt * 1e3, 2) if cnt else None},
+                         "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+                         "avg_launch_us": round(t_ms / cnt * 1e3, 2) if cnt else None,
+                         "level0_rbgs_GBps": round(l0_bytes / (l0_ms * 1e-3) / 1e9, 1) if l0_ms else None},
             "kernel_profile_ms": {k: [round(v[0], 4), v[1]] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
-            "dominant_kernel": dominant[0],
             "clocks": clocks,
         }
-        if cpu is not None:
-            line["cpu_baseline"] = cpu
+        if vcpu is not None:
+            line["cpu_baseline"] = vcpu
+        if poisson is not None:
+            line["poisson"] = poisson
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
