@@ -47,13 +47,27 @@ static void sort_unique_vdb(std::vector<int32_t>& org) {
     org.swap(out);
 }
 static void dilate_leaves(const int32_t* org, int64_t n, const uint64_t* masks, int r, bool face_only,
-                          std::vector<int32_t>& out) {
+                          std::vector<int32_t>& out, bool vdb_order) {
     out.clear();
-    out.reserve((size_t)n * 3 * (face_only ? 7 : 27));
+    if (n <= 0) return;
+    // dense occupancy over the leaf bounding box with a one-leaf margin
+    int mn[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, mx[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    for (int64_t i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) {
+            mn[c] = std::min(mn[c], org[3 * i + c] >> 3);
+            mx[c] = std::max(mx[c], org[3 * i + c] >> 3);
+        }
+    const int64_t d0 = mx[0] - mn[0] + 3, d1 = mx[1] - mn[1] + 3, d2 = mx[2] - mn[2] + 3;
+    if (d0 * d1 * d2 > (int64_t(1) << 30)) {
+        set_error("leaf bounding box too large for the dense leaf map (%lld cells)", (long long)(d0 * d1 * d2));
+        throw UaamgError{UAAMG_ERR_DOMAIN_TOO_LARGE};
+    }
+    std::vector<uint8_t> mark((size_t)(d0 * d1 * d2), 0);
+    auto cell = [&](int a, int b, int c) { return ((size_t)(a - mn[0] + 1) * d1 + (b - mn[1] + 1)) * d2 + (c - mn[2] + 1); };
     const uint64_t ylo = yband(0, r - 1), yhi = yband(8 - r, 7), zlo = zband(0, r - 1), zhi = zband(8 - r, 7);
     for (int64_t i = 0; i < n; ++i) {
-        const int32_t* o = org + 3 * i;
-        out.insert(out.end(), o, o + 3);
+        const int a0 = org[3 * i] >> 3, b0 = org[3 * i + 1] >> 3, c0 = org[3 * i + 2] >> 3;
+        mark[cell(a0, b0, c0)] = 1;
         uint64_t w[8];
         for (int k = 0; k < 8; ++k) w[k] = masks ? masks[8 * i + k] : ~0ull;
         uint64_t xa = 0, xl = 0, xh = 0;
@@ -71,13 +85,18 @@ static void dilate_leaves(const int32_t* org, int64_t n, const uint64_t* masks, 
                     uint64_t p = dx < 0 ? xl : (dx > 0 ? xh : xa);
                     if (dy < 0) p &= ylo; else if (dy > 0) p &= yhi;
                     if (dz < 0) p &= zlo; else if (dz > 0) p &= zhi;
-                    if (!p) continue;
-                    out.push_back(o[0] + 8 * dx);
-                    out.push_back(o[1] + 8 * dy);
-                    out.push_back(o[2] + 8 * dz);
+                    if (p) mark[cell(a0 + dx, b0 + dy, c0 + dz)] = 1;
                 }
     }
-    sort_unique_vdb(out);
+    for (int64_t a = 0; a < d0; ++a)
+        for (int64_t b = 0; b < d1; ++b)
+            for (int64_t c = 0; c < d2; ++c)
+                if (mark[((size_t)a * d1 + b) * d2 + c]) {
+                    out.push_back((int32_t)((a + mn[0] - 1) * 8));
+                    out.push_back((int32_t)((b + mn[1] - 1) * 8));
+                    out.push_back((int32_t)((c + mn[2] - 1) * 8));
+                }
+    if (vdb_order) sort_unique_vdb(out);
 }
 
 struct VHostLevel {
@@ -125,7 +144,7 @@ static void make_pattern_level(const std::vector<int32_t>& dl, const std::vector
     for (int64_t i = 0; i < nd; ++i)
         for (int w = 0; w < 8; ++w)
             uni[8 * i + w] = dm[(0 * nd + i) * 8 + w] | dm[(1 * nd + i) * 8 + w] | dm[(2 * nd + i) * 8 + w];
-    dilate_leaves(dl.data(), nd, uni.data(), r, false, L.org);
+    dilate_leaves(dl.data(), nd, uni.data(), r, false, L.org, true);
     L.nl = (int)(L.org.size() / 3);
     L.dof.assign((size_t)3 * L.nl * 8, 0);
     HostMap dmap;
@@ -216,6 +235,7 @@ struct uaamg_viscosity {
     DGrid mu{};
     SolidInfo S{};
     int* org0 = nullptr;
+    float* zpage = nullptr;  // [512] zeros
     DCoarsestV C{};
     float *x = nullptr, *b = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
     double* partials = nullptr;
@@ -313,6 +333,16 @@ static void upload_vlevel(uaamg_viscosity* h, const VHostLevel& H, VLevelDev& D,
     CK(cudaMemsetAsync(D.rhs, 0, vb, h->stream));
     CK(cudaMemsetAsync(D.tmp, 0, vb, h->stream));
     D.L.coef = (float*)valloc(h, (size_t)27 * H.nl * UAAMG_LEAF * sizeof(float));
+    D.L.nbtrim = nullptr;
+    D.L.zpage = h->zpage;
+}
+// [27][512] pages holding each array's applier default (read for missing and
+// trimmed leaves)
+static void upload_defpage(uaamg_viscosity* h, VLevelDev& D) {
+    std::vector<float> page((size_t)27 * UAAMG_LEAF);
+    for (int ca = 0; ca < 27; ++ca)
+        for (int k = 0; k < UAAMG_LEAF; ++k) page[(size_t)ca * UAAMG_LEAF + k] = D.L.app[ca];
+    D.L.defpage = vupload(h, page.data(), page.size());
 }
 static void upload_parents(uaamg_viscosity* h, const VHostLevel& H, VLevelDev& D) {
     D.L.parent = vupload(h, H.parent.data(), H.parent.size());
@@ -336,9 +366,9 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
 
     // leaf sets of the three dilations of the liquid topology
     std::vector<int32_t> a1, a2, a1f;
-    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 1, false, a1);
-    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 2, false, a2);
-    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 1, true, a1f);
+    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 1, false, a1, false);
+    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 2, false, a2, false);
+    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 1, true, a1f, false);
     const int n1 = (int)(a1.size() / 3), n2 = (int)(a2.size() / 3), n1f = (int)(a1f.size() / 3);
     HostMap m1, m2, m1f;
     m1.build(n1, a1.data());
@@ -386,6 +416,8 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
     CK(cudaStreamSynchronize(s));
     TRACE("visc volumes + dof marking");
 
+    h->zpage = (float*)valloc(h, UAAMG_LEAF * sizeof(float));
+    CK(cudaMemsetAsync(h->zpage, 0, UAAMG_LEAF * sizeof(float), s));
     // level 0: DOF leaves (pruned) and the pattern dilated by 2
     std::vector<int32_t> dl;
     std::vector<int> keep;
@@ -423,6 +455,7 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
             a[VA_T11] = h->def_off;
         }
         h->org0 = D.org;
+        upload_defpage(h, D);
         launch2(k_vcoef0, dim3((unsigned)H.nl, 3), 128, s, D.L, (const int*)D.org, h->V, h->mu, h->factor, h->def_diag,
                 (float*)D.L.coef);
     }
@@ -446,6 +479,7 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
             a[VA_T10] = -1.f;
             a[VA_T11] = 1.f;
         }
+        upload_defpage(h, D);
         launch2(k_vcoarse_coef, dim3((unsigned)h->host[fl + 1].nl, 3), 128, s, h->lv[fl].L, D.L, (float*)D.L.coef);
     }
     h->nlev = (int)h->host.size();
@@ -459,10 +493,13 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
     {
         VLevelDev& D = h->lv[0];
         uint32_t* trim = (uint32_t*)valloc(h, (size_t)(D.L.nl ? D.L.nl : 1) * 4);
+        uint32_t* nbtrim = (uint32_t*)valloc(h, (size_t)(D.L.nl ? D.L.nl : 1) * 27 * 4);
         if (D.L.nl) {
             launch2(k_vtrim, dim3((unsigned)D.L.nl), 128, s, D.L, trim);
+            launch2(k_vnbtrim, dim3((unsigned)D.L.nl), 32, s, D.L, (const uint32_t*)trim, nbtrim);
         }
         D.L.trim = trim;
+        D.L.nbtrim = nbtrim;
     }
     // coarsest explicit matrix (construct_exact_solver, :3650)
     {
@@ -611,11 +648,10 @@ static void venqueue_body(VEnq& E, cudaGraphConditionalHandle cond, int use_cond
     const VLevelDev& D = h->lv[0];
     const dim3 g((unsigned)D.L.nl, 3);
     enqueue_mucycle(E, 0, h->z, h->r, true);
-    const dim3 gd((unsigned)((3 * D.L.nl + 3) / 4));
+    const dim3 gd((unsigned)((3 * D.L.nl + VDOT_THREADS - 1) / VDOT_THREADS));
     float* part = reinterpret_cast<float*>(h->partials);
     if (E.prof) E.pb("L0 pcg rho (z.r)");
-    launch2(k_vdot_leaf, gd, 128, E.s, D.L, (const float*)h->z, (const float*)h->r, part);
-    launch2(k_vdot_final, dim3(1), 32, E.s, D.L.nl, (const float*)part, h->st, 0);
+    launch2(k_vdot, gd, VDOT_THREADS, E.s, D.L, (const float*)h->z, (const float*)h->r, part, h->st, 0);
     E.pe();
     if (E.prof) E.pb("L0 pcg x,p update");
     launch2(k_vpcg_update_p, g, 128, E.s, D.L, (const float*)h->z, h->p, h->x, (const PcgState*)h->st);
@@ -624,13 +660,12 @@ static void venqueue_body(VEnq& E, cudaGraphConditionalHandle cond, int use_cond
     launch2(k_vpcg_Ap, g, 128, E.s, D.L, (const float*)h->p, h->q);
     E.pe();
     if (E.prof) E.pb("L0 pcg sigma (p.q)");
-    launch2(k_vdot_leaf, gd, 128, E.s, D.L, (const float*)h->p, (const float*)h->q, part);
-    launch2(k_vdot_final, dim3(1), 32, E.s, D.L.nl, (const float*)part, h->st, 1);
+    launch2(k_vdot, gd, VDOT_THREADS, E.s, D.L, (const float*)h->p, (const float*)h->q, part, h->st, 1);
     E.pe();
     if (E.prof) E.pb("L0 pcg r update+absmax");
     launch2(k_vpcg_update_r, g, 128, E.s, D.L, (const float*)h->q, h->r, h->partials, h->st, cond, use_cond);
     E.pe();
-    E.count += 7;
+    E.count += 5;
 }
 static void venqueue_finish(VEnq& E) {
     uaamg_viscosity* h = E.h;

@@ -546,6 +546,17 @@ __global__ void __launch_bounds__(128) k_vtrim(VLevel L, uint32_t* trim) {
     if (t == 0) trim[leaf] = bits;
 }
 
+// trim bits of every leaf's 27 neighbours (0 for missing neighbours)
+__global__ void __launch_bounds__(32) k_vnbtrim(VLevel L, const uint32_t* trim, uint32_t* nbtrim) {
+    griddep_wait();
+    griddep_launch();
+    const int leaf = blockIdx.x, k = threadIdx.x;
+    if (k < 27) {
+        const int lf = L.nb[(long long)leaf * 27 + k];
+        nbtrim[(long long)leaf * 27 + k] = lf >= 0 ? trim[lf] : 0u;
+    }
+}
+
 // explicit_matrix_reducer (:2415-2605): one ELL row per DOF, columns ascending
 __device__ __forceinline__ int vdof_number(const VLevel& L, const int* dof_base, const int* nbrow, int c, int X, int Y,
                                            int Z) {

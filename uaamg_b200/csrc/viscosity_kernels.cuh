@@ -32,6 +32,9 @@ struct VLevel {
     const int* nb;                // [nl][27]
     const float* coef;            // [27][nl][512]
     const uint32_t* trim;         // [nl] bit (c*9+a): leaf holds the default
+    const uint32_t* nbtrim;       // [nl][27] trim bits of each neighbour leaf (nullptr: no trimming)
+    const float* defpage;         // [27][512] applier default of every array
+    const float* zpage;           // [512] zeros
     const int* parent;            // [nl] coarse leaf, -1 if none
     const unsigned char* octant;  // [nl] position in the parent: x<<2 | y<<1 | z
     const int* child;             // [nl][8] fine leaf per octant, -1 if none
@@ -50,75 +53,93 @@ __device__ __forceinline__ int vnb_index(int X, int Y, int Z) {
 }
 __device__ __forceinline__ int voff3(int X, int Y, int Z) { return ((X & 7) << 6) | ((Y & 7) << 3) | (Z & 7); }
 
-// Values of a [nl][512] array at the thread's four voxels shifted by
-// (dx, dy, dz), dz in {-1, 0, 1}; leaves that do not exist read `fill`, and
-// leaves whose trim bit is set (trim != nullptr) read `def`.
-__device__ __forceinline__ float vload1(const float* arr, const int* nbrow, const uint32_t* trim, uint32_t bit,
-                                        int X, int Y, int Z, float fill, float def) {
-    const int lf = nbrow[vnb_index(X, Y, Z)];
-    if (lf < 0) return fill;
-    if (trim && (trim[lf] & bit)) return def;
-    return arr[(long long)lf * UAAMG_LEAF + voff3(X, Y, Z)];
-}
-__device__ __forceinline__ float4 vload4(const float* arr, const int* nbrow, const uint32_t* trim, uint32_t bit,
-                                         int x, int y, int z0, int dx, int dy, int dz, float fill, float def) {
-    const int X = x + dx, Y = y + dy;
-    const int lf = nbrow[vnb_index(X, Y, z0)];
-    float4 a;
-    if (lf < 0) a = f4splat(fill);
-    else if (trim && (trim[lf] & bit)) a = f4splat(def);
-    else a = reinterpret_cast<const float4*>(arr)[((long long)lf * UAAMG_LEAF + voff3(X, Y, z0)) >> 2];
-    if (dz == 0) return a;
-    if (dz > 0) {
-        const float n = vload1(arr, nbrow, trim, bit, X, Y, z0 + 4, fill, def);
-        return make_float4(a.y, a.z, a.w, n);
+// The 27-neighbourhood of the CTA's leaf with each neighbour's trim bits,
+// staged in shared memory once per CTA: every later load depends only on a
+// shared-memory read, so all of a thread's global loads are in flight
+// together instead of in dependent chains.
+struct VNbSh {
+    int nb[27];
+    uint32_t tr[27];
+};
+// call with all threads of the CTA (contains __syncthreads)
+__device__ __forceinline__ void vnb_prologue(const VLevel& L, int leaf, VNbSh& sh) {
+    const int t = threadIdx.x;
+    if (t < 27) {
+        sh.nb[t] = L.nb[(long long)leaf * 27 + t];
+        sh.tr[t] = L.nbtrim ? L.nbtrim[(long long)leaf * 27 + t] : 0u;
     }
-    const float p = vload1(arr, nbrow, trim, bit, X, Y, z0 - 1, fill, def);
-    return make_float4(p, a.x, a.y, a.z);
+    __syncthreads();
 }
 
-struct VArr {  // one coefficient array of a level with its trim bit and applier default
+// Address of the leaf block holding neighbourhood slot k of array arr: the
+// fallback page when the leaf does not exist or is trimmed for this array.
+__device__ __forceinline__ const float* vsel(const float* arr, const float* fallback, const VNbSh& sh, uint32_t bit,
+                                             int k) {
+    const int lf = sh.nb[k];
+    const bool ok = lf >= 0 && !(sh.tr[k] & bit);
+    return ok ? arr + (long long)lf * UAAMG_LEAF : fallback;
+}
+
+// Values of a [nl][512] array at the thread's four voxels shifted by
+// (dx, dy, dz), dz in {-1, 0, 1}: missing leaves read the fallback page
+// (zeros for vectors, the applier default for coefficients), and so do
+// trimmed leaves (bit set in the neighbour's trim bits).
+__device__ __forceinline__ float4 vload4(const float* arr, const float* fb, const VNbSh& sh, uint32_t bit, int x, int y,
+                                         int z0, int dx, int dy, int dz) {
+    const int X = x + dx, Y = y + dy;
+    const float* p = vsel(arr, fb, sh, bit, vnb_index(X, Y, z0));
+    const float4 a = *reinterpret_cast<const float4*>(p + voff3(X, Y, z0));
+    if (dz == 0) return a;
+    if (dz > 0) {
+        const float* q = vsel(arr, fb, sh, bit, vnb_index(X, Y, z0 + 4));
+        return make_float4(a.y, a.z, a.w, q[voff3(X, Y, z0 + 4)]);
+    }
+    const float* q = vsel(arr, fb, sh, bit, vnb_index(X, Y, z0 - 1));
+    return make_float4(q[voff3(X, Y, z0 - 1)], a.x, a.y, a.z);
+}
+
+struct VArr {  // one coefficient array of a level with its trim bit and default page
     const float* a;
+    const float* def;
     uint32_t bit;
-    float def;
 };
 __device__ __forceinline__ VArr varr(const VLevel& L, int c, int a) {
     VArr r;
     r.a = L.coef + (long long)(c * VNA + a) * L.nl * UAAMG_LEAF;
+    r.def = L.defpage + (c * VNA + a) * UAAMG_LEAF;
     r.bit = 1u << (c * VNA + a);
-    r.def = L.app[c * VNA + a];
     return r;
 }
-__device__ __forceinline__ float4 cload4(const VArr& A, const VLevel& L, const int* nbrow, int x, int y, int z0, int dx,
-                                         int dy, int dz) {
-    return vload4(A.a, nbrow, L.trim, A.bit, x, y, z0, dx, dy, dz, A.def, A.def);
+__device__ __forceinline__ float4 cload4(const VArr& A, const VNbSh& sh, int x, int y, int z0, int dx, int dy,
+                                         int dz) {
+    return vload4(A.a, A.def, sh, A.bit, x, y, z0, dx, dy, dz);
 }
-__device__ __forceinline__ float4 uload4(const float* v, const VLevel& L, int c, const int* nbrow, int x, int y, int z0,
+__device__ __forceinline__ float4 uload4(const float* v, const VLevel& L, int c, const VNbSh& sh, int x, int y, int z0,
                                          int dx, int dy, int dz) {
-    return vload4(v + (long long)c * L.nl * UAAMG_LEAF, nbrow, nullptr, 0u, x, y, z0, dx, dy, dz, 0.f, 0.f);
+    return vload4(v + (long long)c * L.nl * UAAMG_LEAF, L.zpage, sh, 0u, x, y, z0, dx, dy, dz);
 }
 
 // Off-diagonal sum of channel c at the thread's four voxels (faced_result[1]
 // after the cross terms, :3084-3490) and the centre value.
-__device__ __forceinline__ float4 voffdiag(const VLevel& L, int c, int leaf, int t, const float* x, float4& xc) {
+__device__ __forceinline__ float4 voffdiag(const VLevel& L, const VNbSh& sh, int c, int t, const float* x,
+                                          float4& xc) {
     const int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
-    const int* nbrow = L.nb + (long long)leaf * 27;
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     int e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0};
     e0[d0] = 1;
     e1[d1] = 1;
     e2[d2] = 1;
-    xc = uload4(x, L, c, nbrow, X, Y, Z0, 0, 0, 0);
+    xc = uload4(x, L, c, sh, X, Y, Z0, 0, 0, 0);
     // same channel, absolute axes x, y, z: u(g+e)*neg(g+e) and u(g-e)*neg(g)
     float4 fr[6];
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
         const int px = ax == 0, py = ax == 1, pz = ax == 2;
         const VArr W = varr(L, c, VA_NEGX + ax);
-        const float4 up = uload4(x, L, c, nbrow, X, Y, Z0, px, py, pz);
-        const float4 wp = cload4(W, L, nbrow, X, Y, Z0, px, py, pz);
-        const float4 um = uload4(x, L, c, nbrow, X, Y, Z0, -px, -py, -pz);
-        const float4 wm = cload4(W, L, nbrow, X, Y, Z0, 0, 0, 0);
+        const float4 up = uload4(x, L, c, sh, X, Y, Z0, px, py, pz);
+        const float4 wp = cload4(W, sh, X, Y, Z0, px, py, pz);
+        const float4 um = uload4(x, L, c, sh, X, Y, Z0, -px, -py, -pz);
+        const float4 wm = cload4(W, sh, X, Y, Z0, 0, 0, 0);
         fr[2 * ax] = make_float4(__fmul_rn(up.x, wp.x), __fmul_rn(up.y, wp.y), __fmul_rn(up.z, wp.z),
                                  __fmul_rn(up.w, wp.w));
         fr[2 * ax + 1] = make_float4(__fmul_rn(um.x, wm.x), __fmul_rn(um.y, wm.y), __fmul_rn(um.z, wm.z),
@@ -126,22 +147,22 @@ __device__ __forceinline__ float4 voffdiag(const VLevel& L, int c, int leaf, int
     }
     // Td2 (m_cross_channel[d2], channel d1 velocities) and Td1
     // (m_cross_channel[d1], channel d2 velocities)
-    const float4 u1_g = uload4(x, L, d1, nbrow, X, Y, Z0, 0, 0, 0);
-    const float4 u1_p1 = uload4(x, L, d1, nbrow, X, Y, Z0, e1[0], e1[1], e1[2]);
-    const float4 u1_m0 = uload4(x, L, d1, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
-    const float4 u1_m0p1 = uload4(x, L, d1, nbrow, X, Y, Z0, e1[0] - e0[0], e1[1] - e0[1], e1[2] - e0[2]);
-    const float4 u2_g = uload4(x, L, d2, nbrow, X, Y, Z0, 0, 0, 0);
-    const float4 u2_m0 = uload4(x, L, d2, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
-    const float4 u2_p2 = uload4(x, L, d2, nbrow, X, Y, Z0, e2[0], e2[1], e2[2]);
-    const float4 u2_m0p2 = uload4(x, L, d2, nbrow, X, Y, Z0, e2[0] - e0[0], e2[1] - e0[1], e2[2] - e0[2]);
-    const float4 a00 = cload4(varr(L, d2, VA_T00), L, nbrow, X, Y, Z0, 0, 0, 0);
-    const float4 a01 = cload4(varr(L, d2, VA_T01), L, nbrow, X, Y, Z0, 0, 0, 0);
-    const float4 a10 = cload4(varr(L, d2, VA_T10), L, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
-    const float4 a11 = cload4(varr(L, d2, VA_T11), L, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
-    const float4 b00 = cload4(varr(L, d1, VA_T00), L, nbrow, X, Y, Z0, 0, 0, 0);
-    const float4 b01 = cload4(varr(L, d1, VA_T01), L, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
-    const float4 b10 = cload4(varr(L, d1, VA_T10), L, nbrow, X, Y, Z0, 0, 0, 0);
-    const float4 b11 = cload4(varr(L, d1, VA_T11), L, nbrow, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 u1_g = uload4(x, L, d1, sh, X, Y, Z0, 0, 0, 0);
+    const float4 u1_p1 = uload4(x, L, d1, sh, X, Y, Z0, e1[0], e1[1], e1[2]);
+    const float4 u1_m0 = uload4(x, L, d1, sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 u1_m0p1 = uload4(x, L, d1, sh, X, Y, Z0, e1[0] - e0[0], e1[1] - e0[1], e1[2] - e0[2]);
+    const float4 u2_g = uload4(x, L, d2, sh, X, Y, Z0, 0, 0, 0);
+    const float4 u2_m0 = uload4(x, L, d2, sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 u2_p2 = uload4(x, L, d2, sh, X, Y, Z0, e2[0], e2[1], e2[2]);
+    const float4 u2_m0p2 = uload4(x, L, d2, sh, X, Y, Z0, e2[0] - e0[0], e2[1] - e0[1], e2[2] - e0[2]);
+    const float4 a00 = cload4(varr(L, d2, VA_T00), sh, X, Y, Z0, 0, 0, 0);
+    const float4 a01 = cload4(varr(L, d2, VA_T01), sh, X, Y, Z0, 0, 0, 0);
+    const float4 a10 = cload4(varr(L, d2, VA_T10), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 a11 = cload4(varr(L, d2, VA_T11), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 b00 = cload4(varr(L, d1, VA_T00), sh, X, Y, Z0, 0, 0, 0);
+    const float4 b01 = cload4(varr(L, d1, VA_T01), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 b10 = cload4(varr(L, d1, VA_T10), sh, X, Y, Z0, 0, 0, 0);
+    const float4 b11 = cload4(varr(L, d1, VA_T11), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
     float4 off;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -169,15 +190,14 @@ __device__ __forceinline__ float4 voffdiag(const VLevel& L, int c, int leaf, int
 
 // One applier pass for channel c at the thread's voxels; m = DOF bits.
 template <int MODE>
-__device__ __forceinline__ float4 vapply_value(const VLevel& L, int c, int leaf, int t, const float* x,
+__device__ __forceinline__ float4 vapply_value(const VLevel& L, const VNbSh& sh, int c, int t, const float* x,
                                                const float* b, float w, unsigned m, float4& xc) {
-    const float4 off = voffdiag(L, c, leaf, t, x, xc);
-    const int* nbrow = L.nb + (long long)leaf * 27;
+    const float4 off = voffdiag(L, sh, c, t, x, xc);
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     float4 res = xc;
     if (MODE == VM_RED || MODE == VM_BLACK) {
-        const float4 bb = uload4(b, L, c, nbrow, X, Y, Z0, 0, 0, 0);
-        const float4 iv = cload4(varr(L, c, VA_INV), L, nbrow, X, Y, Z0, 0, 0, 0);
+        const float4 bb = uload4(b, L, c, sh, X, Y, Z0, 0, 0, 0);
+        const float4 iv = cload4(varr(L, c, VA_INV), sh, X, Y, Z0, 0, 0, 0);
         const float one_minus_w = __fsub_rn(1.0f, w);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -190,18 +210,18 @@ __device__ __forceinline__ float4 vapply_value(const VLevel& L, int c, int leaf,
             f4set(res, j, upd ? v : f4get(xc, j));
         }
     } else {
-        const float4 dg = cload4(varr(L, c, VA_DIAG), L, nbrow, X, Y, Z0, 0, 0, 0);
+        const float4 dg = cload4(varr(L, c, VA_DIAG), sh, X, Y, Z0, 0, 0, 0);
         if (MODE == VM_NORMAL) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) f4set(res, j, __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
         } else {
-            const float4 bb = uload4(b, L, c, nbrow, X, Y, Z0, 0, 0, 0);
+            const float4 bb = uload4(b, L, c, sh, X, Y, Z0, 0, 0, 0);
             if (MODE == VM_RESIDUAL) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                     f4set(res, j, __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j))));
             } else {  // JACOBI
-                const float4 iv = cload4(varr(L, c, VA_INV), L, nbrow, X, Y, Z0, 0, 0, 0);
+                const float4 iv = cload4(varr(L, c, VA_INV), sh, X, Y, Z0, 0, 0, 0);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
@@ -222,25 +242,25 @@ __device__ __forceinline__ float4 vapply_value(const VLevel& L, int c, int leaf,
 // (blockIdx.y = channel); RED / BLACK update channel c0 of x in place.
 // Voxel groups without DOFs are not written: every vector holds zeros there.
 template <int MODE>
-__global__ void __launch_bounds__(128) k_vapply(VLevel L, int c0, const float* x, const float* b, float* out,
+__global__ void __launch_bounds__(128, 5) k_vapply(VLevel L, int c0, const float* x, const float* b, float* out,
                                                 float w) {
     griddep_wait();
     griddep_launch();
+    __shared__ VNbSh sh;
     const int leaf = blockIdx.x, t = threadIdx.x;
     const int c = (MODE == VM_RED || MODE == VM_BLACK) ? c0 : (int)blockIdx.y;
     const unsigned m = vmask4(L, c, leaf, t);
+    vnb_prologue(L, leaf, sh);
     if (!m) return;
     float4 xc;
-    const float4 res = vapply_value<MODE>(L, c, leaf, t, x, b, w, m, xc);
+    const float4 res = vapply_value<MODE>(L, sh, c, t, x, b, w, m, xc);
     reinterpret_cast<float4*>(out + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
 }
 
-// restriction (:2353-2413), grid (coarse nl, 3): coarse = (sum of the DOF
-// children) * 0.125 * 0.5 * 2, zero at coarse non-DOF voxels
-__global__ void __launch_bounds__(128) k_vrestrict(VLevel F, VLevel C, const float* fine, float* coarse) {
-    griddep_wait();
-    griddep_launch();
-    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+// restriction (:2353-2413) for one (coarse leaf, channel): coarse = (sum of the
+// DOF children) * 0.125 * 0.5 * 2, zero at coarse non-DOF voxels
+__device__ __forceinline__ void vrestrict_item(const VLevel& F, const VLevel& C, const float* fine, float* coarse,
+                                               int leaf, int c, int t) {
     const unsigned m = vmask4(C, c, leaf, t);
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     float4 res = f4zero();
@@ -270,12 +290,15 @@ __global__ void __launch_bounds__(128) k_vrestrict(VLevel F, VLevel C, const flo
     }
     reinterpret_cast<float4*>(coarse + (long long)c * C.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
 }
-
-// prolongation<true> (:2659-2729), grid (fine nl, 3): fine += coarse parent
-__global__ void __launch_bounds__(128) k_vprolong(VLevel F, VLevel C, const float* coarse, float* fine) {
+__global__ void __launch_bounds__(128) k_vrestrict(VLevel F, VLevel C, const float* fine, float* coarse) {
     griddep_wait();
     griddep_launch();
-    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+    vrestrict_item(F, C, fine, coarse, blockIdx.x, blockIdx.y, threadIdx.x);
+}
+
+// prolongation<true> (:2659-2729) for one (fine leaf, channel): fine += coarse parent
+__device__ __forceinline__ void vprolong_item(const VLevel& F, const VLevel& C, const float* coarse, float* fine,
+                                              int leaf, int c, int t) {
     const unsigned m = vmask4(F, c, leaf, t);
     if (!m) return;
     const int P = F.parent[leaf];
@@ -293,6 +316,11 @@ __global__ void __launch_bounds__(128) k_vprolong(VLevel F, VLevel C, const floa
         f4set(v, j, __fadd_rn(f4get(v, j), cv[(cx << 6) | (cy << 3) | cz]));
     }
     *fp = v;
+}
+__global__ void __launch_bounds__(128) k_vprolong(VLevel F, VLevel C, const float* coarse, float* fine) {
+    griddep_wait();
+    griddep_launch();
+    vprolong_item(F, C, coarse, fine, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 
 // zero every non-DOF voxel of a 3-channel vector (inputs from callers)
@@ -355,12 +383,14 @@ __global__ void __launch_bounds__(128) k_vpcg_init(VLevel L, const float* x, con
     griddep_launch();
     __shared__ float shf[4];
     __shared__ bool last;
+    __shared__ VNbSh sh;
     const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
     const unsigned m = vmask4(L, c, leaf, t);
+    vnb_prologue(L, leaf, sh);
     float a = 0.f;
     if (m) {
         float4 xc;
-        const float4 res = vapply_value<VM_RESIDUAL>(L, c, leaf, t, x, b, 1.f, m, xc);
+        const float4 res = vapply_value<VM_RESIDUAL>(L, sh, c, t, x, b, 1.f, m, xc);
         reinterpret_cast<float4*>(r + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
         a = vabs4(res, m);
     }
@@ -390,55 +420,71 @@ __global__ void __launch_bounds__(128) k_vpcg_init(VLevel L, const float* x, con
 // the leaf partials in leaf order per channel, then of the three channel
 // sums.  (TBB may split the reference's sum anywhere; this is the serial
 // schedule, so the PCG follows the reference's float rounding.)
-// Stage 1: one warp per (channel, leaf) item; lane 0 adds the products in order.
-__global__ void __launch_bounds__(128) k_vdot_leaf(VLevel L, const float* a, const float* b, float* part) {
+// One kernel: a thread per (channel, leaf) item adds the products of its
+// leaf's DOF voxels in offset order; the last CTA to finish (ticket) adds the
+// item partials channel by channel in leaf order and updates the PCG scalar:
+// which = 0: rho_new = z.r (line 13; first iteration: rho = rho_new, beta = 0,
+// later beta = rho_new / rho, rho = rho_new); which = 1: sigma = p.q,
+// alpha = rho / sigma (lines 6-7).
+#define VDOT_THREADS 64
+#define VDOT_CHUNK 2048
+__global__ void __launch_bounds__(VDOT_THREADS) k_vdot(VLevel L, const float* a, const float* b, float* part,
+                                                       PcgState* st, int which) {
     griddep_wait();
     griddep_launch();
-    __shared__ float prod[4][UAAMG_LEAF];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long item = (long long)blockIdx.x * 4 + w;  // c * nl + leaf
-    if (item >= 3LL * L.nl) return;
-    const float* pa = a + item * UAAMG_LEAF;
-    const float* pb = b + item * UAAMG_LEAF;
-    const uint64_t* m = L.dof + item * 8;
-    bool any = false;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) any |= (m[q] != 0ull);
-    if (!any) {
-        if (lane == 0) part[item] = 0.f;
-        return;
-    }
-#pragma unroll 4
-    for (int k = lane; k < UAAMG_LEAF; k += 32) prod[w][k] = __fmul_rn(pa[k], pb[k]);
-    __syncwarp();
-    if (lane == 0) {
+    __shared__ __align__(16) float buf[3][VDOT_CHUNK];  // read as float4
+    __shared__ float cs[3];
+    __shared__ bool last;
+    const int t = threadIdx.x;
+    const long long item = (long long)blockIdx.x * VDOT_THREADS + t;
+    if (item < 3LL * L.nl) {
+        const float4* pa = reinterpret_cast<const float4*>(a + item * UAAMG_LEAF);
+        const float4* pb = reinterpret_cast<const float4*>(b + item * UAAMG_LEAF);
+        const uint64_t* m = L.dof + item * 8;
         float acc = 0.f;
         for (int q = 0; q < 8; ++q) {
-            uint64_t word = m[q];
-            while (word) {
-                const int bit = __ffsll((long long)word) - 1;
-                acc = __fadd_rn(acc, prod[w][q * 64 + bit]);
-                word &= word - 1;
+            const uint64_t word = m[q];
+            if (!word) continue;
+#pragma unroll 4
+            for (int k = 0; k < 16; ++k) {
+                const unsigned nib = (unsigned)(word >> (4 * k)) & 0xFu;
+                if (!nib) continue;
+                const float4 x = pa[q * 16 + k], y = pb[q * 16 + k];
+                if (nib & 1u) acc = __fadd_rn(acc, __fmul_rn(x.x, y.x));
+                if (nib & 2u) acc = __fadd_rn(acc, __fmul_rn(x.y, y.y));
+                if (nib & 4u) acc = __fadd_rn(acc, __fmul_rn(x.z, y.z));
+                if (nib & 8u) acc = __fadd_rn(acc, __fmul_rn(x.w, y.w));
             }
         }
         part[item] = acc;
     }
-}
-// Stage 2 (one block): per-channel sums in leaf order, then the PCG scalar.
-// which = 0: rho_new = z.r (line 13; first iteration: rho = rho_new, beta = 0,
-// later beta = rho_new / rho, rho = rho_new); which = 1: sigma = p.q,
-// alpha = rho / sigma (lines 6-7).
-__global__ void __launch_bounds__(32) k_vdot_final(int nl, const float* part, PcgState* st, int which) {
-    griddep_wait();
-    griddep_launch();
-    __shared__ float cs[3];
-    const int t = threadIdx.x;
-    if (t < 3) {
-        const float* p = part + (long long)t * nl;
-        float acc = 0.f;
-        for (int i = 0; i < nl; ++i) acc = __fadd_rn(acc, p[i]);
-        cs[t] = acc;
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = (atomicAdd(&st->ticket[5], 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    const int nl = L.nl;
+    float acc = 0.f;  // thread c < 3: running sum of channel c
+    for (int base = 0; base < nl; base += VDOT_CHUNK) {
+        const int len = min(VDOT_CHUNK, nl - base);
+        __syncthreads();
+        for (int c = 0; c < 3; ++c)
+            for (int i = t; i < len; i += VDOT_THREADS) buf[c][i] = __ldcg(part + (long long)c * nl + base + i);
+        __syncthreads();
+        if (t < 3) {
+            const float* bb = buf[t];
+            int i = 0;
+            for (; i + 4 <= len; i += 4) {
+                const float4 v = *reinterpret_cast<const float4*>(bb + i);
+                acc = __fadd_rn(acc, v.x);
+                acc = __fadd_rn(acc, v.y);
+                acc = __fadd_rn(acc, v.z);
+                acc = __fadd_rn(acc, v.w);
+            }
+            for (; i < len; ++i) acc = __fadd_rn(acc, bb[i]);
+        }
     }
+    if (t < 3) cs[t] = acc;
     __syncthreads();
     if (t == 0) {
         float r = 0.f;
@@ -453,6 +499,7 @@ __global__ void __launch_bounds__(32) k_vdot_final(int nl, const float* part, Pc
             st->alpha = __fdiv_rn(st->rho, r);
             st->first = 0;
         }
+        st->ticket[5] = 0;
     }
 }
 
@@ -481,15 +528,17 @@ __global__ void __launch_bounds__(128) k_vpcg_update_p(VLevel L, const float* z,
     reinterpret_cast<float4*>(p)[i] = pp;
 }
 
-// line 6: q = A p (sigma and alpha follow in k_vdot_leaf / k_vdot_final)
+// line 6: q = A p (sigma and alpha follow in k_vdot)
 __global__ void __launch_bounds__(128) k_vpcg_Ap(VLevel L, const float* p, float* q) {
     griddep_wait();
     griddep_launch();
+    __shared__ VNbSh sh;
     const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
     const unsigned m = vmask4(L, c, leaf, t);
+    vnb_prologue(L, leaf, sh);
     if (!m) return;
     float4 xc;
-    const float4 res = vapply_value<VM_NORMAL>(L, c, leaf, t, p, nullptr, 1.f, m, xc);
+    const float4 res = vapply_value<VM_NORMAL>(L, sh, c, t, p, nullptr, 1.f, m, xc);
     reinterpret_cast<float4*>(q + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
 }
 
@@ -684,5 +733,6 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
         if (i < n) out[C.slot[i]] = x[k];
     }
 }
+
 
 }  // namespace uaamg
