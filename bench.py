@@ -438,14 +438,21 @@ def main():
     for l in range(levels):
         _, m = lv.topology(l)
         ndof_c.append([int(sum(bin(int(w)).count("1") for w in m[c].reshape(-1))) for c in range(3)])
-    dominant = max(prof.items(), key=lambda kv: kv[1][0])
-    dom_bytes = _visc_pass_bytes(dominant[0], ndof, ndof_c)
-    # the level-0 red-black passes: the bandwidth-heavy kernels of the cycle
-    l0 = [(k, v) for k, v in prof.items() if k.startswith("L0 red_gs") or k.startswith("L0 black_gs")]
+    # The dominant kernel is k_vapply in its red/black GS modes (all levels).
+    # Its bandwidth-relevant launches are the level-0 passes: the roofline is
+    # quoted on the level-0 red pass of channel 0 (the launch the committed ncu
+    # capture measures), and the all-level aggregate is reported beside it.
+    gs = [(k, v) for k, v in prof.items() if " red_gs " in k or " black_gs " in k]
+    gs_bytes = sum(_visc_pass_bytes(k, ndof, ndof_c) * v[1] for k, v in gs)
+    gs_ms = sum(v[0] for k, v in gs)
+    prof_ms = sum(v[0] for v in prof.values())
+    dom_label = "L0 red_gs c0"
+    dom_bytes = _visc_pass_bytes(dom_label, ndof, ndof_c)
+    l0 = [(k, v) for k, v in gs if k.startswith("L0 ")]
     l0_bytes = sum(_visc_pass_bytes(k, ndof, ndof_c) * v[1] for k, v in l0)
     l0_ms = sum(v[0] for k, v in l0)
     peak, peak_kind = _peaks()
-    t_ms, cnt = dominant[1]
+    t_ms, cnt = prof.get(dom_label, (0.0, 0))
     achieved = dom_bytes / (t_ms / cnt * 1e-3) / 1e9 if (dom_bytes and cnt) else None
     traffic = _traffic_from_profile("k_vapply<3>")
     vec_bytes = 3 * 4 * 512 * n0
@@ -537,13 +544,17 @@ def main():
                     # rhs and warm start returned to the caller, solved velocity
                     "d2h_bytes_per_step": int(3 * vec_bytes)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": dominant[0],
+            "roofline": {"bound": "hbm", "kernel": "k_vapply<RED_GS> level 0, channel 0 (2774 CTAs)",
                          "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / peak, 4) if achieved else None,
                          "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
                          "avg_launch_us": round(t_ms / cnt * 1e3, 2) if cnt else None,
-                         "level0_rbgs_GBps": round(l0_bytes / (l0_ms * 1e-3) / 1e9, 1) if l0_ms else None},
+                         "level0_rbgs_GBps": round(l0_bytes / (l0_ms * 1e-3) / 1e9, 1) if l0_ms else None,
+                         "all_levels_rbgs_GBps": round(gs_bytes / (gs_ms * 1e-3) / 1e9, 1) if gs_ms else None,
+                         "rbgs_share_of_solve": round(gs_ms / prof_ms, 3) if prof_ms else None,
+                         "note": "per-launch times from CUDA event pairs in a host-driven solve; coarse-level "
+                                 "passes (23-560 CTAs) are latency-bound"},
             "kernel_profile_ms": {k: [round(v[0], 4), v[1]] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
             "clocks": clocks,
         }

@@ -1,8 +1,11 @@
 // uaamg_simd.hpp -- header-only C++ facade with the reference's class names
-// over the C ABI in uaamg.h, so a FLIP_vdb-style call site
-// (FLIP_vdb.cpp:3118-3168: createPressurePoissonLaplacian, PoissonSolver,
-// mRelativeTolerance, mSmoother, createPressurePoissonRightHandSide,
-// solveMultigridPCG, FAILED -> solvePureMultigrid) reads the same.
+// over the C ABI in uaamg.h, so FLIP_vdb-style call sites read the same:
+// pressure (FLIP_vdb.cpp:3118-3168: createPressurePoissonLaplacian,
+// PoissonSolver, mRelativeTolerance, mSmoother,
+// createPressurePoissonRightHandSide, solveMultigridPCG, FAILED ->
+// solvePureMultigrid) and viscosity (FLIP_vdb.cpp:3170-3216:
+// simd_viscosity3d, m_matrix_levels[0]->get_zero_vec(), warm start,
+// pcg_solve, m_iteration, m_ndof).
 //
 // Grids are flattened OpenVDB leaf lists (uaamg::LeafGrid); the result
 // vectors are leaf-dense float[leaf][512] over the DOF leaves returned by
@@ -127,6 +130,97 @@ private:
         check(uaamg_poisson_set_relative_tolerance(mLevel0->handle(), mRelativeTolerance), "set_tolerance");
     }
     LaplacianWithLevel::Ptr mLevel0;
+};
+
+// Three face-velocity channels (packed_FloatGrid3, SIMD_UAAMG/packed3grids.h:5-23).
+struct PackedLeafGrid3 {
+    LeafGrid v[3];
+};
+
+// L_with_level (SIMD_UAAMG/simd_viscosity3d.h:60-200): the level-0 viscosity
+// matrix together with its device hierarchy.
+class L_with_level {
+public:
+    using Ptr = std::shared_ptr<L_with_level>;
+
+    // create_viscosity_matrix (simd_viscosity3d.h:86-89); dx is the voxel
+    // size of liquid_sdf in the reference
+    static Ptr create_viscosity_matrix(const LeafGrid& viscosity, const LeafGrid& liquidSdf,
+                                       const LeafGrid& solidSdf, float dt, float rho, float dx) {
+        uaamg_leaf_grid m = viscosity.view(), l = liquidSdf.view(), s = solidSdf.view();
+        uaamg_viscosity* h = nullptr;
+        check(uaamg_viscosity_create(&m, &l, &s, dt, rho, dx, &h), "uaamg_viscosity_create");
+        return Ptr(new L_with_level(h));
+    }
+    ~L_with_level() { uaamg_viscosity_destroy(mHandle); }
+    L_with_level(const L_with_level&) = delete;
+    L_with_level& operator=(const L_with_level&) = delete;
+
+    // get_zero_vec: three channels, float[3][leaf][512] over dofTopology()
+    std::vector<float> get_zero_vec(int level = 0) const {
+        return std::vector<float>((size_t)3 * uaamg_viscosity_leaf_count(mHandle, level) * 512, 0.f);
+    }
+    // build_rhs (simd_viscosity3d.cpp:1724-2087)
+    std::vector<float> build_rhs(const PackedLeafGrid3& velocity, const LeafGrid& solidVelocity) {
+        std::vector<float> rhs = get_zero_vec();
+        uaamg_leaf_grid u = velocity.v[0].view(), v = velocity.v[1].view(), w = velocity.v[2].view();
+        uaamg_leaf_grid s = solidVelocity.view();
+        check(uaamg_viscosity_build_rhs(mHandle, &u, &v, &w, &s, rhs.data()), "viscosity build_rhs");
+        return rhs;
+    }
+    // the velocity at every DOF: the warm start of FLIP_vdb.cpp:3186-3198
+    std::vector<float> warm_start(const PackedLeafGrid3& velocity) {
+        std::vector<float> x = get_zero_vec();
+        uaamg_leaf_grid u = velocity.v[0].view(), v = velocity.v[1].view(), w = velocity.v[2].view();
+        check(uaamg_viscosity_gather_velocity(mHandle, &u, &v, &w, x.data()), "gather_velocity");
+        return x;
+    }
+    void dofTopology(std::vector<int32_t>& origins, std::vector<uint64_t>& masks, int level = 0) const {
+        int64_t n = uaamg_viscosity_leaf_count(mHandle, level);
+        origins.resize((size_t)n * 3);
+        masks.resize((size_t)n * 3 * 8);
+        check(uaamg_viscosity_topology(mHandle, level, origins.data(), masks.data()), "viscosity topology");
+    }
+    int64_t m_ndof() const { return uaamg_viscosity_num_dof(mHandle, 0); }
+    uaamg_viscosity* handle() const { return mHandle; }
+
+private:
+    explicit L_with_level(uaamg_viscosity* h) : mHandle(h) {}
+    uaamg_viscosity* mHandle;
+};
+
+// simd_viscosity3d (SIMD_UAAMG/simd_viscosity3d.h:280-330)
+class simd_viscosity3d {
+public:
+    // simd_viscosity3d(viscosity, liquid_sdf, solid_sdf, liquid_velocity,
+    // solid_velocity, dt, rho) (simd_viscosity3d.h:285-290)
+    simd_viscosity3d(const LeafGrid& viscosity, const LeafGrid& liquidSdf, const LeafGrid& solidSdf,
+                     const PackedLeafGrid3& liquidVelocity, const LeafGrid& solidVelocity, float dt, float rho,
+                     float dx)
+        : simd_viscosity3d(L_with_level::create_viscosity_matrix(viscosity, liquidSdf, solidSdf, dt, rho, dx),
+                           liquidVelocity, solidVelocity) {}
+    // simd_viscosity3d(level0, liquid_velocity, solid_velocity) (:292-294)
+    simd_viscosity3d(L_with_level::Ptr level0, const PackedLeafGrid3& liquidVelocity, const LeafGrid& solidVelocity)
+        : m_level0(std::move(level0)) {
+        m_rhs = m_level0->build_rhs(liquidVelocity, solidVelocity);
+        m_ndof = m_level0->m_ndof();
+    }
+
+    // pcg_solve (simd_viscosity3d.cpp:3691-3754): in_lhs holds the warm start
+    // and receives the solution
+    void pcg_solve(std::vector<float>& inLhs, float tolerance) {
+        check(uaamg_viscosity_set_max_iterations(m_level0->handle(), m_max_iter), "set_max_iterations");
+        int it = 0;
+        check(uaamg_viscosity_solve_pcg(m_level0->handle(), inLhs.data(), m_rhs.data(), tolerance, &it),
+              "viscosity solve_pcg");
+        m_iteration = it;
+    }
+
+    L_with_level::Ptr m_level0;  // m_matrix_levels[0]
+    std::vector<float> m_rhs;
+    int m_iteration = 0;
+    int m_max_iter = 100;
+    int64_t m_ndof = 0;
 };
 
 }  // namespace simd_uaamg_b200

@@ -818,27 +818,7 @@ __global__ void __launch_bounds__(128) k_dot_rho(DLevel L, const float* z, const
                                                  PcgState* st) {
     griddep_wait();
     griddep_launch();
-    __shared__ double shd[4];
-    __shared__ bool last;
-    const int leaf = blockIdx.x, t = threadIdx.x;
-    float4 a = ld4(z, leaf, t), c = ld4(r, leaf, t);
-    unsigned m = mask4(L.mask, leaf, t);
-    double s = 0;
-    if (m & 1) s += (double)a.x * c.x;
-    if (m & 2) s += (double)a.y * c.y;
-    if (m & 4) s += (double)a.z * c.z;
-    if (m & 8) s += (double)a.w * c.w;
-    double part = block_sum128(s, shd);
-    if (publish_partial(part, partials, &st->ticket[0], &last)) {
-        double tot = gather_sum(partials, shd);
-        if (t == 0) {
-            float rho_new = (float)tot;
-            st->rho_new = rho_new;
-            st->beta = st->first ? 0.f : __fdiv_rn(rho_new, st->rho);
-            st->rho = rho_new;
-            st->ticket[0] = 0;
-        }
-    }
+    dot_rho_leaf(L, blockIdx.x, gridDim.x, z, r, partials, st);
 }
 
 // muCyclePreconditioner<2, skip_first> (simd_vdb_poisson.cpp:1844-1977) at

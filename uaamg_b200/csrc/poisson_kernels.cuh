@@ -257,27 +257,38 @@ __device__ __forceinline__ float block_max128(float v, float* sh) {
 // |v| with non-finite values propagated (grid_abs_max_op, openvdb_grid_math_op.h:4-43)
 __device__ __forceinline__ float absprop(float v) { return isfinite(v) ? fabsf(v) : (isnan(v) ? v : INFINITY); }
 
-// Writes this block's partial; returns true in every thread of the last block.
-__device__ __forceinline__ bool publish_partial(double part, double* partials, unsigned* ticket, bool* sh_last) {
+// Writes this block's partial into slot `slot` of the `count` partials of one
+// reduction; returns true in every thread of the block that finishes last.
+__device__ __forceinline__ bool publish_partial_at(double part, double* partials, unsigned* ticket, int slot,
+                                                   int count, bool* sh_last) {
     if (threadIdx.x == 0) {
-        partials[blockIdx.x] = part;
+        partials[slot] = part;
         __threadfence();
         unsigned tk = atomicAdd(ticket, 1u);
-        *sh_last = (tk == gridDim.x - 1);
+        *sh_last = (tk == (unsigned)count - 1);
     }
     __syncthreads();
     return *sh_last;
 }
-// Sum of all partials in a fixed order (last block only), valid in thread 0.
-__device__ __forceinline__ double gather_sum(const double* partials, double* sh) {
+__device__ __forceinline__ bool publish_partial(double part, double* partials, unsigned* ticket, bool* sh_last) {
+    return publish_partial_at(part, partials, ticket, blockIdx.x, gridDim.x, sh_last);
+}
+// Sum of the first `count` partials in a fixed order (last block only), valid in thread 0.
+__device__ __forceinline__ double gather_sum_n(const double* partials, int count, double* sh) {
     double acc = 0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) acc += __ldcg(partials + i);
+    for (int i = threadIdx.x; i < count; i += blockDim.x) acc += __ldcg(partials + i);
     return block_sum128(acc, sh);
 }
-__device__ __forceinline__ float gather_max(const double* partials, float* sh) {
+__device__ __forceinline__ float gather_max_n(const double* partials, int count, float* sh) {
     float acc = 0.f;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) acc = nanmax(acc, (float)__ldcg(partials + i));
+    for (int i = threadIdx.x; i < count; i += blockDim.x) acc = nanmax(acc, (float)__ldcg(partials + i));
     return block_max128(acc, sh);
+}
+__device__ __forceinline__ double gather_sum(const double* partials, double* sh) {
+    return gather_sum_n(partials, gridDim.x, sh);
+}
+__device__ __forceinline__ float gather_max(const double* partials, float* sh) {
+    return gather_max_n(partials, gridDim.x, sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -349,12 +360,13 @@ __device__ __forceinline__ float4 sweep_value(const DLevel& L, int leaf, int t, 
     return res;
 }
 
+// One leaf of a sweep (CTA = leaf of a level with `count` leaves, the slot
+// range of the fused dot's partials).
 template <int MODE, class Src>
-__global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b, float* out, float w, float wsor,
-                                               float one_minus_wsor, DotOut dot, int* spai0_ready) {
-    griddep_wait();
-    griddep_launch();
-    const int leaf = blockIdx.x, t = threadIdx.x;
+__device__ __forceinline__ void sweep_leaf(const DLevel& L, int leaf, int count, const Src& src, const float* b,
+                                           float* out, float w, float wsor, float one_minus_wsor, const DotOut& dot,
+                                           int* spai0_ready) {
+    const int t = threadIdx.x;
     float4 xc;
     unsigned m;
     float4 res = sweep_value<MODE>(L, leaf, t, src, b, w, wsor, one_minus_wsor, xc, m);
@@ -366,8 +378,8 @@ __global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b
         float4 rr = ld4(dot.r, leaf, t);
         double s = (double)res.x * rr.x + (double)res.y * rr.y + (double)res.z * rr.z + (double)res.w * rr.w;
         double part = block_sum128(s, shd);
-        if (publish_partial(part, dot.partials, &dot.st->ticket[0], &last)) {
-            double tot = gather_sum(dot.partials, shd);
+        if (publish_partial_at(part, dot.partials, &dot.st->ticket[0], leaf, count, &last)) {
+            double tot = gather_sum_n(dot.partials, count, shd);
             if (t == 0) {
                 PcgState* st = dot.st;
                 float rho_new = (float)tot;
@@ -378,6 +390,14 @@ __global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b
             }
         }
     }
+}
+
+template <int MODE, class Src>
+__global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b, float* out, float w, float wsor,
+                                               float one_minus_wsor, DotOut dot, int* spai0_ready) {
+    griddep_wait();
+    griddep_launch();
+    sweep_leaf<MODE>(L, blockIdx.x, gridDim.x, src, b, out, w, wsor, one_minus_wsor, dot, spai0_ready);
 }
 
 // out = value of a source (materialise a first sweep or a prolongation)
@@ -398,11 +418,10 @@ __global__ void __launch_bounds__(128) k_materialize(DLevel L, Src src, float* o
 // residual (RESID) or plain values, restricted to the parent level:
 // coarse = 0.125 * sum of the active fine values of the 2x2x2 block (.cpp:1624-1684)
 template <bool RESID>
-__global__ void __launch_bounds__(128) k_restrict(DLevel L, const float* x, const float* b, float* coarse) {
-    griddep_wait();
-    griddep_launch();
+__device__ __forceinline__ void restrict_leaf(const DLevel& L, int leaf, const float* x, const float* b,
+                                              float* coarse) {
     __shared__ float rs[UAAMG_LEAF];
-    const int leaf = blockIdx.x, t = threadIdx.x;
+    const int t = threadIdx.x;
     float4 r;
     if (RESID) {
         float4 xc;
@@ -430,6 +449,12 @@ __global__ void __launch_bounds__(128) k_restrict(DLevel L, const float* x, cons
         const int coff = ((((o >> 2) & 1) * 4 + i) << 6) | ((((o >> 1) & 1) * 4 + j) << 3) | ((o & 1) * 4 + k);
         coarse[(long long)L.parent[leaf] * UAAMG_LEAF + coff] = __fmul_rn(s, 0.125f);
     }
+}
+template <bool RESID>
+__global__ void __launch_bounds__(128) k_restrict(DLevel L, const float* x, const float* b, float* coarse) {
+    griddep_wait();
+    griddep_launch();
+    restrict_leaf<RESID>(L, blockIdx.x, x, b, coarse);
 }
 
 // ---------------------------------------------------------------------------
@@ -781,25 +806,25 @@ __device__ __forceinline__ void set_cond(cudaGraphConditionalHandle h, int use, 
     if (use) cudaGraphSetConditional(h, v);
 }
 
+// The PCG steps as per-leaf bodies (CTA = leaf of level 0 with `count`
+// leaves): the single-solve kernels below run them with leaf = blockIdx.x,
+// batched solves with the leaf of the CTA's (instance, leaf) entry.
+
 // lines 2-3: r = b - A x; nu = |r|_inf; numax = tol * nu
-__global__ void __launch_bounds__(128) k_pcg_init(DLevel L, const float* x, const float* b, float* r,
-                                                  double* partials, PcgState* st,
-                                                  cudaGraphConditionalHandle cond, int use_cond) {
-    griddep_wait();
-    griddep_launch();
+__device__ __forceinline__ void pcg_init_leaf(const DLevel& L, int leaf, int count, const float* x, const float* b,
+                                              float* r, double* partials, PcgState* st,
+                                              cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ float shf[4];
-    __shared__ double shd[4];
     __shared__ bool last;
-    const int leaf = blockIdx.x, t = threadIdx.x;
+    const int t = threadIdx.x;
     float4 xc;
     unsigned m;
     float4 res = sweep_value<M_RESIDUAL>(L, leaf, t, SrcPlain{x}, b, 0.f, 0.f, 0.f, xc, m);
     st4(r, leaf, t, res);
     float a = nanmax(nanmax(absprop(res.x), absprop(res.y)), nanmax(absprop(res.z), absprop(res.w)));
     float part = block_max128(a, shf);
-    (void)shd;
-    if (publish_partial((double)part, partials, &st->ticket[1], &last)) {
-        float nu = gather_max(partials, shf);
+    if (publish_partial_at((double)part, partials, &st->ticket[1], leaf, count, &last)) {
+        float nu = gather_max_n(partials, count, shf);
         if (t == 0) {
             st->nu = nu;
             st->nu_old = nu;
@@ -818,13 +843,17 @@ __global__ void __launch_bounds__(128) k_pcg_init(DLevel L, const float* x, cons
         }
     }
 }
-
-// x += alpha_prev * p_prev (line 16, skipped in the first iteration); p = z + beta p (line 16)
-__global__ void __launch_bounds__(128) k_pcg_update_p(DLevel L, const float* z, float* p, float* x,
-                                                      const PcgState* st) {
+__global__ void __launch_bounds__(128) k_pcg_init(DLevel L, const float* x, const float* b, float* r,
+                                                  double* partials, PcgState* st,
+                                                  cudaGraphConditionalHandle cond, int use_cond) {
     griddep_wait();
     griddep_launch();
-    const int leaf = blockIdx.x, t = threadIdx.x;
+    pcg_init_leaf(L, blockIdx.x, gridDim.x, x, b, r, partials, st, cond, use_cond);
+}
+
+// x += alpha_prev * p_prev (line 16, skipped in the first iteration); p = z + beta p (line 16)
+__device__ __forceinline__ void pcg_update_p_leaf(int leaf, const float* z, float* p, float* x, const PcgState* st) {
+    const int t = threadIdx.x;
     const float beta = st->beta, alpha = st->alpha;
     const int first = st->first;
     float4 zz = ld4(z, leaf, t), pp = ld4(p, leaf, t);
@@ -842,22 +871,27 @@ __global__ void __launch_bounds__(128) k_pcg_update_p(DLevel L, const float* z, 
     pp.w = __fmaf_rn(beta, pp.w, zz.w);
     st4(p, leaf, t, pp);
 }
-
-// lines 6-7: q = A p; sigma = p.q; alpha = rho / sigma
-__global__ void __launch_bounds__(128) k_pcg_Ap(DLevel L, const float* p, float* q, double* partials, PcgState* st) {
+__global__ void __launch_bounds__(128) k_pcg_update_p(DLevel L, const float* z, float* p, float* x,
+                                                      const PcgState* st) {
     griddep_wait();
     griddep_launch();
+    pcg_update_p_leaf(blockIdx.x, z, p, x, st);
+}
+
+// lines 6-7: q = A p; sigma = p.q; alpha = rho / sigma
+__device__ __forceinline__ void pcg_Ap_leaf(const DLevel& L, int leaf, int count, const float* p, float* q,
+                                            double* partials, PcgState* st) {
     __shared__ double shd[4];
     __shared__ bool last;
-    const int leaf = blockIdx.x, t = threadIdx.x;
+    const int t = threadIdx.x;
     float4 xc;
     unsigned m;
     float4 res = sweep_value<M_LAPLACIAN>(L, leaf, t, SrcPlain{p}, nullptr, 0.f, 0.f, 0.f, xc, m);
     st4(q, leaf, t, res);
     double s = (double)xc.x * res.x + (double)xc.y * res.y + (double)xc.z * res.z + (double)xc.w * res.w;
     double part = block_sum128(s, shd);
-    if (publish_partial(part, partials, &st->ticket[2], &last)) {
-        double tot = gather_sum(partials, shd);
+    if (publish_partial_at(part, partials, &st->ticket[2], leaf, count, &last)) {
+        double tot = gather_sum_n(partials, count, shd);
         if (t == 0) {
             float sigma = (float)tot;
             st->sigma = sigma;
@@ -867,15 +901,18 @@ __global__ void __launch_bounds__(128) k_pcg_Ap(DLevel L, const float* p, float*
         }
     }
 }
-
-// lines 8-12: r -= alpha q; nu = |r|_inf; convergence / divergence test
-__global__ void __launch_bounds__(128) k_pcg_update_r(DLevel L, const float* q, float* r, double* partials,
-                                                      PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
+__global__ void __launch_bounds__(128) k_pcg_Ap(DLevel L, const float* p, float* q, double* partials, PcgState* st) {
     griddep_wait();
     griddep_launch();
+    pcg_Ap_leaf(L, blockIdx.x, gridDim.x, p, q, partials, st);
+}
+
+// lines 8-12: r -= alpha q; nu = |r|_inf; convergence / divergence test
+__device__ __forceinline__ void pcg_update_r_leaf(int leaf, int count, const float* q, float* r, double* partials,
+                                                  PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ float shf[4];
     __shared__ bool last;
-    const int leaf = blockIdx.x, t = threadIdx.x;
+    const int t = threadIdx.x;
     const float na = -st->alpha;
     float4 qq = ld4(q, leaf, t), rr = ld4(r, leaf, t);
     rr.x = __fmaf_rn(na, qq.x, rr.x);
@@ -885,8 +922,8 @@ __global__ void __launch_bounds__(128) k_pcg_update_r(DLevel L, const float* q, 
     st4(r, leaf, t, rr);
     float a = nanmax(nanmax(absprop(rr.x), absprop(rr.y)), nanmax(absprop(rr.z), absprop(rr.w)));
     float part = block_max128(a, shf);
-    if (publish_partial((double)part, partials, &st->ticket[3], &last)) {
-        float nu = gather_max(partials, shf);
+    if (publish_partial_at((double)part, partials, &st->ticket[3], leaf, count, &last)) {
+        float nu = gather_max_n(partials, count, shf);
         if (t == 0) {
             const int k = st->iter;
             st->nu_old = st->nu;
@@ -909,22 +946,75 @@ __global__ void __launch_bounds__(128) k_pcg_update_r(DLevel L, const float* q, 
         }
     }
 }
-
-// line 10 on success, and line 16 of the last iteration when max_iter is reached
-__global__ void __launch_bounds__(128) k_pcg_finish(DLevel L, const float* p, float* x, const PcgState* st) {
+__global__ void __launch_bounds__(128) k_pcg_update_r(DLevel L, const float* q, float* r, double* partials,
+                                                      PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
     griddep_wait();
     griddep_launch();
+    pcg_update_r_leaf(blockIdx.x, gridDim.x, q, r, partials, st, cond, use_cond);
+}
+
+// line 10 on success, and line 16 of the last iteration when max_iter is reached
+__device__ __forceinline__ bool pcg_finish_applies(const PcgState* st) {
     const int s = st->status;
-    if (s != PCG_SUCCESS && s != PCG_FAILED_MAXITER) return;
-    if (st->iterations_taken == 0 && st->iter == 0) return;  // converged before the loop
-    const int leaf = blockIdx.x, t = threadIdx.x;
+    if (s != PCG_SUCCESS && s != PCG_FAILED_MAXITER) return false;
+    if (st->iterations_taken == 0 && st->iter == 0) return false;  // converged before the loop
+    return true;
+}
+__device__ __forceinline__ float4 pcg_finish_value(int leaf, const float* p, const float* x, const PcgState* st,
+                                                   bool apply) {
+    const int t = threadIdx.x;
+    float4 xx = ld4(x, leaf, t);
+    if (!apply) return xx;
     const float alpha = st->alpha;
-    float4 pp = ld4(p, leaf, t), xx = ld4(x, leaf, t);
+    float4 pp = ld4(p, leaf, t);
     xx.x = __fmaf_rn(alpha, pp.x, xx.x);
     xx.y = __fmaf_rn(alpha, pp.y, xx.y);
     xx.z = __fmaf_rn(alpha, pp.z, xx.z);
     xx.w = __fmaf_rn(alpha, pp.w, xx.w);
-    st4(x, leaf, t, xx);
+    return xx;
+}
+__global__ void __launch_bounds__(128) k_pcg_finish(DLevel L, const float* p, float* x, const PcgState* st) {
+    griddep_wait();
+    griddep_launch();
+    if (!pcg_finish_applies(st)) return;
+    st4(x, blockIdx.x, threadIdx.x, pcg_finish_value(blockIdx.x, p, x, st, true));
+}
+
+// z.r over the DOF (levelDot) and the beta/rho step, for a hierarchy whose
+// level 0 is the coarsest (no sweep is available to carry the dot)
+__device__ __forceinline__ void dot_rho_leaf(const DLevel& L, int leaf, int count, const float* z, const float* r,
+                                             double* partials, PcgState* st) {
+    __shared__ double shd[4];
+    __shared__ bool last;
+    const int t = threadIdx.x;
+    float4 a = ld4(z, leaf, t), c = ld4(r, leaf, t);
+    unsigned m = mask4(L.mask, leaf, t);
+    double s = 0;
+    if (m & 1) s += (double)a.x * c.x;
+    if (m & 2) s += (double)a.y * c.y;
+    if (m & 4) s += (double)a.z * c.z;
+    if (m & 8) s += (double)a.w * c.w;
+    double part = block_sum128(s, shd);
+    if (publish_partial_at(part, partials, &st->ticket[0], leaf, count, &last)) {
+        double tot = gather_sum_n(partials, count, shd);
+        if (t == 0) {
+            float rho_new = (float)tot;
+            st->rho_new = rho_new;
+            st->beta = st->first ? 0.f : __fdiv_rn(rho_new, st->rho);
+            st->rho = rho_new;
+            st->ticket[0] = 0;
+        }
+    }
+}
+
+// v *= DOF mask (inputs of the PCG are zero off the DOF)
+__device__ __forceinline__ float4 masked4(const DLevel& L, int leaf, float4 a) {
+    unsigned m = mask4(L.mask, leaf, threadIdx.x);
+    if (!(m & 1)) a.x = 0.f;
+    if (!(m & 2)) a.y = 0.f;
+    if (!(m & 4)) a.z = 0.f;
+    if (!(m & 8)) a.w = 0.f;
+    return a;
 }
 
 // r = b - A x and |r|_inf (residualApply + levelAbsMax), result in out[0]
