@@ -194,6 +194,42 @@ int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph);
 int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h);
 
 /* ======================================================================== */
+/* Batched pressure solves: PoissonSolver::solveMultigridPCG
+ * (simd_vdb_poisson.cpp:2155-2226) of many independent instances in one CUDA
+ * graph launch.  The reference has no batched form; each instance's result,
+ * iteration count and status are identical to its own solveMultigridPCG.
+ *
+ * A batch references solver handles made by uaamg_poisson_create (hierarchies
+ * of any size and depth); it does not own them, and they must outlive it.
+ * While a batch solve runs, its instances must not be used on their own. */
+typedef struct uaamg_batch uaamg_batch;
+
+int uaamg_batch_create(int count, uaamg_poisson* const* instances, uaamg_batch** out);
+int uaamg_batch_destroy(uaamg_batch* b);
+int uaamg_batch_size(const uaamg_batch* b);
+/* mSmoother, mMaxIteration, mRelativeTolerance for every instance of the
+ * batch (defaults: those of the first instance at creation) */
+int uaamg_batch_set_smoother(uaamg_batch* b, int smoother);
+int uaamg_batch_set_max_iterations(uaamg_batch* b, int max_iterations);
+int uaamg_batch_set_relative_tolerance(uaamg_batch* b, float tolerance);
+/* Solve every instance i: pressure[i] (in: initial guess, out: solution) and
+ * rhs[i] are leaf-dense vectors of instance i (host pointers here, device
+ * pointers in the _device form).  iterations[i] and status[i]
+ * (UAAMG_SUCCESS / UAAMG_FAILED) may be NULL.  Returns UAAMG_SUCCESS when
+ * every instance succeeded, UAAMG_FAILED otherwise, or a negative error. */
+int uaamg_batch_solve_pcg(uaamg_batch* b, float* const* pressure, const float* const* rhs, int* iterations,
+                          int* status);
+int uaamg_batch_solve_pcg_device(uaamg_batch* b, float* const* d_pressure, const float* const* d_rhs,
+                                 int* iterations, int* status);
+/* Per-instance results of the last solve (any pointer may be NULL). */
+int uaamg_batch_results(const uaamg_batch* b, int* iterations, int* status, float* final_residual);
+int uaamg_batch_set_stream(uaamg_batch* b, void* stream);
+/* 1 (default): the CUDA graph with a WHILE node; 0: host-driven loop. */
+int uaamg_batch_set_graph_mode(uaamg_batch* b, int use_graph);
+/* Kernels launched by the last batched solve. */
+int64_t uaamg_batch_kernel_launches(const uaamg_batch* b);
+
+/* ======================================================================== */
 /* Variational viscosity: simd_viscosity3d / L_with_level
  * (SIMD_UAAMG/simd_viscosity3d.h:12-320, simd_viscosity3d.cpp).
  *

@@ -71,6 +71,18 @@ EXPORTS = [
     ("uaamg_poisson_set_stream", i32, [vp, vp]),
     ("uaamg_poisson_set_graph_mode", i32, [vp, i32]),
     ("uaamg_poisson_kernel_launches", i64, [vp]),
+    ("uaamg_batch_create", i32, [i32, vp, C.POINTER(vp)]),
+    ("uaamg_batch_destroy", i32, [vp]),
+    ("uaamg_batch_size", i32, [vp]),
+    ("uaamg_batch_set_smoother", i32, [vp, i32]),
+    ("uaamg_batch_set_max_iterations", i32, [vp, i32]),
+    ("uaamg_batch_set_relative_tolerance", i32, [vp, f32]),
+    ("uaamg_batch_solve_pcg", i32, [vp, vp, vp, vp, vp]),
+    ("uaamg_batch_solve_pcg_device", i32, [vp, vp, vp, vp, vp]),
+    ("uaamg_batch_results", i32, [vp, vp, vp, vp]),
+    ("uaamg_batch_set_stream", i32, [vp, vp]),
+    ("uaamg_batch_set_graph_mode", i32, [vp, i32]),
+    ("uaamg_batch_kernel_launches", i64, [vp]),
     ("uaamg_viscosity_create", i32, [pLG, pLG, pLG, f32, f32, f32, C.POINTER(vp)]),
     ("uaamg_viscosity_destroy", i32, [vp]),
     ("uaamg_viscosity_set_max_iterations", i32, [vp, i32]),

@@ -1,3 +1,4 @@
 // uaamg_lib.cu -- single translation unit of libuaamg_b200.so
 #include "poisson.cu"
+#include "batch.cu"
 #include "viscosity.cu"
