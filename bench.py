@@ -336,6 +336,43 @@ def run_batched(args, dev, stream, timed, max_over_ranks, ws):
     }
 
 
+SERVE_WORKLOAD = ("served stream: Poisson arrivals 200/s and viscosity arrivals 50/s (Poisson process), sides "
+                  "log-uniform in [48,384] voxels, geometry as the batched workload (seeded per request), 1-24 "
+                  "substeps with new face velocities each, pressure warm-started across substeps, hierarchies "
+                  "resident, admission by HBM budget")
+
+
+def run_served(args, ws):
+    """The served stream on this GPU: batched (pressure rounds in one graph,
+    viscosity lanes overlapping) vs the plain form (every solve alone, in
+    arrival order).  Wall-clock latencies from arrival to the last substep."""
+    import torch
+    from uaamg_b200.serve import DeviceBackend, Scheduler, latency_summary, make_stream
+    free, _ = torch.cuda.mem_get_info()
+    out = {"workload": SERVE_WORKLOAD, "window_s": args.serve_window}
+    for mode in ("batched", "plain"):
+        reqs = make_stream(args.serve_window, seed=4)
+        be = DeviceBackend(batching=(mode == "batched"))
+        sch = Scheduler(be, int(0.5 * free))
+        elapsed = sch.run(reqs, time_limit=args.serve_limit)
+        torch.cuda.synchronize()
+        done = sch.done
+        kinds = {}
+        for k in ("poisson", "viscosity"):
+            dk = [r for r in done if r.kind == k]
+            kinds[k] = {"requests": sum(r.kind == k for r in reqs), "completed": len(dk),
+                        "solves": int(sum(r.substeps for r in dk)), **latency_summary(dk)}
+        out[mode] = {"requests": len(reqs), "completed": len(done), "solves": int(sch.solves),
+                     "elapsed_s": round(elapsed, 3), "solves_per_s": round(sch.solves / elapsed, 1),
+                     **latency_summary(done), "by_kind": kinds, "pressure_rounds": sch.rounds,
+                     "batch_graphs_built": be.batch_builds, "peak_budget_GB": round(sch.peak_used / 1e9, 2),
+                     "all_status_success": all(all(s == 0 for s in r.status) for r in done)}
+        del be, sch
+    b, p = out["batched"], out["plain"]
+    out["solves_per_s_vs_plain"] = round(b["solves_per_s"] / p["solves_per_s"], 3) if p["solves_per_s"] else None
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -346,6 +383,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the secondary Poisson measurement")
     ap.add_argument("--batch", type=int, default=64, help="instances of the batched Poisson measurement (0 = skip)")
+    ap.add_argument("--serve-window", type=float, default=0.2,
+                    help="seconds of arrivals of the served request stream (0 = skip)")
+    ap.add_argument("--serve-limit", type=float, default=60.0, help="time limit of each served run (s)")
     ap.add_argument("--no-graph", action="store_true", help="host-driven PCG loop instead of the CUDA graph")
     ap.add_argument("--profile", choices=["solve", "sweep", "vsolve"], default=None,
                     help="short fixed sequence for ncu: 'vsolve' = viscosity build + 2 solves, "
@@ -612,6 +652,11 @@ def main():
     if args.batch > 0:
         batched = run_batched(args, dev, stream, timed, max_over_ranks, ws)
 
+    # ================= served request stream (continuous batching) =================
+    served = None
+    if args.serve_window > 0:
+        served = run_served(args, ws)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -651,6 +696,8 @@ def main():
             line["cpu_baseline"] = vcpu
         if poisson is not None:
             line["poisson"] = poisson
+        if served is not None:
+            line["served"] = served
         if batched is not None:
             line["batched"] = batched
             line["gpu_launches"] = int(line["gpu_launches"] + batched.pop("_launches"))

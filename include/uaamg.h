@@ -76,6 +76,12 @@ typedef struct uaamg_poisson uaamg_poisson;
  * liquid_phi (the reference reads liquid_phi->voxelSize()[0]). */
 int uaamg_poisson_create(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights,
                          float dt, float dx, uaamg_poisson** out);
+/* uaamg_poisson_create with the construction enqueued on `stream` (a
+ * cudaStream_t; NULL = the handle's own stream): it is ordered after the
+ * caller's work on that stream (inputs that stream produced need no host
+ * synchronisation), and the stream stays the handle's (uaamg_poisson_set_stream). */
+int uaamg_poisson_create_on_stream(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights, float dt,
+                                   float dx, void* stream, uaamg_poisson** out);
 /* ~PoissonSolver / ~LaplacianWithLevel */
 int uaamg_poisson_destroy(uaamg_poisson* h);
 
@@ -258,6 +264,11 @@ typedef struct uaamg_viscosity uaamg_viscosity;
 int uaamg_viscosity_create(const uaamg_leaf_grid* viscosity, const uaamg_leaf_grid* liquid_sdf,
                            const uaamg_leaf_grid* solid_sdf, float dt, float rho, float dx,
                            uaamg_viscosity** out);
+/* uaamg_viscosity_create with the construction enqueued on `stream` (see
+ * uaamg_poisson_create_on_stream). */
+int uaamg_viscosity_create_on_stream(const uaamg_leaf_grid* viscosity, const uaamg_leaf_grid* liquid_sdf,
+                                     const uaamg_leaf_grid* solid_sdf, float dt, float rho, float dx, void* stream,
+                                     uaamg_viscosity** out);
 int uaamg_viscosity_destroy(uaamg_viscosity* h);
 /* simd_viscosity3d::m_max_iter (100) */
 int uaamg_viscosity_set_max_iterations(uaamg_viscosity* h, int max_iterations);

@@ -41,6 +41,7 @@ vp, i32, i64, f32 = C.c_void_p, C.c_int, C.c_int64, C.c_float
 pLG = C.POINTER(LeafGridC)
 EXPORTS = [
     ("uaamg_poisson_create", i32, [pLG, pLG, f32, f32, C.POINTER(vp)]),
+    ("uaamg_poisson_create_on_stream", i32, [pLG, pLG, f32, f32, vp, C.POINTER(vp)]),
     ("uaamg_poisson_destroy", i32, [vp]),
     ("uaamg_poisson_set_smoother", i32, [vp, i32]),
     ("uaamg_poisson_set_max_iterations", i32, [vp, i32]),
@@ -84,6 +85,7 @@ EXPORTS = [
     ("uaamg_batch_set_graph_mode", i32, [vp, i32]),
     ("uaamg_batch_kernel_launches", i64, [vp]),
     ("uaamg_viscosity_create", i32, [pLG, pLG, pLG, f32, f32, f32, C.POINTER(vp)]),
+    ("uaamg_viscosity_create_on_stream", i32, [pLG, pLG, pLG, f32, f32, f32, vp, C.POINTER(vp)]),
     ("uaamg_viscosity_destroy", i32, [vp]),
     ("uaamg_viscosity_set_max_iterations", i32, [vp, i32]),
     ("uaamg_viscosity_iterations", i32, [vp]),

@@ -1253,6 +1253,11 @@ int uaamg_device_count(void) {
 
 int uaamg_poisson_create(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights, float dt, float dx,
                          uaamg_poisson** out) {
+    return uaamg_poisson_create_on_stream(liquid_phi, face_weights, dt, dx, nullptr, out);
+}
+
+int uaamg_poisson_create_on_stream(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights, float dt,
+                                   float dx, void* stream, uaamg_poisson** out) {
     {
         const char* e = getenv("UAAMG_PDL");
         g_use_pdl = !(e && e[0] == '0');
@@ -1274,7 +1279,7 @@ int uaamg_poisson_create(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_gri
         CK(ce);
         CK(ctx_stream_acquire(h->ctx, &h->own_stream));
         CK(ctx_stream_acquire(h->ctx, &h->body_stream));
-        h->stream = h->own_stream;
+        h->stream = stream ? (cudaStream_t)stream : h->own_stream;
         CK(ctx_pinned_acquire(h->ctx, sizeof(PcgState) + 256, &h->pin_state, &h->pin_state_cap));
         h->st_host = reinterpret_cast<PcgState*>(h->pin_state);
         h->scalar_host = reinterpret_cast<float*>((char*)h->pin_state + ((sizeof(PcgState) + 63) & ~size_t(63)));

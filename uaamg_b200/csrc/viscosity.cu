@@ -862,6 +862,12 @@ extern "C" {
 
 int uaamg_viscosity_create(const uaamg_leaf_grid* viscosity, const uaamg_leaf_grid* liquid_sdf,
                            const uaamg_leaf_grid* solid_sdf, float dt, float rho, float dx, uaamg_viscosity** out) {
+    return uaamg_viscosity_create_on_stream(viscosity, liquid_sdf, solid_sdf, dt, rho, dx, nullptr, out);
+}
+
+int uaamg_viscosity_create_on_stream(const uaamg_leaf_grid* viscosity, const uaamg_leaf_grid* liquid_sdf,
+                                     const uaamg_leaf_grid* solid_sdf, float dt, float rho, float dx, void* stream,
+                                     uaamg_viscosity** out) {
     {
         const char* e = getenv("UAAMG_PDL");
         g_use_pdl = !(e && e[0] == '0');
@@ -881,7 +887,7 @@ int uaamg_viscosity_create(const uaamg_leaf_grid* viscosity, const uaamg_leaf_gr
         CK(ce);
         CK(ctx_stream_acquire(h->ctx, &h->own_stream));
         CK(ctx_stream_acquire(h->ctx, &h->body_stream));
-        h->stream = h->own_stream;
+        h->stream = stream ? (cudaStream_t)stream : h->own_stream;
         CK(ctx_pinned_acquire(h->ctx, sizeof(PcgState) + 256, &h->pin_state, &h->pin_state_cap));
         h->st_host = reinterpret_cast<PcgState*>(h->pin_state);
         h->scalar_host = reinterpret_cast<float*>((char*)h->pin_state + ((sizeof(PcgState) + 63) & ~size_t(63)));

@@ -61,14 +61,15 @@ class LaplacianWithLevel:
 
     @staticmethod
     def createPressurePoissonLaplacian(liquid_phi: LeafGrid, face_weights: LeafGrid, dt: float,
-                                       dx: float) -> "LaplacianWithLevel":
+                                       dx: float, stream: int | None = None) -> "LaplacianWithLevel":
+        """``stream``: a cudaStream_t (int) to build on; the handle keeps it."""
         L = _lib.lib()
         keep: list = []
         a = _as_c(liquid_phi, keep)
         b = _as_c(face_weights, keep)
         h = C.c_void_p()
-        _lib.check(L.uaamg_poisson_create(C.byref(a), C.byref(b), float(dt), float(dx), C.byref(h)),
-                   "uaamg_poisson_create")
+        _lib.check(L.uaamg_poisson_create_on_stream(C.byref(a), C.byref(b), float(dt), float(dx), stream,
+                                                    C.byref(h)), "uaamg_poisson_create")
         return LaplacianWithLevel(h.value, dt, dx)
 
     def __del__(self):

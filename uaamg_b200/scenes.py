@@ -12,6 +12,7 @@ channels (packed3grids) and a zero solid velocity.
 """
 from __future__ import annotations
 
+import functools
 from dataclasses import dataclass
 
 import numpy as np
@@ -185,3 +186,132 @@ def plain_viscosity_scene(n: int = 128, seed: int = 1, mu: float = 1e3) -> Visco
     rho = 1."""
     return viscosity_box_scene(n, 0.4, [((0.5, 0.7, 0.5), 0.15)], seed, mu,
                                name=f"slab0.4+sphere0.15 {n}^3 mu{mu:g} seed{seed}")
+
+
+# ---------------------------------------------------------------------------
+# Device-side scene construction (served request stream).  Large requests
+# (up to 384^3 voxels) are built directly in HBM with torch: the leaf values
+# live on the device (values_on_device = 1 at the C ABI), origins and masks
+# on the host.
+
+def served_side(seed: int, lo: int = 48, hi: int = 384) -> int:
+    """Domain side log-uniform in [lo, hi] voxels (rounded to a multiple of 8)."""
+    u = float(uniform(seed + 104729, 1, 0.0, 1.0)[0])
+    s = float(np.exp(np.log(lo) + (np.log(hi) - np.log(lo)) * u))
+    return int(max(lo, min(hi, 8 * round(s / 8))))
+
+
+def balls_spheres(seed: int):
+    """1-6 spheres, radii log-uniform in [0.05, 0.3] and centres uniform in the
+    unit box (the geometry of random_balls_scene, box units)."""
+    u = uniform(seed + 7919, 32, 0.0, 1.0).astype(np.float64)
+    k = 1 + min(int(u[1] * 6), 5)
+    out = []
+    for s in range(k):
+        r = float(np.exp(np.log(0.05) + (np.log(0.3) - np.log(0.05)) * u[2 + 4 * s]))
+        out.append(((float(u[3 + 4 * s]), float(u[4 + 4 * s]), float(u[5 + 4 * s])), r))
+    return out
+
+
+def _device_leaf_grid(dense, origin: int, background, components: int) -> LeafGrid:
+    """A dense torch CUDA array [X, Y, Z(, C)] with X, Y, Z multiples of 8 and
+    voxel (0,0,0) at index ``origin`` (all three axes) cut into 8^3 leaves in
+    the order of dense_to_leaves; all voxels active (masks None)."""
+    X, Y, Z = dense.shape[:3]
+    nx, ny, nz = X // 8, Y // 8, Z // 8
+    if components == 1:
+        vals = dense.reshape(nx, 8, ny, 8, nz, 8).permute(0, 2, 4, 1, 3, 5).reshape(-1, LEAF)
+    else:
+        vals = dense.reshape(nx, 8, ny, 8, nz, 8, components).permute(0, 2, 4, 1, 3, 5, 6).reshape(
+            -1, LEAF, components)
+    org = _leaf_origins(nx, ny, nz, origin)
+    g = LeafGrid(origins=np.zeros((0, 3), np.int32),
+                 values=np.zeros((0, LEAF) if components == 1 else (0, LEAF, components), np.float32),
+                 background=background)
+    g.origins = org
+    g.masks = None  # all voxels active (nothing to upload)
+    g.values = vals.contiguous()
+    return g
+
+
+LEAF = 512
+
+
+@functools.lru_cache(maxsize=64)
+def _leaf_origins(nx: int, ny: int, nz: int, origin: int) -> np.ndarray:
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    org = (np.stack([ii.ravel(), jj.ravel(), kk.ravel()], axis=1) * 8 + origin).astype(np.int32)
+    org.setflags(write=False)
+    return org
+
+
+def _device_sdf(n: int, spheres, device, slab_height=None):
+    import torch
+    c = (torch.arange(n, device=device, dtype=torch.float64) + 0.5) / n
+    X, Y, Z = c.view(n, 1, 1), c.view(1, n, 1), c.view(1, 1, n)
+    phi = torch.full((n, n, n), float("inf"), device=device, dtype=torch.float64)
+    if slab_height is not None:
+        phi = torch.minimum(phi, (Y - slab_height).expand(n, n, n))
+    for cen, r in spheres:
+        phi = torch.minimum(phi, torch.sqrt((X - cen[0]) ** 2 + (Y - cen[1]) ** 2 + (Z - cen[2]) ** 2) - r)
+    return torch.clamp(phi, max=3.0 * 4).to(torch.float32)
+
+
+def device_face_velocities(n: int, seed: int, device):
+    """Three face-velocity channels U[-1,1] on the (n+1)^3 face lattice (zero
+    padding up to the next leaf), from a torch generator seeded with ``seed``."""
+    import torch
+    m = n + 8
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed) & 0x7FFFFFFFFFFFFFFF)
+    out = []
+    for _ in range(3):
+        v = torch.zeros((m, m, m), device=device, dtype=torch.float32)
+        v[: n + 1, : n + 1, : n + 1] = torch.rand((n + 1, n + 1, n + 1), generator=gen, device=device) * 2 - 1
+        out.append(_device_leaf_grid(v, 0, 0.0, 1))
+    return out
+
+
+def device_poisson_instance(n: int, seed: int, device):
+    """Pressure inputs of a served request built in HBM: liquid = union of the
+    seeded spheres in an n^3 box (dx = 1/n, dt = 1), walls solid.  Returns
+    (phi, face_weights, solid_velocity, dt, dx)."""
+    import torch
+    assert n % 8 == 0
+    dx = 1.0 / n
+    phi = _device_sdf(n, balls_spheres(seed), device)
+    m = n + 8
+    w = torch.ones((m, m, m, 3), device=device, dtype=torch.float32)
+    f = n + 1  # the face lattice; the padding beyond it keeps the background 1
+    w[0, :f, :f, 0] = 0.0; w[n, :f, :f, 0] = 0.0
+    w[:f, 0, :f, 1] = 0.0; w[:f, n, :f, 1] = 0.0
+    w[:f, :f, 0, 2] = 0.0; w[:f, :f, n, 2] = 0.0
+    phi_g = _device_leaf_grid(phi, 0, np.float32(3.0 * dx), 1)
+    fw_g = _device_leaf_grid(w, 0, np.ones(3, np.float32), 3)
+    sv = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512, 3), np.float32),
+                  background=np.zeros(3, np.float32))
+    return phi_g, fw_g, sv, 1.0, dx
+
+
+def device_viscosity_instance(n: int, seed: int, device, mu: float = 1e3, dt: float = 1.0 / 240.0,
+                              rho: float = 1.0):
+    """Viscosity inputs of a served request built in HBM, in the convention of
+    viscosity_box_scene: liquid SDF (bg 3 dx), solid SDF on the box plus one
+    leaf of margin (nearest wall distance - dx/4, bg -3 dx), constant mu.
+    Returns (liquid_phi, solid_phi, viscosity, solid_velocity, dt, rho, dx)."""
+    import torch
+    assert n % 8 == 0
+    dx = 1.0 / n
+    phi = _device_sdf(n, balls_spheres(seed), device)
+    m = n + 16
+    cs = (torch.arange(m, device=device, dtype=torch.float64) - 8 + 0.5) * dx
+    SX, SY, SZ = cs.view(m, 1, 1), cs.view(1, m, 1), cs.view(1, 1, m)
+    wall = torch.minimum(torch.minimum(torch.minimum(SX, 1.0 - SX), torch.minimum(SY, 1.0 - SY)),
+                         torch.minimum(SZ, 1.0 - SZ)) - 0.25 * dx
+    liquid = _device_leaf_grid(phi, 0, np.float32(3.0 * dx), 1)
+    solid = _device_leaf_grid(wall.to(torch.float32).contiguous(), -8, np.float32(-3.0 * dx), 1)
+    visc = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512), np.float32),
+                    background=np.float32(mu))
+    sv = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512, 3), np.float32),
+                  background=np.zeros(3, np.float32))
+    return liquid, solid, visc, sv, dt, rho, dx

@@ -40,13 +40,14 @@ class L_with_level:
 
     @staticmethod
     def create_viscosity_matrix(viscosity: LeafGrid, liquid_sdf: LeafGrid, solid_sdf: LeafGrid, dt: float,
-                                rho: float, dx: float) -> "L_with_level":
+                                rho: float, dx: float, stream: int | None = None) -> "L_with_level":
+        """``stream``: a cudaStream_t (int) to build on; the handle keeps it."""
         L = _lib.lib()
         keep: list = []
         gs = [_as_c(g, keep) for g in (viscosity, liquid_sdf, solid_sdf)]
         h = C.c_void_p()
-        _lib.check(L.uaamg_viscosity_create(*[C.byref(g) for g in gs], float(dt), float(rho), float(dx),
-                                            C.byref(h)), "uaamg_viscosity_create")
+        _lib.check(L.uaamg_viscosity_create_on_stream(*[C.byref(g) for g in gs], float(dt), float(rho), float(dx),
+                                                      stream, C.byref(h)), "uaamg_viscosity_create")
         return L_with_level(h.value, dt, rho, dx)
 
     def __del__(self):
