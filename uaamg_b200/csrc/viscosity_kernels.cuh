@@ -241,8 +241,11 @@ __device__ __forceinline__ float4 vapply_value(const VLevel& L, const VNbSh& sh,
 // grid (nl, channels): NORMAL / RESIDUAL / JACOBI write all channels of out
 // (blockIdx.y = channel); RED / BLACK update channel c0 of x in place.
 // Voxel groups without DOFs are not written: every vector holds zeros there.
+#ifndef VAPPLY_MINB
+#define VAPPLY_MINB 3  // CTAs per SM: 166 registers, no spills (96 registers at 5 CTAs/SM spill and run 15% slower)
+#endif
 template <int MODE>
-__global__ void __launch_bounds__(128, 5) k_vapply(VLevel L, int c0, const float* x, const float* b, float* out,
+__global__ void __launch_bounds__(128, VAPPLY_MINB) k_vapply(VLevel L, int c0, const float* x, const float* b, float* out,
                                                 float w) {
     griddep_wait();
     griddep_launch();
@@ -661,6 +664,18 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
     __shared__ float red[3][64];
     const int tid = threadIdx.x, n = C.n;
     float x[ROWS], r[ROWS], p[ROWS], z[ROWS], iv[ROWS];
+    // one row per thread: the row's ELL entries stay in registers for the
+    // whole solve (more rows per thread would exceed the 64-register budget
+    // of a 1024-thread CTA; they read the entries through L1 instead)
+    int rc[ROWS == 1 ? VCG_W : 1];
+    float rv[ROWS == 1 ? VCG_W : 1];
+    if (ROWS == 1) {
+#pragma unroll
+        for (int e = 0; e < VCG_W; ++e) {
+            rc[e] = tid < n ? __ldg(C.col + (long long)tid * VCG_W + e) : -1;
+            rv[e] = tid < n ? __ldg(C.val + (long long)tid * VCG_W + e) : 0.f;
+        }
+    }
     float bb = 0.f;
 #pragma unroll
     for (int k = 0; k < ROWS; ++k) {
@@ -694,7 +709,11 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
             for (int k = 0; k < ROWS; ++k) {
                 const int i = tid + k * CG_THREADS;
                 float s = 0.f;
-                if (i < n) {
+                if (ROWS == 1) {
+#pragma unroll
+                    for (int e = 0; e < VCG_W; ++e)
+                        if (rc[e] >= 0) s = __fadd_rn(s, __fmul_rn(rv[e], ps[rc[e]]));
+                } else if (i < n) {
                     const int* cr = C.col + (long long)i * VCG_W;
                     const float* vr = C.val + (long long)i * VCG_W;
 #pragma unroll
