@@ -188,6 +188,142 @@ __device__ __forceinline__ float4 voffdiag(const VLevel& L, const VNbSh& sh, int
     return off;
 }
 
+// The coefficients one applier pass of channel c reads at the thread's
+// voxels.  They do not change during a solve, so k_vapply loads them before it
+// waits for the previous kernel (programmatic dependent launch): only the
+// vector loads remain on the critical path after the wait.
+struct VCoef {
+    float4 wp[3], wm[3];                    // neg_x/y/z at g + e_ax and at g
+    float4 a00, a01, a10, a11;              // m_cross_channel[d2]
+    float4 b00, b01, b10, b11;              // m_cross_channel[d1]
+    float4 dg;                              // 1/diag (GS, Jacobi) or diag (normal, residual)
+};
+template <int MODE>
+__device__ __forceinline__ void vload_coef(const VLevel& L, const VNbSh& sh, int c, int t, VCoef& k) {
+    const int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
+    int e0[3] = {0, 0, 0};
+    e0[d0] = 1;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int px = ax == 0, py = ax == 1, pz = ax == 2;
+        const VArr W = varr(L, c, VA_NEGX + ax);
+        k.wp[ax] = cload4(W, sh, X, Y, Z0, px, py, pz);
+        k.wm[ax] = cload4(W, sh, X, Y, Z0, 0, 0, 0);
+    }
+    k.a00 = cload4(varr(L, d2, VA_T00), sh, X, Y, Z0, 0, 0, 0);
+    k.a01 = cload4(varr(L, d2, VA_T01), sh, X, Y, Z0, 0, 0, 0);
+    k.a10 = cload4(varr(L, d2, VA_T10), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    k.a11 = cload4(varr(L, d2, VA_T11), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    k.b00 = cload4(varr(L, d1, VA_T00), sh, X, Y, Z0, 0, 0, 0);
+    k.b01 = cload4(varr(L, d1, VA_T01), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    k.b10 = cload4(varr(L, d1, VA_T10), sh, X, Y, Z0, 0, 0, 0);
+    k.b11 = cload4(varr(L, d1, VA_T11), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const bool inv = (MODE == VM_RED || MODE == VM_BLACK || MODE == VM_JACOBI);
+    k.dg = cload4(varr(L, c, inv ? VA_INV : VA_DIAG), sh, X, Y, Z0, 0, 0, 0);
+}
+
+// voffdiag with the coefficients already loaded (same operations and order)
+__device__ __forceinline__ float4 voffdiag_k(const VLevel& L, const VNbSh& sh, int c, int t, const float* x,
+                                             const VCoef& k, float4& xc) {
+    const int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
+    int e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0};
+    e0[d0] = 1;
+    e1[d1] = 1;
+    e2[d2] = 1;
+    xc = uload4(x, L, c, sh, X, Y, Z0, 0, 0, 0);
+    float4 fr[6];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int px = ax == 0, py = ax == 1, pz = ax == 2;
+        const float4 up = uload4(x, L, c, sh, X, Y, Z0, px, py, pz);
+        const float4 um = uload4(x, L, c, sh, X, Y, Z0, -px, -py, -pz);
+        const float4 wp = k.wp[ax], wm = k.wm[ax];
+        fr[2 * ax] = make_float4(__fmul_rn(up.x, wp.x), __fmul_rn(up.y, wp.y), __fmul_rn(up.z, wp.z),
+                                 __fmul_rn(up.w, wp.w));
+        fr[2 * ax + 1] = make_float4(__fmul_rn(um.x, wm.x), __fmul_rn(um.y, wm.y), __fmul_rn(um.z, wm.z),
+                                     __fmul_rn(um.w, wm.w));
+    }
+    const float4 u1_g = uload4(x, L, d1, sh, X, Y, Z0, 0, 0, 0);
+    const float4 u1_p1 = uload4(x, L, d1, sh, X, Y, Z0, e1[0], e1[1], e1[2]);
+    const float4 u1_m0 = uload4(x, L, d1, sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 u1_m0p1 = uload4(x, L, d1, sh, X, Y, Z0, e1[0] - e0[0], e1[1] - e0[1], e1[2] - e0[2]);
+    const float4 u2_g = uload4(x, L, d2, sh, X, Y, Z0, 0, 0, 0);
+    const float4 u2_m0 = uload4(x, L, d2, sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 u2_p2 = uload4(x, L, d2, sh, X, Y, Z0, e2[0], e2[1], e2[2]);
+    const float4 u2_m0p2 = uload4(x, L, d2, sh, X, Y, Z0, e2[0] - e0[0], e2[1] - e0[1], e2[2] - e0[2]);
+    float4 off;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float f1 = __fadd_rn(f4get(fr[0], j), f4get(fr[1], j));
+        float f3 = __fadd_rn(f4get(fr[2], j), f4get(fr[3], j));
+        float f5 = __fadd_rn(f4get(fr[4], j), f4get(fr[5], j));
+        f1 = __fadd_rn(f1, f3);
+        f1 = __fadd_rn(f1, f5);
+        const float R0 = __fmul_rn(f4get(u1_g, j), f4get(k.a00, j));
+        const float R1 = __fmul_rn(f4get(k.a01, j), f4get(u1_p1, j));
+        const float R2 = __fmul_rn(f4get(k.a10, j), f4get(u1_m0, j));
+        const float R3 = __fmul_rn(f4get(k.a11, j), f4get(u1_m0p1, j));
+        const float Q0 = __fmul_rn(f4get(k.b00, j), f4get(u2_g, j));
+        const float Q1 = __fmul_rn(f4get(k.b01, j), f4get(u2_m0, j));
+        const float Q2 = __fmul_rn(f4get(k.b10, j), f4get(u2_p2, j));
+        const float Q3 = __fmul_rn(f4get(k.b11, j), f4get(u2_m0p2, j));
+        const float td2 = __fadd_rn(__fadd_rn(R0, R1), __fadd_rn(R2, R3));
+        const float td1 = __fadd_rn(__fadd_rn(Q0, Q1), __fadd_rn(Q2, Q3));
+        f1 = __fadd_rn(f1, td2);
+        f1 = __fadd_rn(f1, td1);
+        f4set(off, j, f1);
+    }
+    return off;
+}
+
+// vapply_value with the coefficients already loaded
+template <int MODE>
+__device__ __forceinline__ float4 vapply_value_k(const VLevel& L, const VNbSh& sh, int c, int t, const float* x,
+                                                 const float* b, float w, unsigned m, const VCoef& k, float4& xc) {
+    const float4 off = voffdiag_k(L, sh, c, t, x, k, xc);
+    const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
+    float4 res = xc;
+    if (MODE == VM_RED || MODE == VM_BLACK) {
+        const float4 bb = uload4(b, L, c, sh, X, Y, Z0, 0, 0, 0);
+        const float4 iv = k.dg;
+        const float one_minus_w = __fsub_rn(1.0f, w);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int par = (X + Y + Z0 + j) & 1;
+            const bool upd = (MODE == VM_RED) ? (par == 0) : (par == 1);
+            float r = __fsub_rn(f4get(bb, j), f4get(off, j));
+            r = __fmul_rn(r, f4get(iv, j));
+            r = __fmul_rn(r, w);
+            const float v = __fmaf_rn(f4get(xc, j), one_minus_w, r);
+            f4set(res, j, upd ? v : f4get(xc, j));
+        }
+    } else if (MODE == VM_NORMAL) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) f4set(res, j, __fmaf_rn(f4get(xc, j), f4get(k.dg, j), f4get(off, j)));
+    } else if (MODE == VM_RESIDUAL) {
+        const float4 bb = uload4(b, L, c, sh, X, Y, Z0, 0, 0, 0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            f4set(res, j, __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(k.dg, j), f4get(off, j))));
+    } else {  // JACOBI: diag from memory, 1/diag preloaded
+        const float4 bb = uload4(b, L, c, sh, X, Y, Z0, 0, 0, 0);
+        const float4 dg = cload4(varr(L, c, VA_DIAG), sh, X, Y, Z0, 0, 0, 0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+            r = __fmul_rn(r, f4get(k.dg, j));
+            f4set(res, j, __fmaf_rn(w, r, f4get(xc, j)));
+        }
+    }
+    if (!(m & 1)) res.x = 0.f;
+    if (!(m & 2)) res.y = 0.f;
+    if (!(m & 4)) res.z = 0.f;
+    if (!(m & 8)) res.w = 0.f;
+    return res;
+}
+
 // One applier pass for channel c at the thread's voxels; m = DOF bits.
 template <int MODE>
 __device__ __forceinline__ float4 vapply_value(const VLevel& L, const VNbSh& sh, int c, int t, const float* x,
@@ -247,16 +383,21 @@ __device__ __forceinline__ float4 vapply_value(const VLevel& L, const VNbSh& sh,
 template <int MODE>
 __global__ void __launch_bounds__(128, VAPPLY_MINB) k_vapply(VLevel L, int c0, const float* x, const float* b, float* out,
                                                 float w) {
-    griddep_wait();
-    griddep_launch();
+    // Static data first (DOF mask, neighbourhood, coefficients): they are
+    // not written during a solve, so they load while the previous kernel is
+    // still running; the vectors are read after griddepcontrol.wait.
     __shared__ VNbSh sh;
     const int leaf = blockIdx.x, t = threadIdx.x;
     const int c = (MODE == VM_RED || MODE == VM_BLACK) ? c0 : (int)blockIdx.y;
     const unsigned m = vmask4(L, c, leaf, t);
     vnb_prologue(L, leaf, sh);
+    VCoef k;
+    if (m) vload_coef<MODE>(L, sh, c, t, k);
+    griddep_wait();
+    griddep_launch();
     if (!m) return;
     float4 xc;
-    const float4 res = vapply_value<MODE>(L, sh, c, t, x, b, w, m, xc);
+    const float4 res = vapply_value_k<MODE>(L, sh, c, t, x, b, w, m, k, xc);
     reinterpret_cast<float4*>(out + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
 }
 
@@ -264,49 +405,58 @@ __global__ void __launch_bounds__(128, VAPPLY_MINB) k_vapply(VLevel L, int c0, c
 // DOF children) * 0.125 * 0.5 * 2, zero at coarse non-DOF voxels
 __device__ __forceinline__ void vrestrict_item(const VLevel& F, const VLevel& C, const float* fine, float* coarse,
                                                int leaf, int c, int t) {
+    // static data (masks, child table) before the wait for the fine vector
     const unsigned m = vmask4(C, c, leaf, t);
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
-    float4 res = f4zero();
+    int fl = -1;
+    uint64_t fw[2] = {0ull, 0ull};  // fine DOF mask words of planes 2X, 2X+1
     if (m) {
         const int q = ((X >= 4) << 2) | ((Y >= 4) << 1) | (Z0 >= 4);
-        const int fl = C.child[leaf * 8 + q];
+        fl = C.child[leaf * 8 + q];
         if (fl >= 0) {
-            const float* fv = fine + ((long long)c * F.nl + fl) * UAAMG_LEAF;
             const uint64_t* fm = F.dof + ((long long)c * F.nl + fl) * 8;
+            fw[0] = fm[(2 * X) & 7];
+            fw[1] = fm[(2 * X + 1) & 7];
+        }
+    }
+    griddep_wait();
+    griddep_launch();
+    float4 res = f4zero();
+    if (m && fl >= 0) {
+        const float* fv = fine + ((long long)c * F.nl + fl) * UAAMG_LEAF;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (!(m >> j & 1)) continue;
-                const int base = voff3(2 * X, 2 * Y, 2 * (Z0 + j));
-                float s = 0.f;
+        for (int j = 0; j < 4; ++j) {
+            if (!(m >> j & 1)) continue;
+            const int base = voff3(2 * X, 2 * Y, 2 * (Z0 + j));
+            float s = 0.f;
 #pragma unroll
-                for (int a = 0; a < 2; ++a)
+            for (int a = 0; a < 2; ++a)
 #pragma unroll
-                    for (int bq = 0; bq < 2; ++bq)
+                for (int bq = 0; bq < 2; ++bq)
 #pragma unroll
-                        for (int k = 0; k < 2; ++k) {
-                            const int fo = base + 64 * a + 8 * bq + k;
-                            if ((fm[fo >> 6] >> (fo & 63)) & 1ull) s = __fadd_rn(s, fv[fo]);
-                        }
-                f4set(res, j, __fmul_rn(__fmul_rn(__fmul_rn(s, 0.125f), 0.5f), 2.0f));
-            }
+                    for (int k = 0; k < 2; ++k) {
+                        const int fo = base + 64 * a + 8 * bq + k;
+                        if ((fw[a] >> (fo & 63)) & 1ull) s = __fadd_rn(s, fv[fo]);
+                    }
+            f4set(res, j, __fmul_rn(__fmul_rn(__fmul_rn(s, 0.125f), 0.5f), 2.0f));
         }
     }
     reinterpret_cast<float4*>(coarse + (long long)c * C.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
 }
 __global__ void __launch_bounds__(128) k_vrestrict(VLevel F, VLevel C, const float* fine, float* coarse) {
-    griddep_wait();
-    griddep_launch();
     vrestrict_item(F, C, fine, coarse, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 
 // prolongation<true> (:2659-2729) for one (fine leaf, channel): fine += coarse parent
 __device__ __forceinline__ void vprolong_item(const VLevel& F, const VLevel& C, const float* coarse, float* fine,
                                               int leaf, int c, int t) {
+    // static data (mask, parent, octant) before the wait for the vectors
     const unsigned m = vmask4(F, c, leaf, t);
-    if (!m) return;
-    const int P = F.parent[leaf];
-    if (P < 0) return;
-    const int oc = F.octant[leaf];
+    const int P = m ? F.parent[leaf] : -1;
+    const int oc = m ? F.octant[leaf] : 0;
+    griddep_wait();
+    griddep_launch();
+    if (!m || P < 0) return;
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     const int cx = ((oc >> 2) & 1) * 4 + (X >> 1), cy = ((oc >> 1) & 1) * 4 + (Y >> 1);
     const float* cv = coarse + ((long long)c * C.nl + P) * UAAMG_LEAF;
@@ -321,8 +471,6 @@ __device__ __forceinline__ void vprolong_item(const VLevel& F, const VLevel& C, 
     *fp = v;
 }
 __global__ void __launch_bounds__(128) k_vprolong(VLevel F, VLevel C, const float* coarse, float* fine) {
-    griddep_wait();
-    griddep_launch();
     vprolong_item(F, C, coarse, fine, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 
@@ -533,15 +681,17 @@ __global__ void __launch_bounds__(128) k_vpcg_update_p(VLevel L, const float* z,
 
 // line 6: q = A p (sigma and alpha follow in k_vdot)
 __global__ void __launch_bounds__(128) k_vpcg_Ap(VLevel L, const float* p, float* q) {
-    griddep_wait();
-    griddep_launch();
     __shared__ VNbSh sh;
     const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
     const unsigned m = vmask4(L, c, leaf, t);
     vnb_prologue(L, leaf, sh);
+    VCoef k;  // static: loaded before the wait for p
+    if (m) vload_coef<VM_NORMAL>(L, sh, c, t, k);
+    griddep_wait();
+    griddep_launch();
     if (!m) return;
     float4 xc;
-    const float4 res = vapply_value<VM_NORMAL>(L, sh, c, t, p, nullptr, 1.f, m, xc);
+    const float4 res = vapply_value_k<VM_NORMAL>(L, sh, c, t, p, nullptr, 1.f, m, k, xc);
     reinterpret_cast<float4*>(q + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
 }
 
@@ -658,8 +808,6 @@ struct DCoarsestV {
 
 template <int ROWS>
 __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, const float* rhs, float* out) {
-    griddep_wait();
-    griddep_launch();
     __shared__ float ps[CG_THREADS * ROWS];
     __shared__ float red[3][64];
     const int tid = threadIdx.x, n = C.n;
@@ -676,14 +824,20 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
             rv[e] = tid < n ? __ldg(C.val + (long long)tid * VCG_W + e) : 0.f;
         }
     }
+    long long sl[ROWS];
+#pragma unroll
+    for (int k = 0; k < ROWS; ++k) {  // static data before the wait for rhs
+        const int i = tid + k * CG_THREADS;
+        sl[k] = i < n ? C.slot[i] : -1;
+        iv[k] = i < n ? C.invd[i] : 0.f;
+    }
+    griddep_wait();
+    griddep_launch();
     float bb = 0.f;
 #pragma unroll
     for (int k = 0; k < ROWS; ++k) {
-        const int i = tid + k * CG_THREADS;
-        const bool ok = i < n;
         x[k] = 0.f;
-        r[k] = ok ? rhs[C.slot[i]] : 0.f;
-        iv[k] = ok ? C.invd[i] : 0.f;
+        r[k] = sl[k] >= 0 ? rhs[sl[k]] : 0.f;
         p[k] = 0.f;
         bb = __fadd_rn(bb, __fmul_rn(r[k], r[k]));
     }
@@ -747,10 +901,8 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
         }
     }
 #pragma unroll
-    for (int k = 0; k < ROWS; ++k) {
-        const int i = tid + k * CG_THREADS;
-        if (i < n) out[C.slot[i]] = x[k];
-    }
+    for (int k = 0; k < ROWS; ++k)
+        if (sl[k] >= 0) out[sl[k]] = x[k];
 }
 
 
