@@ -648,7 +648,7 @@ static void venqueue_body(VEnq& E, cudaGraphConditionalHandle cond, int use_cond
     const VLevelDev& D = h->lv[0];
     const dim3 g((unsigned)D.L.nl, 3);
     enqueue_mucycle(E, 0, h->z, h->r, true);
-    const dim3 gd((unsigned)((3 * D.L.nl + VDOT_THREADS - 1) / VDOT_THREADS));
+    const dim3 gd((unsigned)((3 * D.L.nl + VDOT_ITEMS - 1) / VDOT_ITEMS));
     float* part = reinterpret_cast<float*>(h->partials);
     if (E.prof) E.pb("L0 pcg rho (z.r)");
     launch2(k_vdot, gd, VDOT_THREADS, E.s, D.L, (const float*)h->z, (const float*)h->r, part, h->st, 0);

@@ -577,53 +577,79 @@ __global__ void __launch_bounds__(128) k_vpcg_init(VLevel L, const float* x, con
 // which = 0: rho_new = z.r (line 13; first iteration: rho = rho_new, beta = 0,
 // later beta = rho_new / rho, rho = rho_new); which = 1: sigma = p.q,
 // alpha = rho / sigma (lines 6-7).
-#define VDOT_THREADS 64
+#define VDOT_THREADS 256
+#define VDOT_ITEMS 16      // (channel, leaf) items per CTA
 #define VDOT_CHUNK 2048
+#define VDOT_PITCH 516     // product row pitch (floats): rows start in different banks, 16-byte aligned
+// lv_dot (:3756-3835) in the reference's order: per (channel, leaf) item a
+// sequential float sum of the DOF products in offset order, then the items
+// of each channel in leaf order, then the three channel sums.  A CTA stages
+// the products of VDOT_ITEMS consecutive items in shared memory with
+// coalesced loads; one thread per item then adds them in order.  The CTA
+// that finishes last adds the per-item sums (ticket).
 __global__ void __launch_bounds__(VDOT_THREADS) k_vdot(VLevel L, const float* a, const float* b, float* part,
                                                        PcgState* st, int which) {
-    griddep_wait();
-    griddep_launch();
-    __shared__ __align__(16) float buf[3][VDOT_CHUNK];  // read as float4
+    __shared__ __align__(16) float buf[VDOT_ITEMS * VDOT_PITCH];  // products; reused as [3][VDOT_CHUNK]
+    __shared__ uint64_t mw[VDOT_ITEMS][8];
     __shared__ float cs[3];
     __shared__ bool last;
     const int t = threadIdx.x;
-    const long long item = (long long)blockIdx.x * VDOT_THREADS + t;
-    if (item < 3LL * L.nl) {
-        const float4* pa = reinterpret_cast<const float4*>(a + item * UAAMG_LEAF);
-        const float4* pb = reinterpret_cast<const float4*>(b + item * UAAMG_LEAF);
-        const uint64_t* m = L.dof + item * 8;
+    const long long nitems = 3LL * L.nl;
+    const long long item0 = (long long)blockIdx.x * VDOT_ITEMS;
+    if (t < VDOT_ITEMS * 8) {  // DOF masks: static, loaded before the wait
+        const long long it = item0 + (t >> 3);
+        mw[t >> 3][t & 7] = it < nitems ? L.dof[it * 8 + (t & 7)] : 0ull;
+    }
+    griddep_wait();
+    griddep_launch();
+    // products a*b of every voxel of the CTA's items (non-DOF entries are not read later)
+#pragma unroll 4
+    for (int k = t; k < VDOT_ITEMS * UAAMG_LEAF4; k += VDOT_THREADS) {
+        const int li = k >> 7, q = k & 127;
+        const long long it = item0 + li;
+        float4 pr = f4zero();
+        if (it < nitems) {
+            const float4 x = reinterpret_cast<const float4*>(a + it * UAAMG_LEAF)[q];
+            const float4 y = reinterpret_cast<const float4*>(b + it * UAAMG_LEAF)[q];
+            pr = make_float4(__fmul_rn(x.x, y.x), __fmul_rn(x.y, y.y), __fmul_rn(x.z, y.z), __fmul_rn(x.w, y.w));
+        }
+        *reinterpret_cast<float4*>(buf + li * VDOT_PITCH + 4 * q) = pr;
+    }
+    __syncthreads();
+    if (t < VDOT_ITEMS && item0 + t < nitems) {
+        const float* pr = buf + t * VDOT_PITCH;
         float acc = 0.f;
         for (int q = 0; q < 8; ++q) {
-            const uint64_t word = m[q];
+            const uint64_t word = mw[t][q];
             if (!word) continue;
-#pragma unroll 4
-            for (int k = 0; k < 16; ++k) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {  // DOF in offset order
                 const unsigned nib = (unsigned)(word >> (4 * k)) & 0xFu;
-                if (!nib) continue;
-                const float4 x = pa[q * 16 + k], y = pb[q * 16 + k];
-                if (nib & 1u) acc = __fadd_rn(acc, __fmul_rn(x.x, y.x));
-                if (nib & 2u) acc = __fadd_rn(acc, __fmul_rn(x.y, y.y));
-                if (nib & 4u) acc = __fadd_rn(acc, __fmul_rn(x.z, y.z));
-                if (nib & 8u) acc = __fadd_rn(acc, __fmul_rn(x.w, y.w));
+                const float4 v = *reinterpret_cast<const float4*>(pr + q * 64 + 4 * k);
+                if (nib & 1u) acc = __fadd_rn(acc, v.x);
+                if (nib & 2u) acc = __fadd_rn(acc, v.y);
+                if (nib & 4u) acc = __fadd_rn(acc, v.z);
+                if (nib & 8u) acc = __fadd_rn(acc, v.w);
             }
         }
-        part[item] = acc;
+        part[item0 + t] = acc;
     }
     __threadfence();
     __syncthreads();
     if (t == 0) last = (atomicAdd(&st->ticket[5], 1u) == gridDim.x - 1);
     __syncthreads();
     if (!last) return;
+    float* chunk = buf;  // [3][VDOT_CHUNK] (3 * 2048 <= 16 * 516)
     const int nl = L.nl;
     float acc = 0.f;  // thread c < 3: running sum of channel c
     for (int base = 0; base < nl; base += VDOT_CHUNK) {
         const int len = min(VDOT_CHUNK, nl - base);
         __syncthreads();
         for (int c = 0; c < 3; ++c)
-            for (int i = t; i < len; i += VDOT_THREADS) buf[c][i] = __ldcg(part + (long long)c * nl + base + i);
+            for (int i = t; i < len; i += VDOT_THREADS) chunk[c * VDOT_CHUNK + i] = __ldcg(part + (long long)c * nl + base + i);
         __syncthreads();
         if (t < 3) {
-            const float* bb = buf[t];
+            const float* bb = chunk + t * VDOT_CHUNK;
             int i = 0;
             for (; i + 4 <= len; i += 4) {
                 const float4 v = *reinterpret_cast<const float4*>(bb + i);
