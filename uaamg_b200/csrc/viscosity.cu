@@ -565,7 +565,14 @@ struct VEnq {
         const bool gs = (MODE == VM_RED || MODE == VM_BLACK);
         static const char* names[] = {"normal", "residual", "jacobi", "red_gs", "black_gs"};
         if (prof) pb("L" + std::to_string(l) + " " + names[MODE] + (gs ? " c" + std::to_string(c) : std::string()));
-        launch2(k_vapply<MODE>, dim3((unsigned)D.L.nl, gs ? 1u : 3u), 128, s, D.L, c, x, b, out, 1.0f);
+        if constexpr (MODE == VM_RED || MODE == VM_BLACK) {
+            const dim3 g((unsigned)D.L.nl);
+            if (c == 0) launch2(k_vapply<MODE, 0>, g, 128, s, D.L, x, b, out, 1.0f);
+            else if (c == 1) launch2(k_vapply<MODE, 1>, g, 128, s, D.L, x, b, out, 1.0f);
+            else launch2(k_vapply<MODE, 2>, g, 128, s, D.L, x, b, out, 1.0f);
+        } else {
+            launch2(k_vapply<MODE, -1>, dim3((unsigned)D.L.nl, 3u), 128, s, D.L, x, b, out, 1.0f);
+        }
         pe();
         count++;
     }
@@ -776,6 +783,10 @@ static int vrun_pcg(uaamg_viscosity* h, std::vector<ProfRec>* prof = nullptr) {
     h->last_launches = launches;
     h->launches += launches;
     const PcgState& s = *h->st_host;
+    if (s.error) {
+        set_error("a kernel's bounded wait for its bulk copies timed out");
+        throw UaamgError{UAAMG_ERR_CUDA};
+    }
     h->iterations = s.iterations_taken;
     h->final_residual = s.nu;
     h->status = (s.status == PCG_SUCCESS) ? UAAMG_SUCCESS : UAAMG_FAILED;

@@ -198,9 +198,9 @@ struct VCoef {
     float4 b00, b01, b10, b11;              // m_cross_channel[d1]
     float4 dg;                              // 1/diag (GS, Jacobi) or diag (normal, residual)
 };
-template <int MODE>
-__device__ __forceinline__ void vload_coef(const VLevel& L, const VNbSh& sh, int c, int t, VCoef& k) {
-    const int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+template <int MODE, int c>
+__device__ __forceinline__ void vload_coef(const VLevel& L, const VNbSh& sh, int t, VCoef& k) {
+    constexpr int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     int e0[3] = {0, 0, 0};
     e0[d0] = 1;
@@ -223,10 +223,12 @@ __device__ __forceinline__ void vload_coef(const VLevel& L, const VNbSh& sh, int
     k.dg = cload4(varr(L, c, inv ? VA_INV : VA_DIAG), sh, X, Y, Z0, 0, 0, 0);
 }
 
-// voffdiag with the coefficients already loaded (same operations and order)
-__device__ __forceinline__ float4 voffdiag_k(const VLevel& L, const VNbSh& sh, int c, int t, const float* x,
+// voffdiag with the coefficients already loaded (same operations and order);
+// the channel is a template parameter so every stencil offset is a constant
+template <int c>
+__device__ __forceinline__ float4 voffdiag_k(const VLevel& L, const VNbSh& sh, int t, const float* x,
                                              const VCoef& k, float4& xc) {
-    const int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    constexpr int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     int e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0};
     e0[d0] = 1;
@@ -279,10 +281,10 @@ __device__ __forceinline__ float4 voffdiag_k(const VLevel& L, const VNbSh& sh, i
 }
 
 // vapply_value with the coefficients already loaded
-template <int MODE>
-__device__ __forceinline__ float4 vapply_value_k(const VLevel& L, const VNbSh& sh, int c, int t, const float* x,
+template <int MODE, int c>
+__device__ __forceinline__ float4 vapply_value_k(const VLevel& L, const VNbSh& sh, int t, const float* x,
                                                  const float* b, float w, unsigned m, const VCoef& k, float4& xc) {
-    const float4 off = voffdiag_k(L, sh, c, t, x, k, xc);
+    const float4 off = voffdiag_k<c>(L, sh, t, x, k, xc);
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     float4 res = xc;
     if (MODE == VM_RED || MODE == VM_BLACK) {
@@ -374,31 +376,44 @@ __device__ __forceinline__ float4 vapply_value(const VLevel& L, const VNbSh& sh,
     return res;
 }
 
-// grid (nl, channels): NORMAL / RESIDUAL / JACOBI write all channels of out
-// (blockIdx.y = channel); RED / BLACK update channel c0 of x in place.
-// Voxel groups without DOFs are not written: every vector holds zeros there.
-#ifndef VAPPLY_MINB
-#define VAPPLY_MINB 3  // CTAs per SM: 166 registers, no spills (96 registers at 5 CTAs/SM spill and run 15% slower)
-#endif
-template <int MODE>
-__global__ void __launch_bounds__(128, VAPPLY_MINB) k_vapply(VLevel L, int c0, const float* x, const float* b, float* out,
-                                                float w) {
-    // Static data first (DOF mask, neighbourhood, coefficients): they are
-    // not written during a solve, so they load while the previous kernel is
-    // still running; the vectors are read after griddepcontrol.wait.
-    __shared__ VNbSh sh;
-    const int leaf = blockIdx.x, t = threadIdx.x;
-    const int c = (MODE == VM_RED || MODE == VM_BLACK) ? c0 : (int)blockIdx.y;
+// One applier pass over one leaf and channel c (a constant); m = DOF bits.
+// Static data first (DOF mask, neighbourhood, coefficients): they are not
+// written during a solve, so they load while the previous kernel is still
+// running; the vectors are read after griddepcontrol.wait.
+template <int MODE, int c>
+__device__ __forceinline__ void vapply_leaf(const VLevel& L, VNbSh& sh, int leaf, const float* x, const float* b,
+                                            float* out, float w) {
+    const int t = threadIdx.x;
     const unsigned m = vmask4(L, c, leaf, t);
     vnb_prologue(L, leaf, sh);
     VCoef k;
-    if (m) vload_coef<MODE>(L, sh, c, t, k);
+    if (m) vload_coef<MODE, c>(L, sh, t, k);
     griddep_wait();
     griddep_launch();
     if (!m) return;
     float4 xc;
-    const float4 res = vapply_value_k<MODE>(L, sh, c, t, x, b, w, m, k, xc);
+    const float4 res = vapply_value_k<MODE, c>(L, sh, t, x, b, w, m, k, xc);
     reinterpret_cast<float4*>(out + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
+}
+
+#ifndef VAPPLY_MINB
+#define VAPPLY_MINB 3  // CTAs per SM: no register spills (fewer registers spill and run slower)
+#endif
+// RED / BLACK: one channel C, grid (nl), x updated in place (out == x).
+// NORMAL / RESIDUAL / JACOBI: C = -1, grid (nl, 3), blockIdx.y = channel.
+// Voxel groups without DOFs are not written: every vector holds zeros there.
+template <int MODE, int C>
+__global__ void __launch_bounds__(128, VAPPLY_MINB) k_vapply(VLevel L, const float* x, const float* b, float* out,
+                                                             float w) {
+    __shared__ VNbSh sh;
+    const int leaf = blockIdx.x;
+    if constexpr (C >= 0) {
+        vapply_leaf<MODE, C>(L, sh, leaf, x, b, out, w);
+    } else {
+        if (blockIdx.y == 0) vapply_leaf<MODE, 0>(L, sh, leaf, x, b, out, w);
+        else if (blockIdx.y == 1) vapply_leaf<MODE, 1>(L, sh, leaf, x, b, out, w);
+        else vapply_leaf<MODE, 2>(L, sh, leaf, x, b, out, w);
+    }
 }
 
 // restriction (:2353-2413) for one (coarse leaf, channel): coarse = (sum of the
@@ -708,17 +723,10 @@ __global__ void __launch_bounds__(128) k_vpcg_update_p(VLevel L, const float* z,
 // line 6: q = A p (sigma and alpha follow in k_vdot)
 __global__ void __launch_bounds__(128) k_vpcg_Ap(VLevel L, const float* p, float* q) {
     __shared__ VNbSh sh;
-    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
-    const unsigned m = vmask4(L, c, leaf, t);
-    vnb_prologue(L, leaf, sh);
-    VCoef k;  // static: loaded before the wait for p
-    if (m) vload_coef<VM_NORMAL>(L, sh, c, t, k);
-    griddep_wait();
-    griddep_launch();
-    if (!m) return;
-    float4 xc;
-    const float4 res = vapply_value_k<VM_NORMAL>(L, sh, c, t, p, nullptr, 1.f, m, k, xc);
-    reinterpret_cast<float4*>(q + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
+    const int leaf = blockIdx.x;
+    if (blockIdx.y == 0) vapply_leaf<VM_NORMAL, 0>(L, sh, leaf, p, nullptr, q, 1.f);
+    else if (blockIdx.y == 1) vapply_leaf<VM_NORMAL, 1>(L, sh, leaf, p, nullptr, q, 1.f);
+    else vapply_leaf<VM_NORMAL, 2>(L, sh, leaf, p, nullptr, q, 1.f);
 }
 
 // lines 8-9: r -= alpha q; nu = |r|_inf; stop when nu <= numax or at the
