@@ -328,10 +328,8 @@ static void upload_vlevel(uaamg_viscosity* h, const VHostLevel& H, VLevelDev& D,
     const size_t vb = (size_t)3 * H.nl * UAAMG_LEAF * sizeof(float);
     D.lhs = (float*)valloc(h, vb);
     D.rhs = (float*)valloc(h, vb);
-    D.tmp = (float*)valloc(h, vb);
     CK(cudaMemsetAsync(D.lhs, 0, vb, h->stream));
-    CK(cudaMemsetAsync(D.rhs, 0, vb, h->stream));
-    CK(cudaMemsetAsync(D.tmp, 0, vb, h->stream));
+    CK(cudaMemsetAsync(D.rhs, 0, vb, h->stream));  // restriction leaves voxels without fine leaves untouched
     D.L.coef = (float*)valloc(h, (size_t)27 * H.nl * UAAMG_LEAF * sizeof(float));
     D.L.nbtrim = nullptr;
     D.L.zpage = h->zpage;
@@ -595,6 +593,13 @@ struct VEnq {
         pe();
         count++;
     }
+    // residual of level l restricted into the rhs of level l + 1 (fused)
+    void residual_restrict(int l, const float* x, const float* b, float* coarse) {
+        if (prof) pb("L" + std::to_string(l) + " residual+restrict");
+        launch2(k_vresrestrict, dim3((unsigned)h->lv[l].L.nl, 3), 128, s, h->lv[l].L, h->lv[l + 1].L, x, b, coarse);
+        pe();
+        count++;
+    }
     void prolong(int l, const float* coarse, float* fine) {
         if (prof) pb("L" + std::to_string(l) + " prolong");
         launch2(k_vprolong, dim3((unsigned)h->lv[l].L.nl, 3), 128, s, h->lv[l].L, h->lv[l + 1].L, coarse, fine);
@@ -628,9 +633,8 @@ static void enqueue_mucycle(VEnq& E, int l, float* lhs, const float* rhs, bool f
     if (for_precon) E.zero(l, lhs);
     for (int i = 0; i < 2; ++i) E.rbgs(l, true, lhs, rhs);
     VLevelDev& D = h->lv[l];
-    E.apply<VM_RESIDUAL>(l, 0, lhs, rhs, D.tmp);
     VLevelDev& P = h->lv[l + 1];
-    E.restrict_(l, D.tmp, P.rhs);
+    E.residual_restrict(l, lhs, rhs, P.rhs);
     enqueue_mucycle(E, l + 1, P.lhs, P.rhs, true);
     if (l + 1 != h->nlev - 1) enqueue_mucycle(E, l + 1, P.lhs, P.rhs, false);
     E.prolong(l, P.lhs, lhs);

@@ -462,6 +462,72 @@ __global__ void __launch_bounds__(128) k_vrestrict(VLevel F, VLevel C, const flo
     vrestrict_item(F, C, fine, coarse, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 
+// residual_apply followed by restriction (the two steps of a mu-cycle visit
+// before the coarse visits, :3837-3884) in one pass over the fine leaves: a
+// CTA computes the residual of its fine leaf in shared memory and writes the
+// restricted values of its octant of the parent leaf.  Same operations and
+// summation order as k_vapply<VM_RESIDUAL> + k_vrestrict; the coarse voxels of
+// octants without a fine leaf are never written (they hold no DOF, and the
+// coarse rhs is zero there from allocation).
+template <int c>
+__device__ __forceinline__ void vresrestrict_leaf(const VLevel& F, const VLevel& C, VNbSh& sh, float* rs, int leaf,
+                                                  const float* x, const float* b, float* coarse) {
+    const int t = threadIdx.x;
+    const unsigned m = vmask4(F, c, leaf, t);
+    vnb_prologue(F, leaf, sh);
+    VCoef k;
+    if (m) vload_coef<VM_RESIDUAL, c>(F, sh, t, k);
+    // static: parent, octant, the DOF mask words of this thread's coarse
+    // voxel (t < 64: one of the 4x4x4 coarse voxels of the octant)
+    const int P = F.parent[leaf];
+    const int oc = F.octant[leaf];
+    const int ci = t >> 4, cj = (t >> 2) & 3, ck = t & 3;
+    const int cx = ((oc >> 2) & 1) * 4 + ci, cy = ((oc >> 1) & 1) * 4 + cj, cz = (oc & 1) * 4 + ck;
+    bool cdof = false;
+    uint64_t fw[2] = {0ull, 0ull};
+    if (t < 64 && P >= 0) {
+        cdof = vdof_bit(C, c, P, voff3(cx, cy, cz));
+        const uint64_t* fm = F.dof + ((long long)c * F.nl + leaf) * 8;
+        fw[0] = fm[2 * ci];
+        fw[1] = fm[2 * ci + 1];
+    }
+    griddep_wait();
+    griddep_launch();
+    float4 res = f4zero();
+    if (m) {
+        float4 xc;
+        res = vapply_value_k<VM_RESIDUAL, c>(F, sh, t, x, b, 1.f, m, k, xc);
+    }
+    reinterpret_cast<float4*>(rs)[t] = res;
+    __syncthreads();
+    if (t < 64 && P >= 0) {
+        float s = 0.f;
+        if (cdof) {
+            const int base = voff3(2 * ci, 2 * cj, 2 * ck);
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int bq = 0; bq < 2; ++bq)
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk) {
+                        const int fo = base + 64 * a + 8 * bq + kk;
+                        if ((fw[a] >> (fo & 63)) & 1ull) s = __fadd_rn(s, rs[fo]);
+                    }
+            s = __fmul_rn(__fmul_rn(__fmul_rn(s, 0.125f), 0.5f), 2.0f);
+        }
+        coarse[((long long)c * C.nl + P) * UAAMG_LEAF + voff3(cx, cy, cz)] = s;
+    }
+}
+__global__ void __launch_bounds__(128, VAPPLY_MINB) k_vresrestrict(VLevel F, VLevel C, const float* x, const float* b,
+                                                                   float* coarse) {
+    __shared__ VNbSh sh;
+    __shared__ __align__(16) float rs[UAAMG_LEAF];
+    const int leaf = blockIdx.x;
+    if (blockIdx.y == 0) vresrestrict_leaf<0>(F, C, sh, rs, leaf, x, b, coarse);
+    else if (blockIdx.y == 1) vresrestrict_leaf<1>(F, C, sh, rs, leaf, x, b, coarse);
+    else vresrestrict_leaf<2>(F, C, sh, rs, leaf, x, b, coarse);
+}
+
 // prolongation<true> (:2659-2729) for one (fine leaf, channel): fine += coarse parent
 __device__ __forceinline__ void vprolong_item(const VLevel& F, const VLevel& C, const float* coarse, float* fine,
                                               int leaf, int c, int t) {
