@@ -331,7 +331,6 @@ static void upload_vlevel(uaamg_viscosity* h, const VHostLevel& H, VLevelDev& D,
     CK(cudaMemsetAsync(D.lhs, 0, vb, h->stream));
     CK(cudaMemsetAsync(D.rhs, 0, vb, h->stream));  // restriction leaves voxels without fine leaves untouched
     D.L.coef = (float*)valloc(h, (size_t)27 * H.nl * UAAMG_LEAF * sizeof(float));
-    D.L.nbtrim = nullptr;
     D.L.zpage = h->zpage;
 }
 // [27][512] pages holding each array's applier default (read for missing and
@@ -491,13 +490,11 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
     {
         VLevelDev& D = h->lv[0];
         uint32_t* trim = (uint32_t*)valloc(h, (size_t)(D.L.nl ? D.L.nl : 1) * 4);
-        uint32_t* nbtrim = (uint32_t*)valloc(h, (size_t)(D.L.nl ? D.L.nl : 1) * 27 * 4);
         if (D.L.nl) {
             launch2(k_vtrim, dim3((unsigned)D.L.nl), 128, s, D.L, trim);
-            launch2(k_vnbtrim, dim3((unsigned)D.L.nl), 32, s, D.L, (const uint32_t*)trim, nbtrim);
+            launch2(k_vtrim_fill, dim3((unsigned)D.L.nl), 128, s, D.L, (const uint32_t*)trim, (float*)D.L.coef);
         }
         D.L.trim = trim;
-        D.L.nbtrim = nbtrim;
     }
     // coarsest explicit matrix (construct_exact_solver, :3650)
     {

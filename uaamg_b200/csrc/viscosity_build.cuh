@@ -546,14 +546,21 @@ __global__ void __launch_bounds__(128) k_vtrim(VLevel L, uint32_t* trim) {
     if (t == 0) trim[leaf] = bits;
 }
 
-// trim bits of every leaf's 27 neighbours (0 for missing neighbours)
-__global__ void __launch_bounds__(32) k_vnbtrim(VLevel L, const uint32_t* trim, uint32_t* nbtrim) {
+// A trimmed leaf reads its array's applier default: write that default into
+// the leaf's block of every trimmed array, so the solve kernels read the
+// block as for any other leaf (same values, no trim test per load).
+__global__ void __launch_bounds__(128) k_vtrim_fill(VLevel L, const uint32_t* trim, float* coef) {
     griddep_wait();
     griddep_launch();
-    const int leaf = blockIdx.x, k = threadIdx.x;
-    if (k < 27) {
-        const int lf = L.nb[(long long)leaf * 27 + k];
-        nbtrim[(long long)leaf * 27 + k] = lf >= 0 ? trim[lf] : 0u;
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    const uint32_t bits = trim[leaf];
+    if (!bits) return;
+#pragma unroll 1
+    for (int ca = 0; ca < 3 * VNA; ++ca) {
+        if (!((bits >> ca) & 1u)) continue;
+        const float d = L.app[ca];
+        reinterpret_cast<float4*>(coef + (long long)ca * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] =
+            make_float4(d, d, d, d);
     }
 }
 

@@ -32,7 +32,6 @@ struct VLevel {
     const int* nb;                // [nl][27]
     const float* coef;            // [27][nl][512]
     const uint32_t* trim;         // [nl] bit (c*9+a): leaf holds the default
-    const uint32_t* nbtrim;       // [nl][27] trim bits of each neighbour leaf (nullptr: no trimming)
     const float* defpage;         // [27][512] applier default of every array
     const float* zpage;           // [512] zeros
     const int* parent;            // [nl] coarse leaf, -1 if none
@@ -53,70 +52,62 @@ __device__ __forceinline__ int vnb_index(int X, int Y, int Z) {
 }
 __device__ __forceinline__ int voff3(int X, int Y, int Z) { return ((X & 7) << 6) | ((Y & 7) << 3) | (Z & 7); }
 
-// The 27-neighbourhood of the CTA's leaf with each neighbour's trim bits,
-// staged in shared memory once per CTA: every later load depends only on a
-// shared-memory read, so all of a thread's global loads are in flight
-// together instead of in dependent chains.
+// The 27-neighbourhood of the CTA's leaf, staged in shared memory once per
+// CTA: every later load depends only on a shared-memory read, so all of a
+// thread's global loads are in flight together instead of in dependent
+// chains.  (Trimmed level-0 leaves need no check here: their blocks hold the
+// applier default itself, written by k_vtrim_fill.)
 struct VNbSh {
     int nb[27];
-    uint32_t tr[27];
 };
 // call with all threads of the CTA (contains __syncthreads)
 __device__ __forceinline__ void vnb_prologue(const VLevel& L, int leaf, VNbSh& sh) {
     const int t = threadIdx.x;
-    if (t < 27) {
-        sh.nb[t] = L.nb[(long long)leaf * 27 + t];
-        sh.tr[t] = L.nbtrim ? L.nbtrim[(long long)leaf * 27 + t] : 0u;
-    }
+    if (t < 27) sh.nb[t] = L.nb[(long long)leaf * 27 + t];
     __syncthreads();
 }
 
 // Address of the leaf block holding neighbourhood slot k of array arr: the
-// fallback page when the leaf does not exist or is trimmed for this array.
-__device__ __forceinline__ const float* vsel(const float* arr, const float* fallback, const VNbSh& sh, uint32_t bit,
-                                             int k) {
+// fallback page when the leaf does not exist.
+__device__ __forceinline__ const float* vsel(const float* arr, const float* fallback, const VNbSh& sh, int k) {
     const int lf = sh.nb[k];
-    const bool ok = lf >= 0 && !(sh.tr[k] & bit);
-    return ok ? arr + (long long)lf * UAAMG_LEAF : fallback;
+    return lf >= 0 ? arr + (long long)lf * UAAMG_LEAF : fallback;
 }
 
 // Values of a [nl][512] array at the thread's four voxels shifted by
 // (dx, dy, dz), dz in {-1, 0, 1}: missing leaves read the fallback page
-// (zeros for vectors, the applier default for coefficients), and so do
-// trimmed leaves (bit set in the neighbour's trim bits).
-__device__ __forceinline__ float4 vload4(const float* arr, const float* fb, const VNbSh& sh, uint32_t bit, int x, int y,
-                                         int z0, int dx, int dy, int dz) {
+// (zeros for vectors, the applier default for coefficients).
+__device__ __forceinline__ float4 vload4(const float* arr, const float* fb, const VNbSh& sh, int x, int y, int z0,
+                                         int dx, int dy, int dz) {
     const int X = x + dx, Y = y + dy;
-    const float* p = vsel(arr, fb, sh, bit, vnb_index(X, Y, z0));
+    const float* p = vsel(arr, fb, sh, vnb_index(X, Y, z0));
     const float4 a = *reinterpret_cast<const float4*>(p + voff3(X, Y, z0));
     if (dz == 0) return a;
     if (dz > 0) {
-        const float* q = vsel(arr, fb, sh, bit, vnb_index(X, Y, z0 + 4));
+        const float* q = vsel(arr, fb, sh, vnb_index(X, Y, z0 + 4));
         return make_float4(a.y, a.z, a.w, q[voff3(X, Y, z0 + 4)]);
     }
-    const float* q = vsel(arr, fb, sh, bit, vnb_index(X, Y, z0 - 1));
+    const float* q = vsel(arr, fb, sh, vnb_index(X, Y, z0 - 1));
     return make_float4(q[voff3(X, Y, z0 - 1)], a.x, a.y, a.z);
 }
 
-struct VArr {  // one coefficient array of a level with its trim bit and default page
+struct VArr {  // one coefficient array of a level with its default page
     const float* a;
     const float* def;
-    uint32_t bit;
 };
 __device__ __forceinline__ VArr varr(const VLevel& L, int c, int a) {
     VArr r;
     r.a = L.coef + (long long)(c * VNA + a) * L.nl * UAAMG_LEAF;
     r.def = L.defpage + (c * VNA + a) * UAAMG_LEAF;
-    r.bit = 1u << (c * VNA + a);
     return r;
 }
 __device__ __forceinline__ float4 cload4(const VArr& A, const VNbSh& sh, int x, int y, int z0, int dx, int dy,
                                          int dz) {
-    return vload4(A.a, A.def, sh, A.bit, x, y, z0, dx, dy, dz);
+    return vload4(A.a, A.def, sh, x, y, z0, dx, dy, dz);
 }
 __device__ __forceinline__ float4 uload4(const float* v, const VLevel& L, int c, const VNbSh& sh, int x, int y, int z0,
                                          int dx, int dy, int dz) {
-    return vload4(v + (long long)c * L.nl * UAAMG_LEAF, L.zpage, sh, 0u, x, y, z0, dx, dy, dz);
+    return vload4(v + (long long)c * L.nl * UAAMG_LEAF, L.zpage, sh, x, y, z0, dx, dy, dz);
 }
 
 // Off-diagonal sum of channel c at the thread's four voxels (faced_result[1]
