@@ -502,8 +502,8 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
         VLevelDev& D = h->lv[h->nlev - 1];
         const int n = (int)H.ndof;
         h->C.n = n;
-        if (n > 4 * CG_THREADS) {
-            set_error("coarsest level has %d DOFs (more than %d)", n, 4 * CG_THREADS);
+        if (n > 16 * VCG_THREADS) {
+            set_error("coarsest level has %d DOFs (more than %d)", n, 16 * VCG_THREADS);
             throw UaamgError{UAAMG_ERR_DOMAIN_TOO_LARGE};
         }
         int* col = (int*)valloc(h, (size_t)(n ? n : 1) * VCG_W * 4);
@@ -607,9 +607,10 @@ struct VEnq {
         if (h->C.n == 0) return;
         if (prof) pb("coarsest cg");
         const int n = h->C.n;
-        if (n <= CG_THREADS) launch2(k_vcoarsest_cg<1>, dim3(1), CG_THREADS, s, h->C, rhs, out);
-        else if (n <= 2 * CG_THREADS) launch2(k_vcoarsest_cg<2>, dim3(1), CG_THREADS, s, h->C, rhs, out);
-        else launch2(k_vcoarsest_cg<4>, dim3(1), CG_THREADS, s, h->C, rhs, out);
+        if (n <= 2 * VCG_THREADS) launch2(k_vcoarsest_cg<2>, dim3(1), VCG_THREADS, s, h->C, rhs, out);
+        else if (n <= 4 * VCG_THREADS) launch2(k_vcoarsest_cg<4>, dim3(1), VCG_THREADS, s, h->C, rhs, out);
+        else if (n <= 8 * VCG_THREADS) launch2(k_vcoarsest_cg<8>, dim3(1), VCG_THREADS, s, h->C, rhs, out);
+        else launch2(k_vcoarsest_cg<16>, dim3(1), VCG_THREADS, s, h->C, rhs, out);
         pe();
         count++;
     }

@@ -897,30 +897,64 @@ struct DCoarsestV {
     const float* val;       // [n][15]
 };
 
+// Restatement of Eigen::ConjugateGradient (Upper|Lower, diagonal
+// preconditioner, tolerance FLT_EPSILON, maxIterations 10, zero guess) on the
+// coarsest level, one CTA of VCG_THREADS threads: row i = tid + k *
+// VCG_THREADS, ROWS rows per thread.  With ROWS <= 4 a thread keeps its rows'
+// ELL entries in registers for the whole solve; more rows read them through
+// L1.  Few warps keep the three barriers and two reductions of an iteration
+// short.
+#define VCG_THREADS 256
+#define VCG_WARPS (VCG_THREADS / 32)
+__device__ __forceinline__ float vcg_warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+// block sums in one barrier; every thread gets the same bits
+__device__ __forceinline__ float vcg_block_sum(float v, float* buf) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v = vcg_warp_sum(v);
+    if (lane == 0) buf[w] = v;
+    __syncthreads();
+    return vcg_warp_sum(lane < VCG_WARPS ? buf[lane] : 0.f);
+}
+__device__ __forceinline__ float2 vcg_block_sum2(float a, float b, float* buf) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    a = vcg_warp_sum(a);
+    b = vcg_warp_sum(b);
+    if (lane == 0) {
+        buf[w] = a;
+        buf[32 + w] = b;
+    }
+    __syncthreads();
+    return make_float2(vcg_warp_sum(lane < VCG_WARPS ? buf[lane] : 0.f),
+                       vcg_warp_sum(lane < VCG_WARPS ? buf[32 + lane] : 0.f));
+}
+
 template <int ROWS>
-__global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, const float* rhs, float* out) {
-    __shared__ float ps[CG_THREADS * ROWS];
+__global__ void __launch_bounds__(VCG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, const float* rhs, float* out) {
+    constexpr bool REG = ROWS <= 4;
+    __shared__ float ps[VCG_THREADS * ROWS];
     __shared__ float red[3][64];
     const int tid = threadIdx.x, n = C.n;
     float x[ROWS], r[ROWS], p[ROWS], z[ROWS], iv[ROWS];
-    // one row per thread: the row's ELL entries stay in registers for the
-    // whole solve (more rows per thread would exceed the 64-register budget
-    // of a 1024-thread CTA; they read the entries through L1 instead)
-    int rc[ROWS == 1 ? VCG_W : 1];
-    float rv[ROWS == 1 ? VCG_W : 1];
-    if (ROWS == 1) {
-#pragma unroll
-        for (int e = 0; e < VCG_W; ++e) {
-            rc[e] = tid < n ? __ldg(C.col + (long long)tid * VCG_W + e) : -1;
-            rv[e] = tid < n ? __ldg(C.val + (long long)tid * VCG_W + e) : 0.f;
-        }
-    }
+    int rc[REG ? ROWS : 1][VCG_W];
+    float rv[REG ? ROWS : 1][VCG_W];
     long long sl[ROWS];
+    // static data (rows, 1/diag, slots) before the wait for rhs
 #pragma unroll
-    for (int k = 0; k < ROWS; ++k) {  // static data before the wait for rhs
-        const int i = tid + k * CG_THREADS;
+    for (int k = 0; k < ROWS; ++k) {
+        const int i = tid + k * VCG_THREADS;
         sl[k] = i < n ? C.slot[i] : -1;
         iv[k] = i < n ? C.invd[i] : 0.f;
+        if (REG) {
+#pragma unroll
+            for (int e = 0; e < VCG_W; ++e) {
+                rc[REG ? k : 0][e] = i < n ? __ldg(C.col + (long long)i * VCG_W + e) : -1;
+                rv[REG ? k : 0][e] = i < n ? __ldg(C.val + (long long)i * VCG_W + e) : 0.f;
+            }
+        }
     }
     griddep_wait();
     griddep_launch();
@@ -933,7 +967,7 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
         bb = __fadd_rn(bb, __fmul_rn(r[k], r[k]));
     }
     int rb = 0;
-    const float rhsNorm2 = cg_block_sum(bb, red[rb]);
+    const float rhsNorm2 = vcg_block_sum(bb, red[rb]);
     rb = rb == 2 ? 0 : rb + 1;
     const float threshold = fmaxf(__fmul_rn(__fmul_rn(FLT_EPSILON, FLT_EPSILON), rhsNorm2), FLT_MIN);
     if (rhsNorm2 != 0.f && !(rhsNorm2 < threshold)) {
@@ -943,21 +977,21 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
             p[k] = __fmul_rn(iv[k], r[k]);
             an = __fadd_rn(an, __fmul_rn(r[k], p[k]));
         }
-        float absNew = cg_block_sum(an, red[rb]);
+        float absNew = vcg_block_sum(an, red[rb]);
         rb = rb == 2 ? 0 : rb + 1;
         for (int it = 0; it < 10; ++it) {
 #pragma unroll
-            for (int k = 0; k < ROWS; ++k) ps[tid + k * CG_THREADS] = p[k];
+            for (int k = 0; k < ROWS; ++k) ps[tid + k * VCG_THREADS] = p[k];
             __syncthreads();
             float pt = 0.f, tq[ROWS];
 #pragma unroll
             for (int k = 0; k < ROWS; ++k) {
-                const int i = tid + k * CG_THREADS;
+                const int i = tid + k * VCG_THREADS;
                 float s = 0.f;
-                if (ROWS == 1) {
+                if (REG) {
 #pragma unroll
                     for (int e = 0; e < VCG_W; ++e)
-                        if (rc[e] >= 0) s = __fadd_rn(s, __fmul_rn(rv[e], ps[rc[e]]));
+                        if (rc[REG ? k : 0][e] >= 0) s = __fadd_rn(s, __fmul_rn(rv[REG ? k : 0][e], ps[rc[REG ? k : 0][e]]));
                 } else if (i < n) {
                     const int* cr = C.col + (long long)i * VCG_W;
                     const float* vr = C.val + (long long)i * VCG_W;
@@ -970,7 +1004,7 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
                 tq[k] = s;
                 pt = __fadd_rn(pt, __fmul_rn(p[k], s));
             }
-            const float alpha = __fdiv_rn(absNew, cg_block_sum(pt, red[rb]));
+            const float alpha = __fdiv_rn(absNew, vcg_block_sum(pt, red[rb]));
             rb = rb == 2 ? 0 : rb + 1;
             float rr = 0.f, rz = 0.f;
 #pragma unroll
@@ -981,7 +1015,7 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
                 rr = __fadd_rn(rr, __fmul_rn(r[k], r[k]));
                 rz = __fadd_rn(rz, __fmul_rn(r[k], z[k]));
             }
-            const float2 s2 = cg_block_sum2(rr, rz, red[rb]);
+            const float2 s2 = vcg_block_sum2(rr, rz, red[rb]);
             rb = rb == 2 ? 0 : rb + 1;
             if (s2.x < threshold) break;
             const float absOld = absNew;
@@ -995,6 +1029,5 @@ __global__ void __launch_bounds__(CG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, co
     for (int k = 0; k < ROWS; ++k)
         if (sl[k] >= 0) out[sl[k]] = x[k];
 }
-
 
 }  // namespace uaamg
