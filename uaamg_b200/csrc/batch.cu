@@ -113,17 +113,17 @@ __global__ void __launch_bounds__(128) k_brestrict(const BRec* __restrict__ recs
     restrict_leaf<true>(R.L, e.y, R.v[xr], R.v[br], R.v[BR_CRHS]);
 }
 
-template <int ROWS>
-__global__ void __launch_bounds__(CG_THREADS, 1) k_bcoarsest(const BRec* __restrict__ recs, const int* __restrict__ list,
-                                                             const unsigned* __restrict__ active, int br, int outr) {
+template <int ROWS, int NT>
+__global__ void __launch_bounds__(NT, 1) k_bcoarsest(const BRec* __restrict__ recs, const int* __restrict__ list,
+                                                     const unsigned* __restrict__ active, int br, int outr) {
     griddep_wait();
     griddep_launch();
-    __shared__ float ps[CG_THREADS * ROWS];
+    __shared__ float ps[NT * ROWS];
     __shared__ float red[3][64];
     const int i = list[blockIdx.x];
     if (!active[i]) return;
     const BRec& R = recs[i];
-    coarsest_cg_body<ROWS>(R.C, R.v[br], R.v[outr], ps, red);
+    coarsest_cg_body<ROWS, NT, false>(R.C, R.v[br], R.v[outr], ps, red);
 }
 
 __global__ void __launch_bounds__(128) k_bdot_rho(const BRec* __restrict__ recs, const int2* __restrict__ map,
@@ -300,9 +300,9 @@ struct BEnq {
     void coarsest(int d, int br, int outr, bool dot) {
         const std::array<uaamg_batch::Range, 3>& c = b->coarse[d];
         const unsigned* act = b->active;
-        if (c[0].count) launch(k_bcoarsest<1>, (unsigned)c[0].count, CG_THREADS, s, recs(d), b->lists + c[0].off, act, br, outr);
-        if (c[1].count) launch(k_bcoarsest<2>, (unsigned)c[1].count, CG_THREADS, s, recs(d), b->lists + c[1].off, act, br, outr);
-        if (c[2].count) launch(k_bcoarsest<4>, (unsigned)c[2].count, CG_THREADS, s, recs(d), b->lists + c[2].off, act, br, outr);
+        if (c[0].count) launch(k_bcoarsest<4, 256>, (unsigned)c[0].count, 256, s, recs(d), b->lists + c[0].off, act, br, outr);
+        if (c[1].count) launch(k_bcoarsest<8, 256>, (unsigned)c[1].count, 256, s, recs(d), b->lists + c[1].off, act, br, outr);
+        if (c[2].count) launch(k_bcoarsest<4, 1024>, (unsigned)c[2].count, 1024, s, recs(d), b->lists + c[2].off, act, br, outr);
         count += (c[0].count > 0) + (c[1].count > 0) + (c[2].count > 0);
         if (dot && d == 0 && b->dot1.count) {
             launch(k_bdot_rho, (unsigned)b->dot1.count, 128, s, recs(0), map(b->dot1), act);
@@ -520,7 +520,7 @@ static void bbuild_tables(uaamg_batch* b) {
             for (int i = 0; i < n; ++i) {
                 uaamg_poisson* h = b->inst[i];
                 if (h->lv.empty() || h->lv[0].L.nl == 0 || h->nlev - 1 != d || h->C.n == 0) continue;
-                const int cls = h->C.n <= CG_THREADS ? 0 : (h->C.n <= 2 * CG_THREADS ? 1 : 2);
+                const int cls = coarsest_class(h->C.n);
                 if (cls == k) lists.push_back(i);
             }
             r.count = (int)lists.size() - r.off;

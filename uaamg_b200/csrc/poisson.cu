@@ -55,7 +55,6 @@ struct UaamgError {
         }                                                                                         \
     } while (0)
 #define CHECK_LAUNCH() CK(cudaGetLastError())
-#define BOTTOM_MAX_LEAVES 128
 
 // ---------------------------------------------------------------------------
 // host-side topology helpers
@@ -283,13 +282,6 @@ struct uaamg_poisson {
     float final_residual = 0.f;
     bool spai0_built = false;
     float dt = 0, dx = 0;
-    // bottom of the W-cycle run by k_bottom (levels >= bottom_level), 0 = off
-    int bottom_level = 0;
-    int bottom_cluster = 1;
-    BLevels* d_blevels = nullptr;
-    BStep* d_prog = nullptr;      // program for the skip-first visit, then the full visit
-    int prog_n[2] = {0, 0};
-    int prog_key = -1;
     int64_t solves = 0;
 };
 
@@ -479,8 +471,8 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         }
         const HostLevel& HC = h->host.back();
         size_t nc = (size_t)HC.ndof;
-        if (nc > (size_t)CG_THREADS * CG_MAX_ROWS) {
-            set_error("coarsening stalled: %zu DOF on the coarsest level (max %d)", nc, CG_THREADS * CG_MAX_ROWS);
+        if (nc > (size_t)CG_MAX_DOF) {
+            set_error("coarsening stalled: %zu DOF on the coarsest level (max %d)", nc, CG_MAX_DOF);
             throw UaamgError{UAAMG_ERR_DOMAIN_TOO_LARGE};
         }
         bytes += carve_size(nc, 4) * 3 + carve_size(nc * 6, 4) * 2;
@@ -559,7 +551,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         size_t tot = 0;
         for (auto& u : ups) tot += (u.second.second + 15) & ~size_t(15);
         // kept by the handle until destroy, so create() need not wait for the DMA
-        CK(ctx_pinned_acquire(h->ctx, tot + sizeof(BLevels) + 512, &h->pin_stage, &h->pin_stage_cap));
+        CK(ctx_pinned_acquire(h->ctx, tot + 512, &h->pin_stage, &h->pin_stage_cap));
         char* pin = (char*)h->pin_stage;
         size_t o = 0;
         for (auto& u : ups) {
@@ -593,35 +585,6 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         tofree.clear();
         TRACE("coefficient kernels enqueued");
         h->nlev = nlev;
-        // the bottom of the W-cycle: the deepest run of levels (below level 0)
-        // that each hold at most BOTTOM_MAX_LEAVES leaves
-        h->bottom_level = 0;
-        // Off by default: measured slower than separate PDL launches on the
-        // 128^3 workload (72 us vs ~55 us per level-2 visit), because each
-        // step still pays the L2 round trips and the cluster barrier; kept for
-        // a shared-memory-resident version (UAAMG_BOTTOM=1 enables it).
-        const char* be = getenv("UAAMG_BOTTOM");
-        const bool bottom_on = (be && be[0] == '1');
-        if (bottom_on && nlev >= 2 && nlev <= BOTTOM_MAX_LEVELS) {
-            int bl = nlev - 1, maxnl = 0;
-            while (bl - 1 >= 1 && h->host[bl - 1].nl <= BOTTOM_MAX_LEAVES) bl--;
-            for (int l = bl; l < nlev; ++l) maxnl = std::max(maxnl, h->host[l].nl);
-            h->bottom_level = bl;
-            h->bottom_cluster = std::max(1, std::min(8, (maxnl + BOTTOM_SLOTS - 1) / BOTTOM_SLOTS));
-            BLevels tbl;
-            memset(&tbl, 0, sizeof(tbl));
-            for (int l = 0; l < nlev; ++l) tbl.L[l] = h->lv[l].L;
-            tbl.C = h->C;
-            CK(ctx_dev_alloc(h->ctx, (void**)&h->d_blevels, sizeof(BLevels), s));
-            char* pin = (char*)h->pin_stage + ((o + 255) & ~size_t(255));
-            if ((size_t)(pin - (char*)h->pin_stage) + sizeof(BLevels) <= h->pin_stage_cap) {
-                memcpy(pin, &tbl, sizeof(BLevels));
-                CK(cudaMemcpyAsync(h->d_blevels, pin, sizeof(BLevels), cudaMemcpyHostToDevice, s));
-            } else {
-                CK(cudaMemcpyAsync(h->d_blevels, &tbl, sizeof(BLevels), cudaMemcpyHostToDevice, s));
-                CK(cudaStreamSynchronize(s));
-            }
-        }
     } else {
         h->nlev = 1;
         h->lv.assign(1, LevelDev());
@@ -705,34 +668,11 @@ struct Enq {
         CK(cudaEventRecord(prof->back().b, s));
     }
 
-    std::vector<BStep>* rec = nullptr;  // record steps for k_bottom instead of launching
-
-    static void fill(BStep& st, const SrcPlain& s) { st.src = S_PLAIN; st.x = s.x; }
-    static void fill(BStep& st, const SrcFirstJacobi& s) { st.src = S_FIRST_JACOBI; st.x = s.b; st.alpha = s.w; }
-    static void fill(BStep& st, const SrcFirstSpai0& s) { st.src = S_FIRST_SPAI0; st.x = s.b; st.ready = s.ready; }
-    static void fill(BStep& st, const SrcFirstRbgs& s) { st.src = S_FIRST_RBGS; st.x = s.b; st.red_first = s.red_first; }
-    static void fill(BStep& st, const SrcProlong& s) { st.src = S_PROLONG; st.x = s.x; st.xc = s.xc; st.alpha = s.alpha; }
-
     template <int MODE, class Src>
     void sweep(int l, const Src& src, const float* b, float* out, float w, DotOut dot = DotOut{nullptr, nullptr, nullptr},
                bool mark_spai0 = false) {
         LevelDev& D = h->lv[l];
         float ws = D.w_sor;
-        if (rec) {
-            BStep st = {};
-            st.op = B_SWEEP;
-            st.level = l;
-            st.mode = MODE;
-            fill(st, src);
-            st.b = b;
-            st.out = out;
-            st.mark = mark_spai0 ? D.spai0_ready : nullptr;
-            st.w = w;
-            st.wsor = ws;
-            st.one_minus_wsor = 1.0f - ws;
-            rec->push_back(st);
-            return;
-        }
         if constexpr (std::is_same<Src, SrcPlain>::value) {
             if (g_use_staged && D.L.nl >= STAGED_MIN_LEAVES && !(MODE == M_SPAI0 && mark_spai0)) {
                 if (prof) pb("L" + std::to_string(l) + " " + mode_name(MODE) + " staged" + (dot.r ? "+dot" : ""));
@@ -751,16 +691,6 @@ struct Enq {
     }
     void restrict_resid(int l, const float* x, const float* b) {
         LevelDev& D = h->lv[l];
-        if (rec) {
-            BStep st = {};
-            st.op = B_RESTRICT;
-            st.level = l;
-            st.x = x;
-            st.b = b;
-            st.out = h->lv[l + 1].rhs;
-            rec->push_back(st);
-            return;
-        }
         if (g_use_staged && D.L.nl >= STAGED_MIN_LEAVES) {
             if (prof) pb("L" + std::to_string(l) + " residual+restrict staged");
             launch(k_restrict_staged, (unsigned)D.L.nl, 128, s, D.L, x, b, h->lv[l + 1].rhs, &h->st->error);
@@ -775,20 +705,12 @@ struct Enq {
     }
     void coarsest(const float* rhs, float* out) {
         if (h->C.n == 0) return;
-        if (rec) {
-            BStep st = {};
-            st.op = B_COARSEST;
-            st.level = h->nlev - 1;
-            st.b = rhs;
-            st.out = out;
-            rec->push_back(st);
-            return;
-        }
         pb("coarsest cg");
-        const int n = h->C.n;
-        if (n <= CG_THREADS) launch(k_coarsest_cg<1>, 1, CG_THREADS, s, h->C, rhs, out);
-        else if (n <= 2 * CG_THREADS) launch(k_coarsest_cg<2>, 1, CG_THREADS, s, h->C, rhs, out);
-        else launch(k_coarsest_cg<4>, 1, CG_THREADS, s, h->C, rhs, out);
+        switch (coarsest_class(h->C.n)) {
+            case 0: launch(k_coarsest_cg<4, 256>, 1, 256, s, h->C, rhs, out); break;
+            case 1: launch(k_coarsest_cg<8, 256>, 1, 256, s, h->C, rhs, out); break;
+            default: launch(k_coarsest_cg<4, 1024>, 1, 1024, s, h->C, rhs, out); break;
+        }
         pe();
         count++;
     }
@@ -827,14 +749,8 @@ __global__ void __launch_bounds__(128) k_dot_rho(DLevel L, const float* z, const
 // prolongation-add + first post-smoothing sweep; z.r into the last level-0
 // sweep.  The W-cycle's second visit of the coarsest level re-solves the same
 // system from a zero guess, so it is skipped.
-static void launch_bottom(Enq& E, bool skip_first);
-
 static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool skip_first, DotOut dot) {
     uaamg_poisson* h = E.h;
-    if (!E.rec && h->bottom_level > 0 && l == h->bottom_level) {
-        launch_bottom(E, skip_first);
-        return;
-    }
     LevelDev& D = h->lv[l];
     const int n = 3;
     const int sm = h->smoother;
@@ -911,55 +827,6 @@ static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool sk
 }
 
 static int graph_key(const uaamg_poisson* h);
-
-// Record the two visits of the bottom level (skip-first and full) as step lists.
-static void ensure_bottom_program(uaamg_poisson* h) {
-    if (h->bottom_level <= 0) return;
-    const int key = graph_key(h);
-    if (h->d_prog && h->prog_key == key) return;
-    std::vector<BStep> prog[2];
-    const int l = h->bottom_level;
-    for (int v = 0; v < 2; ++v) {
-        Enq R{h, h->stream};
-        R.rec = &prog[v];
-        enqueue_precond(R, l, h->lv[l].lhs, h->lv[l].rhs, v == 0, DotOut{nullptr, nullptr, nullptr});
-    }
-    const size_t tot = prog[0].size() + prog[1].size();
-    if (!h->d_prog || (size_t)(h->prog_n[0] + h->prog_n[1]) < tot) {
-        if (h->d_prog) CK(cudaFreeAsync(h->d_prog, h->stream));
-        CK(ctx_dev_alloc(h->ctx, (void**)&h->d_prog, tot * sizeof(BStep), h->stream));
-    }
-    std::vector<BStep> all(prog[0]);
-    all.insert(all.end(), prog[1].begin(), prog[1].end());
-    CK(cudaMemcpyAsync(h->d_prog, all.data(), tot * sizeof(BStep), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaStreamSynchronize(h->stream));  // the host vector goes away
-    h->prog_n[0] = (int)prog[0].size();
-    h->prog_n[1] = (int)prog[1].size();
-    h->prog_key = key;
-}
-
-static void launch_bottom(Enq& E, bool skip_first) {
-    uaamg_poisson* h = E.h;
-    const BStep* prog = h->d_prog + (skip_first ? 0 : h->prog_n[0]);
-    const int n = skip_first ? h->prog_n[0] : h->prog_n[1];
-    E.pb("bottom cycle L" + std::to_string(h->bottom_level) + (skip_first ? " (first visit)" : ""));
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(h->bottom_cluster);
-    cfg.blockDim = dim3(BOTTOM_THREADS);
-    cfg.stream = E.s;
-    cudaLaunchAttribute at[2];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = h->bottom_cluster;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[1].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = g_use_pdl ? 2 : 1;
-    CK(cudaLaunchKernelEx(&cfg, k_bottom, prog, n, (const BLevels*)h->d_blevels));
-    E.pe();
-    E.count++;
-}
 
 // muCycleIterative<2> (simd_vdb_poisson.cpp:1979-2110): the MG-as-solver
 // cycle; coarse levels start from whatever their lhs holds, as in the reference.
@@ -1075,7 +942,6 @@ static void destroy_graph(uaamg_poisson* h) {
 
 static void build_graph(uaamg_poisson* h) {
     destroy_graph(h);
-    ensure_bottom_program(h);
     cudaGraph_t g = nullptr;
     CK(cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle cond;
@@ -1154,8 +1020,7 @@ static int run_pcg(uaamg_poisson* h) {
         int iters_run = h->st_host->iter;  // body executions
         launches = h->setup_launches + (int64_t)iters_run * h->body_launches + h->finish_launches;
     } else {
-        ensure_bottom_program(h);
-        Enq E{h, h->stream};
+            Enq E{h, h->stream};
         enqueue_setup(E, 0, 0);
         CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -1302,8 +1167,6 @@ int uaamg_poisson_destroy(uaamg_poisson* h) {
     destroy_graph(h);
     if (h->ctx) {
         if (h->dmem) cudaFreeAsync(h->dmem, h->stream);
-        if (h->d_prog) cudaFreeAsync(h->d_prog, h->stream);
-        if (h->d_blevels) cudaFreeAsync(h->d_blevels, h->stream);
         if (h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
         ctx_pinned_release(h->ctx, h->pin_state, h->pin_state_cap);
         ctx_pinned_release(h->ctx, h->pin_stage, h->pin_stage_cap);
@@ -1639,7 +1502,6 @@ int uaamg_poisson_precondition(uaamg_poisson* h, const float* r, float* z) {
     Scratch S(nb, h->stream);
     CK(cudaMemcpyAsync(S.b, r, nb, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemsetAsync(S.a, 0, nb, h->stream));
-    ensure_bottom_program(h);
     Enq E{h, h->stream};
     enqueue_precond(E, 0, S.a, S.b, true, DotOut{nullptr, nullptr, nullptr});
     CK(cudaMemcpyAsync(z, S.a, nb, cudaMemcpyDeviceToHost, h->stream));
@@ -1730,7 +1592,6 @@ int uaamg_poisson_profile_pcg(uaamg_poisson* h, float* d_pressure, const float* 
     CK(cudaMemcpyAsync(h->x, d_pressure, nb, cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaMemcpyAsync(h->b, d_rhs, nb, cudaMemcpyDeviceToDevice, h->stream));
     init_state(h);
-    ensure_bottom_program(h);
     std::vector<ProfRec> prof;
     Enq E{h, h->stream};
     E.prof = &prof;

@@ -132,6 +132,9 @@ struct SrcProlong {
     }
 };
 
+// source kinds, for kernels that pick one at run time (batched solves)
+enum { S_PLAIN = 0, S_FIRST_JACOBI = 1, S_FIRST_SPAI0 = 2, S_FIRST_RBGS = 3, S_PROLONG = 4 };
+
 // ---------------------------------------------------------------------------
 // The 6-neighbour off-diagonal sum of one float4 (4 z-consecutive voxels):
 // off = ((x+ c_x+ + x- c_x-) + (y+ c_y+ + y- c_y-)) + (z+ c_z+ + z- c_z-)
@@ -1078,8 +1081,12 @@ struct DCoarsest {
     const float* val;      // [n][6]
 };
 
-#define CG_THREADS 1024
-#define CG_MAX_ROWS 4  // CG_THREADS * CG_MAX_ROWS = 4096 > coarsest DOF count (<= 4000)
+// Thread-block shapes of the coarsest CG, by system size (rows per thread,
+// threads): few warps keep the barriers and reductions of an iteration short;
+// the rows' entries stay in registers.  The batched solve uses the same shape
+// for the same size, so its results match the single solve bit for bit.
+#define CG_MAX_DOF 4096
+__host__ __device__ __forceinline__ int coarsest_class(int n) { return n <= 1024 ? 0 : (n <= 2048 ? 1 : 2); }
 
 // Block reductions in one barrier: warps reduce with shfl_down, lane 0 of each
 // warp publishes, every warp reduces the 32 partials the same way and
@@ -1090,13 +1097,15 @@ __device__ __forceinline__ float cg_warp_sum(float v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULLMASK, v, o);
     return __shfl_sync(FULLMASK, v, 0);
 }
+template <int NT>
 __device__ __forceinline__ float cg_block_sum(float v, float* buf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     v = cg_warp_sum(v);
     if (lane == 0) buf[w] = v;
     __syncthreads();
-    return cg_warp_sum(buf[lane]);
+    return cg_warp_sum(lane < NT / 32 ? buf[lane] : 0.f);
 }
+template <int NT>
 __device__ __forceinline__ float2 cg_block_sum2(float a, float b, float* buf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -1106,7 +1115,7 @@ __device__ __forceinline__ float2 cg_block_sum2(float a, float b, float* buf) {
     }
     if (lane == 0) { buf[w] = a; buf[32 + w] = b; }
     __syncthreads();
-    float x = buf[lane], y = buf[32 + lane];
+    float x = lane < NT / 32 ? buf[lane] : 0.f, y = lane < NT / 32 ? buf[32 + lane] : 0.f;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         x += __shfl_down_sync(FULLMASK, x, o);
@@ -1115,21 +1124,22 @@ __device__ __forceinline__ float2 cg_block_sum2(float a, float b, float* buf) {
     return make_float2(__shfl_sync(FULLMASK, x, 0), __shfl_sync(FULLMASK, y, 0));
 }
 
-// ROWS rows per thread (row i = tid + k * CG_THREADS); the matrix rows stay in
-// registers for the whole solve.  Three barriers per CG iteration.
-template <int ROWS>
+// ROWS rows per thread in a block of NT threads (row i = tid + k * NT); the
+// matrix rows stay in registers for the whole solve.  Three barriers per CG
+// iteration.  WAIT: the body itself waits for the previous kernel
+// (griddepcontrol) after loading the matrix, which does not change during a
+// solve; false when the caller has waited already.
+template <int ROWS, int NT, bool WAIT>
 __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float* rhs, float* out, float* ps,
                                                  float (*red)[64]) {
     const int tid = threadIdx.x, n = C.n;
     float x[ROWS], r[ROWS], p[ROWS], z[ROWS], dg[ROWS], iv[ROWS], val[ROWS][6];
-    int col[ROWS][6];
-    float bb = 0.f;
+    int col[ROWS][6], slot[ROWS];
 #pragma unroll
     for (int k = 0; k < ROWS; ++k) {
-        const int i = tid + k * CG_THREADS;
+        const int i = tid + k * NT;
         const bool ok = i < n;
-        x[k] = 0.f;
-        r[k] = ok ? rhs[C.dof_slot[i]] : 0.f;
+        slot[k] = ok ? C.dof_slot[i] : -1;
         dg[k] = ok ? C.diag[i] : 0.f;
         iv[k] = ok ? C.invd[i] : 0.f;
 #pragma unroll
@@ -1137,10 +1147,20 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
             col[k][e] = ok ? C.col[i * 6 + e] : -1;
             val[k][e] = ok ? C.val[i * 6 + e] : 0.f;
         }
+    }
+    if (WAIT) {
+        griddep_wait();
+        griddep_launch();
+    }
+    float bb = 0.f;
+#pragma unroll
+    for (int k = 0; k < ROWS; ++k) {
+        x[k] = 0.f;
+        r[k] = slot[k] >= 0 ? rhs[slot[k]] : 0.f;
         bb = __fadd_rn(bb, __fmul_rn(r[k], r[k]));
     }
     int rb = 0;
-    const float rhsNorm2 = cg_block_sum(bb, red[rb]);
+    const float rhsNorm2 = cg_block_sum<NT>(bb, red[rb]);
     rb = rb == 2 ? 0 : rb + 1;
     const float threshold = fmaxf(__fmul_rn(__fmul_rn(FLT_EPSILON, FLT_EPSILON), rhsNorm2), FLT_MIN);
     // rhsNorm2 == 0 -> x = 0; residualNorm2 (== rhsNorm2 for x = 0) < threshold -> x = 0
@@ -1151,11 +1171,11 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
             p[k] = __fmul_rn(iv[k], r[k]);
             an = __fadd_rn(an, __fmul_rn(r[k], p[k]));
         }
-        float absNew = cg_block_sum(an, red[rb]);
+        float absNew = cg_block_sum<NT>(an, red[rb]);
         rb = rb == 2 ? 0 : rb + 1;
         for (int it = 0; it < 10; ++it) {
 #pragma unroll
-            for (int k = 0; k < ROWS; ++k) ps[tid + k * CG_THREADS] = p[k];
+            for (int k = 0; k < ROWS; ++k) ps[tid + k * NT] = p[k];
             __syncthreads();
             float pt = 0.f, tq[ROWS];
 #pragma unroll
@@ -1167,7 +1187,7 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
                 tq[k] = s;
                 pt = __fadd_rn(pt, __fmul_rn(p[k], s));
             }
-            const float alpha = __fdiv_rn(absNew, cg_block_sum(pt, red[rb]));
+            const float alpha = __fdiv_rn(absNew, cg_block_sum<NT>(pt, red[rb]));
             rb = rb == 2 ? 0 : rb + 1;
             float rr = 0.f, rz = 0.f;
 #pragma unroll
@@ -1178,7 +1198,7 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
                 rr = __fadd_rn(rr, __fmul_rn(r[k], r[k]));
                 rz = __fadd_rn(rz, __fmul_rn(r[k], z[k]));
             }
-            const float2 s2 = cg_block_sum2(rr, rz, red[rb]);
+            const float2 s2 = cg_block_sum2<NT>(rr, rz, red[rb]);
             rb = rb == 2 ? 0 : rb + 1;
             if (s2.x < threshold) break;
             const float absOld = absNew;
@@ -1189,155 +1209,15 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
         }
     }
 #pragma unroll
-    for (int k = 0; k < ROWS; ++k) {
-        const int i = tid + k * CG_THREADS;
-        if (i < n) out[C.dof_slot[i]] = x[k];
-    }
+    for (int k = 0; k < ROWS; ++k)
+        if (slot[k] >= 0) out[slot[k]] = x[k];
 }
 
-template <int ROWS>
-__global__ void __launch_bounds__(CG_THREADS, 1) k_coarsest_cg(DCoarsest C, const float* rhs, float* out) {
-    griddep_wait();
-    griddep_launch();
-    __shared__ float ps[CG_THREADS * ROWS];
+template <int ROWS, int NT>
+__global__ void __launch_bounds__(NT, 1) k_coarsest_cg(DCoarsest C, const float* rhs, float* out) {
+    __shared__ float ps[NT * ROWS];
     __shared__ float red[3][64];  // rotating reduction buffers (no reuse within 2 barriers)
-    coarsest_cg_body<ROWS>(C, rhs, out, ps, red);
-}
-
-// ---------------------------------------------------------------------------
-// Bottom of the W-cycle in one launch.  The coarse levels hold few leaves
-// (tens), so each of their sweeps is a kernel of a few microseconds that is
-// nearly all launch and memory latency.  k_bottom runs a whole recorded visit
-// of such a level -- its sweeps, residual + restriction, the recursive visits
-// below it and the coarsest CG -- as a list of steps inside one thread-block
-// cluster, with a cluster barrier between steps.  Each step runs exactly the
-// device code of the standalone kernel, so results are bit-identical.
-enum { B_SWEEP = 0, B_RESTRICT = 1, B_COARSEST = 2 };
-enum { S_PLAIN = 0, S_FIRST_JACOBI = 1, S_FIRST_SPAI0 = 2, S_FIRST_RBGS = 3, S_PROLONG = 4 };
-
-struct BStep {
-    int op, level, mode, src;
-    const float* x;    // lhs (plain / prolong) or rhs (first-sweep sources)
-    const float* xc;   // coarse vector (prolong)
-    const float* b;
-    float* out;
-    const int* ready;  // SPAI0 first-sweep flag
-    int* mark;         // set by SPAI0 sweeps
-    float w, wsor, one_minus_wsor, alpha;
-    int red_first;
-};
-#define BOTTOM_MAX_LEVELS 32
-struct BLevels {
-    DLevel L[BOTTOM_MAX_LEVELS];
-    DCoarsest C;
-};
-#define BOTTOM_THREADS 1024
-#define BOTTOM_SLOTS (BOTTOM_THREADS / 128)
-
-__device__ __forceinline__ void cluster_sync_all() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-__device__ __forceinline__ unsigned cluster_rank() {
-    unsigned r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ unsigned cluster_size() {
-    unsigned r;
-    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ void slot_barrier(int slot) {
-    asm volatile("bar.sync %0, 128;" ::"r"(slot + 1) : "memory");
-}
-
-template <int MODE, class Src>
-__device__ __forceinline__ void bottom_sweep_leaf(const DLevel& L, int leaf, int t, const Src& src, const BStep& st) {
-    float4 xc;
-    unsigned m;
-    float4 res = sweep_value<MODE>(L, leaf, t, src, st.b, st.w, st.wsor, st.one_minus_wsor, xc, m);
-    st4(st.out, leaf, t, res);
-    if (MODE == M_SPAI0 && st.mark && leaf == 0 && t == 0) *st.mark = 1;
-}
-
-__device__ __noinline__ void bottom_sweep_dispatch(const DLevel& L, int leaf, int t, const BStep& st) {
-    switch (st.src * 8 + st.mode) {
-        case S_PLAIN * 8 + M_JACOBI: bottom_sweep_leaf<M_JACOBI>(L, leaf, t, SrcPlain{st.x}, st); break;
-        case S_FIRST_JACOBI * 8 + M_JACOBI: bottom_sweep_leaf<M_JACOBI>(L, leaf, t, SrcFirstJacobi{st.x, st.alpha}, st); break;
-        case S_PROLONG * 8 + M_JACOBI: bottom_sweep_leaf<M_JACOBI>(L, leaf, t, SrcProlong{st.x, st.xc, st.alpha}, st); break;
-        case S_PLAIN * 8 + M_SPAI0: bottom_sweep_leaf<M_SPAI0>(L, leaf, t, SrcPlain{st.x}, st); break;
-        case S_FIRST_SPAI0 * 8 + M_SPAI0: bottom_sweep_leaf<M_SPAI0>(L, leaf, t, SrcFirstSpai0{st.x, st.ready}, st); break;
-        case S_PROLONG * 8 + M_SPAI0: bottom_sweep_leaf<M_SPAI0>(L, leaf, t, SrcProlong{st.x, st.xc, st.alpha}, st); break;
-        case S_PLAIN * 8 + M_RED: bottom_sweep_leaf<M_RED>(L, leaf, t, SrcPlain{st.x}, st); break;
-        case S_PLAIN * 8 + M_BLACK: bottom_sweep_leaf<M_BLACK>(L, leaf, t, SrcPlain{st.x}, st); break;
-        case S_FIRST_RBGS * 8 + M_BLACK:
-            bottom_sweep_leaf<M_BLACK>(L, leaf, t, SrcFirstRbgs{st.x, st.wsor, st.red_first}, st);
-            break;
-        case S_PROLONG * 8 + M_BLACK: bottom_sweep_leaf<M_BLACK>(L, leaf, t, SrcProlong{st.x, st.xc, st.alpha}, st); break;
-        default: break;
-    }
-}
-
-// residual + restriction of one fine leaf by one 128-thread slot
-__device__ __noinline__ void bottom_restrict_leaf(const DLevel& L, int leaf, int t, const BStep& st, float* rs, int slot) {
-    float4 xc;
-    unsigned m;
-    float4 r = sweep_value<M_RESIDUAL>(L, leaf, t, SrcPlain{st.x}, st.b, 0.f, 0.f, 0.f, xc, m);
-    reinterpret_cast<float4*>(rs)[t] = r;
-    slot_barrier(slot);
-    if (t < 64) {
-        const int i = t >> 4, j = (t >> 2) & 3, k = t & 3;
-        const uint64_t* mk = L.mask + (long long)leaf * 8;
-        float s = 0.f;
-#pragma unroll
-        for (int ii = 0; ii < 2; ++ii)
-#pragma unroll
-            for (int jj = 0; jj < 2; ++jj)
-#pragma unroll
-                for (int kk = 0; kk < 2; ++kk) {
-                    int fo = ((2 * i + ii) << 6) | ((2 * j + jj) << 3) | (2 * k + kk);
-                    if ((mk[fo >> 6] >> (fo & 63)) & 1ull) s = __fadd_rn(s, rs[fo]);
-                }
-        const int o = L.octant[leaf];
-        const int coff = ((((o >> 2) & 1) * 4 + i) << 6) | ((((o >> 1) & 1) * 4 + j) << 3) | ((o & 1) * 4 + k);
-        st.out[(long long)L.parent[leaf] * UAAMG_LEAF + coff] = __fmul_rn(s, 0.125f);
-    }
-    slot_barrier(slot);
-}
-
-__global__ void __launch_bounds__(BOTTOM_THREADS, 1) k_bottom(const BStep* steps, int nsteps, const BLevels* lv) {
-    griddep_wait();
-    griddep_launch();
-    __shared__ float rs[BOTTOM_SLOTS][UAAMG_LEAF];
-    __shared__ float ps[CG_THREADS * CG_MAX_ROWS];
-    __shared__ float red[3][64];
-    __shared__ BStep sst;
-    __shared__ DLevel sl;
-    const int slot = threadIdx.x >> 7, t = threadIdx.x & 127;
-    const int cta = (int)cluster_rank(), ncta = (int)cluster_size();
-    for (int s = 0; s < nsteps; ++s) {
-        if (threadIdx.x == 0) {
-            sst = steps[s];
-            if (sst.op != B_COARSEST) sl = lv->L[sst.level];
-        }
-        __syncthreads();
-        const BStep st = sst;
-        if (st.op == B_COARSEST) {
-            if (cta == 0) {
-                const int n = lv->C.n;
-                if (n <= CG_THREADS) coarsest_cg_body<1>(lv->C, st.b, st.out, ps, red);
-                else if (n <= 2 * CG_THREADS) coarsest_cg_body<2>(lv->C, st.b, st.out, ps, red);
-                else coarsest_cg_body<4>(lv->C, st.b, st.out, ps, red);
-            }
-        } else {
-            const DLevel& L = sl;
-            for (int leaf = cta * BOTTOM_SLOTS + slot; leaf < L.nl; leaf += ncta * BOTTOM_SLOTS) {
-                if (st.op == B_SWEEP) bottom_sweep_dispatch(L, leaf, t, st);
-                else bottom_restrict_leaf(L, leaf, t, st, rs[slot], slot);
-            }
-        }
-        cluster_sync_all();
-    }
+    coarsest_cg_body<ROWS, NT, true>(C, rhs, out, ps, red);
 }
 
 }  // namespace uaamg
