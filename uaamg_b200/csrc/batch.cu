@@ -76,14 +76,14 @@ __device__ __forceinline__ void batch_refresh_active(const BRec* recs0, int n, u
     }
 }
 
+// The block map and the records do not change during a solve: they and the
+// static stencil data load before the wait; the instance's active flag is
+// read after it.
 template <int MODE, int SRC>
-__global__ void __launch_bounds__(128) k_bsweep(const BRec* __restrict__ recs, const int2* __restrict__ map,
-                                                const unsigned* __restrict__ active, int xr, int br, int outr,
+__global__ void __launch_bounds__(128, 7) k_bsweep(const BRec* __restrict__ recs, const int2* __restrict__ map,
+                                                const unsigned* active, int xr, int br, int outr,
                                                 float w, float wsrc, int dot, int mark) {
-    griddep_wait();
-    griddep_launch();
     const int2 e = map[blockIdx.x];
-    if (!active[e.x]) return;
     const BRec& R = recs[e.x];
     const DLevel& L = R.L;
     const float ws = R.w_sor;
@@ -91,26 +91,28 @@ __global__ void __launch_bounds__(128) k_bsweep(const BRec* __restrict__ recs, c
     int* ready = mark ? R.spai0_ready : nullptr;
     const float* b = R.v[br];
     float* out = R.v[outr];
+    const unsigned* g = active + e.x;
     if (SRC == S_PLAIN)
-        sweep_leaf<MODE>(L, e.y, L.nl, SrcPlain{R.v[xr]}, b, out, w, ws, 1.0f - ws, d, ready);
+        sweep_leaf<MODE, SrcPlain, true>(L, e.y, L.nl, SrcPlain{R.v[xr]}, b, out, w, ws, 1.0f - ws, d, ready, g);
     else if (SRC == S_FIRST_JACOBI)
-        sweep_leaf<MODE>(L, e.y, L.nl, SrcFirstJacobi{b, wsrc}, b, out, w, ws, 1.0f - ws, d, ready);
+        sweep_leaf<MODE, SrcFirstJacobi, true>(L, e.y, L.nl, SrcFirstJacobi{b, wsrc}, b, out, w, ws, 1.0f - ws, d,
+                                               ready, g);
     else if (SRC == S_FIRST_SPAI0)
-        sweep_leaf<MODE>(L, e.y, L.nl, SrcFirstSpai0{b, R.spai0_ready}, b, out, w, ws, 1.0f - ws, d, ready);
+        sweep_leaf<MODE, SrcFirstSpai0, true>(L, e.y, L.nl, SrcFirstSpai0{b, R.spai0_ready}, b, out, w, ws,
+                                              1.0f - ws, d, ready, g);
     else if (SRC == S_FIRST_RBGS)
-        sweep_leaf<MODE>(L, e.y, L.nl, SrcFirstRbgs{b, ws, 1}, b, out, w, ws, 1.0f - ws, d, ready);
+        sweep_leaf<MODE, SrcFirstRbgs, true>(L, e.y, L.nl, SrcFirstRbgs{b, ws, 1}, b, out, w, ws, 1.0f - ws, d,
+                                             ready, g);
     else
-        sweep_leaf<MODE>(L, e.y, L.nl, SrcProlong{R.v[xr], R.v[BR_CLHS], 1.0f}, b, out, w, ws, 1.0f - ws, d, ready);
+        sweep_leaf<MODE, SrcProlong, true>(L, e.y, L.nl, SrcProlong{R.v[xr], R.v[BR_CLHS], 1.0f}, b, out, w, ws,
+                                           1.0f - ws, d, ready, g);
 }
 
-__global__ void __launch_bounds__(128) k_brestrict(const BRec* __restrict__ recs, const int2* __restrict__ map,
-                                                   const unsigned* __restrict__ active, int xr, int br) {
-    griddep_wait();
-    griddep_launch();
+__global__ void __launch_bounds__(128, 7) k_brestrict(const BRec* __restrict__ recs, const int2* __restrict__ map,
+                                                   const unsigned* active, int xr, int br) {
     const int2 e = map[blockIdx.x];
-    if (!active[e.x]) return;
     const BRec& R = recs[e.x];
-    restrict_leaf<true>(R.L, e.y, R.v[xr], R.v[br], R.v[BR_CRHS]);
+    restrict_leaf<true, true>(R.L, e.y, R.v[xr], R.v[br], R.v[BR_CRHS], active + e.x);
 }
 
 template <int ROWS, int NT>

@@ -139,89 +139,94 @@ enum { S_PLAIN = 0, S_FIRST_JACOBI = 1, S_FIRST_SPAI0 = 2, S_FIRST_RBGS = 3, S_P
 // The 6-neighbour off-diagonal sum of one float4 (4 z-consecutive voxels):
 // off = ((x+ c_x+ + x- c_x-) + (y+ c_y+ + y- c_y-)) + (z+ c_z+ + z- c_z-)
 // with c_k- this voxel's minus-face entry and c_k+ the +k neighbour's.
-template <class Src>
-__device__ __forceinline__ void stencil4(const DLevel& L, int leaf, int t, const Src& src, float4& xc,
-                                         float4& off) {
+// A thread's static stencil data: the leaf's flags, the neighbour leaves it
+// reads and the face coefficients.  None of it changes during a solve, so the
+// sweep kernels load it before waiting for the previous kernel.
+struct PStatic {
+    unsigned fl;
+    int nxp, nxm, nyp, nym, nzm, nzp;  // neighbour leaves this thread reads (-1: absent or not needed)
+    float4 cxp, cyp, cxm, cym, czo;    // c_x+, c_y+ (neighbour faces), c_x-, c_y-, c_z- of the 4 voxels
+    float czp3;                        // c_z+ of the last voxel
+};
+__device__ __forceinline__ void stencil_static(const DLevel& L, int leaf, int t, PStatic& S) {
     const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
     const unsigned fl = L.flags[leaf];
     const int* nb = L.nbr + (long long)leaf * 6;
     const float df = L.def_face;
     const float4 dfv = f4splat(df);
-    xc = src.get4(L, leaf, t);
-    float4 xp, xm, yp, ym, cxp, cyp;
+    S.fl = fl;
+    S.nxp = S.nxm = S.nyp = S.nym = S.nzm = S.nzp = -1;
     if (X < 7) {
-        xp = src.get4(L, leaf, t + 16);
-        cxp = (fl & TRIM_X) ? dfv : ld4(L.cx, leaf, t + 16);
+        S.cxp = (fl & TRIM_X) ? dfv : ld4(L.cx, leaf, t + 16);
     } else {
-        int n = nb[1];
-        if (n >= 0) {
-            xp = src.get4(L, n, t - 112);
-            cxp = (L.flags[n] & TRIM_X) ? dfv : ld4(L.cx, n, t - 112);
-        } else {
-            xp = f4zero();
-            cxp = dfv;
-        }
+        const int n = nb[1];
+        S.nxp = n;
+        S.cxp = n >= 0 ? ((L.flags[n] & TRIM_X) ? dfv : ld4(L.cx, n, t - 112)) : dfv;
     }
-    if (X > 0) {
-        xm = src.get4(L, leaf, t - 16);
-    } else {
-        int n = nb[0];
-        xm = (n >= 0) ? src.get4(L, n, t + 112) : f4zero();
-    }
+    if (X == 0) S.nxm = nb[0];
     if (Y < 7) {
-        yp = src.get4(L, leaf, t + 2);
-        cyp = (fl & TRIM_Y) ? dfv : ld4(L.cy, leaf, t + 2);
+        S.cyp = (fl & TRIM_Y) ? dfv : ld4(L.cy, leaf, t + 2);
     } else {
-        int n = nb[3];
-        if (n >= 0) {
-            yp = src.get4(L, n, t - 14);
-            cyp = (L.flags[n] & TRIM_Y) ? dfv : ld4(L.cy, n, t - 14);
-        } else {
-            yp = f4zero();
-            cyp = dfv;
-        }
+        const int n = nb[3];
+        S.nyp = n;
+        S.cyp = n >= 0 ? ((L.flags[n] & TRIM_Y) ? dfv : ld4(L.cy, n, t - 14)) : dfv;
     }
-    if (Y > 0) {
-        ym = src.get4(L, leaf, t - 2);
+    if (Y == 0) S.nym = nb[2];
+    S.cxm = (fl & TRIM_X) ? dfv : ld4(L.cx, leaf, t);
+    S.cym = (fl & TRIM_Y) ? dfv : ld4(L.cy, leaf, t);
+    S.czo = (fl & TRIM_Z) ? dfv : ld4(L.cz, leaf, t);
+    S.czp3 = df;
+    if (zh == 0) {
+        S.nzm = nb[4];
     } else {
-        int n = nb[2];
-        ym = (n >= 0) ? src.get4(L, n, t + 14) : f4zero();
+        const int n = nb[5];
+        S.nzp = n;
+        if (n >= 0) S.czp3 = (L.flags[n] & TRIM_Z) ? df : L.cz[(long long)n * UAAMG_LEAF + 4 * t - 4];
     }
-    const float4 cxm = (fl & TRIM_X) ? dfv : ld4(L.cx, leaf, t);
-    const float4 cym = (fl & TRIM_Y) ? dfv : ld4(L.cy, leaf, t);
-    const float4 czo = (fl & TRIM_Z) ? dfv : ld4(L.cz, leaf, t);
+}
+
+// The 6-neighbour off-diagonal sum of one float4 (4 z-consecutive voxels):
+// off = ((x+ c_x+ + x- c_x-) + (y+ c_y+ + y- c_y-)) + (z+ c_z+ + z- c_z-)
+// with c_k- this voxel's minus-face entry and c_k+ the +k neighbour's.
+template <class Src>
+__device__ __forceinline__ void stencil_dyn(const DLevel& L, int leaf, int t, const Src& src, const PStatic& S,
+                                            float4& xc, float4& off) {
+    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
+    xc = src.get4(L, leaf, t);
+    float4 xp, xm, yp, ym;
+    if (X < 7) xp = src.get4(L, leaf, t + 16);
+    else xp = S.nxp >= 0 ? src.get4(L, S.nxp, t - 112) : f4zero();
+    if (X > 0) xm = src.get4(L, leaf, t - 16);
+    else xm = S.nxm >= 0 ? src.get4(L, S.nxm, t + 112) : f4zero();
+    if (Y < 7) yp = src.get4(L, leaf, t + 2);
+    else yp = S.nyp >= 0 ? src.get4(L, S.nyp, t - 14) : f4zero();
+    if (Y > 0) ym = src.get4(L, leaf, t - 2);
+    else ym = S.nym >= 0 ? src.get4(L, S.nym, t + 14) : f4zero();
     const float px = __shfl_xor_sync(FULLMASK, xc.x, 1);
     const float pw = __shfl_xor_sync(FULLMASK, xc.w, 1);
-    const float pcz = __shfl_xor_sync(FULLMASK, czo.x, 1);
+    const float pcz = __shfl_xor_sync(FULLMASK, S.czo.x, 1);
     const int base = 4 * t;
     float zp3, zm0, czp3;
     if (zh == 0) {
         zp3 = px;
         czp3 = pcz;
-        int n = nb[4];
-        zm0 = (n >= 0) ? src.get1(L, n, base + 7) : 0.f;
+        zm0 = (S.nzm >= 0) ? src.get1(L, S.nzm, base + 7) : 0.f;
     } else {
         zm0 = pw;
-        int n = nb[5];
-        if (n >= 0) {
-            zp3 = src.get1(L, n, base - 4);
-            czp3 = (L.flags[n] & TRIM_Z) ? df : L.cz[(long long)n * UAAMG_LEAF + base - 4];
-        } else {
-            zp3 = 0.f;
-            czp3 = df;
-        }
+        zp3 = (S.nzp >= 0) ? src.get1(L, S.nzp, base - 4) : 0.f;
+        czp3 = S.czp3;
     }
     const float zp[4] = {xc.y, xc.z, xc.w, zp3};
     const float zm[4] = {zm0, xc.x, xc.y, xc.z};
-    const float czp[4] = {czo.y, czo.z, czo.w, czp3};
+    const float czp[4] = {S.czo.y, S.czo.z, S.czo.w, czp3};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        float f1 = __fmul_rn(f4get(xp, j), f4get(cxp, j));
-        float f2 = __fmul_rn(f4get(xm, j), f4get(cxm, j));
-        float f3 = __fmul_rn(f4get(yp, j), f4get(cyp, j));
-        float f4 = __fmul_rn(f4get(ym, j), f4get(cym, j));
+        float f1 = __fmul_rn(f4get(xp, j), f4get(S.cxp, j));
+        float f2 = __fmul_rn(f4get(xm, j), f4get(S.cxm, j));
+        float f3 = __fmul_rn(f4get(yp, j), f4get(S.cyp, j));
+        float f4 = __fmul_rn(f4get(ym, j), f4get(S.cym, j));
         float f5 = __fmul_rn(zp[j], czp[j]);
-        float f6 = __fmul_rn(zm[j], f4get(czo, j));
+        float f6 = __fmul_rn(zm[j], f4get(S.czo, j));
         f1 = __fadd_rn(f1, f2);
         f3 = __fadd_rn(f3, f4);
         f5 = __fadd_rn(f5, f6);
@@ -229,6 +234,14 @@ __device__ __forceinline__ void stencil4(const DLevel& L, int leaf, int t, const
         f1 = __fadd_rn(f1, f5);
         f4set(off, j, f1);
     }
+}
+
+template <class Src>
+__device__ __forceinline__ void stencil4(const DLevel& L, int leaf, int t, const Src& src, float4& xc,
+                                         float4& off) {
+    PStatic S;
+    stencil_static(L, leaf, t, S);
+    stencil_dyn(L, leaf, t, src, S, xc, off);
 }
 
 // ---------------------------------------------------------------------------
@@ -305,17 +318,36 @@ struct DotOut {            // optional fused z.r for the PCG (rho_new, beta)
     PcgState* st;
 };
 
+// A thread's static sweep data: the stencil's, the DOF bits and the
+// diagonal terms the mode reads.
+struct SStatic {
+    PStatic P;
+    unsigned m;
+    float4 dg, iv, sp;
+};
+template <int MODE>
+__device__ __forceinline__ void sweep_static(const DLevel& L, int leaf, int t, SStatic& S) {
+    stencil_static(L, leaf, t, S.P);
+    S.m = mask4(L.mask, leaf, t);
+    const unsigned fl = S.P.fl;
+    if (MODE != M_RED && MODE != M_BLACK)
+        S.dg = (fl & TRIM_DIAG) ? f4splat(L.def_diag) : ld4(L.diag, leaf, t);
+    if (MODE == M_RED || MODE == M_BLACK || MODE == M_JACOBI)
+        S.iv = (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : ld4(L.invdiag, leaf, t);
+    if (MODE == M_SPAI0) S.sp = (fl & TRIM_SPAI0) ? f4splat(L.def_spai0) : ld4(L.spai0, leaf, t);
+}
+
 template <int MODE, class Src>
-__device__ __forceinline__ float4 sweep_value(const DLevel& L, int leaf, int t, const Src& src, const float* b,
-                                              float w, float wsor, float one_minus_wsor, float4& xc, unsigned& m) {
+__device__ __forceinline__ float4 sweep_value_s(const DLevel& L, int leaf, int t, const Src& src, const float* b,
+                                                float w, float wsor, float one_minus_wsor, const SStatic& S,
+                                                float4& xc, unsigned& m) {
     float4 off;
-    stencil4(L, leaf, t, src, xc, off);
-    m = mask4(L.mask, leaf, t);
-    const unsigned fl = L.flags[leaf];
+    stencil_dyn(L, leaf, t, src, S.P, xc, off);
+    m = S.m;
     float4 res = f4zero();
     if (MODE == M_RED || MODE == M_BLACK) {
         const float4 bb = ld4(b, leaf, t);
-        const float4 iv = (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : ld4(L.invdiag, leaf, t);
+        const float4 iv = S.iv;
         const int X = t >> 4, Y = (t >> 1) & 7;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -328,7 +360,7 @@ __device__ __forceinline__ float4 sweep_value(const DLevel& L, int leaf, int t, 
             f4set(res, j, upd ? v : f4get(xc, j));
         }
     } else {
-        const float4 dg = (fl & TRIM_DIAG) ? f4splat(L.def_diag) : ld4(L.diag, leaf, t);
+        const float4 dg = S.dg;
         if (MODE == M_LAPLACIAN) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) f4set(res, j, __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
@@ -339,7 +371,7 @@ __device__ __forceinline__ float4 sweep_value(const DLevel& L, int leaf, int t, 
                 for (int j = 0; j < 4; ++j)
                     f4set(res, j, __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j))));
             } else if (MODE == M_JACOBI) {
-                const float4 iv = (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : ld4(L.invdiag, leaf, t);
+                const float4 iv = S.iv;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
@@ -347,7 +379,7 @@ __device__ __forceinline__ float4 sweep_value(const DLevel& L, int leaf, int t, 
                     f4set(res, j, __fmaf_rn(w, r, f4get(xc, j)));
                 }
             } else {  // SPAI0
-                const float4 sp = (fl & TRIM_SPAI0) ? f4splat(L.def_spai0) : ld4(L.spai0, leaf, t);
+                const float4 sp = S.sp;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
@@ -363,16 +395,38 @@ __device__ __forceinline__ float4 sweep_value(const DLevel& L, int leaf, int t, 
     return res;
 }
 
+template <int MODE, class Src>
+__device__ __forceinline__ float4 sweep_value(const DLevel& L, int leaf, int t, const Src& src, const float* b,
+                                              float w, float wsor, float one_minus_wsor, float4& xc, unsigned& m) {
+    SStatic S;
+    sweep_static<MODE>(L, leaf, t, S);
+    return sweep_value_s<MODE>(L, leaf, t, src, b, w, wsor, one_minus_wsor, S, xc, m);
+}
+
 // One leaf of a sweep (CTA = leaf of a level with `count` leaves, the slot
 // range of the fused dot's partials).
-template <int MODE, class Src>
+// WAIT: static data first, then griddepcontrol.wait (false when the caller
+// has waited already).  gate: a flag written by earlier kernels; the CTA does
+// nothing when it is zero (batched solves: the instance has stopped).  A gate
+// only goes from 1 to 0 while a solve runs (it is set again only before the
+// first sweep), so a zero read before the wait is final and skips the static
+// loads; the read after the wait decides.
+template <int MODE, class Src, bool WAIT = false>
 __device__ __forceinline__ void sweep_leaf(const DLevel& L, int leaf, int count, const Src& src, const float* b,
                                            float* out, float w, float wsor, float one_minus_wsor, const DotOut& dot,
-                                           int* spai0_ready) {
+                                           int* spai0_ready, const unsigned* gate = nullptr) {
     const int t = threadIdx.x;
+    if (gate && !*gate) return;
+    SStatic S;
+    sweep_static<MODE>(L, leaf, t, S);
+    if (WAIT) {
+        griddep_wait();
+        griddep_launch();
+    }
+    if (gate && !*gate) return;
     float4 xc;
     unsigned m;
-    float4 res = sweep_value<MODE>(L, leaf, t, src, b, w, wsor, one_minus_wsor, xc, m);
+    float4 res = sweep_value_s<MODE>(L, leaf, t, src, b, w, wsor, one_minus_wsor, S, xc, m);
     st4(out, leaf, t, res);
     if (MODE == M_SPAI0 && spai0_ready && leaf == 0 && t == 0) *spai0_ready = 1;
     if (dot.r) {  // rho_new = z . r (levelDot), then beta and rho (PCG lines 13-15)
@@ -398,9 +452,7 @@ __device__ __forceinline__ void sweep_leaf(const DLevel& L, int leaf, int count,
 template <int MODE, class Src>
 __global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b, float* out, float w, float wsor,
                                                float one_minus_wsor, DotOut dot, int* spai0_ready) {
-    griddep_wait();
-    griddep_launch();
-    sweep_leaf<MODE>(L, blockIdx.x, gridDim.x, src, b, out, w, wsor, one_minus_wsor, dot, spai0_ready);
+    sweep_leaf<MODE, Src, true>(L, blockIdx.x, gridDim.x, src, b, out, w, wsor, one_minus_wsor, dot, spai0_ready);
 }
 
 // out = value of a source (materialise a first sweep or a prolongation)
@@ -420,16 +472,24 @@ __global__ void __launch_bounds__(128) k_materialize(DLevel L, Src src, float* o
 
 // residual (RESID) or plain values, restricted to the parent level:
 // coarse = 0.125 * sum of the active fine values of the 2x2x2 block (.cpp:1624-1684)
-template <bool RESID>
+template <bool RESID, bool WAIT = false>
 __device__ __forceinline__ void restrict_leaf(const DLevel& L, int leaf, const float* x, const float* b,
-                                              float* coarse) {
+                                              float* coarse, const unsigned* gate = nullptr) {
     __shared__ float rs[UAAMG_LEAF];
     const int t = threadIdx.x;
+    if (gate && !*gate) return;  // final when zero (see sweep_leaf)
+    SStatic S;
+    if (RESID) sweep_static<M_RESIDUAL>(L, leaf, t, S);
+    if (WAIT) {
+        griddep_wait();
+        griddep_launch();
+    }
+    if (gate && !*gate) return;
     float4 r;
     if (RESID) {
         float4 xc;
         unsigned m;
-        r = sweep_value<M_RESIDUAL>(L, leaf, t, SrcPlain{x}, b, 0.f, 0.f, 0.f, xc, m);
+        r = sweep_value_s<M_RESIDUAL>(L, leaf, t, SrcPlain{x}, b, 0.f, 0.f, 0.f, S, xc, m);
     } else {
         r = ld4(x, leaf, t);
     }
@@ -455,9 +515,7 @@ __device__ __forceinline__ void restrict_leaf(const DLevel& L, int leaf, const f
 }
 template <bool RESID>
 __global__ void __launch_bounds__(128) k_restrict(DLevel L, const float* x, const float* b, float* coarse) {
-    griddep_wait();
-    griddep_launch();
-    restrict_leaf<RESID>(L, blockIdx.x, x, b, coarse);
+    restrict_leaf<RESID, true>(L, blockIdx.x, x, b, coarse);
 }
 
 // ---------------------------------------------------------------------------
