@@ -336,6 +336,80 @@ def run_batched(args, dev, stream, timed, max_over_ranks, ws):
     }
 
 
+MIXED_WORKLOAD = ("mixed-precision large Poisson: {n}^3, dx = 1/{n}, liquid y<0.45 + 4 spheres r0.1 (seed 2), walls "
+                  "solid, U[-1,1] face velocities (seed 2), rel-res 1e-7, zero initial guess")
+
+
+def run_mixed(args, dev, stream, timed, max_over_ranks, ws):
+    """One large Poisson system solved by the FP32 UAAMG-PCG and by the
+    mixed-precision form (FP16 and BF16 hierarchy storage, FP32 arithmetic and
+    outer CG, FP64 dots, residual replacement every 25 iterations, FP64
+    coarsest solve).  The hierarchy and rhs are built once (setup, reported
+    apart); a step resets the initial guess to zero and solves.  Accuracy: the
+    FP64 true relative residual |b - A x|_inf / |b|_inf of every solution, and
+    the relative 2-norm difference of each mixed solution to the FP32 one."""
+    import torch
+    from uaamg_b200 import scenes
+    from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver
+    n = args.mixed_n
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        phi, fw, vx, vy, vz, sv, dt, dx = scenes.device_large_poisson(n, 2, dev)
+    stream.synchronize()
+    lap = LaplacianWithLevel.createPressurePoissonLaplacian(phi, fw, dt, dx, stream=stream.cuda_stream)
+    nl = lap.leaf_count(0)
+    rhs = torch.empty((nl, 512), dtype=torch.float32, device=dev)
+    lap.createPressurePoissonRightHandSide(fw, vx, vy, vz, sv, dt, out=rhs)
+    del phi, fw, vx, vy, vz
+    solver = PoissonSolver(lap)
+    solver.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    x = torch.zeros_like(rhs)
+    out = {"workload": MIXED_WORKLOAD.format(n=n), "ndof": [lap.num_dof(l) for l in range(lap.num_levels())],
+           "hierarchy_setup_s_host_wall": round(setup_s, 3)}
+    steps = max(2, min(args.steps, 5))
+    launches = 0
+    sols = {}
+    for form in ("fp32", "fp16", "bf16"):
+        if form == "fp32":
+            fn = lambda: solver.solveMultigridPCG(x, rhs)  # noqa: E731
+            setup_ms = 0.0
+        else:
+            setup_ms = solver.prepare_mixed(form)
+            fn = lambda f=form: solver.solveMultigridPCGMixed(x, rhs, f)  # noqa: E731
+        for _ in range(args.warmup):
+            x.zero_()
+            fn()
+        base = solver.kernel_launches
+
+        def step():
+            x.zero_()
+            fn()
+
+        t = timed(step, steps)
+        launches += solver.kernel_launches - base
+        (t,) = max_over_ranks(t)
+        x.zero_()
+        st = fn()
+        rmax, bmax = solver.true_residual_fp64(x, rhs)
+        sols[form] = x.clone()
+        out[form] = {"ms_per_solve": round(t / steps, 3), "solves_per_s": round(steps * 1e3 / t, 2),
+                     "iterations": solver.mIterationTaken, "status": "SUCCESS" if st == 0 else "FAILED",
+                     "true_rel_residual_fp64": rmax / bmax if bmax > 0 else 0.0}
+        if form != "fp32":
+            out[form]["setup_ms"] = round(setup_ms, 1)
+    for form in ("fp16", "bf16"):
+        d = torch.linalg.vector_norm((sols[form] - sols["fp32"]).double())
+        out[form]["rel_diff_vs_fp32"] = float(d / torch.linalg.vector_norm(sols["fp32"].double()))
+        out[form]["speedup_vs_fp32"] = round(out["fp32"]["ms_per_solve"] / out[form]["ms_per_solve"], 3)
+    out["step"] = "zero initial guess, solve to rel-res 1e-7 (hierarchy, rhs resident)"
+    out["_launches"] = int(launches)
+    del lap, solver, sols
+    torch.cuda.empty_cache()
+    return out
+
+
 SERVE_WORKLOAD = ("served stream: Poisson arrivals 200/s and viscosity arrivals 50/s (Poisson process), sides "
                   "log-uniform in [48,384] voxels, geometry as the batched workload (seeded per request), 1-24 "
                   "substeps with new face velocities each, pressure warm-started across substeps, hierarchies "
@@ -383,6 +457,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the secondary Poisson measurement")
     ap.add_argument("--batch", type=int, default=64, help="instances of the batched Poisson measurement (0 = skip)")
+    ap.add_argument("--mixed-n", type=int, default=512, help="domain side of the mixed-precision measurement (0 = skip)")
     ap.add_argument("--serve-window", type=float, default=0.2,
                     help="seconds of arrivals of the served request stream (0 = skip)")
     ap.add_argument("--serve-limit", type=float, default=60.0, help="time limit of each served run (s)")
@@ -652,6 +727,11 @@ def main():
     if args.batch > 0:
         batched = run_batched(args, dev, stream, timed, max_over_ranks, ws)
 
+    # ================= mixed precision: large Poisson solve =================
+    mixed = None
+    if args.mixed_n > 0:
+        mixed = run_mixed(args, dev, stream, timed, max_over_ranks, ws)
+
     # ================= served request stream (continuous batching) =================
     served = None
     if args.serve_window > 0:
@@ -698,6 +778,9 @@ def main():
             line["poisson"] = poisson
         if served is not None:
             line["served"] = served
+        if mixed is not None:
+            line["mixed"] = mixed
+            line["gpu_launches"] = int(line["gpu_launches"] + mixed.pop("_launches"))
         if batched is not None:
             line["batched"] = batched
             line["gpu_launches"] = int(line["gpu_launches"] + batched.pop("_launches"))

@@ -200,6 +200,40 @@ int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph);
 int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h);
 
 /* ======================================================================== */
+/* Mixed-precision pressure solve: PoissonSolver::solveMultigridPCG
+ * (simd_vdb_poisson.cpp:2155-2226) with the preconditioner's hierarchy
+ * (coefficients and mu-cycle vectors of every level) stored in 16-bit floats
+ * and FP32 arithmetic, the outer CG in FP32 on the FP32 level-0 operator with
+ * FP64 dot accumulation, the true residual recomputed every
+ * `replacement interval` iterations, and the coarsest level solved directly
+ * in FP64 (dense inverse).  The reference has no such form; its FP32 solve is
+ * uaamg_poisson_solve_pcg.  Jacobi smoothers only (the default
+ * ScheduledRelaxedJacobi, or WeightedJacobi); the coarsest system must be
+ * positive definite (a domain with a free surface). */
+#define UAAMG_PRECISION_FP16 1
+#define UAAMG_PRECISION_BF16 2
+/* Build the 16-bit hierarchy and the FP64 coarsest inverse now (otherwise the
+ * first mixed solve does it); setup_ms (may be NULL) receives the time taken. */
+int uaamg_poisson_prepare_mixed(uaamg_poisson* h, int precision, double* setup_ms);
+/* True-residual replacement interval of the mixed form (default 25). */
+int uaamg_poisson_set_residual_replacement(uaamg_poisson* h, int every);
+int uaamg_poisson_solve_pcg_mixed(uaamg_poisson* h, int precision, float* pressure, const float* rhs,
+                                  int* iterations);
+int uaamg_poisson_solve_pcg_mixed_device(uaamg_poisson* h, int precision, float* d_pressure, const float* d_rhs,
+                                         int* iterations);
+/* |b - A x|_inf and |b|_inf over the DOF, computed in FP64 from the FP32
+ * level-0 matrix (device vectors): out[0], out[1].  An accuracy check with no
+ * counterpart in the reference. */
+int uaamg_poisson_true_residual_fp64(uaamg_poisson* h, const float* d_x, const float* d_b, double* out);
+
+/* uaamg_poisson_solve_pcg_mixed_device with every kernel launched from a
+ * host-driven loop and timed with CUDA events; per kernel class (label, up to
+ * max_classes, names 64 bytes each) the summed ms and the launch count, as
+ * uaamg_poisson_profile_pcg. */
+int uaamg_poisson_profile_pcg_mixed(uaamg_poisson* h, int precision, float* d_pressure, const float* d_rhs,
+                                    int max_classes, char* names, double* total_ms, int64_t* counts, int* nclasses);
+
+/* ======================================================================== */
 /* Batched pressure solves: PoissonSolver::solveMultigridPCG
  * (simd_vdb_poisson.cpp:2155-2226) of many independent instances in one CUDA
  * graph launch.  The reference has no batched form; each instance's result,

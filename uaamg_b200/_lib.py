@@ -72,6 +72,12 @@ EXPORTS = [
     ("uaamg_poisson_set_stream", i32, [vp, vp]),
     ("uaamg_poisson_set_graph_mode", i32, [vp, i32]),
     ("uaamg_poisson_kernel_launches", i64, [vp]),
+    ("uaamg_poisson_prepare_mixed", i32, [vp, i32, vp]),
+    ("uaamg_poisson_set_residual_replacement", i32, [vp, i32]),
+    ("uaamg_poisson_solve_pcg_mixed", i32, [vp, i32, vp, vp, C.POINTER(C.c_int)]),
+    ("uaamg_poisson_solve_pcg_mixed_device", i32, [vp, i32, vp, vp, C.POINTER(C.c_int)]),
+    ("uaamg_poisson_true_residual_fp64", i32, [vp, vp, vp, vp]),
+    ("uaamg_poisson_profile_pcg_mixed", i32, [vp, i32, vp, vp, i32, vp, vp, vp, C.POINTER(C.c_int)]),
     ("uaamg_batch_create", i32, [i32, vp, C.POINTER(vp)]),
     ("uaamg_batch_destroy", i32, [vp]),
     ("uaamg_batch_size", i32, [vp]),

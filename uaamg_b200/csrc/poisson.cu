@@ -242,6 +242,8 @@ struct LevelDev {
     float dt = 0, dx = 0;
 };
 
+struct MixedData;  // the mixed-precision form's data (mixed.cu)
+
 struct uaamg_poisson {
     DeviceCtx* ctx = nullptr;
     void* pin_state = nullptr;  // pinned block holding st_host and scalar_host
@@ -283,6 +285,8 @@ struct uaamg_poisson {
     bool spai0_built = false;
     float dt = 0, dx = 0;
     int64_t solves = 0;
+    MixedData* mixed = nullptr;  // 16-bit hierarchy copy, FP64 coarsest inverse, graph
+    int replace_every = 25;      // true-residual replacement interval of the mixed form
 };
 
 namespace {
@@ -478,7 +482,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         bytes += carve_size(nc, 4) * 3 + carve_size(nc * 6, 4) * 2;
         size_t n0 = (size_t)L0.nl * UAAMG_LEAF;
         bytes += 6 * carve_size(n0, 4);  // x b r z p q
-        bytes += carve_size(std::max<size_t>((size_t)L0.nl, 1) + 64, 8);
+        bytes += carve_size(red_buffer_doubles(std::max<size_t>((size_t)L0.nl, 1)), 8);
         bytes += carve_size(sizeof(PcgState), 1) + carve_size(64, 4) + carve_size(src.size(), 4);
         CK(ctx_dev_alloc(h->ctx, (void**)&h->dmem, bytes, s));
         h->dmem_bytes = bytes;
@@ -542,7 +546,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         h->z = carve<float>(cur2, n0);
         h->p = carve<float>(cur2, n0);
         h->q = carve<float>(cur2, n0);
-        h->partials = carve<double>(cur2, std::max<size_t>((size_t)L0.nl, 1) + 64);
+        h->partials = carve<double>(cur2, red_buffer_doubles(std::max<size_t>((size_t)L0.nl, 1)));
         h->st = reinterpret_cast<PcgState*>(carve<char>(cur2, sizeof(PcgState)));
         h->scalar_dev = carve<float>(cur2, 64);
         int* dsrc = carve<int>(cur2, src.size());
@@ -637,6 +641,31 @@ struct ProfRec {
     std::string label;
     cudaEvent_t a, b;
 };
+
+// sums the event-timed launches per label (first max_classes labels, in
+// first-seen order) and destroys the events
+static void prof_collect(std::vector<ProfRec>& prof, int max_classes, char* names, double* total_ms, int64_t* counts,
+                         int* nclasses) {
+    std::vector<std::string> lab;
+    for (auto& r : prof) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, r.a, r.b));
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+        int k = (int)(std::find(lab.begin(), lab.end(), r.label) - lab.begin());
+        if (k == (int)lab.size()) {
+            if (k >= max_classes) continue;
+            lab.push_back(r.label);
+            total_ms[k] = 0;
+            counts[k] = 0;
+            snprintf(names + 64 * k, 64, "%s", r.label.c_str());
+        }
+        total_ms[k] += ms;
+        counts[k] += 1;
+    }
+    prof.clear();
+    *nclasses = (int)lab.size();
+}
 
 template <class Src> struct SrcName { static const char* get() { return ""; } };
 template <> struct SrcName<SrcFirstJacobi> { static const char* get() { return "+first"; } };
@@ -1161,10 +1190,13 @@ int uaamg_poisson_create_on_stream(const uaamg_leaf_grid* liquid_phi, const uaam
     return UAAMG_SUCCESS;
 }
 
+static void mixed_free(uaamg_poisson* h);
+
 int uaamg_poisson_destroy(uaamg_poisson* h) {
     if (!h) return UAAMG_SUCCESS;
     if (h->stream) cudaStreamSynchronize(h->stream);
     destroy_graph(h);
+    if (h->ctx) mixed_free(h);
     if (h->ctx) {
         if (h->dmem) cudaFreeAsync(h->dmem, h->stream);
         if (h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
@@ -1528,11 +1560,13 @@ int uaamg_poisson_residual_norm_device(uaamg_poisson* h, const float* d_x, const
 
 // ---------------------------------------------------------------------------
 // Allocation-free variant of uaamg_poisson_residual_norm_device.  Its reduction
-// scratch (one double per level-0 leaf, then the finishing ticket) lives in
-// this file-scope array, which every GPU that loads the library holds until
-// the process exits; the call itself allocates nothing.
+// scratch (a reduction buffer over up to UAAMG_NOALLOC_MAX_LEAVES level-0
+// leaves, then the finishing ticket) lives in this file-scope array, which
+// every GPU that loads the library holds until the process exits; the call
+// itself allocates nothing.
 #define UAAMG_NOALLOC_MAX_LEAVES 262144
-static __device__ __align__(256) unsigned char g_noalloc_scratch[(UAAMG_NOALLOC_MAX_LEAVES + 32) * sizeof(double)];
+#define UAAMG_NOALLOC_RED_DOUBLES (RED_HEADER + UAAMG_NOALLOC_MAX_LEAVES + RED_TICKETS)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[(UAAMG_NOALLOC_RED_DOUBLES + 32) * sizeof(double)];
 
 // Device address of g_noalloc_scratch on each device, resolved once per device
 // (host code may not use the symbol itself: it names a host-side stand-in).
@@ -1568,12 +1602,13 @@ int uaamg_poisson_residual_norm_noalloc(uaamg_poisson* h, const float* d_x, cons
     }
     char* scratch = (char*)noalloc_scratch_on_current_device();
     double* partials = reinterpret_cast<double*>(scratch);
-    unsigned* ticket = reinterpret_cast<unsigned*>(scratch + (size_t)UAAMG_NOALLOC_MAX_LEAVES * sizeof(double));
+    unsigned* ticket = reinterpret_cast<unsigned*>(scratch + (size_t)UAAMG_NOALLOC_RED_DOUBLES * sizeof(double));
     if (D0.L.nl == 0) {
         CK(cudaMemsetAsync(d_norm, 0, sizeof(float), h->stream));
         return UAAMG_SUCCESS;
     }
-    // the array keeps the previous call's contents: the ticket must start at zero
+    // the array keeps the previous call's contents: the tickets must start at zero
+    CK(cudaMemsetAsync(partials, 0, (size_t)RED_HEADER * sizeof(double), h->stream));
     CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned), h->stream));
     launch(k_residual_absmax, (unsigned)D0.L.nl, 128, h->stream, D0.L, d_x, d_b, d_r, partials, ticket, d_norm);
     h->launches++;
@@ -1607,24 +1642,7 @@ int uaamg_poisson_profile_pcg(uaamg_poisson* h, float* d_pressure, const float* 
     CK(cudaStreamSynchronize(h->stream));
     h->launches += E.count;
     h->iterations = h->st_host->iterations_taken;
-    std::vector<std::string> lab;
-    for (auto& r : prof) {
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, r.a, r.b));
-        cudaEventDestroy(r.a);
-        cudaEventDestroy(r.b);
-        int k = (int)(std::find(lab.begin(), lab.end(), r.label) - lab.begin());
-        if (k == (int)lab.size()) {
-            if (k >= max_classes) continue;
-            lab.push_back(r.label);
-            total_ms[k] = 0;
-            counts[k] = 0;
-            snprintf(names + 64 * k, 64, "%s", r.label.c_str());
-        }
-        total_ms[k] += ms;
-        counts[k] += 1;
-    }
-    *nclasses = (int)lab.size();
+    prof_collect(prof, max_classes, names, total_ms, counts, nclasses);
     CK(cudaMemcpyAsync(d_pressure, h->x, nb, cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return h->st_host->status == PCG_SUCCESS ? UAAMG_SUCCESS : UAAMG_FAILED;

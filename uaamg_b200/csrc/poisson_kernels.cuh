@@ -273,38 +273,101 @@ __device__ __forceinline__ float block_max128(float v, float* sh) {
 // |v| with non-finite values propagated (grid_abs_max_op, openvdb_grid_math_op.h:4-43)
 __device__ __forceinline__ float absprop(float v) { return isfinite(v) ? fabsf(v) : (isnan(v) ? v : INFINITY); }
 
-// Writes this block's partial into slot `slot` of the `count` partials of one
-// reduction; returns true in every thread of the block that finishes last.
-__device__ __forceinline__ bool publish_partial_at(double part, double* partials, unsigned* ticket, int slot,
-                                                   int count, bool* sh_last) {
+// Deterministic two-level reduction over the CTAs of one launch.  A
+// reduction buffer holds RED_TICKETS group tickets (RED_HEADER doubles, zero
+// between reductions), then one partial per CTA slot, then one partial per
+// group of red_group_size(count) consecutive slots.  Every CTA stores its
+// partial and takes a ticket of its group; the CTA that completes a group
+// combines the group's partials and takes a ticket of the reduction; the CTA
+// that completes the last group combines the group partials.  The order of
+// the combination depends only on `count` and the block size, so results are
+// reproducible; no CTA reads more than a group's worth of partials, and the
+// reduction's own ticket sees one atomic per group rather than per CTA.
+constexpr int RED_TICKETS = 2048;
+constexpr int RED_HEADER = RED_TICKETS / 2;
+__host__ __device__ __forceinline__ int red_group_size(int count) {
+    return count <= 256 * RED_TICKETS ? 256 : (count + RED_TICKETS - 1) / RED_TICKETS;
+}
+// doubles a reduction buffer over `count` slots needs
+__host__ __device__ __forceinline__ size_t red_buffer_doubles(size_t count) {
+    return (size_t)RED_HEADER + count + RED_TICKETS;
+}
+template <bool MAX>
+__device__ __forceinline__ double red_combine(double a, double b) {
+    return MAX ? (double)nanmax((float)a, (float)b) : a + b;
+}
+// block-wide combination for any multiple of 32 threads up to 256; valid in thread 0
+template <bool MAX>
+__device__ __forceinline__ double block_reduce_n(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = red_combine<MAX>(v, __shfl_down_sync(FULLMASK, v, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double r = 0;
     if (threadIdx.x == 0) {
-        partials[slot] = part;
-        __threadfence();
-        unsigned tk = atomicAdd(ticket, 1u);
-        *sh_last = (tk == (unsigned)count - 1);
+        r = sh[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = red_combine<MAX>(r, sh[w]);
     }
     __syncthreads();
-    return *sh_last;
+    return r;
 }
-__device__ __forceinline__ bool publish_partial(double part, double* partials, unsigned* ticket, bool* sh_last) {
-    return publish_partial_at(part, partials, ticket, blockIdx.x, gridDim.x, sh_last);
+// Publishes this CTA's partial (valid in thread 0) into slot `slot` of a
+// reduction over `count` slots; returns true in every thread of the CTA that
+// completes it, whose thread 0 then holds the result in `total`.  That CTA
+// resets `ticket` itself (the group tickets are reset here).
+template <bool MAX>
+__device__ __forceinline__ bool red_publish(double part, double* buf, unsigned* ticket, int slot, int count,
+                                            double& total) {
+    __shared__ double rsh[8];
+    __shared__ int rflag;
+    unsigned* gt = reinterpret_cast<unsigned*>(buf);
+    double* slots = buf + RED_HEADER;
+    double* groups = slots + count;
+    const int gs = red_group_size(count);
+    const int g = slot / gs;
+    const int g0 = g * gs;
+    const int gn = min(gs, count - g0);
+    const int ng = (count + gs - 1) / gs;
+    if (threadIdx.x == 0) {
+        slots[slot] = part;
+        __threadfence();
+        rflag = (atomicAdd(&gt[g], 1u) == (unsigned)gn - 1);
+    }
+    __syncthreads();
+    if (!rflag) return false;
+    __threadfence();
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < gn; i += blockDim.x) acc = red_combine<MAX>(acc, __ldcg(slots + g0 + i));
+    acc = block_reduce_n<MAX>(acc, rsh);
+    if (ng == 1) {
+        if (threadIdx.x == 0) gt[g] = 0;
+        total = acc;
+        return true;
+    }
+    if (threadIdx.x == 0) {
+        gt[g] = 0;
+        groups[g] = acc;
+        __threadfence();
+        rflag = (atomicAdd(ticket, 1u) == (unsigned)ng - 1);
+    }
+    __syncthreads();
+    if (!rflag) return false;
+    __threadfence();
+    acc = 0.0;
+    for (int i = threadIdx.x; i < ng; i += blockDim.x) acc = red_combine<MAX>(acc, __ldcg(groups + i));
+    total = block_reduce_n<MAX>(acc, rsh);
+    return true;
 }
-// Sum of the first `count` partials in a fixed order (last block only), valid in thread 0.
-__device__ __forceinline__ double gather_sum_n(const double* partials, int count, double* sh) {
-    double acc = 0;
-    for (int i = threadIdx.x; i < count; i += blockDim.x) acc += __ldcg(partials + i);
-    return block_sum128(acc, sh);
+__device__ __forceinline__ bool reduce_sum(double part, double* buf, unsigned* ticket, int slot, int count,
+                                           double& total) {
+    return red_publish<false>(part, buf, ticket, slot, count, total);
 }
-__device__ __forceinline__ float gather_max_n(const double* partials, int count, float* sh) {
-    float acc = 0.f;
-    for (int i = threadIdx.x; i < count; i += blockDim.x) acc = nanmax(acc, (float)__ldcg(partials + i));
-    return block_max128(acc, sh);
-}
-__device__ __forceinline__ double gather_sum(const double* partials, double* sh) {
-    return gather_sum_n(partials, gridDim.x, sh);
-}
-__device__ __forceinline__ float gather_max(const double* partials, float* sh) {
-    return gather_max_n(partials, gridDim.x, sh);
+__device__ __forceinline__ bool reduce_max(double part, double* buf, unsigned* ticket, int slot, int count,
+                                           float& total) {
+    double t = 0.0;
+    const bool done = red_publish<true>(part, buf, ticket, slot, count, t);
+    total = (float)t;
+    return done;
 }
 
 // ---------------------------------------------------------------------------
@@ -431,12 +494,11 @@ __device__ __forceinline__ void sweep_leaf(const DLevel& L, int leaf, int count,
     if (MODE == M_SPAI0 && spai0_ready && leaf == 0 && t == 0) *spai0_ready = 1;
     if (dot.r) {  // rho_new = z . r (levelDot), then beta and rho (PCG lines 13-15)
         __shared__ double shd[4];
-        __shared__ bool last;
         float4 rr = ld4(dot.r, leaf, t);
         double s = (double)res.x * rr.x + (double)res.y * rr.y + (double)res.z * rr.z + (double)res.w * rr.w;
         double part = block_sum128(s, shd);
-        if (publish_partial_at(part, dot.partials, &dot.st->ticket[0], leaf, count, &last)) {
-            double tot = gather_sum_n(dot.partials, count, shd);
+        double tot;
+        if (reduce_sum(part, dot.partials, &dot.st->ticket[0], leaf, count, tot)) {
             if (t == 0) {
                 PcgState* st = dot.st;
                 float rho_new = (float)tot;
@@ -791,12 +853,11 @@ __global__ void __launch_bounds__(128) k_sweep_staged(DLevel L, const float* x, 
     }
     if (dot.r) {  // rho_new = z . r, then beta and rho (PCG lines 13-15)
         __shared__ double shd[4];
-        __shared__ bool last;
         float4 rr = ok ? s4(S.b, t) : f4zero();  // b of this sweep is r
         double s = (double)res.x * rr.x + (double)res.y * rr.y + (double)res.z * rr.z + (double)res.w * rr.w;
         double part = block_sum128(s, shd);
-        if (publish_partial(part, dot.partials, &dot.st->ticket[0], &last)) {
-            double tot = gather_sum(dot.partials, shd);
+        double tot;
+        if (reduce_sum(part, dot.partials, &dot.st->ticket[0], blockIdx.x, gridDim.x, tot)) {
             if (t == 0) {
                 PcgState* st = dot.st;
                 float rho_new = (float)tot;
@@ -876,7 +937,6 @@ __device__ __forceinline__ void pcg_init_leaf(const DLevel& L, int leaf, int cou
                                               float* r, double* partials, PcgState* st,
                                               cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ float shf[4];
-    __shared__ bool last;
     const int t = threadIdx.x;
     float4 xc;
     unsigned m;
@@ -884,8 +944,8 @@ __device__ __forceinline__ void pcg_init_leaf(const DLevel& L, int leaf, int cou
     st4(r, leaf, t, res);
     float a = nanmax(nanmax(absprop(res.x), absprop(res.y)), nanmax(absprop(res.z), absprop(res.w)));
     float part = block_max128(a, shf);
-    if (publish_partial_at((double)part, partials, &st->ticket[1], leaf, count, &last)) {
-        float nu = gather_max_n(partials, count, shf);
+    float nu;
+    if (reduce_max(part, partials, &st->ticket[1], leaf, count, nu)) {
         if (t == 0) {
             st->nu = nu;
             st->nu_old = nu;
@@ -943,7 +1003,6 @@ __global__ void __launch_bounds__(128) k_pcg_update_p(DLevel L, const float* z, 
 __device__ __forceinline__ void pcg_Ap_leaf(const DLevel& L, int leaf, int count, const float* p, float* q,
                                             double* partials, PcgState* st) {
     __shared__ double shd[4];
-    __shared__ bool last;
     const int t = threadIdx.x;
     float4 xc;
     unsigned m;
@@ -951,8 +1010,8 @@ __device__ __forceinline__ void pcg_Ap_leaf(const DLevel& L, int leaf, int count
     st4(q, leaf, t, res);
     double s = (double)xc.x * res.x + (double)xc.y * res.y + (double)xc.z * res.z + (double)xc.w * res.w;
     double part = block_sum128(s, shd);
-    if (publish_partial_at(part, partials, &st->ticket[2], leaf, count, &last)) {
-        double tot = gather_sum_n(partials, count, shd);
+    double tot;
+    if (reduce_sum(part, partials, &st->ticket[2], leaf, count, tot)) {
         if (t == 0) {
             float sigma = (float)tot;
             st->sigma = sigma;
@@ -972,7 +1031,6 @@ __global__ void __launch_bounds__(128) k_pcg_Ap(DLevel L, const float* p, float*
 __device__ __forceinline__ void pcg_update_r_leaf(int leaf, int count, const float* q, float* r, double* partials,
                                                   PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ float shf[4];
-    __shared__ bool last;
     const int t = threadIdx.x;
     const float na = -st->alpha;
     float4 qq = ld4(q, leaf, t), rr = ld4(r, leaf, t);
@@ -983,8 +1041,8 @@ __device__ __forceinline__ void pcg_update_r_leaf(int leaf, int count, const flo
     st4(r, leaf, t, rr);
     float a = nanmax(nanmax(absprop(rr.x), absprop(rr.y)), nanmax(absprop(rr.z), absprop(rr.w)));
     float part = block_max128(a, shf);
-    if (publish_partial_at((double)part, partials, &st->ticket[3], leaf, count, &last)) {
-        float nu = gather_max_n(partials, count, shf);
+    float nu;
+    if (reduce_max(part, partials, &st->ticket[3], leaf, count, nu)) {
         if (t == 0) {
             const int k = st->iter;
             st->nu_old = st->nu;
@@ -1046,7 +1104,6 @@ __global__ void __launch_bounds__(128) k_pcg_finish(DLevel L, const float* p, fl
 __device__ __forceinline__ void dot_rho_leaf(const DLevel& L, int leaf, int count, const float* z, const float* r,
                                              double* partials, PcgState* st) {
     __shared__ double shd[4];
-    __shared__ bool last;
     const int t = threadIdx.x;
     float4 a = ld4(z, leaf, t), c = ld4(r, leaf, t);
     unsigned m = mask4(L.mask, leaf, t);
@@ -1056,8 +1113,8 @@ __device__ __forceinline__ void dot_rho_leaf(const DLevel& L, int leaf, int coun
     if (m & 4) s += (double)a.z * c.z;
     if (m & 8) s += (double)a.w * c.w;
     double part = block_sum128(s, shd);
-    if (publish_partial_at(part, partials, &st->ticket[0], leaf, count, &last)) {
-        double tot = gather_sum_n(partials, count, shd);
+    double tot;
+    if (reduce_sum(part, partials, &st->ticket[0], leaf, count, tot)) {
         if (t == 0) {
             float rho_new = (float)tot;
             st->rho_new = rho_new;
@@ -1084,7 +1141,6 @@ __global__ void __launch_bounds__(128) k_residual_absmax(DLevel L, const float* 
     griddep_wait();
     griddep_launch();
     __shared__ float shf[4];
-    __shared__ bool last;
     const int leaf = blockIdx.x, t = threadIdx.x;
     float4 xc;
     unsigned m;
@@ -1092,8 +1148,8 @@ __global__ void __launch_bounds__(128) k_residual_absmax(DLevel L, const float* 
     st4(r, leaf, t, res);
     float a = nanmax(nanmax(absprop(res.x), absprop(res.y)), nanmax(absprop(res.z), absprop(res.w)));
     float part = block_max128(a, shf);
-    if (publish_partial((double)part, partials, ticket, &last)) {
-        float nu = gather_max(partials, shf);
+    float nu;
+    if (reduce_max(part, partials, ticket, blockIdx.x, gridDim.x, nu)) {
         if (t == 0) {
             *out = nu;
             *ticket = 0;
@@ -1107,7 +1163,6 @@ __global__ void __launch_bounds__(128) k_absmax(DLevel L, const float* v, double
     griddep_wait();
     griddep_launch();
     __shared__ float shf[4];
-    __shared__ bool last;
     const int leaf = blockIdx.x, t = threadIdx.x;
     float4 a = ld4(v, leaf, t);
     unsigned m = mask4(L.mask, leaf, t);
@@ -1117,8 +1172,8 @@ __global__ void __launch_bounds__(128) k_absmax(DLevel L, const float* v, double
     if (m & 4) mx = nanmax(mx, absprop(a.z));
     if (m & 8) mx = nanmax(mx, absprop(a.w));
     float part = block_max128(mx, shf);
-    if (publish_partial((double)part, partials, ticket, &last)) {
-        float r = gather_max(partials, shf);
+    float r;
+    if (reduce_max(part, partials, ticket, blockIdx.x, gridDim.x, r)) {
         if (t == 0) {
             *out = r;
             *ticket = 0;

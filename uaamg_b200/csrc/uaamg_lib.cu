@@ -1,4 +1,5 @@
 // uaamg_lib.cu -- single translation unit of libuaamg_b200.so
 #include "poisson.cu"
 #include "batch.cu"
+#include "mixed.cu"
 #include "viscosity.cu"

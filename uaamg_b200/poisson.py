@@ -75,7 +75,10 @@ class LaplacianWithLevel:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            _lib.lib().uaamg_poisson_destroy(h)
+            try:
+                _lib.lib().uaamg_poisson_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
             self._h = None
 
     # --- topology / sizes
@@ -240,6 +243,45 @@ class PoissonSolver:
     def solvePureMultigrid(self, in_out_pressure, in_rhs) -> int:
         return self._solve("uaamg_poisson_solve_mg", "uaamg_poisson_solve_mg_device", in_out_pressure, in_rhs)
 
+    # --- mixed-precision form (no counterpart in the reference): the
+    # preconditioner's hierarchy in FP16/BF16 with FP32 arithmetic, FP32 outer
+    # CG with FP64 dots, true-residual replacement, FP64 coarsest solve
+    PRECISIONS = {"fp16": 1, "bf16": 2}
+
+    def prepare_mixed(self, precision: str = "fp16") -> float:
+        """Build the 16-bit hierarchy and the FP64 coarsest inverse; returns
+        the time it took (ms)."""
+        L, h = self._configure()
+        ms = C.c_double(0.0)
+        _lib.check(L.uaamg_poisson_prepare_mixed(h, self.PRECISIONS[precision], C.byref(ms)), "prepare_mixed")
+        return float(ms.value)
+
+    def set_residual_replacement(self, every: int) -> None:
+        _lib.check(_lib.lib().uaamg_poisson_set_residual_replacement(self.mMultigridHierarchy._h, int(every)),
+                   "set_residual_replacement")
+
+    def solveMultigridPCGMixed(self, in_out_pressure, in_rhs, precision: str = "fp16") -> int:
+        L, h = self._configure()
+        it = C.c_int(0)
+        prec = self.PRECISIONS[precision]
+        if isinstance(in_out_pressure, np.ndarray):
+            assert in_out_pressure.dtype == np.float32 and in_out_pressure.flags["C_CONTIGUOUS"]
+            rhs = np.ascontiguousarray(in_rhs, np.float32)
+            rc = L.uaamg_poisson_solve_pcg_mixed(h, prec, in_out_pressure.ctypes.data, rhs.ctypes.data, C.byref(it))
+        else:
+            rc = L.uaamg_poisson_solve_pcg_mixed_device(h, prec, in_out_pressure.data_ptr(), in_rhs.data_ptr(),
+                                                        C.byref(it))
+        _lib.check(rc, "solve_pcg_mixed")
+        self.mIterationTaken = int(it.value)
+        return int(rc)
+
+    def true_residual_fp64(self, d_x, d_b) -> tuple[float, float]:
+        """(|b - A x|_inf, |b|_inf) in FP64 from the FP32 level-0 matrix (device tensors)."""
+        out = (C.c_double * 2)()
+        _lib.check(_lib.lib().uaamg_poisson_true_residual_fp64(self.mMultigridHierarchy._h, d_x.data_ptr(),
+                                                                d_b.data_ptr(), out), "true_residual_fp64")
+        return float(out[0]), float(out[1])
+
     def precondition(self, r: np.ndarray) -> np.ndarray:
         L, h = self._configure()
         z = np.zeros_like(r, dtype=np.float32)
@@ -258,10 +300,26 @@ class PoissonSolver:
         rc = L.uaamg_poisson_profile_pcg(h, d_pressure.data_ptr(), d_rhs.data_ptr(), max_classes,
                                          C.addressof(names), ms.ctypes.data, cnt.ctypes.data, C.byref(nc))
         _lib.check(rc, "profile_pcg")
-        self.mIterationTaken = int(L.uaamg_poisson_iterations(h))
+        return self._prof_table(names, ms, cnt, nc.value)
+
+    def profile_pcg_mixed(self, d_pressure, d_rhs, precision: str = "fp16", max_classes: int = 64):
+        """profile_pcg of the mixed-precision form."""
+        L, h = self._configure()
+        names = C.create_string_buffer(64 * max_classes)
+        ms = np.zeros(max_classes, np.float64)
+        cnt = np.zeros(max_classes, np.int64)
+        nc = C.c_int(0)
+        rc = L.uaamg_poisson_profile_pcg_mixed(h, self.PRECISIONS[precision], d_pressure.data_ptr(),
+                                               d_rhs.data_ptr(), max_classes, C.addressof(names), ms.ctypes.data,
+                                               cnt.ctypes.data, C.byref(nc))
+        _lib.check(rc, "profile_pcg_mixed")
+        return self._prof_table(names, ms, cnt, nc.value)
+
+    def _prof_table(self, names, ms, cnt, n):
+        self.mIterationTaken = int(_lib.lib().uaamg_poisson_iterations(self.mMultigridHierarchy._h))
         raw = names.raw
         out = {}
-        for k in range(nc.value):
+        for k in range(n):
             nm = raw[64 * k: 64 * k + 64].split(b"\0", 1)[0].decode()
             out[nm] = (float(ms[k]), int(cnt[k]))
         return out

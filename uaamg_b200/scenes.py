@@ -315,3 +315,30 @@ def device_viscosity_instance(n: int, seed: int, device, mu: float = 1e3, dt: fl
     sv = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512, 3), np.float32),
                   background=np.zeros(3, np.float32))
     return liquid, solid, visc, sv, dt, rho, dx
+
+
+def device_large_poisson(n: int = 512, seed: int = 2, device="cuda"):
+    """Mixed-precision workload built in HBM: n^3 (512^3), dx = 1/n, liquid =
+    {y < 0.45} U 4 spheres of radius 0.1 (centres from ``seed``, as
+    large_poisson_scene), walls solid, face velocities U[-1,1] (seed), dt = 1.
+    Returns (phi, face_weights, vx, vy, vz, solid_velocity, dt, dx)."""
+    import torch
+    assert n % 8 == 0
+    u = uniform(seed + 1000, 12, 0.15, 0.85).reshape(4, 3)
+    spheres = [((float(a), float(b) * 0.4 + 0.5, float(c)), 0.1) for a, b, c in u]
+    dx = 1.0 / n
+    phi = _device_sdf(n, spheres, device, slab_height=0.45)
+    m = n + 8
+    w = torch.ones((m, m, m, 3), device=device, dtype=torch.float32)
+    f = n + 1
+    w[0, :f, :f, 0] = 0.0; w[n, :f, :f, 0] = 0.0
+    w[:f, 0, :f, 1] = 0.0; w[:f, n, :f, 1] = 0.0
+    w[:f, :f, 0, 2] = 0.0; w[:f, :f, n, 2] = 0.0
+    phi_g = _device_leaf_grid(phi, 0, np.float32(3.0 * dx), 1)
+    del phi
+    fw_g = _device_leaf_grid(w, 0, np.ones(3, np.float32), 3)
+    del w
+    vx, vy, vz = device_face_velocities(n, seed, device)
+    sv = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512, 3), np.float32),
+                  background=np.zeros(3, np.float32))
+    return phi_g, fw_g, vx, vy, vz, sv, 1.0, dx
