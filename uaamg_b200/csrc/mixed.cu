@@ -196,12 +196,21 @@ struct MEnq {
         launch(kern, g, b, s, args...);
         pe();
     }
+    template <typename... KArgs, typename... Args>
+    void run_pipe(const char* what, int l, void (*kern)(KArgs...), int nl, size_t smem, Args... args) {
+        pb(what, l);
+        launch_pipe(kern, nl, smem, s, args...);
+        pe();
+    }
 };
 
 // muCyclePreconditioner<2, skip_first> (simd_vdb_poisson.cpp:1844-1977) on
 // the 16-bit hierarchy: the launch sequence of enqueue_precond for the Jacobi
 // smoothers; at level 0 the rhs is the 16-bit copy of the CG residual and the
-// last sweep writes z in FP32 together with z.r.
+// last sweep writes z in FP32 together with z.r.  Levels of at least
+// STAGED_MIN_LEAVES leaves sweep with the staged kernels, and from
+// SPLIT_MIN_LEAVES on the first sweep's source and the prolongation-add are
+// stored first (k_mmaterialize) so that every sweep is a staged plain one.
 template <typename T>
 static void menq_visit(MEnq& E, int l, bool skip_first, DotOut dot, float* z) {
     uaamg_poisson* h = E.h;
@@ -236,34 +245,61 @@ static void menq_visit(MEnq& E, int l, bool skip_first, DotOut dot, float* z) {
     }
     const int sm = h->smoother;
     auto wpre = [&](int i) { return sm == UAAMG_SMOOTHER_WEIGHTED_JACOBI ? 6.0f / 7.0f : sched_weight_precond(3, i); };
+    const bool staged = g_use_staged && L.nl >= STAGED_MIN_LEAVES;
+    const bool split = g_use_staged && L.nl >= SPLIT_MIN_LEAVES;
+    int* err = &h->st->error;
+    const size_t psm = pipe_smem_bytes<MLevel<T>>();
+    auto sweep = [&](const T* x, T* out, float w) {  // plain source
+        if (staged)
+            E.run_pipe("jacobi staged", l, k_pipe<M_JACOBI, MLevel<T>, T, false>, L.nl, psm, L, x, (const T*)rhs, out,
+                       w, 0.f, 0.f, nodot, ns, 0.f, err);
+        else
+            E.run("jacobi", l, k_msweep<T, T, MSrcPlain<T>>, g, 128, L, MSrcPlain<T>{x}, (const T*)rhs, out, w, nodot,
+                  ns);
+    };
     if (skip_first) {
-        E.run("jacobi first", l, k_msweep8<T, T, LSrcFirstJacobi<T>>, g, 64, L, LSrcFirstJacobi<T>{rhs, wpre(0)},
-              (const T*)rhs, lhs, wpre(1), nodot, ns);
-        E.run("jacobi", l, k_msweep8<T, T, LSrcPlain<T>>, g, 64, L, LSrcPlain<T>{lhs}, (const T*)rhs, tmp, wpre(2),
-              nodot, ns);
+        if (split) {
+            E.run("materialize first", l, k_mmaterialize<T, MSrcFirstJacobi<T>>, g, 128, L,
+                  MSrcFirstJacobi<T>{rhs, wpre(0)}, tmp);
+            sweep(tmp, lhs, wpre(1));
+        } else {
+            E.run("jacobi first", l, k_msweep<T, T, MSrcFirstJacobi<T>>, g, 128, L, MSrcFirstJacobi<T>{rhs, wpre(0)},
+                  (const T*)rhs, lhs, wpre(1), nodot, ns);
+        }
+        sweep(lhs, tmp, wpre(2));
     } else {
-        E.run("jacobi", l, k_msweep8<T, T, LSrcPlain<T>>, g, 64, L, LSrcPlain<T>{lhs}, (const T*)rhs, tmp, wpre(0),
-              nodot, ns);
-        E.run("jacobi", l, k_msweep8<T, T, LSrcPlain<T>>, g, 64, L, LSrcPlain<T>{tmp}, (const T*)rhs, lhs, wpre(1),
-              nodot, ns);
-        E.run("jacobi", l, k_msweep8<T, T, LSrcPlain<T>>, g, 64, L, LSrcPlain<T>{lhs}, (const T*)rhs, tmp, wpre(2),
-              nodot, ns);
+        sweep(lhs, tmp, wpre(0));
+        sweep(tmp, lhs, wpre(1));
+        sweep(lhs, tmp, wpre(2));
     }
-    E.run("restrict", l, k_mrestrict8<T>, g, 64, L, (const T*)tmp, (const T*)rhs, (T*)M->lv[l + 1].rhs,
-          1.0f / level_scale(h->lv[l + 1].L));
+    const float cics = 1.0f / level_scale(h->lv[l + 1].L);
+    T* crhs = (T*)M->lv[l + 1].rhs;
+    if (staged)
+        E.run_pipe("restrict staged", l, k_pipe<M_RESIDUAL, MLevel<T>, T, true>, L.nl, psm, L, (const T*)tmp,
+                   (const T*)rhs, crhs, 0.f, 0.f, 0.f, nodot, ns, cics, err);
+    else
+        E.run("restrict", l, k_mrestrict<T>, g, 128, L, (const T*)tmp, (const T*)rhs, crhs, cics);
     menq_visit<T>(E, l + 1, true, nodot, nullptr);
     if (l + 1 != last) menq_visit<T>(E, l + 1, false, nodot, nullptr);
-    T* clhs = (T*)M->lv[l + 1].lhs;
-    E.run("jacobi prolong", l, k_msweep8<T, T, LSrcProlong<T>>, g, 64, L, LSrcProlong<T>{tmp, clhs}, (const T*)rhs,
-          lhs, wpre(2), nodot, ns);
-    E.run("jacobi", l, k_msweep8<T, T, LSrcPlain<T>>, g, 64, L, LSrcPlain<T>{lhs}, (const T*)rhs, tmp, wpre(1), nodot,
-          ns);
-    if (l == 0)
-        E.run("jacobi to fp32 +dot", l, k_msweep8<T, float, LSrcPlain<T>>, g, 64, L, LSrcPlain<T>{tmp},
-              (const T*)rhs, z, wpre(0), dot, (const float*)M->sigma);
-    else
-        E.run("jacobi", l, k_msweep8<T, T, LSrcPlain<T>>, g, 64, L, LSrcPlain<T>{tmp}, (const T*)rhs, lhs, wpre(0),
-              nodot, ns);
+    const T* clhs = (const T*)M->lv[l + 1].lhs;
+    if (split) {  // tmp += P x_c in place (tmp is rewritten before it is read again)
+        E.run("materialize prolong", l, k_mmaterialize<T, MSrcProlong<T>>, g, 128, L, MSrcProlong<T>{tmp, clhs}, tmp);
+        sweep(tmp, lhs, wpre(2));
+    } else {
+        E.run("jacobi prolong", l, k_msweep<T, T, MSrcProlong<T>>, g, 128, L, MSrcProlong<T>{tmp, clhs},
+              (const T*)rhs, lhs, wpre(2), nodot, ns);
+    }
+    sweep(lhs, tmp, wpre(1));
+    if (l == 0) {
+        if (staged)
+            E.run_pipe("jacobi staged to fp32 +dot", l, k_pipe<M_JACOBI, MLevel<T>, float, false>, L.nl, psm, L,
+                       (const T*)tmp, (const T*)rhs, z, wpre(0), 0.f, 0.f, dot, (const float*)M->sigma, 0.f, err);
+        else
+            E.run("jacobi to fp32 +dot", l, k_msweep<T, float, MSrcPlain<T>>, g, 128, L, MSrcPlain<T>{tmp},
+                  (const T*)rhs, z, wpre(0), dot, (const float*)M->sigma);
+    } else {
+        sweep(tmp, lhs, wpre(0));
+    }
 }
 
 template <typename T>
@@ -391,6 +427,10 @@ static int mixed_run_pcg(uaamg_poisson* h, std::vector<ProfRec>* prof = nullptr)
     const PcgState& s = *h->st_host;
     h->last_launches = launches;
     h->launches += launches;
+    if (s.error) {
+        set_error("a kernel's bounded wait for its bulk copies timed out");
+        throw UaamgError{UAAMG_ERR_CUDA};
+    }
     h->iterations = s.iterations_taken;
     h->final_residual = s.nu;
     return (s.status == PCG_SUCCESS) ? UAAMG_SUCCESS : UAAMG_FAILED;

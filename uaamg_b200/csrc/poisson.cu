@@ -28,6 +28,7 @@
 #include "common.cuh"
 #include "poisson_build.cuh"
 #include "poisson_kernels.cuh"
+#include "staged_pipe.cuh"
 #include "resources.cuh"
 
 using namespace uaamg;
@@ -621,12 +622,56 @@ static bool g_use_pdl = true;
 // the bulk-async staged kernels (UAAMG_STAGED=0 turns them off).
 static bool g_use_staged = true;
 #define STAGED_MIN_LEAVES 64
+// On levels of at least SPLIT_MIN_LEAVES leaves a sweep whose source is
+// computed (the first sweep from a zero guess, the prolongation-add) runs as
+// k_materialize of the source and a staged plain sweep: the fused kernel
+// recomputes the source at every stencil neighbour from dependent loads,
+// which costs more than one extra elementwise pass on large levels.  The
+// stored values are the ones the fused kernel computes, so the results are
+// identical.
+#define SPLIT_MIN_LEAVES 1024
 template <typename... KArgs, typename... Args>
 static void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
     cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = g_use_pdl ? 1 : 0;
+    CK(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+}
+
+// Resident CTAs of `kern` (block threads, smem dynamic bytes) on the current
+// GPU: the grid of a persistent kernel.  Cached per kernel and device.
+static int resident_ctas(const void* kern, int block, size_t smem) {
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<const void*, int>, int>> cache;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& e : cache)
+        if (e.first.first == kern && e.first.second == dev) return e.second;
+    int sms = 0, per = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, block, smem));
+    const int r = std::max(1, per) * std::max(1, sms);
+    cache.push_back({{kern, dev}, r});
+    return r;
+}
+
+// Launch of a pipelined staged kernel (staged_pipe.cuh) over nl leaves: at
+// most one CTA per leaf, at most the CTAs the GPU holds at once.
+template <typename... KArgs, typename... Args>
+static void launch_pipe(void (*kern)(KArgs...), int nl, size_t smem, cudaStream_t s, Args... args) {
+    const int g = std::min(nl, resident_ctas((const void*)kern, 128, smem));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)g);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -705,8 +750,9 @@ struct Enq {
         if constexpr (std::is_same<Src, SrcPlain>::value) {
             if (g_use_staged && D.L.nl >= STAGED_MIN_LEAVES && !(MODE == M_SPAI0 && mark_spai0)) {
                 if (prof) pb("L" + std::to_string(l) + " " + mode_name(MODE) + " staged" + (dot.r ? "+dot" : ""));
-                launch(k_sweep_staged<MODE>, (unsigned)D.L.nl, 128, s, D.L, (const float*)src.x, b, out, w, ws,
-                       1.0f - ws, dot, &h->st->error);
+                launch_pipe(k_pipe<MODE, DLevel, float, false>, D.L.nl, pipe_smem_bytes<DLevel>(), s, D.L,
+                            (const float*)src.x, b, out, w, ws, 1.0f - ws, dot, (const float*)nullptr, 0.f,
+                            &h->st->error);
                 pe();
                 count++;
                 return;
@@ -718,11 +764,22 @@ struct Enq {
         pe();
         count++;
     }
+    bool split(int l) const { return g_use_staged && h->lv[l].L.nl >= SPLIT_MIN_LEAVES; }
+    template <class Src>
+    void materialize(int l, const Src& src, float* out) {
+        LevelDev& D = h->lv[l];
+        if (prof) pb("L" + std::to_string(l) + " materialize" + SrcName<Src>::get());
+        launch(k_materialize<Src>, (unsigned)D.L.nl, 128, s, D.L, src, out);
+        pe();
+        count++;
+    }
     void restrict_resid(int l, const float* x, const float* b) {
         LevelDev& D = h->lv[l];
         if (g_use_staged && D.L.nl >= STAGED_MIN_LEAVES) {
             if (prof) pb("L" + std::to_string(l) + " residual+restrict staged");
-            launch(k_restrict_staged, (unsigned)D.L.nl, 128, s, D.L, x, b, h->lv[l + 1].rhs, &h->st->error);
+            launch_pipe(k_pipe<M_RESIDUAL, DLevel, float, true>, D.L.nl, pipe_smem_bytes<DLevel>(), s, D.L, x, b,
+                        h->lv[l + 1].rhs, 0.f, 0.f, 0.f, DotOut{nullptr, nullptr, nullptr}, (const float*)nullptr,
+                        0.f, &h->st->error);
             pe();
             count++;
             return;
@@ -813,7 +870,12 @@ static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool sk
         if (l + 1 != h->nlev - 1) enqueue_precond(E, l + 1, P.lhs, P.rhs, false, DotOut{nullptr, nullptr, nullptr});
         // post: (black, red) x n; the first black pass adds the prolongation,
         // writes T; the last red pass writes back into lhs
-        E.sweep<M_BLACK>(l, SrcProlong{lhs, P.lhs, 1.0f}, rhs, T, 0.f);
+        if (E.split(l)) {
+            E.materialize(l, SrcProlong{lhs, P.lhs, 1.0f}, lhs);
+            E.sweep<M_BLACK>(l, SrcPlain{lhs}, rhs, T, 0.f);
+        } else {
+            E.sweep<M_BLACK>(l, SrcProlong{lhs, P.lhs, 1.0f}, rhs, T, 0.f);
+        }
         for (int i = 0; i < n; ++i) {
             if (i > 0) E.sweep<M_BLACK>(l, SrcPlain{T}, rhs, T, 0.f);
             if (i < n - 1) E.sweep<M_RED>(l, SrcPlain{T}, rhs, T, 0.f);
@@ -824,8 +886,16 @@ static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool sk
     const bool spai = (sm == UAAMG_SMOOTHER_SPAI0);
     // pre-smoothing, ends in T
     if (skip_first) {
-        if (spai) E.sweep<M_SPAI0>(l, SrcFirstSpai0{rhs, D.spai0_ready}, rhs, lhs, 0.f);
-        else E.sweep<M_JACOBI>(l, SrcFirstJacobi{rhs, wpre(0)}, rhs, lhs, wpre(1));
+        if (E.split(l)) {  // T is free until the second sweep writes it
+            if (spai) E.materialize(l, SrcFirstSpai0{rhs, D.spai0_ready}, T);
+            else E.materialize(l, SrcFirstJacobi{rhs, wpre(0)}, T);
+            if (spai) E.sweep<M_SPAI0>(l, SrcPlain{T}, rhs, lhs, 0.f);
+            else E.sweep<M_JACOBI>(l, SrcPlain{T}, rhs, lhs, wpre(1));
+        } else if (spai) {
+            E.sweep<M_SPAI0>(l, SrcFirstSpai0{rhs, D.spai0_ready}, rhs, lhs, 0.f);
+        } else {
+            E.sweep<M_JACOBI>(l, SrcFirstJacobi{rhs, wpre(0)}, rhs, lhs, wpre(1));
+        }
         if (spai) E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f, DotOut{nullptr, nullptr, nullptr}, true);
         else E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(2));
     } else {
@@ -844,6 +914,19 @@ static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool sk
     enqueue_precond(E, l + 1, P.lhs, P.rhs, true, DotOut{nullptr, nullptr, nullptr});
     if (l + 1 != h->nlev - 1) enqueue_precond(E, l + 1, P.lhs, P.rhs, false, DotOut{nullptr, nullptr, nullptr});
     // post-smoothing with reversed weights: T(+P x_c) -> lhs -> T -> lhs
+    if (E.split(l)) {  // T += P x_c in place (T is not read again before it is rewritten)
+        E.materialize(l, SrcProlong{T, P.lhs, 1.0f}, T);
+        if (spai) {
+            E.sweep<M_SPAI0>(l, SrcPlain{T}, rhs, lhs, 0.f);
+            E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f);
+            E.sweep<M_SPAI0>(l, SrcPlain{T}, rhs, lhs, 0.f, dot);
+        } else {
+            E.sweep<M_JACOBI>(l, SrcPlain{T}, rhs, lhs, wpre(2));
+            E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(1));
+            E.sweep<M_JACOBI>(l, SrcPlain{T}, rhs, lhs, wpre(0), dot);
+        }
+        return;
+    }
     if (spai) {
         E.sweep<M_SPAI0>(l, SrcProlong{T, P.lhs, 1.0f}, rhs, lhs, 0.f);
         E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f);

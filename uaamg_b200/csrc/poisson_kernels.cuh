@@ -358,6 +358,71 @@ __device__ __forceinline__ bool red_publish(double part, double* buf, unsigned* 
     total = block_reduce_n<MAX>(acc, rsh);
     return true;
 }
+// Deferred publication for a CTA that has stored the partials of its K slots
+// slot0, slot0 + stride, ... itself (buf + RED_HEADER + slot, thread 0): the
+// group tickets of all of them are taken at once at the end, and the CTA
+// completes every group (and the reduction) it finishes, with the same
+// partials and combination order as red_publish.  Returns true in the CTA
+// that completes the reduction (total valid in thread 0).
+template <bool MAX>
+__device__ __forceinline__ bool red_publish_strided(double* buf, unsigned* ticket, int slot0, int stride, int K,
+                                                    int count, double& total) {
+    __shared__ double rsh[8];
+    __shared__ int rdone[128];
+    __shared__ int rflag;
+    unsigned* gt = reinterpret_cast<unsigned*>(buf);
+    double* slots = buf + RED_HEADER;
+    double* groups = slots + count;
+    const int gs = red_group_size(count);
+    const int ng = (count + gs - 1) / gs;
+    bool fin = false;
+    for (int k0 = 0; k0 < K; k0 += (int)blockDim.x) {
+        const int k = k0 + (int)threadIdx.x;
+        int g = -1;
+        if (k < K) {
+            __threadfence();
+            const int slot = slot0 + k * stride;
+            const int gg = slot / gs;
+            const int gn = min(gs, count - gg * gs);
+            if (atomicAdd(&gt[gg], 1u) == (unsigned)gn - 1) g = gg;
+        }
+        rdone[threadIdx.x] = g;
+        __syncthreads();
+        for (int q = 0; q < (int)blockDim.x; ++q) {
+            const int gg = rdone[q];
+            if (gg < 0) continue;
+            __threadfence();
+            const int g0 = gg * gs;
+            const int gn = min(gs, count - g0);
+            double acc = 0.0;
+            for (int i = threadIdx.x; i < gn; i += blockDim.x) acc = red_combine<MAX>(acc, __ldcg(slots + g0 + i));
+            acc = block_reduce_n<MAX>(acc, rsh);
+            if (ng == 1) {
+                if (threadIdx.x == 0) gt[gg] = 0;
+                total = acc;
+                fin = true;
+                continue;
+            }
+            if (threadIdx.x == 0) {
+                gt[gg] = 0;
+                groups[gg] = acc;
+                __threadfence();
+                rflag = (atomicAdd(ticket, 1u) == (unsigned)ng - 1);
+            }
+            __syncthreads();
+            if (rflag) {
+                __threadfence();
+                double a2 = 0.0;
+                for (int i = threadIdx.x; i < ng; i += blockDim.x) a2 = red_combine<MAX>(a2, __ldcg(groups + i));
+                total = block_reduce_n<MAX>(a2, rsh);
+                fin = true;
+            }
+            __syncthreads();
+        }
+        __syncthreads();
+    }
+    return fin;
+}
 __device__ __forceinline__ bool reduce_sum(double part, double* buf, unsigned* ticket, int slot, int count,
                                            double& total) {
     return red_publish<false>(part, buf, ticket, slot, count, total);
@@ -631,31 +696,45 @@ struct Staged {
     float* cz;
 };
 
-// Issue the bulk copies of one leaf (thread 0) and return the byte count.
+// The bulk copies of one leaf (thread 0), in two parts: the coefficient
+// arrays, which do not change during a solve, are issued before the wait for
+// the previous kernel; x and b (and the SPAI0 array, built during a solve)
+// after it.  The barrier expects all bytes from the first part on.
 template <int MODE>
-__device__ __forceinline__ unsigned stage_issue(const DLevel& L, int leaf, unsigned fl, const float* x, const float* b,
-                                                const Staged& S, uint64_t* bar) {
-    const bool need_b = (MODE != M_LAPLACIAN);
-    const bool need_d = (MODE != M_RED && MODE != M_BLACK) && !(fl & TRIM_DIAG);
-    const bool need_i = (MODE == M_JACOBI || MODE == M_RED || MODE == M_BLACK) ? !(fl & TRIM_DIAG)
-                        : (MODE == M_SPAI0 ? !(fl & TRIM_SPAI0) : false);
-    unsigned bytes = 2048u;
-    bytes += need_b ? 2048u : 0u;
-    bytes += need_d ? 2048u : 0u;
-    bytes += need_i ? 2048u : 0u;
-    bytes += (fl & TRIM_X) ? 0u : 2048u;
-    bytes += (fl & TRIM_Y) ? 0u : 2048u;
-    bytes += (fl & TRIM_Z) ? 0u : 2048u;
-    mbar_expect_tx(bar, bytes);
+struct StageSet {
+    bool b, d, i, cx, cy, cz;
+    __device__ __forceinline__ StageSet(unsigned fl) {
+        b = (MODE != M_LAPLACIAN);
+        d = (MODE != M_RED && MODE != M_BLACK) && !(fl & TRIM_DIAG);
+        i = (MODE == M_JACOBI || MODE == M_RED || MODE == M_BLACK) ? !(fl & TRIM_DIAG)
+            : (MODE == M_SPAI0 ? !(fl & TRIM_SPAI0) : false);
+        cx = !(fl & TRIM_X);
+        cy = !(fl & TRIM_Y);
+        cz = !(fl & TRIM_Z);
+    }
+    __device__ __forceinline__ unsigned bytes() const {
+        return 2048u * (1u + (b ? 1u : 0u) + (d ? 1u : 0u) + (i ? 1u : 0u) + (cx ? 1u : 0u) + (cy ? 1u : 0u) +
+                        (cz ? 1u : 0u));
+    }
+};
+template <int MODE>
+__device__ __forceinline__ void stage_issue_static(const DLevel& L, int leaf, const StageSet<MODE>& Q, const Staged& S,
+                                                   uint64_t* bar) {
+    mbar_expect_tx(bar, Q.bytes());
+    const long long o = (long long)leaf * UAAMG_LEAF;
+    if (Q.d) bulk_g2s(S.d, L.diag + o, 2048u, bar);
+    if (Q.i && MODE != M_SPAI0) bulk_g2s(S.i, L.invdiag + o, 2048u, bar);
+    if (Q.cx) bulk_g2s(S.cx, L.cx + o, 2048u, bar);
+    if (Q.cy) bulk_g2s(S.cy, L.cy + o, 2048u, bar);
+    if (Q.cz) bulk_g2s(S.cz, L.cz + o, 2048u, bar);
+}
+template <int MODE>
+__device__ __forceinline__ void stage_issue_dyn(const DLevel& L, int leaf, const StageSet<MODE>& Q, const float* x,
+                                                const float* b, const Staged& S, uint64_t* bar) {
     const long long o = (long long)leaf * UAAMG_LEAF;
     bulk_g2s(S.x, x + o, 2048u, bar);
-    if (need_b) bulk_g2s(S.b, b + o, 2048u, bar);
-    if (need_d) bulk_g2s(S.d, L.diag + o, 2048u, bar);
-    if (need_i) bulk_g2s(S.i, (MODE == M_SPAI0 ? L.spai0 : L.invdiag) + o, 2048u, bar);
-    if (!(fl & TRIM_X)) bulk_g2s(S.cx, L.cx + o, 2048u, bar);
-    if (!(fl & TRIM_Y)) bulk_g2s(S.cy, L.cy + o, 2048u, bar);
-    if (!(fl & TRIM_Z)) bulk_g2s(S.cz, L.cz + o, 2048u, bar);
-    return bytes;
+    if (Q.b) bulk_g2s(S.b, b + o, 2048u, bar);
+    if (Q.i && MODE == M_SPAI0) bulk_g2s(S.i, L.spai0 + o, 2048u, bar);
 }
 
 __device__ __forceinline__ float4 s4(const float* s, int t) { return reinterpret_cast<const float4*>(s)[t]; }
@@ -762,67 +841,70 @@ __device__ __forceinline__ float4 staged_value(const DLevel& L, int leaf, int t,
     return res;
 }
 
-// Halo loads of one thread (issued while the bulk copies are in flight).
-__device__ __forceinline__ void staged_halo(const DLevel& L, int leaf, int t, const float* x, float4& hxp, float4& hxm,
-                                            float4& hyp, float4& hym, float4& hcxp, float4& hcyp, float& hz, float& hcz) {
+// Halo loads of one thread, in two parts: the neighbour leaves and their
+// face coefficients (static, before the wait) and the neighbours' x values
+// (after it, while the bulk copies are in flight).
+struct HaloNb {
+    int xp, xm, yp, ym, z;  // neighbour leaf whose face this thread reads, or -1
+};
+__device__ __forceinline__ void staged_halo_static(const DLevel& L, int leaf, int t, HaloNb& H, float4& hcxp,
+                                                   float4& hcyp, float& hcz) {
     const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
     const int* nb = L.nbr + (long long)leaf * 6;
     const float df = L.def_face;
-    hxp = hxm = hyp = hym = f4zero();
     hcxp = hcyp = f4splat(df);
-    hz = 0.f;
     hcz = df;
-    if (X == 7) {
-        int n = nb[1];
-        if (n >= 0) {
-            hxp = ld4(x, n, t - 112);
-            if (!(L.flags[n] & TRIM_X)) hcxp = ld4(L.cx, n, t - 112);
-        }
-    }
-    if (X == 0) {
-        int n = nb[0];
-        if (n >= 0) hxm = ld4(x, n, t + 112);
-    }
-    if (Y == 7) {
-        int n = nb[3];
-        if (n >= 0) {
-            hyp = ld4(x, n, t - 14);
-            if (!(L.flags[n] & TRIM_Y)) hcyp = ld4(L.cy, n, t - 14);
-        }
-    }
-    if (Y == 0) {
-        int n = nb[2];
-        if (n >= 0) hym = ld4(x, n, t + 14);
-    }
-    if (zh == 0) {
-        int n = nb[4];
-        if (n >= 0) hz = x[(long long)n * UAAMG_LEAF + 4 * t + 7];
-    } else {
-        int n = nb[5];
-        if (n >= 0) {
-            hz = x[(long long)n * UAAMG_LEAF + 4 * t - 4];
-            if (!(L.flags[n] & TRIM_Z)) hcz = L.cz[(long long)n * UAAMG_LEAF + 4 * t - 4];
-        }
-    }
+    H.xp = (X == 7) ? nb[1] : -1;
+    H.xm = (X == 0) ? nb[0] : -1;
+    H.yp = (Y == 7) ? nb[3] : -1;
+    H.ym = (Y == 0) ? nb[2] : -1;
+    H.z = (zh == 0) ? nb[4] : nb[5];
+    // a trimmed leaf stores its default coefficients (finalize_leaf), so the
+    // face values load without testing the neighbour's flags
+    if (H.xp >= 0) hcxp = ld4(L.cx, H.xp, t - 112);
+    if (H.yp >= 0) hcyp = ld4(L.cy, H.yp, t - 14);
+    if (zh == 1 && H.z >= 0) hcz = L.cz[(long long)H.z * UAAMG_LEAF + 4 * t - 4];
+}
+__device__ __forceinline__ void staged_halo_dyn(const float* x, int t, const HaloNb& H, float4& hxp, float4& hxm,
+                                                float4& hyp, float4& hym, float& hz) {
+    hxp = (H.xp >= 0) ? ld4(x, H.xp, t - 112) : f4zero();
+    hxm = (H.xm >= 0) ? ld4(x, H.xm, t + 112) : f4zero();
+    hyp = (H.yp >= 0) ? ld4(x, H.yp, t - 14) : f4zero();
+    hym = (H.ym >= 0) ? ld4(x, H.ym, t + 14) : f4zero();
+    hz = 0.f;
+    if (H.z >= 0) hz = x[(long long)H.z * UAAMG_LEAF + ((t & 1) ? 4 * t - 4 : 4 * t + 7)];
 }
 
+// resident CTAs per SM the staged kernels are compiled for: they are bound by
+// the latency of their copies, so occupancy sets their throughput
+#ifndef STAGED_MINB
+#define STAGED_MINB 12
+#endif
 #define STAGED_SMEM_DECL                                                         \
     __shared__ __align__(128) float sm_x[UAAMG_LEAF], sm_b[UAAMG_LEAF], sm_d[UAAMG_LEAF], \
         sm_i[UAAMG_LEAF], sm_cx[UAAMG_LEAF], sm_cy[UAAMG_LEAF], sm_cz[UAAMG_LEAF];      \
     __shared__ __align__(8) uint64_t sm_bar;                                     \
     const Staged S{sm_x, sm_b, sm_d, sm_i, sm_cx, sm_cy, sm_cz};
 
-// Stage + halo + wait; false if the wait timed out (error flagged).
+// Stage + halo + wait; false if the wait timed out (error flagged).  Waits
+// for the previous kernel (programmatic dependent launch) after the static
+// part.
 template <int MODE>
 __device__ __forceinline__ bool staged_prologue(const DLevel& L, int leaf, int t, const float* x, const float* b,
                                                 const Staged& S, uint64_t* bar, unsigned& fl, float4& hxp,
                                                 float4& hxm, float4& hyp, float4& hym, float4& hcxp, float4& hcyp,
                                                 float& hz, float& hcz, int* err) {
     fl = L.flags[leaf];
+    const StageSet<MODE> Q(fl);
+    HaloNb H;
+    staged_halo_static(L, leaf, t, H, hcxp, hcyp, hcz);
     if (t == 0) mbar_init(bar, 1);
     __syncthreads();
-    if (t == 0) stage_issue<MODE>(L, leaf, fl, x, b, S, bar);
-    staged_halo(L, leaf, t, x, hxp, hxm, hyp, hym, hcxp, hcyp, hz, hcz);
+    if (t == 0) stage_issue_static<MODE>(L, leaf, Q, S, bar);
+    griddep_wait();
+    griddep_launch();
+    if (t == 0) stage_issue_dyn<MODE>(L, leaf, Q, x, b, S, bar);
+    staged_halo_dyn(x, t, H, hxp, hxm, hyp, hym, hz);
     // every thread of the CTA agrees on the outcome, so no thread leaves a
     // later barrier short-handed
     const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0) != 0;
@@ -834,10 +916,8 @@ __device__ __forceinline__ bool staged_prologue(const DLevel& L, int leaf, int t
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(128) k_sweep_staged(DLevel L, const float* x, const float* b, float* out, float w,
+__global__ void __launch_bounds__(128, STAGED_MINB) k_sweep_staged(DLevel L, const float* x, const float* b, float* out, float w,
                                                       float wsor, float one_minus_wsor, DotOut dot, int* err) {
-    griddep_wait();
-    griddep_launch();
     STAGED_SMEM_DECL
     const int leaf = blockIdx.x, t = threadIdx.x;
     unsigned fl;
@@ -871,10 +951,8 @@ __global__ void __launch_bounds__(128) k_sweep_staged(DLevel L, const float* x, 
 }
 
 // residual + restriction with the fine leaf staged
-__global__ void __launch_bounds__(128) k_restrict_staged(DLevel L, const float* x, const float* b, float* coarse,
+__global__ void __launch_bounds__(128, STAGED_MINB) k_restrict_staged(DLevel L, const float* x, const float* b, float* coarse,
                                                          int* err) {
-    griddep_wait();
-    griddep_launch();
     STAGED_SMEM_DECL
     const int leaf = blockIdx.x, t = threadIdx.x;
     unsigned fl;

@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "poisson_kernels.cuh"
+#include "staged_pipe.cuh"
 
 namespace uaamg {
 
@@ -32,6 +33,7 @@ template <> struct H16<__half> {
         return *reinterpret_cast<unsigned*>(&h);
     }
     static __device__ __forceinline__ float to1(__half v) { return __half2float(v); }
+    static __device__ __forceinline__ float bits1(unsigned short u) { return __half2float(__ushort_as_half(u)); }
     static __device__ __forceinline__ __half from1(float v) { return __float2half_rn(v); }
 };
 template <> struct H16<__nv_bfloat16> {
@@ -44,6 +46,9 @@ template <> struct H16<__nv_bfloat16> {
         return *reinterpret_cast<unsigned*>(&h);
     }
     static __device__ __forceinline__ float to1(__nv_bfloat16 v) { return __bfloat162float(v); }
+    static __device__ __forceinline__ float bits1(unsigned short u) {
+        return __bfloat162float(__ushort_as_bfloat16(u));
+    }
     static __device__ __forceinline__ __nv_bfloat16 from1(float v) { return __float2bfloat16_rn(v); }
 };
 
@@ -106,6 +111,33 @@ template <typename T>
 __device__ __forceinline__ float4 ldi4(const MLevel<T>& L, long long leaf, int t) {
     return f4scale(ldh4(L.invdiag, leaf, t), L.ics);
 }
+
+// storage and level traits of the pipelined staged kernels (staged_pipe.cuh)
+template <typename T>
+struct PipeE16 {
+    static constexpr unsigned ARR = UAAMG_LEAF * 2;
+    static __device__ __forceinline__ float4 s4(const unsigned char* a, int t) {
+        const uint2 u = reinterpret_cast<const uint2*>(a)[t];
+        const float2 p = H16<T>::to2(u.x), q = H16<T>::to2(u.y);
+        return make_float4(p.x, p.y, q.x, q.y);
+    }
+    static __device__ __forceinline__ float s1(const unsigned char* a, int i) {
+        return H16<T>::bits1(reinterpret_cast<const unsigned short*>(a)[i]);
+    }
+    static __device__ __forceinline__ float4 g4(const T* p, long long leaf, int t) { return ldh4(p, leaf, t); }
+    static __device__ __forceinline__ float g1(const T* p, long long i) { return ldh1(p, i); }
+    static __device__ __forceinline__ void st(T* p, long long leaf, int t, float4 v) { sth4(p, leaf, t, v); }
+    static __device__ __forceinline__ void st1(T* p, long long i, float v) { p[i] = H16<T>::from1(v); }
+};
+template <> struct PipeE<__half> : PipeE16<__half> {};
+template <> struct PipeE<__nv_bfloat16> : PipeE16<__nv_bfloat16> {};
+template <typename T>
+struct PipeLv<MLevel<T>> {
+    using E = T;
+    static constexpr bool SCALED = true;
+    static __device__ __forceinline__ float cs(const MLevel<T>& L) { return L.cs; }
+    static __device__ __forceinline__ float ics(const MLevel<T>& L) { return L.ics; }
+};
 
 // lhs sources (16-bit vectors)
 template <typename T>
@@ -391,242 +423,242 @@ __global__ void __launch_bounds__(256) k_mconvert(const float* in, T* out, long 
 }
 
 // ---------------------------------------------------------------------------
-// z-line kernels: one thread per 8-voxel z-line (x = t >> 3, y = t & 7,
-// offset 64x + 8y + z), 64 threads per leaf.  A line of a 16-bit array is
-// one 16-byte load, so a warp reads 512 contiguous bytes per array and each
-// thread keeps ~10 independent loads in flight; the +-z neighbours inside the
-// line are register shifts.  Same per-voxel operations and order as
-// mstencil4 / mjacobi_value.
-struct F8 {
-    float v[8];
+// ---------------------------------------------------------------------------
+// Staged 16-bit sweeps for large levels: the leaf's 16-bit arrays (1 KB each)
+// are bulk-copied into shared memory (the coefficient arrays before the wait
+// for the previous kernel, x and b after it) while each thread loads its
+// halo values from the neighbour leaves; a thread then computes its 4
+// z-consecutive voxels from shared memory with the operation sequence of
+// mstencil4 / mjacobi_value, so a staged sweep gives the same values as
+// k_msweep with a plain source.
+struct MStaged {
+    uint16_t* x;
+    uint16_t* b;
+    uint16_t* d;
+    uint16_t* i;
+    uint16_t* cx;
+    uint16_t* cy;
+    uint16_t* cz;
 };
 template <typename T>
-__device__ __forceinline__ F8 ldl8(const T* p, long long leaf, int line) {  // 8 values of a z-line
-    const uint4 u = reinterpret_cast<const uint4*>(p)[leaf * 64 + line];
-    F8 r;
-    float2 a = H16<T>::to2(u.x), b = H16<T>::to2(u.y), c = H16<T>::to2(u.z), d = H16<T>::to2(u.w);
-    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = b.x; r.v[3] = b.y;
-    r.v[4] = c.x; r.v[5] = c.y; r.v[6] = d.x; r.v[7] = d.y;
-    return r;
+__device__ __forceinline__ float4 msh4(const uint16_t* s, int t) {
+    const uint2 u = reinterpret_cast<const uint2*>(s)[t];
+    const float2 a = H16<T>::to2(u.x), b = H16<T>::to2(u.y);
+    return make_float4(a.x, a.y, b.x, b.y);
 }
 template <typename T>
-__device__ __forceinline__ void stl8(T* p, long long leaf, int line, const F8& f) {
-    uint4 u;
-    u.x = H16<T>::from2(f.v[0], f.v[1]);
-    u.y = H16<T>::from2(f.v[2], f.v[3]);
-    u.z = H16<T>::from2(f.v[4], f.v[5]);
-    u.w = H16<T>::from2(f.v[6], f.v[7]);
-    reinterpret_cast<uint4*>(p)[leaf * 64 + line] = u;
-}
-__device__ __forceinline__ void stl8(float* p, long long leaf, int line, const F8& f) {
-    float4* q = reinterpret_cast<float4*>(p + leaf * UAAMG_LEAF + line * 8);
-    q[0] = make_float4(f.v[0], f.v[1], f.v[2], f.v[3]);
-    q[1] = make_float4(f.v[4], f.v[5], f.v[6], f.v[7]);
-}
-__device__ __forceinline__ F8 f8splat(float x) {
-    F8 r;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) r.v[j] = x;
-    return r;
-}
-__device__ __forceinline__ F8 f8scale(F8 a, float s) {
-#pragma unroll
-    for (int j = 0; j < 8; ++j) a.v[j] = __fmul_rn(a.v[j], s);
-    return a;
-}
-template <typename T>
-__device__ __forceinline__ F8 ldc8(const MLevel<T>& L, const T* a, long long leaf, int line) {
-    return f8scale(ldl8(a, leaf, line), L.cs);
+__device__ __forceinline__ float msh1(const uint16_t* s, int i) {
+    return H16<T>::bits1(s[i]);
 }
 
-// line sources
-template <typename T>
-struct LSrcPlain {
-    const T* x;
-    __device__ __forceinline__ F8 line(const MLevel<T>&, int leaf, int ln) const { return ldl8(x, leaf, ln); }
-    __device__ __forceinline__ float one(const MLevel<T>&, int leaf, int off) const {
-        return ldh1(x, (long long)leaf * UAAMG_LEAF + off);
-    }
-};
-template <typename T>
-struct LSrcFirstJacobi {  // w * (invdiag * b)
-    const T* b;
-    float w;
-    __device__ __forceinline__ F8 line(const MLevel<T>& L, int leaf, int ln) const {
-        const F8 bb = ldc8(L, b, leaf, ln);
-        const F8 iv = (L.flags[leaf] & TRIM_DIAG) ? f8splat(L.def_invdiag) : f8scale(ldl8(L.invdiag, leaf, ln), L.ics);
-        F8 r;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) r.v[j] = __fmul_rn(w, __fmul_rn(iv.v[j], bb.v[j]));
-        return r;
-    }
-    __device__ __forceinline__ float one(const MLevel<T>& L, int leaf, int off) const {
-        const long long i = (long long)leaf * UAAMG_LEAF + off;
-        const float iv = (L.flags[leaf] & TRIM_DIAG) ? L.def_invdiag : __fmul_rn(ldh1(L.invdiag, i), L.ics);
-        return __fmul_rn(w, __fmul_rn(iv, ldc1(L, b, i)));
-    }
-};
-template <typename T>
-struct LSrcProlong {  // x + coarse parent value at active voxels
-    const T* x;
-    const T* xc;
-    __device__ __forceinline__ F8 line(const MLevel<T>& L, int leaf, int ln) const {
-        F8 v = ldl8(x, leaf, ln);
-        const int X = ln >> 3, Y = ln & 7;
-        const unsigned m = (unsigned)((L.mask[(long long)leaf * 8 + X] >> (8 * Y)) & 0xFFull);
-        if (!m) return v;
-        const int P = L.parent[leaf];
-        const int o = L.octant[leaf];
-        const long long cb = (long long)P * UAAMG_LEAF + (((o >> 2) & 1) * 4 + (X >> 1)) * 64 +
-                             (((o >> 1) & 1) * 4 + (Y >> 1)) * 8 + (o & 1) * 4;
-        const uint2 u = *reinterpret_cast<const uint2*>(xc + cb);  // 4 coarse values (z pairs)
-        const float2 c01 = H16<T>::to2(u.x), c23 = H16<T>::to2(u.y);
-        const float c[4] = {c01.x, c01.y, c23.x, c23.y};
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-            if ((m >> j) & 1) v.v[j] = __fadd_rn(v.v[j], c[j >> 1]);
-        return v;
-    }
-    __device__ __forceinline__ float one(const MLevel<T>& L, int leaf, int off) const {
-        float v = ldh1(x, (long long)leaf * UAAMG_LEAF + off);
-        if (!((L.mask[(long long)leaf * 8 + (off >> 6)] >> (off & 63)) & 1ull)) return v;
-        const int P = L.parent[leaf];
-        const int o = L.octant[leaf];
-        const int X = off >> 6, Y = (off >> 3) & 7, Z = off & 7;
-        const int coff =
-            (((o >> 2) & 1) * 4 + (X >> 1)) * 64 + (((o >> 1) & 1) * 4 + (Y >> 1)) * 8 + (o & 1) * 4 + (Z >> 1);
-        return __fadd_rn(v, ldh1(xc, (long long)P * UAAMG_LEAF + coff));
+struct MStageSet {
+    bool d, i, cx, cy, cz;
+    __device__ __forceinline__ MStageSet(unsigned fl) {
+        d = i = !(fl & TRIM_DIAG);
+        cx = !(fl & TRIM_X);
+        cy = !(fl & TRIM_Y);
+        cz = !(fl & TRIM_Z);
     }
 };
 
-template <typename T, class Src>
-__device__ __forceinline__ void mstencil8(const MLevel<T>& L, int leaf, int ln, const Src& src, F8& xc, F8& off) {
-    const int X = ln >> 3, Y = ln & 7;
-    const unsigned fl = L.flags[leaf];
+// thread 0: arrive with the byte count of all copies and issue the
+// coefficient copies (RESID needs no 1/diag)
+template <typename T, bool RESID>
+__device__ __forceinline__ void mstage_static(const MLevel<T>& L, int leaf, const MStageSet& Q, const MStaged& S,
+                                              uint64_t* bar) {
+    const bool ni = Q.i && !RESID;
+    const unsigned bytes = 1024u * (2u + (Q.d ? 1u : 0u) + (ni ? 1u : 0u) + (Q.cx ? 1u : 0u) + (Q.cy ? 1u : 0u) +
+                                    (Q.cz ? 1u : 0u));
+    mbar_expect_tx(bar, bytes);
+    const long long o = (long long)leaf * UAAMG_LEAF;
+    if (Q.d) bulk_g2s(S.d, L.diag + o, 1024u, bar);
+    if (ni) bulk_g2s(S.i, L.invdiag + o, 1024u, bar);
+    if (Q.cx) bulk_g2s(S.cx, L.cx + o, 1024u, bar);
+    if (Q.cy) bulk_g2s(S.cy, L.cy + o, 1024u, bar);
+    if (Q.cz) bulk_g2s(S.cz, L.cz + o, 1024u, bar);
+}
+
+// a thread's halo: neighbour leaves and their face coefficients (static),
+// then the neighbours' x values (after the wait)
+struct MHalo {
+    int xp, xm, yp, ym, z;
+    float4 cxp, cyp;
+    float cz;
+    float4 xpv, xmv, ypv, ymv;
+    float zv;
+};
+template <typename T>
+__device__ __forceinline__ void mhalo_static(const MLevel<T>& L, int leaf, int t, MHalo& H) {
+    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
     const int* nb = L.nbr + (long long)leaf * 6;
     const float df = L.def_face;
-    xc = src.line(L, leaf, ln);
-    F8 xp, xm, yp, ym, cxp, cyp;
-    if (X < 7) {
-        xp = src.line(L, leaf, ln + 8);
-        cxp = (fl & TRIM_X) ? f8splat(df) : ldc8(L, L.cx, leaf, ln + 8);
+    H.xp = (X == 7) ? nb[1] : -1;
+    H.xm = (X == 0) ? nb[0] : -1;
+    H.yp = (Y == 7) ? nb[3] : -1;
+    H.ym = (Y == 0) ? nb[2] : -1;
+    H.z = (zh == 0) ? nb[4] : nb[5];
+    H.cxp = H.cyp = f4splat(df);
+    H.cz = df;
+    // flags and values load together; a trimmed neighbour reads the FP32
+    // default (its stored 16-bit value is the rounded default)
+    if (H.xp >= 0) {
+        const unsigned f = L.flags[H.xp];
+        const float4 v = ldc4(L, L.cx, H.xp, t - 112);
+        if (!(f & TRIM_X)) H.cxp = v;
+    }
+    if (H.yp >= 0) {
+        const unsigned f = L.flags[H.yp];
+        const float4 v = ldc4(L, L.cy, H.yp, t - 14);
+        if (!(f & TRIM_Y)) H.cyp = v;
+    }
+    if (zh == 1 && H.z >= 0) {
+        const unsigned f = L.flags[H.z];
+        const float v = ldc1(L, L.cz, (long long)H.z * UAAMG_LEAF + 4 * t - 4);
+        if (!(f & TRIM_Z)) H.cz = v;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void mhalo_dyn(const T* x, int t, MHalo& H) {
+    H.xpv = (H.xp >= 0) ? ldh4(x, H.xp, t - 112) : f4zero();
+    H.xmv = (H.xm >= 0) ? ldh4(x, H.xm, t + 112) : f4zero();
+    H.ypv = (H.yp >= 0) ? ldh4(x, H.yp, t - 14) : f4zero();
+    H.ymv = (H.ym >= 0) ? ldh4(x, H.ym, t + 14) : f4zero();
+    H.zv = 0.f;
+    if (H.z >= 0) H.zv = ldh1(x, (long long)H.z * UAAMG_LEAF + ((t & 1) ? 4 * t - 4 : 4 * t + 7));
+}
+
+#ifndef MSTAGED_MINB
+#define MSTAGED_MINB 12
+#endif
+#define MSTAGED_SMEM_DECL                                                                                    \
+    __shared__ __align__(128) uint16_t msm_x[UAAMG_LEAF], msm_b[UAAMG_LEAF], msm_d[UAAMG_LEAF],             \
+        msm_i[UAAMG_LEAF], msm_cx[UAAMG_LEAF], msm_cy[UAAMG_LEAF], msm_cz[UAAMG_LEAF];                      \
+    __shared__ __align__(8) uint64_t msm_bar;                                                                \
+    const MStaged S{msm_x, msm_b, msm_d, msm_i, msm_cx, msm_cy, msm_cz};
+
+// static part, wait, x/b copies, halo, bounded wait on the copies; false if
+// the wait timed out (error flagged)
+template <typename T, bool RESID>
+__device__ __forceinline__ bool mstaged_prologue(const MLevel<T>& L, int leaf, int t, const T* x, const T* b,
+                                                 const MStaged& S, uint64_t* bar, unsigned& fl, MHalo& H, int* err) {
+    fl = L.flags[leaf];
+    const MStageSet Q(fl);
+    mhalo_static(L, leaf, t, H);
+    if (t == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (t == 0) mstage_static<T, RESID>(L, leaf, Q, S, bar);
+    griddep_wait();
+    griddep_launch();
+    if (t == 0) {
+        const long long o = (long long)leaf * UAAMG_LEAF;
+        bulk_g2s(S.x, x + o, 1024u, bar);
+        bulk_g2s(S.b, b + o, 1024u, bar);
+    }
+    mhalo_dyn(x, t, H);
+    const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0) != 0;
+    if (!ok) {
+        if (t == 0 && err) atomicExch(err, 1);
+        mbar_wait_bounded(bar, 0);
+    }
+    return ok;
+}
+
+// weighted Jacobi (RESID false) or residual (RESID true) of the thread's 4
+// voxels from the staged leaf
+template <bool RESID, typename T>
+__device__ __forceinline__ float4 mstaged_value(const MLevel<T>& L, int leaf, int t, unsigned fl, const MStaged& S,
+                                                const MHalo& H, float w) {
+    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
+    const float df = L.def_face;
+    const float4 dfv = f4splat(df);
+    const float cs = L.cs;
+    const float4 xc = msh4<T>(S.x, t);
+    const float4 xp = (X < 7) ? msh4<T>(S.x, t + 16) : H.xpv;
+    const float4 xm = (X > 0) ? msh4<T>(S.x, t - 16) : H.xmv;
+    const float4 yp = (Y < 7) ? msh4<T>(S.x, t + 2) : H.ypv;
+    const float4 ym = (Y > 0) ? msh4<T>(S.x, t - 2) : H.ymv;
+    const float4 cxp = (X < 7) ? ((fl & TRIM_X) ? dfv : f4scale(msh4<T>(S.cx, t + 16), cs)) : H.cxp;
+    const float4 cyp = (Y < 7) ? ((fl & TRIM_Y) ? dfv : f4scale(msh4<T>(S.cy, t + 2), cs)) : H.cyp;
+    const float4 cxm = (fl & TRIM_X) ? dfv : f4scale(msh4<T>(S.cx, t), cs);
+    const float4 cym = (fl & TRIM_Y) ? dfv : f4scale(msh4<T>(S.cy, t), cs);
+    const float4 czo = (fl & TRIM_Z) ? dfv : f4scale(msh4<T>(S.cz, t), cs);
+    float zp3, zm0, czp3;
+    if (zh == 0) {
+        zp3 = msh1<T>(S.x, 4 * t + 4);
+        czp3 = (fl & TRIM_Z) ? df : __fmul_rn(msh1<T>(S.cz, 4 * t + 4), cs);
+        zm0 = H.zv;
     } else {
-        const int n = nb[1];
-        if (n >= 0) {
-            xp = src.line(L, n, ln - 56);
-            cxp = (L.flags[n] & TRIM_X) ? f8splat(df) : ldc8(L, L.cx, n, ln - 56);
-        } else {
-            xp = f8splat(0.f);
-            cxp = f8splat(df);
-        }
+        zm0 = msh1<T>(S.x, 4 * t - 1);
+        zp3 = H.zv;
+        czp3 = H.cz;
     }
-    if (X > 0) {
-        xm = src.line(L, leaf, ln - 8);
-    } else {
-        const int n = nb[0];
-        xm = (n >= 0) ? src.line(L, n, ln + 56) : f8splat(0.f);
-    }
-    if (Y < 7) {
-        yp = src.line(L, leaf, ln + 1);
-        cyp = (fl & TRIM_Y) ? f8splat(df) : ldc8(L, L.cy, leaf, ln + 1);
-    } else {
-        const int n = nb[3];
-        if (n >= 0) {
-            yp = src.line(L, n, ln - 7);
-            cyp = (L.flags[n] & TRIM_Y) ? f8splat(df) : ldc8(L, L.cy, n, ln - 7);
-        } else {
-            yp = f8splat(0.f);
-            cyp = f8splat(df);
-        }
-    }
-    if (Y > 0) {
-        ym = src.line(L, leaf, ln - 1);
-    } else {
-        const int n = nb[2];
-        ym = (n >= 0) ? src.line(L, n, ln + 7) : f8splat(0.f);
-    }
-    const F8 cxm = (fl & TRIM_X) ? f8splat(df) : ldc8(L, L.cx, leaf, ln);
-    const F8 cym = (fl & TRIM_Y) ? f8splat(df) : ldc8(L, L.cy, leaf, ln);
-    const F8 czo = (fl & TRIM_Z) ? f8splat(df) : ldc8(L, L.cz, leaf, ln);
-    // the line's ends: z = -1 from the -z leaf, z = 8 (value and c_z) from the +z leaf
-    const int nzm = nb[4], nzp = nb[5];
-    const float zm0 = nzm >= 0 ? src.one(L, nzm, ln * 8 + 7) : 0.f;
-    float zp7 = 0.f, czp7 = df;
-    if (nzp >= 0) {
-        zp7 = src.one(L, nzp, ln * 8);
-        czp7 = (L.flags[nzp] & TRIM_Z) ? df : ldc1(L, L.cz, (long long)nzp * UAAMG_LEAF + ln * 8);
-    }
+    const float zp[4] = {xc.y, xc.z, xc.w, zp3};
+    const float zm[4] = {zm0, xc.x, xc.y, xc.z};
+    const float czp[4] = {czo.y, czo.z, czo.w, czp3};
+    float4 off;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const float zp = j < 7 ? xc.v[j + 1] : zp7;
-        const float zm = j > 0 ? xc.v[j - 1] : zm0;
-        const float czp = j < 7 ? czo.v[j + 1] : czp7;
-        float f1 = __fmul_rn(xp.v[j], cxp.v[j]);
-        float f2 = __fmul_rn(xm.v[j], cxm.v[j]);
-        float f3 = __fmul_rn(yp.v[j], cyp.v[j]);
-        float f4 = __fmul_rn(ym.v[j], cym.v[j]);
-        float f5 = __fmul_rn(zp, czp);
-        float f6 = __fmul_rn(zm, czo.v[j]);
+    for (int j = 0; j < 4; ++j) {
+        float f1 = __fmul_rn(f4get(xp, j), f4get(cxp, j));
+        float f2 = __fmul_rn(f4get(xm, j), f4get(cxm, j));
+        float f3 = __fmul_rn(f4get(yp, j), f4get(cyp, j));
+        float f4 = __fmul_rn(f4get(ym, j), f4get(cym, j));
+        float f5 = __fmul_rn(zp[j], czp[j]);
+        float f6 = __fmul_rn(zm[j], f4get(czo, j));
         f1 = __fadd_rn(f1, f2);
         f3 = __fadd_rn(f3, f4);
         f5 = __fadd_rn(f5, f6);
         f1 = __fadd_rn(f1, f3);
-        off.v[j] = __fadd_rn(f1, f5);
+        f1 = __fadd_rn(f1, f5);
+        f4set(off, j, f1);
     }
-}
-
-template <bool RESID, typename T, class Src>
-__device__ __forceinline__ F8 mjacobi8(const MLevel<T>& L, int leaf, int ln, const Src& src, const T* b, float w) {
-    F8 xc, off;
-    mstencil8(L, leaf, ln, src, xc, off);
-    const int X = ln >> 3, Y = ln & 7;
-    const unsigned m = (unsigned)((L.mask[(long long)leaf * 8 + X] >> (8 * Y)) & 0xFFull);
-    const unsigned fl = L.flags[leaf];
-    const F8 dg = (fl & TRIM_DIAG) ? f8splat(L.def_diag) : ldc8(L, L.diag, leaf, ln);
-    const F8 bb = ldc8(L, b, leaf, ln);
-    F8 res;
+    const unsigned m = mask4(L.mask, leaf, t);
+    const float4 dg = (fl & TRIM_DIAG) ? f4splat(L.def_diag) : f4scale(msh4<T>(S.d, t), cs);
+    const float4 bb = f4scale(msh4<T>(S.b, t), cs);
+    float4 res;
     if (RESID) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) res.v[j] = __fsub_rn(bb.v[j], __fmaf_rn(xc.v[j], dg.v[j], off.v[j]));
+        for (int j = 0; j < 4; ++j)
+            f4set(res, j, __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j))));
     } else {
-        const F8 iv = (fl & TRIM_DIAG) ? f8splat(L.def_invdiag) : f8scale(ldl8(L.invdiag, leaf, ln), L.ics);
+        const float4 iv = (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : f4scale(msh4<T>(S.i, t), L.ics);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            float r = __fsub_rn(bb.v[j], __fmaf_rn(xc.v[j], dg.v[j], off.v[j]));
-            r = __fmul_rn(r, iv.v[j]);
-            res.v[j] = __fmaf_rn(w, r, xc.v[j]);
+        for (int j = 0; j < 4; ++j) {
+            float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
+            r = __fmul_rn(r, f4get(iv, j));
+            f4set(res, j, __fmaf_rn(w, r, f4get(xc, j)));
         }
     }
-#pragma unroll
-    for (int j = 0; j < 8; ++j)
-        if (!((m >> j) & 1)) res.v[j] = 0.f;
+    if (!(m & 1)) res.x = 0.f;
+    if (!(m & 2)) res.y = 0.f;
+    if (!(m & 4)) res.z = 0.f;
+    if (!(m & 8)) res.w = 0.f;
     return res;
 }
 
-template <typename T, typename TOut, class Src>
-__global__ void __launch_bounds__(64) k_msweep8(MLevel<T> L, Src src, const T* b, TOut* out, float w, DotOut dot,
-                                               const float* zscale) {
-    griddep_wait();
-    griddep_launch();
-    const int leaf = blockIdx.x, ln = threadIdx.x;
-    F8 res = mjacobi8<false>(L, leaf, ln, src, b, w);
-    if (zscale) res = f8scale(res, *zscale);
-    stl8(out, leaf, ln, res);
+// One staged Jacobi sweep with a plain source; TOut float (with zscale and
+// the optional z.r) for the last sweep of level 0, as k_msweep.
+template <typename T, typename TOut>
+__global__ void __launch_bounds__(128, MSTAGED_MINB) k_msweep_staged(MLevel<T> L, const T* x, const T* b, TOut* out, float w,
+                                                       DotOut dot, const float* zscale, int* err) {
+    MSTAGED_SMEM_DECL
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    unsigned fl;
+    MHalo H;
+    const bool ok = mstaged_prologue<T, false>(L, leaf, t, x, b, S, &msm_bar, fl, H, err);
+    float4 res = f4zero();
+    if (ok) {
+        res = mstaged_value<false>(L, leaf, t, fl, S, H, w);
+        if (zscale) res = f4scale(res, *zscale);
+        stv4(out, leaf, t, res);
+    }
     if (dot.r) {
-        __shared__ double shd[2];
-        const float4* rp = reinterpret_cast<const float4*>(dot.r + (long long)leaf * UAAMG_LEAF + ln * 8);
-        const float4 r0 = rp[0], r1 = rp[1];
-        double s = (double)res.v[0] * r0.x + (double)res.v[1] * r0.y + (double)res.v[2] * r0.z +
-                   (double)res.v[3] * r0.w + (double)res.v[4] * r1.x + (double)res.v[5] * r1.y +
-                   (double)res.v[6] * r1.z + (double)res.v[7] * r1.w;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(FULLMASK, s, o);
-        if ((threadIdx.x & 31) == 0) shd[threadIdx.x >> 5] = s;
-        __syncthreads();
-        const double part = shd[0] + shd[1];
+        __shared__ double shd[4];
+        const float4 rr = ld4(dot.r, leaf, t);
+        const double s = (double)res.x * rr.x + (double)res.y * rr.y + (double)res.z * rr.z + (double)res.w * rr.w;
+        const double part = block_sum128(s, shd);
         double tot;
         if (reduce_sum(part, dot.partials, &dot.st->ticket[0], leaf, (int)gridDim.x, tot)) {
-            if (threadIdx.x == 0) {
+            if (t == 0) {
                 PcgState* st = dot.st;
                 const float rho_new = (float)tot;
                 st->rho_new = rho_new;
@@ -638,33 +670,52 @@ __global__ void __launch_bounds__(64) k_msweep8(MLevel<T> L, Src src, const T* b
     }
 }
 
+// staged residual + restriction into the next level's 16-bit rhs (as k_mrestrict)
 template <typename T>
-__global__ void __launch_bounds__(64) k_mrestrict8(MLevel<T> L, const T* x, const T* b, T* coarse, float coarse_ics) {
+__global__ void __launch_bounds__(128, MSTAGED_MINB) k_mrestrict_staged(MLevel<T> L, const T* x, const T* b, T* coarse,
+                                                          float coarse_ics, int* err) {
+    MSTAGED_SMEM_DECL
+    __shared__ __align__(16) float rs[UAAMG_LEAF];
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    unsigned fl;
+    MHalo H;
+    if (!mstaged_prologue<T, true>(L, leaf, t, x, b, S, &msm_bar, fl, H, err)) return;
+    reinterpret_cast<float4*>(rs)[t] = mstaged_value<true>(L, leaf, t, fl, S, H, 0.f);
+    __syncthreads();
+    if (t < 64) {
+        const int i = t >> 4, j = (t >> 2) & 3, k = t & 3;
+        const uint64_t* mk = L.mask + (long long)leaf * 8;
+        float s = 0.f;
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    const int fo = ((2 * i + ii) << 6) | ((2 * j + jj) << 3) | (2 * k + kk);
+                    if ((mk[fo >> 6] >> (fo & 63)) & 1ull) s = __fadd_rn(s, rs[fo]);
+                }
+        const int o = L.octant[leaf];
+        const int coff = ((((o >> 2) & 1) * 4 + i) << 6) | ((((o >> 1) & 1) * 4 + j) << 3) | ((o & 1) * 4 + k);
+        coarse[(long long)L.parent[leaf] * UAAMG_LEAF + coff] =
+            H16<T>::from1(__fmul_rn(__fmul_rn(s, 0.125f), coarse_ics));
+    }
+}
+
+// A computed source stored as a 16-bit vector (zero off the DOF): the first
+// sweep's w * (1/diag * b), or the prolongation-add x + P x_c (in place)
+template <typename T, class Src>
+__global__ void __launch_bounds__(128) k_mmaterialize(MLevel<T> L, Src src, T* out) {
     griddep_wait();
     griddep_launch();
-    __shared__ float rs[UAAMG_LEAF];
-    const int leaf = blockIdx.x, ln = threadIdx.x;
-    const F8 r = mjacobi8<true>(L, leaf, ln, LSrcPlain<T>{x}, b, 0.f);
-    float4* q = reinterpret_cast<float4*>(rs + ln * 8);
-    q[0] = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
-    q[1] = make_float4(r.v[4], r.v[5], r.v[6], r.v[7]);
-    __syncthreads();
-    const int t = threadIdx.x;  // 64 coarse voxels of the octant
-    const int i = t >> 4, j = (t >> 2) & 3, k = t & 3;
-    const uint64_t* mk = L.mask + (long long)leaf * 8;
-    float s = 0.f;
-#pragma unroll
-    for (int ii = 0; ii < 2; ++ii)
-#pragma unroll
-        for (int jj = 0; jj < 2; ++jj)
-#pragma unroll
-            for (int kk = 0; kk < 2; ++kk) {
-                const int fo = ((2 * i + ii) << 6) | ((2 * j + jj) << 3) | (2 * k + kk);
-                if ((mk[fo >> 6] >> (fo & 63)) & 1ull) s = __fadd_rn(s, rs[fo]);
-            }
-    const int o = L.octant[leaf];
-    const int coff = ((((o >> 2) & 1) * 4 + i) << 6) | ((((o >> 1) & 1) * 4 + j) << 3) | ((o & 1) * 4 + k);
-    coarse[(long long)L.parent[leaf] * UAAMG_LEAF + coff] = H16<T>::from1(__fmul_rn(__fmul_rn(s, 0.125f), coarse_ics));
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    float4 v = src.get4(L, leaf, t);
+    const unsigned m = mask4(L.mask, leaf, t);
+    if (!(m & 1)) v.x = 0.f;
+    if (!(m & 2)) v.y = 0.f;
+    if (!(m & 4)) v.z = 0.f;
+    if (!(m & 8)) v.w = 0.f;
+    sth4(out, leaf, t, v);
 }
 
 // ---------------------------------------------------------------------------
