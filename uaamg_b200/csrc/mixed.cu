@@ -249,17 +249,20 @@ static void menq_visit(MEnq& E, int l, bool skip_first, DotOut dot, float* z) {
     const bool split = g_use_staged && L.nl >= SPLIT_MIN_LEAVES;
     int* err = &h->st->error;
     const size_t psm = pipe_smem_bytes<MLevel<T>>();
+    const bool pipe = staged && L.nl >= PIPE_MIN_LEAVES;
     auto sweep = [&](const T* x, T* out, float w) {  // plain source
-        if (staged)
+        if (pipe)
             E.run_pipe("jacobi staged", l, k_pipe<M_JACOBI, MLevel<T>, T, false>, L.nl, psm, L, x, (const T*)rhs, out,
                        w, 0.f, 0.f, nodot, ns, 0.f, err);
+        else if (staged)
+            E.run("jacobi staged", l, k_msweep_staged<T, T>, g, 128, L, x, (const T*)rhs, out, w, nodot, ns, err);
         else
             E.run("jacobi", l, k_msweep<T, T, MSrcPlain<T>>, g, 128, L, MSrcPlain<T>{x}, (const T*)rhs, out, w, nodot,
                   ns);
     };
     if (skip_first) {
         if (split) {
-            E.run("materialize first", l, k_mmaterialize<T, MSrcFirstJacobi<T>>, g, 128, L,
+            E.run("materialize first", l, k_mmaterialize<T, MSrcFirstJacobi<T>>, elem_grid(L.nl), 128, L,
                   MSrcFirstJacobi<T>{rhs, wpre(0)}, tmp);
             sweep(tmp, lhs, wpre(1));
         } else {
@@ -274,16 +277,19 @@ static void menq_visit(MEnq& E, int l, bool skip_first, DotOut dot, float* z) {
     }
     const float cics = 1.0f / level_scale(h->lv[l + 1].L);
     T* crhs = (T*)M->lv[l + 1].rhs;
-    if (staged)
+    if (pipe)  // the pipelined kernel computes in stored units: its scale is cs / cs'
         E.run_pipe("restrict staged", l, k_pipe<M_RESIDUAL, MLevel<T>, T, true>, L.nl, psm, L, (const T*)tmp,
-                   (const T*)rhs, crhs, 0.f, 0.f, 0.f, nodot, ns, cics, err);
+                   (const T*)rhs, crhs, 0.f, 0.f, 0.f, nodot, ns, L.cs * cics, err);
+    else if (staged)
+        E.run("restrict staged", l, k_mrestrict_staged<T>, g, 128, L, (const T*)tmp, (const T*)rhs, crhs, cics, err);
     else
         E.run("restrict", l, k_mrestrict<T>, g, 128, L, (const T*)tmp, (const T*)rhs, crhs, cics);
     menq_visit<T>(E, l + 1, true, nodot, nullptr);
     if (l + 1 != last) menq_visit<T>(E, l + 1, false, nodot, nullptr);
     const T* clhs = (const T*)M->lv[l + 1].lhs;
     if (split) {  // tmp += P x_c in place (tmp is rewritten before it is read again)
-        E.run("materialize prolong", l, k_mmaterialize<T, MSrcProlong<T>>, g, 128, L, MSrcProlong<T>{tmp, clhs}, tmp);
+        E.run("materialize prolong", l, k_mmaterialize<T, MSrcProlong<T>>, elem_grid(L.nl), 128, L,
+              MSrcProlong<T>{tmp, clhs}, tmp);
         sweep(tmp, lhs, wpre(2));
     } else {
         E.run("jacobi prolong", l, k_msweep<T, T, MSrcProlong<T>>, g, 128, L, MSrcProlong<T>{tmp, clhs},
@@ -291,9 +297,12 @@ static void menq_visit(MEnq& E, int l, bool skip_first, DotOut dot, float* z) {
     }
     sweep(lhs, tmp, wpre(1));
     if (l == 0) {
-        if (staged)
+        if (pipe)
             E.run_pipe("jacobi staged to fp32 +dot", l, k_pipe<M_JACOBI, MLevel<T>, float, false>, L.nl, psm, L,
                        (const T*)tmp, (const T*)rhs, z, wpre(0), 0.f, 0.f, dot, (const float*)M->sigma, 0.f, err);
+        else if (staged)
+            E.run("jacobi staged to fp32 +dot", l, k_msweep_staged<T, float>, g, 128, L, (const T*)tmp,
+                  (const T*)rhs, z, wpre(0), dot, (const float*)M->sigma, err);
         else
             E.run("jacobi to fp32 +dot", l, k_msweep<T, float, MSrcPlain<T>>, g, 128, L, MSrcPlain<T>{tmp},
                   (const T*)rhs, z, wpre(0), dot, (const float*)M->sigma);
@@ -309,7 +318,7 @@ static void menq_precond(MEnq& E) {
     const LevelDev& D0 = h->lv[0];
     const unsigned g = (unsigned)D0.L.nl;
     const DotOut dot{h->r, h->partials, h->st};
-    E.run("r to 16-bit", 0, k_mto16<T>, g, 128, mlevel<T>(h, 0), (const float*)h->r, (T*)M->lv[0].rhs,
+    E.run("r to 16-bit", 0, k_mto16<T>, elem_grid((int)g), 128, mlevel<T>(h, 0), (const float*)h->r, (T*)M->lv[0].rhs,
           (const PcgState*)h->st, M->sigma);
     if (h->nlev == 1) {  // the coarsest solve is the whole preconditioner
         menq_visit<T>(E, 0, true, dot, h->z);
@@ -327,10 +336,13 @@ static void menq_body(MEnq& E, cudaGraphConditionalHandle cond, int use_cond) {
     const unsigned g = (unsigned)D0.L.nl;
     menq_precond<T>(E);
     E.run("pcg update p", 0, k_pcg_update_p, g, 128, D0.L, (const float*)h->z, h->p, h->x, (const PcgState*)h->st);
-    E.run("pcg replace", 0, k_pcg_replace, g, 128, D0.L, (const float*)h->x, (const float*)h->b, h->r,
+    E.run("pcg replace", 0, k_pcg_replace, elem_grid((int)g), 128, D0.L, (const float*)h->x, (const float*)h->b, h->r,
           (const PcgState*)h->st, h->mixed->replace_every);
-    E.run("pcg Ap", 0, k_pcg_Ap, g, 128, D0.L, (const float*)h->p, h->q, h->partials, h->st);
-    E.run("pcg update r", 0, k_pcg_update_r, g, 128, D0.L, (const float*)h->q, h->r, h->partials, h->st, cond,
+    E.pb("pcg Ap", 0);
+    Enq A{h, E.s};
+    enqueue_Ap(A);
+    E.pe();
+    E.run("pcg update r", 0, k_pcg_update_r, elem_grid((int)g), 128, D0.L, (const float*)h->q, h->r, h->partials, h->st, cond,
           use_cond);
 }
 

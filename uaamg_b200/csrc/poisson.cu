@@ -630,6 +630,17 @@ static bool g_use_staged = true;
 // stored values are the ones the fused kernel computes, so the results are
 // identical.
 #define SPLIT_MIN_LEAVES 1024
+// Levels of at least PIPE_MIN_LEAVES leaves sweep with the persistent
+// pipelined kernels (several leaves per CTA); smaller staged levels with the
+// one-leaf staged kernels, which start faster.
+#define PIPE_MIN_LEAVES 8192
+// Grid of the grid-stride elementwise kernels (k_materialize, the PCG
+// vector updates): 16 CTAs of 128 threads per SM of a 148-SM B200, at most
+// one per leaf.  One CTA per leaf would make a large level's elementwise
+// pass cost the GPU's CTA launch rate (about a nanosecond per CTA) instead
+// of its bytes.
+#define ELEM_CTAS 2368
+static unsigned elem_grid(int nl) { return (unsigned)std::min(nl, ELEM_CTAS); }
 template <typename... KArgs, typename... Args>
 static void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
     cudaLaunchConfig_t cfg = {};
@@ -645,29 +656,11 @@ static void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaSt
     CK(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
 }
 
-// Resident CTAs of `kern` (block threads, smem dynamic bytes) on the current
-// GPU: the grid of a persistent kernel.  Cached per kernel and device.
-static int resident_ctas(const void* kern, int block, size_t smem) {
-    static std::mutex mu;
-    static std::vector<std::pair<std::pair<const void*, int>, int>> cache;
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mu);
-    for (auto& e : cache)
-        if (e.first.first == kern && e.first.second == dev) return e.second;
-    int sms = 0, per = 0;
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, block, smem));
-    const int r = std::max(1, per) * std::max(1, sms);
-    cache.push_back({{kern, dev}, r});
-    return r;
-}
-
-// Launch of a pipelined staged kernel (staged_pipe.cuh) over nl leaves: at
-// most one CTA per leaf, at most the CTAs the GPU holds at once.
+// Launch of a pipelined staged kernel (staged_pipe.cuh) over nl leaves:
+// PIPE_CTAS CTAs, at most one per leaf.
 template <typename... KArgs, typename... Args>
 static void launch_pipe(void (*kern)(KArgs...), int nl, size_t smem, cudaStream_t s, Args... args) {
-    const int g = std::min(nl, resident_ctas((const void*)kern, 128, smem));
+    const int g = std::min(nl, PIPE_CTAS);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)g);
     cfg.blockDim = dim3(128);
@@ -750,9 +743,13 @@ struct Enq {
         if constexpr (std::is_same<Src, SrcPlain>::value) {
             if (g_use_staged && D.L.nl >= STAGED_MIN_LEAVES && !(MODE == M_SPAI0 && mark_spai0)) {
                 if (prof) pb("L" + std::to_string(l) + " " + mode_name(MODE) + " staged" + (dot.r ? "+dot" : ""));
-                launch_pipe(k_pipe<MODE, DLevel, float, false>, D.L.nl, pipe_smem_bytes<DLevel>(), s, D.L,
-                            (const float*)src.x, b, out, w, ws, 1.0f - ws, dot, (const float*)nullptr, 0.f,
-                            &h->st->error);
+                if (D.L.nl >= PIPE_MIN_LEAVES)
+                    launch_pipe(k_pipe<MODE, DLevel, float, false>, D.L.nl, pipe_smem_bytes<DLevel>(), s, D.L,
+                                (const float*)src.x, b, out, w, ws, 1.0f - ws, dot, (const float*)nullptr, 0.f,
+                                &h->st->error);
+                else
+                    launch(k_sweep_staged<MODE>, (unsigned)D.L.nl, 128, s, D.L, (const float*)src.x, b, out, w, ws,
+                           1.0f - ws, dot, &h->st->error);
                 pe();
                 count++;
                 return;
@@ -769,7 +766,7 @@ struct Enq {
     void materialize(int l, const Src& src, float* out) {
         LevelDev& D = h->lv[l];
         if (prof) pb("L" + std::to_string(l) + " materialize" + SrcName<Src>::get());
-        launch(k_materialize<Src>, (unsigned)D.L.nl, 128, s, D.L, src, out);
+        launch(k_materialize<Src>, elem_grid(D.L.nl), 128, s, D.L, src, out);
         pe();
         count++;
     }
@@ -777,9 +774,12 @@ struct Enq {
         LevelDev& D = h->lv[l];
         if (g_use_staged && D.L.nl >= STAGED_MIN_LEAVES) {
             if (prof) pb("L" + std::to_string(l) + " residual+restrict staged");
-            launch_pipe(k_pipe<M_RESIDUAL, DLevel, float, true>, D.L.nl, pipe_smem_bytes<DLevel>(), s, D.L, x, b,
-                        h->lv[l + 1].rhs, 0.f, 0.f, 0.f, DotOut{nullptr, nullptr, nullptr}, (const float*)nullptr,
-                        0.f, &h->st->error);
+            if (D.L.nl >= PIPE_MIN_LEAVES)
+                launch_pipe(k_pipe<M_RESIDUAL, DLevel, float, true>, D.L.nl, pipe_smem_bytes<DLevel>(), s, D.L, x,
+                            b, h->lv[l + 1].rhs, 0.f, 0.f, 0.f, DotOut{nullptr, nullptr, nullptr},
+                            (const float*)nullptr, 0.f, &h->st->error);
+            else
+                launch(k_restrict_staged, (unsigned)D.L.nl, 128, s, D.L, x, b, h->lv[l + 1].rhs, &h->st->error);
             pe();
             count++;
             return;
@@ -1013,6 +1013,18 @@ static void enqueue_setup(Enq& E, cudaGraphConditionalHandle cond, int use_cond)
     E.pe();
     E.count += 3;
 }
+// PCG lines 6-7: q = A p with sigma = p.q and alpha (pipelined staged kernel
+// on large levels)
+static void enqueue_Ap(Enq& E) {
+    uaamg_poisson* h = E.h;
+    LevelDev& D0 = h->lv[0];
+    if (g_use_staged && D0.L.nl >= PIPE_MIN_LEAVES)
+        launch_pipe(k_pipe<M_LAPLACIAN, DLevel, float, false, 1>, D0.L.nl, pipe_smem_bytes<DLevel>(), E.s, D0.L,
+                    (const float*)h->p, (const float*)nullptr, h->q, 0.f, 0.f, 0.f,
+                    DotOut{h->p, h->partials, h->st}, (const float*)nullptr, 0.f, &h->st->error);
+    else
+        launch(k_pcg_Ap, (unsigned)D0.L.nl, 128, E.s, D0.L, (const float*)h->p, h->q, h->partials, h->st);
+}
 static void enqueue_body(Enq& E, cudaGraphConditionalHandle cond, int use_cond) {
     uaamg_poisson* h = E.h;
     LevelDev& D0 = h->lv[0];
@@ -1021,10 +1033,10 @@ static void enqueue_body(Enq& E, cudaGraphConditionalHandle cond, int use_cond) 
     launch(k_pcg_update_p, (unsigned)D0.L.nl, 128, E.s, D0.L, (const float*)h->z, h->p, h->x, (const PcgState*)h->st);
     E.pe();
     E.pb("L0 pcg Ap+dot");
-    launch(k_pcg_Ap, (unsigned)D0.L.nl, 128, E.s, D0.L, (const float*)h->p, h->q, h->partials, h->st);
+    enqueue_Ap(E);
     E.pe();
     E.pb("L0 pcg r update+absmax");
-    launch(k_pcg_update_r, (unsigned)D0.L.nl, 128, E.s, D0.L, (const float*)h->q, h->r, h->partials, h->st, cond,
+    launch(k_pcg_update_r, elem_grid(D0.L.nl), 128, E.s, D0.L, (const float*)h->q, h->r, h->partials, h->st, cond,
            use_cond);
     E.pe();
     E.count += 3;

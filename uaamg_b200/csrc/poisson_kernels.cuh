@@ -358,71 +358,6 @@ __device__ __forceinline__ bool red_publish(double part, double* buf, unsigned* 
     total = block_reduce_n<MAX>(acc, rsh);
     return true;
 }
-// Deferred publication for a CTA that has stored the partials of its K slots
-// slot0, slot0 + stride, ... itself (buf + RED_HEADER + slot, thread 0): the
-// group tickets of all of them are taken at once at the end, and the CTA
-// completes every group (and the reduction) it finishes, with the same
-// partials and combination order as red_publish.  Returns true in the CTA
-// that completes the reduction (total valid in thread 0).
-template <bool MAX>
-__device__ __forceinline__ bool red_publish_strided(double* buf, unsigned* ticket, int slot0, int stride, int K,
-                                                    int count, double& total) {
-    __shared__ double rsh[8];
-    __shared__ int rdone[128];
-    __shared__ int rflag;
-    unsigned* gt = reinterpret_cast<unsigned*>(buf);
-    double* slots = buf + RED_HEADER;
-    double* groups = slots + count;
-    const int gs = red_group_size(count);
-    const int ng = (count + gs - 1) / gs;
-    bool fin = false;
-    for (int k0 = 0; k0 < K; k0 += (int)blockDim.x) {
-        const int k = k0 + (int)threadIdx.x;
-        int g = -1;
-        if (k < K) {
-            __threadfence();
-            const int slot = slot0 + k * stride;
-            const int gg = slot / gs;
-            const int gn = min(gs, count - gg * gs);
-            if (atomicAdd(&gt[gg], 1u) == (unsigned)gn - 1) g = gg;
-        }
-        rdone[threadIdx.x] = g;
-        __syncthreads();
-        for (int q = 0; q < (int)blockDim.x; ++q) {
-            const int gg = rdone[q];
-            if (gg < 0) continue;
-            __threadfence();
-            const int g0 = gg * gs;
-            const int gn = min(gs, count - g0);
-            double acc = 0.0;
-            for (int i = threadIdx.x; i < gn; i += blockDim.x) acc = red_combine<MAX>(acc, __ldcg(slots + g0 + i));
-            acc = block_reduce_n<MAX>(acc, rsh);
-            if (ng == 1) {
-                if (threadIdx.x == 0) gt[gg] = 0;
-                total = acc;
-                fin = true;
-                continue;
-            }
-            if (threadIdx.x == 0) {
-                gt[gg] = 0;
-                groups[gg] = acc;
-                __threadfence();
-                rflag = (atomicAdd(ticket, 1u) == (unsigned)ng - 1);
-            }
-            __syncthreads();
-            if (rflag) {
-                __threadfence();
-                double a2 = 0.0;
-                for (int i = threadIdx.x; i < ng; i += blockDim.x) a2 = red_combine<MAX>(a2, __ldcg(groups + i));
-                total = block_reduce_n<MAX>(a2, rsh);
-                fin = true;
-            }
-            __syncthreads();
-        }
-        __syncthreads();
-    }
-    return fin;
-}
 __device__ __forceinline__ bool reduce_sum(double part, double* buf, unsigned* ticket, int slot, int count,
                                            double& total) {
     return red_publish<false>(part, buf, ticket, slot, count, total);
@@ -584,17 +519,21 @@ __global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b
 
 // out = value of a source (materialise a first sweep or a prolongation)
 template <class Src>
+// (grid-stride over the leaves: any grid size; large levels launch a few
+// CTAs per SM rather than one per leaf, which the CTA launch rate would bound)
 __global__ void __launch_bounds__(128) k_materialize(DLevel L, Src src, float* out) {
     griddep_wait();
     griddep_launch();
-    const int leaf = blockIdx.x, t = threadIdx.x;
-    float4 v = src.get4(L, leaf, t);
-    unsigned m = mask4(L.mask, leaf, t);
-    if (!(m & 1)) v.x = 0.f;
-    if (!(m & 2)) v.y = 0.f;
-    if (!(m & 4)) v.z = 0.f;
-    if (!(m & 8)) v.w = 0.f;
-    st4(out, leaf, t, v);
+    const int t = threadIdx.x;
+    for (int leaf = blockIdx.x; leaf < L.nl; leaf += gridDim.x) {
+        float4 v = src.get4(L, leaf, t);
+        unsigned m = mask4(L.mask, leaf, t);
+        if (!(m & 1)) v.x = 0.f;
+        if (!(m & 2)) v.y = 0.f;
+        if (!(m & 4)) v.z = 0.f;
+        if (!(m & 8)) v.w = 0.f;
+        st4(out, leaf, t, v);
+    }
 }
 
 // residual (RESID) or plain values, restricted to the parent level:
@@ -875,10 +814,10 @@ __device__ __forceinline__ void staged_halo_dyn(const float* x, int t, const Hal
     if (H.z >= 0) hz = x[(long long)H.z * UAAMG_LEAF + ((t & 1) ? 4 * t - 4 : 4 * t + 7)];
 }
 
-// resident CTAs per SM the staged kernels are compiled for: they are bound by
-// the latency of their copies, so occupancy sets their throughput
+// minimum resident CTAs per SM the one-leaf staged kernels are compiled for
+// (1: no register cap; higher values spill)
 #ifndef STAGED_MINB
-#define STAGED_MINB 12
+#define STAGED_MINB 1
 #endif
 #define STAGED_SMEM_DECL                                                         \
     __shared__ __align__(128) float sm_x[UAAMG_LEAF], sm_b[UAAMG_LEAF], sm_d[UAAMG_LEAF], \
@@ -1071,10 +1010,10 @@ __device__ __forceinline__ void pcg_update_p_leaf(int leaf, const float* z, floa
     st4(p, leaf, t, pp);
 }
 __global__ void __launch_bounds__(128) k_pcg_update_p(DLevel L, const float* z, float* p, float* x,
-                                                      const PcgState* st) {
+                                                      const PcgState* st) {  // grid-stride over the leaves
     griddep_wait();
     griddep_launch();
-    pcg_update_p_leaf(blockIdx.x, z, p, x, st);
+    for (int leaf = blockIdx.x; leaf < L.nl; leaf += gridDim.x) pcg_update_p_leaf(leaf, z, p, x, st);
 }
 
 // lines 6-7: q = A p; sigma = p.q; alpha = rho / sigma
@@ -1106,48 +1045,68 @@ __global__ void __launch_bounds__(128) k_pcg_Ap(DLevel L, const float* p, float*
 }
 
 // lines 8-12: r -= alpha q; nu = |r|_inf; convergence / divergence test
-__device__ __forceinline__ void pcg_update_r_leaf(int leaf, int count, const float* q, float* r, double* partials,
-                                                  PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
-    __shared__ float shf[4];
+// the thread's 4 voxels of r -= alpha q; returns their |r|_inf
+__device__ __forceinline__ float pcg_update_r_apply(int leaf, const float* q, float* r, float na) {
     const int t = threadIdx.x;
-    const float na = -st->alpha;
     float4 qq = ld4(q, leaf, t), rr = ld4(r, leaf, t);
     rr.x = __fmaf_rn(na, qq.x, rr.x);
     rr.y = __fmaf_rn(na, qq.y, rr.y);
     rr.z = __fmaf_rn(na, qq.z, rr.z);
     rr.w = __fmaf_rn(na, qq.w, rr.w);
     st4(r, leaf, t, rr);
-    float a = nanmax(nanmax(absprop(rr.x), absprop(rr.y)), nanmax(absprop(rr.z), absprop(rr.w)));
+    return nanmax(nanmax(absprop(rr.x), absprop(rr.y)), nanmax(absprop(rr.z), absprop(rr.w)));
+}
+__device__ __forceinline__ void pcg_update_r_finish(float nu, PcgState* st, cudaGraphConditionalHandle cond,
+                                                    int use_cond);
+__device__ __forceinline__ void pcg_update_r_leaf(int leaf, int count, const float* q, float* r, double* partials,
+                                                  PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
+    __shared__ float shf[4];
+    const int t = threadIdx.x;
+    const float a = pcg_update_r_apply(leaf, q, r, -st->alpha);
     float part = block_max128(a, shf);
     float nu;
     if (reduce_max(part, partials, &st->ticket[3], leaf, count, nu)) {
-        if (t == 0) {
-            const int k = st->iter;
-            st->nu_old = st->nu;
-            st->nu = nu;
-            int status = PCG_RUNNING;
-            if (nu <= st->numax) {
-                status = PCG_SUCCESS;
-                st->iterations_taken = k;
-            } else if (nu > st->nu_old && k > 3) {
-                status = PCG_FAILED_DIVERGED;
-                st->iterations_taken = k;
-            } else if (k + 1 >= st->max_iter) {
-                status = PCG_FAILED_MAXITER;
-                st->iterations_taken = st->max_iter;
-            }
-            st->iter = k + 1;
-            st->status = status;
-            st->ticket[3] = 0;
-            set_cond(cond, use_cond, status == PCG_RUNNING ? 1u : 0u);
-        }
+        if (t == 0) pcg_update_r_finish(nu, st, cond, use_cond);
     }
 }
+// nu, the convergence / divergence test and the loop condition (thread 0 of
+// the CTA that completes the |r|_inf reduction)
+__device__ __forceinline__ void pcg_update_r_finish(float nu, PcgState* st, cudaGraphConditionalHandle cond,
+                                                    int use_cond) {
+    const int k = st->iter;
+    st->nu_old = st->nu;
+    st->nu = nu;
+    int status = PCG_RUNNING;
+    if (nu <= st->numax) {
+        status = PCG_SUCCESS;
+        st->iterations_taken = k;
+    } else if (nu > st->nu_old && k > 3) {
+        status = PCG_FAILED_DIVERGED;
+        st->iterations_taken = k;
+    } else if (k + 1 >= st->max_iter) {
+        status = PCG_FAILED_MAXITER;
+        st->iterations_taken = st->max_iter;
+    }
+    st->iter = k + 1;
+    st->status = status;
+    st->ticket[3] = 0;
+    set_cond(cond, use_cond, status == PCG_RUNNING ? 1u : 0u);
+}
+// grid-stride over the leaves, one |r|_inf partial per CTA (a maximum: the
+// result does not depend on the grid)
 __global__ void __launch_bounds__(128) k_pcg_update_r(DLevel L, const float* q, float* r, double* partials,
                                                       PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
     griddep_wait();
     griddep_launch();
-    pcg_update_r_leaf(blockIdx.x, gridDim.x, q, r, partials, st, cond, use_cond);
+    __shared__ float shf[4];
+    const float na = -st->alpha;
+    float a = 0.f;
+    for (int leaf = blockIdx.x; leaf < L.nl; leaf += gridDim.x) a = nanmax(a, pcg_update_r_apply(leaf, q, r, na));
+    const float part = block_max128(a, shf);
+    float nu;
+    if (reduce_max(part, partials, &st->ticket[3], blockIdx.x, gridDim.x, nu)) {
+        if (threadIdx.x == 0) pcg_update_r_finish(nu, st, cond, use_cond);
+    }
 }
 
 // line 10 on success, and line 16 of the last iteration when max_iter is reached

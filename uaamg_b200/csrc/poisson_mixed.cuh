@@ -124,6 +124,7 @@ struct PipeE16 {
     static __device__ __forceinline__ float s1(const unsigned char* a, int i) {
         return H16<T>::bits1(reinterpret_cast<const unsigned short*>(a)[i]);
     }
+    static __device__ __forceinline__ float bits1(unsigned short u) { return H16<T>::bits1(u); }
     static __device__ __forceinline__ float4 g4(const T* p, long long leaf, int t) { return ldh4(p, leaf, t); }
     static __device__ __forceinline__ float g1(const T* p, long long i) { return ldh1(p, i); }
     static __device__ __forceinline__ void st(T* p, long long leaf, int t, float4 v) { sth4(p, leaf, t, v); }
@@ -132,11 +133,12 @@ struct PipeE16 {
 template <> struct PipeE<__half> : PipeE16<__half> {};
 template <> struct PipeE<__nv_bfloat16> : PipeE16<__nv_bfloat16> {};
 template <typename T>
-struct PipeLv<MLevel<T>> {
+struct PipeLv<MLevel<T>> {  // computes in stored units (staged_pipe.cuh)
     using E = T;
     static constexpr bool SCALED = true;
-    static __device__ __forceinline__ float cs(const MLevel<T>& L) { return L.cs; }
-    static __device__ __forceinline__ float ics(const MLevel<T>& L) { return L.ics; }
+    static __device__ __forceinline__ float def_face(const MLevel<T>& L) { return __fmul_rn(L.def_face, L.ics); }
+    static __device__ __forceinline__ float def_diag(const MLevel<T>& L) { return __fmul_rn(L.def_diag, L.ics); }
+    static __device__ __forceinline__ float def_invdiag(const MLevel<T>& L) { return __fmul_rn(L.def_invdiag, L.cs); }
 };
 
 // lhs sources (16-bit vectors)
@@ -399,7 +401,8 @@ __global__ void __launch_bounds__(128) k_mto16(MLevel<T> L, const float* in, T* 
     if (nu > 0.f && isfinite(nu)) sigma = ldexpf(1.0f, ilogbf(nu) - ilogbf(L.def_diag));
     if (blockIdx.x == 0 && threadIdx.x == 0) *sigma_out = sigma;
     const float sc = __fmul_rn(L.ics, 1.0f / sigma);  // exact: powers of two
-    sth4(out, blockIdx.x, threadIdx.x, f4scale(ld4(in, blockIdx.x, threadIdx.x), sc));
+    for (int leaf = blockIdx.x; leaf < L.nl; leaf += gridDim.x)  // grid-stride
+        sth4(out, leaf, threadIdx.x, f4scale(ld4(in, leaf, threadIdx.x), sc));
 }
 
 // 16-bit -> FP32 copy of a level vector (one-level hierarchies: z)
@@ -527,8 +530,8 @@ __device__ __forceinline__ void mhalo_dyn(const T* x, int t, MHalo& H) {
     if (H.z >= 0) H.zv = ldh1(x, (long long)H.z * UAAMG_LEAF + ((t & 1) ? 4 * t - 4 : 4 * t + 7));
 }
 
-#ifndef MSTAGED_MINB
-#define MSTAGED_MINB 12
+#ifndef MSTAGED_MINB  // minimum resident CTAs per SM (1: no register cap; higher values spill)
+#define MSTAGED_MINB 1
 #endif
 #define MSTAGED_SMEM_DECL                                                                                    \
     __shared__ __align__(128) uint16_t msm_x[UAAMG_LEAF], msm_b[UAAMG_LEAF], msm_d[UAAMG_LEAF],             \
@@ -705,17 +708,19 @@ __global__ void __launch_bounds__(128, MSTAGED_MINB) k_mrestrict_staged(MLevel<T
 // A computed source stored as a 16-bit vector (zero off the DOF): the first
 // sweep's w * (1/diag * b), or the prolongation-add x + P x_c (in place)
 template <typename T, class Src>
-__global__ void __launch_bounds__(128) k_mmaterialize(MLevel<T> L, Src src, T* out) {
+__global__ void __launch_bounds__(128) k_mmaterialize(MLevel<T> L, Src src, T* out) {  // grid-stride
     griddep_wait();
     griddep_launch();
-    const int leaf = blockIdx.x, t = threadIdx.x;
-    float4 v = src.get4(L, leaf, t);
-    const unsigned m = mask4(L.mask, leaf, t);
-    if (!(m & 1)) v.x = 0.f;
-    if (!(m & 2)) v.y = 0.f;
-    if (!(m & 4)) v.z = 0.f;
-    if (!(m & 8)) v.w = 0.f;
-    sth4(out, leaf, t, v);
+    const int t = threadIdx.x;
+    for (int leaf = blockIdx.x; leaf < L.nl; leaf += gridDim.x) {
+        float4 v = src.get4(L, leaf, t);
+        const unsigned m = mask4(L.mask, leaf, t);
+        if (!(m & 1)) v.x = 0.f;
+        if (!(m & 2)) v.y = 0.f;
+        if (!(m & 4)) v.z = 0.f;
+        if (!(m & 8)) v.w = 0.f;
+        sth4(out, leaf, t, v);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -782,10 +787,12 @@ __global__ void __launch_bounds__(128) k_pcg_replace(DLevel L, const float* x, c
     griddep_launch();
     const int it = st->iter;
     if (st->first || it == 0 || (it % every) != 0) return;
-    const int leaf = blockIdx.x, t = threadIdx.x;
-    float4 xc;
-    unsigned m;
-    st4(r, leaf, t, sweep_value<M_RESIDUAL>(L, leaf, t, SrcPlain{x}, b, 0.f, 0.f, 0.f, xc, m));
+    const int t = threadIdx.x;
+    for (int leaf = blockIdx.x; leaf < L.nl; leaf += gridDim.x) {  // grid-stride
+        float4 xc;
+        unsigned m;
+        st4(r, leaf, t, sweep_value<M_RESIDUAL>(L, leaf, t, SrcPlain{x}, b, 0.f, 0.f, 0.f, xc, m));
+    }
 }
 
 // |b - A x|_inf and |b|_inf over the DOF in FP64 (A x from the FP32

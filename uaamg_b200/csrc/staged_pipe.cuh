@@ -12,8 +12,8 @@
 // dependent launch).  Each thread computes 4 z-consecutive voxels with the
 // operation sequence of stencil4 / staged_value (simd_vdb_poisson.cpp
 // LightWeightApplier, :1190-1470), so the results equal those of the one-leaf
-// kernels; a dot product keeps one partial per leaf (reduce_sum over the
-// level's leaves), so reductions match too.
+// kernels.  A fused dot product sums each CTA's leaves in leaf order and
+// reduces the PIPE_CTAS partials with reduce_sum: one ticket per CTA.
 #pragma once
 #include "poisson_kernels.cuh"
 
@@ -35,37 +35,22 @@ template <> struct PipeE<float> {
     static __device__ __forceinline__ void st1(float* p, long long i, float v) { p[i] = v; }
 };
 
-// level traits: the FP32 level reads unscaled values; the 16-bit level
-// (poisson_mixed.cuh) scales coefficients and rhs by cs and 1/diag by ics
+// level traits.  A 16-bit level (poisson_mixed.cuh) stores its coefficients
+// and rhs divided by a power of two cs and 1/diag multiplied by it; since
+// scaling by a power of two is exact, the pipelined kernels compute in the
+// stored units -- off-diagonal sum, diagonal term and residual all come out
+// divided by cs, and the product with the stored 1/diag is the true value --
+// with the defaults of trimmed leaves brought to the same units (def_face /
+// cs, def_diag / cs, def_invdiag * cs).  Each result equals the one computed
+// from rescaled values.
 template <class LV> struct PipeLv;
 template <> struct PipeLv<DLevel> {
     using E = float;
     static constexpr bool SCALED = false;
-    static __device__ __forceinline__ float cs(const DLevel&) { return 1.0f; }
-    static __device__ __forceinline__ float ics(const DLevel&) { return 1.0f; }
+    static __device__ __forceinline__ float def_face(const DLevel& L) { return L.def_face; }
+    static __device__ __forceinline__ float def_diag(const DLevel& L) { return L.def_diag; }
+    static __device__ __forceinline__ float def_invdiag(const DLevel& L) { return L.def_invdiag; }
 };
-
-template <class LV>
-__device__ __forceinline__ float4 pscale4(const LV& L, float4 v) {
-    if constexpr (PipeLv<LV>::SCALED)
-        return make_float4(__fmul_rn(v.x, PipeLv<LV>::cs(L)), __fmul_rn(v.y, PipeLv<LV>::cs(L)),
-                           __fmul_rn(v.z, PipeLv<LV>::cs(L)), __fmul_rn(v.w, PipeLv<LV>::cs(L)));
-    else
-        return v;
-}
-template <class LV>
-__device__ __forceinline__ float pscale1(const LV& L, float v) {
-    if constexpr (PipeLv<LV>::SCALED) return __fmul_rn(v, PipeLv<LV>::cs(L));
-    else return v;
-}
-template <class LV>
-__device__ __forceinline__ float4 piscale4(const LV& L, float4 v) {
-    if constexpr (PipeLv<LV>::SCALED)
-        return make_float4(__fmul_rn(v.x, PipeLv<LV>::ics(L)), __fmul_rn(v.y, PipeLv<LV>::ics(L)),
-                           __fmul_rn(v.z, PipeLv<LV>::ics(L)), __fmul_rn(v.w, PipeLv<LV>::ics(L)));
-    else
-        return v;
-}
 
 // offsets of the arrays inside a stage
 enum { PS_X = 0, PS_B = 1, PS_D = 2, PS_I = 3, PS_CX = 4, PS_CY = 5, PS_CZ = 6, PS_N = 7 };
@@ -118,100 +103,218 @@ __device__ __forceinline__ void pissue_dyn(const LV& L, int leaf, const PSet<MOD
     }
 }
 
-// a thread's halo: the neighbour leaves whose faces it reads and their face
-// coefficients (static), and the neighbours' x values
-struct PHalo {
-    int xp, xm, yp, ym, z;
-    float4 cxp, cyp;
-    float cz;
+// ---------------------------------------------------------------------------
+// Stage layout (bytes): the PS_N leaf arrays, then the halo a leaf's stencil
+// reads from its neighbours -- face chunks of 4 values (x of the +-x and +-y
+// neighbours, c_x of the +x and c_y of the +y neighbour), the z-face values
+// (x of the -z / +z neighbour per thread, c_z of the +z neighbour), the
+// leaf's DOF mask and, for 16-bit levels, the flags of the +x, +y and +z
+// neighbours (a trimmed neighbour reads the default).  Halo values are
+// copied by the threads that use them (cp.async, 4-16 bytes), a 16-bit z
+// value as the aligned pair that holds it.
+template <typename E>
+struct PLayout {
+    static constexpr unsigned A = PipeE<E>::ARR;
+    static constexpr unsigned C = 4u * (unsigned)sizeof(E);
+    static constexpr unsigned HXP = PS_N * A;
+    static constexpr unsigned HXM = HXP + 16 * C;
+    static constexpr unsigned HYP = HXM + 16 * C;
+    static constexpr unsigned HYM = HYP + 16 * C;
+    static constexpr unsigned HCXP = HYM + 16 * C;
+    static constexpr unsigned HCYP = HCXP + 16 * C;
+    static constexpr unsigned HZ = HCYP + 16 * C;  // 128 x 4 B
+    static constexpr unsigned HCZ = HZ + 512;      // 64 x 4 B
+    static constexpr unsigned MASK = HCZ + 256;    // 8 x 8 B
+    static constexpr unsigned FLG = MASK + 64;     // 3 x 4 B
+    static constexpr unsigned STAGE = (FLG + 16 + 127) / 128 * 128;
 };
-struct PHaloX {
-    float4 xp, xm, yp, ym;
-    float z;
-};
-template <class LV>
-__device__ __forceinline__ void phalo_static(const LV& L, int leaf, int t, PHalo& H) {
-    using E = typename PipeLv<LV>::E;
-    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
-    const int* nb = L.nbr + (long long)leaf * 6;
-    const float df = L.def_face;
-    H.xp = (X == 7) ? nb[1] : -1;
-    H.xm = (X == 0) ? nb[0] : -1;
-    H.yp = (Y == 7) ? nb[3] : -1;
-    H.ym = (Y == 0) ? nb[2] : -1;
-    H.z = (zh == 0) ? nb[4] : nb[5];
-    H.cxp = H.cyp = f4splat(df);
-    H.cz = df;
-    if constexpr (PipeLv<LV>::SCALED) {
-        // the stored 16-bit value of a trimmed leaf is the rounded default:
-        // a trimmed neighbour reads the FP32 default (flags and values load together)
-        if (H.xp >= 0) {
-            const unsigned f = L.flags[H.xp];
-            const float4 v = pscale4(L, PipeE<E>::g4(L.cx, H.xp, t - 112));
-            if (!(f & TRIM_X)) H.cxp = v;
-        }
-        if (H.yp >= 0) {
-            const unsigned f = L.flags[H.yp];
-            const float4 v = pscale4(L, PipeE<E>::g4(L.cy, H.yp, t - 14));
-            if (!(f & TRIM_Y)) H.cyp = v;
-        }
-        if (zh == 1 && H.z >= 0) {
-            const unsigned f = L.flags[H.z];
-            const float v = pscale1(L, PipeE<E>::g1(L.cz, (long long)H.z * UAAMG_LEAF + 4 * t - 4));
-            if (!(f & TRIM_Z)) H.cz = v;
-        }
-    } else {
-        // a trimmed FP32 leaf stores its default coefficients (finalize_leaf)
-        if (H.xp >= 0) H.cxp = ld4(L.cx, H.xp, t - 112);
-        if (H.yp >= 0) H.cyp = ld4(L.cy, H.yp, t - 14);
-        if (zh == 1 && H.z >= 0) H.cz = L.cz[(long long)H.z * UAAMG_LEAF + 4 * t - 4];
-    }
+
+__device__ __forceinline__ void cpa16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+// the barrier's next phase also waits for this thread's cp.async copies so far
+__device__ __forceinline__ void cpa_arrive(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+template <typename E>
+__device__ __forceinline__ void cpa_chunk(unsigned char* dst, const E* src) {
+    if constexpr (sizeof(E) == 4) cpa16(dst, src);
+    else cpa8(dst, src);
 }
 template <typename E>
-__device__ __forceinline__ void phalo_dyn(const E* x, int t, const PHalo& H, PHaloX& V) {
-    V.xp = (H.xp >= 0) ? PipeE<E>::g4(x, H.xp, t - 112) : f4zero();
-    V.xm = (H.xm >= 0) ? PipeE<E>::g4(x, H.xm, t + 112) : f4zero();
-    V.yp = (H.yp >= 0) ? PipeE<E>::g4(x, H.yp, t - 14) : f4zero();
-    V.ym = (H.ym >= 0) ? PipeE<E>::g4(x, H.ym, t + 14) : f4zero();
-    V.z = 0.f;
-    if (H.z >= 0) V.z = PipeE<E>::g1(x, (long long)H.z * UAAMG_LEAF + ((t & 1) ? 4 * t - 4 : 4 * t + 7));
+__device__ __forceinline__ void zero_chunk(unsigned char* dst) {
+    if constexpr (sizeof(E) == 4) *reinterpret_cast<float4*>(dst) = f4zero();
+    else *reinterpret_cast<uint2*>(dst) = make_uint2(0u, 0u);
 }
 
-// the value of the thread's 4 voxels in MODE from a staged leaf (the
-// operation sequence of staged_value)
+// neighbour row of a leaf: -x +x -y +y -z +z
+struct PNb {
+    int v[6];
+};
+__device__ __forceinline__ PNb pnb_load(const int* nbr, int leaf) {
+    const int2* p = reinterpret_cast<const int2*>(nbr + (long long)leaf * 6);
+    const int2 a = p[0], b = p[1], c = p[2];
+    PNb r;
+    r.v[0] = a.x;
+    r.v[1] = a.y;
+    r.v[2] = b.x;
+    r.v[3] = b.y;
+    r.v[4] = c.x;
+    r.v[5] = c.y;
+    return r;
+}
+
+// Issue a thread's share of a leaf's halo: STAT the coefficient faces, the
+// mask and the flags (no change during a solve), DYN the x faces.
+template <bool STAT, bool DYN, class LV>
+__device__ __forceinline__ void phalo_issue(const LV& L, int leaf, const PNb& N, int t, unsigned char* st,
+                                            const typename PipeLv<LV>::E* x) {
+    using E = typename PipeLv<LV>::E;
+    using Lo = PLayout<E>;
+    constexpr unsigned C = Lo::C;
+    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
+    const int ys = 2 * X + zh;  // slot of a +-y face thread
+    if constexpr (STAT) {
+        // a missing FP32 neighbour reads the default face coefficient; a
+        // missing 16-bit one is flagged trimmed below
+        if (X == 7) {
+            const int n = N.v[1];
+            unsigned char* d = st + Lo::HCXP + (t - 112) * C;
+            if (n >= 0) cpa_chunk(d, L.cx + (long long)n * UAAMG_LEAF + 4 * (t - 112));
+            else if constexpr (!PipeLv<LV>::SCALED) *reinterpret_cast<float4*>(d) = f4splat(L.def_face);
+        }
+        if (Y == 7) {
+            const int n = N.v[3];
+            unsigned char* d = st + Lo::HCYP + ys * C;
+            if (n >= 0) cpa_chunk(d, L.cy + (long long)n * UAAMG_LEAF + 4 * (t - 14));
+            else if constexpr (!PipeLv<LV>::SCALED) *reinterpret_cast<float4*>(d) = f4splat(L.def_face);
+        }
+        if (zh == 1) {
+            const int n = N.v[5];
+            unsigned char* d = st + Lo::HCZ + 4 * (t >> 1);
+            if (n >= 0) cpa4(d, L.cz + (long long)n * UAAMG_LEAF + 4 * t - 4);
+            else if constexpr (!PipeLv<LV>::SCALED) *reinterpret_cast<float*>(d) = L.def_face;
+        }
+        if (t < 4)
+            cpa16(st + Lo::MASK + 16 * t, reinterpret_cast<const unsigned char*>(L.mask + (long long)leaf * 8) + 16 * t);
+        if constexpr (PipeLv<LV>::SCALED) {
+            if (t >= 4 && t < 7) {
+                const int n = (t == 4) ? N.v[1] : ((t == 5) ? N.v[3] : N.v[5]);  // +x, +y, +z
+                unsigned char* d = st + Lo::FLG + 4 * (t - 4);
+                if (n >= 0) cpa4(d, L.flags + n);
+                else *reinterpret_cast<unsigned*>(d) = 0xFFFFFFFFu;  // missing: the default
+            }
+        }
+    }
+    if constexpr (DYN) {
+        if (X == 7) {
+            const int n = N.v[1];
+            unsigned char* d = st + Lo::HXP + (t - 112) * C;
+            if (n >= 0) cpa_chunk(d, x + (long long)n * UAAMG_LEAF + 4 * (t - 112));
+            else zero_chunk<E>(d);
+        }
+        if (X == 0) {
+            const int n = N.v[0];
+            unsigned char* d = st + Lo::HXM + t * C;
+            if (n >= 0) cpa_chunk(d, x + (long long)n * UAAMG_LEAF + 4 * (t + 112));
+            else zero_chunk<E>(d);
+        }
+        if (Y == 7) {
+            const int n = N.v[3];
+            unsigned char* d = st + Lo::HYP + ys * C;
+            if (n >= 0) cpa_chunk(d, x + (long long)n * UAAMG_LEAF + 4 * (t - 14));
+            else zero_chunk<E>(d);
+        }
+        if (Y == 0) {
+            const int n = N.v[2];
+            unsigned char* d = st + Lo::HYM + ys * C;
+            if (n >= 0) cpa_chunk(d, x + (long long)n * UAAMG_LEAF + 4 * (t + 14));
+            else zero_chunk<E>(d);
+        }
+        const int n = zh ? N.v[5] : N.v[4];
+        unsigned char* d = st + Lo::HZ + 4 * t;
+        if (n >= 0) {
+            // FP32: the value; 16-bit: the aligned pair holding it
+            const long long e =
+                (long long)n * UAAMG_LEAF + (zh ? 4 * t - 4 : (sizeof(E) == 4 ? 4 * t + 7 : 4 * t + 6));
+            cpa4(d, x + e);
+        } else {
+            *reinterpret_cast<unsigned*>(d) = 0u;
+        }
+    }
+}
+
+// a z-face value read back from the stage (16-bit: high or low half of the pair)
+template <typename E>
+__device__ __forceinline__ float phz(const unsigned char* p, bool high) {
+    if constexpr (sizeof(E) == 4) {
+        return *reinterpret_cast<const float*>(p);
+    } else {
+        const unsigned u = *reinterpret_cast<const unsigned*>(p);
+        return PipeE<E>::bits1((unsigned short)(high ? (u >> 16) : (u & 0xFFFFu)));
+    }
+}
+
+// the value of the thread's 4 voxels in MODE from a staged leaf and its halo
+// (the operation sequence of staged_value)
 template <int MODE, class LV>
-__device__ __forceinline__ float4 pvalue(const LV& L, int t, unsigned fl, unsigned m, const unsigned char* st,
-                                         const PHalo& H, const PHaloX& V, float w, float wsor, float one_minus_wsor,
-                                         float4& xc) {
+__device__ __forceinline__ float4 pvalue(const LV& L, int t, unsigned fl, const unsigned char* st, float w,
+                                         float wsor, float one_minus_wsor) {
     using E = typename PipeLv<LV>::E;
     using P = PipeE<E>;
+    using Lo = PLayout<E>;
     constexpr unsigned A = P::ARR;
     const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
-    const float df = L.def_face;
+    const int ys = 2 * X + zh;
+    const float df = PipeLv<LV>::def_face(L);
     const float4 dfv = f4splat(df);
     const unsigned char* sx = st + PS_X * A;
     const unsigned char* scx = st + PS_CX * A;
     const unsigned char* scy = st + PS_CY * A;
     const unsigned char* scz = st + PS_CZ * A;
-    xc = P::s4(sx, t);
-    const float4 xp = (X < 7) ? P::s4(sx, t + 16) : V.xp;
-    const float4 xm = (X > 0) ? P::s4(sx, t - 16) : V.xm;
-    const float4 yp = (Y < 7) ? P::s4(sx, t + 2) : V.yp;
-    const float4 ym = (Y > 0) ? P::s4(sx, t - 2) : V.ym;
-    const float4 cxp = (X < 7) ? ((fl & TRIM_X) ? dfv : pscale4(L, P::s4(scx, t + 16))) : H.cxp;
-    const float4 cyp = (Y < 7) ? ((fl & TRIM_Y) ? dfv : pscale4(L, P::s4(scy, t + 2))) : H.cyp;
-    const float4 cxm = (fl & TRIM_X) ? dfv : pscale4(L, P::s4(scx, t));
-    const float4 cym = (fl & TRIM_Y) ? dfv : pscale4(L, P::s4(scy, t));
-    const float4 czo = (fl & TRIM_Z) ? dfv : pscale4(L, P::s4(scz, t));
+    const float4 xc = P::s4(sx, t);
+    const float4 xp = (X < 7) ? P::s4(sx, t + 16) : P::s4(st + Lo::HXP, t - 112);
+    const float4 xm = (X > 0) ? P::s4(sx, t - 16) : P::s4(st + Lo::HXM, t);
+    const float4 yp = (Y < 7) ? P::s4(sx, t + 2) : P::s4(st + Lo::HYP, ys);
+    const float4 ym = (Y > 0) ? P::s4(sx, t - 2) : P::s4(st + Lo::HYM, ys);
+    const unsigned* nf = reinterpret_cast<const unsigned*>(st + Lo::FLG);
+    float4 cxp, cyp;
+    if (X < 7) {
+        cxp = (fl & TRIM_X) ? dfv : P::s4(scx, t + 16);
+    } else if constexpr (PipeLv<LV>::SCALED) {
+        cxp = (nf[0] & TRIM_X) ? dfv : P::s4(st + Lo::HCXP, t - 112);
+    } else {
+        cxp = P::s4(st + Lo::HCXP, t - 112);
+    }
+    if (Y < 7) {
+        cyp = (fl & TRIM_Y) ? dfv : P::s4(scy, t + 2);
+    } else if constexpr (PipeLv<LV>::SCALED) {
+        cyp = (nf[1] & TRIM_Y) ? dfv : P::s4(st + Lo::HCYP, ys);
+    } else {
+        cyp = P::s4(st + Lo::HCYP, ys);
+    }
+    const float4 cxm = (fl & TRIM_X) ? dfv : P::s4(scx, t);
+    const float4 cym = (fl & TRIM_Y) ? dfv : P::s4(scy, t);
+    const float4 czo = (fl & TRIM_Z) ? dfv : P::s4(scz, t);
     float zp3, zm0, czp3;
     if (zh == 0) {
         zp3 = P::s1(sx, 4 * t + 4);
-        czp3 = (fl & TRIM_Z) ? df : pscale1(L, P::s1(scz, 4 * t + 4));
-        zm0 = V.z;
+        czp3 = (fl & TRIM_Z) ? df : P::s1(scz, 4 * t + 4);
+        zm0 = phz<E>(st + Lo::HZ + 4 * t, true);
     } else {
         zm0 = P::s1(sx, 4 * t - 1);
-        zp3 = V.z;
-        czp3 = H.cz;
+        zp3 = phz<E>(st + Lo::HZ + 4 * t, false);
+        if constexpr (PipeLv<LV>::SCALED)
+            czp3 = (nf[2] & TRIM_Z) ? df : phz<E>(st + Lo::HCZ + 4 * (t >> 1), false);
+        else
+            czp3 = phz<E>(st + Lo::HCZ + 4 * (t >> 1), false);
     }
     const float zp[4] = {xc.y, xc.z, xc.w, zp3};
     const float zm[4] = {zm0, xc.x, xc.y, xc.z};
@@ -232,10 +335,12 @@ __device__ __forceinline__ float4 pvalue(const LV& L, int t, unsigned fl, unsign
         f1 = __fadd_rn(f1, f5);
         f4set(off, j, f1);
     }
+    const uint64_t mw = reinterpret_cast<const uint64_t*>(st + Lo::MASK)[t >> 4];
+    const unsigned m = (unsigned)((mw >> ((t & 15) * 4)) & 0xFull);
     float4 res = f4zero();
     if constexpr (MODE == M_RED || MODE == M_BLACK) {
-        const float4 bb = pscale4(L, P::s4(st + PS_B * A, t));
-        const float4 iv = (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : piscale4(L, P::s4(st + PS_I * A, t));
+        const float4 bb = P::s4(st + PS_B * A, t);
+        const float4 iv = (fl & TRIM_DIAG) ? f4splat(PipeLv<LV>::def_invdiag(L)) : P::s4(st + PS_I * A, t);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int par = (X + Y + j) & 1;
@@ -247,19 +352,19 @@ __device__ __forceinline__ float4 pvalue(const LV& L, int t, unsigned fl, unsign
             f4set(res, j, upd ? v : f4get(xc, j));
         }
     } else {
-        const float4 dg = (fl & TRIM_DIAG) ? f4splat(L.def_diag) : pscale4(L, P::s4(st + PS_D * A, t));
+        const float4 dg = (fl & TRIM_DIAG) ? f4splat(PipeLv<LV>::def_diag(L)) : P::s4(st + PS_D * A, t);
         if constexpr (MODE == M_LAPLACIAN) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) f4set(res, j, __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
         } else {
-            const float4 bb = pscale4(L, P::s4(st + PS_B * A, t));
+            const float4 bb = P::s4(st + PS_B * A, t);
             if constexpr (MODE == M_RESIDUAL) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                     f4set(res, j, __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j))));
             } else if constexpr (MODE == M_JACOBI) {
                 const float4 iv =
-                    (fl & TRIM_DIAG) ? f4splat(L.def_invdiag) : piscale4(L, P::s4(st + PS_I * A, t));
+                    (fl & TRIM_DIAG) ? f4splat(PipeLv<LV>::def_invdiag(L)) : P::s4(st + PS_I * A, t);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(xc, j), f4get(dg, j), f4get(off, j)));
@@ -284,24 +389,37 @@ __device__ __forceinline__ float4 pvalue(const LV& L, int t, unsigned fl, unsign
 }
 
 #ifndef PIPE_MINB
-#define PIPE_MINB 8
+#define PIPE_MINB 6
 #endif
-// dynamic shared memory of a pipelined kernel: two stages of PS_N arrays
+// CTAs of a pipelined launch (at most one per leaf): 6 per SM on a 148-SM
+// B200.  A constant rather than the occupancy of the GPU at hand, so the
+// order of a fused dot product's sum depends only on the level.
+#define PIPE_CTAS 888
+// dynamic shared memory of a pipelined kernel: two stages
 template <class LV>
 constexpr size_t pipe_smem_bytes() {
-    return 2u * PS_N * PipeE<typename PipeLv<LV>::E>::ARR;
+    return 2u * PLayout<typename PipeLv<LV>::E>::STAGE;
 }
 
 // One sweep (RESTRICT false: out[leaf] = value, optionally scaled by *zscale
 // and with the fused z.r of PCG lines 13-15) or one residual + restriction
 // (RESTRICT true, MODE M_RESIDUAL: coarse = 0.125 * sum of the active fine
-// residuals of each 2x2x2 block, times coarse_scale) over a level.
-template <int MODE, class LV, typename TOut, bool RESTRICT>
+// residuals of each 2x2x2 block, times coarse_scale on 16-bit levels) over a
+// level.  Everything a leaf reads -- its arrays by bulk copies (thread 0),
+// its halo, mask and neighbour flags by cp.async (each thread its share) --
+// is in flight into one stage while the CTA computes the leaf in the other;
+// every thread's cp.async arrival and thread 0's byte count complete a
+// stage's barrier phase.
+//
+// DOTK selects the fused dot of a sweep: 0 z.r with the b of a level-0 sweep
+// or dot.r (PCG lines 13-15: rho, beta), 1 p.q with p the swept vector (the
+// Laplacian of PCG lines 6-7: sigma, alpha).
+template <int MODE, class LV, typename TOut, bool RESTRICT, int DOTK = 0>
 __global__ void __launch_bounds__(128, PIPE_MINB)
     k_pipe(LV L, const typename PipeLv<LV>::E* x, const typename PipeLv<LV>::E* b, TOut* out, float w, float wsor,
            float one_minus_wsor, DotOut dot, const float* zscale, float coarse_scale, int* err) {
     using E = typename PipeLv<LV>::E;
-    constexpr unsigned A = PipeE<E>::ARR;
+    using Lo = PLayout<E>;
     extern __shared__ __align__(128) unsigned char psm[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ __align__(16) float rs[RESTRICT ? UAAMG_LEAF : 4];
@@ -310,56 +428,72 @@ __global__ void __launch_bounds__(128, PIPE_MINB)
     const int G = (int)gridDim.x;
     const int nl = L.nl;
     int leaf = (int)blockIdx.x;
-    unsigned char* stg0 = psm;
-    unsigned char* stg1 = psm + PS_N * A;
     if (t == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        mbar_init(&bar[0], 1 + 128);  // thread 0's byte count + every thread's cp.async arrival
+        mbar_init(&bar[1], 1 + 128);
     }
     __syncthreads();
-    // first leaf: static data before the wait
+    // first leaf: static data before the wait for the previous kernel
     unsigned fl = L.flags[leaf];
-    PHalo H;
-    phalo_static(L, leaf, t, H);
-    if (t == 0) pissue_static<MODE>(L, leaf, PSet<MODE>(fl), stg0, &bar[0]);
+    PNb N = pnb_load(L.nbr, leaf);
+    if (t == 0) pissue_static<MODE>(L, leaf, PSet<MODE>(fl), psm, &bar[0]);
+    phalo_issue<true, false>(L, leaf, N, t, psm, x);
     griddep_wait();
     griddep_launch();
-    if (t == 0) pissue_dyn<MODE>(L, leaf, PSet<MODE>(fl), x, b, stg0, &bar[0]);
+    if (t == 0) pissue_dyn<MODE>(L, leaf, PSet<MODE>(fl), x, b, psm, &bar[0]);
+    phalo_issue<false, true>(L, leaf, N, t, psm, x);
+    cpa_arrive(&bar[0]);
+    // the next leaf's row and flags
+    unsigned fln = 0;
+    if (leaf + G < nl) {
+        fln = L.flags[leaf + G];
+        N = pnb_load(L.nbr, leaf + G);
+    }
     int j = 0;
     bool ok = true, next_issued = false;
+    double cta_dot = 0.0;  // thread 0: this CTA's leaves' z.r partials, in leaf order
     for (; leaf < nl; ++j, leaf += G) {
-        unsigned char* cur = (j & 1) ? stg1 : stg0;
-        unsigned char* nst = (j & 1) ? stg0 : stg1;
+        unsigned char* cur = psm + (j & 1) * Lo::STAGE;
+        unsigned char* nst = psm + ((j & 1) ^ 1) * Lo::STAGE;
         uint64_t* cbar = &bar[j & 1];
         uint64_t* nbar = &bar[(j & 1) ^ 1];
         const int nxt = leaf + G;
-        unsigned fln = 0;
-        next_issued = false;
-        if (nxt < nl) {
-            fln = L.flags[nxt];
-            next_issued = true;
+        next_issued = nxt < nl;
+        if (next_issued) {
             if (t == 0) {
                 const PSet<MODE> Qn(fln);
                 pissue_static<MODE>(L, nxt, Qn, nst, nbar);
                 pissue_dyn<MODE>(L, nxt, Qn, x, b, nst, nbar);
             }
+            phalo_issue<true, true>(L, nxt, N, t, nst, x);
+            cpa_arrive(nbar);
         }
-        PHaloX V;
-        phalo_dyn(x, t, H, V);
-        const unsigned m = mask4(L.mask, leaf, t);
-        // the next leaf's neighbour data load while this leaf computes
-        PHalo Hc = H;
-        if (nxt < nl) phalo_static(L, nxt, t, H);
+        const unsigned flc = fl;
+        fl = fln;
+        if (nxt + G < nl) {  // row and flags two leaves ahead, in flight during this leaf
+            fln = L.flags[nxt + G];
+            N = pnb_load(L.nbr, nxt + G);
+        }
+        float4 rr = f4zero();
+        if constexpr (!RESTRICT && PipeLv<LV>::SCALED && DOTK == 0) {
+            if (dot.r) rr = ld4(dot.r, leaf, t);
+        }
+        int par = 0, oct = 0;
+        if constexpr (RESTRICT) {
+            if (t < 64) {
+                par = L.parent[leaf];
+                oct = L.octant[leaf];
+            }
+        }
         ok = __syncthreads_and(mbar_wait_bounded(cbar, (unsigned)((j >> 1) & 1)) ? 1 : 0) != 0;
         if (!ok) break;
-        float4 xc;
-        float4 res = pvalue<MODE>(L, t, fl, m, cur, Hc, V, w, wsor, one_minus_wsor, xc);
+        float4 res = pvalue<MODE>(L, t, flc, cur, w, wsor, one_minus_wsor);
         if constexpr (RESTRICT) {
             reinterpret_cast<float4*>(rs)[t] = res;
             __syncthreads();
             if (t < 64) {
                 const int i = t >> 4, jj0 = (t >> 2) & 3, k = t & 3;
-                const uint64_t* mk = L.mask + (long long)leaf * 8;
+                const uint64_t* mk = reinterpret_cast<const uint64_t*>(cur + Lo::MASK);
                 float s = 0.f;
 #pragma unroll
                 for (int ii = 0; ii < 2; ++ii)
@@ -370,10 +504,9 @@ __global__ void __launch_bounds__(128, PIPE_MINB)
                             const int fo = ((2 * i + ii) << 6) | ((2 * jj0 + jj) << 3) | (2 * k + kk);
                             if ((mk[fo >> 6] >> (fo & 63)) & 1ull) s = __fadd_rn(s, rs[fo]);
                         }
-                const int o = L.octant[leaf];
                 const int coff =
-                    ((((o >> 2) & 1) * 4 + i) << 6) | ((((o >> 1) & 1) * 4 + jj0) << 3) | ((o & 1) * 4 + k);
-                const long long ci = (long long)L.parent[leaf] * UAAMG_LEAF + coff;
+                    ((((oct >> 2) & 1) * 4 + i) << 6) | ((((oct >> 1) & 1) * 4 + jj0) << 3) | ((oct & 1) * 4 + k);
+                const long long ci = (long long)par * UAAMG_LEAF + coff;
                 if constexpr (PipeLv<LV>::SCALED)
                     PipeE<TOut>::st1(out, ci, __fmul_rn(__fmul_rn(s, 0.125f), coarse_scale));
                 else
@@ -388,21 +521,20 @@ __global__ void __launch_bounds__(128, PIPE_MINB)
                 }
             }
             PipeE<TOut>::st(out, leaf, t, res);
-            if (dot.r) {  // rho_new = z . r, then beta and rho (PCG lines 13-15)
-                float4 rr;
-                if constexpr (PipeLv<LV>::SCALED) rr = ld4(dot.r, leaf, t);
-                else rr = PipeE<E>::s4(cur + PS_B * A, t);  // the b of a level-0 sweep is r
+            if (dot.r) {  // this leaf's z.r (p.q) partial into the CTA's sum
+                if constexpr (DOTK == 1) rr = PipeE<E>::s4(cur + PS_X * PipeE<E>::ARR, t);  // p
+                else if constexpr (!PipeLv<LV>::SCALED) rr = PipeE<E>::s4(cur + PS_B * PipeE<E>::ARR, t);  // b is r
                 const double s = (double)res.x * rr.x + (double)res.y * rr.y + (double)res.z * rr.z +
                                  (double)res.w * rr.w;
                 const double part = block_sum128(s, shd);
-                if (t == 0) dot.partials[RED_HEADER + leaf] = part;  // published after the loop
+                if (t == 0) cta_dot += part;
             }
         }
-        fl = fln;
         __syncthreads();  // the stage just read is free for the copies issued next iteration
     }
     if (!ok) {
         // flag the timeout and let the copies in flight land before the CTA exits
+        cpa_wait_all();
         if (t == 0) {
             if (err) atomicExch(err, 1);
             mbar_wait_bounded(&bar[j & 1], (unsigned)((j >> 1) & 1));
@@ -412,17 +544,24 @@ __global__ void __launch_bounds__(128, PIPE_MINB)
         return;
     }
     if constexpr (!RESTRICT) {
-        if (dot.r) {  // the leaves' z.r partials into the level's reduction
-            const int K = (nl - (int)blockIdx.x + G - 1) / G;
+        if (dot.r) {  // one partial per CTA into the launch's reduction (a ticket per CTA, not per leaf)
             double tot = 0.0;
-            if (red_publish_strided<false>(dot.partials, &dot.st->ticket[0], (int)blockIdx.x, G, K, nl, tot)) {
+            constexpr int TK = DOTK == 1 ? 2 : 0;
+            if (reduce_sum(cta_dot, dot.partials, &dot.st->ticket[TK], (int)blockIdx.x, G, tot)) {
                 if (t == 0) {
                     PcgState* st = dot.st;
-                    const float rho_new = (float)tot;
-                    st->rho_new = rho_new;
-                    st->beta = st->first ? 0.f : __fdiv_rn(rho_new, st->rho);
-                    st->rho = rho_new;
-                    st->ticket[0] = 0;
+                    if constexpr (DOTK == 1) {
+                        const float sigma = (float)tot;
+                        st->sigma = sigma;
+                        st->alpha = __fdiv_rn(st->rho, sigma);
+                        st->first = 0;
+                    } else {
+                        const float rho_new = (float)tot;
+                        st->rho_new = rho_new;
+                        st->beta = st->first ? 0.f : __fdiv_rn(rho_new, st->rho);
+                        st->rho = rho_new;
+                    }
+                    st->ticket[TK] = 0;
                 }
             }
         }
