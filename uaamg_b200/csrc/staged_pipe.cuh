@@ -172,72 +172,67 @@ __device__ __forceinline__ PNb pnb_load(const int* nbr, int leaf) {
 }
 
 // Issue a thread's share of a leaf's halo: STAT the coefficient faces, the
-// mask and the flags (no change during a solve), DYN the x faces.
+// mask and the flags (no change during a solve), DYN the x faces.  Each
+// group of 16 threads copies one kind of face chunk (threads 0-15 the -x
+// face, 16-31 +x, 32-47 -y, 48-63 +y, 64-79 c_x of the +x neighbour, 80-95
+// c_y of the +y neighbour, 96-127 c_z of the +z neighbour, two each), so
+// the branches are uniform over half-warps; every thread copies its own
+// z-face value.  The slots are those pvalue reads: a +-y face slot
+// s = 2X + zh holds the chunk of the consumer thread 16X + 14 + zh (+y) or
+// 16X + zh (-y).
 template <bool STAT, bool DYN, class LV>
 __device__ __forceinline__ void phalo_issue(const LV& L, int leaf, const PNb& N, int t, unsigned char* st,
                                             const typename PipeLv<LV>::E* x) {
     using E = typename PipeLv<LV>::E;
     using Lo = PLayout<E>;
     constexpr unsigned C = Lo::C;
-    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
-    const int ys = 2 * X + zh;  // slot of a +-y face thread
+    const int c = t >> 4, i = t & 15;
+    const int ych = 16 * (i >> 1) + (i & 1);  // +y neighbour chunk of y-face slot i (-y: + 14)
     if constexpr (STAT) {
-        // a missing FP32 neighbour reads the default face coefficient; a
-        // missing 16-bit one is flagged trimmed below
-        if (X == 7) {
+        if (c == 4) {
             const int n = N.v[1];
-            unsigned char* d = st + Lo::HCXP + (t - 112) * C;
-            if (n >= 0) cpa_chunk(d, L.cx + (long long)n * UAAMG_LEAF + 4 * (t - 112));
+            unsigned char* d = st + Lo::HCXP + i * C;
+            if (n >= 0) cpa_chunk(d, L.cx + (long long)n * UAAMG_LEAF + 4 * i);
             else if constexpr (!PipeLv<LV>::SCALED) *reinterpret_cast<float4*>(d) = f4splat(L.def_face);
-        }
-        if (Y == 7) {
+        } else if (c == 5) {
             const int n = N.v[3];
-            unsigned char* d = st + Lo::HCYP + ys * C;
-            if (n >= 0) cpa_chunk(d, L.cy + (long long)n * UAAMG_LEAF + 4 * (t - 14));
+            unsigned char* d = st + Lo::HCYP + i * C;
+            if (n >= 0) cpa_chunk(d, L.cy + (long long)n * UAAMG_LEAF + 4 * ych);
             else if constexpr (!PipeLv<LV>::SCALED) *reinterpret_cast<float4*>(d) = f4splat(L.def_face);
-        }
-        if (zh == 1) {
+        } else if (c >= 6) {
+            // c_z entries e = 2j, 2j+1 of the consumers 2e+1 (zh = 1): elements 8e
             const int n = N.v[5];
-            unsigned char* d = st + Lo::HCZ + 4 * (t >> 1);
-            if (n >= 0) cpa4(d, L.cz + (long long)n * UAAMG_LEAF + 4 * t - 4);
-            else if constexpr (!PipeLv<LV>::SCALED) *reinterpret_cast<float*>(d) = L.def_face;
-        }
-        if (t < 4)
-            cpa16(st + Lo::MASK + 16 * t, reinterpret_cast<const unsigned char*>(L.mask + (long long)leaf * 8) + 16 * t);
-        if constexpr (PipeLv<LV>::SCALED) {
-            if (t >= 4 && t < 7) {
-                const int n = (t == 4) ? N.v[1] : ((t == 5) ? N.v[3] : N.v[5]);  // +x, +y, +z
-                unsigned char* d = st + Lo::FLG + 4 * (t - 4);
-                if (n >= 0) cpa4(d, L.flags + n);
-                else *reinterpret_cast<unsigned*>(d) = 0xFFFFFFFFu;  // missing: the default
+            const int e0 = 2 * (t - 96);
+            unsigned char* d = st + Lo::HCZ + 4 * e0;
+            if (n >= 0) {
+                cpa4(d, L.cz + (long long)n * UAAMG_LEAF + 8 * e0);
+                cpa4(d + 4, L.cz + (long long)n * UAAMG_LEAF + 8 * e0 + 8);
+            } else if constexpr (!PipeLv<LV>::SCALED) {
+                *reinterpret_cast<float2*>(d) = make_float2(L.def_face, L.def_face);
+            }
+            if (t < 100) {
+                cpa16(st + Lo::MASK + 16 * (t - 96),
+                      reinterpret_cast<const unsigned char*>(L.mask + (long long)leaf * 8) + 16 * (t - 96));
+            } else if constexpr (PipeLv<LV>::SCALED) {
+                if (t < 103) {
+                    const int nn = (t == 100) ? N.v[1] : ((t == 101) ? N.v[3] : N.v[5]);  // +x, +y, +z
+                    unsigned char* f = st + Lo::FLG + 4 * (t - 100);
+                    if (nn >= 0) cpa4(f, L.flags + nn);
+                    else *reinterpret_cast<unsigned*>(f) = 0xFFFFFFFFu;  // missing: the default
+                }
             }
         }
     }
     if constexpr (DYN) {
-        if (X == 7) {
-            const int n = N.v[1];
-            unsigned char* d = st + Lo::HXP + (t - 112) * C;
-            if (n >= 0) cpa_chunk(d, x + (long long)n * UAAMG_LEAF + 4 * (t - 112));
+        if (c < 4) {
+            const int n = (c == 0) ? N.v[0] : ((c == 1) ? N.v[1] : ((c == 2) ? N.v[2] : N.v[3]));
+            const unsigned off = (c == 0) ? Lo::HXM : ((c == 1) ? Lo::HXP : ((c == 2) ? Lo::HYM : Lo::HYP));
+            const int ch = (c == 0) ? i + 112 : ((c == 1) ? i : ((c == 2) ? ych + 14 : ych));
+            unsigned char* d = st + off + i * C;
+            if (n >= 0) cpa_chunk(d, x + (long long)n * UAAMG_LEAF + 4 * ch);
             else zero_chunk<E>(d);
         }
-        if (X == 0) {
-            const int n = N.v[0];
-            unsigned char* d = st + Lo::HXM + t * C;
-            if (n >= 0) cpa_chunk(d, x + (long long)n * UAAMG_LEAF + 4 * (t + 112));
-            else zero_chunk<E>(d);
-        }
-        if (Y == 7) {
-            const int n = N.v[3];
-            unsigned char* d = st + Lo::HYP + ys * C;
-            if (n >= 0) cpa_chunk(d, x + (long long)n * UAAMG_LEAF + 4 * (t - 14));
-            else zero_chunk<E>(d);
-        }
-        if (Y == 0) {
-            const int n = N.v[2];
-            unsigned char* d = st + Lo::HYM + ys * C;
-            if (n >= 0) cpa_chunk(d, x + (long long)n * UAAMG_LEAF + 4 * (t + 14));
-            else zero_chunk<E>(d);
-        }
+        const int zh = t & 1;
         const int n = zh ? N.v[5] : N.v[4];
         unsigned char* d = st + Lo::HZ + 4 * t;
         if (n >= 0) {
@@ -389,7 +384,10 @@ __device__ __forceinline__ float4 pvalue(const LV& L, int t, unsigned fl, const 
 }
 
 #ifndef PIPE_MINB
-#define PIPE_MINB 6
+#define PIPE_MINB 6  // FP32: 6 stages of 33.5 KB fill the shared memory of an SM
+#endif
+#ifndef PIPE_MINB16
+#define PIPE_MINB16 7  // 16-bit stages are half the size: one more CTA per SM (8 spills)
 #endif
 // CTAs of a pipelined launch (at most one per leaf): 6 per SM on a 148-SM
 // B200.  A constant rather than the occupancy of the GPU at hand, so the
@@ -415,7 +413,7 @@ constexpr size_t pipe_smem_bytes() {
 // or dot.r (PCG lines 13-15: rho, beta), 1 p.q with p the swept vector (the
 // Laplacian of PCG lines 6-7: sigma, alpha).
 template <int MODE, class LV, typename TOut, bool RESTRICT, int DOTK = 0>
-__global__ void __launch_bounds__(128, PIPE_MINB)
+__global__ void __launch_bounds__(128, PipeLv<LV>::SCALED ? PIPE_MINB16 : PIPE_MINB)
     k_pipe(LV L, const typename PipeLv<LV>::E* x, const typename PipeLv<LV>::E* b, TOut* out, float w, float wsor,
            float one_minus_wsor, DotOut dot, const float* zscale, float coarse_scale, int* err) {
     using E = typename PipeLv<LV>::E;
