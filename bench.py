@@ -462,9 +462,16 @@ def main():
                     help="seconds of arrivals of the served request stream (0 = skip)")
     ap.add_argument("--serve-limit", type=float, default=60.0, help="time limit of each served run (s)")
     ap.add_argument("--no-graph", action="store_true", help="host-driven PCG loop instead of the CUDA graph")
-    ap.add_argument("--profile", choices=["solve", "sweep", "vsolve"], default=None,
+    ap.add_argument("--profile", choices=["solve", "sweep", "vsolve", "large"], default=None,
                     help="short fixed sequence for ncu: 'vsolve' = viscosity build + 2 solves, "
-                         "'solve' = Poisson build + 2 graph solves, 'sweep' = Poisson build + 3 level-0 sweeps")
+                         "'solve' = Poisson build + 2 graph solves, 'sweep' = Poisson build + 3 level-0 sweeps, "
+                         "'large' = the mixed-precision workload at --mixed-n, one host-driven solve in "
+                         "--profile-form")
+    ap.add_argument("--profile-form", choices=["fp32", "fp16", "bf16"], default="fp32",
+                    help="precision of the 'large' profile solve")
+    ap.add_argument("--profile-events", action="store_true",
+                    help="'large' profile: time every kernel of the solve with CUDA event pairs and print the "
+                         "per-kernel-class table (ms, launches) as JSON")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -498,6 +505,40 @@ def main():
         d.values = t.numpy()  # numpy view of pinned memory: host pointer path
         d._pin = t
         return d
+
+    if args.profile == "large":
+        with torch.cuda.stream(stream):
+            phi, fw, vx, vy, vz, sv, dt, dx = scenes.device_large_poisson(args.mixed_n, 2, dev)
+        stream.synchronize()
+        lap = LaplacianWithLevel.createPressurePoissonLaplacian(phi, fw, dt, dx, stream=stream.cuda_stream)
+        rhs = torch.empty((lap.leaf_count(0), 512), dtype=torch.float32, device=dev)
+        lap.createPressurePoissonRightHandSide(fw, vx, vy, vz, sv, dt, out=rhs)
+        del phi, fw, vx, vy, vz
+        torch.cuda.synchronize()
+        solver = PoissonSolver(lap)
+        solver.use_graph = 0
+        p = torch.zeros_like(rhs)
+        out = {"profile": "large", "form": args.profile_form, "n": args.mixed_n,
+               "leaves": [lap.leaf_count(l) for l in range(lap.num_levels())]}
+        if args.profile_form != "fp32":
+            solver.prepare_mixed(args.profile_form)
+        if args.profile_events:
+            for _ in range(2):  # the second run is reported
+                p.zero_()
+                if args.profile_form == "fp32":
+                    table = solver.profile_pcg(p, rhs)
+                else:
+                    table = solver.profile_pcg_mixed(p, rhs, args.profile_form)
+            out["kernel_ms"] = {k: [round(v[0], 4), v[1]]
+                                for k, v in sorted(table.items(), key=lambda kv: -kv[1][0])}
+            out["total_ms"] = round(sum(v[0] for v in table.values()), 3)
+        elif args.profile_form == "fp32":
+            solver.solveMultigridPCG(p, rhs)
+        else:
+            solver.solveMultigridPCGMixed(p, rhs, args.profile_form)
+        out["iterations"] = solver.mIterationTaken
+        print(json.dumps(out))
+        return
 
     vsc = scenes.plain_viscosity_scene(n=args.n, seed=1)
     vkeys = ("liquid_phi", "solid_phi", "viscosity", "u", "v", "w", "solid_velocity")
