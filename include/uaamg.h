@@ -234,6 +234,52 @@ int uaamg_poisson_profile_pcg_mixed(uaamg_poisson* h, int precision, float* d_pr
                                     int max_classes, char* names, double* total_ms, int64_t* counts, int* nclasses);
 
 /* ======================================================================== */
+/* The steps either side of the pressure solve in a FLIP projection.        */
+
+/* Solid face weights on a given topology: for every active voxel (masks may
+ * be NULL: all voxels), 1 - fraction_inside of the solid over each of its
+ * three minus faces, from the solid SDF at the 8 voxel corners, clamped to
+ * [0, 1] and set to 0 below 1e-2; inactive voxels get (1, 1, 1).  weights:
+ * float[leaf_count][512][3].  Replaces FLIP_Solver_OpenVDB::
+ * calculate_face_weights (FLIP_vdb/FLIP_vdb.cpp:2669-2752) on the topology
+ * the caller provides there (the liquid SDF's dilated by 2 voxels,
+ * :2672-2675); fraction_inside(bl, br, tl, tr) is levelset_util.cpp:23-100.
+ * The _device form writes device memory on the given stream (NULL: the
+ * default stream) and returns without waiting. */
+int uaamg_face_weights(const uaamg_leaf_grid* solid_sdf, int64_t leaf_count, const int32_t* origins,
+                       const uint64_t* masks, float* weights);
+int uaamg_face_weights_device(const uaamg_leaf_grid* solid_sdf, int64_t leaf_count, const int32_t* origins,
+                              const uint64_t* masks, float* d_weights, void* stream);
+
+/* Pressure-gradient update of one velocity channel (0 x, 1 y, 2 z) with the
+ * pressure solution of handle h (leaf-dense on its level 0): at every active
+ * voxel of `velocity` whose face weight is positive and which has a DOF on
+ * either side, u += -dt (p - p_below) / dx / theta (theta = fraction_inside
+ * of the liquid SDF between the two cells, at least 0.02, when either is
+ * air); the reflected velocity is the updated one plus the update again; a
+ * face with weight w < 1 then becomes (1 - s) u + s u_solid with
+ * s = (1 - w) friction.  Voxels without an update become inactive.  Outputs
+ * (float[leaf][512], uint64[leaf][8]): velocity_out, mask_out (the new active
+ * set), update_out and reflected_out (may be NULL; the input value where
+ * there is no update).  Replaces FLIP_Solver_OpenVDB::apply_pressure_gradient
+ * (FLIP_vdb.cpp:2571-2667) for one channel; friction is
+ * boundary_friction_coefficient. */
+int uaamg_poisson_apply_pressure_gradient(uaamg_poisson* h, const uaamg_leaf_grid* liquid_phi,
+                                          const uaamg_leaf_grid* face_weights, const uaamg_leaf_grid* solid_velocity,
+                                          const float* pressure, float dt, float friction, int channel,
+                                          const uaamg_leaf_grid* velocity, float* velocity_out, uint64_t* mask_out,
+                                          float* update_out, float* reflected_out);
+/* Device form: pressure, velocity (updated in place), the mask and the
+ * optional outputs are device pointers; velocity->masks and ->origins stay
+ * host pointers.  Runs on the handle's stream without waiting. */
+int uaamg_poisson_apply_pressure_gradient_device(uaamg_poisson* h, const uaamg_leaf_grid* liquid_phi,
+                                                 const uaamg_leaf_grid* face_weights,
+                                                 const uaamg_leaf_grid* solid_velocity, const float* d_pressure,
+                                                 float dt, float friction, int channel,
+                                                 const uaamg_leaf_grid* velocity, float* d_velocity,
+                                                 uint64_t* d_mask_out, float* d_update_out, float* d_reflected_out);
+
+/* ======================================================================== */
 /* Batched pressure solves: PoissonSolver::solveMultigridPCG
  * (simd_vdb_poisson.cpp:2155-2226) of many independent instances in one CUDA
  * graph launch.  The reference has no batched form; each instance's result,

@@ -100,6 +100,13 @@ def lib():
         L.orc_visc_abs_max.restype = C.c_float
         L.orc_visc_dot.argtypes = [vp, C.c_int, f32p, f32p]
         L.orc_visc_dot.restype = C.c_float
+        L.orc_fraction_inside4.argtypes = [C.c_float] * 4
+        L.orc_fraction_inside4.restype = C.c_float
+        L.orc_face_weights.argtypes = [C.c_int64, i32p, f32p, C.c_float, C.c_int64, i32p, vp, f32p]
+        L.orc_pressure_gradient.argtypes = [C.c_int64, i32p, f32p, C.c_float, C.c_int64, i32p, f32p, f32p,
+                                            C.c_int64, i32p, f32p, f32p, C.c_int64, i32p, u64p, f32p,
+                                            C.c_float, C.c_float, C.c_float, C.c_int,
+                                            C.c_int64, i32p, vp, f32p, f32p, u64p, f32p, f32p]
         _LIB = L
     return _LIB
 
@@ -362,3 +369,48 @@ class OracleViscosity:
 
 def set_threads(n: int) -> None:
     lib().orc_set_threads(int(n))
+
+
+# ---------------------------------------------------------------------------
+# The steps either side of the pressure solve (projection_oracle.c)
+
+def fraction_inside4(bl, br, tl, tr) -> float:
+    """fraction_inside(bl, br, tl, tr) (levelset_util.cpp:23-100)."""
+    return float(lib().orc_fraction_inside4(float(bl), float(br), float(tl), float(tr)))
+
+
+def face_weights(solid_sdf, origins, masks=None) -> np.ndarray:
+    """calculate_face_weights (FLIP_vdb.cpp:2669-2752) on the given topology:
+    float32 [leaf][512][3]."""
+    org = np.ascontiguousarray(origins, dtype=np.int32)
+    n = org.shape[0]
+    out = np.zeros((n, 512, 3), np.float32)
+    m = None if masks is None else np.ascontiguousarray(masks, dtype=np.uint64)
+    lib().orc_face_weights(*_grid_args(solid_sdf), float(solid_sdf.background.reshape(-1)[0]), n,
+                           org.reshape(-1), None if m is None else m.ctypes.data, out.reshape(-1))
+    return out
+
+
+def pressure_gradient(liquid_phi, face_weights, solid_velocity, p_origins, p_masks, pressure, dt, dx, friction,
+                      channel, velocity):
+    """apply_pressure_gradient (FLIP_vdb.cpp:2571-2667) for one channel.  The
+    pressure is given on its leaves (origins, DOF masks, values [leaf][512]).
+    Returns (velocity, masks, update, reflected)."""
+    v = np.ascontiguousarray(velocity.values.reshape(-1), dtype=np.float32)
+    n = velocity.leaf_count
+    vm = None if velocity.masks is None else np.ascontiguousarray(velocity.masks, dtype=np.uint64)
+    out = np.zeros(n * 512, np.float32)
+    upd = np.zeros(n * 512, np.float32)
+    refl = np.zeros(n * 512, np.float32)
+    mask = np.zeros(n * 8, np.uint64)
+    lib().orc_pressure_gradient(
+        *_grid_args(liquid_phi), float(liquid_phi.background.reshape(-1)[0]),
+        *_grid_args(face_weights), _f32(face_weights.background),
+        *_grid_args(solid_velocity), _f32(solid_velocity.background),
+        int(np.asarray(p_origins).shape[0]), np.ascontiguousarray(p_origins, dtype=np.int32).reshape(-1),
+        np.ascontiguousarray(p_masks, dtype=np.uint64).reshape(-1),
+        np.ascontiguousarray(pressure, dtype=np.float32).reshape(-1),
+        float(dt), float(dx), float(friction), int(channel),
+        n, np.ascontiguousarray(velocity.origins, dtype=np.int32).reshape(-1),
+        None if vm is None else vm.ctypes.data, v, out, mask, upd, refl)
+    return out.reshape(n, 512), mask.reshape(n, 8), upd.reshape(n, 512), refl.reshape(n, 512)

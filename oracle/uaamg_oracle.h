@@ -180,6 +180,19 @@ int orc_visc_pcg(orc_visc* h, float* x, const float* b, float tol, int max_iter,
 float orc_visc_abs_max(const orc_visc* h, int level, const float* v);
 float orc_visc_dot(const orc_visc* h, int level, const float* a, const float* b);
 
+/* ------------------------------------------------------------------------ */
+/* The steps either side of the pressure solve (projection_oracle.c). */
+float orc_fraction_inside4(float phi_bl, float phi_br, float phi_tl, float phi_tr);
+void orc_face_weights(int64_t solid_n, const int32_t* solid_origins, const float* solid_values, float solid_bg,
+                      int64_t n, const int32_t* origins, const uint64_t* masks, float* out);
+void orc_pressure_gradient(int64_t phi_n, const int32_t* phi_origins, const float* phi_values, float phi_bg,
+                           int64_t fw_n, const int32_t* fw_origins, const float* fw_values, const float* fw_bg3,
+                           int64_t sv_n, const int32_t* sv_origins, const float* sv_values, const float* sv_bg3,
+                           int64_t p_n, const int32_t* p_origins, const uint64_t* p_masks, const float* p_values,
+                           float in_dt, float dx, float friction, int channel,
+                           int64_t v_n, const int32_t* v_origins, const uint64_t* v_masks, const float* v_values,
+                           float* v_out, uint64_t* mask_out, float* update_out, float* reflected_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,11 @@ EXPORTS = [
     ("uaamg_poisson_dof_index", i32, [vp, i32, vp]),
     ("uaamg_poisson_build_rhs", i32, [vp, pLG, pLG, pLG, pLG, pLG, f32, vp]),
     ("uaamg_poisson_build_rhs_device", i32, [vp, pLG, pLG, pLG, pLG, pLG, f32, vp]),
+    ("uaamg_face_weights", i32, [pLG, C.c_int64, vp, vp, vp]),
+    ("uaamg_face_weights_device", i32, [pLG, C.c_int64, vp, vp, vp, vp]),
+    ("uaamg_poisson_apply_pressure_gradient", i32, [vp, pLG, pLG, pLG, vp, f32, f32, i32, pLG, vp, vp, vp, vp]),
+    ("uaamg_poisson_apply_pressure_gradient_device", i32,
+     [vp, pLG, pLG, pLG, vp, f32, f32, i32, pLG, vp, vp, vp, vp]),
     ("uaamg_poisson_solve_pcg", i32, [vp, vp, vp, C.POINTER(C.c_int)]),
     ("uaamg_poisson_solve_pcg_device", i32, [vp, vp, vp, C.POINTER(C.c_int)]),
     ("uaamg_poisson_solve_mg", i32, [vp, vp, vp, C.POINTER(C.c_int)]),

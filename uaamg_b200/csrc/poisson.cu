@@ -301,8 +301,8 @@ static T* carve(char*& cur, size_t count) {
 }
 static size_t carve_size(size_t count, size_t elem) { return (count * elem + 255) & ~size_t(255); }
 
-static void upload_grid(uaamg_poisson* h, const uaamg_leaf_grid* gr, DevGrid& dg, HostMap& map,
-                        std::vector<void*>& tofree) {
+static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf_grid* gr, DevGrid& dg, HostMap& map,
+                           std::vector<void*>& tofree) {
     map.build(gr->leaf_count, gr->origins);
     dg.g = DGrid{};
     dg.g.comps = gr->components;
@@ -314,21 +314,26 @@ static void upload_grid(uaamg_poisson* h, const uaamg_leaf_grid* gr, DevGrid& dg
     size_t vbytes = (size_t)gr->leaf_count * UAAMG_LEAF * gr->components * sizeof(float);
     size_t total = carve_size(mapn, 4) + (gr->values_on_device ? 0 : carve_size(vbytes, 1));
     void* mem = nullptr;
-    CK(ctx_dev_alloc(h->ctx, &mem, total, h->stream));
+    CK(ctx_dev_alloc(ctx, &mem, total, stream));
     tofree.push_back(mem);
     char* cur = (char*)mem;
     int* dmap = carve<int>(cur, mapn);
-    CK(cudaMemcpyAsync(dmap, map.idx.data(), mapn * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(dmap, map.idx.data(), mapn * 4, cudaMemcpyHostToDevice, stream));
     const float* vals = gr->values;
     if (!gr->values_on_device) {
         float* dv = carve<float>(cur, vbytes / 4);
-        CK(cudaMemcpyAsync(dv, gr->values, vbytes, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(dv, gr->values, vbytes, cudaMemcpyHostToDevice, stream));
         vals = dv;
     }
     dg.g.val = vals;
     dg.g.map = dmap;
     dg.g.lo0 = map.lo[0]; dg.g.lo1 = map.lo[1]; dg.g.lo2 = map.lo[2];
     dg.g.d0 = map.dim[0]; dg.g.d1 = map.dim[1]; dg.g.d2 = map.dim[2];
+}
+
+static void upload_grid(uaamg_poisson* h, const uaamg_leaf_grid* gr, DevGrid& dg, HostMap& map,
+                        std::vector<void*>& tofree) {
+    upload_grid_cs(h->ctx, h->stream, gr, dg, map, tofree);
 }
 
 static void check_grid(const uaamg_leaf_grid* g, int comps, const char* name) {

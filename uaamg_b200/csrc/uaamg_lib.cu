@@ -3,3 +3,4 @@
 #include "batch.cu"
 #include "mixed.cu"
 #include "viscosity.cu"
+#include "projection.cu"
