@@ -416,6 +416,123 @@ SERVE_WORKLOAD = ("served stream: Poisson arrivals 200/s and viscosity arrivals 
                   "resident, admission by HBM budget")
 
 
+def run_projection(args, dev, stream, timed, max_over_ranks, ws, rank):
+    """The steps either side of the pressure solve on the plain Poisson
+    workload (128^3): the solid face weights on the liquid's dilated topology
+    (walls 1.5 voxels thick and a sphere obstacle of radius n/8 as the solid
+    SDF) and the pressure-gradient update of the three velocity channels with
+    the solved pressure.  Inputs device-resident, L2 flushed before each step;
+    the CPU oracle (OpenMP) is timed on the same inputs."""
+    import ctypes as C
+    import torch
+    from uaamg_b200 import _lib, scenes
+    from uaamg_b200.grids import LeafGrid, dense_to_leaves
+    from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver, _as_c
+    from uaamg_b200.projection import face_weight_topology
+    sc = scenes.plain_poisson_scene(n=args.n, seed=0)
+    n, dx = sc.n, sc.dx
+    lo, size = -8, n + 16
+    c = np.arange(size, dtype=np.float64) + lo
+    X, Y, Z = np.meshgrid(c, c, c, indexing="ij")
+    wall = np.minimum.reduce([X - 1.5, n - 1.5 - X, Y - 1.5, n - 1.5 - Y, Z - 1.5, n - 1.5 - Z])
+    sph = np.sqrt((X - n / 2) ** 2 + (Y - n / 4) ** 2 + (Z - n / 2) ** 2) - n / 8
+    solid = dense_to_leaves((np.minimum(wall, sph) * dx).astype(np.float32), origin=(lo, lo, lo),
+                            background=-3.0 * dx)
+    del X, Y, Z, wall, sph
+    origins, masks = face_weight_topology(sc.phi)
+    nfw = origins.shape[0]
+    keep = []
+
+    def dev_grid(g):
+        d = LeafGrid(origins=g.origins, values=g.values, background=g.background, masks=g.masks)
+        d.values = torch.from_numpy(np.ascontiguousarray(g.values)).to(dev)
+        return d
+
+    solid_d = dev_grid(solid)
+    gs = _as_c(solid_d, keep)
+    w_d = torch.empty((nfw, 512, 3), dtype=torch.float32, device=dev)
+    L = _lib.lib()
+
+    def fw_step():
+        _lib.check(L.uaamg_face_weights_device(C.byref(gs), nfw, origins.ctypes.data, masks.ctypes.data,
+                                               w_d.data_ptr(), C.c_void_p(stream.cuda_stream)), "face_weights")
+
+    for _ in range(args.warmup):
+        fw_step()
+    t_fw = timed(fw_step, args.steps)
+    torch.cuda.synchronize()
+    fw = LeafGrid(origins=origins, values=w_d.cpu().numpy(), background=np.ones(3, np.float32), masks=masks)
+    fw_d = dev_grid(fw)
+    phi_d = dev_grid(sc.phi)
+    lap = LaplacianWithLevel.createPressurePoissonLaplacian(phi_d, fw_d, sc.dt, sc.dx, stream=stream.cuda_stream)
+    rhs = torch.empty((lap.leaf_count(0), 512), dtype=torch.float32, device=dev)
+    lap.createPressurePoissonRightHandSide(fw_d, dev_grid(sc.vx), dev_grid(sc.vy), dev_grid(sc.vz),
+                                          sc.solid_velocity, sc.dt, out=rhs)
+    solver = PoissonSolver(lap)
+    solver.set_stream(stream.cuda_stream)
+    p = torch.zeros_like(rhs)
+    st = solver.solveMultigridPCG(p, rhs)
+    m = n + 1
+    sv = dense_to_leaves(np.random.default_rng(11).uniform(-1, 1, (m, m, m, 3)).astype(np.float32),
+                         background=np.zeros(3, np.float32))
+    sv_d = dev_grid(sv)
+    vels = [sc.vx, sc.vy, sc.vz]
+    vin = [torch.from_numpy(np.ascontiguousarray(v.values)).to(dev) for v in vels]
+    vwork = [x.clone() for x in vin]
+    nv = [v.leaf_count for v in vels]
+    mk = [torch.empty(k * 8, dtype=torch.int64, device=dev) for k in nv]
+    up = [torch.empty_like(x) for x in vin]
+    rf = [torch.empty_like(x) for x in vin]
+    gphi, gfw, gsv = _as_c(phi_d, keep), _as_c(fw_d, keep), _as_c(sv_d, keep)
+    gv = [_as_c(v, keep) for v in vels]
+    friction = 0.5
+
+    def pg_step():
+        for ch in range(3):
+            vwork[ch].copy_(vin[ch])
+            _lib.check(L.uaamg_poisson_apply_pressure_gradient_device(
+                lap._h, C.byref(gphi), C.byref(gfw), C.byref(gsv), p.data_ptr(), float(sc.dt), friction, ch,
+                C.byref(gv[ch]), vwork[ch].data_ptr(), mk[ch].data_ptr(), up[ch].data_ptr(), rf[ch].data_ptr()),
+                "apply_pressure_gradient")
+
+    for _ in range(args.warmup):
+        pg_step()
+    t_pg = timed(pg_step, args.steps)
+    t_fw, t_pg = max_over_ranks(t_fw, t_pg)
+    fw_ms, pg_ms = t_fw / args.steps, t_pg / args.steps
+    fw_vox = int(np.unpackbits(masks.view(np.uint8)).sum())
+    v_vox = int(sum(k * 512 for k in nv))
+    # algorithmic bytes: face weights read the solid SDF once per voxel (4 B) and write 3 weights (12 B); the
+    # gradient update reads u, w, phi, p (two cells each for phi and p) and the solid velocity and writes u, the
+    # update, the reflected value and the mask (36 B per velocity voxel, the copy of u included)
+    out = {"workload": f"projection steps on the plain Poisson workload {n}^3: face weights on the liquid SDF "
+                       f"dilated by 2 voxels (solid = walls + sphere r=n/8), pressure-gradient update of the 3 "
+                       f"velocity channels (friction {friction})",
+           "face_weights": {"ms": round(fw_ms, 4), "voxels": fw_vox, "leaves": nfw,
+                            "GBps_algorithmic": round(16.0 * nfw * 512 / (fw_ms * 1e-3) / 1e9, 1)},
+           "pressure_gradient": {"ms_3_channels": round(pg_ms, 4), "voxels": v_vox, "solve_status": int(st),
+                                 "GBps_algorithmic": round(36.0 * v_vox / (pg_ms * 1e-3) / 1e9, 1)},
+           "l2": "flushed before every timed step (256 MiB write)"}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:  # the oracle as the timed CPU baseline
+        import os
+        import time as _t
+        from oracle import oracle as orc
+        pc = p.cpu().numpy()
+        ref = orc.OraclePoisson(sc.phi, fw, sc.dt, sc.dx, hierarchy=False)
+        po, pm = ref.topology(0)
+        t0 = _t.perf_counter()
+        orc.face_weights(solid, origins, masks)
+        t1 = _t.perf_counter()
+        for ch in range(3):
+            orc.pressure_gradient(sc.phi, fw, sv, po, pm, pc, sc.dt, sc.dx, friction, ch, vels[ch])
+        t2 = _t.perf_counter()
+        out["cpu_oracle_ms"] = {"face_weights": round((t1 - t0) * 1e3, 2),
+                                "pressure_gradient_3_channels": round((t2 - t1) * 1e3, 2),
+                                "threads": os.cpu_count()}
+    out["_launches"] = 4 * args.steps
+    return out
+
+
 def run_served(args, ws):
     """The served stream on this GPU: batched (pressure rounds in one graph,
     viscosity lanes overlapping) vs the plain form (every solve alone, in
@@ -456,6 +573,8 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the secondary Poisson measurement")
+    ap.add_argument("--no-projection", action="store_true",
+                    help="skip the face-weight and pressure-gradient measurement")
     ap.add_argument("--batch", type=int, default=64, help="instances of the batched Poisson measurement (0 = skip)")
     ap.add_argument("--mixed-n", type=int, default=512, help="domain side of the mixed-precision measurement (0 = skip)")
     ap.add_argument("--serve-window", type=float, default=0.2,
@@ -773,6 +892,11 @@ def main():
     if args.mixed_n > 0:
         mixed = run_mixed(args, dev, stream, timed, max_over_ranks, ws)
 
+    # ================= the steps either side of the pressure solve =================
+    projection = None
+    if not args.no_projection:
+        projection = run_projection(args, dev, stream, timed, max_over_ranks, ws, rank)
+
     # ================= served request stream (continuous batching) =================
     served = None
     if args.serve_window > 0:
@@ -822,6 +946,9 @@ def main():
         if mixed is not None:
             line["mixed"] = mixed
             line["gpu_launches"] = int(line["gpu_launches"] + mixed.pop("_launches"))
+        if projection is not None:
+            line["projection"] = projection
+            line["gpu_launches"] = int(line["gpu_launches"] + projection.pop("_launches"))
         if batched is not None:
             line["batched"] = batched
             line["gpu_launches"] = int(line["gpu_launches"] + batched.pop("_launches"))
