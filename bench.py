@@ -498,8 +498,40 @@ def run_projection(args, dev, stream, timed, max_over_ranks, ws, rank):
     for _ in range(args.warmup):
         pg_step()
     t_pg = timed(pg_step, args.steps)
-    t_fw, t_pg = max_over_ranks(t_fw, t_pg)
-    fw_ms, pg_ms = t_fw / args.steps, t_pg / args.steps
+    torch.cuda.synchronize()
+
+    # velocity extrapolation after the gradient update (FLIP_vdb.cpp:2379): the updated voxels of each channel
+    # extrapolated 3 layers into the liquid SDF's topology; the topology set operations run on the host (timed
+    # apart), the layers on the device with the channel values and masks resident
+    from uaamg_b200.extrapolate import prepare_channel, run_layers_device, topology_of
+    import time as _time
+    n_layer = 3
+    target = topology_of(sc.phi)
+    ex_in = [LeafGrid(origins=vels[ch].origins, values=vwork[ch].cpu().numpy(), background=vels[ch].background,
+                      masks=mk[ch].cpu().numpy().view(np.uint64).reshape(-1, 8).copy()) for ch in range(3)]
+    tp0 = _time.perf_counter()
+    preps = [prepare_channel(g, target) for g in ex_in]
+    prep_ms = (_time.perf_counter() - tp0) * 1e3
+    xv_in = [torch.from_numpy(pr[1]).to(dev) for pr in preps]
+    xm_in = [torch.from_numpy(pr[2].view(np.int64)).to(dev) for pr in preps]
+    xv, xm = [x.clone() for x in xv_in], [x.clone() for x in xm_in]
+
+    def ex_step():
+        for ch in range(3):
+            xv[ch].copy_(xv_in[ch])
+            xm[ch].copy_(xm_in[ch])
+            org, _, _, fl, fm = preps[ch]
+            run_layers_device(n_layer, org, xv[ch], xm[ch], fl, fm, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        ex_step()
+    t_ex = timed(ex_step, args.steps)
+    t_fw, t_pg, t_ex = max_over_ranks(t_fw, t_pg, t_ex)
+    fw_ms, pg_ms, ex_ms = t_fw / args.steps, t_pg / args.steps, t_ex / args.steps
+    ex_fill = int(sum(int(np.unpackbits(pr[4].view(np.uint8)).sum()) for pr in preps))
+    ex_leaves = int(sum(pr[0].shape[0] for pr in preps))
+    ex_filled = int(sum(int(np.unpackbits(xm[ch].cpu().numpy().view(np.uint8)).sum())
+                        - int(np.unpackbits(preps[ch][2].view(np.uint8)).sum()) for ch in range(3)))
     fw_vox = int(np.unpackbits(masks.view(np.uint8)).sum())
     v_vox = int(sum(k * 512 for k in nv))
     # algorithmic bytes: face weights read the solid SDF once per voxel (4 B) and write 3 weights (12 B); the
@@ -512,6 +544,11 @@ def run_projection(args, dev, stream, timed, max_over_ranks, ws, rank):
                             "GBps_algorithmic": round(16.0 * nfw * 512 / (fw_ms * 1e-3) / 1e9, 1)},
            "pressure_gradient": {"ms_3_channels": round(pg_ms, 4), "voxels": v_vox, "solve_status": int(st),
                                  "GBps_algorithmic": round(36.0 * v_vox / (pg_ms * 1e-3) / 1e9, 1)},
+           "extrapolation": {"ms_3_channels": round(ex_ms, 4), "layers": n_layer,
+                             "target": "liquid SDF active voxels", "fill_set_voxels": ex_fill,
+                             "voxels_filled": ex_filled, "fill_leaves": int(sum(pr[3].size for pr in preps)),
+                             "output_leaves": ex_leaves, "host_topology_ms": round(prep_ms, 2),
+                             "note": "per channel: upload of the fill set and leaf map, 3 layer launches"},
            "l2": "flushed before every timed step (256 MiB write)"}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:  # the oracle as the timed CPU baseline
         import os
@@ -526,10 +563,14 @@ def run_projection(args, dev, stream, timed, max_over_ranks, ws, rank):
         for ch in range(3):
             orc.pressure_gradient(sc.phi, fw, sv, po, pm, pc, sc.dt, sc.dx, friction, ch, vels[ch])
         t2 = _t.perf_counter()
+        for pr in preps:
+            orc.extrapolate_channel(n_layer, *pr)
+        t3 = _t.perf_counter()
         out["cpu_oracle_ms"] = {"face_weights": round((t1 - t0) * 1e3, 2),
                                 "pressure_gradient_3_channels": round((t2 - t1) * 1e3, 2),
+                                "extrapolation_3_channels": round((t3 - t2) * 1e3, 2),
                                 "threads": os.cpu_count()}
-    out["_launches"] = 4 * args.steps
+    out["_launches"] = (4 + 3 * n_layer) * args.steps
     return out
 
 

@@ -279,6 +279,28 @@ int uaamg_poisson_apply_pressure_gradient_device(uaamg_poisson* h, const uaamg_l
                                                  const uaamg_leaf_grid* velocity, float* d_velocity,
                                                  uint64_t* d_mask_out, float* d_update_out, float* d_reflected_out);
 
+/* Velocity extrapolation of one channel into new voxels, n_layer layers
+ * (vdb_velocity_extrapolator::union_extrapolate, FLIP_vdb/
+ * vdb_velocity_extrapolator.cpp:585-662, the part after its topology steps).
+ * The output grid has n_out leaves (out_origins [n_out][3]); values
+ * [n_out][512] and masks [n_out][8] hold the channel (new leaves: the
+ * background, inactive) and are updated in place.  The fill set lists, for
+ * n_fill distinct output leaves fill_leaf[e], the voxels still to fill
+ * (fill_masks [n_fill][8]: the union topology minus the channel's active
+ * voxels).  Each layer gives every fill voxel with an active face neighbour
+ * (active before the layer) the mean of those neighbours, summed in the order
+ * -x, +x, -y, +y, -z, +z, and makes it active.  Host pointers. */
+int uaamg_extrapolate_channel(int n_layer, int64_t n_out, const int32_t* out_origins, float* values,
+                              uint64_t* masks, int64_t n_fill, const int32_t* fill_leaf,
+                              const uint64_t* fill_masks);
+/* The same with values [n_out][512] and masks [n_out][8] in device memory,
+ * updated in place on `stream` (NULL: the legacy default stream); out_origins,
+ * fill_leaf and fill_masks are host arrays (the topology, uploaded on the
+ * stream).  Enqueued only: the call returns before the layers finish. */
+int uaamg_extrapolate_channel_device(int n_layer, int64_t n_out, const int32_t* out_origins, float* values,
+                                     uint64_t* masks, int64_t n_fill, const int32_t* fill_leaf,
+                                     const uint64_t* fill_masks, void* stream);
+
 /* ======================================================================== */
 /* Batched pressure solves: PoissonSolver::solveMultigridPCG
  * (simd_vdb_poisson.cpp:2155-2226) of many independent instances in one CUDA

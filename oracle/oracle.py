@@ -107,6 +107,7 @@ def lib():
                                             C.c_int64, i32p, f32p, f32p, C.c_int64, i32p, u64p, f32p,
                                             C.c_float, C.c_float, C.c_float, C.c_int,
                                             C.c_int64, i32p, vp, f32p, f32p, u64p, f32p, f32p]
+        L.orc_extrapolate_channel.argtypes = [C.c_int, C.c_int64, i32p, f32p, u64p, C.c_int64, i32p, u64p]
         _LIB = L
     return _LIB
 
@@ -414,3 +415,16 @@ def pressure_gradient(liquid_phi, face_weights, solid_velocity, p_origins, p_mas
         n, np.ascontiguousarray(velocity.origins, dtype=np.int32).reshape(-1),
         None if vm is None else vm.ctypes.data, v, out, mask, upd, refl)
     return out.reshape(n, 512), mask.reshape(n, 8), upd.reshape(n, 512), refl.reshape(n, 512)
+
+
+def extrapolate_channel(n_layer, out_origins, values, masks, fill_leaf, fill_masks):
+    """union_extrapolate's layers (vdb_velocity_extrapolator.cpp:611-659) for
+    one channel; returns the updated (values, masks)."""
+    org = np.ascontiguousarray(out_origins, dtype=np.int32).reshape(-1)
+    v = np.array(values, dtype=np.float32, order="C").reshape(-1)
+    m = np.array(masks, dtype=np.uint64, order="C").reshape(-1)
+    fl = np.ascontiguousarray(fill_leaf, dtype=np.int32).reshape(-1)
+    fm = np.ascontiguousarray(fill_masks, dtype=np.uint64).reshape(-1)
+    n_out = org.size // 3
+    lib().orc_extrapolate_channel(int(n_layer), n_out, org, v, m, fl.size, fl, fm)
+    return v.reshape(n_out, 512), m.reshape(n_out, 8)

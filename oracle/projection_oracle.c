@@ -7,6 +7,8 @@
  *    (and the two-sample form, :4-13)
  *  - FLIP_Solver_OpenVDB::calculate_face_weights: FLIP_vdb/FLIP_vdb.cpp:2669-2752
  *  - FLIP_Solver_OpenVDB::apply_pressure_gradient: FLIP_vdb/FLIP_vdb.cpp:2571-2667
+ *  - vdb_velocity_extrapolator::union_extrapolate, the layers after its
+ *    topology steps: FLIP_vdb/vdb_velocity_extrapolator.cpp:611-659
  *
  * Compiled with -ffp-contract=off: every float operation is the reference's,
  * in its order, unfused.  Grids are flattened leaf grids (OpenVDB leaf
@@ -199,4 +201,53 @@ void orc_pressure_gradient(int64_t phi_n, const int32_t* phi_origins, const floa
     leafmap_free(&fw.map);
     leafmap_free(&sv.map);
     leafmap_free(&pg.map);
+}
+
+/* vdb_velocity_extrapolator.cpp:611-659 for one channel on flattened grids:
+ * the output grid (n_out leaves, values and active masks updated in place)
+ * and the fill set (fill_leaf[e]: output leaf, fill_masks[e]: voxels still to
+ * fill).  Each layer snapshots the channel's topology (valid_vel_topo) and
+ * fills every fill voxel with an active face neighbour by the mean of those
+ * neighbours, -x, +x, -y, +y, -z, +z. */
+void orc_extrapolate_channel(int n_layer, int64_t n_out, const int32_t* out_origins, float* values,
+                             uint64_t* masks, int64_t n_fill, const int32_t* fill_leaf, const uint64_t* fill_masks) {
+    if (n_out <= 0 || n_fill <= 0) return;
+    leafmap map;
+    leafmap_init(&map, n_out, out_origins);
+    uint64_t* snap = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n_out * 8);
+    uint64_t* rem = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n_fill * 8);
+    memcpy(rem, fill_masks, sizeof(uint64_t) * (size_t)n_fill * 8);
+    for (int ilayer = 0; ilayer < n_layer; ilayer++) {
+        memcpy(snap, masks, sizeof(uint64_t) * (size_t)n_out * 8);
+#pragma omp parallel for schedule(static)
+        for (int64_t e = 0; e < n_fill; ++e) {
+            const int32_t li = fill_leaf[e];
+            const int32_t* o = out_origins + 3 * li;
+            for (int off = 0; off < LSZ; ++off) {
+                if (!mbit(rem + 8 * e, off)) continue;
+                int temp_weight = 0;
+                float temp_weighted_sum_val = 0;
+                for (int d = 0; d < 6; d++) {
+                    int direction = d / 2;
+                    int positive = d % 2;
+                    int neib[3] = {o[0] + (off >> 6), o[1] + ((off >> 3) & 7), o[2] + (off & 7)};
+                    if (positive) neib[direction]++;
+                    else neib[direction]--;
+                    int32_t nl = leafmap_find(&map, neib[0], neib[1], neib[2]);
+                    if (nl >= 0 && mbit(snap + 8 * nl, voff(neib[0], neib[1], neib[2]))) {
+                        temp_weight++;
+                        temp_weighted_sum_val += values[(size_t)nl * LSZ + voff(neib[0], neib[1], neib[2])];
+                    }
+                }
+                if (temp_weight != 0) {
+                    values[(size_t)li * LSZ + off] = temp_weighted_sum_val / temp_weight;
+                    masks[8 * li + (off >> 6)] |= 1ull << (off & 63);
+                    rem[8 * e + (off >> 6)] &= ~(1ull << (off & 63));
+                }
+            }
+        }
+    }
+    free(snap);
+    free(rem);
+    leafmap_free(&map);
 }

@@ -1,7 +1,7 @@
 """The oracle's restatement of the steps either side of the pressure solve
 (projection_oracle.c) on CPU: fraction_inside over a square against closed
-forms, its symmetries, and the face-weight topology (the liquid SDF dilated
-by two voxels)."""
+forms, its symmetries, the face-weight topology (the liquid SDF dilated
+by two voxels), and the extrapolation's union topology and layers."""
 import numpy as np
 import pytest
 
@@ -57,3 +57,55 @@ def test_face_weight_topology_is_a_two_voxel_dilation():
             pts.add((org[i][0] + (off >> 6), org[i][1] + ((off >> 3) & 7), org[i][2] + (off & 7)))
     expect = {(10 + a, 11 + b, 12 + c) for a in range(-2, 3) for b in range(-2, 3) for c in range(-2, 3)}
     assert pts == expect
+
+
+def test_union_topology_is_a_face_dilation():
+    from uaamg_b200.extrapolate import topology_coords, union_topology
+    act = np.zeros((16, 16, 16), bool)
+    act[5, 6, 7] = True
+    g = dense_to_leaves(np.zeros((16, 16, 16), np.float32), active=act)
+    pts = {tuple(p) for p in topology_coords(union_topology((g, g, g), 2)).tolist()}
+    expect = {(5 + a, 6 + b, 7 + c) for a in range(-2, 3) for b in range(-2, 3) for c in range(-2, 3)
+              if abs(a) + abs(b) + abs(c) <= 2}
+    assert pts == expect and len(pts) == 25
+
+
+def test_oracle_extrapolation_of_a_single_value():
+    """One active voxel of value 3: two layers fill the face-connected diamond
+    of radius 2 with 3 (every filled voxel averages filled neighbours only)."""
+    from oracle.oracle import extrapolate_channel
+    from uaamg_b200.extrapolate import prepare_channel, union_topology
+    act = np.zeros((16, 16, 16), bool)
+    act[5, 6, 7] = True
+    dense = np.zeros((16, 16, 16), np.float32)
+    dense[5, 6, 7] = 3.0
+    g = dense_to_leaves(dense, active=act)
+    u = union_topology((g,), 2)
+    org, vals, masks, fl, fm = prepare_channel(g, u)
+    v, m = extrapolate_channel(2, org, vals, masks, fl, fm)
+    on = unpack_masks(m)
+    assert on.sum() == 25
+    assert np.all(v[on] == 3.0)
+
+
+@pytest.mark.parametrize("n_layer", [1, 2, 3, 9])
+def test_leaf_level_dilation_matches_voxel_dilation(n_layer):
+    """The leaf-mask dilation (shifts within a leaf, planes from the 6
+    neighbour leaves) against scipy's voxel dilation over a ragged random set
+    spanning many leaves and negative coordinates (9 layers cross a whole
+    leaf)."""
+    from scipy.ndimage import binary_dilation, generate_binary_structure
+    from uaamg_b200.extrapolate import topology_coords, union_topology
+    rng = np.random.default_rng(n_layer)
+    shape = (40, 33, 27)
+    dense_a = rng.random(shape) < 0.004
+    dense_b = np.zeros(shape, bool)
+    dense_b[3:9, 20:22, 5:26] = True
+    ga = dense_to_leaves(np.zeros(shape, np.float32), origin=(-16, 8, -8), active=dense_a)
+    gb = dense_to_leaves(np.zeros(shape, np.float32), origin=(-16, 8, -8), active=dense_b)
+    got = {tuple(p) for p in topology_coords(union_topology((ga, gb), n_layer)).tolist()}
+    pad = n_layer + 1
+    vol = np.pad(dense_a | dense_b, pad)
+    vol = binary_dilation(vol, structure=generate_binary_structure(3, 1), iterations=n_layer)
+    want = {(int(x) - pad - 16, int(y) - pad + 8, int(z) - pad - 8) for x, y, z in np.argwhere(vol)}
+    assert got == want

@@ -56,6 +56,8 @@ EXPORTS = [
     ("uaamg_poisson_build_rhs", i32, [vp, pLG, pLG, pLG, pLG, pLG, f32, vp]),
     ("uaamg_poisson_build_rhs_device", i32, [vp, pLG, pLG, pLG, pLG, pLG, f32, vp]),
     ("uaamg_face_weights", i32, [pLG, C.c_int64, vp, vp, vp]),
+    ("uaamg_extrapolate_channel", i32, [i32, C.c_int64, vp, vp, vp, C.c_int64, vp, vp]),
+    ("uaamg_extrapolate_channel_device", i32, [i32, C.c_int64, vp, vp, vp, C.c_int64, vp, vp, vp]),
     ("uaamg_face_weights_device", i32, [pLG, C.c_int64, vp, vp, vp, vp]),
     ("uaamg_poisson_apply_pressure_gradient", i32, [vp, pLG, pLG, pLG, vp, f32, f32, i32, pLG, vp, vp, vp, vp]),
     ("uaamg_poisson_apply_pressure_gradient_device", i32,

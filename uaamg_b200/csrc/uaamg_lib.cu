@@ -4,3 +4,4 @@
 #include "mixed.cu"
 #include "viscosity.cu"
 #include "projection.cu"
+#include "extrapolate.cu"
