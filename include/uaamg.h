@@ -236,6 +236,29 @@ int uaamg_poisson_profile_pcg_mixed(uaamg_poisson* h, int precision, float* d_pr
 /* ======================================================================== */
 /* The steps either side of the pressure solve in a FLIP projection.        */
 
+/* The liquid SDF adjusted inside solids before the pressure solve:
+ * FLIP_Solver_OpenVDB::immerse_liquid_phi_in_solids (FLIP_vdb/FLIP_vdb.cpp:
+ * 2856-2942), its value passes, on the liquid SDF's own leaves.  In leaves
+ * where the solid SDF has a leaf at the same origin (probeConstLeaf), with the
+ * solid SDF sampled trilinearly (BoxSampler) at voxel centres:
+ *   1. active voxels inside the solid: phi -= dx / 2 (:2860-2877);
+ *   2. voxels active after one 26-neighbour dilation, inside the solid: the
+ *      least of 3 dx and the pass-1 values of the face neighbours visited in
+ *      the order +x, -x, +y, -y, +z, -z up to the first negative one, if there
+ *      is one; else a negative value becomes max(background, -solid)
+ *      (:2883-2938).
+ * values_out: float[leaf_count][512] (may alias the liquid's device values in
+ * the _device form).  The two topology dilations of the reference (:2881, 26
+ * neighbours; :2941, 6 neighbours) are the caller's: leaves they add keep the
+ * background value, as in the reference, whose second pass only visits the
+ * leaves that existed before the first dilation.  The _device form takes the
+ * liquid's values in device memory (values_on_device) or host memory, writes
+ * device memory on `stream` and returns without waiting. */
+int uaamg_immerse_liquid_phi(const uaamg_leaf_grid* solid_sdf, const uaamg_leaf_grid* liquid_phi, float dx,
+                             float* values_out);
+int uaamg_immerse_liquid_phi_device(const uaamg_leaf_grid* solid_sdf, const uaamg_leaf_grid* liquid_phi, float dx,
+                                    float* d_values_out, void* stream);
+
 /* Solid face weights on a given topology: for every active voxel (masks may
  * be NULL: all voxels), 1 - fraction_inside of the solid over each of its
  * three minus faces, from the solid SDF at the 8 voxel corners, clamped to

@@ -108,6 +108,8 @@ def lib():
                                             C.c_float, C.c_float, C.c_float, C.c_int,
                                             C.c_int64, i32p, vp, f32p, f32p, u64p, f32p, f32p]
         L.orc_extrapolate_channel.argtypes = [C.c_int, C.c_int64, i32p, f32p, u64p, C.c_int64, i32p, u64p]
+        L.orc_immerse_liquid_phi.argtypes = [C.c_int64, i32p, f32p, C.c_float, C.c_int64, i32p, vp, f32p,
+                                             C.c_float, C.c_float, f32p]
         _LIB = L
     return _LIB
 
@@ -428,3 +430,17 @@ def extrapolate_channel(n_layer, out_origins, values, masks, fill_leaf, fill_mas
     n_out = org.size // 3
     lib().orc_extrapolate_channel(int(n_layer), n_out, org, v, m, fl.size, fl, fm)
     return v.reshape(n_out, 512), m.reshape(n_out, 8)
+
+
+def immerse_liquid_phi(liquid_phi, solid_sdf, dx):
+    """immerse_liquid_phi_in_solids' value passes (FLIP_vdb.cpp:2856-2938) on
+    the liquid SDF's own leaves: float32 [leaf][512]."""
+    n = liquid_phi.leaf_count
+    out = np.zeros((n, 512), np.float32)
+    m = None if liquid_phi.masks is None else np.ascontiguousarray(liquid_phi.masks, dtype=np.uint64)
+    lib().orc_immerse_liquid_phi(*_grid_args(solid_sdf), float(solid_sdf.background.reshape(-1)[0]), n,
+                                 np.ascontiguousarray(liquid_phi.origins, dtype=np.int32).reshape(-1),
+                                 None if m is None else m.ctypes.data,
+                                 np.ascontiguousarray(liquid_phi.values.reshape(-1), dtype=np.float32),
+                                 float(liquid_phi.background.reshape(-1)[0]), float(dx), out.reshape(-1))
+    return out

@@ -5,6 +5,7 @@
  */
 #ifndef UAAMG_ORACLE_COMMON_H
 #define UAAMG_ORACLE_COMMON_H
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -78,6 +79,27 @@ static inline float ogrid_get(const ogrid* g, int x, int y, int z, int c) {
     int32_t li = leafmap_find(&g->map, x, y, z);
     if (li < 0) return g->bg[c];
     return g->val[((int64_t)li * LSZ + voff(x, y, z)) * g->comps + c];
+}
+
+/* OpenVDB BoxSampler::sample over a getValue accessor (tools/Interpolation.h):
+ * floor, fractional weights in double, three levels of
+ *   a + float((double)(b - a) * w). */
+static inline float vdb_lerp(float a, float b, double w) {
+    float d = b - a;
+    double t = (double)d * w;
+    return a + (float)t;
+}
+static inline float box_sample(const ogrid* g, double px, double py, double pz) {
+    double fx = floor(px), fy = floor(py), fz = floor(pz);
+    int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+    double u = px - fx, v = py - fy, w = pz - fz;
+    float d[2][2][2];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j)
+            for (int k = 0; k < 2; ++k) d[i][j][k] = ogrid_get(g, ix + i, iy + j, iz + k, 0);
+    float a0 = vdb_lerp(vdb_lerp(d[0][0][0], d[0][0][1], w), vdb_lerp(d[0][1][0], d[0][1][1], w), v);
+    float a1 = vdb_lerp(vdb_lerp(d[1][0][0], d[1][0][1], w), vdb_lerp(d[1][1][0], d[1][1][1], w), v);
+    return vdb_lerp(a0, a1, u);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -9,6 +9,8 @@
  *  - FLIP_Solver_OpenVDB::apply_pressure_gradient: FLIP_vdb/FLIP_vdb.cpp:2571-2667
  *  - vdb_velocity_extrapolator::union_extrapolate, the layers after its
  *    topology steps: FLIP_vdb/vdb_velocity_extrapolator.cpp:611-659
+ *  - FLIP_Solver_OpenVDB::immerse_liquid_phi_in_solids, its value passes:
+ *    FLIP_vdb/FLIP_vdb.cpp:2856-2938
  *
  * Compiled with -ffp-contract=off: every float operation is the reference's,
  * in its order, unfused.  Grids are flattened leaf grids (OpenVDB leaf
@@ -250,4 +252,81 @@ void orc_extrapolate_channel(int n_layer, int64_t n_out, const int32_t* out_orig
     free(snap);
     free(rem);
     leafmap_free(&map);
+}
+
+/* FLIP_Solver_OpenVDB::immerse_liquid_phi_in_solids, the value passes
+ * (FLIP_vdb.cpp:2856-2938) over the liquid SDF's leaves as they were before
+ * the 26-neighbour dilation (the reference's LeafManager is built at :2876,
+ * before the dilation at :2881, and reused at :2938).  A leaf is processed
+ * when the solid SDF has a leaf at its origin (probeConstLeaf).
+ *   pass 1 (:2860-2877): active voxels whose solid SDF sampled at the voxel
+ *     centre is negative get phi - 0.5 dx; the result is the reference copy;
+ *   pass 2 (:2883-2938): voxels active after the dilation (the voxel or one
+ *     of its 26 neighbours active) with a negative solid sample take the least
+ *     of 3 dx and the reference values of the face neighbours visited in the
+ *     order +x, -x, +y, -y, +z, -z up to the first negative one, if there is
+ *     one; else a negative value becomes max(background, -solid).
+ * values_out [n][512]: the liquid values after both passes. */
+void orc_immerse_liquid_phi(int64_t solid_n, const int32_t* solid_origins, const float* solid_values, float solid_bg,
+                            int64_t n, const int32_t* origins, const uint64_t* masks, const float* values,
+                            float liquid_bg, float dx, float* values_out) {
+    ogrid solid;
+    const float sbg[3] = {solid_bg, 0.f, 0.f};
+    ogrid_init(&solid, solid_n, solid_origins, NULL, solid_values, 1, sbg);
+    float* ref = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1) * LSZ);
+    memcpy(ref, values, sizeof(float) * (size_t)n * LSZ);
+    const float half_dx = 0.5f * dx, three_dx = dx * 3.0f;
+#pragma omp parallel for schedule(static)
+    for (int64_t li = 0; li < n; ++li) {
+        const int32_t* o = origins + 3 * li;
+        if (leafmap_find(&solid.map, o[0], o[1], o[2]) < 0) continue;
+        for (int off = 0; off < LSZ; ++off) {
+            if (masks && !mbit(masks + 8 * li, off)) continue;
+            float s = box_sample(&solid, o[0] + (off >> 6) + 0.5, o[1] + ((off >> 3) & 7) + 0.5, o[2] + (off & 7) + 0.5);
+            if (s < 0) ref[li * LSZ + off] = values[li * LSZ + off] - half_dx;
+        }
+    }
+    ogrid refg;
+    const float lbg[3] = {liquid_bg, 0.f, 0.f};
+    ogrid_init(&refg, n, origins, masks, ref, 1, lbg);
+    memcpy(values_out, ref, sizeof(float) * (size_t)n * LSZ);
+#pragma omp parallel for schedule(static)
+    for (int64_t li = 0; li < n; ++li) {
+        const int32_t* o = origins + 3 * li;
+        if (leafmap_find(&solid.map, o[0], o[1], o[2]) < 0) continue;
+        for (int off = 0; off < LSZ; ++off) {
+            const int g[3] = {o[0] + (off >> 6), o[1] + ((off >> 3) & 7), o[2] + (off & 7)};
+            int on = 0; /* active after one NN_FACE_EDGE_VERTEX dilation */
+            for (int a = -1; a <= 1 && !on; ++a)
+                for (int b = -1; b <= 1 && !on; ++b)
+                    for (int c = -1; c <= 1 && !on; ++c) {
+                        const int x = g[0] + a, y = g[1] + b, z = g[2] + c;
+                        const int32_t nl = leafmap_find(&refg.map, x, y, z);
+                        if (nl >= 0 && (!masks || mbit(masks + 8 * nl, voff(x, y, z)))) on = 1;
+                    }
+            if (!on) continue;
+            float s = box_sample(&solid, g[0] + 0.5, g[1] + 0.5, g[2] + 0.5);
+            if (!(s < 0)) continue;
+            int found = 0;
+            float min_fluid = three_dx;
+            for (int i = 0; i < 6 && !found; i++) {
+                int comp = i / 2, positive = (i % 2 == 0);
+                int t[3] = {g[0], g[1], g[2]};
+                t[comp] += positive ? 1 : -1;
+                float r = ogrid_get(&refg, t[0], t[1], t[2], 0);
+                min_fluid = (r < min_fluid) ? r : min_fluid; /* std::min */
+                found |= (r < 0);
+            }
+            float* v = values_out + li * LSZ + off;
+            if (found) {
+                *v = min_fluid;
+            } else if (*v < 0) {
+                float ns = -s;
+                *v = (liquid_bg < ns) ? ns : liquid_bg; /* std::max(background, -solid) */
+            }
+        }
+    }
+    leafmap_free(&refg.map);
+    leafmap_free(&solid.map);
+    free(ref);
 }

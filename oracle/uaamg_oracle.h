@@ -192,6 +192,9 @@ void orc_pressure_gradient(int64_t phi_n, const int32_t* phi_origins, const floa
                            float in_dt, float dx, float friction, int channel,
                            int64_t v_n, const int32_t* v_origins, const uint64_t* v_masks, const float* v_values,
                            float* v_out, uint64_t* mask_out, float* update_out, float* reflected_out);
+void orc_immerse_liquid_phi(int64_t solid_n, const int32_t* solid_origins, const float* solid_values, float solid_bg,
+                            int64_t n, const int32_t* origins, const uint64_t* masks, const float* values,
+                            float liquid_bg, float dx, float* values_out);
 void orc_extrapolate_channel(int n_layer, int64_t n_out, const int32_t* out_origins, float* values,
                              uint64_t* masks, int64_t n_fill, const int32_t* fill_leaf, const uint64_t* fill_masks);
 

@@ -9,7 +9,7 @@ import pytest
 from oracle import oracle as orc
 from oracle.oracle import OraclePoisson
 from uaamg_b200 import scenes
-from uaamg_b200.grids import LeafGrid, dense_to_leaves, unpack_masks
+from uaamg_b200.grids import LeafGrid, dense_to_leaves, pack_masks, unpack_masks
 
 pytestmark = pytest.mark.gpu
 
@@ -117,3 +117,73 @@ def test_pressure_gradient_device_path_matches_host(setup, gpu):
     assert np.array_equal(d_mask.cpu().numpy().view(np.uint64).reshape(n, 8), host[1])
     assert np.array_equal(d_upd.cpu().numpy(), host[2])
     assert np.array_equal(d_refl.cpu().numpy(), host[3])
+
+
+@pytest.fixture(scope="module")
+def immersion_case(gpu):
+    """The walled box with a sphere obstacle around the liquid of the plain
+    scene, and a copy of the solid without its leaves at x >= n/2 (the pass
+    gate: no solid leaf, no change, although samples there read the solid's
+    negative background)."""
+    sc = scenes.plain_poisson_scene(n=48, seed=3)
+    solid = solid_box_with_obstacle(sc.n, sc.dx)
+    keep = solid.origins[:, 0] < sc.n // 2
+    half = LeafGrid(origins=solid.origins[keep], values=solid.values[keep], background=solid.background,
+                    masks=solid.masks[keep])
+    # isolated liquid voxels (1 %) in the air: negative values with no negative face neighbour
+    v = sc.phi.values.copy()
+    drop = (np.random.default_rng(12).random(v.shape) < 0.01) & (v > sc.dx)
+    v[drop] = -0.25 * sc.dx
+    # a narrow band, as a level set's active voxels: inactive voxels next to the band are visited after the
+    # 26-neighbour dilation
+    sc.phi = LeafGrid(origins=sc.phi.origins, values=v, background=sc.phi.background,
+                      masks=pack_masks(np.abs(v) < 4 * sc.dx))
+    return sc, solid, half
+
+
+@pytest.mark.parametrize("which", ["full", "half"])
+def test_immersion_bit_exact(immersion_case, which):
+    from uaamg_b200.projection import immerse_liquid_phi_values
+    sc, solid, half = immersion_case
+    s = solid if which == "full" else half
+    g = immerse_liquid_phi_values(sc.phi, s, sc.dx)
+    o = orc.immerse_liquid_phi(sc.phi, s, sc.dx)
+    assert np.array_equal(g, o)
+    before = sc.phi.values
+    changed = g != before
+    assert changed.any()
+    # every branch of the second pass is taken somewhere: a value moved to a negative neighbour's, a value
+    # clamped to max(background, -solid), and pass 1's shift kept
+    assert np.any(changed & (g < 0) & (before >= 0))
+    assert np.any(changed & (g > 0) & (before < 0))
+    assert np.any(changed & ~unpack_masks(sc.phi.masks))  # reached through the 26-neighbour dilation
+    if which == "half":
+        right = sc.phi.origins[:, 0] >= sc.n // 2
+        assert np.array_equal(g[right], before[right])
+
+
+def test_immersion_topology_and_device_path(immersion_case, gpu):
+    import ctypes as C
+    from uaamg_b200 import _lib
+    from uaamg_b200.poisson import _as_c
+    from uaamg_b200.projection import immerse_liquid_phi_in_solids, immerse_liquid_phi_values
+    from uaamg_b200.topology import dilate, topology_coords
+    torch = gpu
+    sc, solid, half = immersion_case
+    out = immerse_liquid_phi_in_solids(sc.phi, solid, sc.dx)
+    n = sc.phi.leaf_count
+    host = immerse_liquid_phi_values(sc.phi, solid, sc.dx)
+    assert np.array_equal(out.values[:n], host)
+    assert np.all(out.values[n:] == sc.phi.background[0])
+    want = {tuple(p) for p in topology_coords(dilate(dilate(sc.phi, 1, 26), 1, 6)).tolist()}
+    assert {tuple(p) for p in topology_coords(out).tolist()} == want
+    # device form, in place over the liquid's device values
+    keep = []
+    d = LeafGrid(origins=sc.phi.origins, values=sc.phi.values, background=sc.phi.background, masks=sc.phi.masks)
+    d.values = torch.from_numpy(sc.phi.values.copy()).cuda()
+    gs, gl = _as_c(solid, keep), _as_c(d, keep)
+    torch.cuda.synchronize()
+    rc = _lib.lib().uaamg_immerse_liquid_phi_device(C.byref(gs), C.byref(gl), float(sc.dx), d.values.data_ptr(), None)
+    _lib.check(rc, "immerse_liquid_phi_device")
+    torch.cuda.synchronize()
+    assert np.array_equal(d.values.cpu().numpy(), host)

@@ -109,3 +109,50 @@ def test_leaf_level_dilation_matches_voxel_dilation(n_layer):
     vol = binary_dilation(vol, structure=generate_binary_structure(3, 1), iterations=n_layer)
     want = {(int(x) - pad - 16, int(y) - pad + 8, int(z) - pad - 8) for x, y, z in np.argwhere(vol)}
     assert got == want
+
+
+@pytest.mark.parametrize("n_layer", [1, 2, 9])
+def test_leaf_level_box_dilation_matches_voxel_dilation(n_layer):
+    """The 26-neighbour dilation (z, y, x 1-D passes at leaf level) against
+    scipy's voxel dilation with a full 3x3x3 structure."""
+    from scipy.ndimage import binary_dilation
+    from uaamg_b200.topology import dilate, topology_coords
+    rng = np.random.default_rng(10 + n_layer)
+    shape = (35, 41, 30)
+    dense = rng.random(shape) < 0.003
+    dense[30:33, 2:4, 20:29] = True
+    g = dense_to_leaves(np.zeros(shape, np.float32), origin=(8, -24, -16), active=dense)
+    got = {tuple(p) for p in topology_coords(dilate(g, n_layer, neighbours=26)).tolist()}
+    pad = n_layer + 1
+    vol = binary_dilation(np.pad(dense, pad), structure=np.ones((3, 3, 3), bool), iterations=n_layer)
+    want = {(int(x) - pad + 8, int(y) - pad - 24, int(z) - pad - 16) for x, y, z in np.argwhere(vol)}
+    assert got == want
+
+
+def test_oracle_immersion_known_answers():
+    """immerse_liquid_phi_in_solids' value passes on a hand-made case: solid
+    everywhere (SDF -1), dx 0.5, liquid background 1.5; leaf 0 (with a solid
+    leaf) has phi 1 except -1 at (3,3,3) and is active for x < 4; leaf 1 at
+    (8,0,0) has no solid leaf and is left alone."""
+    from oracle.oracle import immerse_liquid_phi
+    solid = dense_to_leaves(np.full((8, 8, 8), -1.0, np.float32), background=-1.0)
+    phi = np.ones((16, 8, 8), np.float32)
+    phi[3, 3, 3] = -1.0
+    act = np.zeros((16, 8, 8), bool)
+    act[:4] = True
+    act[8:] = True
+    liq = dense_to_leaves(phi, background=1.5, active=act)
+    assert liq.leaf_count == 2
+    out = immerse_liquid_phi(liq, solid, 0.5)
+
+    def at(x, y, z):
+        return out[x >> 3, ((x & 7) << 6) | (y << 3) | z]
+
+    assert at(3, 3, 3) == 1.5     # no negative neighbour: max(background, -solid) = max(1.5, 1)
+    assert at(4, 3, 3) == -1.25   # inactive, next to an active voxel: its -x neighbour (corrected)
+    assert at(2, 3, 3) == -1.25   # +x neighbour first
+    assert at(3, 3, 2) == -1.25   # +z neighbour, after four positive ones
+    assert at(1, 1, 1) == 0.75    # pass 1 only: 1 - dx/2
+    assert at(4, 0, 0) == 1.0     # processed in pass 2, no negative neighbour, positive: unchanged
+    assert at(6, 6, 6) == 1.0     # not active after the dilation
+    assert np.all(out[1] == 1.0)  # no solid leaf at (8,0,0)

@@ -56,6 +56,8 @@ EXPORTS = [
     ("uaamg_poisson_build_rhs", i32, [vp, pLG, pLG, pLG, pLG, pLG, f32, vp]),
     ("uaamg_poisson_build_rhs_device", i32, [vp, pLG, pLG, pLG, pLG, pLG, f32, vp]),
     ("uaamg_face_weights", i32, [pLG, C.c_int64, vp, vp, vp]),
+    ("uaamg_immerse_liquid_phi", i32, [pLG, pLG, C.c_float, vp]),
+    ("uaamg_immerse_liquid_phi_device", i32, [pLG, pLG, C.c_float, vp, vp]),
     ("uaamg_extrapolate_channel", i32, [i32, C.c_int64, vp, vp, vp, C.c_int64, vp, vp]),
     ("uaamg_extrapolate_channel_device", i32, [i32, C.c_int64, vp, vp, vp, C.c_int64, vp, vp, vp]),
     ("uaamg_face_weights_device", i32, [pLG, C.c_int64, vp, vp, vp, vp]),

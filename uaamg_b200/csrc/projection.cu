@@ -2,7 +2,9 @@
 // projection, on the device: the solid face weights the solver reads
 // (FLIP_Solver_OpenVDB::calculate_face_weights, FLIP_vdb/FLIP_vdb.cpp:2669-2752)
 // and the pressure-gradient velocity update that consumes its solution
-// (FLIP_Solver_OpenVDB::apply_pressure_gradient, FLIP_vdb.cpp:2571-2667).
+// (FLIP_Solver_OpenVDB::apply_pressure_gradient, FLIP_vdb.cpp:2571-2667), and
+// the ghost-fluid adjustment of the liquid SDF inside solids between them
+// (FLIP_Solver_OpenVDB::immerse_liquid_phi_in_solids, FLIP_vdb.cpp:2856-2942).
 // Included by uaamg_lib.cu after poisson.cu (grids, handle, errors).
 
 namespace uaamg {
@@ -311,6 +313,141 @@ static void pressure_gradient_impl(uaamg_poisson* h, const uaamg_leaf_grid* phi,
     for (void* p : tofree) CK(cudaFreeAsync(p, s));
 }
 
+// immerse_liquid_phi_in_solids (FLIP_vdb/FLIP_vdb.cpp:2856-2942), the value
+// passes, over the liquid SDF's leaves as they were before its 26-neighbour
+// dilation (the reference's LeafManager is built at :2876, before the dilation
+// at :2881, and reused at :2938).  A leaf takes part when the solid SDF has a
+// leaf at its origin (probeConstLeaf).  The solid SDF is sampled at voxel
+// centres with BoxSampler.  Pass 1 (:2860-2877): active voxels inside the
+// solid get phi - dx/2; the result is the reference copy `ref` of both passes.
+__global__ void __launch_bounds__(128) k_immerse_correct(DGrid solid, DGrid liq, const int* org,
+                                                         const uint64_t* mask, int nl, float half_dx, float* ref) {
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    if (leaf >= nl) return;
+    const int ox = org[3 * leaf], oy = org[3 * leaf + 1], oz = org[3 * leaf + 2];
+    const bool gated = solid.leaf_of(ox, oy, oz) >= 0;
+    const float* vin = liq.val + (long long)leaf * UAAMG_LEAF;
+    float* r = ref + (long long)leaf * UAAMG_LEAF;
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j) {
+        const int off = t + 128 * j;
+        float v = vin[off];
+        if (gated && (!mask || ((mask[(long long)leaf * 8 + (off >> 6)] >> (off & 63)) & 1ull))) {
+            const float sv = box_sample(solid, (double)(ox + (off >> 6)) + 0.5, (double)(oy + ((off >> 3) & 7)) + 0.5,
+                                        (double)(oz + (off & 7)) + 0.5);
+            if (sv < 0.f) v = __fsub_rn(v, half_dx);
+        }
+        r[off] = v;
+    }
+}
+
+// Pass 2 (:2883-2938): every voxel active after the dilation (itself or one of
+// its 26 neighbours active in `mask`) whose solid sample is negative takes the
+// least of 3 dx and the reference values of its face neighbours, visited in
+// the order +x, -x, +y, -y, +z, -z up to the first negative one, if there is
+// one (std::min: a NaN neighbour is skipped); else a negative value becomes
+// std::max(background, -solid).  Other voxels keep the reference value.
+// refg: the liquid's leaf map over `ref`, background = the liquid's.
+__global__ void __launch_bounds__(128) k_immerse_solid(DGrid solid, DGrid refg, const int* org, const uint64_t* mask,
+                                                       int nl, float three_dx, float* out) {
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    if (leaf >= nl) return;
+    const int ox = org[3 * leaf], oy = org[3 * leaf + 1], oz = org[3 * leaf + 2];
+    const bool gated = solid.leaf_of(ox, oy, oz) >= 0;
+    const float* r = refg.val + (long long)leaf * UAAMG_LEAF;
+    float* o = out + (long long)leaf * UAAMG_LEAF;
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j) {
+        const int off = t + 128 * j;
+        float v = r[off];
+        if (gated) {
+            const int gx = ox + (off >> 6), gy = oy + ((off >> 3) & 7), gz = oz + (off & 7);
+            bool on = false;
+#pragma unroll 1
+            for (int a = -1; a <= 1 && !on; ++a)
+#pragma unroll 1
+                for (int b = -1; b <= 1 && !on; ++b)
+#pragma unroll 1
+                    for (int c = -1; c <= 1 && !on; ++c) {
+                        const int x = gx + a, y = gy + b, z = gz + c;
+                        const int q = refg.leaf_of(x, y, z);
+                        if (q >= 0) {
+                            const int qo = voff3(x, y, z);
+                            on = !mask || ((mask[(long long)q * 8 + (qo >> 6)] >> (qo & 63)) & 1ull);
+                        }
+                    }
+            if (on) {
+                const float sv = box_sample(solid, (double)gx + 0.5, (double)gy + 0.5, (double)gz + 0.5);
+                if (sv < 0.f) {
+                    bool found = false;
+                    float mn = three_dx;
+#pragma unroll 1
+                    for (int i = 0; i < 6 && !found; ++i) {
+                        const int sx = (i == 0) - (i == 1), sy = (i == 2) - (i == 3), sz = (i == 4) - (i == 5);
+                        const float rv = refg.get(gx + sx, gy + sy, gz + sz, 0);
+                        mn = (rv < mn) ? rv : mn;
+                        found = found || (rv < 0.f);
+                    }
+                    if (found) {
+                        v = mn;
+                    } else if (v < 0.f) {
+                        const float ns = -sv;
+                        v = (refg.bg0 < ns) ? ns : refg.bg0;
+                    }
+                }
+            }
+        }
+        o[off] = v;
+    }
+}
+
+static void immerse_impl(const uaamg_leaf_grid* solid, const uaamg_leaf_grid* liquid, float dx, float* d_out,
+                         cudaStream_t s) {
+    check_grid(solid, 1, "solid_sdf");
+    check_grid(liquid, 1, "liquid_phi");
+    require(std::isfinite(dx) && dx > 0.f, "dx must be positive");
+    const int64_t n = liquid->leaf_count;
+    if (n == 0) return;
+    require(d_out != nullptr, "NULL output");
+    cudaError_t ce = cudaSuccess;
+    DeviceCtx* ctx = device_ctx(&ce);
+    CK(ce);
+    std::vector<void*> tofree;
+    try {
+        HostMap ms, ml;
+        DevGrid gs, gl;
+        upload_grid_cs(ctx, s, solid, gs, ms, tofree);
+        upload_grid_cs(ctx, s, liquid, gl, ml, tofree);
+        for (int64_t i = 0; i < n; ++i)
+            if (ml.idx[ml.cell(liquid->origins[3 * i] >> 3, liquid->origins[3 * i + 1] >> 3,
+                               liquid->origins[3 * i + 2] >> 3)] != (int32_t)i) {
+                set_error("liquid_phi: duplicate leaf origin");
+                throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT};
+            }
+        const size_t vn = (size_t)n;
+        void* mem = nullptr;
+        CK(ctx_dev_alloc(ctx, &mem, carve_size(vn * 3, 4) + (liquid->masks ? carve_size(vn * 8, 8) : 0) +
+                                        carve_size(vn * UAAMG_LEAF, 4), s));
+        tofree.push_back(mem);
+        char* cur = (char*)mem;
+        int* dorg = carve<int>(cur, vn * 3);
+        uint64_t* dmask = liquid->masks ? carve<uint64_t>(cur, vn * 8) : nullptr;
+        float* ref = carve<float>(cur, vn * UAAMG_LEAF);
+        CK(cudaMemcpyAsync(dorg, liquid->origins, vn * 12, cudaMemcpyHostToDevice, s));
+        if (dmask) CK(cudaMemcpyAsync(dmask, liquid->masks, vn * 64, cudaMemcpyHostToDevice, s));
+        k_immerse_correct<<<(unsigned)n, 128, 0, s>>>(gs.g, gl.g, dorg, dmask, (int)n, 0.5f * dx, ref);
+        CHECK_LAUNCH();
+        DGrid refg = gl.g;
+        refg.val = ref;
+        k_immerse_solid<<<(unsigned)n, 128, 0, s>>>(gs.g, refg, dorg, dmask, (int)n, dx * 3.0f, d_out);
+        CHECK_LAUNCH();
+    } catch (...) {
+        for (void* p : tofree) cudaFreeAsync(p, s);
+        throw;
+    }
+    for (void* p : tofree) CK(cudaFreeAsync(p, s));
+}
+
 }  // namespace
 
 extern "C" {
@@ -401,6 +538,50 @@ int uaamg_poisson_apply_pressure_gradient_device(uaamg_poisson* h, const uaamg_l
     require(h && velocity, "NULL argument");
     pressure_gradient_impl(h, liquid_phi, face_weights, solid_velocity, d_pressure, channel, velocity, d_velocity,
                            d_mask_out, d_update_out, d_reflected_out, dt, friction);
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_immerse_liquid_phi(const uaamg_leaf_grid* solid_sdf, const uaamg_leaf_grid* liquid_phi, float dx,
+                             float* values_out) {
+    ABI_BEGIN
+    require(liquid_phi != nullptr, "liquid_phi is NULL");
+    const int64_t n = liquid_phi->leaf_count;
+    if (n <= 0) {
+        check_grid(solid_sdf, 1, "solid_sdf");
+        return UAAMG_SUCCESS;
+    }
+    require(values_out != nullptr, "NULL output");
+    cudaError_t ce = cudaSuccess;
+    DeviceCtx* ctx = device_ctx(&ce);
+    CK(ce);
+    cudaStream_t s = nullptr;
+    CK(ctx_stream_acquire(ctx, &s));
+    float* d = nullptr;
+    const size_t bytes = (size_t)n * UAAMG_LEAF * sizeof(float);
+    try {
+        CK(ctx_dev_alloc(ctx, (void**)&d, bytes, s));
+        immerse_impl(solid_sdf, liquid_phi, dx, d, s);
+        CK(cudaMemcpyAsync(values_out, d, bytes, cudaMemcpyDeviceToHost, s));
+        CK(cudaFreeAsync(d, s));
+        d = nullptr;
+        CK(cudaStreamSynchronize(s));
+    } catch (...) {
+        if (d) cudaFreeAsync(d, s);
+        cudaStreamSynchronize(s);
+        ctx_stream_release(ctx, s);
+        throw;
+    }
+    ctx_stream_release(ctx, s);
+    return UAAMG_SUCCESS;
+    ABI_END
+}
+
+int uaamg_immerse_liquid_phi_device(const uaamg_leaf_grid* solid_sdf, const uaamg_leaf_grid* liquid_phi, float dx,
+                                    float* d_values_out, void* stream) {
+    ABI_BEGIN
+    require(liquid_phi != nullptr, "liquid_phi is NULL");
+    immerse_impl(solid_sdf, liquid_phi, dx, d_values_out, (cudaStream_t)stream);
     return UAAMG_SUCCESS;
     ABI_END
 }

@@ -9,6 +9,9 @@ apply_pressure_gradient, FLIP_vdb.cpp:2571-2667).  Both run through the C ABI
 ``face_weight_topology`` computes, on the host, the output topology the
 reference gives the face weights: the liquid SDF's active voxels dilated by
 two voxels over the 26-neighbourhood (FLIP_vdb.cpp:2672-2675).
+``immerse_liquid_phi_in_solids`` adjusts the liquid SDF inside solids between
+the two (FLIP_Solver_OpenVDB::immerse_liquid_phi_in_solids,
+FLIP_vdb.cpp:2856-2942; ``uaamg_immerse_liquid_phi``).
 """
 from __future__ import annotations
 
@@ -17,8 +20,9 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from .grids import LeafGrid, offsets_xyz, pack_masks, unpack_masks
+from .grids import LeafGrid
 from .poisson import LaplacianWithLevel, _as_c
+from .topology import dilate
 
 # the FLIP solver's default boundary_friction_coefficient (FLIP_vdb.cpp:1886)
 DEFAULT_FRICTION = 0.0
@@ -28,30 +32,7 @@ def face_weight_topology(liquid_phi: LeafGrid, layers: int = 2) -> tuple[np.ndar
     """Leaves (origins [n, 3]) and active masks ([n, 8]) of the liquid SDF's
     active voxels dilated ``layers`` times over the 26-neighbourhood
     (openvdb::tools::dilateActiveValues with NN_FACE_EDGE_VERTEX)."""
-    from scipy.ndimage import binary_dilation
-
-    org = np.asarray(liquid_phi.origins, dtype=np.int64)
-    if org.shape[0] == 0:
-        return np.zeros((0, 3), np.int32), np.zeros((0, 8), np.uint64)
-    pad = 8 * (1 + (layers + 7) // 8)
-    lo = org.min(axis=0) - pad
-    hi = org.max(axis=0) + 8 + pad
-    shape = tuple(int(v) for v in (hi - lo))
-    act = np.zeros(shape, dtype=bool)
-    xyz = offsets_xyz()
-    on = unpack_masks(liquid_phi.masks)
-    for i in range(org.shape[0]):
-        g = org[i][None, :] + xyz - lo[None, :]
-        a = on[i]
-        act[g[a, 0], g[a, 1], g[a, 2]] = True
-    if layers > 0:
-        act = binary_dilation(act, structure=np.ones((3, 3, 3), dtype=bool), iterations=layers)
-    nx, ny, nz = (s // 8 for s in shape)
-    blk = act.reshape(nx, 8, ny, 8, nz, 8).transpose(0, 2, 4, 1, 3, 5).reshape(-1, 512)
-    keep = blk.any(axis=1)
-    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
-    origins = (np.stack([ii.ravel(), jj.ravel(), kk.ravel()], axis=1) * 8 + lo[None, :])[keep]
-    return origins.astype(np.int32), pack_masks(blk[keep])
+    return dilate(liquid_phi, layers, neighbours=26)
 
 
 def calculate_face_weights(solid_sdf: LeafGrid, origins: np.ndarray, masks: np.ndarray | None = None) -> np.ndarray:
@@ -76,6 +57,40 @@ def face_weights_grid(solid_sdf: LeafGrid, liquid_phi: LeafGrid) -> LeafGrid:
     origins, masks = face_weight_topology(liquid_phi)
     w = calculate_face_weights(solid_sdf, origins, masks)
     return LeafGrid(origins=origins, values=w, background=np.ones(3, np.float32), masks=masks)
+
+
+def immerse_liquid_phi_values(liquid_phi: LeafGrid, solid_sdf: LeafGrid, dx: float) -> np.ndarray:
+    """The value passes of immerse_liquid_phi_in_solids (FLIP_vdb.cpp:
+    2856-2938) on the liquid SDF's own leaves, on the GPU: float32 [n, 512]."""
+    keep: list = []
+    n = liquid_phi.leaf_count
+    out = np.empty((n, 512), np.float32)
+    gs, gl = _as_c(solid_sdf, keep), _as_c(liquid_phi, keep)
+    rc = _lib.lib().uaamg_immerse_liquid_phi(C.byref(gs), C.byref(gl), float(dx), out.ctypes.data if n else None)
+    _lib.check(rc, "immerse_liquid_phi")
+    return out
+
+
+def immerse_liquid_phi_in_solids(liquid_phi: LeafGrid, solid_sdf: LeafGrid, dx: float) -> LeafGrid:
+    """FLIP_Solver_OpenVDB::immerse_liquid_phi_in_solids (FLIP_vdb.cpp:
+    2856-2942): the liquid SDF with its values adjusted inside solids (GPU)
+    and its topology dilated once over the 26-neighbourhood (:2881) and once
+    over the 6 face neighbours (:2941).  The liquid's leaves come first, then
+    the leaves the dilations add (background values, as OpenVDB creates them);
+    returns a new grid."""
+    from .topology import LeafIndex
+    vals = immerse_liquid_phi_values(liquid_phi, solid_sdf, dx)
+    org, masks = dilate(dilate(liquid_phi, 1, neighbours=26), 1, neighbours=6)
+    j = LeafIndex(liquid_phi.origins).find(org)
+    n = liquid_phi.leaf_count
+    out_masks = np.zeros((n, 8), np.uint64)
+    out_masks[j[j >= 0]] = masks[j >= 0]
+    new = j < 0
+    bg = float(liquid_phi.background.reshape(-1)[0])
+    return LeafGrid(origins=np.concatenate([liquid_phi.origins.astype(np.int32), org[new]], axis=0),
+                    values=np.concatenate([vals, np.full((int(new.sum()), 512), bg, np.float32)], axis=0),
+                    background=liquid_phi.background.copy(),
+                    masks=np.concatenate([out_masks, masks[new]], axis=0))
 
 
 def apply_pressure_gradient(lap: LaplacianWithLevel, liquid_phi: LeafGrid, face_weights: LeafGrid,
