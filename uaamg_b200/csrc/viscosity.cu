@@ -381,22 +381,18 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
     int* a2org = vupload(h, a2.data(), a2.size());
     int* a1forg = vupload(h, a1f.data(), a1f.size());
     const float sub_bg = 1.5f * dx;
-    float* sdf = (float*)valloc(h, (size_t)8 * n1 * UAAMG_LEAF * 4);
     float* svol = (float*)valloc(h, (size_t)8 * n1 * UAAMG_LEAF * 4);
     float* vol7 = (float*)valloc(h, (size_t)7 * n2 * UAAMG_LEAF * 4);
     uint32_t* dofw = (uint32_t*)valloc(h, (size_t)3 * n1f * 64);
     uint32_t* solw = (uint32_t*)valloc(h, (size_t)3 * n1f * 64);
     if (n1) {
-        k_vsub_sdf<<<(unsigned)(8 * n1), 128, 0, s>>>(dliq, a1org, sub_bg, sdf);
-        CHECK_LAUNCH();
-        k_vsub_vol<<<(unsigned)(8 * n1), 128, 0, s>>>(d1, a1org, sdf, sub_bg, svol);
+        k_vsub<<<(unsigned)(8 * n1), 128, 0, s>>>(dliq, d1, a1org, sub_bg, svol);
         CHECK_LAUNCH();
     }
     if (n2) {
         k_vvol<<<(unsigned)n2, 128, 0, s>>>(d1, a2org, n2, svol, vol7);
         CHECK_LAUNCH();
     }
-    vfree_now(h, sdf);
     vfree_now(h, svol);
     h->V.voxel = DField{d2, vol7};
     for (int c = 0; c < 3; ++c) {
@@ -477,7 +473,7 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
             a[VA_T11] = 1.f;
         }
         upload_defpage(h, D);
-        launch2(k_vcoarse_coef, dim3((unsigned)h->host[fl + 1].nl, 3), 128, s, h->lv[fl].L, D.L, (float*)D.L.coef);
+        launch2(k_vcoarse_coef, dim3((unsigned)h->host[fl + 1].nl, 3, 4), 128, s, h->lv[fl].L, D.L, (float*)D.L.coef);
     }
     h->nlev = (int)h->host.size();
     {
@@ -510,7 +506,7 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
         float* val = (float*)valloc(h, (size_t)(n ? n : 1) * VCG_W * 4);
         float* invd = (float*)valloc(h, (size_t)(n ? n : 1) * 4);
         long long* slot = (long long*)valloc(h, (size_t)(n ? n : 1) * 8);
-        if (n) launch2(k_vcoarsest_ell, dim3((unsigned)H.nl, 3), 128, s, D.L, (const int*)D.dof_base, col, val, invd, slot);
+        if (n) launch2(k_vcoarsest_ell, dim3((unsigned)H.nl, 3, 4), 128, s, D.L, (const int*)D.dof_base, col, val, invd, slot);
         h->C.col = col;
         h->C.val = val;
         h->C.invd = invd;

@@ -42,17 +42,30 @@ __device__ __forceinline__ float vdb_lerp(float a, float b, double w) {
     const float d = __fsub_rn(b, a);
     return __fadd_rn(a, __double2float_rn(__dmul_rn((double)d, w)));
 }
+__device__ __forceinline__ float box_interp(float d000, float d001, float d010, float d011, float d100, float d101,
+                                            float d110, float d111, double u, double v, double w) {
+    const float a0 = vdb_lerp(vdb_lerp(d000, d001, w), vdb_lerp(d010, d011, w), v);
+    const float a1 = vdb_lerp(vdb_lerp(d100, d101, w), vdb_lerp(d110, d111, w), v);
+    return vdb_lerp(a0, a1, u);
+}
 __device__ __forceinline__ float box_sample(const DGrid& g, double px, double py, double pz) {
     const double fx = floor(px), fy = floor(py), fz = floor(pz);
     const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
     const double u = __dsub_rn(px, fx), v = __dsub_rn(py, fy), w = __dsub_rn(pz, fz);
-    const float d000 = g.get(ix, iy, iz, 0), d001 = g.get(ix, iy, iz + 1, 0);
-    const float d010 = g.get(ix, iy + 1, iz, 0), d011 = g.get(ix, iy + 1, iz + 1, 0);
-    const float d100 = g.get(ix + 1, iy, iz, 0), d101 = g.get(ix + 1, iy, iz + 1, 0);
-    const float d110 = g.get(ix + 1, iy + 1, iz, 0), d111 = g.get(ix + 1, iy + 1, iz + 1, 0);
-    const float a0 = vdb_lerp(vdb_lerp(d000, d001, w), vdb_lerp(d010, d011, w), v);
-    const float a1 = vdb_lerp(vdb_lerp(d100, d101, w), vdb_lerp(d110, d111, w), v);
-    return vdb_lerp(a0, a1, u);
+    return box_interp(g.get(ix, iy, iz, 0), g.get(ix, iy, iz + 1, 0), g.get(ix, iy + 1, iz, 0),
+                      g.get(ix, iy + 1, iz + 1, 0), g.get(ix + 1, iy, iz, 0), g.get(ix + 1, iy, iz + 1, 0),
+                      g.get(ix + 1, iy + 1, iz, 0), g.get(ix + 1, iy + 1, iz + 1, 0), u, v, w);
+}
+
+// box_sample over a 10^3 block of a grid staged in shared memory, the block's
+// voxel (0,0,0) at (bx, by, bz); the caller guarantees floor(p) + 1 lies in it.
+__device__ __forceinline__ float box_sample_block(const float (*blk)[10][10], int bx, int by, int bz, double px,
+                                                  double py, double pz) {
+    const double fx = floor(px), fy = floor(py), fz = floor(pz);
+    const int ix = (int)fx - bx, iy = (int)fy - by, iz = (int)fz - bz;
+    return box_interp(blk[ix][iy][iz], blk[ix][iy][iz + 1], blk[ix][iy + 1][iz], blk[ix][iy + 1][iz + 1],
+                      blk[ix + 1][iy][iz], blk[ix + 1][iy][iz + 1], blk[ix + 1][iy + 1][iz],
+                      blk[ix + 1][iy + 1][iz + 1], __dsub_rn(px, fx), __dsub_rn(py, fy), __dsub_rn(pz, fz));
 }
 
 // volume_fractions.cpp:82-120 (float versions)
@@ -90,6 +103,10 @@ __device__ __forceinline__ float cube_fraction(float p000, float p100, float p01
     if (p000 < 0.f && p100 < 0.f && p010 < 0.f && p110 < 0.f && p001 < 0.f && p101 < 0.f && p011 < 0.f &&
         p111 < 0.f)
         return 1.0f;
+    // all corners outside: every tet fraction is +0, so is the mean
+    if (p000 > 0.f && p100 > 0.f && p010 > 0.f && p110 > 0.f && p001 > 0.f && p101 > 0.f && p011 > 0.f &&
+        p111 > 0.f)
+        return 0.0f;
     float s = tet_fraction(p000, p001, p101, p011);
     s = __fadd_rn(s, tet_fraction(p000, p101, p100, p110));
     s = __fadd_rn(s, tet_fraction(p000, p010, p011, p110));
@@ -114,45 +131,49 @@ __device__ __forceinline__ int sub_leaf_of(const DMap& a1, int sx, int sy, int s
     return li * 8 + (((sx >> 3) & 1) << 2) + (((sy >> 3) & 1) << 1) + ((sz >> 3) & 1);
 }
 
-__global__ void __launch_bounds__(128) k_vsub_sdf(DGrid liq, const int* a1org, float bg, float* sdf) {
+// One subcell leaf per CTA (8 per liquid leaf of the dilated set): the
+// subcell SDF at the 9^3 corners the leaf's cubes need, then the cubes'
+// liquid fractions.  The SDF at subcell s is min(BoxSampler of the liquid SDF
+// at s/2 - 1/2, 1.5 dx) where s's subcell leaf exists, else 1.5 dx (the
+// subcell grid's background).  The liquid values those samples read -- a 6^3
+// block from s0/2 - 1 -- are staged in shared memory first, so each cube reads
+// its 8 corners from shared memory instead of through the leaf map.
+__global__ void __launch_bounds__(128) k_vsub(DGrid liq, DMap a1, const int* a1org, float bg, float* svol) {
+    __shared__ float lq[6][6][6];
+    __shared__ float cs[9][9][9];
+    __shared__ int halo[8];
     const int b = blockIdx.x, t = threadIdx.x;
     const int li = b >> 3, q = b & 7;
     const int ox = 2 * a1org[3 * li] + 8 * (q >> 2), oy = 2 * a1org[3 * li + 1] + 8 * ((q >> 1) & 1),
               oz = 2 * a1org[3 * li + 2] + 8 * (q & 1);
-    const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
-    float4 r;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int sx = ox + X, sy = oy + Y, sz = oz + Z0 + j;
-        const float v = box_sample(liq, 0.5 * sx - 0.5, 0.5 * sy - 0.5, 0.5 * sz - 0.5);
-        f4set(r, j, v < bg ? v : bg);
+    const int lx = (ox >> 1) - 1, ly = (oy >> 1) - 1, lz = (oz >> 1) - 1;
+    for (int i = t; i < 216; i += 128) lq[i / 36][(i / 6) % 6][i % 6] = liq.get(lx + i / 36, ly + (i / 6) % 6, lz + i % 6, 0);
+    if (t < 8) halo[t] = sub_leaf_of(a1, ox + 8 * (t >> 2), oy + 8 * ((t >> 1) & 1), oz + 8 * (t & 1)) >= 0;
+    __syncthreads();
+    for (int i = t; i < 729; i += 128) {
+        const int k0 = i / 81, k1 = (i / 9) % 9, k2 = i % 9;
+        float v = bg;
+        if (halo[((k0 >> 3) << 2) | ((k1 >> 3) << 1) | (k2 >> 3)]) {
+            const double px = 0.5 * (ox + k0) - 0.5, py = 0.5 * (oy + k1) - 0.5, pz = 0.5 * (oz + k2) - 0.5;
+            const double fx = floor(px), fy = floor(py), fz = floor(pz);
+            const int ix = (int)fx - lx, iy = (int)fy - ly, iz = (int)fz - lz;
+            const float sv = box_interp(lq[ix][iy][iz], lq[ix][iy][iz + 1], lq[ix][iy + 1][iz], lq[ix][iy + 1][iz + 1],
+                                        lq[ix + 1][iy][iz], lq[ix + 1][iy][iz + 1], lq[ix + 1][iy + 1][iz],
+                                        lq[ix + 1][iy + 1][iz + 1], __dsub_rn(px, fx), __dsub_rn(py, fy),
+                                        __dsub_rn(pz, fz));
+            v = sv < bg ? sv : bg;
+        }
+        cs[k0][k1][k2] = v;
     }
-    reinterpret_cast<float4*>(sdf)[(long long)b * UAAMG_LEAF4 + t] = r;
-}
-
-__global__ void __launch_bounds__(128) k_vsub_vol(DMap a1, const int* a1org, const float* sdf, float bg,
-                                                  float* svol) {
-    const int b = blockIdx.x, t = threadIdx.x;
-    const int li = b >> 3, q = b & 7;
-    const int ox = 2 * a1org[3 * li] + 8 * (q >> 2), oy = 2 * a1org[3 * li + 1] + 8 * ((q >> 1) & 1),
-              oz = 2 * a1org[3 * li + 2] + 8 * (q & 1);
+    __syncthreads();
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     float4 r;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const int sx = ox + X, sy = oy + Y, sz = oz + Z0 + j;
-        float p[2][2][2];
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int bb = 0; bb < 2; ++bb)
-#pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const int sl = sub_leaf_of(a1, sx + a, sy + bb, sz + c);
-                    p[a][bb][c] = sl < 0 ? bg : sdf[(long long)sl * UAAMG_LEAF + voff3(sx + a, sy + bb, sz + c)];
-                }
-        const float f = cube_fraction(p[0][0][0], p[1][0][0], p[0][1][0], p[1][1][0], p[0][0][1], p[1][0][1],
-                                      p[0][1][1], p[1][1][1]);
+        const int Z = Z0 + j;
+        const float f = cube_fraction(cs[X][Y][Z], cs[X + 1][Y][Z], cs[X][Y + 1][Z], cs[X + 1][Y + 1][Z],
+                                      cs[X][Y][Z + 1], cs[X + 1][Y][Z + 1], cs[X][Y + 1][Z + 1],
+                                      cs[X + 1][Y + 1][Z + 1]);
         f4set(r, j, f > 0 ? f : 0.f);
     }
     reinterpret_cast<float4*>(svol)[(long long)b * UAAMG_LEAF4 + t] = r;
@@ -160,24 +181,36 @@ __global__ void __launch_bounds__(128) k_vsub_vol(DMap a1, const int* a1org, con
 
 // calculate_matrix_coefficients_volume (:332-406) over the liquid leaves
 // dilated by two voxels: out[0] voxel, out[1+c] face c, out[4+c] edge c.
+// The 3^3 subcells around 2g of every voxel g of the leaf lie in the 17^3
+// block of subcells from 2*origin - 1; the block is staged in shared memory
+// (0 where the subcell leaf does not exist) with the 8 liquid leaves it
+// touches looked up once.
 __global__ void __launch_bounds__(128) k_vvol(DMap a1, const int* a2org, int n2, const float* svol, float* out) {
+    __shared__ float sb[17][17][17];
+    __shared__ int lv[8];  // liquid leaf of (origin + 8*(i>>2, (i>>1)&1, i&1) - 8), or -1
     const int leaf = blockIdx.x, t = threadIdx.x;
+    const int ax = a2org[3 * leaf], ay = a2org[3 * leaf + 1], az = a2org[3 * leaf + 2];
+    if (t < 8) lv[t] = a1.find(ax - 8 + 8 * (t >> 2), ay - 8 + 8 * ((t >> 1) & 1), az - 8 + 8 * (t & 1));
+    __syncthreads();
+    const int s0x = 2 * ax - 1, s0y = 2 * ay - 1, s0z = 2 * az - 1;
+    for (int i = t; i < 17 * 17 * 17; i += 128) {
+        const int a = i / 289, b = (i / 17) % 17, c = i % 17;
+        const int sx = s0x + a, sy = s0y + b, sz = s0z + c;
+        // liquid voxel sx>>1 lies in the leaf before the origin's (a == 0) or in the origin's own
+        const int l = lv[((a > 0) << 2) | ((b > 0) << 1) | (c > 0)];
+        float v = 0.f;
+        if (l >= 0) {
+            const int sl = l * 8 + (((sx >> 3) & 1) << 2) + (((sy >> 3) & 1) << 1) + ((sz >> 3) & 1);
+            v = svol[(long long)sl * UAAMG_LEAF + voff3(sx, sy, sz)];
+        }
+        sb[a][b][c] = v;
+    }
+    __syncthreads();
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     float4 res[7];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const int g0 = a2org[3 * leaf] + X, g1 = a2org[3 * leaf + 1] + Y, g2 = a2org[3 * leaf + 2] + Z0 + j;
-        float sv[3][3][3];  // subcell volumes at 2g + (-1..1)^3
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const int sx = 2 * g0 + a - 1, sy = 2 * g1 + b - 1, sz = 2 * g2 + c - 1;
-                    const int sl = sub_leaf_of(a1, sx, sy, sz);
-                    sv[a][b][c] = sl < 0 ? 0.f : svol[(long long)sl * UAAMG_LEAF + voff3(sx, sy, sz)];
-                }
+        const int bx = 2 * X, by = 2 * Y, bz = 2 * (Z0 + j);  // subcell 2g - 1 in the block
         float vol_c = 0.f, vf[3] = {0.f, 0.f, 0.f}, ve[3] = {0.f, 0.f, 0.f};
 #pragma unroll
         for (int i = 0; i < 2; ++i)
@@ -185,14 +218,14 @@ __global__ void __launch_bounds__(128) k_vvol(DMap a1, const int* a2org, int n2,
             for (int jj = 0; jj < 2; ++jj)
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
-                    vol_c = __fadd_rn(vol_c, sv[i + 1][jj + 1][k + 1]);
+                    vol_c = __fadd_rn(vol_c, sb[bx + i + 1][by + jj + 1][bz + k + 1]);
                     // face c: subcell - e_c; edge c: subcell - (1,1,1) + e_c
-                    vf[0] = __fadd_rn(vf[0], sv[i][jj + 1][k + 1]);
-                    ve[0] = __fadd_rn(ve[0], sv[i + 1][jj][k]);
-                    vf[1] = __fadd_rn(vf[1], sv[i + 1][jj][k + 1]);
-                    ve[1] = __fadd_rn(ve[1], sv[i][jj + 1][k]);
-                    vf[2] = __fadd_rn(vf[2], sv[i + 1][jj + 1][k]);
-                    ve[2] = __fadd_rn(ve[2], sv[i][jj][k + 1]);
+                    vf[0] = __fadd_rn(vf[0], sb[bx + i][by + jj + 1][bz + k + 1]);
+                    ve[0] = __fadd_rn(ve[0], sb[bx + i + 1][by + jj][bz + k]);
+                    vf[1] = __fadd_rn(vf[1], sb[bx + i + 1][by + jj][bz + k + 1]);
+                    ve[1] = __fadd_rn(ve[1], sb[bx + i][by + jj + 1][bz + k]);
+                    vf[2] = __fadd_rn(vf[2], sb[bx + i + 1][by + jj + 1][bz + k]);
+                    ve[2] = __fadd_rn(ve[2], sb[bx + i][by + jj][bz + k + 1]);
                 }
         f4set(res[0], j, vol_c > 0 ? __fmul_rn(vol_c, 0.125f) : 0.f);
 #pragma unroll
@@ -221,20 +254,32 @@ __device__ __forceinline__ void store_bits(uint32_t* words, int leaf, int t, uns
 struct VolFields {
     DField voxel, face[3], edge[3];
 };
+// The solid samples at the minus-face centres g - e_c / 2 read the solid SDF
+// at g - e_c .. g + 1: the 10^3 block from origin - 1, staged in shared memory.
 __global__ void __launch_bounds__(128) k_vdof(DGrid sol, VolFields V, const int* org, int n, uint32_t* dofw,
                                               uint32_t* solidw) {
+    __shared__ float sb[10][10][10];
     const int leaf = blockIdx.x, t = threadIdx.x;
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
-#pragma unroll 1
+    const int ox = org[3 * leaf], oy = org[3 * leaf + 1], oz = org[3 * leaf + 2];
+    for (int i = t; i < 1000; i += 128) sb[i / 100][(i / 10) % 10][i % 10] = sol.get(ox - 1 + i / 100, oy - 1 + (i / 10) % 10, oz - 1 + i % 10, 0);
+    __syncthreads();
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
         const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
         unsigned dn = 0, sn = 0;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const int g[3] = {org[3 * leaf] + X, org[3 * leaf + 1] + Y, org[3 * leaf + 2] + Z0 + j};
+            const int g[3] = {ox + X, oy + Y, oz + Z0 + j};
             double p[3] = {(double)g[0], (double)g[1], (double)g[2]};
             p[c] -= 0.5;
-            const float s = box_sample(sol, p[0], p[1], p[2]);
+            // box_sample over the staged block: floor(p) - (origin - 1) in 0..8
+            const double fx = floor(p[0]), fy = floor(p[1]), fz = floor(p[2]);
+            const int ix = (int)fx - ox + 1, iy = (int)fy - oy + 1, iz = (int)fz - oz + 1;
+            const float s = box_interp(sb[ix][iy][iz], sb[ix][iy][iz + 1], sb[ix][iy + 1][iz], sb[ix][iy + 1][iz + 1],
+                                       sb[ix + 1][iy][iz], sb[ix + 1][iy][iz + 1], sb[ix + 1][iy + 1][iz],
+                                       sb[ix + 1][iy + 1][iz + 1], __dsub_rn(p[0], fx), __dsub_rn(p[1], fy),
+                                       __dsub_rn(p[2], fz));
             if (s < 0) {
                 sn |= 1u << j;
                 continue;
@@ -271,12 +316,12 @@ __device__ __forceinline__ bool vdof_at(const VLevel& L, const int* nbrow, int c
 // finest_level_matrix_setter::channel_op (:617-844), grid (nl, 3).  Voxels of
 // pattern leaves outside the DOF pattern get the same formulas; nothing reads
 // them (every read is within two voxels of a DOF).
-__global__ void __launch_bounds__(128) k_vcoef0(VLevel L, const int* org, VolFields V, DGrid mu, float factor,
-                                                float ddiag, float* coef) {
-    griddep_wait();
-    griddep_launch();
-    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
+template <int C>
+__device__ __forceinline__ void vcoef0_body(const VLevel& L, const int* org, const VolFields& V, const DGrid& mu,
+                                            float factor, float ddiag, float* coef, float (*mub)[10][10]) {
+    const int leaf = blockIdx.x, c = C, t = threadIdx.x;
     const int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    const int bx = org[3 * leaf] - 1, by = org[3 * leaf + 1] - 1, bz = org[3 * leaf + 2] - 1;
     const int* nbrow = L.nb + (long long)leaf * 27;
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     int e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0};
@@ -295,13 +340,13 @@ __global__ void __launch_bounds__(128) k_vcoef0(VLevel L, const int* org, VolFie
             if (fv < 1e-1f) fv = 1e-1f;
             float diag = __fadd_rn(0.f, fv);
             {
-                const float term = __fmul_rn(__fmul_rn(two_f, V.voxel.get(g[0], g[1], g[2])), mu.get(g[0], g[1], g[2], 0));
+                const float term = __fmul_rn(__fmul_rn(two_f, V.voxel.get(g[0], g[1], g[2])), mub[X + 1][Y + 1][lz + 1]);
                 diag = __fadd_rn(diag, term);
             }
             float negv[3];
             {
                 const int m[3] = {g[0] - e0[0], g[1] - e0[1], g[2] - e0[2]};
-                const float term = __fmul_rn(__fmul_rn(two_f, V.voxel.get(m[0], m[1], m[2])), mu.get(m[0], m[1], m[2], 0));
+                const float term = __fmul_rn(__fmul_rn(two_f, V.voxel.get(m[0], m[1], m[2])), mub[m[0] - bx][m[1] - by][m[2] - bz]);
                 diag = __fadd_rn(diag, term);
                 negv[0] = vdof_at(L, nbrow, c, X - e0[0], Y - e0[1], lz - e0[2]) ? -term : 0.f;
             }
@@ -318,7 +363,7 @@ __global__ void __launch_bounds__(128) k_vcoef0(VLevel L, const int* org, VolFie
                 const float ev = V.edge[ech].get(q[0], q[1], q[2]);
                 float p[3] = {fc[0], fc[1], fc[2]};
                 p[ax] = pos ? __fadd_rn(p[ax], 0.5f) : __fsub_rn(p[ax], 0.5f);
-                const float sm = box_sample(mu, p[0], p[1], p[2]);
+                const float sm = box_sample_block(mub, bx, by, bz, p[0], p[1], p[2]);
                 const float term = __fmul_rn(__fmul_rn(factor, ev), sm);
                 diag = __fadd_rn(diag, term);
                 if (!pos) {
@@ -362,7 +407,7 @@ __global__ void __launch_bounds__(128) k_vcoef0(VLevel L, const int* org, VolFie
             float p[3] = {(float)g[0], (float)g[1], (float)g[2]};
             p[d1] = jj ? __fadd_rn(p[d1], 0.5f) : __fsub_rn(p[d1], 0.5f);
             p[d2] = kk ? __fadd_rn(p[d2], 0.5f) : __fsub_rn(p[d2], 0.5f);
-            const float sm = box_sample(mu, p[0], p[1], p[2]);
+            const float sm = box_sample_block(mub, bx, by, bz, p[0], p[1], p[2]);
             const float f = (jj == kk) ? factor : -factor;
             val[VA_T00 + jk] = __fmul_rn(__fmul_rn(f, ev), sm);
         }
@@ -375,7 +420,22 @@ __global__ void __launch_bounds__(128) k_vcoef0(VLevel L, const int* org, VolFie
             out[a];
 }
 
-// coarse_matrix_coef_setter (:1068-1350), grid (coarse nl, 3): R A P with
+__global__ void __launch_bounds__(128) k_vcoef0(VLevel L, const int* org, VolFields V, DGrid mu, float factor,
+                                                float ddiag, float* coef) {
+    // mu on the 10^3 block from origin - 1: every sample lies within half a voxel of the leaf's voxels
+    __shared__ float mub[10][10][10];
+    griddep_wait();
+    griddep_launch();
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    const int bx = org[3 * leaf] - 1, by = org[3 * leaf + 1] - 1, bz = org[3 * leaf + 2] - 1;
+    for (int i = t; i < 1000; i += 128) mub[i / 100][(i / 10) % 10][i % 10] = mu.get(bx + i / 100, by + (i / 10) % 10, bz + i % 10, 0);
+    __syncthreads();
+    if (blockIdx.y == 0) vcoef0_body<0>(L, org, V, mu, factor, ddiag, coef, mub);
+    else if (blockIdx.y == 1) vcoef0_body<1>(L, org, V, mu, factor, ddiag, coef, mub);
+    else vcoef0_body<2>(L, org, V, mu, factor, ddiag, coef, mub);
+}
+
+// coarse_matrix_coef_setter (:1068-1350), grid (coarse nl, 3, 4): R A P with
 // rap_factor 0.125 from the fine level's (untrimmed) coefficients
 __global__ void __launch_bounds__(128) k_vcoarse_coef(VLevel F, VLevel C, float* coef) {
     griddep_wait();
@@ -385,10 +445,9 @@ __global__ void __launch_bounds__(128) k_vcoarse_coef(VLevel F, VLevel C, float*
     const int* nbrow = C.nb + (long long)leaf * 27;
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
     const float rap = 0.125f;
-    float4 out[VNA];
     const float* fdiag = F.coef + (long long)(c * VNA + VA_DIAG) * F.nl * UAAMG_LEAF;
-#pragma unroll 1
-    for (int j = 0; j < 4; ++j) {
+    {
+        const int j = blockIdx.z;  // one voxel per thread: the grid's z splits a thread's 4 z-consecutive voxels
         const int lz = Z0 + j;
         const int L3[3] = {X, Y, lz};
         const int q = ((X >= 4) << 2) | ((Y >= 4) << 1) | (lz >= 4);
@@ -490,12 +549,9 @@ __global__ void __launch_bounds__(128) k_vcoarse_coef(VLevel F, VLevel C, float*
         }
         (void)L3;
 #pragma unroll
-        for (int a = 0; a < VNA; ++a) f4set(out[a], j, val[a]);
+        for (int a = 0; a < VNA; ++a)
+            coef[(long long)(c * VNA + a) * C.nl * UAAMG_LEAF + (long long)leaf * UAAMG_LEAF + 4 * t + j] = val[a];
     }
-#pragma unroll
-    for (int a = 0; a < VNA; ++a)
-        reinterpret_cast<float4*>(coef + (long long)(c * VNA + a) * C.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] =
-            out[a];
 }
 
 // trim_default_nodes (:1692-1721) with LaplacianWithLevel::trimDefaultNodes
@@ -505,45 +561,54 @@ __global__ void __launch_bounds__(128) k_vcoarse_coef(VLevel F, VLevel C, float*
 __global__ void __launch_bounds__(128) k_vtrim(VLevel L, uint32_t* trim) {
     griddep_wait();
     griddep_launch();
-    __shared__ float shf[4];
+    // A leaf's array is trimmed when max over its active voxels of |v - default| (NaN differences skipped, 0
+    // when there are none) is <= |default * 1e-3|: every active voxel's difference is NaN or <= the tolerance,
+    // and the tolerance is not NaN.  All 27 arrays are tested at once and AND-reduced over the block.
+    __shared__ uint32_t shm[4];
     const int leaf = blockIdx.x, t = threadIdx.x;
     const int* nbrow = L.nb + (long long)leaf * 27;
     const int X = t >> 4, Y = (t >> 1) & 7, Z0 = (t & 1) * 4;
-    uint32_t bits = 0;
-#pragma unroll 1
+    uint32_t ok = 0, tolok = 0;
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
         const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
-#pragma unroll 1
+        const int e1[3] = {d1 == 0, d1 == 1, d1 == 2}, e2[3] = {d2 == 0, d2 == 1, d2 == 2};
+        bool own[4], mneg[3][4], a1n[4], a1p[4], a2n[4], a2p[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int lz = Z0 + j;
+            own[j] = vdof_at(L, nbrow, c, X, Y, lz);
+            mneg[0][j] = vdof_at(L, nbrow, c, X - 1, Y, lz);
+            mneg[1][j] = vdof_at(L, nbrow, c, X, Y - 1, lz);
+            mneg[2][j] = vdof_at(L, nbrow, c, X, Y, lz - 1);
+            a1n[j] = vdof_at(L, nbrow, d1, X, Y, lz);
+            a1p[j] = vdof_at(L, nbrow, d1, X + e1[0], Y + e1[1], lz + e1[2]);
+            a2n[j] = vdof_at(L, nbrow, d2, X, Y, lz);
+            a2p[j] = vdof_at(L, nbrow, d2, X + e2[0], Y + e2[1], lz + e2[2]);
+        }
+#pragma unroll
         for (int a = 0; a < VNA; ++a) {
             const float def = L.app[c * VNA + a];
             const float tol = fabsf(__fmul_rn(def, 1e-3f));
             const float4 v = reinterpret_cast<const float4*>(L.coef + (long long)(c * VNA + a) * L.nl * UAAMG_LEAF)
                 [(long long)leaf * UAAMG_LEAF4 + t];
-            float mx = 0.f;
+            bool good = true;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const int lz = Z0 + j;
                 bool act;
-                if (a == VA_DIAG || a == VA_INV) {
-                    act = vdof_at(L, nbrow, c, X, Y, lz);
-                } else if (a <= VA_NEGZ) {
-                    int m[3] = {X, Y, lz};
-                    m[a - VA_NEGX] -= 1;
-                    act = vdof_at(L, nbrow, c, X, Y, lz) && vdof_at(L, nbrow, c, m[0], m[1], m[2]);
-                } else {
-                    const int tt = a - VA_T00;
-                    int p1[3] = {X, Y, lz}, p2[3] = {X, Y, lz};
-                    if (tt & 2) p1[d1] += 1;
-                    if (tt & 1) p2[d2] += 1;
-                    act = vdof_at(L, nbrow, d1, p1[0], p1[1], p1[2]) && vdof_at(L, nbrow, d2, p2[0], p2[1], p2[2]);
-                }
-                if (act) mx = fmaxf(mx, fabsf(__fsub_rn(f4get(v, j), def)));
+                if (a == VA_DIAG || a == VA_INV) act = own[j];
+                else if (a <= VA_NEGZ) act = own[j] && mneg[a - VA_NEGX][j];
+                else act = (((a - VA_T00) & 2) ? a1p[j] : a1n[j]) && (((a - VA_T00) & 1) ? a2p[j] : a2n[j]);
+                if (act && fabsf(__fsub_rn(f4get(v, j), def)) > tol) good = false;
             }
-            const float blockmax = block_max128(mx, shf);
-            if (t == 0 && blockmax <= tol) bits |= 1u << (c * VNA + a);
+            if (good) ok |= 1u << (c * VNA + a);
+            if (tol == tol) tolok |= 1u << (c * VNA + a);
         }
     }
-    if (t == 0) trim[leaf] = bits;
+    ok = __reduce_and_sync(FULLMASK, ok);
+    if ((t & 31) == 0) shm[t >> 5] = ok;
+    __syncthreads();
+    if (t == 0) trim[leaf] = shm[0] & shm[1] & shm[2] & shm[3] & tolok;
 }
 
 // A trimmed leaf reads its array's applier default: write that default into
@@ -596,11 +661,10 @@ __global__ void __launch_bounds__(128) k_vcoarsest_ell(VLevel L, const int* dof_
     e0[d0] = 1;
     e1[d1] = 1;
     e2[d2] = 1;
-#pragma unroll 1
-    for (int j = 0; j < 4; ++j) {
-        const int lz = Z0 + j;
+    {
+        const int lz = Z0 + blockIdx.z;  // one voxel per thread: the grid's z splits a thread's 4 voxels
         const int row = vdof_number(L, dof_base, nbrow, c, X, Y, lz);
-        if (row < 0) continue;
+        if (row < 0) return;
         int cc[VCG_W];
         float vv[VCG_W];
         int n = 0;
