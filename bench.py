@@ -15,7 +15,9 @@ FLIP_vdb.cpp:3118-3168.
 
   value      device-resident inputs (torch CUDA tensors) through the C ABI
   e2e        the same step through the host-pointer C ABI from pinned host
-             memory, host<->device copies inside the timed region
+             memory (uaamg_viscosity_create, then uaamg_viscosity_solve_velocity:
+             the velocity in, the solved velocity out), host<->device copies
+             inside the timed region
   cpu_baseline / --impl reference
              the CPU restatement of the reference's SIMD solvers (oracle/),
              OpenMP over all host cores, on a bounded sample of solves
@@ -645,8 +647,9 @@ def main():
                     help="seconds of arrivals of the served request stream (0 = skip)")
     ap.add_argument("--serve-limit", type=float, default=60.0, help="time limit of each served run (s)")
     ap.add_argument("--no-graph", action="store_true", help="host-driven PCG loop instead of the CUDA graph")
-    ap.add_argument("--profile", choices=["solve", "sweep", "vsolve", "large"], default=None,
-                    help="short fixed sequence for ncu: 'vsolve' = viscosity build + 2 solves, "
+    ap.add_argument("--profile", choices=["solve", "sweep", "vsolve", "vbuild", "large"], default=None,
+                    help="short fixed sequence for ncu: 'vsolve' = viscosity build + 2 solves, 'vbuild' = "
+                         "3 viscosity matrix + hierarchy builds, "
                          "'solve' = Poisson build + 2 graph solves, 'sweep' = Poisson build + 3 level-0 sweeps, "
                          "'large' = the mixed-precision workload at --mixed-n, one host-driven solve in "
                          "--profile-form")
@@ -726,6 +729,15 @@ def main():
     vsc = scenes.plain_viscosity_scene(n=args.n, seed=1)
     vkeys = ("liquid_phi", "solid_phi", "viscosity", "u", "v", "w", "solid_velocity")
     vdg = {k: on_device(getattr(vsc, k)) for k in vkeys}
+
+    if args.profile == "vbuild":
+        for _ in range(3):
+            lv = L_with_level.create_viscosity_matrix(vdg["viscosity"], vdg["liquid_phi"], vdg["solid_phi"], vsc.dt,
+                                                      vsc.rho, vsc.dx)
+            torch.cuda.synchronize()
+            del lv
+        print(json.dumps({"profile": "vbuild", "builds": 3}))
+        return
 
     if args.profile == "vsolve":
         lv = L_with_level.create_viscosity_matrix(vdg["viscosity"], vdg["liquid_phi"], vdg["solid_phi"], vsc.dt,
@@ -820,13 +832,12 @@ def main():
                                                   vsc.rho, vsc.dx)
         n = lv.leaf_count(0)
         if vhost.get("n") != n:
-            vhost["rhs_t"] = torch.empty((3, n, 512), dtype=torch.float32).pin_memory()
             vhost["x_t"] = torch.empty((3, n, 512), dtype=torch.float32).pin_memory()
-            vhost["rhs"], vhost["x"], vhost["n"] = vhost["rhs_t"].numpy(), vhost["x_t"].numpy(), n
-        lv.build_rhs(vhg["u"], vhg["v"], vhg["w"], vhg["solid_velocity"], out=vhost["rhs"])
-        lv.gather_velocity(vhg["u"], vhg["v"], vhg["w"], out=vhost["x"])
+            vhost["x"], vhost["n"] = vhost["x_t"].numpy(), n
+        # the call site's viscosity step in one call: velocity uploaded once, rhs and warm start on the device,
+        # the solved velocity returned
         s = simd_viscosity3d(lv)
-        st = s.pcg_solve(vhost["x"], 1e-6, vhost["rhs"])
+        st, _ = s.solve_velocity(vhg["u"], vhg["v"], vhg["w"], vhg["solid_velocity"], 1e-6, out=vhost["x"])
         vstats["launches"] += s.kernel_launches
         return lv, st
 
@@ -980,12 +991,12 @@ def main():
                        "parallelism": f"replicas x{ws}", "solves_per_s": round(1e3 / value, 2),
                        "dof_updates_per_s": round(ndof[0] * (viters[0] + 1) * 1e3 / value, 1)},
             "e2e": {"value": round(e2e, 4), "unit": UNIT,
-                    # create: viscosity, liquid SDF (+mask), solid SDF; rhs and warm
-                    # start: three velocity channels each; solve: x and rhs
+                    # create: viscosity, liquid SDF (+mask), solid SDF; solve: the three
+                    # velocity channels and the solid velocity, once
                     "h2d_bytes_per_step": int(_grid_bytes(vsc.viscosity, vsc.liquid_phi, vsc.solid_phi)
-                                              + 2 * _grid_bytes(vsc.u, vsc.v, vsc.w) + 2 * vec_bytes),
-                    # rhs and warm start returned to the caller, solved velocity
-                    "d2h_bytes_per_step": int(3 * vec_bytes)},
+                                              + _grid_bytes(vsc.u, vsc.v, vsc.w, vsc.solid_velocity)),
+                    # the solved velocity
+                    "d2h_bytes_per_step": int(vec_bytes)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "k_vapply<RED_GS> level 0, channel 0 (2774 CTAs)",
                          "achieved": round(achieved, 1) if achieved else None, "peak": peak,

@@ -436,6 +436,16 @@ int uaamg_viscosity_solve_pcg(uaamg_viscosity* h, float* velocity, const float* 
                               int* iterations);
 int uaamg_viscosity_solve_pcg_device(uaamg_viscosity* h, float* d_velocity, const float* d_rhs,
                                      float tolerance, int* iterations);
+/* The viscosity step of the reference's call site in one call
+ * (FLIP_vdb.cpp:3178-3219: simd_viscosity3d(L, liquid_velocity, solid_velocity),
+ * the warm start from the velocity, pcg_solve): u, v, w (and the solid
+ * velocity, which may be NULL) are uploaded once, the rhs and the initial
+ * guess are built on the device, and only the solved velocity [3][nl][512]
+ * is returned (host pointer).  Identical results to uaamg_viscosity_build_rhs +
+ * uaamg_viscosity_gather_velocity + uaamg_viscosity_solve_pcg. */
+int uaamg_viscosity_solve_velocity(uaamg_viscosity* h, const uaamg_leaf_grid* u, const uaamg_leaf_grid* v,
+                                   const uaamg_leaf_grid* w, const uaamg_leaf_grid* solid_velocity, float tolerance,
+                                   float* velocity_out, int* iterations);
 
 /* Level operations (host pointers), for parity checks against the reference's
  * L_with_level members: one light_weight_applier pass (L_apply,

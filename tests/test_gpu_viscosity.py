@@ -17,7 +17,7 @@ import pytest
 
 from oracle.oracle import OracleViscosity
 from uaamg_b200 import scenes
-from uaamg_b200.grids import LeafGrid
+from uaamg_b200.grids import LeafGrid, dense_to_leaves
 
 pytestmark = pytest.mark.gpu
 
@@ -229,6 +229,26 @@ def test_device_api_matches_host_api(scene32, gpu):
     assert np.array_equal(d_rhs.cpu().numpy(), rhs)
     s.pcg_solve(d_x, 1e-6, d_rhs)
     assert np.array_equal(d_x.cpu().numpy(), xh)
+
+
+def test_solve_velocity_matches_step_by_step(gpu):
+    """uaamg_viscosity_solve_velocity (velocity uploaded once, rhs and warm
+    start on the device) gives the bits of build_rhs + gather_velocity +
+    pcg_solve, with a moving solid."""
+    from uaamg_b200.viscosity import simd_viscosity3d
+    sc = scenes.plain_viscosity_scene(n=32, seed=2)
+    m = 33
+    sv = dense_to_leaves(np.random.default_rng(4).uniform(-1, 1, (m, m, m, 3)).astype(np.float32),
+                         background=np.zeros(3, np.float32))
+    lv, _ = make(sc)
+    rhs = lv.build_rhs(sc.u, sc.v, sc.w, sv)
+    x = lv.gather_velocity(sc.u, sc.v, sc.w)
+    s1 = simd_viscosity3d(lv)
+    st1 = s1.pcg_solve(x, 1e-6, rhs)
+    s2 = simd_viscosity3d(lv)
+    st2, x2 = s2.solve_velocity(sc.u, sc.v, sc.w, sv, 1e-6)
+    assert st1 == st2 == 0 and s1.m_iteration == s2.m_iteration
+    assert np.array_equal(x, x2)
 
 
 def test_golden_fixture_on_gpu(gpu):

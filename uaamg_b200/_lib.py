@@ -116,6 +116,7 @@ EXPORTS = [
     ("uaamg_viscosity_gather_velocity_device", i32, [vp, pLG, pLG, pLG, vp]),
     ("uaamg_viscosity_solve_pcg", i32, [vp, vp, vp, f32, C.POINTER(C.c_int)]),
     ("uaamg_viscosity_solve_pcg_device", i32, [vp, vp, vp, f32, C.POINTER(C.c_int)]),
+    ("uaamg_viscosity_solve_velocity", i32, [vp, pLG, pLG, pLG, pLG, f32, vp, C.POINTER(C.c_int)]),
     ("uaamg_viscosity_level_apply", i32, [vp, i32, i32, i32, vp, vp, vp]),
     ("uaamg_viscosity_level_rbgs", i32, [vp, i32, i32, vp, vp]),
     ("uaamg_viscosity_level_restrict", i32, [vp, i32, vp, vp]),

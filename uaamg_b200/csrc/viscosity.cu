@@ -1043,6 +1043,58 @@ int uaamg_viscosity_solve_pcg_device(uaamg_viscosity* h, float* d_velocity, cons
     ABI_END
 }
 
+int uaamg_viscosity_solve_velocity(uaamg_viscosity* h, const uaamg_leaf_grid* u, const uaamg_leaf_grid* v,
+                                   const uaamg_leaf_grid* w, const uaamg_leaf_grid* solid_velocity, float tolerance,
+                                   float* velocity_out, int* iterations) {
+    ABI_BEGIN
+    require(h != nullptr && velocity_out != nullptr, "NULL argument");
+    vgrids3(u, v, w);
+    bool moving = false;
+    if (solid_velocity) {
+        check_grid(solid_velocity, 3, "solid_velocity");
+        moving = solid_velocity->leaf_count > 0 || solid_velocity->background[0] != 0.f ||
+                 solid_velocity->background[1] != 0.f || solid_velocity->background[2] != 0.f;
+    }
+    const size_t mark = h->allocs.size();
+    int st = UAAMG_FAILED;
+    try {
+        VelGrids U;
+        U.v[0] = vupload_grid(h, u);
+        U.v[1] = vupload_grid(h, v);
+        U.v[2] = vupload_grid(h, w);
+        const VLevelDev& D = h->lv[0];
+        const size_t vb = vvec_bytes(h, 0);
+        // the rhs (simd_viscosity3d ctor, .cpp:3660-3689) and the warm start (FLIP_vdb.cpp:3186-3198) straight
+        // into the PCG vectors
+        CK(cudaMemsetAsync(h->b, 0, vb, h->stream));
+        launch2(k_vrhs, dim3((unsigned)D.L.nl, 3), 128, h->stream, D.L, (const int*)D.org, h->V, U, h->b);
+        if (moving) {
+            DGrid dsv = vupload_grid(h, solid_velocity);
+            launch2(k_vrhs_solid, dim3((unsigned)D.L.nl, 3), 128, h->stream, D.L, (const int*)D.org, h->V, h->mu,
+                    h->S, dsv, h->factor, h->b);
+        }
+        launch2(k_vgather, dim3((unsigned)D.L.nl, 3), 128, h->stream, D.L, (const int*)D.org, U, h->x);
+        h->tol = tolerance;
+        st = vrun_pcg(h);
+        CK(cudaMemcpyAsync(velocity_out, h->x, vb, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    } catch (...) {
+        cudaStreamSynchronize(h->stream);
+        while (h->allocs.size() > mark) {
+            cudaFreeAsync(h->allocs.back(), h->stream);
+            h->allocs.pop_back();
+        }
+        throw;
+    }
+    while (h->allocs.size() > mark) {
+        CK(cudaFreeAsync(h->allocs.back(), h->stream));
+        h->allocs.pop_back();
+    }
+    if (iterations) *iterations = h->iterations;
+    return st;
+    ABI_END
+}
+
 // level operations (host pointers; parity tests)
 int uaamg_viscosity_level_apply(uaamg_viscosity* h, int level, int mode, int channel, const float* lhs,
                                 const float* rhs, float* out) {

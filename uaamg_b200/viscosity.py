@@ -228,6 +228,26 @@ class simd_viscosity3d:
         self.m_iteration = int(it.value)
         return int(rc)
 
+    def solve_velocity(self, u: LeafGrid, v: LeafGrid, w: LeafGrid, solid_velocity: LeafGrid | None,
+                       tolerance: float, out: np.ndarray | None = None):
+        """The call site's viscosity step in one C-ABI call (FLIP_vdb.cpp:
+        3178-3219; uaamg_viscosity_solve_velocity): the rhs and the warm start
+        from the velocity, uploaded once, then PCG.  Returns (status, the solved
+        DOF velocity [3, n, 512] in ``out`` or a new array); identical to
+        build_rhs + gather_velocity + pcg_solve."""
+        L, h = self._configure()
+        keep: list = []
+        gs = [_as_c(g, keep) for g in (u, v, w)]
+        sv = C.byref(_as_c(solid_velocity, keep)) if solid_velocity is not None else None
+        x = self.level0.get_zero_vec() if out is None else out
+        assert x.dtype == np.float32 and x.flags["C_CONTIGUOUS"]
+        it = C.c_int(0)
+        rc = L.uaamg_viscosity_solve_velocity(h, *[C.byref(g) for g in gs], sv, float(tolerance), x.ctypes.data,
+                                              C.byref(it))
+        _lib.check(rc, "solve_velocity")
+        self.m_iteration = int(it.value)
+        return int(rc), x
+
     def precondition(self, r: np.ndarray) -> np.ndarray:
         L, h = self._configure()
         z = np.zeros_like(r, dtype=np.float32)
