@@ -84,6 +84,15 @@ static inline bool key_less(const VdbKey& a, const VdbKey& b) {
     return false;
 }
 
+// population count of a 64-bit mask on the host (SWAR bit count; inline, no
+// library call on CPUs compiled without a popcount instruction)
+static inline int host_popc64(uint64_t x) {
+    x = x - ((x >> 1) & 0x5555555555555555ull);
+    x = (x & 0x3333333333333333ull) + ((x >> 2) & 0x3333333333333333ull);
+    x = (x + (x >> 4)) & 0x0F0F0F0F0F0F0F0Full;
+    return (int)((x * 0x0101010101010101ull) >> 56);
+}
+
 struct HostMap {  // dense leaf-index volume over the bounding box
     int lo[3] = {0, 0, 0}, dim[3] = {0, 0, 0};
     std::vector<int32_t> idx;
@@ -150,7 +159,7 @@ static void finalize_host_level(HostLevel& L) {
     int64_t acc = 0;
     for (int i = 0; i < L.nl; ++i) {
         L.dof_base[i] = (int32_t)acc;
-        for (int w = 0; w < 8; ++w) acc += __builtin_popcountll(L.mask[8 * i + w]);
+        for (int w = 0; w < 8; ++w) acc += host_popc64(L.mask[8 * i + w]);
     }
     L.ndof = acc;
 }

@@ -31,16 +31,26 @@ static inline uint64_t yband(int lo, int hi) {
     for (int y = lo; y <= hi; ++y) b |= 0xFFull << (8 * y);
     return b;
 }
+// vdb_key packed into one unsigned 128-bit number with the same order: the
+// root tile origins (multiples of 4096) biased into 20 bits each, then the
+// 15-bit and 12-bit child offsets of the two internal levels.
+static inline unsigned __int128 vdb_key128(const int32_t* o) {
+    const VdbKey k = vdb_key(o);
+    const uint64_t rx = (uint64_t)((k.k[0] >> 12) + (1 << 19)), ry = (uint64_t)((k.k[1] >> 12) + (1 << 19)),
+                   rz = (uint64_t)((k.k[2] >> 12) + (1 << 19));
+    const uint64_t hi = (rx << 40) | (ry << 20) | rz;
+    const uint64_t lo = ((uint64_t)k.k[3] << 12) | (uint64_t)k.k[4];
+    return ((unsigned __int128)hi << 27) | lo;
+}
 static void sort_unique_vdb(std::vector<int32_t>& org) {
     const size_t n = org.size() / 3;
-    std::vector<std::pair<VdbKey, size_t>> keys(n);
-    for (size_t i = 0; i < n; ++i) keys[i] = {vdb_key(&org[3 * i]), i};
-    std::sort(keys.begin(), keys.end(),
-              [](const std::pair<VdbKey, size_t>& a, const std::pair<VdbKey, size_t>& b) { return key_less(a.first, b.first); });
+    std::vector<std::pair<unsigned __int128, uint32_t>> keys(n);
+    for (size_t i = 0; i < n; ++i) keys[i] = {vdb_key128(&org[3 * i]), (uint32_t)i};
+    std::sort(keys.begin(), keys.end());
     std::vector<int32_t> out;
     out.reserve(org.size());
     for (size_t i = 0; i < n; ++i) {
-        if (i > 0 && !key_less(keys[i - 1].first, keys[i].first)) continue;
+        if (i > 0 && keys[i - 1].first == keys[i].first) continue;
         const int32_t* o = &org[3 * keys[i].second];
         out.insert(out.end(), o, o + 3);
     }
@@ -115,12 +125,20 @@ struct VHostLevel {
 // set_dof (:500-538): per channel, leaves in tree order, offsets ascending;
 // numbering continues across channels
 static void finalize_vlevel(VHostLevel& L) {
-    L.map.build(L.nl, L.org.data());
+    // a one-leaf margin puts every leaf's 27 neighbour cells inside the map
+    L.map.build(L.nl, L.org.data(), 1);
     L.nb.assign((size_t)L.nl * 27, -1);
-    for (int i = 0; i < L.nl; ++i) {
-        const int32_t* o = &L.org[3 * i];
-        for (int a = 0; a < 27; ++a)
-            L.nb[27 * i + a] = L.map.find_leaf((o[0] >> 3) + a / 9 - 1, (o[1] >> 3) + (a / 3) % 3 - 1, (o[2] >> 3) + a % 3 - 1);
+    if (L.nl > 0) {
+        const int64_t s0 = (int64_t)L.map.dim[1] * L.map.dim[2], s1 = L.map.dim[2];
+        int64_t off[27];
+        for (int a = 0; a < 27; ++a) off[a] = (a / 9 - 1) * s0 + ((a / 3) % 3 - 1) * s1 + (a % 3 - 1);
+        const int32_t* idx = L.map.idx.data();
+        for (int i = 0; i < L.nl; ++i) {
+            const int32_t* o = &L.org[3 * i];
+            const int64_t base = L.map.cell(o[0] >> 3, o[1] >> 3, o[2] >> 3);
+            int32_t* nb = &L.nb[27 * (size_t)i];
+            for (int a = 0; a < 27; ++a) nb[a] = idx[base + off[a]];
+        }
     }
     L.dof_base.assign((size_t)3 * L.nl, 0);
     int64_t acc = 0;
@@ -128,7 +146,7 @@ static void finalize_vlevel(VHostLevel& L) {
         for (int i = 0; i < L.nl; ++i) {
             L.dof_base[(size_t)c * L.nl + i] = (int32_t)acc;
             const uint64_t* m = &L.dof[((size_t)c * L.nl + i) * 8];
-            for (int w = 0; w < 8; ++w) acc += __builtin_popcountll(m[w]);
+            for (int w = 0; w < 8; ++w) acc += host_popc64(m[w]);
         }
     L.ndof = acc;
     L.child.assign((size_t)L.nl * 8, -1);
@@ -187,10 +205,13 @@ static void coarsen_vlevel(VHostLevel& F, VHostLevel& C) {
                     uint64_t p = fm[2 * px] | fm[2 * px + 1];
                     p |= (p >> 1);
                     p |= (p >> 8);
+                    // bit 16*yy + 2*zz holds coarse voxel (yy, zz): compress each 16-bit group's bits 0, 2, 4, 6
+                    // into its low nibble, then place nibble yy at row oy*4 + yy, columns oz*4 ..
+                    uint64_t x = p & 0x0055005500550055ull;
+                    x = (x | (x >> 1)) & 0x0033003300330033ull;
+                    x = (x | (x >> 2)) & 0x000F000F000F000Full;
                     uint64_t& w = dm[((size_t)c * nd + i) * 8 + ox * 4 + px];
-                    for (int yy = 0; yy < 4; ++yy)
-                        for (int zz = 0; zz < 4; ++zz)
-                            if ((p >> (16 * yy + 2 * zz)) & 1ull) w |= 1ull << ((oy * 4 + yy) * 8 + oz * 4 + zz);
+                    for (int yy = 0; yy < 4; ++yy) w |= ((x >> (16 * yy)) & 0xFull) << ((oy * 4 + yy) * 8 + oz * 4);
                 }
             }
         }
@@ -361,34 +382,38 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
     h->def_diag = 1.0f + 8.0f * h->def_off;
     cudaStream_t s = h->stream;
 
-    // leaf sets of the three dilations of the liquid topology
+    // leaf sets of the three dilations of the liquid topology; the subcell kernel, which needs only the first,
+    // runs while the host builds the other two
     std::vector<int32_t> a1, a2, a1f;
     dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 1, false, a1, false);
-    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 2, false, a2, false);
-    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 1, true, a1f, false);
-    const int n1 = (int)(a1.size() / 3), n2 = (int)(a2.size() / 3), n1f = (int)(a1f.size() / 3);
-    HostMap m1, m2, m1f;
+    const int n1 = (int)(a1.size() / 3);
+    HostMap m1;
     m1.build(n1, a1.data());
-    m2.build(n2, a2.data());
-    m1f.build(n1f, a1f.data());
-    TRACE("visc host leaf sets");
-
     DGrid dliq = vupload_grid(h, liq);
-    DGrid dsol = vupload_grid(h, sol);
-    h->mu = vupload_grid(h, mu_g);
-    DMap d1 = vupload_map(h, m1), d2 = vupload_map(h, m2), d1f = vupload_map(h, m1f);
+    DMap d1 = vupload_map(h, m1);
     int* a1org = vupload(h, a1.data(), a1.size());
-    int* a2org = vupload(h, a2.data(), a2.size());
-    int* a1forg = vupload(h, a1f.data(), a1f.size());
     const float sub_bg = 1.5f * dx;
     float* svol = (float*)valloc(h, (size_t)8 * n1 * UAAMG_LEAF * 4);
-    float* vol7 = (float*)valloc(h, (size_t)7 * n2 * UAAMG_LEAF * 4);
-    uint32_t* dofw = (uint32_t*)valloc(h, (size_t)3 * n1f * 64);
-    uint32_t* solw = (uint32_t*)valloc(h, (size_t)3 * n1f * 64);
     if (n1) {
         k_vsub<<<(unsigned)(8 * n1), 128, 0, s>>>(dliq, d1, a1org, sub_bg, svol);
         CHECK_LAUNCH();
     }
+    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 2, false, a2, false);
+    dilate_leaves(liq->origins, liq->leaf_count, liq->masks, 1, true, a1f, false);
+    const int n2 = (int)(a2.size() / 3), n1f = (int)(a1f.size() / 3);
+    HostMap m2, m1f;
+    m2.build(n2, a2.data());
+    m1f.build(n1f, a1f.data());
+    TRACE("visc host leaf sets");
+
+    DGrid dsol = vupload_grid(h, sol);
+    h->mu = vupload_grid(h, mu_g);
+    DMap d2 = vupload_map(h, m2), d1f = vupload_map(h, m1f);
+    int* a2org = vupload(h, a2.data(), a2.size());
+    int* a1forg = vupload(h, a1f.data(), a1f.size());
+    float* vol7 = (float*)valloc(h, (size_t)7 * n2 * UAAMG_LEAF * 4);
+    uint32_t* dofw = (uint32_t*)valloc(h, (size_t)3 * n1f * 64);
+    uint32_t* solw = (uint32_t*)valloc(h, (size_t)3 * n1f * 64);
     if (n2) {
         k_vvol<<<(unsigned)n2, 128, 0, s>>>(d1, a2org, n2, svol, vol7);
         CHECK_LAUNCH();
