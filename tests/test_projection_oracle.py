@@ -156,3 +156,62 @@ def test_oracle_immersion_known_answers():
     assert at(4, 0, 0) == 1.0     # processed in pass 2, no negative neighbour, positive: unchanged
     assert at(6, 6, 6) == 1.0     # not active after the dilation
     assert np.all(out[1] == 1.0)  # no solid leaf at (8,0,0)
+
+
+def test_topology_edge_cases():
+    from uaamg_b200.topology import dilate, topology_coords, union
+    empty = (np.zeros((0, 3), np.int32), np.zeros((0, 8), np.uint64))
+    assert union([empty, empty])[0].shape == (0, 3)
+    assert dilate(empty, 3, 6)[0].shape == (0, 3) and dilate(empty, 2, 26)[0].shape == (0, 3)
+    org = np.array([[0, 0, 0], [8, 0, 0]], np.int32)
+    masks = np.zeros((2, 8), np.uint64)
+    masks[0, 3] = np.uint64(1 << 9)  # voxel (3, 1, 1)
+    o, m = dilate((org, masks), 0, 6)  # no layers: the non-empty leaves as they are
+    assert np.array_equal(o, org[:1]) and np.array_equal(m, masks[:1])
+    with pytest.raises(ValueError):
+        dilate((org, masks), 1, 18)
+    assert {tuple(p) for p in topology_coords(dilate((org, masks), 1, 26)).tolist()} == {
+        (3 + a, 1 + b, 1 + c) for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1)}
+
+
+def test_prepare_channel_touches_target_leaves():
+    """touchLeaf semantics: every target leaf the channel lacks becomes an
+    inactive leaf of background values, also one with no voxel to fill; a
+    target leaf whose voxels the channel already has gets no fill entry."""
+    from uaamg_b200.extrapolate import prepare_channel
+    ch = LeafGrid(origins=np.array([[0, 0, 0]], np.int32), values=np.full((1, 512), 2.0, np.float32),
+                  background=np.float32(-7.0), masks=np.full((1, 8), np.uint64(0xFFFFFFFFFFFFFFFF)))
+    torg = np.array([[0, 0, 0], [8, 0, 0], [16, 0, 0]], np.int32)
+    tmask = np.zeros((3, 8), np.uint64)
+    tmask[0] = np.uint64(0xFF)        # covered by the channel
+    tmask[1, 0] = np.uint64(0x3)       # two voxels to fill
+    org, vals, masks, fl, fm = prepare_channel(ch, (torg, tmask))  # leaf 2: empty target leaf
+    assert np.array_equal(org, torg) and vals.shape == (3, 512)
+    assert np.all(vals[0] == 2.0) and np.all(vals[1:] == -7.0)
+    assert np.all(masks[1:] == 0)
+    assert fl.tolist() == [1] and fm[0, 0] == np.uint64(0x3) and not fm[0, 1:].any()
+    # an empty channel: every target leaf is new and every active target voxel is filled
+    e = LeafGrid(origins=np.zeros((0, 3), np.int32), values=np.zeros((0, 512), np.float32),
+                 background=np.float32(0.0), masks=np.zeros((0, 8), np.uint64))
+    org, vals, masks, fl, fm = prepare_channel(e, (torg, tmask))
+    assert org.shape == (3, 3) and fl.tolist() == [0, 1] and not masks.any()
+
+
+def test_extrapolation_abi_rejects_bad_input_on_the_host():
+    """The C ABI checks the leaf list and the fill set before any device work."""
+    from uaamg_b200 import _lib
+    from uaamg_b200.extrapolate import run_layers
+    org = np.array([[0, 0, 0], [8, 0, 0]], np.int32)
+    vals = np.zeros((2, 512), np.float32)
+    masks = np.zeros((2, 8), np.uint64)
+    fm = np.ones((2, 8), np.uint64)
+    bad = [
+        (np.array([[0, 0, 0], [4, 0, 0]], np.int32), np.array([0], np.int32)),   # origin not a multiple of 8
+        (org, np.array([2], np.int32)),                                           # fill leaf out of range
+        (org, np.array([1, 1], np.int32)),                                        # a leaf listed twice
+        (np.array([[0, 0, 0], [0, 0, 0]], np.int32), np.array([0], np.int32)),   # duplicate output origin
+    ]
+    for o, fl in bad:
+        with pytest.raises(_lib.UaamgError):
+            run_layers(2, o, vals.copy(), masks.copy(), fl, np.ascontiguousarray(fm[: fl.size]))
+    run_layers(2, org, vals, masks, np.zeros(0, np.int32), np.zeros((0, 8), np.uint64))  # nothing to fill
