@@ -215,3 +215,17 @@ def test_extrapolation_abi_rejects_bad_input_on_the_host():
         with pytest.raises(_lib.UaamgError):
             run_layers(2, o, vals.copy(), masks.copy(), fl, np.ascontiguousarray(fm[: fl.size]))
     run_layers(2, org, vals, masks, np.zeros(0, np.int32), np.zeros((0, 8), np.uint64))  # nothing to fill
+
+
+@pytest.mark.parametrize("neighbours,n_layer", [(6, 3), (26, 2), (6, 10)])
+def test_dense_and_sorted_dilation_agree(monkeypatch, neighbours, n_layer):
+    """The dense bounding-box dilation and the sorted-leaf one (used for huge
+    sparse boxes) give the same leaves, in the same order, and masks."""
+    from uaamg_b200 import topology as T
+    rng = np.random.default_rng(neighbours + n_layer)
+    shape = (37, 29, 44)
+    g = dense_to_leaves(np.zeros(shape, np.float32), origin=(-24, 0, 8), active=rng.random(shape) < 0.002)
+    a = T.dilate(g, n_layer, neighbours)
+    monkeypatch.setattr(T, "_DENSE_MAX_CELLS", 0)
+    b = T.dilate(g, n_layer, neighbours)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])

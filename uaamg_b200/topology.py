@@ -70,10 +70,12 @@ def union(topos) -> tuple[np.ndarray, np.ndarray]:
     masks = np.concatenate([t[1] for t in topos], axis=0).reshape(-1, 8)
     if org.shape[0] == 0:
         return org.astype(np.int32), masks.astype(np.uint64)
-    uk, first, inv = np.unique(leaf_keys(org), return_index=True, return_inverse=True)
-    out = np.zeros((uk.size, 8), np.uint64)
-    np.bitwise_or.at(out, inv.reshape(-1), masks)
-    return org[first].astype(np.int32), out
+    k = leaf_keys(org)
+    order = np.argsort(k, kind="stable")
+    ks = k[order]
+    starts = np.flatnonzero(np.r_[True, ks[1:] != ks[:-1]])
+    out = np.bitwise_or.reduceat(masks[order], starts, axis=0)
+    return org[order[starts]].astype(np.int32), np.ascontiguousarray(out, dtype=np.uint64)
 
 
 def _nonempty(org, masks):
@@ -144,12 +146,69 @@ def dilate_box_once(org, masks):
     return org, masks
 
 
+# ---------------------------------------------------------------------------
+# Dense form: the masks of every leaf cell of the bounding box (plus a margin)
+# in one [X, Y, Z, 8] array, where a 1-D pass is a few whole-array shifts and
+# the neighbour planes come from the adjacent cells.  Used when the box is
+# small enough; same results and leaf order (x-major) as the sorted form.
+_DENSE_MAX_CELLS = 1 << 24
+
+
+def _dense_z(V):
+    D = V | ((V << _U(1)) & ~_Z_LO) | ((V >> _U(1)) & ~_Z_HI)
+    D[:, :, 1:] |= (V[:, :, :-1] >> _U(7)) & _Z_LO
+    D[:, :, :-1] |= (V[:, :, 1:] << _U(7)) & _Z_HI
+    return D
+
+
+def _dense_y(V):
+    D = V | (V << _U(8)) | (V >> _U(8))
+    D[:, 1:] |= V[:, :-1] >> _U(56)
+    D[:, :-1] |= V[:, 1:] << _U(56)
+    return D
+
+
+def _dense_x(V):
+    D = V.copy()
+    D[..., 1:] |= V[..., :-1]
+    D[..., :-1] |= V[..., 1:]
+    D[1:, :, :, 0] |= V[:-1, :, :, 7]
+    D[:-1, :, :, 7] |= V[1:, :, :, 0]
+    return D
+
+
+def _dilate_dense(org, masks, n, neighbours):
+    lc = org.astype(np.int64) >> 3
+    pad = 1 + (int(n) + 7) // 8
+    lo = lc.min(axis=0) - pad
+    dims = lc.max(axis=0) + pad + 1 - lo
+    V = np.zeros((int(dims[0]), int(dims[1]), int(dims[2]), 8), np.uint64)
+    c = lc - lo
+    V[c[:, 0], c[:, 1], c[:, 2]] = masks
+    for _ in range(int(n)):
+        if neighbours == 6:
+            V = _dense_x(V) | _dense_y(V) | _dense_z(V)
+        else:
+            V = _dense_x(_dense_y(_dense_z(V)))
+    live = V.any(axis=3)
+    cells = np.argwhere(live)
+    return ((cells + lo) * 8).astype(np.int32), np.ascontiguousarray(V[live])
+
+
 def dilate(topo, n: int, neighbours: int = 6) -> tuple[np.ndarray, np.ndarray]:
     """dilateActiveValues(n, NN_FACE) (neighbours=6) or
     (n, NN_FACE_EDGE_VERTEX) (neighbours=26) of a topology."""
     if neighbours not in (6, 26):
         raise ValueError("neighbours must be 6 or 26")
     org, masks = _nonempty(*topology_of(topo))
+    if org.shape[0] == 0 or int(n) <= 0:
+        return org, masks
+    org, masks = union([(org, masks)])  # one entry per leaf
+    lc = org.astype(np.int64) >> 3
+    pad = 1 + (int(n) + 7) // 8
+    cells = int(np.prod(lc.max(axis=0) - lc.min(axis=0) + 1 + 2 * pad))
+    if cells <= _DENSE_MAX_CELLS:
+        return _dilate_dense(org, masks, n, neighbours)
     step = dilate_face_once if neighbours == 6 else dilate_box_once
     for _ in range(int(n)):
         org, masks = step(org, masks)
