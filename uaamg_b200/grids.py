@@ -2,8 +2,8 @@
 
 The reference keeps every field in an OpenVDB tree of 8^3 leaves
 (``openvdb::FloatGrid`` / ``Vec3fGrid``; see SIMD_UAAMG/simd_vdb_poisson.h:54-65).
-OpenVDB is not part of this build, so a grid crosses the boundary as its leaf
-list, which is exactly the payload of an OpenVDB ``LeafNode<T,3>``:
+This package does not depend on OpenVDB, so a grid crosses the boundary as its
+leaf list, which is exactly the payload of an OpenVDB ``LeafNode<T,3>``:
 
 * ``origins``  int32 [n, 3]  leaf origins (multiples of 8, index space)
 * ``masks``    uint64 [n, 8] value masks (bit ``off & 63`` of word ``off >> 6``)
