@@ -216,11 +216,93 @@ public:
         m_iteration = it;
     }
 
+    // The call site's whole viscosity step in one C-ABI call (FLIP_vdb.cpp:3178-3219): the rhs and the warm
+    // start built on the device from the velocity, uploaded once, then PCG; returns the solved velocity
+    // float[3][leaf][512] over dofTopology().  Bit-identical to warm_start + pcg_solve.
+    static std::vector<float> solve_velocity(L_with_level& level0, const PackedLeafGrid3& velocity,
+                                             const LeafGrid& solidVelocity, float tolerance, int* iterations = nullptr,
+                                             int maxIterations = 100) {
+        std::vector<float> x = level0.get_zero_vec();
+        uaamg_leaf_grid u = velocity.v[0].view(), v = velocity.v[1].view(), w = velocity.v[2].view();
+        uaamg_leaf_grid s = solidVelocity.view();
+        check(uaamg_viscosity_set_max_iterations(level0.handle(), maxIterations), "set_max_iterations");
+        int it = 0;
+        check(uaamg_viscosity_solve_velocity(level0.handle(), &u, &v, &w, &s, tolerance, x.data(), &it),
+              "viscosity solve_velocity");
+        if (iterations) *iterations = it;
+        return x;
+    }
+
     L_with_level::Ptr m_level0;  // m_matrix_levels[0]
     std::vector<float> m_rhs;
     int m_iteration = 0;
     int m_max_iter = 100;
     int64_t m_ndof = 0;
 };
+
+// ---------------------------------------------------------------------------
+// The steps around the pressure solve of a FLIP substep.
+
+// calculate_face_weights (FLIP_vdb.cpp:2669-2752) on the given topology
+// (origins [n][3], masks [n][8] or empty = all active): float[n][512][3].
+inline std::vector<float> calculate_face_weights(const LeafGrid& solidSdf, const std::vector<int32_t>& origins,
+                                                 const std::vector<uint64_t>& masks) {
+    const int64_t n = (int64_t)(origins.size() / 3);
+    std::vector<float> w((size_t)n * 512 * 3);
+    uaamg_leaf_grid s = solidSdf.view();
+    check(uaamg_face_weights(&s, n, n ? origins.data() : nullptr, masks.empty() ? nullptr : masks.data(),
+                             n ? w.data() : nullptr),
+          "face_weights");
+    return w;
+}
+
+// immerse_liquid_phi_in_solids (FLIP_vdb.cpp:2856-2942), its value passes on
+// the liquid SDF's own leaves: float[n][512].  The two topology dilations of
+// the reference (:2881, :2941) are the caller's.
+inline std::vector<float> immerse_liquid_phi_values(const LeafGrid& solidSdf, const LeafGrid& liquidPhi, float dx) {
+    std::vector<float> out((size_t)liquidPhi.leafCount() * 512);
+    uaamg_leaf_grid s = solidSdf.view(), l = liquidPhi.view();
+    check(uaamg_immerse_liquid_phi(&s, &l, dx, out.empty() ? nullptr : out.data()), "immerse_liquid_phi");
+    return out;
+}
+
+// apply_pressure_gradient (FLIP_vdb.cpp:2571-2667) for one velocity channel
+// with the pressure solved on `level0`; outputs over the channel's leaves.
+struct PressureGradientResult {
+    std::vector<float> velocity, update, reflected;  // [n][512]
+    std::vector<uint64_t> masks;                      // [n][8]: voxels with an update
+};
+inline PressureGradientResult apply_pressure_gradient(LaplacianWithLevel& level0, const LeafGrid& liquidPhi,
+                                                      const LeafGrid& faceWeights, const LeafGrid& solidVelocity,
+                                                      const std::vector<float>& pressure, float dt, int channel,
+                                                      const LeafGrid& velocity, float friction = 0.f) {
+    const size_t n = (size_t)velocity.leafCount();
+    PressureGradientResult r;
+    r.velocity.resize(n * 512);
+    r.update.resize(n * 512);
+    r.reflected.resize(n * 512);
+    r.masks.resize(n * 8);
+    uaamg_leaf_grid a = liquidPhi.view(), b = faceWeights.view(), c = solidVelocity.view(), v = velocity.view();
+    check(uaamg_poisson_apply_pressure_gradient(level0.handle(), &a, &b, &c, pressure.data(), dt, friction, channel,
+                                                &v, r.velocity.data(), r.masks.data(), r.update.data(),
+                                                r.reflected.data()),
+          "apply_pressure_gradient");
+    return r;
+}
+
+// union_extrapolate's layers (vdb_velocity_extrapolator.cpp:611-659) for one
+// channel, after the caller's topology steps: values [n_out][512] and masks
+// [n_out][8] of the channel's leaves extended by the touched ones, updated in
+// place; fill_leaf / fill_masks: per leaf with voxels to fill, its index and
+// those voxels.
+inline void extrapolate_channel(int nLayer, const std::vector<int32_t>& outOrigins, std::vector<float>& values,
+                                std::vector<uint64_t>& masks, const std::vector<int32_t>& fillLeaf,
+                                const std::vector<uint64_t>& fillMasks) {
+    const int64_t nOut = (int64_t)(outOrigins.size() / 3), nFill = (int64_t)fillLeaf.size();
+    check(uaamg_extrapolate_channel(nLayer, nOut, nOut ? outOrigins.data() : nullptr,
+                                    nOut ? values.data() : nullptr, nOut ? masks.data() : nullptr, nFill,
+                                    nFill ? fillLeaf.data() : nullptr, nFill ? fillMasks.data() : nullptr),
+          "extrapolate_channel");
+}
 
 }  // namespace simd_uaamg_b200
