@@ -87,8 +87,9 @@ def test_cpp_facade_compiles():
 
 def test_cpp_facade_links_and_checks_arguments(cuda_lib, tmp_path):
     """A C++ call site built against the facade links with the library and
-    gets the library's argument errors as exceptions; calls with nothing to
-    do return without touching a device."""
+    gets the library's argument errors as status codes (never exceptions: the
+    program is built with -fno-exceptions); calls with nothing to do return
+    without touching a device."""
     from uaamg_b200 import _lib
     prog = tmp_path / "facade.cpp"
     prog.write_text(r'''
@@ -99,29 +100,35 @@ int main() {
     std::vector<int32_t> org = {0, 0, 0, 8, 0, 0};
     std::vector<float> vals(2 * 512, 0.f);
     std::vector<uint64_t> masks(2 * 8, 0);
-    extrapolate_channel(3, org, vals, masks, {}, {});             // no voxel to fill
-    int caught = 0;
-    try {
-        extrapolate_channel(3, org, vals, masks, {0, 0}, std::vector<uint64_t>(16, 1));  // a leaf listed twice
-    } catch (const std::runtime_error& e) { caught += std::string(e.what()).find("twice") != std::string::npos; }
-    try {
-        std::vector<int32_t> bad = {0, 0, 0, 4, 0, 0};
-        extrapolate_channel(3, bad, vals, masks, {1}, std::vector<uint64_t>(8, 1));
-    } catch (const std::runtime_error&) { caught += 1; }
+    int ok = extrapolate_channel(3, org, vals, masks, {}, {});             // no voxel to fill
+    int errors = 0;
+    int rc = extrapolate_channel(3, org, vals, masks, {0, 0}, std::vector<uint64_t>(16, 1));  // a leaf listed twice
+    errors += (rc == UAAMG_ERR_INVALID_ARGUMENT && lastError().find("twice") != std::string::npos);
+    std::vector<int32_t> bad = {0, 0, 0, 4, 0, 0};
+    rc = extrapolate_channel(3, bad, vals, masks, {1}, std::vector<uint64_t>(8, 1));
+    errors += (rc == UAAMG_ERR_INVALID_ARGUMENT);
     LeafGrid solid;
     solid.background[0] = 1.f;
-    std::vector<float> w = calculate_face_weights(solid, {}, {});  // empty topology
+    int st = 1;
+    std::vector<float> w = calculate_face_weights(solid, {}, {}, &st);  // empty topology
     LeafGrid liquid;
     std::vector<float> im = immerse_liquid_phi_values(solid, liquid, 0.1f);  // no liquid leaves
-    std::printf("%d %zu %zu\n", caught, w.size(), im.size());
-    return caught == 2 ? 0 : 1;
+    LeafGrid phi;  // components 1, but the face weights need 3: a factory error, an empty pointer
+    int cst = 0;
+    LaplacianWithLevel::Ptr lap = LaplacianWithLevel::createPressurePoissonLaplacian(phi, phi, 1.f, 0.1f, &cst);
+    errors += (!lap && cst < 0);
+    PoissonSolver solver(lap);
+    std::vector<float> p, b;
+    errors += (solver.solveMultigridPCG(p, b) == UAAMG_ERR_INVALID_ARGUMENT);
+    std::printf("%d %d %d %zu %zu\n", ok, errors, st, w.size(), im.size());
+    return errors == 4 ? 0 : 1;
 }
 ''')
     exe = tmp_path / "facade"
     libdir = os.path.dirname(_lib.LIB_PATH)
-    r = subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe),
-                        _lib.LIB_PATH, f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    r = subprocess.run(["g++", "-std=c++17", "-fno-exceptions", "-I", os.path.join(ROOT, "include"), str(prog),
+                        "-o", str(exe), _lib.LIB_PATH, f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.split() == ["2", "0", "0"]
+    assert r.stdout.split() == ["0", "4", "0", "0", "0"]
