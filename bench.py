@@ -1,26 +1,28 @@
 #!/usr/bin/env python
 """UAAMG-PCG benchmark: ms per solve.
 
-Headline workload (one "step" = one viscosity solve as at FLIP_vdb's call site,
-FLIP_vdb.cpp:3170-3208): the 128^3 domain, dx = 1/128, liquid = {y < 0.4} U
-sphere(r 0.15 at (0.5, 0.7, 0.5)), domain walls solid, face velocities
-U[-1,1] (seed 1), constant viscosity 1e3, dt = 1/240, rho = 1; build the
-level-0 viscosity matrix and the multigrid hierarchy, the right-hand side and
-the warm start (velocity at the DOFs), and run UAAMG-PCG to 1e-6 relative
-inf-norm residual (simd_viscosity3d::pcg_solve).
+Headline workload (one "step" = one pressure projection solve as at FLIP_vdb's
+call site, FLIP_vdb.cpp:3118-3168): the 128^3 domain, dx = 1/128, liquid =
+{y < 0.4} U sphere(r 0.15 at (0.5, 0.7, 0.5)), domain walls solid (face
+fraction 0), free surface as Dirichlet p = 0 with ghost-fluid fractions from the
+SDF, rhs = negative divergence of face velocities U[-1,1] (seed 0), dt = 1; build
+the level-0 matrix, the multigrid hierarchy and the right-hand side, and run
+UAAMG-PCG (scheduled relaxed Jacobi) from a zero pressure to 1e-7 relative
+inf-norm residual (PoissonSolver::solveMultigridPCG).
 
-Secondary (the "poisson" object of the same line): the plain pressure Poisson
-solve on the same geometry (face velocities seed 0, dt = 1) to 1e-7, as at
-FLIP_vdb.cpp:3118-3168.
+Secondary objects of the same line: the plain variational viscosity solve on
+the same geometry ("viscosity"), the batched, mixed-precision and served forms,
+and the projection steps around the solve.
 
   value      device-resident inputs (torch CUDA tensors) through the C ABI
+             (uaamg_poisson_create_with_rhs, uaamg_poisson_solve_pcg_resident_device)
   e2e        the same step through the host-pointer C ABI from pinned host
-             memory (uaamg_viscosity_create, then uaamg_viscosity_solve_velocity:
-             the velocity in, the solved velocity out), host<->device copies
-             inside the timed region
+             memory (uaamg_poisson_create_with_rhs with host grids, then
+             uaamg_poisson_solve_pcg_resident: the pressure back to the host),
+             host<->device copies inside the timed region
   cpu_baseline / --impl reference
-             the CPU restatement of the reference's SIMD solvers (oracle/),
-             OpenMP over all host cores, on a bounded sample of solves
+             the CPU restatement of the reference's SIMD solver (oracle/),
+             OpenMP over all host cores, full solves of the same workload
 
 Multi-GPU: every rank solves its own independent instances (replicas; no
 collective on the solve path); the step time is the max over ranks and value
@@ -43,9 +45,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "UAAMG-PCG ms/solve to 1e-7 rel-res (plain vs batched/mixed), p99 served latency"
 UNIT = "ms/solve"
-WORKLOAD = ("plain variational viscosity 128^3, liquid y<0.4 + sphere r0.15, walls solid, U[-1,1] face velocities "
-            "seed 1, mu 1e3, dt 1/240, rho 1, rel-res 1e-6, warm start = velocity")
-POISSON_WORKLOAD = "plain pressure Poisson 128^3, liquid y<0.4 + sphere r0.15, walls solid, U[-1,1] face velocities seed 0"
+POISSON_WORKLOAD = ("plain pressure Poisson 128^3, dx 1/128, liquid y<0.4 + sphere r0.15 at (0.5,0.7,0.5), walls solid, "
+                    "ghost-fluid free surface, rhs = -div of U[-1,1] face velocities seed 0, dt 1, rel-res 1e-7, "
+                    "zero initial pressure")
 
 
 def _peaks():
@@ -193,27 +195,29 @@ def cpu_baseline(fn, sc, what: str, budget_s: float = 12.0, min_samples: int = 3
 
 
 def run_reference(args, rank, ws):
-    """--impl reference: the CPU restatement of the reference's solver (rank 0 only)."""
+    """--impl reference: the CPU restatement of the reference's solver on the
+    headline workload (rank 0 only; the other ranks exit without work)."""
     if rank != 0:
         return
     from uaamg_b200 import scenes
-    sc = scenes.plain_viscosity_scene(n=args.n, seed=1)
+    sc = scenes.plain_poisson_scene(n=args.n, seed=0)
     threads = _threads()
     for _ in range(args.warmup):
-        cpu_visc_solve_once(sc, threads)
+        cpu_solve_once(sc, threads)
     times, iters = [], []
     for _ in range(args.steps):
-        dt, it, _ = cpu_visc_solve_once(sc, threads)
+        dt, it, _ = cpu_solve_once(sc, threads)
         times.append(dt)
         iters.append(it)
     ms = sum(times) / len(times) * 1e3
     line = {"metric": METRIC, "value": round(ms, 3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "n": args.n, "iterations": iters[0]},
+            "config": poisson_config(args),
+            "solve": {"pcg_iterations": iters[0]},
             "cpu_baseline": {"value": round(ms, 3), "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} full solves (build+rhs+warm start+PCG), mean; CPU restatement "
-                                       f"oracle/viscosity_oracle.c (the reference needs OpenVDB/TBB/Eigen, absent)"},
+                             "sample": f"{args.steps} full solves (build+rhs+PCG), mean; CPU restatement "
+                                       f"oracle/poisson_oracle.c (the reference needs OpenVDB/TBB/Eigen, absent)"},
             "e2e": {"value": round(ms, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -253,6 +257,198 @@ def _visc_pass_bytes(label: str, ndof_level: list[int], ndof_c: list[list[int]])
     if parts[1] == "prolong":
         return 8.5 * ndof_level[lv]
     return None
+
+
+def poisson_config(args) -> dict:
+    """The headline workload's configuration; both arms print the same dict."""
+    return {"workload": POISSON_WORKLOAD, "n": args.n, "rel_tol": 1e-7, "smoother": "scheduled relaxed Jacobi",
+            "step": "build level-0 matrix + multigrid hierarchy + rhs, UAAMG-PCG from a zero pressure",
+            "l2": "flushed before every timed step (256 MiB write)", "parallelism": "replicas"}
+
+
+class PoissonBytes:
+    """Algorithmic bytes per launch of the Poisson solve's kernel classes (the
+    labels of the event-timed profile): every array a kernel must touch,
+    counted once per DOF of its level at 4 B; the coefficient arrays (diag,
+    1/diag, c_x, c_y, c_z) only for DOF in leaves where they are stored (a
+    trimmed leaf holds the default and is not read); halo re-reads and
+    inactive voxels not credited; a restriction writes 4 B per 8 fine DOF, a
+    prolongation reads as much."""
+
+    TRIM_DIAG, TRIM_X, TRIM_Y, TRIM_Z = 1, 2, 4, 8
+
+    def __init__(self, lap):
+        self.levels = []
+        for l in range(lap.num_levels()):
+            _, masks = lap.dof_topology(l)
+            dof = np.array([sum(bin(int(w)).count("1") for w in row) for row in masks], np.int64)
+            _, flags = lap.coefficients(l)
+            fl = flags.astype(np.int64)
+            stored = {k: int(dof[(fl & bit) == 0].sum()) for k, bit in
+                      (("diag", self.TRIM_DIAG), ("cx", self.TRIM_X), ("cy", self.TRIM_Y), ("cz", self.TRIM_Z))}
+            self.levels.append((int(dof.sum()), stored))
+
+    def _coef(self, l, with_inv: bool) -> float:
+        n, st = self.levels[l]
+        b = 4.0 * (st["diag"] + st["cx"] + st["cy"] + st["cz"])
+        return b + (4.0 * st["diag"] if with_inv else 0.0)
+
+    def launch_bytes(self, label: str):
+        parts = label.split()
+        if not parts or not parts[0].startswith("L") or not parts[0][1:].isdigit():
+            return None
+        l = int(parts[0][1:])
+        if l >= len(self.levels):
+            return None
+        n = float(self.levels[l][0])
+        kind = " ".join(parts[1:]).replace(" staged", "")
+        dot = 4.0 * n if kind.endswith("+dot") else 0.0
+        kind = kind.replace("+dot", "")
+        if kind == "jacobi":                     # x, b, out + coefficients and 1/diag
+            return 12.0 * n + self._coef(l, True) + dot
+        if kind == "jacobi+first":               # b, out (x computed from b) + coefficients and 1/diag
+            return 8.0 * n + self._coef(l, True) + dot
+        if kind == "jacobi+prolong":             # x, b, out, coarse x + coefficients and 1/diag
+            return 12.5 * n + self._coef(l, True) + dot
+        if kind == "residual+restrict":          # x, b + coefficients, coarse rhs
+            return 8.5 * n + self._coef(l, False)
+        if kind == "materialize+first":          # b, 1/diag, out
+            return 8.0 * n + 4.0 * self.levels[l][1]["diag"]
+        if kind == "materialize+prolong":        # x in place, coarse x
+            return 8.5 * n
+        if kind == "pcg Ap":                     # p, q + coefficients (+ p.q)
+            return 8.0 * n + self._coef(l, False)
+        if kind == "pcg r update+absmax":        # q, r in place
+            return 12.0 * n
+        if kind == "pcg x,p update":             # z, p in place, x in place
+            return 20.0 * n
+        return None
+
+    @staticmethod
+    def ncu_tag(label: str) -> str:
+        """The kernel name the committed ncu summaries use for this class."""
+        if "jacobi staged" in label:
+            return "k_sweep_staged<0>"
+        return label
+
+
+VISC_WORKLOAD = ("plain variational viscosity 128^3, liquid y<0.4 + sphere r0.15, walls solid, U[-1,1] face velocities "
+                 "seed 1, mu 1e3, dt 1/240, rho 1, rel-res 1e-6, warm start = velocity")
+
+
+def run_viscosity(args, dev, stream, timed, max_over_ranks, ws, rank, vsc, vdg, pinned):
+    """The plain variational viscosity solve (FLIP_vdb.cpp:3170-3208): build the
+    level-0 matrix and the hierarchy, the rhs and the warm start (the velocity
+    at the DOFs), UAAMG-PCG to 1e-6.  value: device-resident grids; e2e: the
+    host-pointer C ABI from pinned memory (uaamg_viscosity_create, then
+    uaamg_viscosity_solve_velocity: the velocity in, the solved velocity out)."""
+    import torch
+    from uaamg_b200.viscosity import L_with_level, simd_viscosity3d
+    vstats = {"launches": 0, "iters": [], "status": []}
+
+    def vstep_device():
+        lv = L_with_level.create_viscosity_matrix(vdg["viscosity"], vdg["liquid_phi"], vdg["solid_phi"], vsc.dt,
+                                                  vsc.rho, vsc.dx)
+        lv.set_stream(stream.cuda_stream)
+        n = lv.leaf_count(0)
+        rhs = torch.empty((3, n, 512), dtype=torch.float32, device=dev)
+        lv.build_rhs(vdg["u"], vdg["v"], vdg["w"], vdg["solid_velocity"], out=rhs)
+        x = torch.empty_like(rhs)
+        lv.gather_velocity(vdg["u"], vdg["v"], vdg["w"], out=x)
+        s = simd_viscosity3d(lv)
+        st = s.pcg_solve(x, 1e-6, rhs)
+        vstats["launches"] += s.kernel_launches
+        vstats["iters"].append(s.m_iteration)
+        vstats["status"].append(st)
+        return lv, x
+
+    vkeys = ("liquid_phi", "solid_phi", "viscosity", "u", "v", "w", "solid_velocity")
+    vhg = {k: pinned(getattr(vsc, k)) for k in vkeys}
+    vhost = {}
+
+    def vstep_host():
+        lv = L_with_level.create_viscosity_matrix(vhg["viscosity"], vhg["liquid_phi"], vhg["solid_phi"], vsc.dt,
+                                                  vsc.rho, vsc.dx)
+        n = lv.leaf_count(0)
+        if vhost.get("n") != n:
+            vhost["x_t"] = torch.empty((3, n, 512), dtype=torch.float32).pin_memory()
+            vhost["x"], vhost["n"] = vhost["x_t"].numpy(), n
+        s = simd_viscosity3d(lv)
+        st, _ = s.solve_velocity(vhg["u"], vhg["v"], vhg["w"], vhg["solid_velocity"], 1e-6, out=vhost["x"])
+        vstats["launches"] += s.kernel_launches
+        return lv, st
+
+    for _ in range(args.warmup):
+        vstep_device()
+    vstats.update(launches=0, iters=[], status=[])
+    t_dev = timed(vstep_device, args.steps)
+    launches = vstats["launches"]
+    viters, vstatus = list(vstats["iters"]), list(vstats["status"])
+    for _ in range(args.warmup):
+        vstep_host()
+    t_host = timed(vstep_host, args.steps)
+    t_dev, t_host = max_over_ranks(t_dev, t_host)
+    total = args.steps * ws
+    value, e2e = t_dev / total, t_host / total
+
+    # per-kernel device times (event pairs, host-driven loop) for the roofline
+    lv, _ = vstep_device()
+    n0 = lv.leaf_count(0)
+    rhs = torch.empty((3, n0, 512), dtype=torch.float32, device=dev)
+    lv.build_rhs(vdg["u"], vdg["v"], vdg["w"], vdg["solid_velocity"], out=rhs)
+    x0 = torch.empty_like(rhs)
+    lv.gather_velocity(vdg["u"], vdg["v"], vdg["w"], out=x0)
+    s = simd_viscosity3d(lv)
+    prof = s.profile_pcg(x0.clone(), rhs, 1e-6)
+    levels = lv.num_levels()
+    ndof = [lv.num_dof(l) for l in range(levels)]
+    ndof_c = []
+    for l in range(levels):
+        _, m = lv.topology(l)
+        ndof_c.append([int(sum(bin(int(w)).count("1") for w in m[c].reshape(-1))) for c in range(3)])
+    # The dominant kernel is k_vapply in its red/black GS modes (all levels);
+    # the roofline is quoted on the level-0 red pass of channel 0 (the launch
+    # the committed ncu capture measures), the all-level aggregate beside it.
+    gs = [(k, v) for k, v in prof.items() if " red_gs " in k or " black_gs " in k]
+    gs_bytes = sum(_visc_pass_bytes(k, ndof, ndof_c) * v[1] for k, v in gs)
+    gs_ms = sum(v[0] for k, v in gs)
+    prof_ms = sum(v[0] for v in prof.values())
+    dom_label = "L0 red_gs c0"
+    dom_bytes = _visc_pass_bytes(dom_label, ndof, ndof_c)
+    l0 = [(k, v) for k, v in gs if k.startswith("L0 ")]
+    l0_bytes = sum(_visc_pass_bytes(k, ndof, ndof_c) * v[1] for k, v in l0)
+    l0_ms = sum(v[0] for k, v in l0)
+    peak, peak_kind = _peaks()
+    t_ms, cnt = prof.get(dom_label, (0.0, 0))
+    achieved = dom_bytes / (t_ms / cnt * 1e-3) / 1e9 if (dom_bytes and cnt) else None
+    vec_bytes = 3 * 4 * 512 * n0
+    out = {"workload": VISC_WORKLOAD, "value": round(value, 4), "unit": UNIT,
+           "e2e": {"value": round(e2e, 4), "unit": UNIT,
+                   # create: viscosity, liquid SDF (+mask), solid SDF; solve: the three velocity channels and the
+                   # solid velocity, once
+                   "h2d_bytes_per_step": int(_grid_bytes(vsc.viscosity, vsc.liquid_phi, vsc.solid_phi)
+                                             + _grid_bytes(vsc.u, vsc.v, vsc.w, vsc.solid_velocity)),
+                   "d2h_bytes_per_step": int(vec_bytes)},
+           "ndof": ndof, "ndof_per_channel_l0": ndof_c[0], "levels": levels, "pcg_iterations": viters[0],
+           "status": "SUCCESS" if all(x == 0 for x in vstatus) else "FAILED",
+           "step": "create viscosity matrix+hierarchy, rhs, warm start, UAAMG-PCG",
+           "solves_per_s": round(1e3 / value, 2),
+           "roofline": {"bound": "hbm", "kernel": f"k_vapply<RED_GS> level 0, channel 0 ({n0} CTAs)",
+                        "achieved": round(achieved, 1) if achieved else None, "peak": peak,
+                        "peak_kind": peak_kind, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4) if achieved else None,
+                        "traffic": _traffic_from_profile("k_vapply<3>"), "algorithmic_bytes_per_launch": dom_bytes,
+                        "avg_launch_us": round(t_ms / cnt * 1e3, 2) if cnt else None,
+                        "level0_rbgs_GBps": round(l0_bytes / (l0_ms * 1e-3) / 1e9, 1) if l0_ms else None,
+                        "all_levels_rbgs_GBps": round(gs_bytes / (gs_ms * 1e-3) / 1e9, 1) if gs_ms else None,
+                        "rbgs_share_of_solve": round(gs_ms / prof_ms, 3) if prof_ms else None},
+           "kernel_profile_ms": {k: [round(v[0], 4), v[1]] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+           "_launches": int(launches)}
+    if rank == 0 and not args.no_cpu_baseline and ws == 1:
+        out["cpu_baseline"] = cpu_baseline(cpu_visc_solve_once, vsc,
+                                           "oracle/viscosity_oracle.c (build+rhs+warm start+PCG)",
+                                           budget_s=20.0, min_samples=2, max_samples=10)
+    return out
 
 
 BATCH_WORKLOAD = ("batched Poisson: instance i = cubic box of side from {32,64,96,128,192} (seed i), 1-6 spheres "
@@ -405,6 +601,20 @@ def run_mixed(args, dev, stream, timed, max_over_ranks, ws):
         d = torch.linalg.vector_norm((sols[form] - sols["fp32"]).double())
         out[form]["rel_diff_vs_fp32"] = float(d / torch.linalg.vector_norm(sols["fp32"].double()))
         out[form]["speedup_vs_fp32"] = round(out["fp32"]["ms_per_solve"] / out[form]["ms_per_solve"], 3)
+    # every form's error against the FP64 reference solution of the same system (flexible FP64 PCG to a true
+    # relative 2-norm residual of 1e-12, uaamg_poisson_solve_fp64_reference)
+    x64 = torch.empty(rhs.shape, dtype=torch.float64, device=dev)
+    t0 = time.perf_counter()
+    st64, it64, res64 = solver.solve_fp64_reference(rhs, x64, 1e-12, 200)
+    torch.cuda.synchronize()
+    out["fp64_reference"] = {"status": "SUCCESS" if st64 == 0 else "FAILED", "iterations": it64,
+                             "true_rel_residual_2norm": res64, "s_host_wall": round(time.perf_counter() - t0, 3),
+                             "method": "flexible FP64 PCG on the FP32-assembled level-0 matrix, FP32 W-cycle "
+                                       "preconditioner on the scaled residual, stop at |b-Ax|_2 <= 1e-12 |b|_2"}
+    n64 = torch.linalg.vector_norm(x64)
+    for form in ("fp32", "fp16", "bf16"):
+        out[form]["rel_err_vs_fp64"] = float(torch.linalg.vector_norm(sols[form].double() - x64) / n64)
+    del x64
     out["step"] = "zero initial guess, solve to rel-res 1e-7 (hierarchy, rhs resident)"
     out["_launches"] = int(launches)
     del lap, solver, sols
@@ -638,7 +848,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-poisson", action="store_true", help="skip the secondary Poisson measurement")
+    ap.add_argument("--no-viscosity", action="store_true", help="skip the secondary viscosity measurement")
     ap.add_argument("--no-projection", action="store_true",
                     help="skip the face-weight and pressure-gradient measurement")
     ap.add_argument("--batch", type=int, default=64, help="instances of the batched Poisson measurement (0 = skip)")
@@ -805,157 +1015,84 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         return tuple(float(v) for v in tt)
 
-    # ================= headline: variational viscosity =================
-    vstats = {"launches": 0, "iters": [], "status": []}
+    # ================= headline: plain pressure Poisson (the metric's configuration) =================
+    pstats = {"launches": 0, "iters": [], "status": []}
 
-    def vstep_device():
-        lv = L_with_level.create_viscosity_matrix(vdg["viscosity"], vdg["liquid_phi"], vdg["solid_phi"], vsc.dt,
-                                                  vsc.rho, vsc.dx)
-        lv.set_stream(stream.cuda_stream)
-        n = lv.leaf_count(0)
-        rhs = torch.empty((3, n, 512), dtype=torch.float32, device=dev)
-        lv.build_rhs(vdg["u"], vdg["v"], vdg["w"], vdg["solid_velocity"], out=rhs)
-        x = torch.empty_like(rhs)
-        lv.gather_velocity(vdg["u"], vdg["v"], vdg["w"], out=x)
-        s = simd_viscosity3d(lv)
-        st = s.pcg_solve(x, 1e-6, rhs)
-        vstats["launches"] += s.kernel_launches
-        vstats["iters"].append(s.m_iteration)
-        vstats["status"].append(st)
-        return lv, x
+    def pstep_device():
+        # createPressurePoissonLaplacian + PoissonSolver + createPressurePoissonRightHandSide in one call
+        # (device-resident grids), then solveMultigridPCG from a zero pressure
+        lap = LaplacianWithLevel.createPressurePoissonLaplacianWithRhs(
+            pdg["phi"], pdg["face_weights"], pdg["vx"], pdg["vy"], pdg["vz"], pdg["solid_velocity"], psc.dt,
+            psc.dx, stream=stream.cuda_stream)
+        solver = PoissonSolver(lap)
+        p = torch.empty((lap.leaf_count(0), 512), dtype=torch.float32, device=dev)
+        st = solver.solveMultigridPCGResident(p)
+        pstats["launches"] += solver.kernel_launches
+        pstats["iters"].append(solver.mIterationTaken)
+        pstats["status"].append(st)
+        return lap, p
 
-    vhg = {k: pinned(getattr(vsc, k)) for k in vkeys}
-    vhost = {}
+    phg = {k: pinned(getattr(psc, k)) for k in pkeys}
+    phost = {}
 
-    def vstep_host():
-        lv = L_with_level.create_viscosity_matrix(vhg["viscosity"], vhg["liquid_phi"], vhg["solid_phi"], vsc.dt,
-                                                  vsc.rho, vsc.dx)
-        n = lv.leaf_count(0)
-        if vhost.get("n") != n:
-            vhost["x_t"] = torch.empty((3, n, 512), dtype=torch.float32).pin_memory()
-            vhost["x"], vhost["n"] = vhost["x_t"].numpy(), n
-        # the call site's viscosity step in one call: velocity uploaded once, rhs and warm start on the device,
-        # the solved velocity returned
-        s = simd_viscosity3d(lv)
-        st, _ = s.solve_velocity(vhg["u"], vhg["v"], vhg["w"], vhg["solid_velocity"], 1e-6, out=vhost["x"])
-        vstats["launches"] += s.kernel_launches
-        return lv, st
+    def pstep_host():
+        # the same step through the host-pointer C ABI: the pinned input grids go up once each, the pressure
+        # comes back to pinned host memory
+        lap = LaplacianWithLevel.createPressurePoissonLaplacianWithRhs(
+            phg["phi"], phg["face_weights"], phg["vx"], phg["vy"], phg["vz"], phg["solid_velocity"], psc.dt,
+            psc.dx, stream=stream.cuda_stream)
+        solver = PoissonSolver(lap)
+        n = lap.leaf_count(0)
+        if phost.get("n") != n:
+            phost["p_t"] = torch.empty((n, 512), dtype=torch.float32).pin_memory()
+            phost["p"], phost["n"] = phost["p_t"].numpy(), n
+        st = solver.solveMultigridPCGResident(phost["p"])
+        pstats["launches"] += solver.kernel_launches
+        return lap, st
 
     for _ in range(args.warmup):
-        vstep_device()
-    vstats.update(launches=0, iters=[], status=[])
+        pstep_device()
+    pstats.update(launches=0, iters=[], status=[])
     clk = ClockSampler(local)
     clk.start()
-    t_dev = timed(vstep_device, args.steps)
+    tp_dev = timed(pstep_device, args.steps)
     clocks = clk.stop()
-    launches = vstats["launches"]
-    viters, vstatus = list(vstats["iters"]), list(vstats["status"])
+    launches = pstats["launches"]
+    piters, pstatus = list(pstats["iters"]), list(pstats["status"])
     for _ in range(args.warmup):
-        vstep_host()
-    t_host = timed(vstep_host, args.steps)
-    t_dev, t_host = max_over_ranks(t_dev, t_host)
+        pstep_host()
+    tp_host = timed(pstep_host, args.steps)
+    tp_dev, tp_host = max_over_ranks(tp_dev, tp_host)
     total = args.steps * ws
-    value, e2e = t_dev / total, t_host / total
+    value, e2e = tp_dev / total, tp_host / total
 
-    # per-kernel device times (event pairs, host-driven loop) for the roofline
-    lv, _ = vstep_device()
-    n0 = lv.leaf_count(0)
-    rhs = torch.empty((3, n0, 512), dtype=torch.float32, device=dev)
-    lv.build_rhs(vdg["u"], vdg["v"], vdg["w"], vdg["solid_velocity"], out=rhs)
-    x0 = torch.empty_like(rhs)
-    lv.gather_velocity(vdg["u"], vdg["v"], vdg["w"], out=x0)
-    s = simd_viscosity3d(lv)
-    prof = s.profile_pcg(x0.clone(), rhs, 1e-6)
-    levels = lv.num_levels()
-    ndof = [lv.num_dof(l) for l in range(levels)]
-    ndof_c = []
-    for l in range(levels):
-        _, m = lv.topology(l)
-        ndof_c.append([int(sum(bin(int(w)).count("1") for w in m[c].reshape(-1))) for c in range(3)])
-    # The dominant kernel is k_vapply in its red/black GS modes (all levels).
-    # Its bandwidth-relevant launches are the level-0 passes: the roofline is
-    # quoted on the level-0 red pass of channel 0 (the launch the committed ncu
-    # capture measures), and the all-level aggregate is reported beside it.
-    gs = [(k, v) for k, v in prof.items() if " red_gs " in k or " black_gs " in k]
-    gs_bytes = sum(_visc_pass_bytes(k, ndof, ndof_c) * v[1] for k, v in gs)
-    gs_ms = sum(v[0] for k, v in gs)
-    prof_ms = sum(v[0] for v in prof.values())
-    dom_label = "L0 red_gs c0"
-    dom_bytes = _visc_pass_bytes(dom_label, ndof, ndof_c)
-    l0 = [(k, v) for k, v in gs if k.startswith("L0 ")]
-    l0_bytes = sum(_visc_pass_bytes(k, ndof, ndof_c) * v[1] for k, v in l0)
-    l0_ms = sum(v[0] for k, v in l0)
+    # per-kernel device times of one solve (event pairs around every launch, host-driven loop) for the roofline
+    lap, p_ref = pstep_device()
+    solver = PoissonSolver(lap)
+    rhs_d = lap.copy_rhs(torch.empty_like(p_ref))
+    pprof = solver.profile_pcg(torch.zeros_like(rhs_d), rhs_d)
+    pndof = [lap.num_dof(l) for l in range(lap.num_levels())]
+    pleaves = [lap.leaf_count(l) for l in range(lap.num_levels())]
+    pbytes = PoissonBytes(lap)
     peak, peak_kind = _peaks()
-    t_ms, cnt = prof.get(dom_label, (0.0, 0))
-    achieved = dom_bytes / (t_ms / cnt * 1e-3) / 1e9 if (dom_bytes and cnt) else None
-    traffic = _traffic_from_profile("k_vapply<3>")
-    vec_bytes = 3 * 4 * 512 * n0
-    vcpu = None
+    prof_ms = sum(v[0] for v in pprof.values())
+    ranked = sorted(((k, v) for k, v in pprof.items() if pbytes.launch_bytes(k) is not None), key=lambda kv: -kv[1][0])
+    dom_label, (dom_ms, dom_cnt) = ranked[0]
+    dom_bytes = pbytes.launch_bytes(dom_label)
+    dom_us = dom_ms / dom_cnt * 1e3
+    achieved = dom_bytes / (dom_us * 1e-6) / 1e9
+    agg_bytes = sum(pbytes.launch_bytes(k) * v[1] for k, v in ranked)
+    agg_ms = sum(v[0] for k, v in ranked)
+    pvec = 4 * 512 * pleaves[0]
+    pcpu = None
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
-        vcpu = cpu_baseline(cpu_visc_solve_once, vsc, "oracle/viscosity_oracle.c (build+rhs+warm start+PCG)",
-                            budget_s=20.0, min_samples=2, max_samples=10)
+        pcpu = cpu_baseline(cpu_solve_once, psc, "oracle/poisson_oracle.c (build+rhs+PCG)")
 
-    # ================= secondary: plain pressure Poisson =================
-    poisson = None
-    if not args.no_poisson:
-        pstats = {"launches": 0, "iters": [], "status": []}
-
-        def pstep_device():
-            lap = LaplacianWithLevel.createPressurePoissonLaplacian(pdg["phi"], pdg["face_weights"], psc.dt, psc.dx)
-            solver = PoissonSolver(lap)
-            solver.set_stream(stream.cuda_stream)
-            rhs = torch.empty((lap.leaf_count(0), 512), dtype=torch.float32, device=dev)
-            lap.createPressurePoissonRightHandSide(pdg["face_weights"], pdg["vx"], pdg["vy"], pdg["vz"],
-                                                  pdg["solid_velocity"], psc.dt, out=rhs)
-            p = torch.zeros_like(rhs)
-            st = solver.solveMultigridPCG(p, rhs)
-            pstats["launches"] += solver.kernel_launches
-            pstats["iters"].append(solver.mIterationTaken)
-            pstats["status"].append(st)
-            return lap
-
-        phg = {k: pinned(getattr(psc, k)) for k in pkeys}
-        phost = {}
-
-        def pstep_host():
-            lap = LaplacianWithLevel.createPressurePoissonLaplacian(phg["phi"], phg["face_weights"], psc.dt, psc.dx)
-            solver = PoissonSolver(lap)
-            n = lap.leaf_count(0)
-            if phost.get("n") != n:
-                phost["rhs_t"] = torch.empty((n, 512), dtype=torch.float32).pin_memory()
-                phost["p_t"] = torch.empty((n, 512), dtype=torch.float32).pin_memory()
-                phost["rhs"], phost["p"], phost["n"] = phost["rhs_t"].numpy(), phost["p_t"].numpy(), n
-            lap.createPressurePoissonRightHandSide(phg["face_weights"], phg["vx"], phg["vy"], phg["vz"],
-                                                  phg["solid_velocity"], psc.dt, out=phost["rhs"])
-            phost["p"][:] = 0.0
-            st = solver.solveMultigridPCG(phost["p"], phost["rhs"])
-            pstats["launches"] += solver.kernel_launches
-            return lap, st
-
-        for _ in range(args.warmup):
-            pstep_device()
-        pstats.update(launches=0, iters=[], status=[])
-        tp_dev = timed(pstep_device, args.steps)
-        plaunch = pstats["launches"]
-        piters, pstatus = list(pstats["iters"]), list(pstats["status"])
-        for _ in range(args.warmup):
-            pstep_host()
-        tp_host = timed(pstep_host, args.steps)
-        tp_dev, tp_host = max_over_ranks(tp_dev, tp_host)
-        lap = pstep_device()
-        pvec = 4 * 512 * lap.leaf_count(0)
-        pndof = [lap.num_dof(l) for l in range(lap.num_levels())]
-        poisson = {"workload": POISSON_WORKLOAD, "value": round(tp_dev / total, 4), "unit": UNIT,
-                   "e2e": {"value": round(tp_host / total, 4), "unit": UNIT,
-                           "h2d_bytes_per_step": int(_grid_bytes(psc.phi, psc.face_weights, psc.face_weights, psc.vx,
-                                                                 psc.vy, psc.vz) + 2 * pvec),
-                           "d2h_bytes_per_step": int(2 * pvec)},
-                   "ndof": pndof, "pcg_iterations": piters[0],
-                   "status": "SUCCESS" if all(x == 0 for x in pstatus) else "FAILED",
-                   "gpu_launches": int(plaunch)}
-        launches += plaunch
-        if rank == 0 and not args.no_cpu_baseline and ws == 1:
-            poisson["cpu_baseline"] = cpu_baseline(cpu_solve_once, psc, "oracle/poisson_oracle.c (build+rhs+PCG)")
+    # ================= secondary: plain variational viscosity =================
+    viscosity = None
+    if not args.no_viscosity:
+        viscosity = run_viscosity(args, dev, stream, timed, max_over_ranks, ws, rank, vsc, vdg, pinned)
+        launches += viscosity.pop("_launches")
 
     # ================= batched Poisson: many instances in one graph =================
     batched = None
@@ -980,42 +1117,42 @@ def main():
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(t_dev / args.steps, 4), "higher_is_better": False,
+            "warmup": args.warmup, "ms_per_step": round(tp_dev / args.steps, 4), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": args.n, "ndof": ndof, "ndof_per_channel_l0": ndof_c[0],
-                       "levels": levels, "pcg_iterations": viters[0],
-                       "status": "SUCCESS" if all(x == 0 for x in vstatus) else "FAILED",
-                       "step": "create viscosity matrix+hierarchy, rhs, warm start, UAAMG-PCG "
-                               "(device-resident inputs)",
-                       "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": f"replicas x{ws}", "solves_per_s": round(1e3 / value, 2),
-                       "dof_updates_per_s": round(ndof[0] * (viters[0] + 1) * 1e3 / value, 1)},
+            "config": poisson_config(args),
+            "solve": {"ndof": pndof, "leaves": pleaves, "levels": len(pndof), "pcg_iterations": piters[0],
+                      "status": "SUCCESS" if all(x == 0 for x in pstatus) else "FAILED",
+                      "solves_per_s": round(1e3 / value, 2),
+                      "voxel_updates_per_s": round(pndof[0] * piters[0] * 1e3 / value, 1),
+                      "step": "create level-0 matrix + hierarchy + rhs (uaamg_poisson_create_with_rhs, device-"
+                              "resident grids), then UAAMG-PCG from a zero pressure "
+                              "(uaamg_poisson_solve_pcg_resident_device)"},
             "e2e": {"value": round(e2e, 4), "unit": UNIT,
-                    # create: viscosity, liquid SDF (+mask), solid SDF; solve: the three
-                    # velocity channels and the solid velocity, once
-                    "h2d_bytes_per_step": int(_grid_bytes(vsc.viscosity, vsc.liquid_phi, vsc.solid_phi)
-                                              + _grid_bytes(vsc.u, vsc.v, vsc.w, vsc.solid_velocity)),
-                    # the solved velocity
-                    "d2h_bytes_per_step": int(vec_bytes)},
+                    # uaamg_poisson_create_with_rhs: the liquid SDF, the face weights and the three velocity
+                    # channels (values, origins, masks) once each; the solid velocity grid is empty here
+                    "h2d_bytes_per_step": int(_grid_bytes(psc.phi, psc.face_weights, psc.vx, psc.vy, psc.vz,
+                                                          psc.solid_velocity)),
+                    # the pressure
+                    "d2h_bytes_per_step": int(pvec)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_vapply<RED_GS> level 0, channel 0 (2774 CTAs)",
-                         "achieved": round(achieved, 1) if achieved else None, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4) if achieved else None,
-                         "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
-                         "avg_launch_us": round(t_ms / cnt * 1e3, 2) if cnt else None,
-                         "level0_rbgs_GBps": round(l0_bytes / (l0_ms * 1e-3) / 1e9, 1) if l0_ms else None,
-                         "all_levels_rbgs_GBps": round(gs_bytes / (gs_ms * 1e-3) / 1e9, 1) if gs_ms else None,
-                         "rbgs_share_of_solve": round(gs_ms / prof_ms, 3) if prof_ms else None,
-                         "note": "per-launch times from CUDA event pairs in a host-driven solve; coarse-level "
-                                 "passes (23-560 CTAs) are latency-bound"},
-            "kernel_profile_ms": {k: [round(v[0], 4), v[1]] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            "roofline": {"bound": "hbm", "kernel": f"{dom_label} ({pleaves[int(dom_label[1])]} leaves)",
+                         "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4),
+                         "traffic": _traffic_from_profile(pbytes.ncu_tag(dom_label)),
+                         "algorithmic_bytes_per_launch": round(dom_bytes),
+                         "avg_launch_us": round(dom_us, 2), "launches": dom_cnt,
+                         "share_of_solve": round(dom_ms / prof_ms, 3),
+                         "all_bandwidth_kernels_GBps": round(agg_bytes / (agg_ms * 1e-3) / 1e9, 1),
+                         "note": "the kernel class with the largest device time in one solve (CUDA event pairs "
+                                 "around every launch, host-driven loop); algorithmic bytes: every array the "
+                                 "kernel must touch once per DOF at 4 B, coefficient arrays only where stored"},
+            "kernel_profile_ms": {k: [round(v[0], 4), v[1]] for k, v in sorted(pprof.items(), key=lambda kv: -kv[1][0])},
             "clocks": clocks,
         }
-        if vcpu is not None:
-            line["cpu_baseline"] = vcpu
-        if poisson is not None:
-            line["poisson"] = poisson
+        if pcpu is not None:
+            line["cpu_baseline"] = pcpu
+        if viscosity is not None:
+            line["viscosity"] = viscosity
         if served is not None:
             line["served"] = served
         if mixed is not None:

@@ -82,6 +82,19 @@ int uaamg_poisson_create(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_gri
  * synchronisation), and the stream stays the handle's (uaamg_poisson_set_stream). */
 int uaamg_poisson_create_on_stream(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights, float dt,
                                    float dx, void* stream, uaamg_poisson** out);
+/* The pressure step of FLIP_vdb's solve_pressure_simd (FLIP_vdb.cpp:3132-3148)
+ * up to the solve, in one call: createPressurePoissonLaplacian(liquid_phi,
+ * face_weights, dt) + PoissonSolver(level0) (as uaamg_poisson_create) and
+ * createPressurePoissonRightHandSide(face_weights, vx, vy, vz, solid_velocity,
+ * dt) (simd_vdb_poisson.cpp:101-127), with the rhs kept on the device for
+ * uaamg_poisson_solve_*_resident.  Each host input crosses the bus once (the
+ * face weights feed both the matrix and the rhs), and the velocity uploads run
+ * on a second stream while the hierarchy is built.  Pinned host inputs make
+ * the uploads asynchronous; device inputs (values_on_device) are read in place. */
+int uaamg_poisson_create_with_rhs(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights,
+                                  const uaamg_leaf_grid* vx, const uaamg_leaf_grid* vy, const uaamg_leaf_grid* vz,
+                                  const uaamg_leaf_grid* solid_velocity, float dt, float dx, void* stream,
+                                  uaamg_poisson** out);
 /* ~PoissonSolver / ~LaplacianWithLevel */
 int uaamg_poisson_destroy(uaamg_poisson* h);
 
@@ -124,6 +137,17 @@ int uaamg_poisson_build_rhs_device(uaamg_poisson* h, const uaamg_leaf_grid* face
 int uaamg_poisson_solve_pcg(uaamg_poisson* h, float* pressure, const float* rhs, int* iterations);
 int uaamg_poisson_solve_pcg_device(uaamg_poisson* h, float* d_pressure, const float* d_rhs,
                                    int* iterations);
+/* The rest of solve_pressure_simd (FLIP_vdb.cpp:3143-3157) on a handle made by
+ * uaamg_poisson_create_with_rhs: the pressure set to zero, solveMultigridPCG
+ * (or, after FAILED, solvePureMultigrid) with the rhs built at creation, the
+ * pressure (float[leaf][512] over the level-0 DOF leaves) written to host or
+ * device memory.  Returns as uaamg_poisson_solve_pcg / _solve_mg;
+ * UAAMG_ERR_INVALID_ARGUMENT when the handle holds no rhs. */
+int uaamg_poisson_solve_pcg_resident(uaamg_poisson* h, float* pressure, int* iterations);
+int uaamg_poisson_solve_pcg_resident_device(uaamg_poisson* h, float* d_pressure, int* iterations);
+int uaamg_poisson_solve_mg_resident(uaamg_poisson* h, float* pressure, int* iterations);
+/* The rhs built at creation, into host or device memory (cudaMemcpyDefault). */
+int uaamg_poisson_copy_rhs(uaamg_poisson* h, float* rhs_out);
 /* PoissonSolver::solvePureMultigrid (simd_vdb_poisson.h:163, .cpp:2228-2267) */
 int uaamg_poisson_solve_mg(uaamg_poisson* h, float* pressure, const float* rhs, int* iterations);
 int uaamg_poisson_solve_mg_device(uaamg_poisson* h, float* d_pressure, const float* d_rhs,
@@ -148,11 +172,12 @@ int uaamg_poisson_residual_norm_device(uaamg_poisson* h, const float* d_x, const
  * kept until the process exits) instead of memory allocated per handle;
  * nothing is allocated by the call.  Limit: level 0 may hold at most 262144
  * leaves (134 M voxels); larger levels are rejected with
- * UAAMG_ERR_INVALID_ARGUMENT.  The first call on a device resolves the array's
- * device address (cudaGetSymbolAddress) with that device current; make that
- * first call before any stream capture.  All calls on a device share the one
- * array, so calls whose kernels overlap on the GPU (different streams or
- * handles) race and must be serialised by the caller. */
+ * UAAMG_ERR_INVALID_ARGUMENT.  The array's device address is looked up
+ * (cudaGetSymbolAddress) when the handle is created, with the handle's device
+ * current; the call must be made with that device current too, otherwise it is
+ * rejected with UAAMG_ERR_INVALID_ARGUMENT and nothing is launched.  All calls
+ * on a device share the one array, so calls whose kernels overlap on the GPU
+ * (different streams or handles) race and must be serialised by the caller. */
 int uaamg_poisson_residual_norm_noalloc(uaamg_poisson* h, const float* d_x, const float* d_b, float* d_r,
                                         float* d_norm);
 
@@ -225,6 +250,18 @@ int uaamg_poisson_solve_pcg_mixed_device(uaamg_poisson* h, int precision, float*
  * level-0 matrix (device vectors): out[0], out[1].  An accuracy check with no
  * counterpart in the reference. */
 int uaamg_poisson_true_residual_fp64(uaamg_poisson* h, const float* d_x, const float* d_b, double* out);
+/* FP64 reference solution of the level-0 system A x = b (device pointers:
+ * d_rhs float[leaf][512], d_x double[leaf][512] out), the yardstick the
+ * accuracy of every form is stated against.  A is the matrix of getTriplets
+ * (SIMD_UAAMG/simd_vdb_poisson.cpp:129-206) assembled from the FP32
+ * coefficients, exactly in FP64; flexible PCG in FP64 preconditioned by the
+ * handle's FP32 W-cycle on a power-of-two-scaled residual; stops when the true
+ * residual |b - A x|_2 <= rel_tol |b|_2 (the criterion of Eigen's CG).
+ * Returns UAAMG_SUCCESS, or UAAMG_FAILED after max_iter iterations;
+ * *rel_residual = the final |b - A x|_2 / |b|_2.  No counterpart in the
+ * reference (its harness compares against Eigen solvers). */
+int uaamg_poisson_solve_fp64_reference(uaamg_poisson* h, const float* d_rhs, double* d_x, double rel_tol,
+                                       int max_iter, int* iterations, double* rel_residual);
 
 /* uaamg_poisson_solve_pcg_mixed_device with every kernel launched from a
  * host-driven loop and timed with CUDA events; per kernel class (label, up to

@@ -93,6 +93,7 @@ def lib():
         L.orc_visc_restrict.argtypes = [vp, C.c_int, f32p, f32p]
         L.orc_visc_prolongate.argtypes = [vp, C.c_int, f32p, f32p]
         L.orc_visc_coarsest_solve.argtypes = [vp, f32p, f32p]
+        L.orc_visc_set_coarsest_order.argtypes = [vp, C.c_int]
         L.orc_visc_precondition.argtypes = [vp, f32p, f32p]
         L.orc_visc_pcg.argtypes = [vp, f32p, f32p, C.c_float, C.c_int, C.POINTER(C.c_int),
                                    C.POINTER(C.c_float)]
@@ -346,6 +347,13 @@ class OracleViscosity:
         out = np.array(fine, dtype=np.float32, copy=True)
         lib().orc_visc_prolongate(self._h, fine_level, _f32(coarse), out)
         return out
+
+    ORDER_KERNEL, ORDER_SEQUENTIAL = 0, 1
+
+    def set_coarsest_order(self, order: int):
+        """Summation order of the coarsest CG: ORDER_KERNEL (the CUDA kernel's
+        tree order, the default) or ORDER_SEQUENTIAL (plain sequential sums)."""
+        lib().orc_visc_set_coarsest_order(self._h, int(order))
 
     def coarsest_solve(self, rhs):
         out = self.zeros(self.num_levels - 1)

@@ -170,6 +170,12 @@ void orc_visc_restrict(const orc_visc* h, int fine_level, const float* fine, flo
 /* prolongation<true>: fine += P coarse */
 void orc_visc_prolongate(const orc_visc* h, int fine_level, const float* coarse, float* fine);
 void orc_visc_coarsest_solve(orc_visc* h, const float* rhs, float* out);
+/* Summation order of the viscosity coarsest CG (the reference leaves it to
+ * Eigen): the CUDA kernel's 256-thread tree order with fused vector updates
+ * (the default), or plain sequential sums with separate multiply and add. */
+#define ORC_CG_ORDER_KERNEL 0
+#define ORC_CG_ORDER_SEQUENTIAL 1
+void orc_visc_set_coarsest_order(orc_visc* h, int order);
 /* out = mucycle(0, r, mu=2, for_precon=true, level 0, n=2) */
 void orc_visc_precondition(orc_visc* h, const float* r, float* out);
 /* simd_viscosity3d::pcg_solve (:3691-3754) on x in place.  Returns 0 when

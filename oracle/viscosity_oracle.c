@@ -218,6 +218,7 @@ struct orc_visc {
     int c_n;
     int32_t *c_rowptr, *c_col, *c_row_ch, *c_row_leaf, *c_row_off;
     float *c_val, *c_invdiag, *c_b, *c_x, *c_r, *c_p, *c_z, *c_t;
+    int c_order;            /* summation order of the coarsest CG (ORC_CG_ORDER_*) */
 };
 
 static inline size_t vidx(const vlevel* L, int c, int32_t leaf, int off) {
@@ -998,10 +999,100 @@ static void coarsest_cg(orc_visc* h) {
     }
 }
 
+/* The same CG with the operation order of the CUDA coarsest kernel
+ * (uaamg_b200/csrc/viscosity_kernels.cuh, k_vcoarsest_cg<ROWS>): row i belongs
+ * to thread tid = i % 256 (the k-th row of a thread is tid + 256 k, ROWS rows
+ * per thread by system size); a dot product is every thread's float sum over
+ * its rows, then a shuffle-down tree inside each 32-lane warp, then the same
+ * tree over the 8 warp sums; the vector updates are fused multiply-adds
+ * (x += alpha p, r -= alpha A p, p = z + beta p).  Eigen's own summation order
+ * depends on its vectorisation (and its version is not pinned), so either
+ * order restates the reference's coarsest solve; this one makes the oracle's
+ * whole viscosity PCG reproducible bit for bit on the GPU. */
+#define VCG_NT 256
+static float warp_tree32(const float* lane_in) {
+    /* lane 0 of v += __shfl_down_sync(v, o), o = 16, 8, 4, 2, 1 (a lane
+     * whose source lane is out of range reads its own value) */
+    float a[32], b[32];
+    memcpy(a, lane_in, sizeof(a));
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int l = 0; l < 32; ++l) b[l] = a[l] + (l + o < 32 ? a[l + o] : a[l]);
+        memcpy(a, b, sizeof(a));
+    }
+    return a[0];
+}
+static float block_tree256(const float* part) {
+    float w[32];
+    for (int k = 0; k < 8; ++k) w[k] = warp_tree32(part + 32 * k);
+    for (int k = 8; k < 32; ++k) w[k] = 0.f;
+    return warp_tree32(w);
+}
+static int vcg_rows(int n) {
+    return n <= 2 * VCG_NT ? 2 : (n <= 4 * VCG_NT ? 4 : (n <= 8 * VCG_NT ? 8 : 16));
+}
+static void coarsest_cg_kernel_order(orc_visc* h) {
+    const int n = h->c_n, R = vcg_rows(n), N = R * VCG_NT;
+    /* per row slot j = tid + k * 256 (j >= n: padding, zero) */
+    float* x = (float*)vcalloc((size_t)N, sizeof(float));
+    float* r = (float*)vcalloc((size_t)N, sizeof(float));
+    float* p = (float*)vcalloc((size_t)N, sizeof(float));
+    float* z = (float*)vcalloc((size_t)N, sizeof(float));
+    float* t = (float*)vcalloc((size_t)N, sizeof(float));
+    float* iv = (float*)vcalloc((size_t)N, sizeof(float));
+    float part[VCG_NT], part2[VCG_NT];
+    for (int j = 0; j < n; ++j) { r[j] = h->c_b[j]; iv[j] = h->c_invdiag[j]; }
+#define THREAD_SUM(dst, expr)                                   \
+    for (int tid = 0; tid < VCG_NT; ++tid) {                    \
+        float v_ = 0.f;                                         \
+        for (int k = 0; k < R; ++k) {                           \
+            const int j = tid + k * VCG_NT;                     \
+            v_ = v_ + (expr);                                   \
+        }                                                       \
+        dst[tid] = v_;                                          \
+    }
+    THREAD_SUM(part, r[j] * r[j]);
+    const float rhsNorm2 = block_tree256(part);
+    const float threshold = fmaxf((FLT_EPSILON * FLT_EPSILON) * rhsNorm2, FLT_MIN);
+    if (rhsNorm2 != 0.f && !(rhsNorm2 < threshold)) {
+        for (int j = 0; j < N; ++j) p[j] = iv[j] * r[j];
+        THREAD_SUM(part, r[j] * p[j]);
+        float absNew = block_tree256(part);
+        for (int it = 0; it < 10; ++it) {
+            for (int j = 0; j < N; ++j) {
+                float sacc = 0.f;
+                if (j < n)
+                    for (int k = h->c_rowptr[j]; k < h->c_rowptr[j + 1]; ++k) sacc = sacc + h->c_val[k] * p[h->c_col[k]];
+                t[j] = sacc;
+            }
+            THREAD_SUM(part, p[j] * t[j]);
+            const float alpha = absNew / block_tree256(part);
+            for (int j = 0; j < N; ++j) {
+                x[j] = fmaf(alpha, p[j], x[j]);
+                r[j] = fmaf(-alpha, t[j], r[j]);
+                z[j] = iv[j] * r[j];
+            }
+            THREAD_SUM(part, r[j] * r[j]);
+            THREAD_SUM(part2, r[j] * z[j]);
+            const float rr = block_tree256(part), rz = block_tree256(part2);
+            if (rr < threshold) break;
+            const float absOld = absNew;
+            absNew = rz;
+            const float beta = absNew / absOld;
+            for (int j = 0; j < N; ++j) p[j] = fmaf(beta, p[j], z[j]);
+        }
+    }
+#undef THREAD_SUM
+    for (int j = 0; j < n; ++j) h->c_x[j] = x[j];
+    free(x); free(r); free(p); free(z); free(t); free(iv);
+}
+
+void orc_visc_set_coarsest_order(orc_visc* h, int order) { h->c_order = order; }
+
 void orc_visc_coarsest_solve(orc_visc* h, const float* rhs, float* out) {
     const vlevel* L = &h->lv[h->nlev - 1];
     for (int i = 0; i < h->c_n; ++i) h->c_b[i] = rhs[vidx(L, h->c_row_ch[i], h->c_row_leaf[i], h->c_row_off[i])];
-    coarsest_cg(h);
+    if (h->c_order == ORC_CG_ORDER_SEQUENTIAL) coarsest_cg(h);
+    else coarsest_cg_kernel_order(h);
     for (int i = 0; i < h->c_n; ++i) out[vidx(L, h->c_row_ch[i], h->c_row_leaf[i], h->c_row_off[i])] = h->c_x[i];
 }
 

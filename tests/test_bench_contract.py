@@ -30,7 +30,16 @@ def test_reference_arm_line():
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     cb = line["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
-    assert line["config"]["iterations"] > 0
+    assert line["solve"]["pcg_iterations"] > 0
+    # the same configuration dict as the GPU arm's headline (the metric's plain Poisson case)
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class A:
+        n = 32
+
+    assert line["config"] == bench.poisson_config(A)
+    assert "Poisson" in line["config"]["workload"] and line["config"]["rel_tol"] == 1e-7
 
 
 def test_reference_arm_ranks():

@@ -353,3 +353,97 @@ def test_residual_norm_device(scene64, gpu):
     r = ref.apply(0, "residual", x, rhs)
     assert np.array_equal(dr.cpu().numpy(), r)
     assert float(dn.item()) == ref.abs_max(r)
+
+
+def test_create_with_rhs_one_call_identical(scene64, gpu):
+    """uaamg_poisson_create_with_rhs (matrix, hierarchy and rhs in one call,
+    each input uploaded once) + the resident solve give the same hierarchy,
+    rhs, pressure, iterations and status, bit for bit, as
+    create + createPressurePoissonRightHandSide + solveMultigridPCG; host and
+    device inputs alike; pure multigrid from the resident rhs too."""
+    torch = gpu
+    from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver
+    sc, lap, ref = scene64
+    rhs = lap.createPressurePoissonRightHandSide(sc.face_weights, sc.vx, sc.vy, sc.vz, sc.solid_velocity, sc.dt)
+    s0 = PoissonSolver(lap)
+    p0 = lap.getZeroVectorGrid()
+    st0 = s0.solveMultigridPCG(p0, rhs)
+
+    def on_device(g):
+        d = LeafGrid(origins=g.origins, values=g.values, background=g.background, masks=g.masks)
+        d.values = torch.from_numpy(g.values).cuda()
+        return d
+
+    for dev in (False, True):
+        grids = [getattr(sc, k) for k in ("phi", "face_weights", "vx", "vy", "vz", "solid_velocity")]
+        if dev:
+            grids = [on_device(g) for g in grids]
+        lap1 = LaplacianWithLevel.createPressurePoissonLaplacianWithRhs(*grids, sc.dt, sc.dx)
+        assert lap1.num_levels() == lap.num_levels()
+        for l in range(lap.num_levels()):
+            assert np.array_equal(lap1.dof_index(l), lap.dof_index(l))
+        assert np.array_equal(lap1.copy_rhs(), rhs)
+        s1 = PoissonSolver(lap1)
+        p1 = np.full_like(p0, 3.0)  # the resident solve starts from zero whatever the buffer holds
+        st1 = s1.solveMultigridPCGResident(p1)
+        assert st1 == st0 == 0 and s1.mIterationTaken == s0.mIterationTaken
+        assert np.array_equal(p1, p0)
+        pd = torch.full(p0.shape, 5.0, device="cuda")
+        assert s1.solveMultigridPCGResident(pd) == st0
+        assert np.array_equal(pd.cpu().numpy(), p0)
+    # solvePureMultigrid from the resident rhs = from the same rhs passed in (fresh handles: the coarse
+    # levels of pure multigrid start from what the previous cycle left, as in the reference)
+    lap2 = LaplacianWithLevel.createPressurePoissonLaplacian(sc.phi, sc.face_weights, sc.dt, sc.dx)
+    s2 = PoissonSolver(lap2)
+    pm0 = lap2.getZeroVectorGrid()
+    stm0 = s2.solvePureMultigrid(pm0, rhs)
+    lap3 = LaplacianWithLevel.createPressurePoissonLaplacianWithRhs(sc.phi, sc.face_weights, sc.vx, sc.vy, sc.vz,
+                                                                   sc.solid_velocity, sc.dt, sc.dx)
+    s3 = PoissonSolver(lap3)
+    pm1 = lap3.getZeroVectorGrid()
+    stm1 = s3.solveMultigridPCGResident(pm1, pure_multigrid=True)
+    assert stm0 == stm1 and s3.mIterationTaken == s2.mIterationTaken and np.array_equal(pm0, pm1)
+    # a handle made without the velocities holds no rhs
+    with pytest.raises(Exception):
+        PoissonSolver(lap).solveMultigridPCGResident(lap.getZeroVectorGrid())
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_bottom_cycle_cluster_kernel_identical(gpu, n):
+    """The two visits of the level next to the coarsest and their coarsest
+    solves run as one thread-block-cluster launch (k_bottom) with the level
+    resident in distributed shared memory.  Its preconditioner and PCG results
+    are bit-identical to the launch sequence it replaces (UAAMG_BOTTOM=0 at
+    handle creation), for both Jacobi-family smoothers, and the profile shows
+    the cluster kernel in place of the small-level launches."""
+    import os
+    torch = gpu
+    from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver
+    sc = scenes.plain_poisson_scene(n=n, seed=3)
+    os.environ["UAAMG_BOTTOM"] = "0"
+    try:
+        lap_off = LaplacianWithLevel.createPressurePoissonLaplacian(sc.phi, sc.face_weights, sc.dt, sc.dx)
+    finally:
+        del os.environ["UAAMG_BOTTOM"]
+    lap_on = LaplacianWithLevel.createPressurePoissonLaplacian(sc.phi, sc.face_weights, sc.dt, sc.dx)
+    assert lap_on.num_levels() >= 3
+    rhs = lap_on.createPressurePoissonRightHandSide(sc.face_weights, sc.vx, sc.vy, sc.vz, sc.solid_velocity, sc.dt)
+    lb = lap_on.num_levels() - 2
+    for sm in (PoissonSolver.SmootherOption.ScheduledRelaxedJacobi, PoissonSolver.SmootherOption.WeightedJacobi):
+        s_off, s_on = PoissonSolver(lap_off), PoissonSolver(lap_on)
+        s_off.mSmoother = s_on.mSmoother = sm
+        z_off, z_on = s_off.precondition(rhs), s_on.precondition(rhs)
+        assert np.array_equal(z_off, z_on)
+        for graph in (0, 2):
+            s_off.use_graph = s_on.use_graph = graph
+            p_off, p_on = lap_on.getZeroVectorGrid(), lap_on.getZeroVectorGrid()
+            st_off, st_on = s_off.solveMultigridPCG(p_off, rhs), s_on.solveMultigridPCG(p_on, rhs)
+            assert st_off == st_on == 0 and s_off.mIterationTaken == s_on.mIterationTaken
+            assert np.array_equal(p_off, p_on)
+        d = torch.from_numpy(rhs).cuda()
+        prof_on = s_on.profile_pcg(torch.zeros_like(d), d)
+        prof_off = s_off.profile_pcg(torch.zeros_like(d), d)
+        label = f"L{lb} bottom (2 visits + coarsest)"
+        assert label in prof_on and label not in prof_off
+        assert "coarsest cg" in prof_off and "coarsest cg" not in prof_on
+        assert sum(v[1] for v in prof_on.values()) < sum(v[1] for v in prof_off.values())

@@ -42,6 +42,13 @@ pLG = C.POINTER(LeafGridC)
 EXPORTS = [
     ("uaamg_poisson_create", i32, [pLG, pLG, f32, f32, C.POINTER(vp)]),
     ("uaamg_poisson_create_on_stream", i32, [pLG, pLG, f32, f32, vp, C.POINTER(vp)]),
+    ("uaamg_poisson_create_with_rhs", i32, [pLG, pLG, pLG, pLG, pLG, pLG, f32, f32, vp, C.POINTER(vp)]),
+    ("uaamg_poisson_solve_pcg_resident", i32, [vp, vp, C.POINTER(i32)]),
+    ("uaamg_poisson_solve_pcg_resident_device", i32, [vp, vp, C.POINTER(i32)]),
+    ("uaamg_poisson_solve_mg_resident", i32, [vp, vp, C.POINTER(i32)]),
+    ("uaamg_poisson_copy_rhs", i32, [vp, vp]),
+    ("uaamg_poisson_solve_fp64_reference", i32, [vp, vp, vp, C.c_double, i32, C.POINTER(i32),
+                                                 C.POINTER(C.c_double)]),
     ("uaamg_poisson_destroy", i32, [vp]),
     ("uaamg_poisson_set_smoother", i32, [vp, i32]),
     ("uaamg_poisson_set_max_iterations", i32, [vp, i32]),

@@ -29,6 +29,7 @@
 #include "poisson_build.cuh"
 #include "poisson_kernels.cuh"
 #include "staged_pipe.cuh"
+#include "poisson_bottom.cuh"
 #include "resources.cuh"
 
 using namespace uaamg;
@@ -297,6 +298,14 @@ struct uaamg_poisson {
     int64_t solves = 0;
     MixedData* mixed = nullptr;  // 16-bit hierarchy copy, FP64 coarsest inverse, graph
     int replace_every = 25;      // true-residual replacement interval of the mixed form
+    void* noalloc_scratch = nullptr;  // device address of the allocation-free entry point's array
+    float* rhs0 = nullptr;  // the rhs built by uaamg_poisson_create_with_rhs (level-0 vector)
+    bool rhs_resident = false;
+    // the bottom of the W-cycle in one cluster launch (k_bottom): decided once
+    // per handle; level lb = nlev - 2, P leaves per CTA, a cluster of bot_C
+    int bot_state = -1;  // -1 undecided, 0 not used (or turned off by UAAMG_BOTTOM=0 at creation), 1 used
+    int bot_C = 0, bot_P = 0, bot_rows = 0;
+    size_t bot_smem = 0;
 };
 
 namespace {
@@ -404,11 +413,30 @@ static bool trace_on() {
         }                                                                              \
     } while (0)
 
+struct EventGuard {
+    cudaEvent_t e = nullptr;
+    ~EventGuard() {
+        if (e) cudaEventDestroy(e);
+    }
+};
+
+// The face-velocity inputs of the right-hand side, when the hierarchy build
+// also builds it (uaamg_poisson_create_with_rhs).
+struct RhsInputs {
+    const uaamg_leaf_grid *vx, *vy, *vz, *sv;
+};
+
 static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const uaamg_leaf_grid* fw, float dt,
-                            float dx) {
+                            float dx, const RhsInputs* ri = nullptr) {
     double trace_t0 = trace_now();
     check_grid(phi, 1, "liquid_phi");
     check_grid(fw, 3, "face_weights");
+    if (ri) {
+        check_grid(ri->vx, 1, "vx");
+        check_grid(ri->vy, 1, "vy");
+        check_grid(ri->vz, 1, "vz");
+        check_grid(ri->sv, 3, "solid_velocity");
+    }
     if (!(dx > 0.f)) { set_error("dx must be positive"); throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT}; }
     h->dt = dt;
     h->dx = dx;
@@ -427,6 +455,22 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         DevGrid dphi, dfw;
         upload_grid(h, phi, dphi, phimap, tofree);
         upload_grid(h, fw, dfw, fwmap, tofree);
+        // The velocities of the right-hand side go up on a second stream once
+        // the SDF and the face weights are up, so their copies overlap the DOF
+        // mask kernel, the host topology and the coefficient kernels.
+        HostMap vmap[4];
+        DevGrid dvel[4];
+        EventGuard ev_in, ev_vel;
+        if (ri) {
+            cudaStream_t s2 = h->body_stream;
+            CK(cudaEventCreateWithFlags(&ev_in.e, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ev_vel.e, cudaEventDisableTiming));
+            CK(cudaEventRecord(ev_in.e, s));
+            CK(cudaStreamWaitEvent(s2, ev_in.e, 0));
+            const uaamg_leaf_grid* vg[4] = {ri->vx, ri->vy, ri->vz, ri->sv};
+            for (int k = 0; k < 4; ++k) upload_grid_cs(h->ctx, s2, vg[k], dvel[k], vmap[k], tofree);
+            CK(cudaEventRecord(ev_vel.e, s2));
+        }
         TRACE("upload inputs");
         size_t extra = carve_size((size_t)nphi * 8, 8) * 2 + carve_size((size_t)nphi * 3, 4);
         void* mem = nullptr;
@@ -496,7 +540,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         }
         bytes += carve_size(nc, 4) * 3 + carve_size(nc * 6, 4) * 2;
         size_t n0 = (size_t)L0.nl * UAAMG_LEAF;
-        bytes += 6 * carve_size(n0, 4);  // x b r z p q
+        bytes += (ri ? 7 : 6) * carve_size(n0, 4);  // x b r z p q (+ the built rhs)
         bytes += carve_size(red_buffer_doubles(std::max<size_t>((size_t)L0.nl, 1)), 8);
         bytes += carve_size(sizeof(PcgState), 1) + carve_size(64, 4) + carve_size(src.size(), 4);
         CK(ctx_dev_alloc(h->ctx, (void**)&h->dmem, bytes, s));
@@ -561,6 +605,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         h->z = carve<float>(cur2, n0);
         h->p = carve<float>(cur2, n0);
         h->q = carve<float>(cur2, n0);
+        if (ri) h->rhs0 = carve<float>(cur2, n0);
         h->partials = carve<double>(cur2, red_buffer_doubles(std::max<size_t>((size_t)L0.nl, 1)));
         h->st = reinterpret_cast<PcgState*>(carve<char>(cur2, sizeof(PcgState)));
         h->scalar_dev = carve<float>(cur2, 64);
@@ -600,6 +645,19 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             CHECK_LAUNCH();
             h->launches++;
         }
+        if (ri) {
+            // createPressurePoissonRightHandSide into the PCG's b (the face
+            // weights uploaded once serve the matrix and the rhs)
+            CK(cudaStreamWaitEvent(s, ev_vel.e, 0));
+            LevelDev& D0 = h->lv[0];
+            if (D0.L.nl > 0) {
+                k_build_rhs<<<(unsigned)D0.L.nl, 128, 0, s>>>(D0.L.mask, D0.org, dfw.g, dvel[0].g, dvel[1].g,
+                                                              dvel[2].g, dvel[3].g, 1.0f / dx, h->rhs0);
+                CHECK_LAUNCH();
+                h->launches++;
+            }
+            h->rhs_resident = true;
+        }
         for (void* pmem : tofree) CK(cudaFreeAsync(pmem, s));
         tofree.clear();
         TRACE("coefficient kernels enqueued");
@@ -607,6 +665,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
     } else {
         h->nlev = 1;
         h->lv.assign(1, LevelDev());
+        h->rhs_resident = ri != nullptr;
     }
 }
 
@@ -803,6 +862,36 @@ struct Enq {
         pe();
         count++;
     }
+    // both mu-visits of level lb = nlev - 2 with their coarsest solves, in one cluster launch
+    void bottom(int lb, float* lhs, const float* rhs, const float w[3]) {
+        BottomArgs A;
+        A.L = h->lv[lb].L;
+        A.rhs = rhs;
+        A.lhs = lhs;
+        A.C = h->C;
+        A.nlc = h->lv[lb + 1].L.nl;
+        A.P = h->bot_P;
+        A.w[0] = w[0]; A.w[1] = w[1]; A.w[2] = w[2];
+        if (prof) pb("L" + std::to_string(lb) + " bottom (2 visits + coarsest)");
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)h->bot_C);
+        cfg.blockDim = dim3(BOT_THREADS);
+        cfg.dynamicSmemBytes = h->bot_smem;
+        cfg.stream = s;
+        cudaLaunchAttribute at[2];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)h->bot_C;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = g_use_pdl ? 2 : 1;
+        if (h->bot_rows == 4) CK(cudaLaunchKernelEx(&cfg, k_bottom<4>, A));
+        else CK(cudaLaunchKernelEx(&cfg, k_bottom<8>, A));
+        pe();
+        count++;
+    }
     void coarsest(const float* rhs, float* out) {
         if (h->C.n == 0) return;
         pb("coarsest cg");
@@ -815,6 +904,62 @@ struct Enq {
         count++;
     }
 };
+
+// Whether the two visits of level nlev - 2 (with the coarsest solves) run as
+// one k_bottom cluster launch: Jacobi-family smoothers, at least three levels,
+// a coarsest system the 256-thread CG shape takes (at most 2048 DOF), and a
+// cluster of at most 16 CTAs whose shared memory holds level nlev - 2 and
+// that the device can schedule.  The shape is decided once per handle.
+static bool g_use_bottom = true;
+template <int R>
+static int bottom_clusters(int C, size_t smem, int max_dynamic) {
+    // the largest size any handle may use, so that no handle's setting limits another's launches
+    CK(cudaFuncSetAttribute(k_bottom<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic));
+    CK(cudaFuncSetAttribute(k_bottom<R>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)C);
+    cfg.blockDim = dim3(BOT_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_bottom<R>, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+static bool use_bottom(uaamg_poisson* h) {
+    if (h->smoother != UAAMG_SMOOTHER_SCHEDULED_RELAXED_JACOBI && h->smoother != UAAMG_SMOOTHER_WEIGHTED_JACOBI)
+        return false;
+    if (h->bot_state >= 0) return h->bot_state == 1;
+    h->bot_state = 0;
+    if (h->nlev < 3) return false;
+    const int lb = h->nlev - 2;
+    const int nl = h->lv[lb].L.nl, nlc = h->lv[lb + 1].L.nl;
+    if (nl <= 0 || nlc <= 0 || h->C.n <= 0 || coarsest_class(h->C.n) > 1) return false;
+    const int P = (nl + BOT_MAX_CLUSTER - 1) / BOT_MAX_CLUSTER;
+    const int C = (nl + P - 1) / P;
+    const int rows = coarsest_class(h->C.n) == 0 ? 4 : 8;
+    const size_t smem = bottom_smem_bytes(P, nlc, rows);
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->ctx->device));
+    const int max_dynamic = optin - 1024;  // above the kernel's static shared memory
+    if (smem > (size_t)max_dynamic) return false;
+    if ((rows == 4 ? bottom_clusters<4>(C, smem, max_dynamic) : bottom_clusters<8>(C, smem, max_dynamic)) < 1)
+        return false;
+    h->bot_C = C;
+    h->bot_P = P;
+    h->bot_rows = rows;
+    h->bot_smem = smem;
+    h->bot_state = 1;
+    return true;
+}
 
 static float sched_weight_precond(int n, int it) {
     // muCyclePreconditioner's get_scheduled_weight (simd_vdb_poisson.cpp:1848-1866)
@@ -925,8 +1070,13 @@ static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool sk
     }
     cur = T;
     E.restrict_resid(l, cur, rhs);
-    enqueue_precond(E, l + 1, P.lhs, P.rhs, true, DotOut{nullptr, nullptr, nullptr});
-    if (l + 1 != h->nlev - 1) enqueue_precond(E, l + 1, P.lhs, P.rhs, false, DotOut{nullptr, nullptr, nullptr});
+    if (l + 1 == h->nlev - 2 && use_bottom(h)) {
+        const float w[3] = {wpre(0), wpre(1), wpre(2)};
+        E.bottom(l + 1, P.lhs, P.rhs, w);
+    } else {
+        enqueue_precond(E, l + 1, P.lhs, P.rhs, true, DotOut{nullptr, nullptr, nullptr});
+        if (l + 1 != h->nlev - 1) enqueue_precond(E, l + 1, P.lhs, P.rhs, false, DotOut{nullptr, nullptr, nullptr});
+    }
     // post-smoothing with reversed weights: T(+P x_c) -> lhs -> T -> lhs
     if (E.split(l)) {  // T += P x_c in place (T is not read again before it is rewritten)
         E.materialize(l, SrcProlong{T, P.lhs, 1.0f}, T);
@@ -1259,13 +1409,17 @@ int uaamg_poisson_create(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_gri
     return uaamg_poisson_create_on_stream(liquid_phi, face_weights, dt, dx, nullptr, out);
 }
 
-int uaamg_poisson_create_on_stream(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights, float dt,
-                                   float dx, void* stream, uaamg_poisson** out) {
+static void noalloc_resolve(uaamg_poisson* h);
+
+static int create_impl(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights, float dt, float dx,
+                       void* stream, const RhsInputs* ri, uaamg_poisson** out) {
     {
         const char* e = getenv("UAAMG_PDL");
         g_use_pdl = !(e && e[0] == '0');
         e = getenv("UAAMG_STAGED");
         g_use_staged = !(e && e[0] == '0');
+        e = getenv("UAAMG_BOTTOM");
+        g_use_bottom = !(e && e[0] == '0');
     }
     if (!out) { set_error("out is NULL"); return UAAMG_ERR_INVALID_ARGUMENT; }
     *out = nullptr;
@@ -1286,7 +1440,9 @@ int uaamg_poisson_create_on_stream(const uaamg_leaf_grid* liquid_phi, const uaam
         CK(ctx_pinned_acquire(h->ctx, sizeof(PcgState) + 256, &h->pin_state, &h->pin_state_cap));
         h->st_host = reinterpret_cast<PcgState*>(h->pin_state);
         h->scalar_host = reinterpret_cast<float*>((char*)h->pin_state + ((sizeof(PcgState) + 63) & ~size_t(63)));
-        build_hierarchy(h, liquid_phi, face_weights, dt, dx);
+        noalloc_resolve(h);
+        h->bot_state = g_use_bottom ? -1 : 0;
+        build_hierarchy(h, liquid_phi, face_weights, dt, dx, ri);
     } catch (const UaamgError& e) {
         uaamg_poisson_destroy(h);
         return e.code;
@@ -1297,6 +1453,19 @@ int uaamg_poisson_create_on_stream(const uaamg_leaf_grid* liquid_phi, const uaam
     }
     *out = h;
     return UAAMG_SUCCESS;
+}
+
+int uaamg_poisson_create_on_stream(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights, float dt,
+                                   float dx, void* stream, uaamg_poisson** out) {
+    return create_impl(liquid_phi, face_weights, dt, dx, stream, nullptr, out);
+}
+
+int uaamg_poisson_create_with_rhs(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights,
+                                  const uaamg_leaf_grid* vx, const uaamg_leaf_grid* vy, const uaamg_leaf_grid* vz,
+                                  const uaamg_leaf_grid* solid_velocity, float dt, float dx, void* stream,
+                                  uaamg_poisson** out) {
+    RhsInputs ri{vx, vy, vz, solid_velocity};
+    return create_impl(liquid_phi, face_weights, dt, dx, stream, &ri, out);
 }
 
 static void mixed_free(uaamg_poisson* h);
@@ -1476,6 +1645,58 @@ int uaamg_poisson_solve_mg_device(uaamg_poisson* h, float* d_pressure, const flo
     }
     if (iterations) *iterations = h->iterations;
     return st;
+    ABI_END
+}
+
+// Solves from a zero pressure with the rhs built by uaamg_poisson_create_with_rhs.
+static int solve_resident(uaamg_poisson* h, float* pressure, int* iterations, bool on_device, bool mg) {
+    require(h && pressure, "NULL argument");
+    if (!h->rhs_resident) {
+        set_error("the handle holds no right-hand side (create it with uaamg_poisson_create_with_rhs)");
+        return UAAMG_ERR_INVALID_ARGUMENT;
+    }
+    size_t nb = vec_bytes(h, 0);
+    if (nb) {
+        CK(cudaMemsetAsync(h->x, 0, nb, h->stream));
+        CK(cudaMemcpyAsync(h->b, h->rhs0, nb, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    int st = mg ? run_mg(h) : run_pcg(h);
+    if (nb) {
+        CK(cudaMemcpyAsync(pressure, h->x, nb, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (iterations) *iterations = h->iterations;
+    return st;
+}
+int uaamg_poisson_solve_pcg_resident(uaamg_poisson* h, float* pressure, int* iterations) {
+    ABI_BEGIN
+    return solve_resident(h, pressure, iterations, false, false);
+    ABI_END
+}
+int uaamg_poisson_solve_pcg_resident_device(uaamg_poisson* h, float* d_pressure, int* iterations) {
+    ABI_BEGIN
+    return solve_resident(h, d_pressure, iterations, true, false);
+    ABI_END
+}
+int uaamg_poisson_solve_mg_resident(uaamg_poisson* h, float* pressure, int* iterations) {
+    ABI_BEGIN
+    return solve_resident(h, pressure, iterations, false, true);
+    ABI_END
+}
+int uaamg_poisson_copy_rhs(uaamg_poisson* h, float* rhs_out) {
+    ABI_BEGIN
+    require(h && rhs_out, "NULL argument");
+    if (!h->rhs_resident) {
+        set_error("the handle holds no right-hand side (create it with uaamg_poisson_create_with_rhs)");
+        return UAAMG_ERR_INVALID_ARGUMENT;
+    }
+    size_t nb = vec_bytes(h, 0);
+    if (nb) {
+        CK(cudaMemcpyAsync(rhs_out, h->rhs0, nb, cudaMemcpyDefault, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return UAAMG_SUCCESS;
     ABI_END
 }
 
@@ -1677,39 +1898,48 @@ int uaamg_poisson_residual_norm_device(uaamg_poisson* h, const float* d_x, const
 #define UAAMG_NOALLOC_RED_DOUBLES (RED_HEADER + UAAMG_NOALLOC_MAX_LEAVES + RED_TICKETS)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[(UAAMG_NOALLOC_RED_DOUBLES + 32) * sizeof(double)];
 
-// Device address of g_noalloc_scratch on each device, resolved once per device
-// (host code may not use the symbol itself: it names a host-side stand-in).
-static std::mutex g_noalloc_mutex;
-static void* g_noalloc_addr[64] = {nullptr};
+// The array's device address on the handle's device, looked up when the handle
+// is created (its device is current then).  Host code may not use the symbol
+// itself: it names a host-side stand-in, not device memory.  Keeping the
+// address in the handle ties it to the context the handle lives in.
+static void noalloc_resolve(uaamg_poisson* h) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    h->noalloc_scratch = p;
+}
 
-static void* noalloc_scratch_on_current_device() {
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) {
-        set_error("device index %d out of range", dev);
-        throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT};
+// Level-0 leaf limit of the allocation-free variant; a test may lower it
+// through UAAMG_NOALLOC_TEST_MAX_LEAVES to reach the rejection path on a small
+// domain (it can only be lowered).
+static int noalloc_max_leaves() {
+    const char* e = getenv("UAAMG_NOALLOC_TEST_MAX_LEAVES");
+    if (e && e[0]) {
+        long v = strtol(e, nullptr, 10);
+        if (v >= 0 && v < UAAMG_NOALLOC_MAX_LEAVES) return (int)v;
     }
-    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
-        void* p = nullptr;
-        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_noalloc_addr[dev] = p;
-    }
-    return g_noalloc_addr[dev];
+    return UAAMG_NOALLOC_MAX_LEAVES;
 }
 
 int uaamg_poisson_residual_norm_noalloc(uaamg_poisson* h, const float* d_x, const float* d_b, float* d_r,
                                         float* d_norm) {
     ABI_BEGIN
     require(h && d_x && d_b && d_r && d_norm, "NULL argument");
-    LevelDev& D0 = h->lv[0];
-    if (D0.L.nl > UAAMG_NOALLOC_MAX_LEAVES) {
-        set_error("uaamg_poisson_residual_norm_noalloc: level 0 has %d leaves, the allocation-free variant "
-                  "handles at most %d (use uaamg_poisson_residual_norm_device)",
-                  D0.L.nl, UAAMG_NOALLOC_MAX_LEAVES);
+    int cur = -1;
+    CK(cudaGetDevice(&cur));
+    if (cur != h->ctx->device || !h->noalloc_scratch) {
+        set_error("uaamg_poisson_residual_norm_noalloc: the handle lives on device %d but device %d is current",
+                  h->ctx->device, cur);
         return UAAMG_ERR_INVALID_ARGUMENT;
     }
-    char* scratch = (char*)noalloc_scratch_on_current_device();
+    LevelDev& D0 = h->lv[0];
+    const int maxl = noalloc_max_leaves();
+    if (D0.L.nl > maxl) {
+        set_error("uaamg_poisson_residual_norm_noalloc: level 0 has %d leaves, the allocation-free variant "
+                  "handles at most %d (use uaamg_poisson_residual_norm_device)",
+                  D0.L.nl, maxl);
+        return UAAMG_ERR_INVALID_ARGUMENT;
+    }
+    char* scratch = (char*)h->noalloc_scratch;
     double* partials = reinterpret_cast<double*>(scratch);
     unsigned* ticket = reinterpret_cast<unsigned*>(scratch + (size_t)UAAMG_NOALLOC_RED_DOUBLES * sizeof(double));
     if (D0.L.nl == 0) {

@@ -1275,38 +1275,43 @@ __device__ __forceinline__ float2 cg_block_sum2(float a, float b, float* buf) {
 }
 
 // ROWS rows per thread in a block of NT threads (row i = tid + k * NT); the
-// matrix rows stay in registers for the whole solve.  Three barriers per CG
-// iteration.  WAIT: the body itself waits for the previous kernel
-// (griddepcontrol) after loading the matrix, which does not change during a
-// solve; false when the caller has waited already.
-template <int ROWS, int NT, bool WAIT>
-__device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float* rhs, float* out, float* ps,
-                                                 float (*red)[64]) {
-    const int tid = threadIdx.x, n = C.n;
-    float x[ROWS], r[ROWS], p[ROWS], z[ROWS], dg[ROWS], iv[ROWS], val[ROWS][6];
+// matrix rows stay in registers for the whole solve (CgRows), so a kernel that
+// solves the same system twice loads them once.  Three barriers per CG
+// iteration.
+template <int ROWS>
+struct CgRows {
+    float dg[ROWS], iv[ROWS], val[ROWS][6];
     int col[ROWS][6], slot[ROWS];
+};
+template <int ROWS, int NT>
+__device__ __forceinline__ void cg_rows_load(const DCoarsest& C, CgRows<ROWS>& M) {
+    const int tid = threadIdx.x, n = C.n;
 #pragma unroll
     for (int k = 0; k < ROWS; ++k) {
         const int i = tid + k * NT;
         const bool ok = i < n;
-        slot[k] = ok ? C.dof_slot[i] : -1;
-        dg[k] = ok ? C.diag[i] : 0.f;
-        iv[k] = ok ? C.invd[i] : 0.f;
+        M.slot[k] = ok ? C.dof_slot[i] : -1;
+        M.dg[k] = ok ? C.diag[i] : 0.f;
+        M.iv[k] = ok ? C.invd[i] : 0.f;
 #pragma unroll
         for (int e = 0; e < 6; ++e) {
-            col[k][e] = ok ? C.col[i * 6 + e] : -1;
-            val[k][e] = ok ? C.val[i * 6 + e] : 0.f;
+            M.col[k][e] = ok ? C.col[i * 6 + e] : -1;
+            M.val[k][e] = ok ? C.val[i * 6 + e] : 0.f;
         }
     }
-    if (WAIT) {
-        griddep_wait();
-        griddep_launch();
-    }
+}
+// out[slot] = the 10-step CG solution for the rhs gathered from rhs[slot]
+// (every thread of the NT-thread block takes part)
+template <int ROWS, int NT>
+__device__ __forceinline__ void cg_rows_solve(const CgRows<ROWS>& M, const float* rhs, float* out, float* ps,
+                                              float (*red)[64]) {
+    const int tid = threadIdx.x;
+    float x[ROWS], r[ROWS], p[ROWS], z[ROWS];
     float bb = 0.f;
 #pragma unroll
     for (int k = 0; k < ROWS; ++k) {
         x[k] = 0.f;
-        r[k] = slot[k] >= 0 ? rhs[slot[k]] : 0.f;
+        r[k] = M.slot[k] >= 0 ? rhs[M.slot[k]] : 0.f;
         bb = __fadd_rn(bb, __fmul_rn(r[k], r[k]));
     }
     int rb = 0;
@@ -1318,7 +1323,7 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
         float an = 0.f;
 #pragma unroll
         for (int k = 0; k < ROWS; ++k) {
-            p[k] = __fmul_rn(iv[k], r[k]);
+            p[k] = __fmul_rn(M.iv[k], r[k]);
             an = __fadd_rn(an, __fmul_rn(r[k], p[k]));
         }
         float absNew = cg_block_sum<NT>(an, red[rb]);
@@ -1330,10 +1335,10 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
             float pt = 0.f, tq[ROWS];
 #pragma unroll
             for (int k = 0; k < ROWS; ++k) {
-                float s = __fmul_rn(dg[k], p[k]);
+                float s = __fmul_rn(M.dg[k], p[k]);
 #pragma unroll
                 for (int e = 0; e < 6; ++e)
-                    if (col[k][e] >= 0) s = __fadd_rn(s, __fmul_rn(val[k][e], ps[col[k][e]]));
+                    if (M.col[k][e] >= 0) s = __fadd_rn(s, __fmul_rn(M.val[k][e], ps[M.col[k][e]]));
                 tq[k] = s;
                 pt = __fadd_rn(pt, __fmul_rn(p[k], s));
             }
@@ -1344,7 +1349,7 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
             for (int k = 0; k < ROWS; ++k) {
                 x[k] = __fmaf_rn(alpha, p[k], x[k]);
                 r[k] = __fmaf_rn(-alpha, tq[k], r[k]);
-                z[k] = __fmul_rn(iv[k], r[k]);
+                z[k] = __fmul_rn(M.iv[k], r[k]);
                 rr = __fadd_rn(rr, __fmul_rn(r[k], r[k]));
                 rz = __fadd_rn(rz, __fmul_rn(r[k], z[k]));
             }
@@ -1360,7 +1365,22 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
     }
 #pragma unroll
     for (int k = 0; k < ROWS; ++k)
-        if (slot[k] >= 0) out[slot[k]] = x[k];
+        if (M.slot[k] >= 0) out[M.slot[k]] = x[k];
+}
+
+// The whole coarsest solve.  WAIT: the body itself waits for the previous
+// kernel (griddepcontrol) after loading the matrix, which does not change
+// during a solve; false when the caller has waited already.
+template <int ROWS, int NT, bool WAIT>
+__device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float* rhs, float* out, float* ps,
+                                                 float (*red)[64]) {
+    CgRows<ROWS> M;
+    cg_rows_load<ROWS, NT>(C, M);
+    if (WAIT) {
+        griddep_wait();
+        griddep_launch();
+    }
+    cg_rows_solve<ROWS, NT>(M, rhs, out, ps, red);
 }
 
 template <int ROWS, int NT>

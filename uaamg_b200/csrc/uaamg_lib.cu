@@ -2,6 +2,7 @@
 #include "poisson.cu"
 #include "batch.cu"
 #include "mixed.cu"
+#include "fp64ref.cu"
 #include "viscosity.cu"
 #include "projection.cu"
 #include "extrapolate.cu"

@@ -72,6 +72,30 @@ class LaplacianWithLevel:
                                                     C.byref(h)), "uaamg_poisson_create")
         return LaplacianWithLevel(h.value, dt, dx)
 
+    @staticmethod
+    def createPressurePoissonLaplacianWithRhs(liquid_phi: LeafGrid, face_weights: LeafGrid, vx: LeafGrid,
+                                              vy: LeafGrid, vz: LeafGrid, solid_velocity: LeafGrid, dt: float,
+                                              dx: float, stream: int | None = None) -> "LaplacianWithLevel":
+        """createPressurePoissonLaplacian + createPressurePoissonRightHandSide
+        in one C-ABI call (uaamg_poisson_create_with_rhs): every input crosses
+        the bus once and the rhs stays on the device for
+        ``PoissonSolver.solveMultigridPCGResident``."""
+        L = _lib.lib()
+        keep: list = []
+        gs = [_as_c(g, keep) for g in (liquid_phi, face_weights, vx, vy, vz, solid_velocity)]
+        h = C.c_void_p()
+        _lib.check(L.uaamg_poisson_create_with_rhs(*[C.byref(g) for g in gs], float(dt), float(dx), stream,
+                                                   C.byref(h)), "uaamg_poisson_create_with_rhs")
+        return LaplacianWithLevel(h.value, dt, dx)
+
+    def copy_rhs(self, out=None):
+        """The rhs built by createPressurePoissonLaplacianWithRhs (numpy, or
+        into a torch CUDA tensor)."""
+        rhs = self.getZeroVectorGrid() if out is None else out
+        ptr = rhs.ctypes.data if isinstance(rhs, np.ndarray) else rhs.data_ptr()
+        _lib.check(_lib.lib().uaamg_poisson_copy_rhs(self._h, ptr), "copy_rhs")
+        return rhs
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
@@ -243,6 +267,25 @@ class PoissonSolver:
     def solvePureMultigrid(self, in_out_pressure, in_rhs) -> int:
         return self._solve("uaamg_poisson_solve_mg", "uaamg_poisson_solve_mg_device", in_out_pressure, in_rhs)
 
+    def solveMultigridPCGResident(self, out_pressure, pure_multigrid: bool = False) -> int:
+        """solveMultigridPCG (or solvePureMultigrid) from a zero pressure with
+        the rhs built at creation (a level 0 made by
+        createPressurePoissonLaplacianWithRhs); the pressure is written to
+        ``out_pressure`` (numpy or a torch CUDA tensor)."""
+        L, h = self._configure()
+        it = C.c_int(0)
+        if isinstance(out_pressure, np.ndarray):
+            assert out_pressure.dtype == np.float32 and out_pressure.flags["C_CONTIGUOUS"]
+            fn = "uaamg_poisson_solve_mg_resident" if pure_multigrid else "uaamg_poisson_solve_pcg_resident"
+            rc = getattr(L, fn)(h, out_pressure.ctypes.data, C.byref(it))
+        else:
+            assert not pure_multigrid, "the device form is PCG only"
+            fn = "uaamg_poisson_solve_pcg_resident_device"
+            rc = L.uaamg_poisson_solve_pcg_resident_device(h, out_pressure.data_ptr(), C.byref(it))
+        _lib.check(rc, fn)
+        self.mIterationTaken = int(it.value)
+        return int(rc)
+
     # --- mixed-precision form (no counterpart in the reference): the
     # preconditioner's hierarchy in FP16/BF16 with FP32 arithmetic, FP32 outer
     # CG with FP64 dots, true-residual replacement, FP64 coarsest solve
@@ -281,6 +324,19 @@ class PoissonSolver:
         _lib.check(_lib.lib().uaamg_poisson_true_residual_fp64(self.mMultigridHierarchy._h, d_x.data_ptr(),
                                                                 d_b.data_ptr(), out), "true_residual_fp64")
         return float(out[0]), float(out[1])
+
+    def solve_fp64_reference(self, d_rhs, d_x, rel_tol: float = 1e-12, max_iter: int = 200):
+        """The FP64 reference solution of the level-0 system (torch CUDA
+        tensors: d_rhs float32 [n, 512], d_x float64 [n, 512] out): flexible
+        FP64 PCG with the FP32 W-cycle as preconditioner, to a true relative
+        2-norm residual of rel_tol.  Returns (status, iterations, residual)."""
+        L, h = self._configure()
+        it = C.c_int(0)
+        rr = C.c_double(0.0)
+        rc = L.uaamg_poisson_solve_fp64_reference(h, d_rhs.data_ptr(), d_x.data_ptr(), float(rel_tol),
+                                                  int(max_iter), C.byref(it), C.byref(rr))
+        _lib.check(rc, "solve_fp64_reference")
+        return int(rc), int(it.value), float(rr.value)
 
     def precondition(self, r: np.ndarray) -> np.ndarray:
         L, h = self._configure()
