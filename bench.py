@@ -151,18 +151,30 @@ def cpu_solve_once(sc, threads: int):
 
 
 def _visc_warm_start(o, sc):
-    """The velocity at every DOF (FLIP_vdb.cpp:3188-3198), from the oracle's topology."""
+    """The velocity at every DOF (FLIP_vdb.cpp:3188-3198), from the oracle's
+    topology: each DOF leaf is matched to the velocity grid's leaf at the same
+    origin by a sorted-key search, then the values are copied under the DOF
+    masks, all as whole-array operations."""
     org, _ = o.topology(0)
     idx = o.dof_index(0)
     out = o.zeros(0)
+
+    def keys(a):
+        a = a.astype(np.int64) + (1 << 20)
+        return (a[:, 0] << 42) | (a[:, 1] << 21) | a[:, 2]
+
+    k0 = keys(org)
     for c, g in enumerate((sc.u, sc.v, sc.w)):
-        lut = {tuple(x): i for i, x in enumerate(g.origins)}
-        for li in range(org.shape[0]):
-            j = lut.get(tuple(org[li]))
-            if j is None:
-                continue
-            m = idx[c, li] >= 0
-            out[c, li, m] = g.values[j].reshape(512)[m]
+        kg = keys(g.origins)
+        order = np.argsort(kg)
+        pos = np.searchsorted(kg[order], k0)
+        pos = np.minimum(pos, len(kg) - 1)
+        j = order[pos]
+        hit = kg[j] == k0
+        vals = np.zeros((org.shape[0], 512), np.float32)
+        vals[hit] = g.values[j[hit]].reshape(-1, 512)
+        m = idx[c] >= 0
+        out[c][m] = vals[m]
     return out
 
 

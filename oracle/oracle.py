@@ -71,6 +71,7 @@ def lib():
         L.orc_triplets.restype = C.c_int64
         L.orc_dof_index.argtypes = [vp, C.c_int, i32p]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_set_simd.argtypes = [C.c_int]
         # variational viscosity
         L.orc_visc_create.restype = vp
         L.orc_visc_create.argtypes = [C.c_int64, i32p, u64p, f32p, C.c_float,
@@ -376,6 +377,12 @@ class OracleViscosity:
 
     def dot(self, a, b, level=0):
         return float(lib().orc_visc_dot(self._h, level, _f32(a), _f32(b)))
+
+
+def set_simd(on: bool) -> None:
+    """The Poisson applier's AVX2 path (default) or the scalar per-voxel path
+    (the same bits)."""
+    lib().orc_set_simd(1 if on else 0)
 
 
 def set_threads(n: int) -> None:

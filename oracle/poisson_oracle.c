@@ -419,10 +419,124 @@ static void level_init_spai0(olevel* L) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* LaplacianApplySIMD::LightWeightApplier::operator() (simd_vdb_poisson.cpp:755-1031) */
+/* LaplacianApplySIMD::LightWeightApplier::operator() (simd_vdb_poisson.cpp:755-1031)
+ * in the reference's lane layout: one __m256 per (x, y) row of a leaf holds its
+ * 8 z voxels; the +-x / +-y rows come from the leaf or its neighbour leaf, the
+ * +-z values are the row shifted by one lane with the neighbour leaf's boundary
+ * voxel blended into the end lane (vdb_SIMD_IO.h:25-191); inactive lanes are
+ * written as 0.  Every lane performs the scalar path's operations in the same
+ * order (products, the three pair sums, two more sums, then the mode's
+ * fused multiply-adds), so both paths give the same bits. */
+#include <immintrin.h>
+static int g_orc_simd = 1;
+void orc_set_simd(int on) { g_orc_simd = on; }
+
+static void apply_level_avx2(olevel* L, int mode, float weight, float w_sor, const float* lhs,
+                             const float* rhs, float* out) {
+    const __m256i up = _mm256_setr_epi32(1, 2, 3, 4, 5, 6, 7, 7);
+    const __m256i dn = _mm256_setr_epi32(0, 0, 1, 2, 3, 4, 5, 6);
+    const __m256i bitsel = _mm256_setr_epi32(1, 2, 4, 8, 16, 32, 64, 128);
+    const __m256 zero = _mm256_setzero_ps();
+    const __m256 dface = _mm256_set1_ps(L->def_face);
+    const __m256 vw = _mm256_set1_ps(weight), vsor = _mm256_set1_ps(w_sor), v1m = _mm256_set1_ps(1.0f - w_sor);
+    const __m256 even = _mm256_castsi256_ps(_mm256_setr_epi32(-1, 0, -1, 0, -1, 0, -1, 0));
+    const __m256 odd = _mm256_castsi256_ps(_mm256_setr_epi32(0, -1, 0, -1, 0, -1, 0, -1));
+    const float* cx = L->cx;
+    const float* cy = L->cy;
+    const float* cz = L->cz;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < L->nl; ++i) {
+        const int32_t* nb = L->nbr + 6 * i;
+        const uint64_t* m = L->mask + 8 * i;
+        for (int X = 0; X < 8; ++X)
+            for (int Y = 0; Y < 8; ++Y) {
+                const size_t row = (size_t)i * LSZ + (size_t)X * 64 + (size_t)Y * 8;
+                const unsigned bits = (unsigned)((m[X] >> (Y * 8)) & 0xFFu);
+                if (!bits) { _mm256_storeu_ps(out + row, zero); continue; }
+                const __m256 xc = _mm256_loadu_ps(lhs + row);
+                __m256 xp, cxp, xm, yp, cyp, ym;
+                if (X < 7) { xp = _mm256_loadu_ps(lhs + row + 64); cxp = _mm256_loadu_ps(cx + row + 64); }
+                else if (nb[1] >= 0) {
+                    const size_t r = (size_t)nb[1] * LSZ + (size_t)Y * 8;
+                    xp = _mm256_loadu_ps(lhs + r); cxp = _mm256_loadu_ps(cx + r);
+                } else { xp = zero; cxp = dface; }
+                if (X > 0) xm = _mm256_loadu_ps(lhs + row - 64);
+                else xm = nb[0] >= 0 ? _mm256_loadu_ps(lhs + (size_t)nb[0] * LSZ + 448 + (size_t)Y * 8) : zero;
+                if (Y < 7) { yp = _mm256_loadu_ps(lhs + row + 8); cyp = _mm256_loadu_ps(cy + row + 8); }
+                else if (nb[3] >= 0) {
+                    const size_t r = (size_t)nb[3] * LSZ + (size_t)X * 64;
+                    yp = _mm256_loadu_ps(lhs + r); cyp = _mm256_loadu_ps(cy + r);
+                } else { yp = zero; cyp = dface; }
+                if (Y > 0) ym = _mm256_loadu_ps(lhs + row - 8);
+                else ym = nb[2] >= 0 ? _mm256_loadu_ps(lhs + (size_t)nb[2] * LSZ + (size_t)X * 64 + 56) : zero;
+                float zp7 = 0.f, czp7 = L->def_face, zm0 = 0.f;
+                if (nb[5] >= 0) {
+                    const size_t r = (size_t)nb[5] * LSZ + (size_t)X * 64 + (size_t)Y * 8;
+                    zp7 = lhs[r];
+                    czp7 = cz[r];
+                }
+                if (nb[4] >= 0) zm0 = lhs[(size_t)nb[4] * LSZ + (size_t)X * 64 + (size_t)Y * 8 + 7];
+                const __m256 czo = _mm256_loadu_ps(cz + row);
+                const __m256 zp = _mm256_blend_ps(_mm256_permutevar8x32_ps(xc, up), _mm256_set1_ps(zp7), 0x80);
+                const __m256 czp = _mm256_blend_ps(_mm256_permutevar8x32_ps(czo, up), _mm256_set1_ps(czp7), 0x80);
+                const __m256 zm = _mm256_blend_ps(_mm256_permutevar8x32_ps(xc, dn), _mm256_set1_ps(zm0), 0x01);
+                __m256 f1 = _mm256_mul_ps(xp, cxp), f2 = _mm256_mul_ps(xm, _mm256_loadu_ps(cx + row));
+                __m256 f3 = _mm256_mul_ps(yp, cyp), f4 = _mm256_mul_ps(ym, _mm256_loadu_ps(cy + row));
+                __m256 f5 = _mm256_mul_ps(zp, czp), f6 = _mm256_mul_ps(zm, czo);
+                f1 = _mm256_add_ps(f1, f2);
+                f3 = _mm256_add_ps(f3, f4);
+                f5 = _mm256_add_ps(f5, f6);
+                f1 = _mm256_add_ps(f1, f3);
+                f1 = _mm256_add_ps(f1, f5);
+                __m256 r;
+                switch (mode) {
+                case ORC_MODE_JACOBI: {
+                    __m256 res = _mm256_sub_ps(_mm256_loadu_ps(rhs + row),
+                                               _mm256_fmadd_ps(xc, _mm256_loadu_ps(L->diag + row), f1));
+                    res = _mm256_mul_ps(res, _mm256_loadu_ps(L->invdiag + row));
+                    r = _mm256_fmadd_ps(vw, res, xc);
+                    break;
+                }
+                case ORC_MODE_RESIDUAL:
+                    r = _mm256_sub_ps(_mm256_loadu_ps(rhs + row), _mm256_fmadd_ps(xc, _mm256_loadu_ps(L->diag + row), f1));
+                    break;
+                case ORC_MODE_RED_GS:
+                case ORC_MODE_BLACK_GS: {
+                    __m256 res = _mm256_sub_ps(_mm256_loadu_ps(rhs + row), f1);
+                    res = _mm256_mul_ps(res, _mm256_loadu_ps(L->invdiag + row));
+                    res = _mm256_mul_ps(res, vsor);
+                    const __m256 v = _mm256_fmadd_ps(xc, v1m, res);
+                    /* red: (x + y + z) even */
+                    const int xy_even = ((X + Y) & 1) == 0;
+                    const __m256 red = xy_even ? even : odd;
+                    const __m256 upd = mode == ORC_MODE_RED_GS ? red : (xy_even ? odd : even);
+                    r = _mm256_blendv_ps(xc, v, upd);
+                    break;
+                }
+                case ORC_MODE_SPAI0: {
+                    const __m256 res = _mm256_sub_ps(_mm256_loadu_ps(rhs + row),
+                                                     _mm256_fmadd_ps(xc, _mm256_loadu_ps(L->diag + row), f1));
+                    r = _mm256_fmadd_ps(_mm256_loadu_ps(L->spai0 + row), res, xc);
+                    break;
+                }
+                default:
+                    r = _mm256_fmadd_ps(xc, _mm256_loadu_ps(L->diag + row), f1);
+                    break;
+                }
+                const __m256 act = _mm256_castsi256_ps(
+                    _mm256_cmpeq_epi32(_mm256_and_si256(_mm256_set1_epi32((int)bits), bitsel), bitsel));
+                _mm256_storeu_ps(out + row, _mm256_blendv_ps(zero, r, act));
+            }
+    }
+}
+
 static void apply_level(olevel* L, int mode, float weight, float w_sor, const float* lhs,
                         const float* rhs, float* out) {
     if (mode == ORC_MODE_SPAI0) level_init_spai0(L);
+    if (g_orc_simd) {
+        apply_level_avx2(L, mode, weight, w_sor, lhs, rhs, out);
+        return;
+    }
     const float one_minus_sor = 1.0f - w_sor;
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < L->nl; ++i) {
@@ -488,8 +602,28 @@ static void apply_level(olevel* L, int mode, float weight, float w_sor, const fl
     }
 }
 
-/* setGridToResultAfterFirstJacobi (:1435-1479) */
+/* 8 activity bits of a row as a lane mask */
+static inline __m256 row_mask(unsigned bits) {
+    const __m256i bitsel = _mm256_setr_epi32(1, 2, 4, 8, 16, 32, 64, 128);
+    return _mm256_castsi256_ps(_mm256_cmpeq_epi32(_mm256_and_si256(_mm256_set1_epi32((int)bits), bitsel), bitsel));
+}
+
+/* setGridToResultAfterFirstJacobi (:1435-1479): AVX lanes as in the reference
+ * (:1472-1473), or the scalar loop */
 static void first_jacobi(olevel* L, float weight, const float* rhs, float* out) {
+    if (g_orc_simd) {
+        const __m256 w = _mm256_set1_ps(weight), zero = _mm256_setzero_ps();
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < L->nl; ++i)
+            for (int xy = 0; xy < 64; ++xy) {
+                const size_t row = (size_t)i * LSZ + (size_t)xy * 8;
+                const unsigned bits = (unsigned)((L->mask[8 * i + (xy >> 3)] >> ((xy & 7) * 8)) & 0xFFu);
+                __m256 r = _mm256_mul_ps(_mm256_loadu_ps(L->invdiag + row), _mm256_loadu_ps(rhs + row));
+                r = _mm256_mul_ps(w, r);
+                _mm256_storeu_ps(out + row, _mm256_blendv_ps(zero, r, row_mask(bits)));
+            }
+        return;
+    }
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < L->nl; ++i)
         for (int off = 0; off < LSZ; ++off) {
@@ -504,6 +638,19 @@ static void first_jacobi(olevel* L, float weight, const float* rhs, float* out) 
  * no leaves and every voxel uses the default 1/(7 dt/dx^2). */
 static void first_spai0(olevel* L, const float* rhs, float* out) {
     const int ready = L->spai0_ready;
+    if (g_orc_simd) {
+        const __m256 zero = _mm256_setzero_ps(), def = _mm256_set1_ps(L->def_spai0);
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < L->nl; ++i)
+            for (int xy = 0; xy < 64; ++xy) {
+                const size_t row = (size_t)i * LSZ + (size_t)xy * 8;
+                const unsigned bits = (unsigned)((L->mask[8 * i + (xy >> 3)] >> ((xy & 7) * 8)) & 0xFFu);
+                const __m256 sp = ready ? _mm256_loadu_ps(L->spai0 + row) : def;
+                const __m256 r = _mm256_mul_ps(sp, _mm256_loadu_ps(rhs + row));
+                _mm256_storeu_ps(out + row, _mm256_blendv_ps(zero, r, row_mask(bits)));
+            }
+        return;
+    }
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < L->nl; ++i)
         for (int off = 0; off < LSZ; ++off) {

@@ -173,6 +173,9 @@ void orc_visc_coarsest_solve(orc_visc* h, const float* rhs, float* out);
 /* Summation order of the viscosity coarsest CG (the reference leaves it to
  * Eigen): the CUDA kernel's 256-thread tree order with fused vector updates
  * (the default), or plain sequential sums with separate multiply and add. */
+/* 1 (default): the Poisson applier runs 8-wide AVX2 z-lanes; 0: the scalar
+ * per-voxel path.  Both give the same bits. */
+void orc_set_simd(int on);
 #define ORC_CG_ORDER_KERNEL 0
 #define ORC_CG_ORDER_SEQUENTIAL 1
 void orc_visc_set_coarsest_order(orc_visc* h, int order);

@@ -1,16 +1,16 @@
 """GPU parity of the variational-viscosity UAAMG-PCG through the C ABI against
 the oracle (restatement of SIMD_UAAMG/simd_viscosity3d.cpp).
 
-Construction, every apply mode, the red-black Gauss-Seidel passes and the
-transfers are bit-exact (the kernels follow the reference's float operation
-order).  Whole solves: iteration count within +-2, and the GPU solution meets
-the reference's stopping test in exact arithmetic as well as the oracle's does
-(FP64 residual with the assembled matrix; FP64 direct solve where the system
-is small).  A tighter solution-to-solution bound is not a property of the
-reference itself here: its stopping test is relative to the warm-start
-residual, and the oracle's own solution moves by ~1e-3 (relative) when only
-the rounding of its dot products changes, so solutions are compared at
-SOL_TOL = 2e-3.
+Construction, every apply mode, the red-black Gauss-Seidel passes, the
+transfers, the coarsest CG and whole PCG solves are bit-exact: the kernels
+follow the reference's float operation order, the PCG's dot products sum in
+the reference's order (lv_dot), and the oracle's coarsest CG uses the
+summation order of the CUDA coarsest kernel (the reference leaves that order
+to Eigen, whose vectorised order is not pinned).  Bit-exactness is the only
+meaningful parity here: two FP32 solves that differ in that order alone end up
+to ~2e-3 apart at every tolerance (tests/test_oracle_viscosity.py::
+test_summation_order_sensitivity), because FP32 residuals of this system
+stagnate.  Each solve is still checked in FP64 against the assembled matrix.
 """
 import numpy as np
 import pytest
@@ -21,8 +21,7 @@ from uaamg_b200.grids import LeafGrid, dense_to_leaves
 
 pytestmark = pytest.mark.gpu
 
-ITER_TOL = 2
-SOL_TOL = 2e-3
+ITER_TOL = 0   # identical iteration counts
 
 
 def _fp64_check(ref, x, xr, b, x0, tol, exact=False):
@@ -49,7 +48,7 @@ def _fp64_check(ref, x, xr, b, x0, tol, exact=False):
         xs = spla.spsolve(A.tocsc(), bv)
         eg, eo = np.abs(vec(x) - xs).max(), np.abs(vec(xr) - xs).max()
         assert eg <= 2.0 * eo + 1e-6 * np.abs(xs).max(), (eg, eo)
-    assert np.abs(x - xr).max() <= SOL_TOL * np.abs(xr).max()
+    assert np.array_equal(x, xr)
 
 
 @pytest.fixture(scope="module")
@@ -154,17 +153,17 @@ def test_restriction_prolongation_bit_exact(scene32):
         assert np.array_equal(lv.prolongation(c, f, l), ref.prolongate(l, c, f))
 
 
-def test_coarsest_and_preconditioner_close(scene32):
+def test_coarsest_and_preconditioner_bit_exact(scene32):
     sc, lv, ref = scene32
     L = ref.num_levels - 1
     b = rand_vec(ref, L, 90)
     g, c = lv.solve_exact(b), ref.coarsest_solve(b)
-    assert np.abs(g - c).max() <= 1e-3 * max(np.abs(c).max(), 1e-30)
+    assert np.array_equal(g, c)
     from uaamg_b200.viscosity import simd_viscosity3d
     s = simd_viscosity3d(lv)
     r = rand_vec(ref, 0, 91)
     zg, zc = s.precondition(r), ref.precondition(r)
-    assert np.abs(zg - zc).max() <= 1e-2 * np.abs(zc).max()
+    assert np.array_equal(zg, zc)
 
 
 def _solve_pair(sc, lv, ref, tol=1e-6, warm=True, max_iter=100, graph=1):
@@ -270,8 +269,8 @@ def test_golden_fixture_on_gpu(gpu):
     s = simd_viscosity3d(lv)
     st = s.pcg_solve(x, 1e-6, rhs)
     assert st == int(g["pcg_status"])
-    assert abs(s.m_iteration - int(g["pcg_iters"])) <= ITER_TOL
-    assert np.abs(x - g["pcg_x"]).max() <= SOL_TOL * np.abs(g["pcg_x"]).max()
+    assert s.m_iteration == int(g["pcg_iters"])
+    assert np.array_equal(x, g["pcg_x"])
 
 
 @pytest.mark.parametrize("spheres,slab", [((), 0.45), ((((0.5, 0.5, 0.5), 0.3),), None)])

@@ -334,3 +334,39 @@ def test_translation_and_leaf_order_invariance():
     r2, st2, it2, _ = o2.solve_pcg(o2.zeros(), rhs2)
     assert st1 == st2 == 0 and it1 == it2
     assert np.allclose(r2[perm], r1, rtol=1e-5, atol=1e-6 * np.abs(r1).max())
+
+
+def test_avx2_applier_matches_scalar_path():
+    """The oracle's 8-lane AVX2 applier (the reference's lane layout) gives the
+    scalar per-voxel path's bits in every mode, on every level, at leaf
+    boundaries and in place (red/black passes)."""
+    from oracle.oracle import set_simd
+    sc = scenes.plain_poisson_scene(n=48, seed=5)
+    o = OraclePoisson(sc.phi, sc.face_weights, sc.dt, sc.dx)
+    rng = np.random.default_rng(3)
+    try:
+        for l in range(o.num_levels):
+            act = o.dof_index(l) >= 0
+            x = (rng.standard_normal(act.shape) * act).astype(np.float32)
+            b = (rng.standard_normal(act.shape) * act).astype(np.float32)
+            for mode in ("jacobi", "residual", "laplacian", "red_gs", "black_gs", "spai0"):
+                for w, wsor in ((0.8571, 1.2), (2.2473, 1.0)):
+                    set_simd(True)
+                    a = o.apply(l, mode, x, b, weight=w, w_sor=wsor)
+                    set_simd(False)
+                    c = o.apply(l, mode, x, b, weight=w, w_sor=wsor)
+                    assert np.array_equal(a, c), (l, mode)
+            for first in ("jacobi", "spai0"):
+                set_simd(True)
+                a = o.first_jacobi(l, b, 2.2473) if first == "jacobi" else o.first_spai0(l, b)
+                set_simd(False)
+                c = o.first_jacobi(l, b, 2.2473) if first == "jacobi" else o.first_spai0(l, b)
+                assert np.array_equal(a, c), (l, first)
+        set_simd(True)
+        rhs = o.build_rhs(sc.face_weights, sc.vx, sc.vy, sc.vz, sc.solid_velocity)
+        xa, sta, ita, _ = o.solve_pcg(o.zeros(), rhs, tol=1e-7)
+        set_simd(False)
+        xb, stb, itb, _ = o.solve_pcg(o.zeros(), rhs, tol=1e-7)
+        assert sta == stb and ita == itb and np.array_equal(xa, xb)
+    finally:
+        set_simd(True)
