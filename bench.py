@@ -901,6 +901,12 @@ def main():
 
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
+    # the autotuner's kernel-shape table for this GPU, when one is committed (results do not depend on it)
+    from uaamg_b200 import autotune
+    tuning_table = autotune.apply(device=local)
+    tuning = {"setting": autotune.get(),
+              "source": os.path.relpath(autotune.table_path(tuning_table["gpu"], tuning_table["sm_count"]), ROOT)
+              if tuning_table else "built-in defaults"}
 
     def on_device(g: LeafGrid) -> LeafGrid:
         d = LeafGrid(origins=g.origins, values=g.values, background=g.background, masks=g.masks)
@@ -1089,6 +1095,7 @@ def main():
     peak, peak_kind = _peaks()
     prof_ms = sum(v[0] for v in pprof.values())
     ranked = sorted(((k, v) for k, v in pprof.items() if pbytes.launch_bytes(k) is not None), key=lambda kv: -kv[1][0])
+    top_label, (top_ms, top_cnt) = max(pprof.items(), key=lambda kv: kv[1][0])
     dom_label, (dom_ms, dom_cnt) = ranked[0]
     dom_bytes = pbytes.launch_bytes(dom_label)
     dom_us = dom_ms / dom_cnt * 1e3
@@ -1155,9 +1162,14 @@ def main():
                          "avg_launch_us": round(dom_us, 2), "launches": dom_cnt,
                          "share_of_solve": round(dom_ms / prof_ms, 3),
                          "all_bandwidth_kernels_GBps": round(agg_bytes / (agg_ms * 1e-3) / 1e9, 1),
-                         "note": "the kernel class with the largest device time in one solve (CUDA event pairs "
-                                 "around every launch, host-driven loop); algorithmic bytes: every array the "
-                                 "kernel must touch once per DOF at 4 B, coefficient arrays only where stored"},
+                         "top_kernel_by_time": {"label": top_label, "share_of_solve": round(top_ms / prof_ms, 3),
+                                                "avg_launch_us": round(top_ms / top_cnt * 1e3, 2)},
+                         "note": "the bandwidth kernel class with the largest device time in one solve (CUDA event "
+                                 "pairs around every launch, host-driven loop); algorithmic bytes: every array the "
+                                 "kernel must touch once per DOF at 4 B, coefficient arrays only where stored; "
+                                 "top_kernel_by_time may be a latency-bound one (the cluster bottom-cycle kernel "
+                                 "with the coarsest CG)"},
+            "tuning": tuning,
             "kernel_profile_ms": {k: [round(v[0], 4), v[1]] for k, v in sorted(pprof.items(), key=lambda kv: -kv[1][0])},
             "clocks": clocks,
         }

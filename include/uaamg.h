@@ -38,6 +38,7 @@ extern "C" {
 #define UAAMG_ERR_OUT_OF_MEMORY (-3)
 #define UAAMG_ERR_DOMAIN_TOO_LARGE (-4)
 #define UAAMG_ERR_NO_DEVICE (-5)
+#define UAAMG_ERR_TIMEOUT (-6)
 
 /* PoissonSolver::SmootherOption (SIMD_UAAMG/simd_vdb_poisson.h:143-148) */
 #define UAAMG_SMOOTHER_SCHEDULED_RELAXED_JACOBI 0
@@ -95,6 +96,24 @@ int uaamg_poisson_create_with_rhs(const uaamg_leaf_grid* liquid_phi, const uaamg
                                   const uaamg_leaf_grid* vx, const uaamg_leaf_grid* vy, const uaamg_leaf_grid* vz,
                                   const uaamg_leaf_grid* solid_velocity, float dt, float dx, void* stream,
                                   uaamg_poisson** out);
+/* Kernel shapes of the solves by level size (process-wide).  Every setting
+ * gives the same results, except pipe_min_leaves where a level-0 dot product
+ * rides on the pipelined kernels (their per-CTA partials set the summation
+ * order; still deterministic for a given setting).  The defaults are the
+ * measured ones; uaamg_b200/tuning holds tables an autotuner wrote.  A change
+ * applies to the next solve of every handle (cached graphs are rebuilt).  No
+ * counterpart in the reference (its kernels have one shape). */
+typedef struct {
+    int32_t staged_min_leaves;  /* levels of at least this many leaves sweep with the bulk-copy staged kernels (64) */
+    int32_t split_min_leaves;   /* ... store a computed source (first sweep, prolongation) before sweeping (1024) */
+    int32_t pipe_min_leaves;    /* ... sweep with the persistent pipelined kernels (8192) */
+    int32_t elem_ctas_per_sm;   /* CTAs per SM of the grid-stride passes, 1..32 (16) */
+    int32_t bottom_cycle;       /* 1: both visits of the level above the coarsest, with the coarsest solves, as one
+                                 * thread-block-cluster launch where the level fits (1) */
+} uaamg_tuning;
+int uaamg_get_tuning(uaamg_tuning* out);
+int uaamg_set_tuning(const uaamg_tuning* tuning);
+
 /* ~PoissonSolver / ~LaplacianWithLevel */
 int uaamg_poisson_destroy(uaamg_poisson* h);
 
@@ -513,6 +532,71 @@ int uaamg_viscosity_set_stream(uaamg_viscosity* h, void* stream);
 /* 1 (default): host-driven first solve, CUDA graph afterwards; 2 graph always; 0 never. */
 int uaamg_viscosity_set_graph_mode(uaamg_viscosity* h, int use_graph);
 int64_t uaamg_viscosity_kernel_launches(const uaamg_viscosity* h);
+
+/* ---------------------------------------------------------------------------
+ * Served form: many simulations' solves on one GPU (no counterpart in the
+ * reference, which solves one domain per call).  A request is one simulation
+ * domain asking for `substeps` solves of one kind -- FLIP_vdb's pressure
+ * projection (FLIP_vdb.cpp:3118-3168) or its viscosity step (:3170-3216) --
+ * each substep with new face velocities (uaamg_server_push_velocity).  The
+ * server admits queued requests in submission order while their estimated
+ * device footprint fits budget_bytes (and the resident caps), keeps each
+ * request's hierarchy, face weights and warm start (the previous pressure)
+ * on the device until its last substep, solves the pending substeps of all
+ * resident pressure requests in one batched CUDA graph per round (batching 1)
+ * or one after another (batching 0), and runs every viscosity request on a
+ * lane of its own (a thread and a stream) in both modes.  Each pressure result
+ * is checked in FP64 (|b - A x|_inf / |b|_inf).  A result is the same alone
+ * and in the mix.  The loop runs on a thread of its own; every call below is
+ * thread-safe.  Inputs are copied at the call (host grids into host memory,
+ * device grids into device memory), so the caller may free them at once. */
+typedef struct uaamg_server uaamg_server;
+#define UAAMG_SERVER_POISSON 0
+#define UAAMG_SERVER_VISCOSITY 1
+typedef struct {
+    int64_t budget_bytes;       /* device memory the resident requests may use (64 GiB) */
+    int32_t max_poisson;        /* resident pressure requests at most (256) */
+    int32_t max_viscosity;      /* resident viscosity requests, i.e. lanes, at most (16) */
+    int32_t admit_per_round;    /* admissions per loop round at most (8) */
+    int32_t batching;           /* 1: one batched graph per pressure round; 0: every solve alone (1) */
+    int32_t keep_results;       /* 1: keep every substep's solution for uaamg_server_result (0) */
+    float pressure_tolerance;   /* relative residual of the pressure PCG (1e-7) */
+    float viscosity_tolerance;  /* relative residual of the viscosity PCG (1e-6) */
+} uaamg_server_options;
+typedef struct {
+    int64_t submitted, queued, resident, done, failed;
+    int64_t solves, rounds, batch_builds;
+    int64_t used_bytes, peak_bytes;
+} uaamg_server_stats_t;
+int uaamg_server_default_options(uaamg_server_options* options);
+int uaamg_server_create(const uaamg_server_options* options, uaamg_server** out);
+/* Stops the loop after the work in flight, frees every request. */
+int uaamg_server_destroy(uaamg_server* s);
+/* A pressure request: createPressurePoissonLaplacian's inputs (liquid SDF, face
+ * weights), the solid velocity of its rhs, dt, dx.  UAAMG_ERR_OUT_OF_MEMORY
+ * when its estimated footprint exceeds the whole budget. */
+int uaamg_server_submit_poisson(uaamg_server* s, const uaamg_leaf_grid* liquid_phi,
+                                const uaamg_leaf_grid* face_weights, const uaamg_leaf_grid* solid_velocity, float dt,
+                                float dx, int substeps, int64_t* request);
+/* A viscosity request: simd_viscosity3d's inputs (simd_viscosity3d.h:285-290). */
+int uaamg_server_submit_viscosity(uaamg_server* s, const uaamg_leaf_grid* viscosity,
+                                  const uaamg_leaf_grid* liquid_sdf, const uaamg_leaf_grid* solid_sdf,
+                                  const uaamg_leaf_grid* solid_velocity, float dt, float rho, float dx, int substeps,
+                                  int64_t* request);
+/* The face velocities (packed3grids channels) of the request's next substep. */
+int uaamg_server_push_velocity(uaamg_server* s, int64_t request, const uaamg_leaf_grid* u, const uaamg_leaf_grid* v,
+                               const uaamg_leaf_grid* w);
+/* Waits up to timeout_s for substep `substep` of a request; its PCG status
+ * (UAAMG_SUCCESS / UAAMG_FAILED), iterations, FP64 relative residual
+ * (pressure; -1 for viscosity) and latency (seconds from submission).
+ * UAAMG_ERR_TIMEOUT when it is not solved in time. */
+int uaamg_server_wait(uaamg_server* s, int64_t request, int substep, double timeout_s, int* status, int* iterations,
+                      double* fp64_residual, double* latency_s);
+/* A solved substep's solution (keep_results 1): *leaf_count leaves of level 0
+ * (float[leaf][512] pressure, float[3][leaf][512] velocity); x may be NULL to
+ * ask for the size. */
+int uaamg_server_result(uaamg_server* s, int64_t request, int substep, int64_t* leaf_count, float* x);
+int uaamg_server_stats(uaamg_server* s, uaamg_server_stats_t* out);
 
 const char* uaamg_last_error(void);
 int uaamg_device_count(void);

@@ -34,6 +34,16 @@ class LeafGridC(C.Structure):
     ]
 
 
+class TuningC(C.Structure):
+    _fields_ = [
+        ("staged_min_leaves", C.c_int32),
+        ("split_min_leaves", C.c_int32),
+        ("pipe_min_leaves", C.c_int32),
+        ("elem_ctas_per_sm", C.c_int32),
+        ("bottom_cycle", C.c_int32),
+    ]
+
+
 _lib = None
 
 # (name, restype, argtypes) of every exported entry point in include/uaamg.h
@@ -49,6 +59,8 @@ EXPORTS = [
     ("uaamg_poisson_copy_rhs", i32, [vp, vp]),
     ("uaamg_poisson_solve_fp64_reference", i32, [vp, vp, vp, C.c_double, i32, C.POINTER(i32),
                                                  C.POINTER(C.c_double)]),
+    ("uaamg_get_tuning", i32, [C.POINTER(TuningC)]),
+    ("uaamg_set_tuning", i32, [C.POINTER(TuningC)]),
     ("uaamg_poisson_destroy", i32, [vp]),
     ("uaamg_poisson_set_smoother", i32, [vp, i32]),
     ("uaamg_poisson_set_max_iterations", i32, [vp, i32]),

@@ -85,6 +85,38 @@ static inline bool key_less(const VdbKey& a, const VdbKey& b) {
     return false;
 }
 
+// vdb_key packed into one unsigned 128-bit number with the same order: the
+// root tile origins (multiples of 4096) biased into 20 bits each, then the
+// 15-bit and 12-bit child offsets of the two internal levels.
+static inline unsigned __int128 vdb_key128(const int32_t* o) {
+    const VdbKey k = vdb_key(o);
+    const uint64_t rx = (uint64_t)((k.k[0] >> 12) + (1 << 19)), ry = (uint64_t)((k.k[1] >> 12) + (1 << 19)),
+                   rz = (uint64_t)((k.k[2] >> 12) + (1 << 19));
+    const uint64_t hi = (rx << 40) | (ry << 20) | rz;
+    const uint64_t lo = ((uint64_t)k.k[3] << 12) | (uint64_t)k.k[4];
+    return ((unsigned __int128)hi << 27) | lo;
+}
+
+// The coarse DOF bits one fine leaf contributes to its parent (a coarse voxel
+// is a DOF if any of its 2x2x2 fine voxels is): fine word x holds the (y,z)
+// plane (bit 8y + z); pairs of planes are OR-ed, then pairs in y and z, and the
+// 4x4 bits at (2yy, 2zz) are compressed into nibbles and placed at the
+// octant's (y, z) quarter of the coarse words ox*4 .. ox*4+3.
+static inline void coarse_bits_from_child(const uint64_t* fm, int a, uint64_t* cw) {
+    const int ox = (a >> 2) & 1, oy = (a >> 1) & 1, oz = a & 1;
+    for (int px = 0; px < 4; ++px) {
+        uint64_t p = fm[2 * px] | fm[2 * px + 1];
+        p |= p >> 1;  // z pairs
+        p |= p >> 8;  // y pairs
+        uint64_t q = p & 0x0055005500550055ull;       // bits 16 yy + 2 zz
+        q = (q | (q >> 1)) & 0x0033003300330033ull;
+        q = (q | (q >> 2)) & 0x000F000F000F000Full;   // nibble yy (bit zz) at bit 16 yy
+        const uint64_t dep = (q & 0xFull) | (((q >> 16) & 0xFull) << 8) | (((q >> 32) & 0xFull) << 16) |
+                             (((q >> 48) & 0xFull) << 24);
+        cw[ox * 4 + px] |= dep << (oy * 32 + oz * 4);
+    }
+}
+
 // population count of a 64-bit mask on the host (SWAR bit count; inline, no
 // library call on CPUs compiled without a popcount instruction)
 static inline int host_popc64(uint64_t x) {
@@ -172,55 +204,64 @@ static void finalize_host_level(HostLevel& L) {
 static void coarsen_topology(HostLevel& F, HostLevel& C) {
     C.dt = F.dt;
     C.dx = 2.0f * F.dx;
-    std::vector<std::pair<VdbKey, int>> keys(F.nl);
-    std::vector<int32_t> corg((size_t)F.nl * 3);
+    // the coarse leaf of fine leaf l (origin / 2, leaf-aligned) is at leaf
+    // coordinate l >> 1; unique coarse leaves through a dense mark over their
+    // bounding box, then only those sorted into tree order
+    const int clo[3] = {F.map.lo[0] >> 1, F.map.lo[1] >> 1, F.map.lo[2] >> 1};
+    const int cdim[3] = {((F.map.lo[0] + F.map.dim[0] - 1) >> 1) - clo[0] + 1,
+                         ((F.map.lo[1] + F.map.dim[1] - 1) >> 1) - clo[1] + 1,
+                         ((F.map.lo[2] + F.map.dim[2] - 1) >> 1) - clo[2] + 1};
+    std::vector<uint8_t> seen((size_t)cdim[0] * cdim[1] * cdim[2], 0);
+    std::vector<std::pair<unsigned __int128, int>> keys;
+    std::vector<int32_t> corg;
+    keys.reserve(F.nl / 4 + 8);
+    corg.reserve((size_t)(F.nl / 4 + 8) * 3);
     for (int i = 0; i < F.nl; ++i) {
-        for (int c = 0; c < 3; ++c) corg[3 * i + c] = (F.org[3 * i + c] / 2) & ~7;
-        keys[i] = {vdb_key(&corg[3 * i]), i};
+        const int l[3] = {F.org[3 * i] >> 4, F.org[3 * i + 1] >> 4, F.org[3 * i + 2] >> 4};
+        const size_t cell = ((size_t)(l[0] - clo[0]) * cdim[1] + (l[1] - clo[1])) * cdim[2] + (l[2] - clo[2]);
+        if (seen[cell]) continue;
+        seen[cell] = 1;
+        const int k = (int)keys.size();
+        corg.push_back(l[0] * 8);
+        corg.push_back(l[1] * 8);
+        corg.push_back(l[2] * 8);
+        keys.push_back({vdb_key128(&corg[3 * (size_t)k]), k});
     }
-    std::sort(keys.begin(), keys.end(), [](const std::pair<VdbKey, int>& a, const std::pair<VdbKey, int>& b) {
-        return key_less(a.first, b.first);
-    });
-    std::vector<int32_t> uorg;
-    for (int i = 0; i < F.nl; ++i) {
-        if (i > 0 && !key_less(keys[i - 1].first, keys[i].first)) continue;
-        const int32_t* o = &corg[3 * keys[i].second];
-        uorg.insert(uorg.end(), o, o + 3);
-    }
-    int nu = (int)(uorg.size() / 3);
+    std::sort(keys.begin(), keys.end());
+    const int nu = (int)keys.size();
+    std::vector<int32_t> uorg((size_t)nu * 3);
+    for (int i = 0; i < nu; ++i) std::copy(&corg[3 * (size_t)keys[i].second], &corg[3 * (size_t)keys[i].second] + 3, &uorg[3 * (size_t)i]);
     std::vector<uint64_t> cmask((size_t)nu * 8, 0);
     std::vector<int32_t> child((size_t)nu * 8, -1);
     for (int i = 0; i < nu; ++i) {
         for (int a = 0; a < 8; ++a) {
-            int fo[3] = {2 * uorg[3 * i] + ((a >> 2) & 1) * 8, 2 * uorg[3 * i + 1] + ((a >> 1) & 1) * 8,
-                         2 * uorg[3 * i + 2] + (a & 1) * 8};
-            int fl = F.map.find_leaf(fo[0] >> 3, fo[1] >> 3, fo[2] >> 3);
+            const int lx = (2 * uorg[3 * i] + ((a >> 2) & 1) * 8) >> 3, ly = (2 * uorg[3 * i + 1] + ((a >> 1) & 1) * 8) >> 3,
+                      lz = (2 * uorg[3 * i + 2] + (a & 1) * 8) >> 3;
+            const int fl = F.map.find_leaf(lx, ly, lz);
             child[8 * i + a] = fl;
-            if (fl < 0) continue;
-            const int ox = (a >> 2) & 1, oy = (a >> 1) & 1, oz = a & 1;
-            // fine word x holds the (y,z) plane; OR pairs of planes, then pairs in y and z
-            for (int px = 0; px < 4; ++px) {
-                uint64_t p = F.mask[8 * fl + 2 * px] | F.mask[8 * fl + 2 * px + 1];
-                p |= (p >> 1);  // z pairs (bit z and z+1 of a row)
-                p |= (p >> 8);  // y pairs
-                uint64_t& w = cmask[8 * i + ox * 4 + px];
-                for (int yy = 0; yy < 4; ++yy)
-                    for (int zz = 0; zz < 4; ++zz)
-                        if ((p >> (16 * yy + 2 * zz)) & 1ull) w |= 1ull << ((oy * 4 + yy) * 8 + oz * 4 + zz);
-            }
+            if (fl >= 0) coarse_bits_from_child(&F.mask[8 * (size_t)fl], a, &cmask[8 * (size_t)i]);
         }
     }
     // drop leaves without DOF
-    C.org.clear(); C.mask.clear(); C.child.clear();
+    int nc = 0;
     for (int i = 0; i < nu; ++i) {
         uint64_t any = 0;
         for (int w = 0; w < 8; ++w) any |= cmask[8 * i + w];
-        if (!any) continue;
-        C.org.insert(C.org.end(), &uorg[3 * i], &uorg[3 * i] + 3);
-        C.mask.insert(C.mask.end(), &cmask[8 * i], &cmask[8 * i] + 8);
-        C.child.insert(C.child.end(), &child[8 * i], &child[8 * i] + 8);
+        nc += any != 0;
     }
-    C.nl = (int)(C.org.size() / 3);
+    C.org.resize((size_t)nc * 3);
+    C.mask.resize((size_t)nc * 8);
+    C.child.resize((size_t)nc * 8);
+    for (int i = 0, k = 0; i < nu; ++i) {
+        uint64_t any = 0;
+        for (int w = 0; w < 8; ++w) any |= cmask[8 * i + w];
+        if (!any) continue;
+        std::copy(&uorg[3 * i], &uorg[3 * i] + 3, &C.org[3 * (size_t)k]);
+        std::copy(&cmask[8 * i], &cmask[8 * i] + 8, &C.mask[8 * (size_t)k]);
+        std::copy(&child[8 * i], &child[8 * i] + 8, &C.child[8 * (size_t)k]);
+        ++k;
+    }
+    C.nl = nc;
     finalize_host_level(C);
     F.parent.assign(F.nl, -1);
     F.octant.assign(F.nl, 0);
@@ -319,24 +360,40 @@ static T* carve(char*& cur, size_t count) {
 }
 static size_t carve_size(size_t count, size_t elem) { return (count * elem + 255) & ~size_t(255); }
 
+// Device copy of an input grid and its leaf map.  When `share` (a grid whose
+// device map `share_dg` is already built) lists the same leaves in the same
+// order, as the face-velocity channels and the face weights of a staggered
+// grid usually do, its map is reused and only the values go up.
 static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf_grid* gr, DevGrid& dg, HostMap& map,
-                           std::vector<void*>& tofree) {
-    map.build(gr->leaf_count, gr->origins);
+                           std::vector<void*>& tofree, const uaamg_leaf_grid* share = nullptr,
+                           const DevGrid* share_dg = nullptr) {
+    const bool same = share && share_dg && share_dg->g.map && share->leaf_count == gr->leaf_count &&
+                      gr->leaf_count > 0 &&
+                      (share->origins == gr->origins ||
+                       memcmp(share->origins, gr->origins, (size_t)gr->leaf_count * 3 * sizeof(int32_t)) == 0);
+    if (!same) map.build(gr->leaf_count, gr->origins);
     dg.g = DGrid{};
     dg.g.comps = gr->components;
     dg.g.bg0 = gr->background[0];
     dg.g.bg1 = gr->components > 1 ? gr->background[1] : 0.f;
     dg.g.bg2 = gr->components > 2 ? gr->background[2] : 0.f;
     if (gr->leaf_count == 0) return;
-    size_t mapn = map.idx.size();
+    size_t mapn = same ? 0 : map.idx.size();
     size_t vbytes = (size_t)gr->leaf_count * UAAMG_LEAF * gr->components * sizeof(float);
     size_t total = carve_size(mapn, 4) + (gr->values_on_device ? 0 : carve_size(vbytes, 1));
     void* mem = nullptr;
     CK(ctx_dev_alloc(ctx, &mem, total, stream));
     tofree.push_back(mem);
     char* cur = (char*)mem;
-    int* dmap = carve<int>(cur, mapn);
-    CK(cudaMemcpyAsync(dmap, map.idx.data(), mapn * 4, cudaMemcpyHostToDevice, stream));
+    int* dmap = nullptr;
+    if (same) {
+        dmap = const_cast<int*>(share_dg->g.map);
+        dg.g.lo0 = share_dg->g.lo0; dg.g.lo1 = share_dg->g.lo1; dg.g.lo2 = share_dg->g.lo2;
+        dg.g.d0 = share_dg->g.d0; dg.g.d1 = share_dg->g.d1; dg.g.d2 = share_dg->g.d2;
+    } else {
+        dmap = carve<int>(cur, mapn);
+        CK(cudaMemcpyAsync(dmap, map.idx.data(), mapn * 4, cudaMemcpyHostToDevice, stream));
+    }
     const float* vals = gr->values;
     if (!gr->values_on_device) {
         float* dv = carve<float>(cur, vbytes / 4);
@@ -345,8 +402,10 @@ static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf
     }
     dg.g.val = vals;
     dg.g.map = dmap;
-    dg.g.lo0 = map.lo[0]; dg.g.lo1 = map.lo[1]; dg.g.lo2 = map.lo[2];
-    dg.g.d0 = map.dim[0]; dg.g.d1 = map.dim[1]; dg.g.d2 = map.dim[2];
+    if (!same) {
+        dg.g.lo0 = map.lo[0]; dg.g.lo1 = map.lo[1]; dg.g.lo2 = map.lo[2];
+        dg.g.d0 = map.dim[0]; dg.g.d1 = map.dim[1]; dg.g.d2 = map.dim[2];
+    }
 }
 
 static void upload_grid(uaamg_poisson* h, const uaamg_leaf_grid* gr, DevGrid& dg, HostMap& map,
@@ -468,7 +527,9 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             CK(cudaEventRecord(ev_in.e, s));
             CK(cudaStreamWaitEvent(s2, ev_in.e, 0));
             const uaamg_leaf_grid* vg[4] = {ri->vx, ri->vy, ri->vz, ri->sv};
-            for (int k = 0; k < 4; ++k) upload_grid_cs(h->ctx, s2, vg[k], dvel[k], vmap[k], tofree);
+            // the channels' maps come from the face weights' when the leaves match (the face-weight map
+            // was uploaded on the first stream, which the second stream waits for)
+            for (int k = 0; k < 4; ++k) upload_grid_cs(h->ctx, s2, vg[k], dvel[k], vmap[k], tofree, fw, &dfw);
             CK(cudaEventRecord(ev_vel.e, s2));
         }
         TRACE("upload inputs");
@@ -495,22 +556,22 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         CK(cudaStreamSynchronize(s));
         TRACE("DOF mask kernel + D2H");
         // ---- level-0 DOF leaves in tree order
-        std::vector<std::pair<VdbKey, int>> keys;
+        std::vector<std::pair<unsigned __int128, int>> keys;
         keys.reserve(nphi);
         for (int64_t i = 0; i < nphi; ++i) {
             uint64_t any = 0;
             for (int w = 0; w < 8; ++w) any |= dofmask[8 * i + w];
-            if (any) keys.push_back({vdb_key(&phi->origins[3 * i]), (int)i});
+            if (any) keys.push_back({vdb_key128(&phi->origins[3 * i]), (int)i});
         }
-        std::sort(keys.begin(), keys.end(), [](const std::pair<VdbKey, int>& a, const std::pair<VdbKey, int>& b) {
-            return key_less(a.first, b.first);
-        });
+        std::sort(keys.begin(), keys.end());
         std::vector<int32_t> src(keys.size());
+        L0.org.resize(keys.size() * 3);
+        L0.mask.resize(keys.size() * 8);
         for (size_t i = 0; i < keys.size(); ++i) {
-            int sidx = keys[i].second;
+            const int sidx = keys[i].second;
             src[i] = sidx;
-            L0.org.insert(L0.org.end(), &phi->origins[3 * sidx], &phi->origins[3 * sidx] + 3);
-            L0.mask.insert(L0.mask.end(), &dofmask[8 * (size_t)sidx], &dofmask[8 * (size_t)sidx] + 8);
+            std::copy(&phi->origins[3 * sidx], &phi->origins[3 * sidx] + 3, &L0.org[3 * i]);
+            std::copy(&dofmask[8 * (size_t)sidx], &dofmask[8 * (size_t)sidx] + 8, &L0.mask[8 * i]);
         }
         L0.nl = (int)keys.size();
         finalize_host_level(L0);
@@ -694,7 +755,14 @@ static bool g_use_pdl = true;
 // Level sweeps with SrcPlain on levels of at least STAGED_MIN_LEAVES leaves run
 // the bulk-async staged kernels (UAAMG_STAGED=0 turns them off).
 static bool g_use_staged = true;
-#define STAGED_MIN_LEAVES 64
+// Kernel shapes by level size (uaamg_set_tuning): the defaults below, or the
+// table an autotuner wrote.  Every choice gives the same results; only the
+// speed differs.  g_tune_gen is part of every graph's key, so a change rebuilds
+// cached graphs.
+static uaamg_tuning g_tune = {64, 1024, 8192, 16, 1};
+static int g_tune_gen = 0;
+static int g_sms = 148;  // SMs of the device (set when a handle is created)
+#define STAGED_MIN_LEAVES (g_tune.staged_min_leaves)
 // On levels of at least SPLIT_MIN_LEAVES leaves a sweep whose source is
 // computed (the first sweep from a zero guess, the prolongation-add) runs as
 // k_materialize of the source and a staged plain sweep: the fused kernel
@@ -702,18 +770,17 @@ static bool g_use_staged = true;
 // which costs more than one extra elementwise pass on large levels.  The
 // stored values are the ones the fused kernel computes, so the results are
 // identical.
-#define SPLIT_MIN_LEAVES 1024
+#define SPLIT_MIN_LEAVES (g_tune.split_min_leaves)
 // Levels of at least PIPE_MIN_LEAVES leaves sweep with the persistent
 // pipelined kernels (several leaves per CTA); smaller staged levels with the
 // one-leaf staged kernels, which start faster.
-#define PIPE_MIN_LEAVES 8192
+#define PIPE_MIN_LEAVES (g_tune.pipe_min_leaves)
 // Grid of the grid-stride elementwise kernels (k_materialize, the PCG
 // vector updates): 16 CTAs of 128 threads per SM of a 148-SM B200, at most
 // one per leaf.  One CTA per leaf would make a large level's elementwise
 // pass cost the GPU's CTA launch rate (about a nanosecond per CTA) instead
 // of its bytes.
-#define ELEM_CTAS 2368
-static unsigned elem_grid(int nl) { return (unsigned)std::min(nl, ELEM_CTAS); }
+static unsigned elem_grid(int nl) { return (unsigned)std::min(nl, g_tune.elem_ctas_per_sm * g_sms); }
 template <typename... KArgs, typename... Args>
 static void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
     cudaLaunchConfig_t cfg = {};
@@ -1215,7 +1282,7 @@ static void enqueue_finish(Enq& E) {
 }
 
 static int graph_key(const uaamg_poisson* h) {
-    int k = h->smoother;
+    int k = h->smoother + 4 * g_tune_gen;
     for (int l = 0; l < h->nlev; ++l) k = k * 3 + (h->lv[l].w_sor == 1.2f ? 0 : 1);
     return k;
 }
@@ -1441,7 +1508,12 @@ static int create_impl(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid*
         h->st_host = reinterpret_cast<PcgState*>(h->pin_state);
         h->scalar_host = reinterpret_cast<float*>((char*)h->pin_state + ((sizeof(PcgState) + 63) & ~size_t(63)));
         noalloc_resolve(h);
-        h->bot_state = g_use_bottom ? -1 : 0;
+        h->bot_state = (g_use_bottom && g_tune.bottom_cycle) ? -1 : 0;
+        {
+            int sms = 0;
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->ctx->device) == cudaSuccess && sms > 0)
+                g_sms = sms;
+        }
         build_hierarchy(h, liquid_phi, face_weights, dt, dx, ri);
     } catch (const UaamgError& e) {
         uaamg_poisson_destroy(h);
@@ -1986,6 +2058,23 @@ int uaamg_poisson_profile_pcg(uaamg_poisson* h, float* d_pressure, const float* 
     CK(cudaStreamSynchronize(h->stream));
     return h->st_host->status == PCG_SUCCESS ? UAAMG_SUCCESS : UAAMG_FAILED;
     ABI_END
+}
+
+int uaamg_get_tuning(uaamg_tuning* out) {
+    if (!out) { set_error("out is NULL"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    *out = g_tune;
+    return UAAMG_SUCCESS;
+}
+int uaamg_set_tuning(const uaamg_tuning* t) {
+    if (!t) { set_error("tuning is NULL"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    if (t->staged_min_leaves < 1 || t->split_min_leaves < 1 || t->pipe_min_leaves < 1 || t->elem_ctas_per_sm < 1 ||
+        t->elem_ctas_per_sm > 32 || (t->bottom_cycle != 0 && t->bottom_cycle != 1)) {
+        set_error("tuning out of range (leaf thresholds >= 1, elem_ctas_per_sm 1..32, bottom_cycle 0/1)");
+        return UAAMG_ERR_INVALID_ARGUMENT;
+    }
+    g_tune = *t;
+    ++g_tune_gen;
+    return UAAMG_SUCCESS;
 }
 
 int uaamg_poisson_set_stream(uaamg_poisson* h, void* stream) {

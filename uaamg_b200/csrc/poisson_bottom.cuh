@@ -251,8 +251,6 @@ __global__ void __launch_bounds__(BOT_THREADS, 1) k_bottom(BottomArgs A) {
             me->oct = L.octant[leaf];
         }
     }
-    CgRows<ROWS> M;
-    if (rank == 0) cg_rows_load<ROWS, BOT_NT>(A.C, M);
     griddep_wait();
     griddep_launch();
     for (int j = group; j < P; j += NG) {
@@ -281,8 +279,10 @@ __global__ void __launch_bounds__(BOT_THREADS, 1) k_bottom(BottomArgs A) {
         }
         // residual of T restricted into the coarsest rhs
         BOT_EACH(bot_restrict(me, t, rs, bc0c, group));
-        // coarsest solve (its second visit in the W-cycle re-solves the same system: skipped)
-        if (rank == 0) cg_rows_solve<ROWS, BOT_NT>(M, bc0, xc0, ps, red);
+        // coarsest solve (its second visit in the W-cycle re-solves the same system: skipped).  The rows
+        // are loaded from L2 for each solve: holding them in registers across the whole kernel measured
+        // three times slower (31 against 11 us per solve on the 1916-DOF level)
+        if (rank == 0) coarsest_cg_body<ROWS, BOT_NT, false>(A.C, bc0, xc0, ps, red);
         cluster_sync_all();
         // post-smoothing with reversed weights: T += P x_c, x = J(T), T = J(x), x = J(T)
         BOT_EACH(bot_prolong(me, t, xc0c));

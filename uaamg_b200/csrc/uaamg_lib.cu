@@ -6,3 +6,4 @@
 #include "viscosity.cu"
 #include "projection.cu"
 #include "extrapolate.cu"
+#include "server.cu"

@@ -31,17 +31,6 @@ static inline uint64_t yband(int lo, int hi) {
     for (int y = lo; y <= hi; ++y) b |= 0xFFull << (8 * y);
     return b;
 }
-// vdb_key packed into one unsigned 128-bit number with the same order: the
-// root tile origins (multiples of 4096) biased into 20 bits each, then the
-// 15-bit and 12-bit child offsets of the two internal levels.
-static inline unsigned __int128 vdb_key128(const int32_t* o) {
-    const VdbKey k = vdb_key(o);
-    const uint64_t rx = (uint64_t)((k.k[0] >> 12) + (1 << 19)), ry = (uint64_t)((k.k[1] >> 12) + (1 << 19)),
-                   rz = (uint64_t)((k.k[2] >> 12) + (1 << 19));
-    const uint64_t hi = (rx << 40) | (ry << 20) | rz;
-    const uint64_t lo = ((uint64_t)k.k[3] << 12) | (uint64_t)k.k[4];
-    return ((unsigned __int128)hi << 27) | lo;
-}
 static void sort_unique_vdb(std::vector<int32_t>& org) {
     const size_t n = org.size() / 3;
     std::vector<std::pair<unsigned __int128, uint32_t>> keys(n);
