@@ -822,31 +822,83 @@ def run_projection(args, dev, stream, timed, max_over_ranks, ws, rank):
 
 
 def run_served(args, ws):
-    """The served stream on this GPU: batched (pressure rounds in one graph,
-    viscosity lanes overlapping) vs the plain form (every solve alone, in
-    arrival order).  Wall-clock latencies from arrival to the last substep."""
+    """The served stream through the native server (uaamg_server_*): requests
+    are submitted at their arrival times; each simulation pushes its next
+    substep's face velocities once its previous substep is solved (a closed
+    loop, as a FLIP substep needs the previous solution), so requests arrive
+    and progress while others are being served.  Batched (pressure rounds in
+    one graph) vs plain (every pressure solve alone); viscosity requests run
+    on lanes of their own in both.  Latency: arrival to the last substep.
+    Every pressure result carries its FP64 relative residual."""
     import torch
-    from uaamg_b200.serve import DeviceBackend, Scheduler, latency_summary, make_stream
+    from uaamg_b200 import scenes
+    from uaamg_b200.serve import make_stream
+    from uaamg_b200.server import NativeServer
+    dev = torch.device("cuda", torch.cuda.current_device())
     free, _ = torch.cuda.mem_get_info()
-    out = {"workload": SERVE_WORKLOAD, "window_s": args.serve_window}
+    out = {"workload": SERVE_WORKLOAD, "window_s": args.serve_window, "server": "native (uaamg_server_*)"}
     for mode in ("batched", "plain"):
         reqs = make_stream(args.serve_window, seed=4)
-        be = DeviceBackend(batching=(mode == "batched"))
-        sch = Scheduler(be, int(0.5 * free))
-        elapsed = sch.run(reqs, time_limit=args.serve_limit)
+        srv = NativeServer(batching=(mode == "batched"), budget_bytes=int(0.5 * free))
+        t0 = time.perf_counter()
+        pending = sorted(reqs, key=lambda r: r.arrival)
+        live = []  # [request, server id, next substep to push, substeps waited]
+        lat, res64, it_p, stat_ok, solves = [], [], [], True, 0
+        by_kind = {"poisson": [], "viscosity": []}
+        while pending or live:
+            now = time.perf_counter() - t0
+            if now > args.serve_limit:
+                break
+            while pending and pending[0].arrival <= now:
+                r = pending.pop(0)
+                if r.kind == "poisson":
+                    phi, fw, sv, dt, dx = scenes.device_poisson_instance(r.side, r.seed, dev)
+                    rid = srv.submit_poisson(phi, fw, sv, dt, dx, r.substeps)
+                else:
+                    liq, sol, mu, sv, dt, rho, dx = scenes.device_viscosity_instance(r.side, r.seed, dev)
+                    rid = srv.submit_viscosity(mu, liq, sol, sv, dt, rho, dx, r.substeps)
+                srv.push_velocity(rid, *scenes.device_face_velocities(r.side, r.seed * 1000003, dev))
+                live.append([r, rid, 1, 0])
+            progressed = False
+            for e in list(live):
+                r, rid, nxt, got = e
+                try:
+                    w = srv.wait(rid, got, 0.0)
+                except Exception:
+                    continue  # not solved yet
+                progressed = True
+                e[3] = got = got + 1
+                solves += 1
+                stat_ok &= w["status"] == 0
+                if r.kind == "poisson":
+                    res64.append(w["fp64_residual"])
+                    it_p.append(w["iterations"])
+                if nxt < r.substeps:
+                    srv.push_velocity(rid, *scenes.device_face_velocities(r.side, r.seed * 1000003 + nxt, dev))
+                    e[2] = nxt + 1
+                if got == r.substeps:
+                    live.remove(e)
+                    lat.append(w["latency_s"])
+                    by_kind[r.kind].append(w["latency_s"])
+            if not progressed:
+                time.sleep(0.0005)
+        elapsed = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
         torch.cuda.synchronize()
-        done = sch.done
-        kinds = {}
-        for k in ("poisson", "viscosity"):
-            dk = [r for r in done if r.kind == k]
-            kinds[k] = {"requests": sum(r.kind == k for r in reqs), "completed": len(dk),
-                        "solves": int(sum(r.substeps for r in dk)), **latency_summary(dk)}
-        out[mode] = {"requests": len(reqs), "completed": len(done), "solves": int(sch.solves),
-                     "elapsed_s": round(elapsed, 3), "solves_per_s": round(sch.solves / elapsed, 1),
-                     **latency_summary(done), "by_kind": kinds, "pressure_rounds": sch.rounds,
-                     "batch_graphs_built": be.batch_builds, "peak_budget_GB": round(sch.peak_used / 1e9, 2),
-                     "all_status_success": all(all(s == 0 for s in r.status) for r in done)}
-        del be, sch
+
+        def pct(a, q):
+            return round(float(np.percentile(np.array(a), q)) * 1e3, 2) if a else None
+
+        out[mode] = {"requests": len(reqs), "completed": st["done"], "solves": solves, "elapsed_s": round(elapsed, 3),
+                     "solves_per_s": round(solves / elapsed, 1), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+                     "by_kind": {k: {"completed": len(v), "p50_ms": pct(v, 50), "p99_ms": pct(v, 99)}
+                                 for k, v in by_kind.items()},
+                     "pressure_rounds": st["rounds"], "batch_graphs_built": st["batch_builds"],
+                     "peak_budget_GB": round(st["peak_bytes"] / 1e9, 2), "all_status_success": bool(stat_ok),
+                     "pressure_fp64_rel_residual_max": max(res64) if res64 else None,
+                     "pressure_iterations_mean": round(float(np.mean(it_p)), 2) if it_p else None}
+        del srv
     b, p = out["batched"], out["plain"]
     out["solves_per_s_vs_plain"] = round(b["solves_per_s"] / p["solves_per_s"], 3) if p["solves_per_s"] else None
     return out

@@ -97,16 +97,15 @@ int uaamg_poisson_create_with_rhs(const uaamg_leaf_grid* liquid_phi, const uaamg
                                   const uaamg_leaf_grid* solid_velocity, float dt, float dx, void* stream,
                                   uaamg_poisson** out);
 /* Kernel shapes of the solves by level size (process-wide).  Every setting
- * gives the same results, except pipe_min_leaves where a level-0 dot product
- * rides on the pipelined kernels (their per-CTA partials set the summation
- * order; still deterministic for a given setting).  The defaults are the
+ * gives the same results (a pass that carries a level-0 dot product switches
+ * kernels at a fixed size, whatever pipe_min_leaves is).  The defaults are the
  * measured ones; uaamg_b200/tuning holds tables an autotuner wrote.  A change
  * applies to the next solve of every handle (cached graphs are rebuilt).  No
  * counterpart in the reference (its kernels have one shape). */
 typedef struct {
     int32_t staged_min_leaves;  /* levels of at least this many leaves sweep with the bulk-copy staged kernels (64) */
     int32_t split_min_leaves;   /* ... store a computed source (first sweep, prolongation) before sweeping (1024) */
-    int32_t pipe_min_leaves;    /* ... sweep with the persistent pipelined kernels (8192) */
+    int32_t pipe_min_leaves;    /* ... sweep and restrict with the persistent pipelined kernels (8192) */
     int32_t elem_ctas_per_sm;   /* CTAs per SM of the grid-stride passes, 1..32 (16) */
     int32_t bottom_cycle;       /* 1: both visits of the level above the coarsest, with the coarsest solves, as one
                                  * thread-block-cluster launch where the level fits (1) */

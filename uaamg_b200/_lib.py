@@ -44,6 +44,24 @@ class TuningC(C.Structure):
     ]
 
 
+class ServerOptionsC(C.Structure):
+    _fields_ = [
+        ("budget_bytes", C.c_int64),
+        ("max_poisson", C.c_int32),
+        ("max_viscosity", C.c_int32),
+        ("admit_per_round", C.c_int32),
+        ("batching", C.c_int32),
+        ("keep_results", C.c_int32),
+        ("pressure_tolerance", C.c_float),
+        ("viscosity_tolerance", C.c_float),
+    ]
+
+
+class ServerStatsC(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "queued", "resident", "done", "failed", "solves", "rounds",
+                                         "batch_builds", "used_bytes", "peak_bytes")]
+
+
 _lib = None
 
 # (name, restype, argtypes) of every exported entry point in include/uaamg.h
@@ -59,6 +77,16 @@ EXPORTS = [
     ("uaamg_poisson_copy_rhs", i32, [vp, vp]),
     ("uaamg_poisson_solve_fp64_reference", i32, [vp, vp, vp, C.c_double, i32, C.POINTER(i32),
                                                  C.POINTER(C.c_double)]),
+    ("uaamg_server_default_options", i32, [C.POINTER(ServerOptionsC)]),
+    ("uaamg_server_create", i32, [C.POINTER(ServerOptionsC), C.POINTER(vp)]),
+    ("uaamg_server_destroy", i32, [vp]),
+    ("uaamg_server_submit_poisson", i32, [vp, pLG, pLG, pLG, f32, f32, i32, C.POINTER(C.c_int64)]),
+    ("uaamg_server_submit_viscosity", i32, [vp, pLG, pLG, pLG, pLG, f32, f32, f32, i32, C.POINTER(C.c_int64)]),
+    ("uaamg_server_push_velocity", i32, [vp, C.c_int64, pLG, pLG, pLG]),
+    ("uaamg_server_wait", i32, [vp, C.c_int64, i32, C.c_double, C.POINTER(i32), C.POINTER(i32),
+                                C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("uaamg_server_result", i32, [vp, C.c_int64, i32, C.POINTER(C.c_int64), vp]),
+    ("uaamg_server_stats", i32, [vp, C.POINTER(ServerStatsC)]),
     ("uaamg_get_tuning", i32, [C.POINTER(TuningC)]),
     ("uaamg_set_tuning", i32, [C.POINTER(TuningC)]),
     ("uaamg_poisson_destroy", i32, [vp]),

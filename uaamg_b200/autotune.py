@@ -21,9 +21,10 @@ candidate settings on representative solves and keeps the fastest:
   and sets it with ``uaamg_set_tuning``.  Nothing applies a table implicitly:
   the library starts from its built-in defaults.
 
-``pipe_min_leaves`` is not searched: the pipelined kernels carry the level-0
-dot products with one partial per CTA, so moving that threshold across the
-level-0 size changes the summation order of the PCG's dots.
+``pipe_min_leaves`` moves only the passes without a dot product: the passes
+that carry the PCG's level-0 dot products switch to the pipelined kernels at a
+fixed size (their per-CTA partials set the summation order), so no setting
+changes a result.
 
     python -m uaamg_b200.autotune --out uaamg_b200/tuning/NVIDIA_B200.json
 """
@@ -45,6 +46,7 @@ NEVER = 1 << 30  # a leaf threshold no level reaches
 # the searched values of each result-neutral knob
 SPACE = {
     "bottom_cycle": [0, 1],
+    "pipe_min_leaves": [1024, 2048, 4096, 8192, 16384],
     "staged_min_leaves": [16, 32, 64, 128, 256, 512],
     "split_min_leaves": [256, 512, 1024, 2048, 4096, NEVER],
     "elem_ctas_per_sm": [4, 8, 16, 32],

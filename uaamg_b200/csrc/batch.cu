@@ -302,8 +302,8 @@ struct BEnq {
     void coarsest(int d, int br, int outr, bool dot) {
         const std::array<uaamg_batch::Range, 3>& c = b->coarse[d];
         const unsigned* act = b->active;
-        if (c[0].count) launch(k_bcoarsest<4, 256>, (unsigned)c[0].count, 256, s, recs(d), b->lists + c[0].off, act, br, outr);
-        if (c[1].count) launch(k_bcoarsest<8, 256>, (unsigned)c[1].count, 256, s, recs(d), b->lists + c[1].off, act, br, outr);
+        if (c[0].count) launch(k_bcoarsest<2, 512>, (unsigned)c[0].count, 512, s, recs(d), b->lists + c[0].off, act, br, outr);
+        if (c[1].count) launch(k_bcoarsest<4, 512>, (unsigned)c[1].count, 512, s, recs(d), b->lists + c[1].off, act, br, outr);
         if (c[2].count) launch(k_bcoarsest<4, 1024>, (unsigned)c[2].count, 1024, s, recs(d), b->lists + c[2].off, act, br, outr);
         count += (c[0].count > 0) + (c[1].count > 0) + (c[2].count > 0);
         if (dot && d == 0 && b->dot1.count) {

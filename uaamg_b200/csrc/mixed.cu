@@ -249,7 +249,7 @@ static void menq_visit(MEnq& E, int l, bool skip_first, DotOut dot, float* z) {
     const bool split = g_use_staged && L.nl >= SPLIT_MIN_LEAVES;
     int* err = &h->st->error;
     const size_t psm = pipe_smem_bytes<MLevel<T>>();
-    const bool pipe = staged && L.nl >= PIPE_MIN_LEAVES;
+    const bool pipe = staged && L.nl >= PIPE_DOT_MIN_LEAVES;
     auto sweep = [&](const T* x, T* out, float w) {  // plain source
         if (pipe)
             E.run_pipe("jacobi staged", l, k_pipe<M_JACOBI, MLevel<T>, T, false>, L.nl, psm, L, x, (const T*)rhs, out,

@@ -273,6 +273,22 @@ static void coarsen_topology(HostLevel& F, HostLevel& C) {
 }
 
 // ---------------------------------------------------------------------------
+// Bump allocator over a pinned host block.  Small tables go up through it: a
+// cudaMemcpyAsync from pageable memory first waits for the work already in the
+// stream (the large input copies), a copy from pinned memory does not.  An
+// item that does not fit goes up from its pageable source.
+struct PinStage {
+    char* base = nullptr;
+    size_t cap = 0, off = 0;
+    const void* put(const void* src, size_t bytes) {
+        if (!base || off + bytes > cap) return src;
+        char* p = base + off;
+        memcpy(p, src, bytes);
+        off = (off + bytes + 15) & ~size_t(15);
+        return p;
+    }
+};
+
 struct DevGrid {  // device copy of an input grid + its leaf map
     DGrid g{};
     void* mem = nullptr;
@@ -302,6 +318,8 @@ struct uaamg_poisson {
     size_t pin_state_cap = 0;
     void* pin_stage = nullptr;  // pinned staging of the topology upload
     size_t pin_stage_cap = 0;
+    void* pin_in = nullptr;  // pinned staging of the small input tables (leaf maps, origins, masks)
+    size_t pin_in_cap = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t body_stream = nullptr;
@@ -366,7 +384,7 @@ static size_t carve_size(size_t count, size_t elem) { return (count * elem + 255
 // grid usually do, its map is reused and only the values go up.
 static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf_grid* gr, DevGrid& dg, HostMap& map,
                            std::vector<void*>& tofree, const uaamg_leaf_grid* share = nullptr,
-                           const DevGrid* share_dg = nullptr) {
+                           const DevGrid* share_dg = nullptr, PinStage* stage = nullptr) {
     const bool same = share && share_dg && share_dg->g.map && share->leaf_count == gr->leaf_count &&
                       gr->leaf_count > 0 &&
                       (share->origins == gr->origins ||
@@ -392,7 +410,8 @@ static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf
         dg.g.d0 = share_dg->g.d0; dg.g.d1 = share_dg->g.d1; dg.g.d2 = share_dg->g.d2;
     } else {
         dmap = carve<int>(cur, mapn);
-        CK(cudaMemcpyAsync(dmap, map.idx.data(), mapn * 4, cudaMemcpyHostToDevice, stream));
+        const void* src = stage ? stage->put(map.idx.data(), mapn * 4) : map.idx.data();
+        CK(cudaMemcpyAsync(dmap, src, mapn * 4, cudaMemcpyHostToDevice, stream));
     }
     const float* vals = gr->values;
     if (!gr->values_on_device) {
@@ -409,8 +428,8 @@ static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf
 }
 
 static void upload_grid(uaamg_poisson* h, const uaamg_leaf_grid* gr, DevGrid& dg, HostMap& map,
-                        std::vector<void*>& tofree) {
-    upload_grid_cs(h->ctx, h->stream, gr, dg, map, tofree);
+                        std::vector<void*>& tofree, PinStage* stage = nullptr) {
+    upload_grid_cs(h->ctx, h->stream, gr, dg, map, tofree, nullptr, nullptr, stage);
 }
 
 static void check_grid(const uaamg_leaf_grid* g, int comps, const char* name) {
@@ -512,8 +531,11 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         // ---- inputs to the device
         HostMap phimap, fwmap;
         DevGrid dphi, dfw;
-        upload_grid(h, phi, dphi, phimap, tofree);
-        upload_grid(h, fw, dfw, fwmap, tofree);
+        // the small input tables go up through a pinned block the handle keeps
+        CK(ctx_pinned_acquire(h->ctx, (size_t)4 << 20, &h->pin_in, &h->pin_in_cap));
+        PinStage stage{(char*)h->pin_in, h->pin_in_cap, 0};
+        upload_grid(h, phi, dphi, phimap, tofree, &stage);
+        upload_grid(h, fw, dfw, fwmap, tofree, &stage);
         // The velocities of the right-hand side go up on a second stream once
         // the SDF and the face weights are up, so their copies overlap the DOF
         // mask kernel, the host topology and the coefficient kernels.
@@ -529,7 +551,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             const uaamg_leaf_grid* vg[4] = {ri->vx, ri->vy, ri->vz, ri->sv};
             // the channels' maps come from the face weights' when the leaves match (the face-weight map
             // was uploaded on the first stream, which the second stream waits for)
-            for (int k = 0; k < 4; ++k) upload_grid_cs(h->ctx, s2, vg[k], dvel[k], vmap[k], tofree, fw, &dfw);
+            for (int k = 0; k < 4; ++k) upload_grid_cs(h->ctx, s2, vg[k], dvel[k], vmap[k], tofree, fw, &dfw, &stage);
             CK(cudaEventRecord(ev_vel.e, s2));
         }
         TRACE("upload inputs");
@@ -541,10 +563,12 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         uint64_t* dphimask = carve<uint64_t>(cur, (size_t)nphi * 8);
         uint64_t* ddofmask = carve<uint64_t>(cur, (size_t)nphi * 8);
         int* dphiorg = carve<int>(cur, (size_t)nphi * 3);
-        CK(cudaMemcpyAsync(dphiorg, phi->origins, (size_t)nphi * 12, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(dphiorg, stage.put(phi->origins, (size_t)nphi * 12), (size_t)nphi * 12,
+                           cudaMemcpyHostToDevice, s));
         const uint64_t* pm = nullptr;
         if (phi->masks) {
-            CK(cudaMemcpyAsync(dphimask, phi->masks, (size_t)nphi * 64, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(dphimask, stage.put(phi->masks, (size_t)nphi * 64), (size_t)nphi * 64,
+                               cudaMemcpyHostToDevice, s));
             pm = dphimask;
         }
         const float dtOverDxSqr = dt / (dx * dx);
@@ -775,6 +799,11 @@ static int g_sms = 148;  // SMs of the device (set when a handle is created)
 // pipelined kernels (several leaves per CTA); smaller staged levels with the
 // one-leaf staged kernels, which start faster.
 #define PIPE_MIN_LEAVES (g_tune.pipe_min_leaves)
+// A pass that carries a level-0 dot product (the last post-smoothing sweep
+// with z.r, A p with p.q) uses the pipelined kernel from this fixed size on:
+// its per-CTA partials set the dot's summation order, which must not depend
+// on the tuning.  The mixed-precision form uses it for all its passes.
+#define PIPE_DOT_MIN_LEAVES 8192
 // Grid of the grid-stride elementwise kernels (k_materialize, the PCG
 // vector updates): 16 CTAs of 128 threads per SM of a 148-SM B200, at most
 // one per leaf.  One CTA per leaf would make a large level's elementwise
@@ -883,7 +912,7 @@ struct Enq {
         if constexpr (std::is_same<Src, SrcPlain>::value) {
             if (g_use_staged && D.L.nl >= STAGED_MIN_LEAVES && !(MODE == M_SPAI0 && mark_spai0)) {
                 if (prof) pb("L" + std::to_string(l) + " " + mode_name(MODE) + " staged" + (dot.r ? "+dot" : ""));
-                if (D.L.nl >= PIPE_MIN_LEAVES)
+                if (D.L.nl >= (dot.r ? PIPE_DOT_MIN_LEAVES : PIPE_MIN_LEAVES))
                     launch_pipe(k_pipe<MODE, DLevel, float, false>, D.L.nl, pipe_smem_bytes<DLevel>(), s, D.L,
                                 (const float*)src.x, b, out, w, ws, 1.0f - ws, dot, (const float*)nullptr, 0.f,
                                 &h->st->error);
@@ -954,8 +983,8 @@ struct Enq {
         at[1].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = at;
         cfg.numAttrs = g_use_pdl ? 2 : 1;
-        if (h->bot_rows == 4) CK(cudaLaunchKernelEx(&cfg, k_bottom<4>, A));
-        else CK(cudaLaunchKernelEx(&cfg, k_bottom<8>, A));
+        if (h->bot_rows == 2) CK(cudaLaunchKernelEx(&cfg, k_bottom<2>, A));
+        else CK(cudaLaunchKernelEx(&cfg, k_bottom<4>, A));
         pe();
         count++;
     }
@@ -963,8 +992,8 @@ struct Enq {
         if (h->C.n == 0) return;
         pb("coarsest cg");
         switch (coarsest_class(h->C.n)) {
-            case 0: launch(k_coarsest_cg<4, 256>, 1, 256, s, h->C, rhs, out); break;
-            case 1: launch(k_coarsest_cg<8, 256>, 1, 256, s, h->C, rhs, out); break;
+            case 0: launch(k_coarsest_cg<2, 512>, 1, 512, s, h->C, rhs, out); break;
+            case 1: launch(k_coarsest_cg<4, 512>, 1, 512, s, h->C, rhs, out); break;
             default: launch(k_coarsest_cg<4, 1024>, 1, 1024, s, h->C, rhs, out); break;
         }
         pe();
@@ -1012,13 +1041,13 @@ static bool use_bottom(uaamg_poisson* h) {
     if (nl <= 0 || nlc <= 0 || h->C.n <= 0 || coarsest_class(h->C.n) > 1) return false;
     const int P = (nl + BOT_MAX_CLUSTER - 1) / BOT_MAX_CLUSTER;
     const int C = (nl + P - 1) / P;
-    const int rows = coarsest_class(h->C.n) == 0 ? 4 : 8;
+    const int rows = coarsest_class(h->C.n) == 0 ? 2 : 4;
     const size_t smem = bottom_smem_bytes(P, nlc, rows);
     int optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->ctx->device));
     const int max_dynamic = optin - 1024;  // above the kernel's static shared memory
     if (smem > (size_t)max_dynamic) return false;
-    if ((rows == 4 ? bottom_clusters<4>(C, smem, max_dynamic) : bottom_clusters<8>(C, smem, max_dynamic)) < 1)
+    if ((rows == 2 ? bottom_clusters<2>(C, smem, max_dynamic) : bottom_clusters<4>(C, smem, max_dynamic)) < 1)
         return false;
     h->bot_C = C;
     h->bot_P = P;
@@ -1249,7 +1278,7 @@ static void enqueue_setup(Enq& E, cudaGraphConditionalHandle cond, int use_cond)
 static void enqueue_Ap(Enq& E) {
     uaamg_poisson* h = E.h;
     LevelDev& D0 = h->lv[0];
-    if (g_use_staged && D0.L.nl >= PIPE_MIN_LEAVES)
+    if (g_use_staged && D0.L.nl >= PIPE_DOT_MIN_LEAVES)
         launch_pipe(k_pipe<M_LAPLACIAN, DLevel, float, false, 1>, D0.L.nl, pipe_smem_bytes<DLevel>(), E.s, D0.L,
                     (const float*)h->p, (const float*)nullptr, h->q, 0.f, 0.f, 0.f,
                     DotOut{h->p, h->partials, h->st}, (const float*)nullptr, 0.f, &h->st->error);
@@ -1552,6 +1581,7 @@ int uaamg_poisson_destroy(uaamg_poisson* h) {
         if (h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
         ctx_pinned_release(h->ctx, h->pin_state, h->pin_state_cap);
         ctx_pinned_release(h->ctx, h->pin_stage, h->pin_stage_cap);
+        ctx_pinned_release(h->ctx, h->pin_in, h->pin_in_cap);
         ctx_stream_release(h->ctx, h->body_stream);
         ctx_stream_release(h->ctx, h->own_stream);
     }

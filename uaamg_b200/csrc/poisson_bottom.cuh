@@ -24,9 +24,9 @@ namespace uaamg {
 
 namespace cgx = cooperative_groups;
 
-constexpr int BOT_THREADS = 256;     // two 128-thread leaf groups; the coarsest CG's block shape
+constexpr int BOT_THREADS = 512;     // four 128-thread leaf groups; the coarsest CG's block shape
 constexpr int BOT_MAX_CLUSTER = 16;  // non-portable cluster size limit
-constexpr int BOT_NT = 256;          // threads of the coarsest CG (coarsest_class 0 and 1)
+constexpr int BOT_NT = 512;          // threads of the coarsest CG (coarsest_class 0 and 1)
 
 // One leaf of level lb in shared memory.
 struct __align__(16) SLeaf {

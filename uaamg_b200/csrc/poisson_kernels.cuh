@@ -1232,9 +1232,10 @@ struct DCoarsest {
 };
 
 // Thread-block shapes of the coarsest CG, by system size (rows per thread,
-// threads): few warps keep the barriers and reductions of an iteration short;
-// the rows' entries stay in registers.  The batched solve uses the same shape
-// for the same size, so its results match the single solve bit for bit.
+// threads): 512 threads with 2 or 4 rows each up to 2048 DOF, 1024 threads
+// with 4 rows above; the rows' entries stay in registers.  The batched solve
+// and the cluster bottom-cycle kernel use the same shape for the same size, so
+// their results match the single solve bit for bit.
 #define CG_MAX_DOF 4096
 __host__ __device__ __forceinline__ int coarsest_class(int n) { return n <= 1024 ? 0 : (n <= 2048 ? 1 : 2); }
 

@@ -282,15 +282,29 @@ static void srv_viscosity_lane(uaamg_server* s, SrvReq* r) {
 
 // One pressure round over `act` (requests with a pending substep whose
 // inputs were taken out of their queues into `subs`).
-static void srv_pressure_round(uaamg_server* s, std::vector<SrvReq*>& act,
+static void srv_fail(uaamg_server* s, SrvReq& r, const char* what) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r.state = RQ_FAILED;
+    r.error = std::string(what) + ": " + uaamg_last_error();
+    s->cv.notify_all();
+}
+
+static void srv_pressure_round(uaamg_server* s, std::vector<SrvReq*>& act_in,
                                std::vector<std::unique_ptr<SrvSubstep>>& subs) {
-    const size_t n = act.size();
-    for (size_t i = 0; i < n; ++i) {
-        SrvReq& r = *act[i];
+    // the substep's rhs of every request; a request whose inputs fail leaves the round, failed
+    std::vector<SrvReq*> act;
+    for (size_t i = 0; i < act_in.size(); ++i) {
+        SrvReq& r = *act_in[i];
         uaamg_leaf_grid fw = srv_fw_view(r), u = subs[i]->u.view(), v = subs[i]->v.view(), w = subs[i]->w.view();
         uaamg_leaf_grid sv = r.sv.view();
-        CKC(uaamg_poisson_build_rhs_device(r.hp, &fw, &u, &v, &w, &sv, r.dt, r.drhs));
+        if (uaamg_poisson_build_rhs_device(r.hp, &fw, &u, &v, &w, &sv, r.dt, r.drhs) < 0) {
+            srv_fail(s, r, "right-hand side");
+            continue;
+        }
+        act.push_back(&r);
     }
+    const size_t n = act.size();
+    if (n == 0) return;
     std::vector<int> iters(n, 0), status(n, 0);
     if (s->opt.batching) {
         std::vector<int64_t> key(n);
@@ -429,12 +443,21 @@ static void srv_loop(uaamg_server* s) {
                         r->lane = std::thread(srv_viscosity_lane, s, r);
                     }
                 } catch (const UaamgError&) {
-                    std::lock_guard<std::mutex> lk(s->mu);
-                    r->state = RQ_FAILED;
-                    r->error = uaamg_last_error();
+                    srv_fail(s, *r, "admission");
                 }
             }
-            if (!act.empty()) srv_pressure_round(s, act, subs);
+            if (!act.empty()) {
+                try {
+                    srv_pressure_round(s, act, subs);
+                } catch (const UaamgError&) {
+                    // a solve of the round failed: its requests fail, the server goes on
+                    std::string msg = uaamg_last_error();
+                    if (s->batch) uaamg_batch_destroy(s->batch);
+                    s->batch = nullptr;
+                    s->batch_key.clear();
+                    for (SrvReq* r : act) srv_fail(s, *r, ("pressure round: " + msg).c_str());
+                }
+            }
             if (!admit.empty() || !act.empty()) srv_notify(s);
         }
     } catch (const UaamgError&) {
