@@ -232,8 +232,16 @@ int uaamg_poisson_precondition(uaamg_poisson* h, const float* r, float* z);
 int uaamg_poisson_profile_pcg(uaamg_poisson* h, float* d_pressure, const float* d_rhs, int max_classes,
                               char* names, double* total_ms, int64_t* counts, int* nclasses);
 
-/* Stream (cudaStream_t as void*) used by *_device calls; NULL = the handle's own stream. */
+/* Stream (cudaStream_t as void*) used by *_device calls; NULL = the handle's own stream.
+ * The handle's own stream is non-blocking: it is not ordered with the legacy
+ * default stream or any other stream, so device inputs written on another
+ * stream must be complete (or that stream's work ordered before the call, by
+ * an event the handle's stream waits on) before a call reads them, and work
+ * on other streams that reads a call's device outputs waits for the handle's
+ * stream the same way.  uaamg_poisson_get_stream returns the stream the
+ * handle's calls run on. */
 int uaamg_poisson_set_stream(uaamg_poisson* h, void* stream);
+int uaamg_poisson_get_stream(const uaamg_poisson* h, void** stream);
 /* PCG driver: 1 (default) host-driven loop for a handle's first solve and the
  * CUDA-graph solve (conditional WHILE node) from the second solve on; 2 the
  * graph always; 0 the host-driven loop always. */
@@ -409,7 +417,10 @@ int uaamg_batch_solve_pcg_device(uaamg_batch* b, float* const* d_pressure, const
                                  int* iterations, int* status);
 /* Per-instance results of the last solve (any pointer may be NULL). */
 int uaamg_batch_results(const uaamg_batch* b, int* iterations, int* status, float* final_residual);
+/* Stream of the batch's calls (NULL = its own non-blocking stream; the
+ * ordering rules of uaamg_poisson_set_stream apply). */
 int uaamg_batch_set_stream(uaamg_batch* b, void* stream);
+int uaamg_batch_get_stream(const uaamg_batch* b, void** stream);
 /* 1 (default): the CUDA graph with a WHILE node; 0: host-driven loop. */
 int uaamg_batch_set_graph_mode(uaamg_batch* b, int use_graph);
 /* Kernels launched by the last batched solve. */
@@ -527,7 +538,10 @@ int uaamg_viscosity_precondition(uaamg_viscosity* h, const float* r, float* z);
 int uaamg_viscosity_profile_pcg(uaamg_viscosity* h, float* d_velocity, const float* d_rhs, float tolerance,
                                 int max_classes, char* names, double* total_ms, int64_t* counts,
                                 int* nclasses);
+/* Stream of the handle's calls (NULL = its own non-blocking stream; the
+ * ordering rules of uaamg_poisson_set_stream apply). */
 int uaamg_viscosity_set_stream(uaamg_viscosity* h, void* stream);
+int uaamg_viscosity_get_stream(const uaamg_viscosity* h, void** stream);
 /* 1 (default): host-driven first solve, CUDA graph afterwards; 2 graph always; 0 never. */
 int uaamg_viscosity_set_graph_mode(uaamg_viscosity* h, int use_graph);
 int64_t uaamg_viscosity_kernel_launches(const uaamg_viscosity* h);
@@ -548,7 +562,9 @@ int64_t uaamg_viscosity_kernel_launches(const uaamg_viscosity* h);
  * is checked in FP64 (|b - A x|_inf / |b|_inf).  A result is the same alone
  * and in the mix.  The loop runs on a thread of its own; every call below is
  * thread-safe.  Inputs are copied at the call (host grids into host memory,
- * device grids into device memory), so the caller may free them at once. */
+ * device grids into device memory), so the caller may free them at once;
+ * device grids must be complete when the call is made (the copy is not
+ * ordered after work on the caller's streams). */
 typedef struct uaamg_server uaamg_server;
 #define UAAMG_SERVER_POISSON 0
 #define UAAMG_SERVER_VISCOSITY 1

@@ -132,3 +132,26 @@ int main() {
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.split() == ["0", "4", "0", "0", "0"]
+
+
+def test_torch_ordering_detects_cuda_arguments():
+    """The Python classes order a call with torch's stream when an argument is
+    a CUDA tensor, a LeafGrid holding one, or a list of either; host data is
+    not ordered (no torch calls)."""
+    import torch
+    from uaamg_b200 import _lib
+    from uaamg_b200.grids import LeafGrid
+
+    class FakeCuda:  # stands in for a CUDA tensor on a machine without a GPU
+        is_cuda = True
+
+    g = LeafGrid(origins=np.zeros((1, 3), np.int32), values=np.zeros((1, 512), np.float32), background=0.0)
+    assert not _lib.is_cuda(g, np.zeros(3), torch.zeros(3), [torch.zeros(2)], None)
+    assert _lib.is_cuda(FakeCuda())
+    assert _lib.is_cuda([torch.zeros(1), FakeCuda()])
+    g.values = FakeCuda()
+    assert _lib.is_cuda(None, g)
+    # nothing to order: the context manager neither loads torch.cuda state nor the library
+    with _lib.torch_ordered("poisson", None, np.zeros(3), torch.zeros(3)):
+        pass
+    _lib.torch_inputs_ready(None, np.zeros(3), torch.zeros(3))

@@ -447,3 +447,41 @@ def test_bottom_cycle_cluster_kernel_identical(gpu, n):
         assert label in prof_on and label not in prof_off
         assert "coarsest cg" in prof_off and "coarsest cg" not in prof_on
         assert sum(v[1] for v in prof_on.values()) < sum(v[1] for v in prof_off.values())
+
+
+def test_torch_stream_ordering(gpu):
+    """Device inputs that torch's current stream is still writing when a call
+    is made: the Python classes order the handle's stream after torch's and
+    torch's after the handle's, so creation, the rhs and the solve see the
+    final values (each input is first set to a wrong value, then written again
+    behind a device sleep of a few ms, with no host synchronisation)."""
+    import copy
+    torch = gpu
+    from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver
+    dev = torch.device("cuda")
+    n = 64
+    phi, fw, sv, dt, dx = scenes.device_poisson_instance(n, 5, dev)
+    vel = scenes.device_face_velocities(n, 7, dev)
+    torch.cuda.synchronize()
+    lap0 = LaplacianWithLevel.createPressurePoissonLaplacian(phi, fw, dt, dx)
+    rhs0 = lap0.createPressurePoissonRightHandSide(fw, *vel, sv, dt)
+    x0 = lap0.getZeroVectorGrid()
+    assert PoissonSolver(lap0).solveMultigridPCG(x0, rhs0) == 0
+
+    def late(g, wrong):
+        h = copy.copy(g)
+        h.values = torch.full_like(g.values, wrong)
+        torch.cuda._sleep(20_000_000)
+        h.values.copy_(g.values)
+        return h
+
+    lap = LaplacianWithLevel.createPressurePoissonLaplacian(late(phi, -1.0), late(fw, 0.5), dt, dx)
+    assert lap.leaf_count(0) == lap0.leaf_count(0) and lap.num_levels() == lap0.num_levels()
+    rhs = torch.full((lap.leaf_count(0), 512), float("nan"), device=dev)
+    lap.createPressurePoissonRightHandSide(fw, *[late(v, 9.0) for v in vel], sv, dt, out=rhs)
+    x = torch.full_like(rhs, 7.0)
+    torch.cuda._sleep(20_000_000)
+    x.zero_()
+    s = PoissonSolver(lap)
+    assert s.solveMultigridPCG(x, rhs) == 0
+    assert np.array_equal(rhs.cpu().numpy(), rhs0) and np.array_equal(x.cpu().numpy(), x0)

@@ -120,10 +120,17 @@ def test_served_under_a_tight_budget(gpu):
     as others complete, and the results do not change."""
     torch = gpu
     from uaamg_b200.server import NativeServer
-    big = 48
-    phi, fw, sv, dt, dx = scenes.device_poisson_instance(big, 12, torch.device("cuda"))
-    # the server's own estimate for the largest request, plus a little
-    est = phi.leaf_count * 512 * 4 * 20 + (64 << 20)
+    dev = torch.device("cuda")
+    # the server's own estimate (leaf arrays of the largest input grid, plus
+    # 64 MiB) for the largest request, plus a little
+    ests = []
+    for side, seed, _ in POIS:
+        phi, fw, sv, dt, dx = scenes.device_poisson_instance(side, seed, dev)
+        ests.append(max(phi.leaf_count, fw.leaf_count) * 512 * 4 * 20 + (64 << 20))
+    for side, seed, _ in VISC:
+        liq, sol, mu, sv, dt, rho, dx = scenes.device_viscosity_instance(side, seed, dev)
+        ests.append(max(liq.leaf_count, sol.leaf_count) * 512 * 4 * 110 + (64 << 20))
+    est = max(ests)
     reqs, res, stats = _served(torch, True, budget=int(est * 1.2), interleave=False)
     assert stats["peak_bytes"] <= int(est * 1.2) and stats["done"] == len(reqs)
     alone = [_alone_poisson(torch, *p) for p in POIS] + [_alone_viscosity(torch, *v) for v in VISC]

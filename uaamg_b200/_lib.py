@@ -6,6 +6,7 @@ different code path.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 
@@ -126,6 +127,7 @@ EXPORTS = [
     ("uaamg_poisson_precondition", i32, [vp, vp, vp]),
     ("uaamg_poisson_profile_pcg", i32, [vp, vp, vp, i32, vp, vp, vp, C.POINTER(C.c_int)]),
     ("uaamg_poisson_set_stream", i32, [vp, vp]),
+    ("uaamg_poisson_get_stream", i32, [vp, C.POINTER(vp)]),
     ("uaamg_poisson_set_graph_mode", i32, [vp, i32]),
     ("uaamg_poisson_kernel_launches", i64, [vp]),
     ("uaamg_poisson_prepare_mixed", i32, [vp, i32, vp]),
@@ -144,6 +146,7 @@ EXPORTS = [
     ("uaamg_batch_solve_pcg_device", i32, [vp, vp, vp, vp, vp]),
     ("uaamg_batch_results", i32, [vp, vp, vp, vp]),
     ("uaamg_batch_set_stream", i32, [vp, vp]),
+    ("uaamg_batch_get_stream", i32, [vp, C.POINTER(vp)]),
     ("uaamg_batch_set_graph_mode", i32, [vp, i32]),
     ("uaamg_batch_kernel_launches", i64, [vp]),
     ("uaamg_viscosity_create", i32, [pLG, pLG, pLG, f32, f32, f32, C.POINTER(vp)]),
@@ -173,6 +176,7 @@ EXPORTS = [
     ("uaamg_viscosity_precondition", i32, [vp, vp, vp]),
     ("uaamg_viscosity_profile_pcg", i32, [vp, vp, vp, f32, i32, vp, vp, vp, C.POINTER(C.c_int)]),
     ("uaamg_viscosity_set_stream", i32, [vp, vp]),
+    ("uaamg_viscosity_get_stream", i32, [vp, C.POINTER(vp)]),
     ("uaamg_viscosity_set_graph_mode", i32, [vp, i32]),
     ("uaamg_viscosity_kernel_launches", i64, [vp]),
     ("uaamg_last_error", C.c_char_p, []),
@@ -210,3 +214,70 @@ def ptr(a) -> int | None:
         assert a.flags["C_CONTIGUOUS"]
         return a.ctypes.data
     return a.data_ptr()
+
+
+# ----------------------------------------------------------------------------- torch stream ordering
+# The library's handles run on streams of their own (non-blocking: not ordered
+# with torch's streams).  The Python classes order every call that passes torch
+# CUDA tensors with torch's current stream, so tensors torch is still writing
+# are not read early and torch's kernels do not read outputs (or reuse input
+# memory) before the library is done with them.
+def is_cuda(*objs) -> bool:
+    """True when an argument is, or holds (a LeafGrid's values, a list), a
+    torch CUDA tensor."""
+    for o in objs:
+        if isinstance(o, (list, tuple)):
+            if is_cuda(*o):
+                return True
+            continue
+        if hasattr(o, "is_cuda"):  # a tensor (whose .values is a method, not data)
+            if o.is_cuda:
+                return True
+            continue
+        if getattr(getattr(o, "values", None), "is_cuda", False):  # a LeafGrid
+            return True
+    return False
+
+
+def handle_stream(kind: str, h) -> int:
+    """The stream a poisson / viscosity / batch handle's calls run on."""
+    s = C.c_void_p()
+    check(getattr(lib(), f"uaamg_{kind}_get_stream")(h, C.byref(s)), f"uaamg_{kind}_get_stream")
+    return int(s.value or 0)
+
+
+@contextlib.contextmanager
+def torch_ordered(kind: str, h, *objs):
+    """Around a call on handle ``h`` that reads or writes ``objs``: when one
+    of them is a torch CUDA tensor, the handle's stream first waits for the
+    work torch's current stream holds, and torch's current stream then waits
+    for the call's work.  Both waits are device events; the host does not
+    block."""
+    if not is_cuda(*objs):
+        yield
+        return
+    import torch
+    cur = torch.cuda.current_stream()
+    ext = torch.cuda.ExternalStream(handle_stream(kind, h))
+    ext.wait_stream(cur)
+    try:
+        yield
+    finally:
+        cur.wait_stream(ext)
+
+
+def torch_inputs_ready(stream, *objs) -> None:
+    """Before a call that takes torch CUDA tensors without a handle to order
+    on (a creation on the new handle's own stream, a server submission):
+    torch's current stream is synchronised, so the tensors are written."""
+    if not stream and is_cuda(*objs):
+        import torch
+        torch.cuda.current_stream().synchronize()
+
+
+def torch_after(kind: str, h, *objs) -> None:
+    """After a creation that read torch CUDA tensors: torch's current stream
+    waits for the new handle's stream (kernels still reading the inputs)."""
+    if is_cuda(*objs):
+        import torch
+        torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(handle_stream(kind, h)))

@@ -85,7 +85,8 @@ class PoissonBatch:
                 xs[i], bs[i] = x.data_ptr(), b.data_ptr()
         its, sts = (C.c_int * n)(), (C.c_int * n)()
         fn = L.uaamg_batch_solve_pcg if host else L.uaamg_batch_solve_pcg_device
-        rc = _lib.check(fn(self._h, xs, bs, its, sts), "uaamg_batch_solve_pcg")
+        with _lib.torch_ordered("batch", self._h, in_out_pressures, rhss):
+            rc = _lib.check(fn(self._h, xs, bs, its, sts), "uaamg_batch_solve_pcg")
         self.mIterationTaken = [int(v) for v in its]
         self.status = [int(v) for v in sts]
         return int(rc)

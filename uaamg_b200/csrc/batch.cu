@@ -799,6 +799,11 @@ int uaamg_batch_set_stream(uaamg_batch* b, void* stream) {
     return UAAMG_SUCCESS;
 }
 
+int uaamg_batch_get_stream(const uaamg_batch* b, void** stream) {
+    if (!b || !stream) { set_error("NULL argument"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    *stream = (void*)b->stream;
+    return UAAMG_SUCCESS;
+}
 int uaamg_batch_set_graph_mode(uaamg_batch* b, int use_graph) {
     if (!b) { set_error("NULL batch"); return UAAMG_ERR_INVALID_ARGUMENT; }
     b->use_graph = use_graph ? 1 : 0;

@@ -2116,6 +2116,11 @@ int uaamg_poisson_set_stream(uaamg_poisson* h, void* stream) {
     }
     return UAAMG_SUCCESS;
 }
+int uaamg_poisson_get_stream(const uaamg_poisson* h, void** stream) {
+    if (!h || !stream) { set_error("NULL argument"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    *stream = (void*)h->stream;
+    return UAAMG_SUCCESS;
+}
 int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph) {
     if (!h || use_graph < 0 || use_graph > 2) { set_error("invalid graph mode"); return UAAMG_ERR_INVALID_ARGUMENT; }
     h->use_graph = use_graph;

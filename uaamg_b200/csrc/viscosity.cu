@@ -1296,6 +1296,11 @@ int uaamg_viscosity_set_stream(uaamg_viscosity* h, void* stream) {
     return UAAMG_SUCCESS;
     ABI_END
 }
+int uaamg_viscosity_get_stream(const uaamg_viscosity* h, void** stream) {
+    if (!h || !stream) { set_error("NULL argument"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    *stream = (void*)h->stream;
+    return UAAMG_SUCCESS;
+}
 int uaamg_viscosity_set_graph_mode(uaamg_viscosity* h, int use_graph) {
     ABI_BEGIN
     require(h != nullptr, "handle is NULL");

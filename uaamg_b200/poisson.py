@@ -68,8 +68,10 @@ class LaplacianWithLevel:
         a = _as_c(liquid_phi, keep)
         b = _as_c(face_weights, keep)
         h = C.c_void_p()
+        _lib.torch_inputs_ready(stream, liquid_phi, face_weights)
         _lib.check(L.uaamg_poisson_create_on_stream(C.byref(a), C.byref(b), float(dt), float(dx), stream,
                                                     C.byref(h)), "uaamg_poisson_create")
+        _lib.torch_after("poisson", h.value, liquid_phi, face_weights)
         return LaplacianWithLevel(h.value, dt, dx)
 
     @staticmethod
@@ -82,10 +84,13 @@ class LaplacianWithLevel:
         ``PoissonSolver.solveMultigridPCGResident``."""
         L = _lib.lib()
         keep: list = []
-        gs = [_as_c(g, keep) for g in (liquid_phi, face_weights, vx, vy, vz, solid_velocity)]
+        grids = (liquid_phi, face_weights, vx, vy, vz, solid_velocity)
+        gs = [_as_c(g, keep) for g in grids]
         h = C.c_void_p()
+        _lib.torch_inputs_ready(stream, grids)
         _lib.check(L.uaamg_poisson_create_with_rhs(*[C.byref(g) for g in gs], float(dt), float(dx), stream,
                                                    C.byref(h)), "uaamg_poisson_create_with_rhs")
+        _lib.torch_after("poisson", h.value, grids)
         return LaplacianWithLevel(h.value, dt, dx)
 
     def copy_rhs(self, out=None):
@@ -93,7 +98,8 @@ class LaplacianWithLevel:
         into a torch CUDA tensor)."""
         rhs = self.getZeroVectorGrid() if out is None else out
         ptr = rhs.ctypes.data if isinstance(rhs, np.ndarray) else rhs.data_ptr()
-        _lib.check(_lib.lib().uaamg_poisson_copy_rhs(self._h, ptr), "copy_rhs")
+        with _lib.torch_ordered("poisson", self._h, rhs):
+            _lib.check(_lib.lib().uaamg_poisson_copy_rhs(self._h, ptr), "copy_rhs")
         return rhs
 
     def __del__(self):
@@ -142,9 +148,11 @@ class LaplacianWithLevel:
         gs = [_as_c(g, keep) for g in (face_weights, vx, vy, vz, solid_velocity)]
         L = _lib.lib()
         if out is not None and not isinstance(out, np.ndarray):
-            _lib.check(L.uaamg_poisson_build_rhs_device(self._h, *[C.byref(g) for g in gs], float(dt),
-                                                        out.data_ptr()), "build_rhs_device")
+            with _lib.torch_ordered("poisson", self._h, out, face_weights, vx, vy, vz, solid_velocity):
+                _lib.check(L.uaamg_poisson_build_rhs_device(self._h, *[C.byref(g) for g in gs], float(dt),
+                                                            out.data_ptr()), "build_rhs_device")
             return out
+        _lib.torch_inputs_ready(None, face_weights, vx, vy, vz, solid_velocity)
         rhs = self.getZeroVectorGrid() if out is None else out
         _lib.check(L.uaamg_poisson_build_rhs(self._h, *[C.byref(g) for g in gs], float(dt), rhs.ctypes.data),
                    "build_rhs")
@@ -152,9 +160,10 @@ class LaplacianWithLevel:
 
     def residual_norm_device(self, d_x, d_b, d_r, d_norm) -> None:
         """r = b - A x and |r|_inf into device tensors (enqueued on the handle's stream)."""
-        _lib.check(_lib.lib().uaamg_poisson_residual_norm_device(self._h, d_x.data_ptr(), d_b.data_ptr(),
-                                                                 d_r.data_ptr(), d_norm.data_ptr()),
-                   "residual_norm_device")
+        with _lib.torch_ordered("poisson", self._h, d_x, d_b, d_r, d_norm):
+            _lib.check(_lib.lib().uaamg_poisson_residual_norm_device(self._h, d_x.data_ptr(), d_b.data_ptr(),
+                                                                     d_r.data_ptr(), d_norm.data_ptr()),
+                       "residual_norm_device")
 
     def set_stream(self, stream_ptr) -> None:
         _lib.check(_lib.lib().uaamg_poisson_set_stream(self._h, stream_ptr), "set_stream")
@@ -256,7 +265,8 @@ class PoissonSolver:
             rhs = np.ascontiguousarray(rhs, np.float32)
             rc = getattr(L, host_fn)(h, pressure.ctypes.data, rhs.ctypes.data, C.byref(it))
         else:
-            rc = getattr(L, dev_fn)(h, pressure.data_ptr(), rhs.data_ptr(), C.byref(it))
+            with _lib.torch_ordered("poisson", h, pressure, rhs):
+                rc = getattr(L, dev_fn)(h, pressure.data_ptr(), rhs.data_ptr(), C.byref(it))
         _lib.check(rc, host_fn)
         self.mIterationTaken = int(it.value)
         return int(rc)
@@ -281,7 +291,8 @@ class PoissonSolver:
         else:
             assert not pure_multigrid, "the device form is PCG only"
             fn = "uaamg_poisson_solve_pcg_resident_device"
-            rc = L.uaamg_poisson_solve_pcg_resident_device(h, out_pressure.data_ptr(), C.byref(it))
+            with _lib.torch_ordered("poisson", h, out_pressure):
+                rc = L.uaamg_poisson_solve_pcg_resident_device(h, out_pressure.data_ptr(), C.byref(it))
         _lib.check(rc, fn)
         self.mIterationTaken = int(it.value)
         return int(rc)
@@ -312,8 +323,9 @@ class PoissonSolver:
             rhs = np.ascontiguousarray(in_rhs, np.float32)
             rc = L.uaamg_poisson_solve_pcg_mixed(h, prec, in_out_pressure.ctypes.data, rhs.ctypes.data, C.byref(it))
         else:
-            rc = L.uaamg_poisson_solve_pcg_mixed_device(h, prec, in_out_pressure.data_ptr(), in_rhs.data_ptr(),
-                                                        C.byref(it))
+            with _lib.torch_ordered("poisson", h, in_out_pressure, in_rhs):
+                rc = L.uaamg_poisson_solve_pcg_mixed_device(h, prec, in_out_pressure.data_ptr(), in_rhs.data_ptr(),
+                                                            C.byref(it))
         _lib.check(rc, "solve_pcg_mixed")
         self.mIterationTaken = int(it.value)
         return int(rc)
@@ -321,8 +333,10 @@ class PoissonSolver:
     def true_residual_fp64(self, d_x, d_b) -> tuple[float, float]:
         """(|b - A x|_inf, |b|_inf) in FP64 from the FP32 level-0 matrix (device tensors)."""
         out = (C.c_double * 2)()
-        _lib.check(_lib.lib().uaamg_poisson_true_residual_fp64(self.mMultigridHierarchy._h, d_x.data_ptr(),
-                                                                d_b.data_ptr(), out), "true_residual_fp64")
+        h = self.mMultigridHierarchy._h
+        with _lib.torch_ordered("poisson", h, d_x, d_b):
+            _lib.check(_lib.lib().uaamg_poisson_true_residual_fp64(h, d_x.data_ptr(), d_b.data_ptr(), out),
+                       "true_residual_fp64")
         return float(out[0]), float(out[1])
 
     def solve_fp64_reference(self, d_rhs, d_x, rel_tol: float = 1e-12, max_iter: int = 200):
@@ -333,8 +347,9 @@ class PoissonSolver:
         L, h = self._configure()
         it = C.c_int(0)
         rr = C.c_double(0.0)
-        rc = L.uaamg_poisson_solve_fp64_reference(h, d_rhs.data_ptr(), d_x.data_ptr(), float(rel_tol),
-                                                  int(max_iter), C.byref(it), C.byref(rr))
+        with _lib.torch_ordered("poisson", h, d_rhs, d_x):
+            rc = L.uaamg_poisson_solve_fp64_reference(h, d_rhs.data_ptr(), d_x.data_ptr(), float(rel_tol),
+                                                      int(max_iter), C.byref(it), C.byref(rr))
         _lib.check(rc, "solve_fp64_reference")
         return int(rc), int(it.value), float(rr.value)
 
@@ -353,8 +368,9 @@ class PoissonSolver:
         ms = np.zeros(max_classes, np.float64)
         cnt = np.zeros(max_classes, np.int64)
         nc = C.c_int(0)
-        rc = L.uaamg_poisson_profile_pcg(h, d_pressure.data_ptr(), d_rhs.data_ptr(), max_classes,
-                                         C.addressof(names), ms.ctypes.data, cnt.ctypes.data, C.byref(nc))
+        with _lib.torch_ordered("poisson", h, d_pressure, d_rhs):
+            rc = L.uaamg_poisson_profile_pcg(h, d_pressure.data_ptr(), d_rhs.data_ptr(), max_classes,
+                                             C.addressof(names), ms.ctypes.data, cnt.ctypes.data, C.byref(nc))
         _lib.check(rc, "profile_pcg")
         return self._prof_table(names, ms, cnt, nc.value)
 
@@ -365,9 +381,10 @@ class PoissonSolver:
         ms = np.zeros(max_classes, np.float64)
         cnt = np.zeros(max_classes, np.int64)
         nc = C.c_int(0)
-        rc = L.uaamg_poisson_profile_pcg_mixed(h, self.PRECISIONS[precision], d_pressure.data_ptr(),
-                                               d_rhs.data_ptr(), max_classes, C.addressof(names), ms.ctypes.data,
-                                               cnt.ctypes.data, C.byref(nc))
+        with _lib.torch_ordered("poisson", h, d_pressure, d_rhs):
+            rc = L.uaamg_poisson_profile_pcg_mixed(h, self.PRECISIONS[precision], d_pressure.data_ptr(),
+                                                   d_rhs.data_ptr(), max_classes, C.addressof(names),
+                                                   ms.ctypes.data, cnt.ctypes.data, C.byref(nc))
         _lib.check(rc, "profile_pcg_mixed")
         return self._prof_table(names, ms, cnt, nc.value)
 

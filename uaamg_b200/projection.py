@@ -44,6 +44,7 @@ def calculate_face_weights(solid_sdf: LeafGrid, origins: np.ndarray, masks: np.n
     out = np.empty((n, 512, 3), np.float32)
     m = None if masks is None else np.ascontiguousarray(masks, dtype=np.uint64).reshape(n, 8)
     g = _as_c(solid_sdf, keep)
+    _lib.torch_inputs_ready(None, solid_sdf)
     rc = _lib.lib().uaamg_face_weights(C.byref(g), n, org.ctypes.data if n else None,
                                        None if m is None or n == 0 else m.ctypes.data,
                                        out.ctypes.data if n else None)
@@ -66,6 +67,7 @@ def immerse_liquid_phi_values(liquid_phi: LeafGrid, solid_sdf: LeafGrid, dx: flo
     n = liquid_phi.leaf_count
     out = np.empty((n, 512), np.float32)
     gs, gl = _as_c(solid_sdf, keep), _as_c(liquid_phi, keep)
+    _lib.torch_inputs_ready(None, solid_sdf, liquid_phi)
     rc = _lib.lib().uaamg_immerse_liquid_phi(C.byref(gs), C.byref(gl), float(dx), out.ctypes.data if n else None)
     _lib.check(rc, "immerse_liquid_phi")
     return out
@@ -108,6 +110,7 @@ def apply_pressure_gradient(lap: LaplacianWithLevel, liquid_phi: LeafGrid, face_
     refl = np.empty((n, 512), np.float32)
     p = np.ascontiguousarray(pressure, dtype=np.float32)
     gphi, gfw, gsv, gv = (_as_c(x, keep) for x in (liquid_phi, face_weights, solid_velocity, velocity))
+    _lib.torch_inputs_ready(None, liquid_phi, face_weights, solid_velocity, velocity)
     rc = _lib.lib().uaamg_poisson_apply_pressure_gradient(
         lap._h, C.byref(gphi), C.byref(gfw), C.byref(gsv), p.ctypes.data, float(dt), float(friction), int(channel),
         C.byref(gv), vel.ctypes.data, mask.ctypes.data, upd.ctypes.data, refl.ctypes.data)

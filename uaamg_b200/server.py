@@ -5,7 +5,7 @@ with their operator inputs, each substep's face velocities are pushed as the
 simulation produces them, and results are waited for per substep.  See the
 header for the admission, batching and lane rules.  Grids may live on the host
 (numpy) or on the device (torch CUDA tensors); the server copies them at the
-call.
+call, after synchronising torch's current stream when a grid is on the device.
 """
 from __future__ import annotations
 
@@ -65,6 +65,7 @@ class NativeServer:
                        dx: float, substeps: int) -> int:
         keep: list = []
         gs = [_as_c(g, keep) for g in (liquid_phi, face_weights, solid_velocity)]
+        _lib.torch_inputs_ready(None, liquid_phi, face_weights, solid_velocity)
         rid = C.c_int64(0)
         _lib.check(_lib.lib().uaamg_server_submit_poisson(self._h, *[C.byref(g) for g in gs], float(dt), float(dx),
                                                           int(substeps), C.byref(rid)), "uaamg_server_submit_poisson")
@@ -74,6 +75,7 @@ class NativeServer:
                          solid_velocity: LeafGrid, dt: float, rho: float, dx: float, substeps: int) -> int:
         keep: list = []
         gs = [_as_c(g, keep) for g in (viscosity, liquid_sdf, solid_sdf, solid_velocity)]
+        _lib.torch_inputs_ready(None, viscosity, liquid_sdf, solid_sdf, solid_velocity)
         rid = C.c_int64(0)
         _lib.check(_lib.lib().uaamg_server_submit_viscosity(self._h, *[C.byref(g) for g in gs], float(dt), float(rho),
                                                             float(dx), int(substeps), C.byref(rid)),
@@ -83,6 +85,7 @@ class NativeServer:
     def push_velocity(self, request: int, u: LeafGrid, v: LeafGrid, w: LeafGrid) -> None:
         keep: list = []
         gs = [_as_c(g, keep) for g in (u, v, w)]
+        _lib.torch_inputs_ready(None, u, v, w)
         _lib.check(_lib.lib().uaamg_server_push_velocity(self._h, int(request), *[C.byref(g) for g in gs]),
                    "uaamg_server_push_velocity")
 

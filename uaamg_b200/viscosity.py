@@ -44,10 +44,13 @@ class L_with_level:
         """``stream``: a cudaStream_t (int) to build on; the handle keeps it."""
         L = _lib.lib()
         keep: list = []
-        gs = [_as_c(g, keep) for g in (viscosity, liquid_sdf, solid_sdf)]
+        grids = (viscosity, liquid_sdf, solid_sdf)
+        gs = [_as_c(g, keep) for g in grids]
         h = C.c_void_p()
+        _lib.torch_inputs_ready(stream, grids)
         _lib.check(L.uaamg_viscosity_create_on_stream(*[C.byref(g) for g in gs], float(dt), float(rho), float(dx),
                                                       stream, C.byref(h)), "uaamg_viscosity_create")
+        _lib.torch_after("viscosity", h.value, grids)
         return L_with_level(h.value, dt, rho, dx)
 
     def __del__(self):
@@ -95,9 +98,11 @@ class L_with_level:
         sv = C.byref(_as_c(solid_velocity, keep)) if solid_velocity is not None else None
         L = _lib.lib()
         if out is not None and not isinstance(out, np.ndarray):
-            _lib.check(L.uaamg_viscosity_build_rhs_device(self._h, *[C.byref(g) for g in gs], sv, out.data_ptr()),
-                       "build_rhs_device")
+            with _lib.torch_ordered("viscosity", self._h, out, u, v, w, solid_velocity):
+                _lib.check(L.uaamg_viscosity_build_rhs_device(self._h, *[C.byref(g) for g in gs], sv,
+                                                              out.data_ptr()), "build_rhs_device")
             return out
+        _lib.torch_inputs_ready(None, u, v, w, solid_velocity)
         rhs = self.get_zero_vec() if out is None else out
         _lib.check(L.uaamg_viscosity_build_rhs(self._h, *[C.byref(g) for g in gs], sv, rhs.ctypes.data), "build_rhs")
         return rhs
@@ -109,9 +114,11 @@ class L_with_level:
         gs = [_as_c(g, keep) for g in (u, v, w)]
         L = _lib.lib()
         if out is not None and not isinstance(out, np.ndarray):
-            _lib.check(L.uaamg_viscosity_gather_velocity_device(self._h, *[C.byref(g) for g in gs], out.data_ptr()),
-                       "gather_velocity_device")
+            with _lib.torch_ordered("viscosity", self._h, out, u, v, w):
+                _lib.check(L.uaamg_viscosity_gather_velocity_device(self._h, *[C.byref(g) for g in gs],
+                                                                    out.data_ptr()), "gather_velocity_device")
             return out
+        _lib.torch_inputs_ready(None, u, v, w)
         x = self.get_zero_vec() if out is None else out
         _lib.check(L.uaamg_viscosity_gather_velocity(self._h, *[C.byref(g) for g in gs], x.ctypes.data),
                    "gather_velocity")
@@ -222,8 +229,9 @@ class simd_viscosity3d:
             rhs = _f32(rhs)
             rc = L.uaamg_viscosity_solve_pcg(h, in_lhs.ctypes.data, rhs.ctypes.data, float(tolerance), C.byref(it))
         else:
-            rc = L.uaamg_viscosity_solve_pcg_device(h, in_lhs.data_ptr(), rhs.data_ptr(), float(tolerance),
-                                                    C.byref(it))
+            with _lib.torch_ordered("viscosity", h, in_lhs, rhs):
+                rc = L.uaamg_viscosity_solve_pcg_device(h, in_lhs.data_ptr(), rhs.data_ptr(), float(tolerance),
+                                                        C.byref(it))
         _lib.check(rc, "pcg_solve")
         self.m_iteration = int(it.value)
         return int(rc)
@@ -242,6 +250,7 @@ class simd_viscosity3d:
         x = self.level0.get_zero_vec() if out is None else out
         assert x.dtype == np.float32 and x.flags["C_CONTIGUOUS"]
         it = C.c_int(0)
+        _lib.torch_inputs_ready(None, u, v, w, solid_velocity)
         rc = L.uaamg_viscosity_solve_velocity(h, *[C.byref(g) for g in gs], sv, float(tolerance), x.ctypes.data,
                                               C.byref(it))
         _lib.check(rc, "solve_velocity")
@@ -261,8 +270,9 @@ class simd_viscosity3d:
         ms = np.zeros(max_classes, np.float64)
         cnt = np.zeros(max_classes, np.int64)
         nc = C.c_int(0)
-        rc = L.uaamg_viscosity_profile_pcg(h, d_lhs.data_ptr(), d_rhs.data_ptr(), float(tolerance), max_classes,
-                                           C.addressof(names), ms.ctypes.data, cnt.ctypes.data, C.byref(nc))
+        with _lib.torch_ordered("viscosity", h, d_lhs, d_rhs):
+            rc = L.uaamg_viscosity_profile_pcg(h, d_lhs.data_ptr(), d_rhs.data_ptr(), float(tolerance), max_classes,
+                                               C.addressof(names), ms.ctypes.data, cnt.ctypes.data, C.byref(nc))
         _lib.check(rc, "profile_pcg")
         self.m_iteration = int(L.uaamg_viscosity_iterations(h))
         raw = names.raw
