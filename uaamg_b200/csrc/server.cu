@@ -122,6 +122,7 @@ struct SrvReq {
     int64_t id = 0;
     int kind = 0;  // UAAMG_SERVER_POISSON / UAAMG_SERVER_VISCOSITY
     int substeps = 0;
+    int pushed = 0;  // velocities pushed (a substep in flight is in neither pending nor results)
     int64_t cost = 0;
     SrvGrid a, b, c, sv;  // pressure: liquid SDF, face weights; viscosity: viscosity, liquid SDF, solid SDF
     float dt = 0, dx = 0, rho = 0;
@@ -641,12 +642,13 @@ int uaamg_server_push_velocity(uaamg_server* s, int64_t request, const uaamg_lea
     auto it = s->reqs.find(request);
     if (it == s->reqs.end()) { set_error("unknown request %lld", (long long)request); return UAAMG_ERR_INVALID_ARGUMENT; }
     SrvReq& r = *it->second;
-    if ((int)(r.results.size() + r.pending.size()) >= r.substeps) {
+    if (r.pushed >= r.substeps) {
         set_error("request %lld already has all its %d substeps", (long long)request, r.substeps);
         return UAAMG_ERR_INVALID_ARGUMENT;
     }
     if (r.state == RQ_FAILED) { set_error("request %lld failed: %s", (long long)request, r.error.c_str()); return UAAMG_ERR_CUDA; }
     r.pending.push_back(std::move(sub));
+    ++r.pushed;
     s->cv.notify_all();
     return UAAMG_SUCCESS;
     ABI_END
