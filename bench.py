@@ -248,6 +248,48 @@ def _grid_bytes(*gs) -> int:
     return int(sum(_gbytes(g) + (g.masks.nbytes if g.masks is not None else 0) for g in gs))
 
 
+def _map_bytes(g) -> int:
+    """The dense leaf map the library uploads for a grid (one int32 per leaf
+    cell of the origins' bounding box)."""
+    if g.leaf_count == 0:
+        return 0
+    c = np.asarray(g.origins).reshape(-1, 3) >> 3
+    return int(np.prod(c.max(0) - c.min(0) + 1)) * 4
+
+
+def _pressure_h2d_bytes(phi, fw, vels) -> int:
+    """Bytes uaamg_poisson_create_with_rhs moves host->device for pinned
+    inputs: the liquid SDF whole (values, origins, active masks, leaf map); of
+    each face grid only the leaves the construction reads (at a liquid leaf
+    or the next leaf above one along x, y or z), with its origins and leaf map
+    (the velocity channels share the face weights' map and read flags when
+    their leaves are the same)."""
+    po = np.asarray(phi.origins).reshape(-1, 3)
+    vals = np.asarray(phi.values).reshape(phi.leaf_count, 512)
+    liq = vals < 0
+    if phi.masks is not None:
+        bits = np.unpackbits(np.asarray(phi.masks, np.uint64).reshape(-1, 8).view(np.uint8), axis=1,
+                             bitorder="little").astype(bool)
+        liq &= bits
+    liquid = {tuple(o) for o in po[liq.any(1)]}
+    total = _gbytes(phi) + po.nbytes + (phi.masks.nbytes if phi.masks is not None else 0) + _map_bytes(phi)
+    shared = None
+    for i, g in enumerate([fw] + list(vels)):
+        if g.leaf_count == 0:
+            continue
+        org = np.asarray(g.origins).reshape(-1, 3)
+        if i > 0 and shared is not None and np.array_equal(org, shared):
+            pass  # map and read flags of the face weights
+        else:
+            total += _map_bytes(g) + org.nbytes
+            if i == 0:
+                shared = org
+        read = np.array([any(tuple(o - d) in liquid for d in ((0, 0, 0), (8, 0, 0), (0, 8, 0), (0, 0, 8)))
+                         for o in org])
+        total += int(read.sum()) * 512 * 4 * g.components
+    return int(total)
+
+
 # algorithmic bytes of one pass per DOF it updates (canonical model: every array
 # read or written once at 4 B, halos excluded): GS colour pass of one channel =
 # half of the 44 B two-colour channel sweep; residual 44 B and A.x 40 B per
@@ -1199,10 +1241,11 @@ def main():
                               "resident grids), then UAAMG-PCG from a zero pressure "
                               "(uaamg_poisson_solve_pcg_resident_device)"},
             "e2e": {"value": round(e2e, 4), "unit": UNIT,
-                    # uaamg_poisson_create_with_rhs: the liquid SDF, the face weights and the three velocity
-                    # channels (values, origins, masks) once each; the solid velocity grid is empty here
-                    "h2d_bytes_per_step": int(_grid_bytes(psc.phi, psc.face_weights, psc.vx, psc.vy, psc.vz,
-                                                          psc.solid_velocity)),
+                    # uaamg_poisson_create_with_rhs from pinned grids: the liquid SDF whole, the face weights
+                    # and the three velocity channels at the leaves the construction reads; the solid velocity
+                    # grid is empty here
+                    "h2d_bytes_per_step": _pressure_h2d_bytes(psc.phi, psc.face_weights,
+                                                              (psc.vx, psc.vy, psc.vz, psc.solid_velocity)),
                     # the pressure
                     "d2h_bytes_per_step": int(pvec)},
             "gpu_launches": int(launches),

@@ -91,7 +91,13 @@ int uaamg_poisson_create_on_stream(const uaamg_leaf_grid* liquid_phi, const uaam
  * uaamg_poisson_solve_*_resident.  Each host input crosses the bus once (the
  * face weights feed both the matrix and the rhs), and the velocity uploads run
  * on a second stream while the hierarchy is built.  Pinned host inputs make
- * the uploads asynchronous; device inputs (values_on_device) are read in place. */
+ * the uploads asynchronous, and a face grid (face weights, velocities, solid
+ * velocity) in pinned memory is read by a kernel through its device mapping,
+ * only at the leaves the construction reads (those holding liquid and the
+ * next leaf above them along x, y or z); pinned inputs stay unchanged until
+ * the handle's stream has passed the construction (a solve has returned).
+ * Device inputs (values_on_device) are read in place.  uaamg_poisson_create
+ * reads its face weights the same way. */
 int uaamg_poisson_create_with_rhs(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid* face_weights,
                                   const uaamg_leaf_grid* vx, const uaamg_leaf_grid* vy, const uaamg_leaf_grid* vz,
                                   const uaamg_leaf_grid* solid_velocity, float dt, float dx, void* stream,

@@ -359,8 +359,10 @@ def test_create_with_rhs_one_call_identical(scene64, gpu):
     """uaamg_poisson_create_with_rhs (matrix, hierarchy and rhs in one call,
     each input uploaded once) + the resident solve give the same hierarchy,
     rhs, pressure, iterations and status, bit for bit, as
-    create + createPressurePoissonRightHandSide + solveMultigridPCG; host and
-    device inputs alike; pure multigrid from the resident rhs too."""
+    create + createPressurePoissonRightHandSide + solveMultigridPCG; pageable
+    host, pinned host (face grids gathered by a kernel at the leaves the
+    construction reads, the others NaN on the device) and device inputs alike;
+    pure multigrid from the resident rhs too."""
     torch = gpu
     from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver
     sc, lap, ref = scene64
@@ -374,15 +376,30 @@ def test_create_with_rhs_one_call_identical(scene64, gpu):
         d.values = torch.from_numpy(g.values).cuda()
         return d
 
-    for dev in (False, True):
+    keep = []
+
+    def pinned(g):
+        t = torch.from_numpy(np.ascontiguousarray(g.values)).pin_memory()
+        keep.append(t)
+        return LeafGrid(origins=g.origins, values=t.numpy(), background=g.background, masks=g.masks)
+
+    for mode in ("host", "device", "pinned"):
         grids = [getattr(sc, k) for k in ("phi", "face_weights", "vx", "vy", "vz", "solid_velocity")]
-        if dev:
+        if mode == "device":
             grids = [on_device(g) for g in grids]
+        if mode == "pinned":
+            grids = [pinned(g) for g in grids]
         lap1 = LaplacianWithLevel.createPressurePoissonLaplacianWithRhs(*grids, sc.dt, sc.dx)
         assert lap1.num_levels() == lap.num_levels()
         for l in range(lap.num_levels()):
             assert np.array_equal(lap1.dof_index(l), lap.dof_index(l))
-        assert np.array_equal(lap1.copy_rhs(), rhs)
+            (a1, f1), (a0, f0) = lap1.coefficients(l), lap.coefficients(l)
+            assert all(np.array_equal(x, y) for x, y in zip(a1, a0)) and np.array_equal(f1, f0), (mode, l)
+        assert np.array_equal(lap1.copy_rhs(), rhs), mode
+        if mode == "pinned":  # the one-step create (no rhs) gathers its face weights the same way
+            lap4 = LaplacianWithLevel.createPressurePoissonLaplacian(grids[0], grids[1], sc.dt, sc.dx)
+            for l in range(lap.num_levels()):
+                assert all(np.array_equal(x, y) for x, y in zip(lap4.coefficients(l)[0], lap.coefficients(l)[0]))
         s1 = PoissonSolver(lap1)
         p1 = np.full_like(p0, 3.0)  # the resident solve starts from zero whatever the buffer holds
         st1 = s1.solveMultigridPCGResident(p1)

@@ -292,7 +292,28 @@ struct PinStage {
 struct DevGrid {  // device copy of an input grid + its leaf map
     DGrid g{};
     void* mem = nullptr;
+    const uint8_t* read = nullptr;  // per leaf: read by the construction (set when only those were copied)
 };
+
+// What a face grid in pinned host memory needs to copy only the leaves the
+// construction reads (k_face_leaves_read): the liquid SDF on the device and its
+// per-leaf liquid flags.
+struct FaceGather {
+    const DGrid* phi;
+    const uint8_t* liquid;
+    int64_t* launches;
+};
+// The device address of pinned (page-locked, mapped) host memory, or null for
+// pageable memory or an address a float4 load cannot start at.
+static const void* host_mapped(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer || ((uintptr_t)a.devicePointer & 15)) return nullptr;
+    return a.devicePointer;
+}
 
 }  // namespace
 
@@ -381,10 +402,13 @@ static size_t carve_size(size_t count, size_t elem) { return (count * elem + 255
 // Device copy of an input grid and its leaf map.  When `share` (a grid whose
 // device map `share_dg` is already built) lists the same leaves in the same
 // order, as the face-velocity channels and the face weights of a staggered
-// grid usually do, its map is reused and only the values go up.
+// grid usually do, its map is reused and only the values go up.  With `fg`, a
+// face grid whose values are in pinned host memory is gathered by a kernel
+// that reads only the leaves the construction reads (the others are NaN).
 static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf_grid* gr, DevGrid& dg, HostMap& map,
                            std::vector<void*>& tofree, const uaamg_leaf_grid* share = nullptr,
-                           const DevGrid* share_dg = nullptr, PinStage* stage = nullptr) {
+                           const DevGrid* share_dg = nullptr, PinStage* stage = nullptr,
+                           const FaceGather* fg = nullptr) {
     const bool same = share && share_dg && share_dg->g.map && share->leaf_count == gr->leaf_count &&
                       gr->leaf_count > 0 &&
                       (share->origins == gr->origins ||
@@ -397,8 +421,12 @@ static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf
     dg.g.bg2 = gr->components > 2 ? gr->background[2] : 0.f;
     if (gr->leaf_count == 0) return;
     size_t mapn = same ? 0 : map.idx.size();
-    size_t vbytes = (size_t)gr->leaf_count * UAAMG_LEAF * gr->components * sizeof(float);
-    size_t total = carve_size(mapn, 4) + (gr->values_on_device ? 0 : carve_size(vbytes, 1));
+    const size_t n = (size_t)gr->leaf_count;
+    size_t vbytes = n * UAAMG_LEAF * gr->components * sizeof(float);
+    const void* mapped = (fg && !gr->values_on_device) ? host_mapped(gr->values) : nullptr;
+    const bool own_read = mapped && !(same && share_dg->read);  // this grid's read flags are computed here
+    size_t total = carve_size(mapn, 4) + (gr->values_on_device ? 0 : carve_size(vbytes, 1)) +
+                   (own_read ? carve_size(n * 3, 4) + carve_size(n, 1) : 0);
     void* mem = nullptr;
     CK(ctx_dev_alloc(ctx, &mem, total, stream));
     tofree.push_back(mem);
@@ -416,7 +444,27 @@ static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf
     const float* vals = gr->values;
     if (!gr->values_on_device) {
         float* dv = carve<float>(cur, vbytes / 4);
-        CK(cudaMemcpyAsync(dv, gr->values, vbytes, cudaMemcpyHostToDevice, stream));
+        if (mapped) {
+            const uint8_t* read = same ? share_dg->read : nullptr;
+            if (own_read) {
+                int* dorg = carve<int>(cur, n * 3);
+                uint8_t* rd = carve<uint8_t>(cur, n);
+                const void* osrc = stage ? stage->put(gr->origins, n * 12) : gr->origins;
+                CK(cudaMemcpyAsync(dorg, osrc, n * 12, cudaMemcpyHostToDevice, stream));
+                k_face_leaves_read<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(dorg, (int)n, *fg->phi, fg->liquid,
+                                                                                    rd);
+                CHECK_LAUNCH();
+                ++*fg->launches;
+                read = rd;
+            }
+            k_gather_host_leaves<<<(unsigned)n, 128, 0, stream>>>(static_cast<const float4*>(mapped), gr->components,
+                                                                  read, reinterpret_cast<float4*>(dv));
+            CHECK_LAUNCH();
+            ++*fg->launches;
+            dg.read = read;
+        } else {
+            CK(cudaMemcpyAsync(dv, gr->values, vbytes, cudaMemcpyHostToDevice, stream));
+        }
         vals = dv;
     }
     dg.g.val = vals;
@@ -535,7 +583,41 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         CK(ctx_pinned_acquire(h->ctx, (size_t)4 << 20, &h->pin_in, &h->pin_in_cap));
         PinStage stage{(char*)h->pin_in, h->pin_in_cap, 0};
         upload_grid(h, phi, dphi, phimap, tofree, &stage);
-        upload_grid(h, fw, dfw, fwmap, tofree, &stage);
+        // the liquid SDF's origins and active masks, its DOF masks, its per-leaf liquid flags
+        size_t extra = carve_size((size_t)nphi * 8, 8) * 2 + carve_size((size_t)nphi * 3, 4) + carve_size((size_t)nphi, 1);
+        void* mem = nullptr;
+        CK(ctx_dev_alloc(h->ctx, &mem, extra, s));
+        tofree.push_back(mem);
+        char* cur = (char*)mem;
+        uint64_t* dphimask = carve<uint64_t>(cur, (size_t)nphi * 8);
+        uint64_t* ddofmask = carve<uint64_t>(cur, (size_t)nphi * 8);
+        int* dphiorg = carve<int>(cur, (size_t)nphi * 3);
+        uint8_t* dliquid = carve<uint8_t>(cur, (size_t)nphi);
+        CK(cudaMemcpyAsync(dphiorg, stage.put(phi->origins, (size_t)nphi * 12), (size_t)nphi * 12,
+                           cudaMemcpyHostToDevice, s));
+        const uint64_t* pm = nullptr;
+        if (phi->masks) {
+            CK(cudaMemcpyAsync(dphimask, stage.put(phi->masks, (size_t)nphi * 64), (size_t)nphi * 64,
+                               cudaMemcpyHostToDevice, s));
+            pm = dphimask;
+        }
+        // Face grids in pinned host memory cross the bus only where the construction reads them (the leaves
+        // at and above liquid leaves): the liquid flags come first.
+        FaceGather fgather{&dphi.g, dliquid, &h->launches};
+        const FaceGather* fgp = nullptr;
+        {
+            bool host_faces = !fw->values_on_device;
+            if (ri)
+                for (const uaamg_leaf_grid* g : {ri->vx, ri->vy, ri->vz, ri->sv})
+                    host_faces = host_faces || (!g->values_on_device && g->leaf_count > 0);
+            if (host_faces) {
+                k_liquid_leaves<<<(unsigned)nphi, 128, 0, s>>>(dphi.g, pm, dliquid);
+                CHECK_LAUNCH();
+                h->launches++;
+                fgp = &fgather;
+            }
+        }
+        upload_grid_cs(h->ctx, s, fw, dfw, fwmap, tofree, nullptr, nullptr, &stage, fgp);
         // The velocities of the right-hand side go up on a second stream once
         // the SDF and the face weights are up, so their copies overlap the DOF
         // mask kernel, the host topology and the coefficient kernels.
@@ -551,26 +633,11 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             const uaamg_leaf_grid* vg[4] = {ri->vx, ri->vy, ri->vz, ri->sv};
             // the channels' maps come from the face weights' when the leaves match (the face-weight map
             // was uploaded on the first stream, which the second stream waits for)
-            for (int k = 0; k < 4; ++k) upload_grid_cs(h->ctx, s2, vg[k], dvel[k], vmap[k], tofree, fw, &dfw, &stage);
+            for (int k = 0; k < 4; ++k)
+                upload_grid_cs(h->ctx, s2, vg[k], dvel[k], vmap[k], tofree, fw, &dfw, &stage, fgp);
             CK(cudaEventRecord(ev_vel.e, s2));
         }
         TRACE("upload inputs");
-        size_t extra = carve_size((size_t)nphi * 8, 8) * 2 + carve_size((size_t)nphi * 3, 4);
-        void* mem = nullptr;
-        CK(ctx_dev_alloc(h->ctx, &mem, extra, s));
-        tofree.push_back(mem);
-        char* cur = (char*)mem;
-        uint64_t* dphimask = carve<uint64_t>(cur, (size_t)nphi * 8);
-        uint64_t* ddofmask = carve<uint64_t>(cur, (size_t)nphi * 8);
-        int* dphiorg = carve<int>(cur, (size_t)nphi * 3);
-        CK(cudaMemcpyAsync(dphiorg, stage.put(phi->origins, (size_t)nphi * 12), (size_t)nphi * 12,
-                           cudaMemcpyHostToDevice, s));
-        const uint64_t* pm = nullptr;
-        if (phi->masks) {
-            CK(cudaMemcpyAsync(dphimask, stage.put(phi->masks, (size_t)nphi * 64), (size_t)nphi * 64,
-                               cudaMemcpyHostToDevice, s));
-            pm = dphimask;
-        }
         const float dtOverDxSqr = dt / (dx * dx);
         k_finest_mask<<<(unsigned)nphi, 128, 0, s>>>(dphi.g, pm, dphiorg, dfw.g, dtOverDxSqr, ddofmask);
         CHECK_LAUNCH();

@@ -82,6 +82,61 @@ __device__ __forceinline__ float finest_voxel(const DGrid& phi, const DGrid& fw,
     return dg;
 }
 
+// ---------------------------------------------------------------------------
+// Inputs in pinned host memory: only the leaves the construction reads cross
+// the bus.  The DOF mask, the coefficients and the rhs read a face grid (face
+// weights, face velocities, solid velocity) at the six faces of liquid voxels
+// (active, phi < 0): in the voxel's own leaf and, for its + faces on a leaf
+// boundary, in the next leaf along x, y or z.  So a face-grid leaf is read
+// exactly when the liquid-SDF leaf at its origin or one leaf below it along x,
+// y or z holds a liquid voxel.
+
+// per liquid-SDF leaf: does it hold a liquid voxel?
+__global__ void __launch_bounds__(128) k_liquid_leaves(DGrid phi, const uint64_t* phi_mask, uint8_t* out) {
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int off = 4 * t + j;
+        if (phi_mask && !((phi_mask[(long long)leaf * 8 + (off >> 6)] >> (off & 63)) & 1ull)) continue;
+        if (phi.val[(long long)leaf * UAAMG_LEAF + off] < 0.f) any = true;
+    }
+    any = __syncthreads_or(any) != 0;
+    if (t == 0) out[leaf] = any ? 1 : 0;
+}
+// per leaf of a face grid (origins org[n][3]): does the construction read it?
+__global__ void k_face_leaves_read(const int* org, int n, DGrid phi, const uint8_t* liquid, uint8_t* need) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int ox = org[3 * i], oy = org[3 * i + 1], oz = org[3 * i + 2];
+    const int l0 = phi.leaf_of(ox, oy, oz), lx = phi.leaf_of(ox - 8, oy, oz), ly = phi.leaf_of(ox, oy - 8, oz),
+              lz = phi.leaf_of(ox, oy, oz - 8);
+    need[i] = ((l0 >= 0 && liquid[l0]) || (lx >= 0 && liquid[lx]) || (ly >= 0 && liquid[ly]) ||
+               (lz >= 0 && liquid[lz]))
+                  ? 1
+                  : 0;
+}
+// A face grid's values [n][512][comps] from pinned host memory (read by the
+// kernel through its device mapping): the leaves the construction reads are
+// copied, the others hold NaN, which no result may depend on.
+__global__ void __launch_bounds__(128) k_gather_host_leaves(const float4* __restrict__ src, int comps,
+                                                            const uint8_t* need, float4* __restrict__ dst) {
+    const int leaf = blockIdx.x, t = threadIdx.x;
+    const long long base = (long long)leaf * comps * (UAAMG_LEAF / 4);
+    if (need[leaf]) {
+        float4 v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            if (c < comps) v[c] = src[base + c * 128 + t];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            if (c < comps) dst[base + c * 128 + t] = v[c];
+    } else {
+        const float q = __int_as_float(0x7fffffff);
+        for (int c = 0; c < comps; ++c) dst[base + c * 128 + t] = make_float4(q, q, q, q);
+    }
+}
+
 // pass 0: DOF masks of every input leaf (liquid, active, diag != 0)
 __global__ void __launch_bounds__(128) k_finest_mask(DGrid phi, const uint64_t* phi_mask, const int* phi_org, DGrid fw,
                                                      float dtOverDxSqr, uint64_t* out_mask) {
