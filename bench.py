@@ -1101,13 +1101,16 @@ def main():
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    def timed(fn, steps):
+    step_log: dict[str, list[float]] = {}
+
+    def timed(fn, steps, name=None):
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         total = 0.0
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        each = []
         for _ in range(steps):
             flush.fill_(1.0)  # evict L2 between timed steps (256 MiB > 126 MB L2)
             torch.cuda.synchronize()
@@ -1115,7 +1118,10 @@ def main():
             fn()
             e1.record(stream)
             torch.cuda.synchronize()
-            total += e0.elapsed_time(e1)
+            each.append(e0.elapsed_time(e1))
+            total += each[-1]
+        if name:
+            step_log[name] = each
         if dist is not None:
             dist.barrier()
         return total
@@ -1167,13 +1173,13 @@ def main():
     pstats.update(launches=0, iters=[], status=[])
     clk = ClockSampler(local)
     clk.start()
-    tp_dev = timed(pstep_device, args.steps)
+    tp_dev = timed(pstep_device, args.steps, "device")
     clocks = clk.stop()
     launches = pstats["launches"]
     piters, pstatus = list(pstats["iters"]), list(pstats["status"])
     for _ in range(args.warmup):
         pstep_host()
-    tp_host = timed(pstep_host, args.steps)
+    tp_host = timed(pstep_host, args.steps, "e2e")
     tp_dev, tp_host = max_over_ranks(tp_dev, tp_host)
     total = args.steps * ws
     value, e2e = tp_dev / total, tp_host / total
@@ -1239,7 +1245,10 @@ def main():
                       "voxel_updates_per_s": round(pndof[0] * piters[0] * 1e3 / value, 1),
                       "step": "create level-0 matrix + hierarchy + rhs (uaamg_poisson_create_with_rhs, device-"
                               "resident grids), then UAAMG-PCG from a zero pressure "
-                              "(uaamg_poisson_solve_pcg_resident_device)"},
+                              "(uaamg_poisson_solve_pcg_resident_device)",
+                      # per-step spread (the step has host phases: topology, the first solve's host-driven loop)
+                      "step_ms": {k: {"min": round(min(v), 4), "median": round(float(np.median(v)), 4),
+                                      "max": round(max(v), 4)} for k, v in step_log.items()}},
             "e2e": {"value": round(e2e, 4), "unit": UNIT,
                     # uaamg_poisson_create_with_rhs from pinned grids: the liquid SDF whole, the face weights
                     # and the three velocity channels at the leaves the construction reads; the solid velocity

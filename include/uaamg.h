@@ -427,7 +427,9 @@ int uaamg_batch_results(const uaamg_batch* b, int* iterations, int* status, floa
  * ordering rules of uaamg_poisson_set_stream apply). */
 int uaamg_batch_set_stream(uaamg_batch* b, void* stream);
 int uaamg_batch_get_stream(const uaamg_batch* b, void** stream);
-/* 1 (default): the CUDA graph with a WHILE node; 0: host-driven loop. */
+/* 1 (default): host-driven loop for the batch's first solve, the CUDA graph
+ * with a WHILE node from the second solve on; 2: the graph always; 0: the
+ * host-driven loop always. */
 int uaamg_batch_set_graph_mode(uaamg_batch* b, int use_graph);
 /* Kernels launched by the last batched solve. */
 int64_t uaamg_batch_kernel_launches(const uaamg_batch* b);

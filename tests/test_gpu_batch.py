@@ -107,7 +107,7 @@ def test_batch_bit_identical_to_standalone(batch_scenes, smoother):
 
 
 def test_batch_device_and_host_paths_and_graph_modes_agree(batch_scenes):
-    _, p_host, b1, _ = _batched(batch_scenes, 0)
+    _, p_host, b1, _ = _batched(batch_scenes, 0, use_graph=2)  # the graph from the first solve
     _, p_dev, b2, _ = _batched(batch_scenes, 0, device=True)
     _, p_eager, b3, _ = _batched(batch_scenes, 0, use_graph=False)
     for a, c, e in zip(p_host, p_dev, p_eager):

@@ -59,7 +59,9 @@ class PoissonBatch:
         _lib.check(L.uaamg_batch_set_max_iterations(self._h, int(self.mMaxIteration)), "batch set_max_iterations")
         _lib.check(L.uaamg_batch_set_relative_tolerance(self._h, float(self.mRelativeTolerance)),
                    "batch set_tolerance")
-        _lib.check(L.uaamg_batch_set_graph_mode(self._h, 1 if self.use_graph else 0), "batch set_graph_mode")
+        mode = self.use_graph if isinstance(self.use_graph, int) and not isinstance(self.use_graph, bool) \
+            else (1 if self.use_graph else 0)
+        _lib.check(L.uaamg_batch_set_graph_mode(self._h, mode), "batch set_graph_mode")
         return L
 
     def solveMultigridPCG(self, in_out_pressures: list, rhss: list) -> int:

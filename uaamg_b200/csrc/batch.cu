@@ -246,6 +246,7 @@ struct uaamg_batch {
     int smoother = UAAMG_SMOOTHER_SCHEDULED_RELAXED_JACOBI, max_iter = 100;
     float rel_tol = 1e-7f;
     int use_graph = 1;
+    int64_t solves = 0;
     // device tables (one allocation)
     char* dmem = nullptr;
     BRec* recs = nullptr;  // [depth][n]
@@ -600,8 +601,13 @@ static int brun_pcg(uaamg_batch* b, float* const* d_x, const float* const* d_b) 
     CK(cudaMemcpyAsync(b->ub, ub, (size_t)n * 8, cudaMemcpyHostToDevice, b->stream));
     int64_t launches = 0;
     PcgState* hs = bpin_states(b);
+    // A batch's first solve runs host-driven, as a handle's does: a batch
+    // formed for one solve (a served round whose set of requests changed)
+    // would pay the graph's capture and instantiation for a single launch.
+    const bool graph = b->use_graph == 2 || (b->use_graph == 1 && b->solves > 0);
+    b->solves++;
     if (b->all0.count > 0) {
-        if (b->use_graph) {
+        if (graph) {
             if (!b->exec || b->graph_key != b->smoother) bbuild_graph(b);
             CK(cudaGraphLaunch(b->exec, b->stream));
             CK(cudaMemcpyAsync(hs, b->states, (size_t)n * sizeof(PcgState), cudaMemcpyDeviceToHost, b->stream));
@@ -805,8 +811,8 @@ int uaamg_batch_get_stream(const uaamg_batch* b, void** stream) {
     return UAAMG_SUCCESS;
 }
 int uaamg_batch_set_graph_mode(uaamg_batch* b, int use_graph) {
-    if (!b) { set_error("NULL batch"); return UAAMG_ERR_INVALID_ARGUMENT; }
-    b->use_graph = use_graph ? 1 : 0;
+    if (!b || use_graph < 0 || use_graph > 2) { set_error("NULL batch or invalid graph mode"); return UAAMG_ERR_INVALID_ARGUMENT; }
+    b->use_graph = use_graph;
     return UAAMG_SUCCESS;
 }
 

@@ -1392,6 +1392,7 @@ static void destroy_graph(uaamg_poisson* h) {
 }
 
 static void build_graph(uaamg_poisson* h) {
+    double trace_t0 = trace_now();
     destroy_graph(h);
     cudaGraph_t g = nullptr;
     CK(cudaGraphCreate(&g, 0));
@@ -1434,7 +1435,9 @@ static void build_graph(uaamg_poisson* h) {
     }
     cudaGraph_t out = nullptr;
     CK(cudaStreamEndCapture(h->stream, &out));
+    TRACE("solve graph captured");
     CK(cudaGraphInstantiate(&h->graph_exec, g, 0));
+    TRACE("solve graph instantiated");
     h->graph = g;
     h->graph_key = graph_key(h);
 }
