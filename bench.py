@@ -937,12 +937,19 @@ def run_served(args, ws):
                      "by_kind": {k: {"completed": len(v), "p50_ms": pct(v, 50), "p99_ms": pct(v, 99)}
                                  for k, v in by_kind.items()},
                      "pressure_rounds": st["rounds"], "batch_graphs_built": st["batch_builds"],
+                     # what batching changes: pressure solves per second of pressure rounds (the rounds share the
+                     # GPU with the viscosity lanes in both forms)
+                     "pressure_solves_per_busy_s": round(st["pressure_solves"] / (st["pressure_busy_us"] * 1e-6), 1)
+                     if st["pressure_busy_us"] else None,
                      "peak_budget_GB": round(st["peak_bytes"] / 1e9, 2), "all_status_success": bool(stat_ok),
                      "pressure_fp64_rel_residual_max": max(res64) if res64 else None,
                      "pressure_iterations_mean": round(float(np.mean(it_p)), 2) if it_p else None}
         del srv
     b, p = out["batched"], out["plain"]
     out["solves_per_s_vs_plain"] = round(b["solves_per_s"] / p["solves_per_s"], 3) if p["solves_per_s"] else None
+    if b.get("pressure_solves_per_busy_s") and p.get("pressure_solves_per_busy_s"):
+        out["pressure_round_throughput_vs_plain"] = round(b["pressure_solves_per_busy_s"] /
+                                                          p["pressure_solves_per_busy_s"], 3)
     return out
 
 

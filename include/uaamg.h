@@ -590,6 +590,8 @@ typedef struct {
     int64_t submitted, queued, resident, done, failed;
     int64_t solves, rounds, batch_builds;
     int64_t used_bytes, peak_bytes;
+    int64_t pressure_solves;   /* solves done in pressure rounds */
+    int64_t pressure_busy_us;  /* wall time inside pressure rounds (rhs, solves, FP64 checks), microseconds */
 } uaamg_server_stats_t;
 int uaamg_server_default_options(uaamg_server_options* options);
 int uaamg_server_create(const uaamg_server_options* options, uaamg_server** out);

@@ -60,7 +60,8 @@ class ServerOptionsC(C.Structure):
 
 class ServerStatsC(C.Structure):
     _fields_ = [(k, C.c_int64) for k in ("submitted", "queued", "resident", "done", "failed", "solves", "rounds",
-                                         "batch_builds", "used_bytes", "peak_bytes")]
+                                         "batch_builds", "used_bytes", "peak_bytes", "pressure_solves",
+                                         "pressure_busy_us")]
 
 
 _lib = None

@@ -152,6 +152,8 @@ struct uaamg_server {
     std::deque<int64_t> queue;
     int64_t used = 0, peak = 0, next_id = 1;
     int64_t rounds = 0, solves = 0, batch_builds = 0;
+    int64_t pressure_solves = 0;
+    double pressure_busy_s = 0.0;  // wall time inside pressure rounds (rhs, solves, FP64 checks)
     srv_clock::time_point t0;
     std::thread loop;
     std::atomic<bool> stop{false};
@@ -292,6 +294,7 @@ static void srv_fail(uaamg_server* s, SrvReq& r, const char* what) {
 
 static void srv_pressure_round(uaamg_server* s, std::vector<SrvReq*>& act_in,
                                std::vector<std::unique_ptr<SrvSubstep>>& subs) {
+    const double t_start = s->now();
     // the substep's rhs of every request; a request whose inputs fail leaves the round, failed
     std::vector<SrvReq*> act;
     for (size_t i = 0; i < act_in.size(); ++i) {
@@ -359,6 +362,8 @@ static void srv_pressure_round(uaamg_server* s, std::vector<SrvReq*>& act_in,
     }
     s->rounds++;
     s->solves += (int64_t)n;
+    s->pressure_solves += (int64_t)n;
+    s->pressure_busy_s += t - t_start;
     s->cv.notify_all();
 }
 
@@ -720,6 +725,8 @@ int uaamg_server_stats(uaamg_server* s, uaamg_server_stats_t* out) {
     out->batch_builds = s->batch_builds;
     out->used_bytes = s->used;
     out->peak_bytes = s->peak;
+    out->pressure_solves = s->pressure_solves;
+    out->pressure_busy_us = (int64_t)(s->pressure_busy_s * 1e6);
     return UAAMG_SUCCESS;
     ABI_END
 }
