@@ -554,6 +554,29 @@ int uaamg_viscosity_get_stream(const uaamg_viscosity* h, void** stream);
 int uaamg_viscosity_set_graph_mode(uaamg_viscosity* h, int use_graph);
 int64_t uaamg_viscosity_kernel_launches(const uaamg_viscosity* h);
 
+/* packed_FloatGrid3 (SIMD_UAAMG/packed3grids.h, .cpp:11-83): the velocity of
+ * the reference's call sites as three staggered channel FloatGrids.
+ * from_vec3 (:11-43): channel c of a Vec3fGrid (components 3) with the vec3
+ * grid's leaf topology (its origins and masks): component c at active voxels,
+ * background[c] elsewhere.  out_c* are [leaf_count][512] floats, host memory
+ * (host values) or device memory (the _device form, device values, enqueued on
+ * `stream`).  The reference also shifts channel c's world transform by -dx/2
+ * along c; leaf grids are in index space and carry no transform. */
+int uaamg_packed3_from_vec3(const uaamg_leaf_grid* vec3, float* out_c0, float* out_c1, float* out_c2);
+int uaamg_packed3_from_vec3_device(const uaamg_leaf_grid* vec3, float* d_c0, float* d_c1, float* d_c2, void* stream);
+/* to_vec3 (:46-83): the Vec3fGrid over the union of the channels' leaves
+ * (OpenVDB tree order) and active masks; component c is channel c's value at
+ * its active voxels and 0 elsewhere (background (0,0,0)).  The topology call
+ * returns the union's leaf count (out_origins NULL) or fills out_origins
+ * [n][3] and out_masks [n][8] (leaf_count in: their capacity).  The value call
+ * fills [n][512][3] floats in that order. */
+int uaamg_packed3_to_vec3_topology(const uaamg_leaf_grid* c0, const uaamg_leaf_grid* c1, const uaamg_leaf_grid* c2,
+                                   int64_t* leaf_count, int32_t* out_origins, uint64_t* out_masks);
+int uaamg_packed3_to_vec3(const uaamg_leaf_grid* c0, const uaamg_leaf_grid* c1, const uaamg_leaf_grid* c2,
+                          float* out_values);
+int uaamg_packed3_to_vec3_device(const uaamg_leaf_grid* c0, const uaamg_leaf_grid* c1, const uaamg_leaf_grid* c2,
+                                 float* d_out_values, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Served form: many simulations' solves on one GPU (no counterpart in the
  * reference, which solves one domain per call).  A request is one simulation

@@ -79,6 +79,11 @@ EXPORTS = [
     ("uaamg_poisson_copy_rhs", i32, [vp, vp]),
     ("uaamg_poisson_solve_fp64_reference", i32, [vp, vp, vp, C.c_double, i32, C.POINTER(i32),
                                                  C.POINTER(C.c_double)]),
+    ("uaamg_packed3_from_vec3", i32, [pLG, vp, vp, vp]),
+    ("uaamg_packed3_from_vec3_device", i32, [pLG, vp, vp, vp, vp]),
+    ("uaamg_packed3_to_vec3_topology", i32, [pLG, pLG, pLG, C.POINTER(C.c_int64), vp, vp]),
+    ("uaamg_packed3_to_vec3", i32, [pLG, pLG, pLG, vp]),
+    ("uaamg_packed3_to_vec3_device", i32, [pLG, pLG, pLG, vp, vp]),
     ("uaamg_server_default_options", i32, [C.POINTER(ServerOptionsC)]),
     ("uaamg_server_create", i32, [C.POINTER(ServerOptionsC), C.POINTER(vp)]),
     ("uaamg_server_destroy", i32, [vp]),
