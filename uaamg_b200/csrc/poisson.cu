@@ -787,7 +787,12 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         for (int l = 1; l < nlev; ++l) {
             LevelDev& D = h->lv[l];
             if (D.L.nl == 0) continue;
-            k_coarsen<<<(unsigned)D.L.nl, 128, 0, s>>>(h->lv[l - 1].L, D.L.child, D.L.mask, level_out(D));
+            static bool coarsen_smem_set = false;
+            if (!coarsen_smem_set) {
+                CK(cudaFuncSetAttribute(k_coarsen, cudaFuncAttributeMaxDynamicSharedMemorySize, COARSEN_SMEM));
+                coarsen_smem_set = true;
+            }
+            k_coarsen<<<(unsigned)D.L.nl, 128, COARSEN_SMEM, s>>>(h->lv[l - 1].L, D.L.child, D.L.mask, level_out(D));
             CHECK_LAUNCH();
             h->launches++;
         }

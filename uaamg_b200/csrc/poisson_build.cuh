@@ -33,6 +33,33 @@ struct DGrid {
     }
 };
 
+// A grid seen from one leaf: the leaf indices of the leaf at `o` and of its six
+// face neighbours, resolved once per CTA (slot 0: the leaf; 1 + 2 axis +
+// (+ side): the neighbour), so a read at a voxel of the leaf or one voxel
+// across a face costs one load instead of a map lookup and a load.  get()
+// returns what DGrid::get returns for those voxels.
+struct DGridNb {
+    const DGrid* g;
+    const int* li;  // [7], shared memory
+    int ox, oy, oz;
+    __device__ __forceinline__ float get(int x, int y, int z, int c) const {
+        const int lx = (x - ox) >> 3, ly = (y - oy) >> 3, lz = (z - oz) >> 3;
+        const int slot = lx ? (lx < 0 ? 1 : 2) : (ly ? (ly < 0 ? 3 : 4) : (lz ? (lz < 0 ? 5 : 6) : 0));
+        const int l = li[slot];
+        if (l < 0) return c == 0 ? g->bg0 : (c == 1 ? g->bg1 : g->bg2);
+        const int off = ((x & 7) << 6) | ((y & 7) << 3) | (z & 7);
+        return g->val[((long long)l * UAAMG_LEAF + off) * g->comps + c];
+    }
+};
+// the seven leaf indices of grid g around origin o, by threads t < 7 (the caller syncs)
+__device__ __forceinline__ void nb7_resolve(const DGrid& g, int ox, int oy, int oz, int t, int* li) {
+    if (t < 7) {
+        const int ax = (t - 1) >> 1, sg = ((t - 1) & 1) ? 8 : -8;
+        li[t] = g.leaf_of(ox + (t > 0 && ax == 0 ? sg : 0), oy + (t > 0 && ax == 1 ? sg : 0),
+                          oz + (t > 0 && ax == 2 ? sg : 0));
+    }
+}
+
 // levelset_util.cpp:4-13
 __device__ __forceinline__ float fraction_inside1(float l, float r) {
     if (l < 0 && r < 0) return 1.f;
@@ -56,7 +83,8 @@ struct LevelOut {
 
 // BuildFinestMatrix for one voxel (simd_vdb_poisson.cpp:520-584): returns diag
 // (0 = not a DOF) and the three minus-face entries.
-__device__ __forceinline__ float finest_voxel(const DGrid& phi, const DGrid& fw, int gx, int gy, int gz, float phic,
+template <class GP, class GF>
+__device__ __forceinline__ float finest_voxel(const GP& phi, const GF& fw, int gx, int gy, int gz, float phic,
                                               float dtOverDxSqr, float* xyz) {
     float dg = 0.f;
     xyz[0] = xyz[1] = xyz[2] = 0.f;
@@ -141,10 +169,14 @@ __global__ void __launch_bounds__(128) k_gather_host_leaves(const float4* __rest
 __global__ void __launch_bounds__(128) k_finest_mask(DGrid phi, const uint64_t* phi_mask, const int* phi_org, DGrid fw,
                                                      float dtOverDxSqr, uint64_t* out_mask) {
     __shared__ uint32_t bits[16];
+    __shared__ int pli[7], fli[7];
     const int leaf = blockIdx.x, t = threadIdx.x;
     if (t < 16) bits[t] = 0;
-    __syncthreads();
     const int ox = phi_org[3 * leaf], oy = phi_org[3 * leaf + 1], oz = phi_org[3 * leaf + 2];
+    nb7_resolve(phi, ox, oy, oz, t, pli);
+    nb7_resolve(fw, ox, oy, oz, t, fli);
+    __syncthreads();
+    const DGridNb P{&phi, pli, ox, oy, oz}, W{&fw, fli, ox, oy, oz};
     unsigned my = 0;
     for (int j = 0; j < 4; ++j) {
         const int off = 4 * t + j;
@@ -152,7 +184,7 @@ __global__ void __launch_bounds__(128) k_finest_mask(DGrid phi, const uint64_t* 
         const float phic = phi.val[(long long)leaf * UAAMG_LEAF + off];
         if (!(phic < 0.f)) continue;
         float xyz[3];
-        float dg = finest_voxel(phi, fw, ox + (off >> 6), oy + ((off >> 3) & 7), oz + (off & 7), phic, dtOverDxSqr, xyz);
+        float dg = finest_voxel(P, W, ox + (off >> 6), oy + ((off >> 3) & 7), oz + (off & 7), phic, dtOverDxSqr, xyz);
         if (dg != 0.f) my |= 1u << j;
     }
     // thread t's 4 bits belong to word t>>4 at bit (t&15)*4: 8 threads per 32-bit half
@@ -218,9 +250,14 @@ __device__ __forceinline__ void finalize_leaf(const LevelOut& O, int leaf, int t
 // pass 1: level-0 coefficients into the compacted (DOF-leaf) order
 __global__ void __launch_bounds__(128) k_finest_coef(DGrid phi, const int* phi_org, DGrid fw, float dtOverDxSqr,
                                                      const int* src_leaf, const uint64_t* mask, LevelOut O) {
+    __shared__ int pli[7], fli[7];
     const int leaf = blockIdx.x, t = threadIdx.x;
     const int s = src_leaf[leaf];
     const int ox = phi_org[3 * s], oy = phi_org[3 * s + 1], oz = phi_org[3 * s + 2];
+    nb7_resolve(phi, ox, oy, oz, t, pli);
+    nb7_resolve(fw, ox, oy, oz, t, fli);
+    __syncthreads();
+    const DGridNb P{&phi, pli, ox, oy, oz}, W{&fw, fli, ox, oy, oz};
     const unsigned m = mask4(mask, leaf, t);
     float4 dg = f4splat(O.def_diag), vx = f4splat(O.def_face), vy = vx, vz = vx;
 #pragma unroll
@@ -229,7 +266,7 @@ __global__ void __launch_bounds__(128) k_finest_coef(DGrid phi, const int* phi_o
         const int off = 4 * t + j;
         const float phic = phi.val[(long long)s * UAAMG_LEAF + off];
         float xyz[3];
-        float d = finest_voxel(phi, fw, ox + (off >> 6), oy + ((off >> 3) & 7), oz + (off & 7), phic, dtOverDxSqr, xyz);
+        float d = finest_voxel(P, W, ox + (off >> 6), oy + ((off >> 3) & 7), oz + (off & 7), phic, dtOverDxSqr, xyz);
         f4set(dg, j, d);
         f4set(vx, j, xyz[0]);
         f4set(vy, j, xyz[1]);
@@ -239,9 +276,42 @@ __global__ void __launch_bounds__(128) k_finest_coef(DGrid phi, const int* phi_o
 }
 
 // Galerkin coarsening of the 7-point operator (initializeFromFineLevel,
-// .cpp:353-467): 0.5 * R A P with R = 1/8 sum, P = injection.
+// .cpp:353-467): 0.5 * R A P with R = 1/8 sum, P = injection.  One CTA per
+// coarse leaf.  Its 8 child leaves' diag, c_x, c_y, c_z (the effective
+// values; a trimmed leaf holds its default) and the DOF masks a fine voxel
+// consults (its own leaf's and its -x, -y, -z neighbours') are staged into
+// shared memory with coalesced loads first; each thread then sums its 4
+// coarse voxels' 8 fine voxels in the order of the unstaged loop.  (Loading
+// per fine voxel, every thread ran a chain of 32 dependent global loads: 50 us
+// for a 284-leaf level.)
+constexpr int COARSEN_SMEM = 4 * 8 * UAAMG_LEAF * 4;  // dynamic shared memory of k_coarsen (64 KB)
 __global__ void __launch_bounds__(128) k_coarsen(DLevel F, const int* child, const uint64_t* cmask, LevelOut O) {
+    extern __shared__ __align__(16) float cst[];  // [4 arrays][8 children][512]
+    __shared__ uint64_t msk[8][4][8];            // [child][own, -x, -y, -z][word]
+    __shared__ int kid[8];
     const int leaf = blockIdx.x, t = threadIdx.x;
+    if (t < 8) kid[t] = child[leaf * 8 + t];
+    __syncthreads();
+    for (int i = t; i < 8 * 4 * 8; i += 128) {
+        const int q = i >> 5, r = (i >> 3) & 3, w = i & 7;
+        const int fl = kid[q];
+        uint64_t v = 0;
+        if (fl >= 0) {
+            const int src = r == 0 ? fl : F.nbr[(long long)fl * 6 + 2 * (r - 1)];
+            if (src >= 0) v = F.mask[(long long)src * 8 + w];
+        }
+        msk[q][r][w] = v;
+    }
+    const float* arr[4] = {F.diag, F.cx, F.cy, F.cz};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int fl = kid[q];
+        if (fl < 0) continue;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+            reinterpret_cast<float4*>(cst + (a * 8 + q) * UAAMG_LEAF)[t] = ld4(arr[a], fl, t);
+    }
+    __syncthreads();
     const unsigned m = mask4(cmask, leaf, t);
     float4 dg = f4splat(O.def_diag), vx = f4splat(O.def_face), vy = vx, vz = vx;
     const float factor = 0.5f * (1.0f / 8.0f);
@@ -250,9 +320,12 @@ __global__ void __launch_bounds__(128) k_coarsen(DLevel F, const int* child, con
         if (!((m >> j) & 1)) continue;
         const int off = 4 * t + j;
         const int X = off >> 6, Y = (off >> 3) & 7, Z = off & 7;
-        const int fl = child[leaf * 8 + (((X >= 4) << 2) | ((Y >= 4) << 1) | (Z >= 4))];
-        const uint64_t* fm = F.mask + (long long)fl * 8;
-        const int* fn = F.nbr + (long long)fl * 6;
+        const int q = ((X >= 4) << 2) | ((Y >= 4) << 1) | (Z >= 4);
+        const uint64_t* fm = msk[q][0];
+        const float* sd = cst + (0 * 8 + q) * UAAMG_LEAF;
+        const float* sx = cst + (1 * 8 + q) * UAAMG_LEAF;
+        const float* sy = cst + (2 * 8 + q) * UAAMG_LEAF;
+        const float* sz = cst + (3 * 8 + q) * UAAMG_LEAF;
         float d = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
         for (int ii = 0; ii < 2; ++ii)
             for (int jj = 0; jj < 2; ++jj)
@@ -260,19 +333,18 @@ __global__ void __launch_bounds__(128) k_coarsen(DLevel F, const int* child, con
                     const int fx = (2 * X + ii) & 7, fy = (2 * Y + jj) & 7, fz = (2 * Z + kk) & 7;
                     const int fo = (fx << 6) | (fy << 3) | fz;
                     if (!((fm[fo >> 6] >> (fo & 63)) & 1ull)) continue;
-                    const long long fi = (long long)fl * UAAMG_LEAF + fo;
-                    d = __fadd_rn(d, F.diag[fi]);
+                    d = __fadd_rn(d, sd[fo]);
                     // -x neighbour a DOF?
                     bool on;
                     if (fx > 0) on = (fm[(fo - 64) >> 6] >> ((fo - 64) & 63)) & 1ull;
-                    else { int n = fn[0]; on = n >= 0 && ((F.mask[(long long)n * 8 + 7] >> ((fo + 448) & 63)) & 1ull); }
-                    if (on) { if (ii == 0) tx = __fadd_rn(tx, F.cx[fi]); else d = __fadd_rn(d, __fmul_rn(2.f, F.cx[fi])); }
+                    else on = (msk[q][1][7] >> ((fo + 448) & 63)) & 1ull;
+                    if (on) { if (ii == 0) tx = __fadd_rn(tx, sx[fo]); else d = __fadd_rn(d, __fmul_rn(2.f, sx[fo])); }
                     if (fy > 0) on = (fm[(fo - 8) >> 6] >> ((fo - 8) & 63)) & 1ull;
-                    else { int n = fn[2]; on = n >= 0 && ((F.mask[(long long)n * 8 + ((fo + 56) >> 6)] >> ((fo + 56) & 63)) & 1ull); }
-                    if (on) { if (jj == 0) ty = __fadd_rn(ty, F.cy[fi]); else d = __fadd_rn(d, __fmul_rn(2.f, F.cy[fi])); }
+                    else on = (msk[q][2][(fo + 56) >> 6] >> ((fo + 56) & 63)) & 1ull;
+                    if (on) { if (jj == 0) ty = __fadd_rn(ty, sy[fo]); else d = __fadd_rn(d, __fmul_rn(2.f, sy[fo])); }
                     if (fz > 0) on = (fm[(fo - 1) >> 6] >> ((fo - 1) & 63)) & 1ull;
-                    else { int n = fn[4]; on = n >= 0 && ((F.mask[(long long)n * 8 + ((fo + 7) >> 6)] >> ((fo + 7) & 63)) & 1ull); }
-                    if (on) { if (kk == 0) tz = __fadd_rn(tz, F.cz[fi]); else d = __fadd_rn(d, __fmul_rn(2.f, F.cz[fi])); }
+                    else on = (msk[q][3][(fo + 7) >> 6] >> ((fo + 7) & 63)) & 1ull;
+                    if (on) { if (kk == 0) tz = __fadd_rn(tz, sz[fo]); else d = __fadd_rn(d, __fmul_rn(2.f, sz[fo])); }
                 }
         f4set(dg, j, __fmul_rn(d, factor));
         f4set(vx, j, __fmul_rn(tx, factor));
@@ -330,16 +402,27 @@ __global__ void __launch_bounds__(128) k_spai0(DLevel L, float* spai0, uint32_t*
 // explicit coarsest matrix in DOF order (getTriplets, .cpp:129-206)
 __global__ void __launch_bounds__(128) k_coarsest_ell(DLevel L, const int* dof_base, int* dof_slot, float* diag,
                                                       float* invd, int* col, float* val) {
+    // the leaf's and its six face neighbours' DOF masks and DOF bases, staged
+    // once (slot 0: the leaf, 1 + 2c + s: neighbour -/+ along axis c)
+    __shared__ uint64_t mks[7][8];
+    __shared__ int nbl[7], nbase[7];
     const int leaf = blockIdx.x, t = threadIdx.x;
+    if (t < 7) {
+        const int n = t == 0 ? leaf : L.nbr[(long long)leaf * 6 + t - 1];
+        nbl[t] = n;
+        nbase[t] = n >= 0 ? dof_base[n] : 0;
+    }
+    __syncthreads();
+    if (t < 56) mks[t >> 3][t & 7] = nbl[t >> 3] >= 0 ? L.mask[(long long)nbl[t >> 3] * 8 + (t & 7)] : 0ull;
+    __syncthreads();
     const unsigned m = mask4(L.mask, leaf, t);
-    const uint64_t* mk = L.mask + (long long)leaf * 8;
-    const int* nb = L.nbr + (long long)leaf * 6;
+    const uint64_t* mk = mks[0];
     const float* arr[3] = {L.cx, L.cy, L.cz};
     for (int j = 0; j < 4; ++j) {
         if (!((m >> j) & 1)) continue;
         const int off = 4 * t + j;
         const long long me = (long long)leaf * UAAMG_LEAF + off;
-        int row = dof_base[leaf];
+        int row = nbase[0];
         for (int w = 0; w < (off >> 6); ++w) row += __popcll(mk[w]);
         row += __popcll(mk[off >> 6] & ((1ull << (off & 63)) - 1ull));
         dof_slot[row] = (int)me;
@@ -350,13 +433,14 @@ __global__ void __launch_bounds__(128) k_coarsest_ell(DLevel L, const int* dof_b
             const int sh_ = (c == 0) ? 64 : (c == 1 ? 8 : 1);
             const int loc = (c == 0) ? (off >> 6) : (c == 1 ? ((off >> 3) & 7) : (off & 7));
             for (int s = 0; s < 2; ++s) {
-                int nl = leaf, no;
-                if (s == 0) { no = off - sh_; if (loc == 0) { nl = nb[2 * c]; no = off + 7 * sh_; } }
-                else { no = off + sh_; if (loc == 7) { nl = nb[2 * c + 1]; no = off - 7 * sh_; } }
-                int e = 2 * c + s;
-                if (nl >= 0 && ((L.mask[(long long)nl * 8 + (no >> 6)] >> (no & 63)) & 1ull)) {
-                    const uint64_t* nm = L.mask + (long long)nl * 8;
-                    int d = dof_base[nl];
+                int slot = 0, no;
+                if (s == 0) { no = off - sh_; if (loc == 0) { slot = 1 + 2 * c; no = off + 7 * sh_; } }
+                else { no = off + sh_; if (loc == 7) { slot = 2 + 2 * c; no = off - 7 * sh_; } }
+                const int nl = nbl[slot];
+                const int e = 2 * c + s;
+                const uint64_t* nm = mks[slot];
+                if (nl >= 0 && ((nm[no >> 6] >> (no & 63)) & 1ull)) {
+                    int d = nbase[slot];
                     for (int w = 0; w < (no >> 6); ++w) d += __popcll(nm[w]);
                     d += __popcll(nm[no >> 6] & ((1ull << (no & 63)) - 1ull));
                     col[row * 6 + e] = d;
@@ -374,11 +458,20 @@ __global__ void __launch_bounds__(128) k_coarsest_ell(DLevel L, const int* dof_b
 // F = w u + (1-w) u_solid; zero when all six face weights are zero.
 __global__ void __launch_bounds__(128) k_build_rhs(const uint64_t* mask, const int* org, DGrid fw, DGrid vx, DGrid vy,
                                                    DGrid vz, DGrid sv, float invdx, float* rhs) {
+    __shared__ int li[5][7];
     const int leaf = blockIdx.x, t = threadIdx.x;
     const unsigned m = mask4(mask, leaf, t);
     float4 out = f4zero();
     const int ox = org[3 * leaf], oy = org[3 * leaf + 1], oz = org[3 * leaf + 2];
-    const DGrid* vel[3] = {&vx, &vy, &vz};
+    nb7_resolve(fw, ox, oy, oz, t, li[0]);
+    nb7_resolve(vx, ox, oy, oz, t, li[1]);
+    nb7_resolve(vy, ox, oy, oz, t, li[2]);
+    nb7_resolve(vz, ox, oy, oz, t, li[3]);
+    nb7_resolve(sv, ox, oy, oz, t, li[4]);
+    __syncthreads();
+    const DGridNb FW{&fw, li[0], ox, oy, oz}, SV{&sv, li[4], ox, oy, oz};
+    const DGridNb VX{&vx, li[1], ox, oy, oz}, VY{&vy, li[2], ox, oy, oz}, VZ{&vz, li[3], ox, oy, oz};
+    const DGridNb* vel[3] = {&VX, &VY, &VZ};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (!((m >> j) & 1)) continue;
@@ -391,10 +484,10 @@ __global__ void __launch_bounds__(128) k_build_rhs(const uint64_t* mask, const i
             const bool pos = (f & 1) == 0;
             int c[3] = {g[0], g[1], g[2]};
             if (pos) c[ch] += 1;
-            const float w = fw.get(c[0], c[1], c[2], ch);
+            const float w = FW.get(c[0], c[1], c[2], ch);
             if (w != 0.f) nz = true;
             const float v = vel[ch]->get(c[0], c[1], c[2], 0);
-            const float s = sv.get(c[0], c[1], c[2], ch);
+            const float s = SV.get(c[0], c[1], c[2], ch);
             const float flux = __fmul_rn(invdx, __fadd_rn(__fmul_rn(w, v), __fmul_rn(__fsub_rn(1.0f, w), s)));
             r = pos ? __fsub_rn(r, flux) : __fadd_rn(r, flux);
         }
