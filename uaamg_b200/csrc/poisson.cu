@@ -227,7 +227,7 @@ static void coarsen_topology(HostLevel& F, HostLevel& C) {
         corg.push_back(l[2] * 8);
         keys.push_back({vdb_key128(&corg[3 * (size_t)k]), k});
     }
-    std::sort(keys.begin(), keys.end());
+    if (!std::is_sorted(keys.begin(), keys.end())) std::sort(keys.begin(), keys.end());
     const int nu = (int)keys.size();
     std::vector<int32_t> uorg((size_t)nu * 3);
     for (int i = 0; i < nu; ++i) std::copy(&corg[3 * (size_t)keys[i].second], &corg[3 * (size_t)keys[i].second] + 3, &uorg[3 * (size_t)i]);
@@ -583,6 +583,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         CK(ctx_pinned_acquire(h->ctx, (size_t)4 << 20, &h->pin_in, &h->pin_in_cap));
         PinStage stage{(char*)h->pin_in, h->pin_in_cap, 0};
         upload_grid(h, phi, dphi, phimap, tofree, &stage);
+        TRACE("  liquid SDF up");
         // the liquid SDF's origins and active masks, its DOF masks, its per-leaf liquid flags
         size_t extra = carve_size((size_t)nphi * 8, 8) * 2 + carve_size((size_t)nphi * 3, 4) + carve_size((size_t)nphi, 1);
         void* mem = nullptr;
@@ -617,7 +618,9 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
                 fgp = &fgather;
             }
         }
+        TRACE("  SDF tables up");
         upload_grid_cs(h->ctx, s, fw, dfw, fwmap, tofree, nullptr, nullptr, &stage, fgp);
+        TRACE("  face weights up");
         // The velocities of the right-hand side go up on a second stream once
         // the SDF and the face weights are up, so their copies overlap the DOF
         // mask kernel, the host topology and the coefficient kernels.
@@ -654,7 +657,9 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             for (int w = 0; w < 8; ++w) any |= dofmask[8 * i + w];
             if (any) keys.push_back({vdb_key128(&phi->origins[3 * i]), (int)i});
         }
-        std::sort(keys.begin(), keys.end());
+        // inputs from an OpenVDB leaf iteration are in tree order already
+        if (!std::is_sorted(keys.begin(), keys.end())) std::sort(keys.begin(), keys.end());
+        TRACE("  level-0 leaves ordered");
         std::vector<int32_t> src(keys.size());
         L0.org.resize(keys.size() * 3);
         L0.mask.resize(keys.size() * 8);
@@ -666,12 +671,14 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         }
         L0.nl = (int)keys.size();
         finalize_host_level(L0);
+        TRACE("  level-0 tables");
         // ---- coarse topology: constructMultigridHierarchy (.cpp:1813-1842)
         while (h->host.back().ndof > 4000 && h->host.size() < 32) {
             h->host.emplace_back();
             HostLevel& F = h->host[h->host.size() - 2];
             HostLevel& C = h->host.back();
             coarsen_topology(F, C);
+            TRACE("  coarse level");
         }
         const int nlev = (int)h->host.size();
         TRACE("host topology");
