@@ -379,10 +379,11 @@ class PoissonBytes:
         return None
 
     @staticmethod
-    def ncu_tag(label: str) -> str:
-        """The kernel name the committed ncu summaries use for this class."""
-        if "jacobi staged" in label:
-            return "k_sweep_staged<0>"
+    def ncu_tag(label: str, leaves: int) -> str:
+        """The kernel name and level size the committed ncu summaries use for
+        this class (a kernel's traffic depends on the level it sweeps)."""
+        if "jacobi staged" in label and "+dot" not in label:
+            return f"k_sweep_staged<0> ({leaves} leaves)"
         return label
 
 
@@ -1201,7 +1202,11 @@ def main():
     pbytes = PoissonBytes(lap)
     peak, peak_kind = _peaks()
     prof_ms = sum(v[0] for v in pprof.values())
-    ranked = sorted(((k, v) for k, v in pprof.items() if pbytes.launch_bytes(k) is not None), key=lambda kv: -kv[1][0])
+    # The dominant bandwidth kernel class: the most algorithmic bytes per solve.  (Event pairs around every launch
+    # add each launch's latency, so ranking by event time would favour the many small coarse-level launches; the
+    # ncu launch list, with device times, ranks the level-0 Jacobi sweep first among the bandwidth kernels.)
+    ranked = sorted(((k, v) for k, v in pprof.items() if pbytes.launch_bytes(k) is not None),
+                    key=lambda kv: -pbytes.launch_bytes(kv[0]) * kv[1][1])
     top_label, (top_ms, top_cnt) = max(pprof.items(), key=lambda kv: kv[1][0])
     dom_label, (dom_ms, dom_cnt) = ranked[0]
     dom_bytes = pbytes.launch_bytes(dom_label)
@@ -1268,18 +1273,21 @@ def main():
             "roofline": {"bound": "hbm", "kernel": f"{dom_label} ({pleaves[int(dom_label[1])]} leaves)",
                          "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
-                         "traffic": _traffic_from_profile(pbytes.ncu_tag(dom_label)),
+                         "traffic": _traffic_from_profile(pbytes.ncu_tag(dom_label, pleaves[int(dom_label[1])])),
                          "algorithmic_bytes_per_launch": round(dom_bytes),
                          "avg_launch_us": round(dom_us, 2), "launches": dom_cnt,
                          "share_of_solve": round(dom_ms / prof_ms, 3),
                          "all_bandwidth_kernels_GBps": round(agg_bytes / (agg_ms * 1e-3) / 1e9, 1),
                          "top_kernel_by_time": {"label": top_label, "share_of_solve": round(top_ms / prof_ms, 3),
                                                 "avg_launch_us": round(top_ms / top_cnt * 1e3, 2)},
-                         "note": "the bandwidth kernel class with the largest device time in one solve (CUDA event "
-                                 "pairs around every launch, host-driven loop); algorithmic bytes: every array the "
-                                 "kernel must touch once per DOF at 4 B, coefficient arrays only where stored; "
-                                 "top_kernel_by_time may be a latency-bound one (the cluster bottom-cycle kernel "
-                                 "with the coarsest CG)"},
+                         "note": "the bandwidth kernel class moving the most algorithmic bytes in one solve (the "
+                                 "ncu launch list ranks it first of the bandwidth kernels by device time, "
+                                 "profiles/poisson128_pcg_solve_launch_list.md); duration from CUDA event pairs "
+                                 "around every launch of a host-driven solve (they include the launch latency); "
+                                 "algorithmic bytes: every array the kernel must touch once per DOF at 4 B, "
+                                 "coefficient arrays only where stored; traffic: ncu DRAM bytes of one launch of the "
+                                 "same kernel on the same level; top_kernel_by_time may be a latency-bound one (the "
+                                 "cluster bottom-cycle kernel with the coarsest CG)"},
             "tuning": tuning,
             "kernel_profile_ms": {k: [round(v[0], 4), v[1]] for k, v in sorted(pprof.items(), key=lambda kv: -kv[1][0])},
             "clocks": clocks,
