@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <immintrin.h>
 #include <climits>
 #include <cmath>
 #include <cstdint>
@@ -102,6 +103,25 @@ static inline unsigned __int128 vdb_key128(const int32_t* o) {
 // plane (bit 8y + z); pairs of planes are OR-ed, then pairs in y and z, and the
 // 4x4 bits at (2yy, 2zz) are compressed into nibbles and placed at the
 // octant's (y, z) quarter of the coarse words ox*4 .. ox*4+3.
+__attribute__((target("avx2"))) static void coarse_bits_from_child_avx2(const uint64_t* fm, int a, uint64_t* cw) {
+    // the four plane pairs (2px, 2px+1) as the four lanes: the same integer steps as the scalar form
+    const int ox = (a >> 2) & 1, oy = (a >> 1) & 1, oz = a & 1;
+    __m256i p = _mm256_or_si256(_mm256_setr_epi64x((long long)fm[0], (long long)fm[2], (long long)fm[4], (long long)fm[6]),
+                                _mm256_setr_epi64x((long long)fm[1], (long long)fm[3], (long long)fm[5], (long long)fm[7]));
+    p = _mm256_or_si256(p, _mm256_srli_epi64(p, 1));
+    p = _mm256_or_si256(p, _mm256_srli_epi64(p, 8));
+    __m256i q = _mm256_and_si256(p, _mm256_set1_epi64x(0x0055005500550055ll));
+    q = _mm256_and_si256(_mm256_or_si256(q, _mm256_srli_epi64(q, 1)), _mm256_set1_epi64x(0x0033003300330033ll));
+    q = _mm256_and_si256(_mm256_or_si256(q, _mm256_srli_epi64(q, 2)), _mm256_set1_epi64x(0x000F000F000F000Fll));
+    const __m256i nib = _mm256_set1_epi64x(0xF);
+    __m256i dep = _mm256_and_si256(q, nib);
+    dep = _mm256_or_si256(dep, _mm256_slli_epi64(_mm256_and_si256(_mm256_srli_epi64(q, 16), nib), 8));
+    dep = _mm256_or_si256(dep, _mm256_slli_epi64(_mm256_and_si256(_mm256_srli_epi64(q, 32), nib), 16));
+    dep = _mm256_or_si256(dep, _mm256_slli_epi64(_mm256_and_si256(_mm256_srli_epi64(q, 48), nib), 24));
+    dep = _mm256_sll_epi64(dep, _mm_cvtsi32_si128(oy * 32 + oz * 4));
+    __m256i* dst = reinterpret_cast<__m256i*>(cw + ox * 4);
+    _mm256_storeu_si256(dst, _mm256_or_si256(_mm256_loadu_si256(dst), dep));
+}
 static inline void coarse_bits_from_child(const uint64_t* fm, int a, uint64_t* cw) {
     const int ox = (a >> 2) & 1, oy = (a >> 1) & 1, oz = a & 1;
     for (int px = 0; px < 4; ++px) {
@@ -119,6 +139,29 @@ static inline void coarse_bits_from_child(const uint64_t* fm, int a, uint64_t* c
 
 // population count of a 64-bit mask on the host (SWAR bit count; inline, no
 // library call on CPUs compiled without a popcount instruction)
+static inline int host_popc64(uint64_t x);
+// base[i] = acc + the set bits of the 8-word masks before leaf i; returns the
+// total.  The CPU's popcount instruction where it has one (a DOF-numbering
+// pass over a level's masks is on the host side of every construction).
+__attribute__((target("popcnt"))) static int64_t popc_prefix_hw(const uint64_t* m, size_t nleaves, int32_t* base,
+                                                                 int64_t acc) {
+    for (size_t i = 0; i < nleaves; ++i) {
+        base[i] = (int32_t)acc;
+        for (int w = 0; w < 8; ++w) acc += __builtin_popcountll(m[8 * i + w]);
+    }
+    return acc;
+}
+static int64_t popc_prefix_sw(const uint64_t* m, size_t nleaves, int32_t* base, int64_t acc) {
+    for (size_t i = 0; i < nleaves; ++i) {
+        base[i] = (int32_t)acc;
+        for (int w = 0; w < 8; ++w) acc += host_popc64(m[8 * i + w]);
+    }
+    return acc;
+}
+static int64_t popc_prefix(const uint64_t* m, size_t nleaves, int32_t* base, int64_t acc) {
+    static const bool hw = __builtin_cpu_supports("popcnt");
+    return hw ? popc_prefix_hw(m, nleaves, base, acc) : popc_prefix_sw(m, nleaves, base, acc);
+}
 static inline int host_popc64(uint64_t x) {
     x = x - ((x >> 1) & 0x5555555555555555ull);
     x = (x & 0x3333333333333333ull) + ((x >> 2) & 0x3333333333333333ull);
@@ -178,23 +221,21 @@ struct HostLevel {
 };
 
 static void finalize_host_level(HostLevel& L) {
-    L.map.build(L.nl, L.org.data());
+    // a one-leaf margin puts every leaf's face-neighbour cells inside the map
+    L.map.build(L.nl, L.org.data(), 1);
     L.nbr.assign((size_t)L.nl * 6, -1);
-    for (int i = 0; i < L.nl; ++i) {
-        const int32_t* o = &L.org[3 * i];
-        for (int d = 0; d < 6; ++d) {
-            int p[3] = {o[0] >> 3, o[1] >> 3, o[2] >> 3};
-            p[d >> 1] += (d & 1) ? 1 : -1;
-            L.nbr[6 * i + d] = L.map.find_leaf(p[0], p[1], p[2]);
+    if (L.nl > 0) {
+        const int64_t s0 = (int64_t)L.map.dim[1] * L.map.dim[2], s1 = L.map.dim[2];
+        const int64_t off[6] = {-s0, s0, -s1, s1, -1, 1};
+        const int32_t* idx = L.map.idx.data();
+        for (int i = 0; i < L.nl; ++i) {
+            const int32_t* o = &L.org[3 * i];
+            const int64_t base = L.map.cell(o[0] >> 3, o[1] >> 3, o[2] >> 3);
+            for (int d = 0; d < 6; ++d) L.nbr[6 * i + d] = idx[base + off[d]];
         }
     }
     L.dof_base.resize(L.nl);
-    int64_t acc = 0;
-    for (int i = 0; i < L.nl; ++i) {
-        L.dof_base[i] = (int32_t)acc;
-        for (int w = 0; w < 8; ++w) acc += host_popc64(L.mask[8 * i + w]);
-    }
-    L.ndof = acc;
+    L.ndof = popc_prefix(L.mask.data(), (size_t)L.nl, L.dof_base.data(), 0);
 }
 
 // coarse level topology from the fine level (TouchCoarseLeafReducer,
@@ -233,13 +274,19 @@ static void coarsen_topology(HostLevel& F, HostLevel& C) {
     for (int i = 0; i < nu; ++i) std::copy(&corg[3 * (size_t)keys[i].second], &corg[3 * (size_t)keys[i].second] + 3, &uorg[3 * (size_t)i]);
     std::vector<uint64_t> cmask((size_t)nu * 8, 0);
     std::vector<int32_t> child((size_t)nu * 8, -1);
+    // the children of coarse leaf c are the fine leaves 2c + {0,1}^3: inside the fine map's one-leaf margin
+    const int64_t fs0 = (int64_t)F.map.dim[1] * F.map.dim[2], fs1 = F.map.dim[2];
+    const int64_t coff[8] = {0, 1, fs1, fs1 + 1, fs0, fs0 + 1, fs0 + fs1, fs0 + fs1 + 1};
+    const int32_t* fidx = F.map.idx.data();
+    static const bool avx2 = __builtin_cpu_supports("avx2");
     for (int i = 0; i < nu; ++i) {
+        const int64_t c0 = F.map.cell(uorg[3 * i] >> 2, uorg[3 * i + 1] >> 2, uorg[3 * i + 2] >> 2);
         for (int a = 0; a < 8; ++a) {
-            const int lx = (2 * uorg[3 * i] + ((a >> 2) & 1) * 8) >> 3, ly = (2 * uorg[3 * i + 1] + ((a >> 1) & 1) * 8) >> 3,
-                      lz = (2 * uorg[3 * i + 2] + (a & 1) * 8) >> 3;
-            const int fl = F.map.find_leaf(lx, ly, lz);
+            const int fl = fidx[c0 + coff[a]];
             child[8 * i + a] = fl;
-            if (fl >= 0) coarse_bits_from_child(&F.mask[8 * (size_t)fl], a, &cmask[8 * (size_t)i]);
+            if (fl < 0) continue;
+            if (avx2) coarse_bits_from_child_avx2(&F.mask[8 * (size_t)fl], a, &cmask[8 * (size_t)i]);
+            else coarse_bits_from_child(&F.mask[8 * (size_t)fl], a, &cmask[8 * (size_t)i]);
         }
     }
     // drop leaves without DOF

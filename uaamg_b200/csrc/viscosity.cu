@@ -132,11 +132,7 @@ static void finalize_vlevel(VHostLevel& L) {
     L.dof_base.assign((size_t)3 * L.nl, 0);
     int64_t acc = 0;
     for (int c = 0; c < 3; ++c)
-        for (int i = 0; i < L.nl; ++i) {
-            L.dof_base[(size_t)c * L.nl + i] = (int32_t)acc;
-            const uint64_t* m = &L.dof[((size_t)c * L.nl + i) * 8];
-            for (int w = 0; w < 8; ++w) acc += host_popc64(m[w]);
-        }
+        acc = popc_prefix(&L.dof[(size_t)c * L.nl * 8], (size_t)L.nl, &L.dof_base[(size_t)c * L.nl], acc);
     L.ndof = acc;
     L.child.assign((size_t)L.nl * 8, -1);
     L.parent.assign((size_t)L.nl, -1);
