@@ -537,11 +537,12 @@ static void check_grid(const uaamg_leaf_grid* g, int comps, const char* name) {
         set_error("%s has no origins/values", name);
         throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT};
     }
-    for (int64_t i = 0; i < 3 * g->leaf_count; ++i)
-        if (g->origins[i] & 7) {
-            set_error("%s: leaf origins must be multiples of 8", name);
-            throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT};
-        }
+    int32_t low = 0;  // the OR of every origin coordinate's low bits (one vectorisable pass)
+    for (int64_t i = 0; i < 3 * g->leaf_count; ++i) low |= g->origins[i];
+    if (low & 7) {
+        set_error("%s: leaf origins must be multiples of 8", name);
+        throw UaamgError{UAAMG_ERR_INVALID_ARGUMENT};
+    }
 }
 
 static LevelOut level_out(LevelDev& d) {
@@ -751,24 +752,47 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         bytes += carve_size(sizeof(PcgState), 1) + carve_size(64, 4) + carve_size(src.size(), 4);
         CK(ctx_dev_alloc(h->ctx, (void**)&h->dmem, bytes, s));
         h->dmem_bytes = bytes;
-        CK(cudaMemsetAsync(h->dmem, 0, bytes, s));
         char* cur2 = h->dmem;
-        // topology staging (pinned) so the uploads are plain DMA
-        std::vector<std::pair<void*, std::pair<const void*, size_t>>> ups;
         h->lv.assign(nlev, LevelDev());
+        // The tables the host built lie contiguous at the start of the block, so their pinned staging image goes up
+        // in one copy; the rest of the block (coefficients, vectors, reduction tickets, flags) is zeroed on the device.
+        struct Tab {
+            uint64_t* m;
+            int *nb, *ch, *par;
+            uint8_t* oc;
+        };
+        std::vector<Tab> tabs(nlev);
+        std::vector<std::pair<void*, std::pair<const void*, size_t>>> ups;
         for (int l = 0; l < nlev; ++l) {
             HostLevel& H = h->host[l];
             LevelDev& D = h->lv[l];
-            size_t n = (size_t)H.nl;
-            D.dt = H.dt;
-            D.dx = H.dx;
-            uint64_t* m = carve<uint64_t>(cur2, n * 8);
-            int* nb = carve<int>(cur2, n * 6);
-            int* ch = carve<int>(cur2, n * 8);
-            int* par = carve<int>(cur2, n);
-            uint8_t* oc = carve<uint8_t>(cur2, n);
+            const size_t n = (size_t)H.nl;
+            Tab& T = tabs[l];
+            T.m = carve<uint64_t>(cur2, n * 8);
+            T.nb = carve<int>(cur2, n * 6);
+            T.ch = carve<int>(cur2, n * 8);
+            T.par = carve<int>(cur2, n);
+            T.oc = carve<uint8_t>(cur2, n);
             D.dof_base = carve<int>(cur2, n);
             D.org = carve<int>(cur2, n * 3);
+            ups.push_back({T.m, {H.mask.data(), n * 64}});
+            ups.push_back({T.nb, {H.nbr.data(), n * 24}});
+            if (!H.child.empty()) ups.push_back({T.ch, {H.child.data(), n * 32}});
+            if (!H.parent.empty()) ups.push_back({T.par, {H.parent.data(), n * 4}});
+            if (!H.octant.empty()) ups.push_back({T.oc, {H.octant.data(), n}});
+            ups.push_back({D.dof_base, {H.dof_base.data(), n * 4}});
+            ups.push_back({D.org, {H.org.data(), n * 12}});
+        }
+        int* dsrc = carve<int>(cur2, src.size());
+        ups.push_back({dsrc, {src.data(), src.size() * 4}});
+        const size_t table_bytes = (size_t)(cur2 - h->dmem);
+        CK(cudaMemsetAsync(cur2, 0, bytes - table_bytes, s));
+        for (int l = 0; l < nlev; ++l) {
+            HostLevel& H = h->host[l];
+            LevelDev& D = h->lv[l];
+            const size_t n = (size_t)H.nl;
+            D.dt = H.dt;
+            D.dx = H.dx;
             D.flags = carve<uint32_t>(cur2, n);
             D.spai0_ready = carve<int>(cur2, 1);
             float* dg = carve<float>(cur2, n * UAAMG_LEAF);
@@ -781,17 +805,11 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             D.rhs = carve<float>(cur2, n * UAAMG_LEAF);
             D.tmp = carve<float>(cur2, n * UAAMG_LEAF);
             carve<float>(cur2, n * UAAMG_LEAF);
-            ups.push_back({m, {H.mask.data(), n * 64}});
-            ups.push_back({nb, {H.nbr.data(), n * 24}});
-            if (!H.child.empty()) ups.push_back({ch, {H.child.data(), n * 32}});
-            if (!H.parent.empty()) ups.push_back({par, {H.parent.data(), n * 4}});
-            if (!H.octant.empty()) ups.push_back({oc, {H.octant.data(), n}});
-            ups.push_back({D.dof_base, {H.dof_base.data(), n * 4}});
-            ups.push_back({D.org, {H.org.data(), n * 12}});
             const float t = H.dt / (H.dx * H.dx);  // LaplacianApplySIMD ctor (.cpp:1045-1065)
             DLevel& L = D.L;
+            const Tab& T = tabs[l];
             L.nl = (int)n;
-            L.mask = m; L.nbr = nb; L.child = ch; L.parent = par; L.octant = oc;
+            L.mask = T.m; L.nbr = T.nb; L.child = T.ch; L.parent = T.par; L.octant = T.oc;
             L.diag = dg; L.cx = cx; L.cy = cy; L.cz = cz; L.invdiag = iv; L.spai0 = D.spai0; L.flags = D.flags;
             L.def_face = -t;
             L.def_diag = 6.f * t;
@@ -815,20 +833,13 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         h->partials = carve<double>(cur2, red_buffer_doubles(std::max<size_t>((size_t)L0.nl, 1)));
         h->st = reinterpret_cast<PcgState*>(carve<char>(cur2, sizeof(PcgState)));
         h->scalar_dev = carve<float>(cur2, 64);
-        int* dsrc = carve<int>(cur2, src.size());
-        ups.push_back({dsrc, {src.data(), src.size() * 4}});
-        // one pinned staging buffer for all tables
-        size_t tot = 0;
-        for (auto& u : ups) tot += (u.second.second + 15) & ~size_t(15);
-        // kept by the handle until destroy, so create() need not wait for the DMA
-        CK(ctx_pinned_acquire(h->ctx, tot + 512, &h->pin_stage, &h->pin_stage_cap));
+        // the table region's image in pinned memory (kept by the handle until destroy, so create() need not wait
+        // for the copy); the arrays not uploaded and the alignment gaps are zero, as the device memset made them
+        CK(ctx_pinned_acquire(h->ctx, table_bytes + 512, &h->pin_stage, &h->pin_stage_cap));
         char* pin = (char*)h->pin_stage;
-        size_t o = 0;
-        for (auto& u : ups) {
-            memcpy(pin + o, u.second.first, u.second.second);
-            CK(cudaMemcpyAsync(u.first, pin + o, u.second.second, cudaMemcpyHostToDevice, s));
-            o += (u.second.second + 15) & ~size_t(15);
-        }
+        memset(pin, 0, table_bytes);
+        for (auto& u : ups) memcpy(pin + ((char*)u.first - h->dmem), u.second.first, u.second.second);
+        CK(cudaMemcpyAsync(h->dmem, pin, table_bytes, cudaMemcpyHostToDevice, s));
         TRACE("alloc + table upload");
         // ---- numeric construction on the device
         if (L0.nl > 0) {
