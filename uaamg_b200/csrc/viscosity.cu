@@ -35,7 +35,8 @@ static void sort_unique_vdb(std::vector<int32_t>& org) {
     const size_t n = org.size() / 3;
     std::vector<std::pair<unsigned __int128, uint32_t>> keys(n);
     for (size_t i = 0; i < n; ++i) keys[i] = {vdb_key128(&org[3 * i]), (uint32_t)i};
-    std::sort(keys.begin(), keys.end());
+    // a dense scan of a bounding box inside one 128^3 node is in tree order already
+    if (!std::is_sorted(keys.begin(), keys.end())) std::sort(keys.begin(), keys.end());
     std::vector<int32_t> out;
     out.reserve(org.size());
     for (size_t i = 0; i < n; ++i) {
