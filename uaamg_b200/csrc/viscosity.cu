@@ -597,10 +597,11 @@ struct VEnq {
         pe();
         count++;
     }
-    // residual of level l restricted into the rhs of level l + 1 (fused)
-    void residual_restrict(int l, const float* x, const float* b, float* coarse) {
+    // residual of level l restricted into the rhs of level l + 1 (fused); coarse_lhs (optional) is zeroed
+    void residual_restrict(int l, const float* x, const float* b, float* coarse, float* coarse_lhs) {
         if (prof) pb("L" + std::to_string(l) + " residual+restrict");
-        launch2(k_vresrestrict, dim3((unsigned)h->lv[l].L.nl, 3), 128, s, h->lv[l].L, h->lv[l + 1].L, x, b, coarse);
+        launch2(k_vresrestrict, dim3((unsigned)h->lv[l].L.nl, 3), 128, s, h->lv[l].L, h->lv[l + 1].L, x, b, coarse,
+                coarse_lhs);
         pe();
         count++;
     }
@@ -622,25 +623,31 @@ struct VEnq {
         count++;
     }
     void zero(int l, float* v) {
-        CK(cudaMemsetAsync(v, 0, (size_t)3 * h->lv[l].L.nl * UAAMG_LEAF * 4, s));
+        const long long n4 = (long long)3 * h->lv[l].L.nl * (UAAMG_LEAF / 4);
+        if (n4 == 0) return;
+        const long long g = std::min<long long>((n4 + 255) / 256, (long long)g_sms * 8);
+        launch2(k_vzero, dim3((unsigned)g), 256, s, reinterpret_cast<float4*>(v), n4);
+        count++;
     }
 };
 
 // simd_viscosity3d::mucycle (:3837-3884) with mu = 2, n = 2.  The second
 // visit of the coarsest level solves the same rhs from the same zero guess as
 // the first, so it is not repeated.
-static void enqueue_mucycle(VEnq& E, int l, float* lhs, const float* rhs, bool for_precon) {
+// lhs_zeroed: the restriction before this visit already zeroed lhs.
+static void enqueue_mucycle(VEnq& E, int l, float* lhs, const float* rhs, bool for_precon, bool lhs_zeroed = false) {
     uaamg_viscosity* h = E.h;
     if (l == h->nlev - 1) {
         E.coarsest(rhs, lhs);
         return;
     }
-    if (for_precon) E.zero(l, lhs);
+    if (for_precon && !lhs_zeroed) E.zero(l, lhs);
     for (int i = 0; i < 2; ++i) E.rbgs(l, true, lhs, rhs);
     VLevelDev& D = h->lv[l];
     VLevelDev& P = h->lv[l + 1];
-    E.residual_restrict(l, lhs, rhs, P.rhs);
-    enqueue_mucycle(E, l + 1, P.lhs, P.rhs, true);
+    const bool coarse_visit = l + 1 != h->nlev - 1;  // the coarsest solve writes its own result
+    E.residual_restrict(l, lhs, rhs, P.rhs, coarse_visit ? P.lhs : nullptr);
+    enqueue_mucycle(E, l + 1, P.lhs, P.rhs, true, coarse_visit);
     if (l + 1 != h->nlev - 1) enqueue_mucycle(E, l + 1, P.lhs, P.rhs, false);
     E.prolong(l, P.lhs, lhs);
     for (int i = 0; i < 2; ++i) E.rbgs(l, false, lhs, rhs);

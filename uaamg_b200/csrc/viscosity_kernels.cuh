@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(128) k_vrestrict(VLevel F, VLevel C, const flo
 // coarse rhs is zero there from allocation).
 template <int c>
 __device__ __forceinline__ void vresrestrict_leaf(const VLevel& F, const VLevel& C, VNbSh& sh, float* rs, int leaf,
-                                                  const float* x, const float* b, float* coarse) {
+                                                  const float* x, const float* b, float* coarse, float* coarse_lhs) {
     const int t = threadIdx.x;
     const unsigned m = vmask4(F, c, leaf, t);
     vnb_prologue(F, leaf, sh);
@@ -507,16 +507,28 @@ __device__ __forceinline__ void vresrestrict_leaf(const VLevel& F, const VLevel&
             s = __fmul_rn(__fmul_rn(__fmul_rn(s, 0.125f), 0.5f), 2.0f);
         }
         coarse[((long long)c * C.nl + P) * UAAMG_LEAF + voff3(cx, cy, cz)] = s;
+        // the coarse visit that follows starts from zero: every coarse DOF of channel c lies in an octant whose
+        // fine leaf has a DOF of c, so these writes cover them (the memset they replace was a graph node of its own)
+        if (coarse_lhs) coarse_lhs[((long long)c * C.nl + P) * UAAMG_LEAF + voff3(cx, cy, cz)] = 0.f;
     }
 }
 __global__ void __launch_bounds__(128, VAPPLY_MINB) k_vresrestrict(VLevel F, VLevel C, const float* x, const float* b,
-                                                                   float* coarse) {
+                                                                   float* coarse, float* coarse_lhs) {
     __shared__ VNbSh sh;
     __shared__ __align__(16) float rs[UAAMG_LEAF];
     const int leaf = blockIdx.x;
-    if (blockIdx.y == 0) vresrestrict_leaf<0>(F, C, sh, rs, leaf, x, b, coarse);
-    else if (blockIdx.y == 1) vresrestrict_leaf<1>(F, C, sh, rs, leaf, x, b, coarse);
-    else vresrestrict_leaf<2>(F, C, sh, rs, leaf, x, b, coarse);
+    if (blockIdx.y == 0) vresrestrict_leaf<0>(F, C, sh, rs, leaf, x, b, coarse, coarse_lhs);
+    else if (blockIdx.y == 1) vresrestrict_leaf<1>(F, C, sh, rs, leaf, x, b, coarse, coarse_lhs);
+    else vresrestrict_leaf<2>(F, C, sh, rs, leaf, x, b, coarse, coarse_lhs);
+}
+
+// v = 0 over n floats (grid-stride, float4), a kernel so that it keeps the
+// chain of programmatic dependent launches
+__global__ void __launch_bounds__(256) k_vzero(float4* v, long long n4) {
+    griddep_wait();
+    griddep_launch();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x)
+        v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // prolongation<true> (:2659-2729) for one (fine leaf, channel): fine += coarse parent
