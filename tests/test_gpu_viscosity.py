@@ -144,6 +144,29 @@ def test_rbgs_sweeps_bit_exact(scene32):
             assert np.array_equal(lv.rbgs(l, x, b, order), ref.rbgs(l, x, b, order)), (l, order)
 
 
+@pytest.mark.parametrize("n,seed", [(32, 1), (48, 3)])
+def test_fused_rbgs_steps_identical(gpu, monkeypatch, n, seed):
+    """The fused red-black step (one launch per channel, first-colour halo
+    recomputed per leaf) gives the bits of the separate red and black passes:
+    the preconditioner and a whole solve, with every level fused and none."""
+    from uaamg_b200.viscosity import L_with_level, simd_viscosity3d
+    sc = scenes.plain_viscosity_scene(n=n, seed=seed)
+    out = []
+    for leaves in ("0", str(2**31 - 1)):
+        monkeypatch.setenv("UAAMG_VISC_FUSED_RB_LEAVES", leaves)
+        lv = L_with_level.create_viscosity_matrix(sc.viscosity, sc.liquid_phi, sc.solid_phi, sc.dt, sc.rho, sc.dx)
+        rhs = lv.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+        x = lv.gather_velocity(sc.u, sc.v, sc.w)
+        s = simd_viscosity3d(lv)
+        z = s.precondition(rhs)
+        st = s.pcg_solve(x, 1e-6, rhs)
+        out.append((z, st, s.m_iteration, x))
+    (z0, st0, it0, x0), (z1, st1, it1, x1) = out
+    assert np.array_equal(z0, z1)
+    assert st0 == st1 == 0 and it0 == it1
+    assert np.array_equal(x0, x1)
+
+
 def test_restriction_prolongation_bit_exact(scene32):
     sc, lv, ref = scene32
     for l in range(ref.num_levels - 1):

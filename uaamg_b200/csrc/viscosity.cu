@@ -12,6 +12,8 @@
 //    scalars, optionally one CUDA graph with a conditional WHILE node).
 // Compiled into the same translation unit as poisson.cu (uaamg_lib.cu) and
 // shares its error handling, resource pools and launch helpers.
+#include <climits>
+
 #include "viscosity_build.cuh"
 
 namespace {
@@ -219,7 +221,7 @@ struct VLevelDev {
     VLevel L{};
     float* lhs = nullptr;
     float* rhs = nullptr;
-    float* tmp = nullptr;
+    float* alt = nullptr;  // second buffer of the fused red-black steps (zero at non-DOF voxel groups), when used
     int* dof_base = nullptr;
     int* org = nullptr;
 };
@@ -236,6 +238,11 @@ struct uaamg_viscosity {
     std::vector<VHostLevel> host;
     std::vector<VLevelDev> lv;
     int nlev = 0;
+    // levels of at most this many leaves smooth with the fused red-black step
+    // (k_vrbgs): latency-bound levels of about one wave at 2 CTAs per SM; larger
+    // levels are issue-bound and the step's face-layer recomputation costs more
+    // than the launch it saves
+    int rb_fused_max_leaves = 0;
     std::vector<void*> allocs;
     // level-0 construction products kept for the right-hand side
     VolFields V{};
@@ -336,6 +343,10 @@ static void upload_vlevel(uaamg_viscosity* h, const VHostLevel& H, VLevelDev& D,
     D.lhs = (float*)valloc(h, vb);
     D.rhs = (float*)valloc(h, vb);
     CK(cudaMemsetAsync(D.lhs, 0, vb, h->stream));
+    if (H.nl <= h->rb_fused_max_leaves) {
+        D.alt = (float*)valloc(h, vb);
+        CK(cudaMemsetAsync(D.alt, 0, vb, h->stream));
+    }
     CK(cudaMemsetAsync(D.rhs, 0, vb, h->stream));  // restriction leaves voxels without fine leaves untouched
     D.L.coef = (float*)valloc(h, (size_t)27 * H.nl * UAAMG_LEAF * sizeof(float));
     D.L.zpage = h->zpage;
@@ -578,6 +589,45 @@ struct VEnq {
         pe();
         count++;
     }
+    // Two red-black sweeps (XYZ or ZYX order) of level l on x in place.  A level
+    // the fused step covers runs one k_vrbgs per channel and sweep, alternating
+    // between x and the level's second buffer; each channel moves twice, so the
+    // result is back in x.
+    void rbgs2(int l, bool xyz, float* x, const float* b) {
+        const VLevelDev& D = h->lv[l];
+        if (!D.alt) {
+            rbgs(l, xyz, x, b);
+            rbgs(l, xyz, x, b);
+            return;
+        }
+        const size_t cs = (size_t)D.L.nl * UAAMG_LEAF;
+        float* buf[2] = {x, D.alt};
+        int where[3] = {0, 0, 0};
+        for (int i = 0; i < 2; ++i)
+            for (int s3 = 0; s3 < 3; ++s3) {
+                const int c = xyz ? s3 : 2 - s3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+                VRbIo io;
+                io.xc = buf[where[c]] + c * cs;
+                io.x1 = buf[where[c1]] + c1 * cs;
+                io.x2 = buf[where[c2]] + c2 * cs;
+                io.b = b + c * cs;
+                io.out = buf[where[c] ^ 1] + c * cs;
+                if (prof) pb("L" + std::to_string(l) + " rbgs step c" + std::to_string(c));
+                const dim3 g((unsigned)D.L.nl);
+                if (xyz) {
+                    if (c == 0) launch2(k_vrbgs<0, 0>, g, VRB_THREADS, s, D.L, io, 1.0f);
+                    else if (c == 1) launch2(k_vrbgs<1, 0>, g, VRB_THREADS, s, D.L, io, 1.0f);
+                    else launch2(k_vrbgs<2, 0>, g, VRB_THREADS, s, D.L, io, 1.0f);
+                } else {
+                    if (c == 0) launch2(k_vrbgs<0, 1>, g, VRB_THREADS, s, D.L, io, 1.0f);
+                    else if (c == 1) launch2(k_vrbgs<1, 1>, g, VRB_THREADS, s, D.L, io, 1.0f);
+                    else launch2(k_vrbgs<2, 1>, g, VRB_THREADS, s, D.L, io, 1.0f);
+                }
+                pe();
+                count++;
+                where[c] ^= 1;
+            }
+    }
     void rbgs(int l, bool xyz, float* x, const float* b) {
         if (xyz) {
             for (int c = 0; c < 3; ++c) {
@@ -642,7 +692,7 @@ static void enqueue_mucycle(VEnq& E, int l, float* lhs, const float* rhs, bool f
         return;
     }
     if (for_precon && !lhs_zeroed) E.zero(l, lhs);
-    for (int i = 0; i < 2; ++i) E.rbgs(l, true, lhs, rhs);
+    E.rbgs2(l, true, lhs, rhs);
     VLevelDev& D = h->lv[l];
     VLevelDev& P = h->lv[l + 1];
     const bool coarse_visit = l + 1 != h->nlev - 1;  // the coarsest solve writes its own result
@@ -650,7 +700,7 @@ static void enqueue_mucycle(VEnq& E, int l, float* lhs, const float* rhs, bool f
     enqueue_mucycle(E, l + 1, P.lhs, P.rhs, true, coarse_visit);
     if (l + 1 != h->nlev - 1) enqueue_mucycle(E, l + 1, P.lhs, P.rhs, false);
     E.prolong(l, P.lhs, lhs);
-    for (int i = 0; i < 2; ++i) E.rbgs(l, false, lhs, rhs);
+    E.rbgs2(l, false, lhs, rhs);
 }
 
 static void venqueue_setup(VEnq& E, cudaGraphConditionalHandle cond, int use_cond) {
@@ -918,6 +968,13 @@ int uaamg_viscosity_create_on_stream(const uaamg_leaf_grid* viscosity, const uaa
         CK(ctx_pinned_acquire(h->ctx, sizeof(PcgState) + 256, &h->pin_state, &h->pin_state_cap));
         h->st_host = reinterpret_cast<PcgState*>(h->pin_state);
         h->scalar_host = reinterpret_cast<float*>((char*)h->pin_state + ((sizeof(PcgState) + 63) & ~size_t(63)));
+        {
+            int sms = 0;
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->ctx->device) == cudaSuccess && sms > 0)
+                g_sms = sms;
+        }
+        h->rb_fused_max_leaves = 2 * g_sms;
+        if (const char* e = getenv("UAAMG_VISC_FUSED_RB_LEAVES")) h->rb_fused_max_leaves = atoi(e);
         build_viscosity(h, viscosity, liquid_sdf, solid_sdf, dt, rho, dx);
     } catch (const UaamgError& e) {
         uaamg_viscosity_destroy(h);

@@ -189,6 +189,31 @@ struct VCoef {
     float4 b00, b01, b10, b11;              // m_cross_channel[d1]
     float4 dg;                              // 1/diag (GS, Jacobi) or diag (normal, residual)
 };
+// at the 4-voxel group (X, Y, Z0..Z0+3) relative to the CTA's leaf, X and Y in
+// -1..8, Z0 in {0, 4}; inv: 1/diag instead of diag
+template <int c>
+__device__ __forceinline__ void vload_coef_at(const VLevel& L, const VNbSh& sh, int X, int Y, int Z0, bool inv,
+                                              VCoef& k) {
+    constexpr int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    int e0[3] = {0, 0, 0};
+    e0[d0] = 1;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int px = ax == 0, py = ax == 1, pz = ax == 2;
+        const VArr W = varr(L, c, VA_NEGX + ax);
+        k.wp[ax] = cload4(W, sh, X, Y, Z0, px, py, pz);
+        k.wm[ax] = cload4(W, sh, X, Y, Z0, 0, 0, 0);
+    }
+    k.a00 = cload4(varr(L, d2, VA_T00), sh, X, Y, Z0, 0, 0, 0);
+    k.a01 = cload4(varr(L, d2, VA_T01), sh, X, Y, Z0, 0, 0, 0);
+    k.a10 = cload4(varr(L, d2, VA_T10), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    k.a11 = cload4(varr(L, d2, VA_T11), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    k.b00 = cload4(varr(L, d1, VA_T00), sh, X, Y, Z0, 0, 0, 0);
+    k.b01 = cload4(varr(L, d1, VA_T01), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    k.b10 = cload4(varr(L, d1, VA_T10), sh, X, Y, Z0, 0, 0, 0);
+    k.b11 = cload4(varr(L, d1, VA_T11), sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    k.dg = cload4(varr(L, c, inv ? VA_INV : VA_DIAG), sh, X, Y, Z0, 0, 0, 0);
+}
 template <int MODE, int c>
 __device__ __forceinline__ void vload_coef(const VLevel& L, const VNbSh& sh, int t, VCoef& k) {
     constexpr int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
@@ -405,6 +430,283 @@ __global__ void __launch_bounds__(128, VAPPLY_MINB) k_vapply(VLevel L, const flo
         else if (blockIdx.y == 1) vapply_leaf<MODE, 1>(L, sh, leaf, x, b, out, w);
         else vapply_leaf<MODE, 2>(L, sh, leaf, x, b, out, w);
     }
+}
+
+// ---------------------------------------------------------------------------
+// One red-black Gauss-Seidel step of one channel in one launch: the first
+// colour's update followed by the second's (XYZ_RBGS_apply runs red then black
+// per channel, ZYX_RBGS_apply black then red; simd_viscosity3d.cpp:2238-2302).
+//
+// The first-colour update at a voxel reads only second-colour values of its
+// own channel and the other two channels, none of which that update changes,
+// so a CTA can compute it for its own leaf and for the first-colour voxels of
+// the six face layers around it (the ones its second-colour voxels read),
+// which the neighbouring CTAs compute as well from the same inputs in the same
+// order: bit-identical values, no exchange between CTAs.  The second colour
+// then reads its same-channel neighbours from shared memory; its cross-channel
+// sums are the first colour's, kept in registers.  The step reads channel c
+// from one buffer and writes it to another (neighbouring CTAs still read the
+// old values), so a pair of steps over the three channels ends where it began.
+//
+// Threads: 0-127 the leaf's 4-voxel groups (as k_vapply); 128-191 the groups
+// of the -x, +x, -y, +y face layers (x or y = -1 or 8, z0 = 0 or 4); 192-255
+// the first-colour voxels of the -z and +z layers, one each.
+struct VRbIo {
+    const float* xc;  // channel c before the step
+    const float* x1;  // channel (c + 1) % 3
+    const float* x2;  // channel (c + 2) % 3
+    const float* b;   // channel c of the right-hand side
+    float* out;       // channel c after the step
+};
+#define VRB_THREADS 256
+#ifndef VRB_MINB
+#define VRB_MINB 2
+#endif
+#define VRB_HALO 10  // shared-memory cube: the leaf and one voxel around it
+__device__ __forceinline__ int vrb_idx(int X, int Y, int Z) {
+    return ((X + 1) * VRB_HALO + (Y + 1)) * VRB_HALO + (Z + 1);
+}
+
+// faced_result[1] of one voxel from its seven products and two cross sums,
+// in the order of voffdiag
+__device__ __forceinline__ float vsum_off(float p0, float p1, float p2, float p3, float p4, float p5, float td2,
+                                          float td1) {
+    float f1 = __fadd_rn(p0, p1);
+    const float f3 = __fadd_rn(p2, p3);
+    const float f5 = __fadd_rn(p4, p5);
+    f1 = __fadd_rn(f1, f3);
+    f1 = __fadd_rn(f1, f5);
+    f1 = __fadd_rn(f1, td2);
+    return __fadd_rn(f1, td1);
+}
+// Gauss-Seidel update of vapply_value_k
+__device__ __forceinline__ float vgs_update(float bb, float off, float iv, float w, float one_minus_w, float xc) {
+    float r = __fsub_rn(bb, off);
+    r = __fmul_rn(r, iv);
+    r = __fmul_rn(r, w);
+    return __fmaf_rn(xc, one_minus_w, r);
+}
+__device__ __forceinline__ float vload1(const float* arr, const float* fb, const VNbSh& sh, int X, int Y, int Z) {
+    return vsel(arr, fb, sh, vnb_index(X, Y, Z))[voff3(X, Y, Z)];
+}
+
+// Cross-channel sums (td2, td1 of voffdiag) at a 4-voxel group.
+template <int c>
+__device__ __forceinline__ void vcross4(const VLevel& L, const VNbSh& sh, const VRbIo& io, int X, int Y, int Z0,
+                                        const VCoef& k, float4& td2, float4& td1) {
+    constexpr int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    int e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0};
+    e0[d0] = 1;
+    e1[d1] = 1;
+    e2[d2] = 1;
+    const float* zp = L.zpage;
+    const float4 u1_g = vload4(io.x1, zp, sh, X, Y, Z0, 0, 0, 0);
+    const float4 u1_p1 = vload4(io.x1, zp, sh, X, Y, Z0, e1[0], e1[1], e1[2]);
+    const float4 u1_m0 = vload4(io.x1, zp, sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 u1_m0p1 = vload4(io.x1, zp, sh, X, Y, Z0, e1[0] - e0[0], e1[1] - e0[1], e1[2] - e0[2]);
+    const float4 u2_g = vload4(io.x2, zp, sh, X, Y, Z0, 0, 0, 0);
+    const float4 u2_m0 = vload4(io.x2, zp, sh, X, Y, Z0, -e0[0], -e0[1], -e0[2]);
+    const float4 u2_p2 = vload4(io.x2, zp, sh, X, Y, Z0, e2[0], e2[1], e2[2]);
+    const float4 u2_m0p2 = vload4(io.x2, zp, sh, X, Y, Z0, e2[0] - e0[0], e2[1] - e0[1], e2[2] - e0[2]);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float R0 = __fmul_rn(f4get(u1_g, j), f4get(k.a00, j));
+        const float R1 = __fmul_rn(f4get(k.a01, j), f4get(u1_p1, j));
+        const float R2 = __fmul_rn(f4get(k.a10, j), f4get(u1_m0, j));
+        const float R3 = __fmul_rn(f4get(k.a11, j), f4get(u1_m0p1, j));
+        const float Q0 = __fmul_rn(f4get(k.b00, j), f4get(u2_g, j));
+        const float Q1 = __fmul_rn(f4get(k.b01, j), f4get(u2_m0, j));
+        const float Q2 = __fmul_rn(f4get(k.b10, j), f4get(u2_p2, j));
+        const float Q3 = __fmul_rn(f4get(k.b11, j), f4get(u2_m0p2, j));
+        f4set(td2, j, __fadd_rn(__fadd_rn(R0, R1), __fadd_rn(R2, R3)));
+        f4set(td1, j, __fadd_rn(__fadd_rn(Q0, Q1), __fadd_rn(Q2, Q3)));
+    }
+}
+
+// First-colour update of a 4-voxel group (lanes of the other colour keep xc);
+// m = DOF bits of the group, non-DOF lanes 0.
+template <int c, int FP>
+__device__ __forceinline__ float4 vrb_first4(const VLevel& L, const VNbSh& sh, const VRbIo& io, int X, int Y,
+                                             int Z0, unsigned m, float w, const VCoef& k, float4& td2, float4& td1,
+                                             float4& bb) {
+    const float* zp = L.zpage;
+    const float4 xc = vload4(io.xc, zp, sh, X, Y, Z0, 0, 0, 0);
+    float4 fr[6];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int px = ax == 0, py = ax == 1, pz = ax == 2;
+        const float4 up = vload4(io.xc, zp, sh, X, Y, Z0, px, py, pz);
+        const float4 um = vload4(io.xc, zp, sh, X, Y, Z0, -px, -py, -pz);
+        fr[2 * ax] = make_float4(__fmul_rn(up.x, k.wp[ax].x), __fmul_rn(up.y, k.wp[ax].y),
+                                 __fmul_rn(up.z, k.wp[ax].z), __fmul_rn(up.w, k.wp[ax].w));
+        fr[2 * ax + 1] = make_float4(__fmul_rn(um.x, k.wm[ax].x), __fmul_rn(um.y, k.wm[ax].y),
+                                     __fmul_rn(um.z, k.wm[ax].z), __fmul_rn(um.w, k.wm[ax].w));
+    }
+    vcross4<c>(L, sh, io, X, Y, Z0, k, td2, td1);
+    bb = vload4(io.b, zp, sh, X, Y, Z0, 0, 0, 0);
+    const float one_minus_w = __fsub_rn(1.0f, w);
+    float4 res;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float off = vsum_off(f4get(fr[0], j), f4get(fr[1], j), f4get(fr[2], j), f4get(fr[3], j),
+                                   f4get(fr[4], j), f4get(fr[5], j), f4get(td2, j), f4get(td1, j));
+        const bool upd = ((X + Y + Z0 + j) & 1) == FP;
+        const float v = vgs_update(f4get(bb, j), off, f4get(k.dg, j), w, one_minus_w, f4get(xc, j));
+        f4set(res, j, (m >> j & 1) ? (upd ? v : f4get(xc, j)) : 0.f);
+    }
+    return res;
+}
+
+// The coefficients of one voxel (VCoef's fifteen values).
+struct VCoef1 {
+    float wp[3], wm[3], a00, a01, a10, a11, b00, b01, b10, b11, iv;
+};
+template <int c>
+__device__ __forceinline__ void vload_coef1(const VLevel& L, const VNbSh& sh, int X, int Y, int Z, VCoef1& k) {
+    constexpr int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    int e0[3] = {0, 0, 0};
+    e0[d0] = 1;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int px = ax == 0, py = ax == 1, pz = ax == 2;
+        const VArr W = varr(L, c, VA_NEGX + ax);
+        k.wp[ax] = vload1(W.a, W.def, sh, X + px, Y + py, Z + pz);
+        k.wm[ax] = vload1(W.a, W.def, sh, X, Y, Z);
+    }
+    const VArr A00 = varr(L, d2, VA_T00), A01 = varr(L, d2, VA_T01), A10 = varr(L, d2, VA_T10),
+               A11 = varr(L, d2, VA_T11), B00 = varr(L, d1, VA_T00), B01 = varr(L, d1, VA_T01),
+               B10 = varr(L, d1, VA_T10), B11 = varr(L, d1, VA_T11), IV = varr(L, c, VA_INV);
+    const int Xm = X - e0[0], Ym = Y - e0[1], Zm = Z - e0[2];
+    k.a00 = vload1(A00.a, A00.def, sh, X, Y, Z);
+    k.a01 = vload1(A01.a, A01.def, sh, X, Y, Z);
+    k.a10 = vload1(A10.a, A10.def, sh, Xm, Ym, Zm);
+    k.a11 = vload1(A11.a, A11.def, sh, Xm, Ym, Zm);
+    k.b00 = vload1(B00.a, B00.def, sh, X, Y, Z);
+    k.b01 = vload1(B01.a, B01.def, sh, Xm, Ym, Zm);
+    k.b10 = vload1(B10.a, B10.def, sh, X, Y, Z);
+    k.b11 = vload1(B11.a, B11.def, sh, Xm, Ym, Zm);
+    k.iv = vload1(IV.a, IV.def, sh, X, Y, Z);
+}
+// First-colour update of one DOF voxel (X, Y, Z), one of them -1 or 8.
+template <int c>
+__device__ __forceinline__ float vrb_first1(const VLevel& L, const VNbSh& sh, const VRbIo& io, int X, int Y, int Z,
+                                            float w, const VCoef1& k) {
+    constexpr int d0 = c, d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    int e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0};
+    e0[d0] = 1;
+    e1[d1] = 1;
+    e2[d2] = 1;
+    const float* zp = L.zpage;
+    const float xc = vload1(io.xc, zp, sh, X, Y, Z);
+    float fr[6];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int px = ax == 0, py = ax == 1, pz = ax == 2;
+        fr[2 * ax] = __fmul_rn(vload1(io.xc, zp, sh, X + px, Y + py, Z + pz), k.wp[ax]);
+        fr[2 * ax + 1] = __fmul_rn(vload1(io.xc, zp, sh, X - px, Y - py, Z - pz), k.wm[ax]);
+    }
+    const int Xm = X - e0[0], Ym = Y - e0[1], Zm = Z - e0[2];
+    const float u1_g = vload1(io.x1, zp, sh, X, Y, Z);
+    const float u1_p1 = vload1(io.x1, zp, sh, X + e1[0], Y + e1[1], Z + e1[2]);
+    const float u1_m0 = vload1(io.x1, zp, sh, Xm, Ym, Zm);
+    const float u1_m0p1 = vload1(io.x1, zp, sh, Xm + e1[0], Ym + e1[1], Zm + e1[2]);
+    const float u2_g = vload1(io.x2, zp, sh, X, Y, Z);
+    const float u2_m0 = vload1(io.x2, zp, sh, Xm, Ym, Zm);
+    const float u2_p2 = vload1(io.x2, zp, sh, X + e2[0], Y + e2[1], Z + e2[2]);
+    const float u2_m0p2 = vload1(io.x2, zp, sh, Xm + e2[0], Ym + e2[1], Zm + e2[2]);
+    const float bb = vload1(io.b, zp, sh, X, Y, Z);
+    const float R0 = __fmul_rn(u1_g, k.a00);
+    const float R1 = __fmul_rn(k.a01, u1_p1);
+    const float R2 = __fmul_rn(k.a10, u1_m0);
+    const float R3 = __fmul_rn(k.a11, u1_m0p1);
+    const float Q0 = __fmul_rn(k.b00, u2_g);
+    const float Q1 = __fmul_rn(k.b01, u2_m0);
+    const float Q2 = __fmul_rn(k.b10, u2_p2);
+    const float Q3 = __fmul_rn(k.b11, u2_m0p2);
+    const float td2 = __fadd_rn(__fadd_rn(R0, R1), __fadd_rn(R2, R3));
+    const float td1 = __fadd_rn(__fadd_rn(Q0, Q1), __fadd_rn(Q2, Q3));
+    const float off = vsum_off(fr[0], fr[1], fr[2], fr[3], fr[4], fr[5], td2, td1);
+    return vgs_update(bb, off, k.iv, w, __fsub_rn(1.0f, w), xc);
+}
+
+// FP: parity of the first colour (0 red first, XYZ order; 1 black first, ZYX).
+// grid (nl), VRB_THREADS threads.
+template <int c, int FP>
+__global__ void __launch_bounds__(VRB_THREADS, VRB_MINB) k_vrbgs(VLevel L, VRbIo io, float w) {
+    __shared__ VNbSh sh;
+    __shared__ float cur[VRB_HALO * VRB_HALO * VRB_HALO];
+    const int t = threadIdx.x;
+    const int leaf = blockIdx.x;
+    vnb_prologue(L, leaf, sh);
+    // static data before the wait: group / voxel coordinates, DOF bits, coefficients
+    int X, Y, Z0;
+    unsigned m = 0;
+    VCoef k;
+    VCoef1 k1;
+    if (t < 128) {
+        X = t >> 4;
+        Y = (t >> 1) & 7;
+        Z0 = (t & 1) * 4;
+        m = vmask4(L, c, leaf, t);
+        if (m) vload_coef_at<c>(L, sh, X, Y, Z0, true, k);
+    } else if (t < 192) {
+        const int h = t - 128, face = h >> 4, u = (h >> 1) & 7;
+        Z0 = (h & 1) * 4;
+        if (face < 2) {
+            X = face ? 8 : -1;
+            Y = u;
+        } else {
+            X = u;
+            Y = face == 3 ? 8 : -1;
+        }
+        const int lf = sh.nb[vnb_index(X, Y, Z0)];
+        if (lf >= 0) {
+            const int tg = ((X & 7) << 4) | ((Y & 7) << 1) | (Z0 >> 2);
+            m = vmask4(L, c, lf, tg);
+        }
+        if (m) vload_coef_at<c>(L, sh, X, Y, Z0, true, k);
+    } else {
+        const int h = t - 192, i = h & 31;
+        Z0 = (h >> 5) ? 8 : -1;  // the voxel's z
+        X = i >> 2;
+        Y = 2 * (i & 3) + ((FP + Z0 + X) & 1);
+        const int lf = sh.nb[vnb_index(X, Y, Z0)];
+        if (lf >= 0 && vdof_bit(L, c, lf, voff3(X, Y, Z0))) m = 1;
+        if (m) vload_coef1<c>(L, sh, X, Y, Z0, k1);
+    }
+    griddep_wait();
+    griddep_launch();
+    // first colour: every first-colour position of the cube is written (0 where
+    // there is no DOF), the only positions the second colour reads
+    float4 td2, td1, bb, res = f4zero();
+    if (t < 192) {
+        if (m) res = vrb_first4<c, FP>(L, sh, io, X, Y, Z0, m, w, k, td2, td1, bb);
+        const int base = vrb_idx(X, Y, Z0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (((X + Y + Z0 + j) & 1) == FP) cur[base + j] = f4get(res, j);
+    } else {
+        cur[vrb_idx(X, Y, Z0)] = m ? vrb_first1<c>(L, sh, io, X, Y, Z0, w, k1) : 0.f;
+    }
+    __syncthreads();
+    if (t >= 128 || !m) return;
+    // second colour: same-channel neighbours (all first colour) from shared memory
+    const float one_minus_w = __fsub_rn(1.0f, w);
+    float4 out = res;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int Z = Z0 + j;
+        if (((X + Y + Z) & 1) == FP || !(m >> j & 1)) continue;
+        const float p0 = __fmul_rn(cur[vrb_idx(X + 1, Y, Z)], f4get(k.wp[0], j));
+        const float p1 = __fmul_rn(cur[vrb_idx(X - 1, Y, Z)], f4get(k.wm[0], j));
+        const float p2 = __fmul_rn(cur[vrb_idx(X, Y + 1, Z)], f4get(k.wp[1], j));
+        const float p3 = __fmul_rn(cur[vrb_idx(X, Y - 1, Z)], f4get(k.wm[1], j));
+        const float p4 = __fmul_rn(cur[vrb_idx(X, Y, Z + 1)], f4get(k.wp[2], j));
+        const float p5 = __fmul_rn(cur[vrb_idx(X, Y, Z - 1)], f4get(k.wm[2], j));
+        const float off = vsum_off(p0, p1, p2, p3, p4, p5, f4get(td2, j), f4get(td1, j));
+        f4set(out, j, vgs_update(f4get(bb, j), off, f4get(k.dg, j), w, one_minus_w, f4get(res, j)));
+    }
+    reinterpret_cast<float4*>(io.out)[(long long)leaf * UAAMG_LEAF4 + t] = out;
 }
 
 // restriction (:2353-2413) for one (coarse leaf, channel): coarse = (sum of the
