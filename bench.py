@@ -302,6 +302,9 @@ def _visc_pass_bytes(label: str, ndof_level: list[int], ndof_c: list[list[int]])
     if len(parts) >= 3 and parts[1] in ("red_gs", "black_gs"):
         c = int(parts[2][1:])
         return 22.0 * ndof_c[lv][c]
+    if len(parts) >= 4 and parts[1] == "rbgs" and parts[2] == "step":  # fused red+black: one pass's bytes
+        c = int(parts[3][1:])
+        return 22.0 * ndof_c[lv][c]
     if parts[1] == "residual":
         return 44.0 * ndof_level[lv]
     if parts[1] == "normal":
@@ -464,7 +467,7 @@ def run_viscosity(args, dev, stream, timed, max_over_ranks, ws, rank, vsc, vdg, 
     # The dominant kernel is k_vapply in its red/black GS modes (all levels);
     # the roofline is quoted on the level-0 red pass of channel 0 (the launch
     # the committed ncu capture measures), the all-level aggregate beside it.
-    gs = [(k, v) for k, v in prof.items() if " red_gs " in k or " black_gs " in k]
+    gs = [(k, v) for k, v in prof.items() if " red_gs " in k or " black_gs " in k or " rbgs step " in k]
     gs_bytes = sum(_visc_pass_bytes(k, ndof, ndof_c) * v[1] for k, v in gs)
     gs_ms = sum(v[0] for k, v in gs)
     prof_ms = sum(v[0] for v in prof.values())

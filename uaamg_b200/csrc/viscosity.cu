@@ -511,6 +511,10 @@ static void build_viscosity(uaamg_viscosity* h, const uaamg_leaf_grid* mu_g, con
         if (D.L.nl) {
             launch2(k_vtrim, dim3((unsigned)D.L.nl), 128, s, D.L, trim);
             launch2(k_vtrim_fill, dim3((unsigned)D.L.nl), 128, s, D.L, (const uint32_t*)trim, (float*)D.L.coef);
+            int* cnb = (int*)valloc(h, (size_t)D.L.nl * 27 * sizeof(int));
+            launch2(k_vcnb, dim3((unsigned)(((long long)D.L.nl * 27 + 127) / 128)), 128, s, D.L,
+                    (const uint32_t*)trim, cnb);
+            D.L.cnb = cnb;
         }
         D.L.trim = trim;
     }

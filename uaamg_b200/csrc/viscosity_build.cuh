@@ -629,6 +629,18 @@ __global__ void __launch_bounds__(128) k_vtrim_fill(VLevel L, const uint32_t* tr
     }
 }
 
+// Coefficient neighbour table of a trimmed level: slot k of leaf i is -1 where
+// nb is -1 or names a leaf whose 27 arrays are all trimmed (its blocks hold the
+// defaults that the default page holds), else nb.  grid ceil(nl*27 / 128).
+__global__ void __launch_bounds__(128) k_vcnb(VLevel L, const uint32_t* trim, int* cnb) {
+    griddep_wait();
+    griddep_launch();
+    const long long i = (long long)blockIdx.x * 128 + threadIdx.x;
+    if (i >= (long long)L.nl * 27) return;
+    const int lf = L.nb[i];
+    cnb[i] = (lf >= 0 && trim[lf] == (1u << (3 * VNA)) - 1u) ? -1 : lf;
+}
+
 // explicit_matrix_reducer (:2415-2605): one ELL row per DOF, columns ascending
 __device__ __forceinline__ int vdof_number(const VLevel& L, const int* dof_base, const int* nbrow, int c, int X, int Y,
                                            int Z) {

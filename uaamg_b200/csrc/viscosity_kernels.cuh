@@ -30,6 +30,7 @@ struct VLevel {
     int nl;
     const uint64_t* dof;          // [3][nl][8]
     const int* nb;                // [nl][27]
+    const int* cnb;               // [nl][27] nb for coefficient reads: -1 at fully trimmed leaves; NULL = nb
     const float* coef;            // [27][nl][512]
     const uint32_t* trim;         // [nl] bit (c*9+a): leaf holds the default
     const float* defpage;         // [27][512] applier default of every array
@@ -57,37 +58,49 @@ __device__ __forceinline__ int voff3(int X, int Y, int Z) { return ((X & 7) << 6
 // thread's global loads are in flight together instead of in dependent
 // chains.  (Trimmed level-0 leaves need no check here: their blocks hold the
 // applier default itself, written by k_vtrim_fill.)
+// Coefficient reads use a second table in which a leaf whose 27 arrays are
+// all trimmed is replaced by -1: its blocks hold exactly the applier defaults,
+// which the default page also holds, and that page stays in L1 while the
+// leaf's own blocks would stream from DRAM.
 struct VNbSh {
     int nb[27];
+    int cnb[27];
 };
 // call with all threads of the CTA (contains __syncthreads)
 __device__ __forceinline__ void vnb_prologue(const VLevel& L, int leaf, VNbSh& sh) {
     const int t = threadIdx.x;
-    if (t < 27) sh.nb[t] = L.nb[(long long)leaf * 27 + t];
+    if (t < 27) {
+        const int v = L.nb[(long long)leaf * 27 + t];
+        sh.nb[t] = v;
+        sh.cnb[t] = L.cnb ? L.cnb[(long long)leaf * 27 + t] : v;
+    }
     __syncthreads();
 }
 
 // Address of the leaf block holding neighbourhood slot k of array arr: the
-// fallback page when the leaf does not exist.
+// fallback page when the leaf does not exist (or, for coefficients, is fully
+// trimmed).
+template <bool COEF = false>
 __device__ __forceinline__ const float* vsel(const float* arr, const float* fallback, const VNbSh& sh, int k) {
-    const int lf = sh.nb[k];
+    const int lf = COEF ? sh.cnb[k] : sh.nb[k];
     return lf >= 0 ? arr + (long long)lf * UAAMG_LEAF : fallback;
 }
 
 // Values of a [nl][512] array at the thread's four voxels shifted by
 // (dx, dy, dz), dz in {-1, 0, 1}: missing leaves read the fallback page
 // (zeros for vectors, the applier default for coefficients).
+template <bool COEF = false>
 __device__ __forceinline__ float4 vload4(const float* arr, const float* fb, const VNbSh& sh, int x, int y, int z0,
                                          int dx, int dy, int dz) {
     const int X = x + dx, Y = y + dy;
-    const float* p = vsel(arr, fb, sh, vnb_index(X, Y, z0));
+    const float* p = vsel<COEF>(arr, fb, sh, vnb_index(X, Y, z0));
     const float4 a = *reinterpret_cast<const float4*>(p + voff3(X, Y, z0));
     if (dz == 0) return a;
     if (dz > 0) {
-        const float* q = vsel(arr, fb, sh, vnb_index(X, Y, z0 + 4));
+        const float* q = vsel<COEF>(arr, fb, sh, vnb_index(X, Y, z0 + 4));
         return make_float4(a.y, a.z, a.w, q[voff3(X, Y, z0 + 4)]);
     }
-    const float* q = vsel(arr, fb, sh, vnb_index(X, Y, z0 - 1));
+    const float* q = vsel<COEF>(arr, fb, sh, vnb_index(X, Y, z0 - 1));
     return make_float4(q[voff3(X, Y, z0 - 1)], a.x, a.y, a.z);
 }
 
@@ -103,7 +116,7 @@ __device__ __forceinline__ VArr varr(const VLevel& L, int c, int a) {
 }
 __device__ __forceinline__ float4 cload4(const VArr& A, const VNbSh& sh, int x, int y, int z0, int dx, int dy,
                                          int dz) {
-    return vload4(A.a, A.def, sh, x, y, z0, dx, dy, dz);
+    return vload4<true>(A.a, A.def, sh, x, y, z0, dx, dy, dz);
 }
 __device__ __forceinline__ float4 uload4(const float* v, const VLevel& L, int c, const VNbSh& sh, int x, int y, int z0,
                                          int dx, int dy, int dz) {
@@ -486,8 +499,9 @@ __device__ __forceinline__ float vgs_update(float bb, float off, float iv, float
     r = __fmul_rn(r, w);
     return __fmaf_rn(xc, one_minus_w, r);
 }
+template <bool COEF = false>
 __device__ __forceinline__ float vload1(const float* arr, const float* fb, const VNbSh& sh, int X, int Y, int Z) {
-    return vsel(arr, fb, sh, vnb_index(X, Y, Z))[voff3(X, Y, Z)];
+    return vsel<COEF>(arr, fb, sh, vnb_index(X, Y, Z))[voff3(X, Y, Z)];
 }
 
 // Cross-channel sums (td2, td1 of voffdiag) at a 4-voxel group.
@@ -570,22 +584,22 @@ __device__ __forceinline__ void vload_coef1(const VLevel& L, const VNbSh& sh, in
     for (int ax = 0; ax < 3; ++ax) {
         const int px = ax == 0, py = ax == 1, pz = ax == 2;
         const VArr W = varr(L, c, VA_NEGX + ax);
-        k.wp[ax] = vload1(W.a, W.def, sh, X + px, Y + py, Z + pz);
-        k.wm[ax] = vload1(W.a, W.def, sh, X, Y, Z);
+        k.wp[ax] = vload1<true>(W.a, W.def, sh, X + px, Y + py, Z + pz);
+        k.wm[ax] = vload1<true>(W.a, W.def, sh, X, Y, Z);
     }
     const VArr A00 = varr(L, d2, VA_T00), A01 = varr(L, d2, VA_T01), A10 = varr(L, d2, VA_T10),
                A11 = varr(L, d2, VA_T11), B00 = varr(L, d1, VA_T00), B01 = varr(L, d1, VA_T01),
                B10 = varr(L, d1, VA_T10), B11 = varr(L, d1, VA_T11), IV = varr(L, c, VA_INV);
     const int Xm = X - e0[0], Ym = Y - e0[1], Zm = Z - e0[2];
-    k.a00 = vload1(A00.a, A00.def, sh, X, Y, Z);
-    k.a01 = vload1(A01.a, A01.def, sh, X, Y, Z);
-    k.a10 = vload1(A10.a, A10.def, sh, Xm, Ym, Zm);
-    k.a11 = vload1(A11.a, A11.def, sh, Xm, Ym, Zm);
-    k.b00 = vload1(B00.a, B00.def, sh, X, Y, Z);
-    k.b01 = vload1(B01.a, B01.def, sh, Xm, Ym, Zm);
-    k.b10 = vload1(B10.a, B10.def, sh, X, Y, Z);
-    k.b11 = vload1(B11.a, B11.def, sh, Xm, Ym, Zm);
-    k.iv = vload1(IV.a, IV.def, sh, X, Y, Z);
+    k.a00 = vload1<true>(A00.a, A00.def, sh, X, Y, Z);
+    k.a01 = vload1<true>(A01.a, A01.def, sh, X, Y, Z);
+    k.a10 = vload1<true>(A10.a, A10.def, sh, Xm, Ym, Zm);
+    k.a11 = vload1<true>(A11.a, A11.def, sh, Xm, Ym, Zm);
+    k.b00 = vload1<true>(B00.a, B00.def, sh, X, Y, Z);
+    k.b01 = vload1<true>(B01.a, B01.def, sh, Xm, Ym, Zm);
+    k.b10 = vload1<true>(B10.a, B10.def, sh, X, Y, Z);
+    k.b11 = vload1<true>(B11.a, B11.def, sh, Xm, Ym, Zm);
+    k.iv = vload1<true>(IV.a, IV.def, sh, X, Y, Z);
 }
 // First-colour update of one DOF voxel (X, Y, Z), one of them -1 or 8.
 template <int c>
