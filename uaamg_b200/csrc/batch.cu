@@ -120,8 +120,8 @@ __global__ void __launch_bounds__(NT, 1) k_bcoarsest(const BRec* __restrict__ re
                                                      const unsigned* __restrict__ active, int br, int outr) {
     griddep_wait();
     griddep_launch();
-    __shared__ float ps[NT * ROWS];
-    __shared__ float red[3][64];
+    __shared__ float ps[NT * ROWS + 4];
+    __shared__ __align__(16) float red[3][64];
     const int i = list[blockIdx.x];
     if (!active[i]) return;
     const BRec& R = recs[i];

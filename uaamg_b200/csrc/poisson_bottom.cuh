@@ -194,14 +194,14 @@ __device__ __forceinline__ void cluster_sync_all() {
 // coarsest level's lhs and rhs, the CG's vector, one restriction scratch per
 // leaf group.
 __host__ __device__ inline size_t bottom_smem_bytes(int P, int nlc, int rows) {
-    return (size_t)P * sizeof(SLeaf) + (size_t)nlc * UAAMG_LEAF * 4 * 2 + (size_t)BOT_NT * rows * 4 +
+    return (size_t)P * sizeof(SLeaf) + (size_t)nlc * UAAMG_LEAF * 4 * 2 + (size_t)(BOT_NT * rows + 4) * 4 +
            (size_t)(BOT_THREADS / 128) * UAAMG_LEAF * 4;
 }
 
 template <int ROWS>
 __global__ void __launch_bounds__(BOT_THREADS, 1) k_bottom(BottomArgs A) {
     extern __shared__ __align__(16) unsigned char bsm[];
-    __shared__ float red[3][64];
+    __shared__ __align__(16) float red[3][64];
     cgx::cluster_group cl = cgx::this_cluster();
     const unsigned rank = cl.block_rank();
     const int group = threadIdx.x >> 7, t = threadIdx.x & 127;
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(BOT_THREADS, 1) k_bottom(BottomArgs A) {
     float* xc0 = reinterpret_cast<float*>(bsm + (size_t)P * sizeof(SLeaf));  // coarsest lhs (CTA 0)
     float* bc0 = xc0 + (size_t)A.nlc * UAAMG_LEAF;                            // coarsest rhs (CTA 0)
     float* ps = bc0 + (size_t)A.nlc * UAAMG_LEAF;
-    float* rs = ps + BOT_NT * ROWS + group * UAAMG_LEAF;
+    float* rs = ps + BOT_NT * ROWS + 4 + group * UAAMG_LEAF;
     // the coarsest vectors of CTA 0 as every CTA addresses them
     float* xc0c = cl.map_shared_rank(xc0, 0);
     float* bc0c = cl.map_shared_rank(bc0, 0);

@@ -1239,22 +1239,39 @@ struct DCoarsest {
 #define CG_MAX_DOF 4096
 __host__ __device__ __forceinline__ int coarsest_class(int n) { return n <= 1024 ? 0 : (n <= 2048 ? 1 : 2); }
 
-// Block reductions in one barrier: warps reduce with shfl_down, lane 0 of each
-// warp publishes, every warp reduces the 32 partials the same way and
-// broadcasts lane 0, so all threads hold bit-identical scalars (the CG's
-// control flow depends on them).
-__device__ __forceinline__ float cg_warp_sum(float v) {
+// Block reductions in one barrier: warps reduce with shfl_down into lane 0,
+// lane 0 of each warp publishes its partial, and every thread then adds the
+// NT/32 partials in one fixed pairwise order from shared memory (broadcast
+// float4 reads), so all threads hold bit-identical scalars (the CG's control
+// flow depends on them).  buf: 16-byte aligned, [2][32] floats for the pair
+// form.
+__device__ __forceinline__ float cg_warp_partial(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULLMASK, v, o);
-    return __shfl_sync(FULLMASK, v, 0);
+    return v;  // the warp's sum in lane 0
+}
+template <int NW>  // 8, 16 or 32 partials
+__device__ __forceinline__ float cg_tree_sum(const float* buf) {
+    static_assert(NW == 8 || NW == 16 || NW == 32, "partials");
+    float s[NW / 4];
+#pragma unroll
+    for (int q = 0; q < NW / 4; ++q) {
+        const float4 v = reinterpret_cast<const float4*>(buf)[q];
+        s[q] = (v.x + v.y) + (v.z + v.w);
+    }
+#pragma unroll
+    for (int step = 1; step < NW / 4; step *= 2)
+#pragma unroll
+        for (int q = 0; q + step < NW / 4; q += 2 * step) s[q] += s[q + step];
+    return s[0];
 }
 template <int NT>
 __device__ __forceinline__ float cg_block_sum(float v, float* buf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    v = cg_warp_sum(v);
+    v = cg_warp_partial(v);
     if (lane == 0) buf[w] = v;
     __syncthreads();
-    return cg_warp_sum(lane < NT / 32 ? buf[lane] : 0.f);
+    return cg_tree_sum<NT / 32>(buf);
 }
 template <int NT>
 __device__ __forceinline__ float2 cg_block_sum2(float a, float b, float* buf) {
@@ -1266,27 +1283,27 @@ __device__ __forceinline__ float2 cg_block_sum2(float a, float b, float* buf) {
     }
     if (lane == 0) { buf[w] = a; buf[32 + w] = b; }
     __syncthreads();
-    float x = lane < NT / 32 ? buf[lane] : 0.f, y = lane < NT / 32 ? buf[32 + lane] : 0.f;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        x += __shfl_down_sync(FULLMASK, x, o);
-        y += __shfl_down_sync(FULLMASK, y, o);
-    }
-    return make_float2(__shfl_sync(FULLMASK, x, 0), __shfl_sync(FULLMASK, y, 0));
+    return make_float2(cg_tree_sum<NT / 32>(buf), cg_tree_sum<NT / 32>(buf + 32));
 }
 
 // ROWS rows per thread in a block of NT threads (row i = tid + k * NT); the
 // matrix rows stay in registers for the whole solve (CgRows), so a kernel that
 // solves the same system twice loads them once.  Three barriers per CG
-// iteration.
+// iteration.  (Publishing z and the old p with the second reduction, so that
+// each thread forms its neighbours' new p itself and one barrier goes, doubles
+// the shared-memory reads in flight and pushes the rows out of registers:
+// measured 1.6 times slower.)
 template <int ROWS>
 struct CgRows {
     float dg[ROWS], iv[ROWS], val[ROWS][6];
-    int col[ROWS][6], slot[ROWS];
+    unsigned col[ROWS][6];  // shared-memory address of the column's p (the zero slot when absent)
+    int slot[ROWS];
 };
+// ps: NT * ROWS + 4 floats in shared memory; slot NT * ROWS holds 0
 template <int ROWS, int NT>
-__device__ __forceinline__ void cg_rows_load(const DCoarsest& C, CgRows<ROWS>& M) {
+__device__ __forceinline__ void cg_rows_load(const DCoarsest& C, CgRows<ROWS>& M, const float* ps) {
     const int tid = threadIdx.x, n = C.n;
+    const unsigned base = (unsigned)__cvta_generic_to_shared(ps);
 #pragma unroll
     for (int k = 0; k < ROWS; ++k) {
         const int i = tid + k * NT;
@@ -1296,24 +1313,34 @@ __device__ __forceinline__ void cg_rows_load(const DCoarsest& C, CgRows<ROWS>& M
         M.iv[k] = ok ? C.invd[i] : 0.f;
 #pragma unroll
         for (int e = 0; e < 6; ++e) {
-            M.col[k][e] = ok ? C.col[i * 6 + e] : -1;
-            M.val[k][e] = ok ? C.val[i * 6 + e] : 0.f;
+            const int c = ok ? C.col[i * 6 + e] : -1;
+            M.col[k][e] = base + 4u * (unsigned)(c >= 0 ? c : NT * ROWS);
+            M.val[k][e] = c >= 0 ? C.val[i * 6 + e] : 0.f;
         }
     }
 }
+__device__ __forceinline__ float lds_f32(unsigned addr) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+    return v;
+}
 // out[slot] = the 10-step CG solution for the rhs gathered from rhs[slot]
-// (every thread of the NT-thread block takes part)
+// (every thread of the NT-thread block takes part); ps: NT * ROWS + 4 floats,
+// red: 16-byte aligned.  The products and sums use fused multiply-adds (the
+// coarsest solve's summation order is this kernel's own; the unfused
+// reference solve differs from it by rounding only).
 template <int ROWS, int NT>
 __device__ __forceinline__ void cg_rows_solve(const CgRows<ROWS>& M, const float* rhs, float* out, float* ps,
                                               float (*red)[64]) {
     const int tid = threadIdx.x;
     float x[ROWS], r[ROWS], p[ROWS], z[ROWS];
     float bb = 0.f;
+    if (tid == 0) ps[NT * ROWS] = 0.f;  // the absent columns' slot (published by the first barrier)
 #pragma unroll
     for (int k = 0; k < ROWS; ++k) {
         x[k] = 0.f;
         r[k] = M.slot[k] >= 0 ? rhs[M.slot[k]] : 0.f;
-        bb = __fadd_rn(bb, __fmul_rn(r[k], r[k]));
+        bb = __fmaf_rn(r[k], r[k], bb);
     }
     int rb = 0;
     const float rhsNorm2 = cg_block_sum<NT>(bb, red[rb]);
@@ -1325,7 +1352,7 @@ __device__ __forceinline__ void cg_rows_solve(const CgRows<ROWS>& M, const float
 #pragma unroll
         for (int k = 0; k < ROWS; ++k) {
             p[k] = __fmul_rn(M.iv[k], r[k]);
-            an = __fadd_rn(an, __fmul_rn(r[k], p[k]));
+            an = __fmaf_rn(r[k], p[k], an);
         }
         float absNew = cg_block_sum<NT>(an, red[rb]);
         rb = rb == 2 ? 0 : rb + 1;
@@ -1338,10 +1365,9 @@ __device__ __forceinline__ void cg_rows_solve(const CgRows<ROWS>& M, const float
             for (int k = 0; k < ROWS; ++k) {
                 float s = __fmul_rn(M.dg[k], p[k]);
 #pragma unroll
-                for (int e = 0; e < 6; ++e)
-                    if (M.col[k][e] >= 0) s = __fadd_rn(s, __fmul_rn(M.val[k][e], ps[M.col[k][e]]));
+                for (int e = 0; e < 6; ++e) s = __fmaf_rn(M.val[k][e], lds_f32(M.col[k][e]), s);
                 tq[k] = s;
-                pt = __fadd_rn(pt, __fmul_rn(p[k], s));
+                pt = __fmaf_rn(p[k], s, pt);
             }
             const float alpha = __fdiv_rn(absNew, cg_block_sum<NT>(pt, red[rb]));
             rb = rb == 2 ? 0 : rb + 1;
@@ -1351,8 +1377,8 @@ __device__ __forceinline__ void cg_rows_solve(const CgRows<ROWS>& M, const float
                 x[k] = __fmaf_rn(alpha, p[k], x[k]);
                 r[k] = __fmaf_rn(-alpha, tq[k], r[k]);
                 z[k] = __fmul_rn(M.iv[k], r[k]);
-                rr = __fadd_rn(rr, __fmul_rn(r[k], r[k]));
-                rz = __fadd_rn(rz, __fmul_rn(r[k], z[k]));
+                rr = __fmaf_rn(r[k], r[k], rr);
+                rz = __fmaf_rn(r[k], z[k], rz);
             }
             const float2 s2 = cg_block_sum2<NT>(rr, rz, red[rb]);
             rb = rb == 2 ? 0 : rb + 1;
@@ -1376,7 +1402,7 @@ template <int ROWS, int NT, bool WAIT>
 __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float* rhs, float* out, float* ps,
                                                  float (*red)[64]) {
     CgRows<ROWS> M;
-    cg_rows_load<ROWS, NT>(C, M);
+    cg_rows_load<ROWS, NT>(C, M, ps);
     if (WAIT) {
         griddep_wait();
         griddep_launch();
@@ -1386,8 +1412,8 @@ __device__ __forceinline__ void coarsest_cg_body(const DCoarsest& C, const float
 
 template <int ROWS, int NT>
 __global__ void __launch_bounds__(NT, 1) k_coarsest_cg(DCoarsest C, const float* rhs, float* out) {
-    __shared__ float ps[NT * ROWS];
-    __shared__ float red[3][64];  // rotating reduction buffers (no reuse within 2 barriers)
+    __shared__ float ps[NT * ROWS + 4];
+    __shared__ __align__(16) float red[3][64];  // rotating reduction buffers (no reuse within 2 barriers)
     coarsest_cg_body<ROWS, NT, true>(C, rhs, out, ps, red);
 }
 
