@@ -1002,10 +1002,12 @@ static void coarsest_cg(orc_visc* h) {
 /* The same CG with the operation order of the CUDA coarsest kernel
  * (uaamg_b200/csrc/viscosity_kernels.cuh, k_vcoarsest_cg<ROWS>): row i belongs
  * to thread tid = i % 256 (the k-th row of a thread is tid + 256 k, ROWS rows
- * per thread by system size); a dot product is every thread's float sum over
- * its rows, then a shuffle-down tree inside each 32-lane warp, then the same
- * tree over the 8 warp sums; the vector updates are fused multiply-adds
- * (x += alpha p, r -= alpha A p, p = z + beta p).  Eigen's own summation order
+ * per thread by system size); a dot product is every thread's fused
+ * multiply-add chain over its rows, then a shuffle-down tree inside each
+ * 32-lane warp, then ((w0+w1)+(w2+w3)) + ((w4+w5)+(w6+w7)) over the 8 warp
+ * sums; a row of A p is a fused multiply-add chain over its 15 ELL entries in
+ * column order, the padding entries adding 0 * 0; the vector updates are fused
+ * multiply-adds (x += alpha p, r -= alpha A p, p = z + beta p).  Eigen's own summation order
  * depends on its vectorisation (and its version is not pinned), so either
  * order restates the reference's coarsest solve; this one makes the oracle's
  * whole viscosity PCG reproducible bit for bit on the GPU. */
@@ -1022,11 +1024,11 @@ static float warp_tree32(const float* lane_in) {
     return a[0];
 }
 static float block_tree256(const float* part) {
-    float w[32];
+    float w[8];
     for (int k = 0; k < 8; ++k) w[k] = warp_tree32(part + 32 * k);
-    for (int k = 8; k < 32; ++k) w[k] = 0.f;
-    return warp_tree32(w);
+    return ((w[0] + w[1]) + (w[2] + w[3])) + ((w[4] + w[5]) + (w[6] + w[7]));
 }
+#define VCG_ELL 15 /* entries per row of the kernel's ELL matrix */
 static int vcg_rows(int n) {
     return n <= 2 * VCG_NT ? 2 : (n <= 4 * VCG_NT ? 4 : (n <= 8 * VCG_NT ? 8 : 16));
 }
@@ -1041,38 +1043,41 @@ static void coarsest_cg_kernel_order(orc_visc* h) {
     float* iv = (float*)vcalloc((size_t)N, sizeof(float));
     float part[VCG_NT], part2[VCG_NT];
     for (int j = 0; j < n; ++j) { r[j] = h->c_b[j]; iv[j] = h->c_invdiag[j]; }
-#define THREAD_SUM(dst, expr)                                   \
+#define THREAD_SUM(dst, ea, eb)                                 \
     for (int tid = 0; tid < VCG_NT; ++tid) {                    \
         float v_ = 0.f;                                         \
         for (int k = 0; k < R; ++k) {                           \
             const int j = tid + k * VCG_NT;                     \
-            v_ = v_ + (expr);                                   \
+            v_ = fmaf((ea), (eb), v_);                          \
         }                                                       \
         dst[tid] = v_;                                          \
     }
-    THREAD_SUM(part, r[j] * r[j]);
+    THREAD_SUM(part, r[j], r[j]);
     const float rhsNorm2 = block_tree256(part);
     const float threshold = fmaxf((FLT_EPSILON * FLT_EPSILON) * rhsNorm2, FLT_MIN);
     if (rhsNorm2 != 0.f && !(rhsNorm2 < threshold)) {
         for (int j = 0; j < N; ++j) p[j] = iv[j] * r[j];
-        THREAD_SUM(part, r[j] * p[j]);
+        THREAD_SUM(part, r[j], p[j]);
         float absNew = block_tree256(part);
         for (int it = 0; it < 10; ++it) {
             for (int j = 0; j < N; ++j) {
                 float sacc = 0.f;
-                if (j < n)
-                    for (int k = h->c_rowptr[j]; k < h->c_rowptr[j + 1]; ++k) sacc = sacc + h->c_val[k] * p[h->c_col[k]];
+                if (j < n) {
+                    const int len = h->c_rowptr[j + 1] - h->c_rowptr[j];
+                    for (int k = h->c_rowptr[j]; k < h->c_rowptr[j + 1]; ++k) sacc = fmaf(h->c_val[k], p[h->c_col[k]], sacc);
+                    for (int e = len; e < VCG_ELL; ++e) sacc = fmaf(0.f, 0.f, sacc);
+                }
                 t[j] = sacc;
             }
-            THREAD_SUM(part, p[j] * t[j]);
+            THREAD_SUM(part, p[j], t[j]);
             const float alpha = absNew / block_tree256(part);
             for (int j = 0; j < N; ++j) {
                 x[j] = fmaf(alpha, p[j], x[j]);
                 r[j] = fmaf(-alpha, t[j], r[j]);
                 z[j] = iv[j] * r[j];
             }
-            THREAD_SUM(part, r[j] * r[j]);
-            THREAD_SUM(part2, r[j] * z[j]);
+            THREAD_SUM(part, r[j], r[j]);
+            THREAD_SUM(part2, r[j], z[j]);
             const float rr = block_tree256(part), rz = block_tree256(part2);
             if (rr < threshold) break;
             const float absOld = absNew;

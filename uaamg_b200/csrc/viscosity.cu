@@ -243,6 +243,10 @@ struct uaamg_viscosity {
     // levels are issue-bound and the step's face-layer recomputation costs more
     // than the launch it saves
     int rb_fused_max_leaves = 0;
+    // levels of more leaves run their red / black passes as k_vapply_seq
+    // (more leaves than resident CTAs: the next leaf's table loads hide behind
+    // the current leaf)
+    int seq_min_leaves = INT_MAX;
     std::vector<void*> allocs;
     // level-0 construction products kept for the right-hand side
     VolFields V{};
@@ -583,10 +587,17 @@ struct VEnq {
         static const char* names[] = {"normal", "residual", "jacobi", "red_gs", "black_gs"};
         if (prof) pb("L" + std::to_string(l) + " " + names[MODE] + (gs ? " c" + std::to_string(c) : std::string()));
         if constexpr (MODE == VM_RED || MODE == VM_BLACK) {
-            const dim3 g((unsigned)D.L.nl);
-            if (c == 0) launch2(k_vapply<MODE, 0>, g, 128, s, D.L, x, b, out, 1.0f);
-            else if (c == 1) launch2(k_vapply<MODE, 1>, g, 128, s, D.L, x, b, out, 1.0f);
-            else launch2(k_vapply<MODE, 2>, g, 128, s, D.L, x, b, out, 1.0f);
+            if (D.L.nl >= h->seq_min_leaves) {
+                const dim3 g((unsigned)std::min(D.L.nl, VAPPLY_MINB * g_sms));
+                if (c == 0) launch2(k_vapply_seq<MODE, 0>, g, 128, s, D.L, x, b, out, 1.0f);
+                else if (c == 1) launch2(k_vapply_seq<MODE, 1>, g, 128, s, D.L, x, b, out, 1.0f);
+                else launch2(k_vapply_seq<MODE, 2>, g, 128, s, D.L, x, b, out, 1.0f);
+            } else {
+                const dim3 g((unsigned)D.L.nl);
+                if (c == 0) launch2(k_vapply<MODE, 0>, g, 128, s, D.L, x, b, out, 1.0f);
+                else if (c == 1) launch2(k_vapply<MODE, 1>, g, 128, s, D.L, x, b, out, 1.0f);
+                else launch2(k_vapply<MODE, 2>, g, 128, s, D.L, x, b, out, 1.0f);
+            }
         } else {
             launch2(k_vapply<MODE, -1>, dim3((unsigned)D.L.nl, 3u), 128, s, D.L, x, b, out, 1.0f);
         }
@@ -978,7 +989,9 @@ int uaamg_viscosity_create_on_stream(const uaamg_leaf_grid* viscosity, const uaa
                 g_sms = sms;
         }
         h->rb_fused_max_leaves = 2 * g_sms;
+        h->seq_min_leaves = 2 * g_sms + 1;
         if (const char* e = getenv("UAAMG_VISC_FUSED_RB_LEAVES")) h->rb_fused_max_leaves = atoi(e);
+        if (const char* e = getenv("UAAMG_VISC_SEQ_LEAVES")) h->seq_min_leaves = atoi(e);
         build_viscosity(h, viscosity, liquid_sdf, solid_sdf, dt, rho, dx);
     } catch (const UaamgError& e) {
         uaamg_viscosity_destroy(h);

@@ -723,6 +723,67 @@ __global__ void __launch_bounds__(VRB_THREADS, VRB_MINB) k_vrbgs(VLevel L, VRbIo
     reinterpret_cast<float4*>(io.out)[(long long)leaf * UAAMG_LEAF4 + t] = out;
 }
 
+// k_vapply<RED / BLACK, c> over many leaves: a grid of a few CTAs per SM, each
+// looping over leaves blockIdx.x, blockIdx.x + gridDim.x, ...  A one-leaf CTA
+// starts with a dependent chain (neighbour table into shared memory, barrier,
+// then the coefficient and vector loads); here the next leaf's table entries
+// and DOF bits load while the current leaf computes, so every leaf after the
+// first starts at its coefficient loads.  Same per-voxel arithmetic as
+// k_vapply.
+template <int MODE, int c>
+__global__ void __launch_bounds__(128, VAPPLY_MINB) k_vapply_seq(VLevel L, const float* x, const float* b, float* out,
+                                                                 float w) {
+    __shared__ VNbSh sh[2];
+    const int t = threadIdx.x;
+    int leaf = blockIdx.x;
+    unsigned m = 0;
+    if (leaf < L.nl) {
+        if (t < 27) {
+            const int v = L.nb[(long long)leaf * 27 + t];
+            sh[0].nb[t] = v;
+            sh[0].cnb[t] = L.cnb ? L.cnb[(long long)leaf * 27 + t] : v;
+        }
+        m = vmask4(L, c, leaf, t);
+    }
+    __syncthreads();
+    bool waited = false;
+    for (int it = 0; leaf < L.nl; ++it, leaf += gridDim.x) {
+        const VNbSh& cur = sh[it & 1];
+        const int next = leaf + (int)gridDim.x;
+        int nb_n = -1, cnb_n = -1;
+        unsigned m_n = 0;
+        if (next < L.nl) {
+            if (t < 27) {
+                nb_n = L.nb[(long long)next * 27 + t];
+                cnb_n = L.cnb ? L.cnb[(long long)next * 27 + t] : nb_n;
+            }
+            m_n = vmask4(L, c, next, t);
+        }
+        VCoef k;
+        if (m) vload_coef<MODE, c>(L, cur, t, k);
+        if (!waited) {
+            griddep_wait();
+            griddep_launch();
+            waited = true;
+        }
+        if (m) {
+            float4 xc;
+            const float4 res = vapply_value_k<MODE, c>(L, cur, t, x, b, w, m, k, xc);
+            reinterpret_cast<float4*>(out + (long long)c * L.nl * UAAMG_LEAF)[(long long)leaf * UAAMG_LEAF4 + t] = res;
+        }
+        if (t < 27) {
+            sh[(it + 1) & 1].nb[t] = nb_n;
+            sh[(it + 1) & 1].cnb[t] = cnb_n;
+        }
+        m = m_n;
+        __syncthreads();
+    }
+    if (!waited) {
+        griddep_wait();
+        griddep_launch();
+    }
+}
+
 // restriction (:2353-2413) for one (coarse leaf, channel): coarse = (sum of the
 // DOF children) * 0.125 * 0.5 * 2, zero at coarse non-DOF voxels
 __device__ __forceinline__ void vrestrict_item(const VLevel& F, const VLevel& C, const float* fine, float* coarse,
@@ -1234,40 +1295,43 @@ struct DCoarsestV {
 // short.
 #define VCG_THREADS 256
 #define VCG_WARPS (VCG_THREADS / 32)
-__device__ __forceinline__ float vcg_warp_sum(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return __shfl_sync(0xffffffffu, v, 0);
-}
-// block sums in one barrier; every thread gets the same bits
+// Block sums in one barrier: a shuffle-down tree inside each warp, then every
+// thread adds the 8 warp sums from shared memory as ((w0+w1)+(w2+w3)) +
+// ((w4+w5)+(w6+w7)) (cg_tree_sum), so every thread gets the same bits.
+// buf: 16-byte aligned.
 __device__ __forceinline__ float vcg_block_sum(float v, float* buf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    v = vcg_warp_sum(v);
+    v = cg_warp_partial(v);
     if (lane == 0) buf[w] = v;
     __syncthreads();
-    return vcg_warp_sum(lane < VCG_WARPS ? buf[lane] : 0.f);
+    return cg_tree_sum<VCG_WARPS>(buf);
 }
 __device__ __forceinline__ float2 vcg_block_sum2(float a, float b, float* buf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    a = vcg_warp_sum(a);
-    b = vcg_warp_sum(b);
+    a = cg_warp_partial(a);
+    b = cg_warp_partial(b);
     if (lane == 0) {
         buf[w] = a;
         buf[32 + w] = b;
     }
     __syncthreads();
-    return make_float2(vcg_warp_sum(lane < VCG_WARPS ? buf[lane] : 0.f),
-                       vcg_warp_sum(lane < VCG_WARPS ? buf[32 + lane] : 0.f));
+    return make_float2(cg_tree_sum<VCG_WARPS>(buf), cg_tree_sum<VCG_WARPS>(buf + 32));
 }
 
+// Rows of ROWS <= 4 stay in registers with the shared-memory address of each
+// entry's p (padding entries: value 0 at a slot that holds 0); larger systems
+// read their rows from global memory each iteration.  A row's product is
+// s = fma(v_e, p[c_e], s) over its VCG_W entries, padding included.
 template <int ROWS>
 __global__ void __launch_bounds__(VCG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, const float* rhs, float* out) {
     constexpr bool REG = ROWS <= 4;
-    __shared__ float ps[VCG_THREADS * ROWS];
-    __shared__ float red[3][64];
+    constexpr int ZERO = VCG_THREADS * ROWS;  // the zero slot
+    __shared__ float ps[VCG_THREADS * ROWS + 4];
+    __shared__ __align__(16) float red[3][64];
     const int tid = threadIdx.x, n = C.n;
+    const unsigned psb = (unsigned)__cvta_generic_to_shared(ps);
     float x[ROWS], r[ROWS], p[ROWS], z[ROWS], iv[ROWS];
-    int rc[REG ? ROWS : 1][VCG_W];
+    unsigned rc[REG ? ROWS : 1][VCG_W];
     float rv[REG ? ROWS : 1][VCG_W];
     long long sl[ROWS];
     // static data (rows, 1/diag, slots) before the wait for rhs
@@ -1279,11 +1343,13 @@ __global__ void __launch_bounds__(VCG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, c
         if (REG) {
 #pragma unroll
             for (int e = 0; e < VCG_W; ++e) {
-                rc[REG ? k : 0][e] = i < n ? __ldg(C.col + (long long)i * VCG_W + e) : -1;
-                rv[REG ? k : 0][e] = i < n ? __ldg(C.val + (long long)i * VCG_W + e) : 0.f;
+                const int cc = i < n ? __ldg(C.col + (long long)i * VCG_W + e) : -1;
+                rc[REG ? k : 0][e] = psb + 4u * (unsigned)(cc >= 0 ? cc : ZERO);
+                rv[REG ? k : 0][e] = cc >= 0 ? __ldg(C.val + (long long)i * VCG_W + e) : 0.f;
             }
         }
     }
+    if (tid == 0) ps[ZERO] = 0.f;  // published by the first reduction's barrier
     griddep_wait();
     griddep_launch();
     float bb = 0.f;
@@ -1292,7 +1358,7 @@ __global__ void __launch_bounds__(VCG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, c
         x[k] = 0.f;
         r[k] = sl[k] >= 0 ? rhs[sl[k]] : 0.f;
         p[k] = 0.f;
-        bb = __fadd_rn(bb, __fmul_rn(r[k], r[k]));
+        bb = __fmaf_rn(r[k], r[k], bb);
     }
     int rb = 0;
     const float rhsNorm2 = vcg_block_sum(bb, red[rb]);
@@ -1303,7 +1369,7 @@ __global__ void __launch_bounds__(VCG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, c
 #pragma unroll
         for (int k = 0; k < ROWS; ++k) {
             p[k] = __fmul_rn(iv[k], r[k]);
-            an = __fadd_rn(an, __fmul_rn(r[k], p[k]));
+            an = __fmaf_rn(r[k], p[k], an);
         }
         float absNew = vcg_block_sum(an, red[rb]);
         rb = rb == 2 ? 0 : rb + 1;
@@ -1318,19 +1384,18 @@ __global__ void __launch_bounds__(VCG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, c
                 float s = 0.f;
                 if (REG) {
 #pragma unroll
-                    for (int e = 0; e < VCG_W; ++e)
-                        if (rc[REG ? k : 0][e] >= 0) s = __fadd_rn(s, __fmul_rn(rv[REG ? k : 0][e], ps[rc[REG ? k : 0][e]]));
+                    for (int e = 0; e < VCG_W; ++e) s = __fmaf_rn(rv[REG ? k : 0][e], lds_f32(rc[REG ? k : 0][e]), s);
                 } else if (i < n) {
                     const int* cr = C.col + (long long)i * VCG_W;
                     const float* vr = C.val + (long long)i * VCG_W;
 #pragma unroll
                     for (int e = 0; e < VCG_W; ++e) {
                         const int cc = __ldg(cr + e);
-                        if (cc >= 0) s = __fadd_rn(s, __fmul_rn(__ldg(vr + e), ps[cc]));
+                        s = __fmaf_rn(cc >= 0 ? __ldg(vr + e) : 0.f, ps[cc >= 0 ? cc : ZERO], s);
                     }
                 }
                 tq[k] = s;
-                pt = __fadd_rn(pt, __fmul_rn(p[k], s));
+                pt = __fmaf_rn(p[k], s, pt);
             }
             const float alpha = __fdiv_rn(absNew, vcg_block_sum(pt, red[rb]));
             rb = rb == 2 ? 0 : rb + 1;
@@ -1340,8 +1405,8 @@ __global__ void __launch_bounds__(VCG_THREADS, 1) k_vcoarsest_cg(DCoarsestV C, c
                 x[k] = __fmaf_rn(alpha, p[k], x[k]);
                 r[k] = __fmaf_rn(-alpha, tq[k], r[k]);
                 z[k] = __fmul_rn(iv[k], r[k]);
-                rr = __fadd_rn(rr, __fmul_rn(r[k], r[k]));
-                rz = __fadd_rn(rz, __fmul_rn(r[k], z[k]));
+                rr = __fmaf_rn(r[k], r[k], rr);
+                rz = __fmaf_rn(r[k], z[k], rz);
             }
             const float2 s2 = vcg_block_sum2(rr, rz, red[rb]);
             rb = rb == 2 ? 0 : rb + 1;
