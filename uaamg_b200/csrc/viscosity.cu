@@ -718,6 +718,12 @@ static void enqueue_mucycle(VEnq& E, int l, float* lhs, const float* rhs, bool f
     E.rbgs2(l, false, lhs, rhs);
 }
 
+// grid of the level-0 vector streams: 16 CTAs of 128 threads per SM at most
+static dim3 vstream_grid(int nl) {
+    const long long n4 = 3LL * nl * UAAMG_LEAF4;
+    return dim3((unsigned)std::max(1LL, std::min((n4 + 127) / 128, 16LL * g_sms)));
+}
+
 static void venqueue_setup(VEnq& E, cudaGraphConditionalHandle cond, int use_cond) {
     uaamg_viscosity* h = E.h;
     const VLevelDev& D = h->lv[0];
@@ -742,7 +748,8 @@ static void venqueue_body(VEnq& E, cudaGraphConditionalHandle cond, int use_cond
     launch2(k_vdot, gd, VDOT_THREADS, E.s, D.L, (const float*)h->z, (const float*)h->r, part, h->st, 0);
     E.pe();
     if (E.prof) E.pb("L0 pcg x,p update");
-    launch2(k_vpcg_update_p, g, 128, E.s, D.L, (const float*)h->z, h->p, h->x, (const PcgState*)h->st);
+    launch2(k_vpcg_update_p, vstream_grid(D.L.nl), 128, E.s, D.L, (const float*)h->z, h->p, h->x,
+            (const PcgState*)h->st);
     E.pe();
     if (E.prof) E.pb("L0 pcg Ap");
     launch2(k_vpcg_Ap, g, 128, E.s, D.L, (const float*)h->p, h->q);
@@ -751,7 +758,8 @@ static void venqueue_body(VEnq& E, cudaGraphConditionalHandle cond, int use_cond
     launch2(k_vdot, gd, VDOT_THREADS, E.s, D.L, (const float*)h->p, (const float*)h->q, part, h->st, 1);
     E.pe();
     if (E.prof) E.pb("L0 pcg r update+absmax");
-    launch2(k_vpcg_update_r, g, 128, E.s, D.L, (const float*)h->q, h->r, h->partials, h->st, cond, use_cond);
+    launch2(k_vpcg_update_r, vstream_grid(D.L.nl), 128, E.s, D.L, (const float*)h->q, h->r, h->partials, h->st,
+            cond, use_cond);
     E.pe();
     E.count += 5;
 }

@@ -1144,26 +1144,34 @@ __global__ void __launch_bounds__(VDOT_THREADS) k_vdot(VLevel L, const float* a,
 // line 16: x += alpha p (not in the first iteration); p = z + beta p
 __global__ void __launch_bounds__(128) k_vpcg_update_p(VLevel L, const float* z, float* p, float* x,
                                                        const PcgState* st) {
+    // one grid-stride stream over the level's three channels (a few CTAs per
+    // SM); non-DOF voxels hold 0 in x, p and z, and 0 + a * 0 keeps them 0
     griddep_wait();
     griddep_launch();
-    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
-    const long long i = (long long)c * L.nl * UAAMG_LEAF4 + (long long)leaf * UAAMG_LEAF4 + t;
+    const long long n4 = 3LL * L.nl * UAAMG_LEAF4;
     const float beta = st->beta, alpha = st->alpha;
-    float4 pp = reinterpret_cast<float4*>(p)[i];
-    const float4 zz = reinterpret_cast<const float4*>(z)[i];
-    if (!st->first) {
-        float4 xx = reinterpret_cast<float4*>(x)[i];
-        xx.x = __fadd_rn(xx.x, __fmul_rn(alpha, pp.x));
-        xx.y = __fadd_rn(xx.y, __fmul_rn(alpha, pp.y));
-        xx.z = __fadd_rn(xx.z, __fmul_rn(alpha, pp.z));
-        xx.w = __fadd_rn(xx.w, __fmul_rn(alpha, pp.w));
-        reinterpret_cast<float4*>(x)[i] = xx;
+    const bool first = st->first;
+    float4* p4 = reinterpret_cast<float4*>(p);
+    float4* x4 = reinterpret_cast<float4*>(x);
+    const float4* z4 = reinterpret_cast<const float4*>(z);
+#pragma unroll 2
+    for (long long i = (long long)blockIdx.x * 128 + threadIdx.x; i < n4; i += (long long)gridDim.x * 128) {
+        float4 pp = p4[i];
+        const float4 zz = z4[i];
+        if (!first) {
+            float4 xx = x4[i];
+            xx.x = __fadd_rn(xx.x, __fmul_rn(alpha, pp.x));
+            xx.y = __fadd_rn(xx.y, __fmul_rn(alpha, pp.y));
+            xx.z = __fadd_rn(xx.z, __fmul_rn(alpha, pp.z));
+            xx.w = __fadd_rn(xx.w, __fmul_rn(alpha, pp.w));
+            x4[i] = xx;
+        }
+        pp.x = __fadd_rn(zz.x, __fmul_rn(beta, pp.x));
+        pp.y = __fadd_rn(zz.y, __fmul_rn(beta, pp.y));
+        pp.z = __fadd_rn(zz.z, __fmul_rn(beta, pp.z));
+        pp.w = __fadd_rn(zz.w, __fmul_rn(beta, pp.w));
+        p4[i] = pp;
     }
-    pp.x = __fadd_rn(zz.x, __fmul_rn(beta, pp.x));
-    pp.y = __fadd_rn(zz.y, __fmul_rn(beta, pp.y));
-    pp.z = __fadd_rn(zz.z, __fmul_rn(beta, pp.z));
-    pp.w = __fadd_rn(zz.w, __fmul_rn(beta, pp.w));
-    reinterpret_cast<float4*>(p)[i] = pp;
 }
 
 // line 6: q = A p (sigma and alpha follow in k_vdot)
@@ -1179,24 +1187,29 @@ __global__ void __launch_bounds__(128) k_vpcg_Ap(VLevel L, const float* p, float
 // last allowed iteration (no divergence test in this solver)
 __global__ void __launch_bounds__(128) k_vpcg_update_r(VLevel L, const float* q, float* r, double* partials,
                                                        PcgState* st, cudaGraphConditionalHandle cond, int use_cond) {
+    // one grid-stride stream over the level's three channels; non-DOF voxels
+    // hold 0 in r and q (0 - alpha * 0 keeps them 0), so the max over every
+    // voxel is the max over the DOFs
     griddep_wait();
     griddep_launch();
     __shared__ float shf[4];
     __shared__ bool last;
-    const int leaf = blockIdx.x, c = blockIdx.y, t = threadIdx.x;
-    const unsigned m = vmask4(L, c, leaf, t);
-    const long long i = (long long)c * L.nl * UAAMG_LEAF4 + (long long)leaf * UAAMG_LEAF4 + t;
+    const int t = threadIdx.x;
+    const long long n4 = 3LL * L.nl * UAAMG_LEAF4;
     const float na = -st->alpha;
+    float4* r4 = reinterpret_cast<float4*>(r);
+    const float4* q4 = reinterpret_cast<const float4*>(q);
     float a = 0.f;
-    if (m) {
-        const float4 qq = reinterpret_cast<const float4*>(q)[i];
-        float4 rr = reinterpret_cast<float4*>(r)[i];
+#pragma unroll 2
+    for (long long i = (long long)blockIdx.x * 128 + t; i < n4; i += (long long)gridDim.x * 128) {
+        const float4 qq = q4[i];
+        float4 rr = r4[i];
         rr.x = __fadd_rn(rr.x, __fmul_rn(na, qq.x));
         rr.y = __fadd_rn(rr.y, __fmul_rn(na, qq.y));
         rr.z = __fadd_rn(rr.z, __fmul_rn(na, qq.z));
         rr.w = __fadd_rn(rr.w, __fmul_rn(na, qq.w));
-        reinterpret_cast<float4*>(r)[i] = rr;
-        a = vabs4(rr, m);
+        r4[i] = rr;
+        a = nanmax(a, vabs4(rr, 0xFu));
     }
     const float part = block_max128(a, shf);
     if (vpublish((double)part, partials, &st->ticket[4], &last)) {
