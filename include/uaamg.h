@@ -250,8 +250,19 @@ int uaamg_poisson_set_stream(uaamg_poisson* h, void* stream);
 int uaamg_poisson_get_stream(const uaamg_poisson* h, void** stream);
 /* PCG driver: 1 (default) host-driven loop for a handle's first solve and the
  * CUDA-graph solve (conditional WHILE node) from the second solve on; 2 the
- * graph always; 0 the host-driven loop always. */
+ * graph always; 0 the host-driven loop always.
+ * In mode 1 a handle's first solve may replay a graph from the process's
+ * solve-graph cache instead: when the exact launch sequence of the solve
+ * (kernels, shapes, argument bytes, i.e. the same hierarchy shape with its
+ * buffers at the same addresses) equals that of a graph captured for an
+ * earlier handle.  A graph is captured for the cache the second time a launch
+ * sequence is seen.  Results are the same bits as the host-driven loop.
+ * Environment UAAMG_SOLVE_GRAPH_CACHE=0 (read at handle creation) turns it off. */
 int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph);
+/* Solve-graph cache counters of the process (pressure and viscosity solves):
+ * first solves that replayed a cached graph, and graphs captured into the
+ * cache. */
+int uaamg_solve_graph_cache_stats(int64_t* hits, int64_t* captures);
 /* Kernels launched through this handle since it was created: hierarchy build,
  * right-hand side and every solve (kernels inside the solve graph included). */
 int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h);
@@ -550,7 +561,9 @@ int uaamg_viscosity_profile_pcg(uaamg_viscosity* h, float* d_velocity, const flo
  * ordering rules of uaamg_poisson_set_stream apply). */
 int uaamg_viscosity_set_stream(uaamg_viscosity* h, void* stream);
 int uaamg_viscosity_get_stream(const uaamg_viscosity* h, void** stream);
-/* 1 (default): host-driven first solve, CUDA graph afterwards; 2 graph always; 0 never. */
+/* 1 (default): host-driven first solve, CUDA graph afterwards; 2 graph always; 0 never.
+ * In mode 1 the first solve may replay a graph of the solve-graph cache, as
+ * for uaamg_poisson_set_graph_mode. */
 int uaamg_viscosity_set_graph_mode(uaamg_viscosity* h, int use_graph);
 int64_t uaamg_viscosity_kernel_launches(const uaamg_viscosity* h);
 

@@ -355,6 +355,44 @@ def test_residual_norm_device(scene64, gpu):
     assert float(dn.item()) == ref.abs_max(r)
 
 
+def test_solve_graph_cache_replay_identical(scene64, gpu):
+    """Fresh handles on the same inputs, each solved once in the default mode:
+    once the launch sequence recurs, the first solve captures a graph for the
+    cache and later handles (buffers at the same pool addresses) replay it.
+    Every pressure, iteration count and status is the host-driven loop's."""
+    import gc
+    torch = gpu
+    from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver, solve_graph_cache_stats
+    sc, lap, ref = scene64
+    grids = []
+    for k in ("phi", "face_weights", "vx", "vy", "vz", "solid_velocity"):
+        g = getattr(sc, k)
+        d = LeafGrid(origins=g.origins, values=g.values, background=g.background, masks=g.masks)
+        d.values = torch.from_numpy(g.values).cuda()
+        grids.append(d)
+
+    def solve(mode):
+        lp = LaplacianWithLevel.createPressurePoissonLaplacianWithRhs(*grids, sc.dt, sc.dx)
+        s = PoissonSolver(lp)
+        s.use_graph = mode
+        p = torch.empty((lp.leaf_count(0), 512), dtype=torch.float32, device="cuda")
+        st = s.solveMultigridPCGResident(p)
+        out = (st, s.mIterationTaken, p.cpu().numpy())
+        del s, lp, p
+        gc.collect()
+        torch.cuda.synchronize()
+        return out
+
+    st0, it0, p0 = solve(0)
+    h0, c0 = solve_graph_cache_stats()
+    for _ in range(6):
+        st, it, p = solve(1)
+        assert st == st0 and it == it0
+        assert np.array_equal(p, p0)
+    h1, c1 = solve_graph_cache_stats()
+    assert c1 > c0 and h1 > h0, (h0, c0, h1, c1)
+
+
 def test_create_with_rhs_one_call_identical(scene64, gpu):
     """uaamg_poisson_create_with_rhs (matrix, hierarchy and rhs in one call,
     each input uploaded once) + the resident solve give the same hierarchy,

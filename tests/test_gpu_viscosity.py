@@ -167,6 +167,37 @@ def test_fused_rbgs_steps_identical(gpu, monkeypatch, n, seed):
     assert np.array_equal(x0, x1)
 
 
+def test_solve_graph_cache_replay_identical(gpu):
+    """Fresh viscosity handles on the same inputs, each solved once in the
+    default mode: the recurring launch sequence gets a cached graph that later
+    handles replay; every solution is the host-driven loop's bits."""
+    import gc
+    from uaamg_b200.poisson import solve_graph_cache_stats
+    from uaamg_b200.viscosity import L_with_level, simd_viscosity3d
+    sc = scenes.plain_viscosity_scene(n=32, seed=5)
+
+    def solve(mode):
+        lv = L_with_level.create_viscosity_matrix(sc.viscosity, sc.liquid_phi, sc.solid_phi, sc.dt, sc.rho, sc.dx)
+        rhs = lv.build_rhs(sc.u, sc.v, sc.w, sc.solid_velocity)
+        x = lv.gather_velocity(sc.u, sc.v, sc.w)
+        s = simd_viscosity3d(lv)
+        s.use_graph = mode
+        st = s.pcg_solve(x, 1e-6, rhs)
+        out = (st, s.m_iteration, x)
+        del s, lv
+        gc.collect()
+        return out
+
+    st0, it0, x0 = solve(0)
+    h0, c0 = solve_graph_cache_stats()
+    for _ in range(6):
+        st, it, x = solve(1)
+        assert st == st0 and it == it0
+        assert np.array_equal(x, x0)
+    h1, c1 = solve_graph_cache_stats()
+    assert c1 > c0 and h1 > h0, (h0, c0, h1, c1)
+
+
 def test_restriction_prolongation_bit_exact(scene32):
     sc, lv, ref = scene32
     for l in range(ref.num_levels - 1):

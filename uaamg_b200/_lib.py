@@ -136,6 +136,7 @@ EXPORTS = [
     ("uaamg_poisson_get_stream", i32, [vp, C.POINTER(vp)]),
     ("uaamg_poisson_set_graph_mode", i32, [vp, i32]),
     ("uaamg_poisson_kernel_launches", i64, [vp]),
+    ("uaamg_solve_graph_cache_stats", i32, [C.POINTER(i64), C.POINTER(i64)]),
     ("uaamg_poisson_prepare_mixed", i32, [vp, i32, vp]),
     ("uaamg_poisson_set_residual_replacement", i32, [vp, i32]),
     ("uaamg_poisson_solve_pcg_mixed", i32, [vp, i32, vp, vp, C.POINTER(C.c_int)]),

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <type_traits>
@@ -415,6 +416,7 @@ struct uaamg_poisson {
     cudaGraphExec_t graph_exec = nullptr;
     cudaGraph_t graph = nullptr;
     int graph_key = -1;
+    std::shared_ptr<struct SolveGraph> shared_graph;  // set when graph / graph_exec belong to the solve-graph cache
     int64_t body_launches = 0, setup_launches = 0, finish_launches = 0;
     int64_t launches = 0;
     int64_t last_launches = 0;
@@ -947,8 +949,55 @@ static int g_sms = 148;  // SMs of the device (set when a handle is created)
 // pass cost the GPU's CTA launch rate (about a nanosecond per CTA) instead
 // of its bytes.
 static unsigned elem_grid(int nl) { return (unsigned)std::min(nl, g_tune.elem_ctas_per_sm * g_sms); }
+// ---------------------------------------------------------------------------
+// Launch recorder.  While t_rec is set (on this thread), the launch helpers
+// append each launch -- kernel, grid, block, shared memory, attributes and the
+// bytes of its arguments -- and each memset to t_rec instead of issuing it.
+// Two recordings of the PCG's enqueue code are equal exactly when the graphs
+// captured from them would be equal (the conditional handle is recorded as 0),
+// which lets a new handle replay a graph captured for an earlier handle whose
+// buffers sat at the same addresses (solve_graph_cache).
+struct LaunchRec {
+    std::vector<unsigned char> bytes;
+    void put(const void* p, size_t n) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        bytes.insert(bytes.end(), c, c + n);
+    }
+    template <class T>
+    void val(const T& v) {
+        static_assert(std::is_trivially_copyable<T>::value, "recorded argument");
+        put(&v, sizeof(T));
+    }
+};
+static thread_local LaunchRec* t_rec = nullptr;
+template <typename... KArgs, typename... Args>
+static void rec_launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, int attrs, Args... args) {
+    LaunchRec& r = *t_rec;
+    r.val((unsigned char)'K');
+    r.val(reinterpret_cast<const void*>(kern));
+    r.val(grid);
+    r.val(block);
+    r.val(smem);
+    r.val(attrs);
+    (r.val(static_cast<KArgs>(args)), ...);
+}
+static void enq_memset(void* p, int v, size_t n, cudaStream_t s) {
+    if (t_rec) {
+        t_rec->val((unsigned char)'M');
+        t_rec->val(p);
+        t_rec->val(v);
+        t_rec->val(n);
+        return;
+    }
+    CK(cudaMemsetAsync(p, v, n, s));
+}
+
 template <typename... KArgs, typename... Args>
 static void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+    if (t_rec) {
+        rec_launch(kern, dim3(grid), dim3(block), 0, g_use_pdl ? 1 : 0, args...);
+        return;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
@@ -967,6 +1016,10 @@ static void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaSt
 template <typename... KArgs, typename... Args>
 static void launch_pipe(void (*kern)(KArgs...), int nl, size_t smem, cudaStream_t s, Args... args) {
     const int g = std::min(nl, PIPE_CTAS);
+    if (t_rec) {
+        rec_launch(kern, dim3((unsigned)g), dim3(128), smem, g_use_pdl ? 1 : 0, args...);
+        return;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)g);
     cfg.blockDim = dim3(128);
@@ -1098,6 +1151,7 @@ struct Enq {
     // both mu-visits of level lb = nlev - 2 with their coarsest solves, in one cluster launch
     void bottom(int lb, float* lhs, const float* rhs, const float w[3]) {
         BottomArgs A;
+        memset(&A, 0, sizeof(A));  // padding included: the recorder compares argument bytes
         A.L = h->lv[lb].L;
         A.rhs = rhs;
         A.lhs = lhs;
@@ -1120,8 +1174,15 @@ struct Enq {
         at[1].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = at;
         cfg.numAttrs = g_use_pdl ? 2 : 1;
-        if (h->bot_rows == 2) CK(cudaLaunchKernelEx(&cfg, k_bottom<2>, A));
-        else CK(cudaLaunchKernelEx(&cfg, k_bottom<4>, A));
+        if (t_rec) {
+            const int attrs = (int)cfg.numAttrs * 1000 + h->bot_C;  // the cluster shape
+            if (h->bot_rows == 2) rec_launch(k_bottom<2>, cfg.gridDim, cfg.blockDim, cfg.dynamicSmemBytes, attrs, A);
+            else rec_launch(k_bottom<4>, cfg.gridDim, cfg.blockDim, cfg.dynamicSmemBytes, attrs, A);
+        } else if (h->bot_rows == 2) {
+            CK(cudaLaunchKernelEx(&cfg, k_bottom<2>, A));
+        } else {
+            CK(cudaLaunchKernelEx(&cfg, k_bottom<4>, A));
+        }
         pe();
         count++;
     }
@@ -1399,7 +1460,7 @@ static void enqueue_setup(Enq& E, cudaGraphConditionalHandle cond, int use_cond)
     uaamg_poisson* h = E.h;
     LevelDev& D0 = h->lv[0];
     const size_t n0 = (size_t)D0.L.nl * UAAMG_LEAF;
-    CK(cudaMemsetAsync(h->p, 0, n0 * 4, E.s));
+    enq_memset(h->p, 0, n0 * 4, E.s);
     E.pb("L0 mask inputs");
     launch(k_mask_vec, (unsigned)D0.L.nl, 128, E.s, D0.L, h->x);
     launch(k_mask_vec, (unsigned)D0.L.nl, 128, E.s, D0.L, h->b);
@@ -1453,9 +1514,93 @@ static int graph_key(const uaamg_poisson* h) {
     return k;
 }
 
+// ---------------------------------------------------------------------------
+// Solve-graph cache of the process.  A FLIP-style caller creates a fresh
+// hierarchy every substep, and a fresh handle's first solve runs host-driven
+// (capturing a graph costs about what it saves).  When a new handle's
+// recording (t_rec) equals the one a cached graph was captured from -- the same
+// kernels, shapes and argument bytes, i.e. its buffers sit where a destroyed
+// handle's did -- its first solve replays that graph.  A graph is captured
+// for the cache only for a recording seen once before, so a stream of
+// different hierarchies keeps the host-driven first solve.  The cache lives
+// on the heap for the whole process (no destruction after the CUDA runtime).
+struct SolveGraph {
+    std::vector<unsigned char> sig;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    int64_t setup = 0, body = 0, finish = 0;
+    ~SolveGraph() {
+        if (x) cudaGraphExecDestroy(x);
+        if (g) cudaGraphDestroy(g);
+    }
+};
+struct SolveGraphCache {
+    std::mutex mu;
+    std::vector<std::shared_ptr<SolveGraph>> graphs;  // most recent first
+    std::vector<uint64_t> seen;                       // recordings without a graph, most recent first
+    int64_t hits = 0, captures = 0;
+};
+static SolveGraphCache& solve_graph_cache() {
+    static SolveGraphCache* c = new SolveGraphCache();
+    return *c;
+}
+static constexpr size_t SGC_GRAPHS = 4, SGC_SEEN = 16;
+static bool g_solve_graph_cache = true;
+static uint64_t fnv1a(const std::vector<unsigned char>& v) {
+    uint64_t x = 1469598103934665603ull;
+    for (unsigned char c : v) x = (x ^ c) * 1099511628211ull;
+    return x;
+}
+
+// A recording's cached graph (hit), or whether to capture one for the cache:
+// true on its second sighting.
+static bool solve_graph_lookup(const std::vector<unsigned char>& sig, std::shared_ptr<SolveGraph>& hit) {
+    const uint64_t hs = fnv1a(sig);
+    SolveGraphCache& c = solve_graph_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    for (size_t i = 0; i < c.graphs.size(); ++i)
+        if (c.graphs[i]->sig == sig) {
+            hit = c.graphs[i];
+            c.graphs.erase(c.graphs.begin() + (long)i);
+            c.graphs.insert(c.graphs.begin(), hit);
+            c.hits++;
+            return false;
+        }
+    auto f = std::find(c.seen.begin(), c.seen.end(), hs);
+    if (f != c.seen.end()) {
+        c.seen.erase(f);
+        return true;
+    }
+    c.seen.insert(c.seen.begin(), hs);
+    if (c.seen.size() > SGC_SEEN) c.seen.pop_back();
+    return false;
+}
+// Hands a just-captured graph to the cache (the handle keeps a reference).
+static std::shared_ptr<SolveGraph> solve_graph_insert(std::vector<unsigned char> sig, cudaGraph_t g,
+                                                      cudaGraphExec_t x, int64_t setup, int64_t body,
+                                                      int64_t finish) {
+    auto sg = std::make_shared<SolveGraph>();
+    sg->sig = std::move(sig);
+    sg->g = g;
+    sg->x = x;
+    sg->setup = setup;
+    sg->body = body;
+    sg->finish = finish;
+    SolveGraphCache& c = solve_graph_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.graphs.insert(c.graphs.begin(), sg);
+    if (c.graphs.size() > SGC_GRAPHS) c.graphs.pop_back();
+    c.captures++;
+    return sg;
+}
+
 static void destroy_graph(uaamg_poisson* h) {
-    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->shared_graph) {
+        h->shared_graph.reset();
+    } else {
+        if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+        if (h->graph) cudaGraphDestroy(h->graph);
+    }
     h->graph_exec = nullptr;
     h->graph = nullptr;
     h->graph_key = -1;
@@ -1512,6 +1657,31 @@ static void build_graph(uaamg_poisson* h) {
     h->graph_key = graph_key(h);
 }
 
+// The recording of one PCG solve's enqueue (setup, body, finish) as the
+// graph captures it.
+static std::vector<unsigned char> record_solve(uaamg_poisson* h) {
+    LaunchRec rec;
+    rec.val((unsigned char)'P');
+    rec.val(g_use_pdl);
+    rec.val(h->ctx->device);
+    t_rec = &rec;
+    try {
+        Enq E{h, h->stream};
+        enqueue_setup(E, 0, 1);
+        rec.val((unsigned char)'|');
+        Enq B{h, h->body_stream};
+        enqueue_body(B, 0, 1);
+        rec.val((unsigned char)'|');
+        Enq F{h, h->stream};
+        enqueue_finish(F);
+    } catch (...) {
+        t_rec = nullptr;
+        throw;
+    }
+    t_rec = nullptr;
+    return std::move(rec.bytes);
+}
+
 static void init_state(uaamg_poisson* h) {
     PcgState s;
     memset(&s, 0, sizeof(s));
@@ -1534,10 +1704,32 @@ static int run_pcg(uaamg_poisson* h) {
     // A handle's first solve runs host-driven: capturing and instantiating the
     // graph costs about as much as the launches it saves, and a FLIP substep
     // solves each hierarchy once.  Later solves on the handle use the graph.
-    const bool use_graph = h->use_graph && (h->use_graph == 2 || h->solves > 0);
+    bool use_graph = h->use_graph && (h->use_graph == 2 || h->solves > 0);
+    std::shared_ptr<SolveGraph> hit;
+    std::vector<unsigned char> sig;
+    bool share = false;
+    if (!use_graph && h->use_graph == 1 && g_solve_graph_cache) {  // the cache may take this first solve
+        sig = record_solve(h);
+        share = solve_graph_lookup(sig, hit);
+        use_graph = hit || share;
+    }
     h->solves++;
     if (use_graph) {
-        if (!h->graph_exec || h->graph_key != graph_key(h)) build_graph(h);
+        if (hit) {
+            destroy_graph(h);
+            h->shared_graph = hit;
+            h->graph = hit->g;
+            h->graph_exec = hit->x;
+            h->graph_key = graph_key(h);
+            h->setup_launches = hit->setup;
+            h->body_launches = hit->body;
+            h->finish_launches = hit->finish;
+        } else if (!h->graph_exec || h->graph_key != graph_key(h)) {
+            build_graph(h);
+            if (share)
+                h->shared_graph = solve_graph_insert(std::move(sig), h->graph, h->graph_exec, h->setup_launches,
+                                                     h->body_launches, h->finish_launches);
+        }
         CK(cudaGraphLaunch(h->graph_exec, h->stream));
         CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -1656,6 +1848,8 @@ static int create_impl(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid*
         g_use_staged = !(e && e[0] == '0');
         e = getenv("UAAMG_BOTTOM");
         g_use_bottom = !(e && e[0] == '0');
+        e = getenv("UAAMG_SOLVE_GRAPH_CACHE");
+        g_solve_graph_cache = !(e && e[0] == '0');
     }
     if (!out) { set_error("out is NULL"); return UAAMG_ERR_INVALID_ARGUMENT; }
     *out = nullptr;
@@ -2267,5 +2461,13 @@ int uaamg_poisson_set_graph_mode(uaamg_poisson* h, int use_graph) {
     return UAAMG_SUCCESS;
 }
 int64_t uaamg_poisson_kernel_launches(const uaamg_poisson* h) { return h ? h->launches : 0; }
+
+int uaamg_solve_graph_cache_stats(int64_t* hits, int64_t* captures) {
+    SolveGraphCache& c = solve_graph_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (hits) *hits = c.hits;
+    if (captures) *captures = c.captures;
+    return UAAMG_SUCCESS;
+}
 
 }  // extern "C"

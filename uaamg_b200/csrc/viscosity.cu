@@ -267,6 +267,7 @@ struct uaamg_viscosity {
     int use_graph = 1;
     cudaGraphExec_t graph_exec = nullptr;
     cudaGraph_t graph = nullptr;
+    std::shared_ptr<SolveGraph> shared_graph;  // set when graph / graph_exec belong to the solve-graph cache
     int64_t setup_launches = 0, body_launches = 0, finish_launches = 0;
     int64_t launches = 0, last_launches = 0;
     int iterations = 0;
@@ -323,6 +324,10 @@ static DGrid vupload_grid(uaamg_viscosity* h, const uaamg_leaf_grid* gr) {
 template <typename... KArgs, typename... Args>
 static void launch2(void (*kern)(KArgs...), dim3 grid, unsigned block, cudaStream_t s, Args... args) {
     if (grid.x == 0 || grid.y == 0) return;
+    if (t_rec) {  // recording a solve for the solve-graph cache
+        rec_launch(kern, grid, dim3(block), 0, g_use_pdl ? 1 : 0, args...);
+        return;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = dim3(block);
@@ -773,10 +778,39 @@ static void venqueue_finish(VEnq& E) {
 }
 
 static void vdestroy_graph(uaamg_viscosity* h) {
-    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->shared_graph) {
+        h->shared_graph.reset();
+    } else {
+        if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+        if (h->graph) cudaGraphDestroy(h->graph);
+    }
     h->graph_exec = nullptr;
     h->graph = nullptr;
+}
+
+// The recording of one PCG solve's enqueue (setup, body, finish) as the
+// graph captures it (the solve-graph cache of poisson.cu).
+static std::vector<unsigned char> vrecord_solve(uaamg_viscosity* h) {
+    LaunchRec rec;
+    rec.val((unsigned char)'V');
+    rec.val(g_use_pdl);
+    rec.val(h->ctx->device);
+    t_rec = &rec;
+    try {
+        VEnq E{h, h->stream};
+        venqueue_setup(E, 0, 1);
+        rec.val((unsigned char)'|');
+        VEnq B{h, h->body_stream};
+        venqueue_body(B, 0, 1);
+        rec.val((unsigned char)'|');
+        VEnq F{h, h->stream};
+        venqueue_finish(F);
+    } catch (...) {
+        t_rec = nullptr;
+        throw;
+    }
+    t_rec = nullptr;
+    return std::move(rec.bytes);
 }
 
 static void vbuild_graph(uaamg_viscosity* h) {
@@ -846,10 +880,31 @@ static int vrun_pcg(uaamg_viscosity* h, std::vector<ProfRec>* prof = nullptr) {
     }
     vinit_state(h);
     int64_t launches = 0;
-    const bool use_graph = !prof && h->use_graph && (h->use_graph == 2 || h->solves > 0);
+    bool use_graph = !prof && h->use_graph && (h->use_graph == 2 || h->solves > 0);
+    std::shared_ptr<SolveGraph> hit;
+    std::vector<unsigned char> sig;
+    bool share = false;
+    if (!prof && !use_graph && h->use_graph == 1 && g_solve_graph_cache) {  // the cache may take this first solve
+        sig = vrecord_solve(h);
+        share = solve_graph_lookup(sig, hit);
+        use_graph = hit || share;
+    }
     h->solves++;
     if (use_graph) {
-        if (!h->graph_exec) vbuild_graph(h);
+        if (hit) {
+            vdestroy_graph(h);
+            h->shared_graph = hit;
+            h->graph = hit->g;
+            h->graph_exec = hit->x;
+            h->setup_launches = hit->setup;
+            h->body_launches = hit->body;
+            h->finish_launches = hit->finish;
+        } else if (!h->graph_exec) {
+            vbuild_graph(h);
+            if (share)
+                h->shared_graph = solve_graph_insert(std::move(sig), h->graph, h->graph_exec, h->setup_launches,
+                                                     h->body_launches, h->finish_launches);
+        }
         CK(cudaGraphLaunch(h->graph_exec, h->stream));
         CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -971,6 +1026,8 @@ int uaamg_viscosity_create_on_stream(const uaamg_leaf_grid* viscosity, const uaa
     {
         const char* e = getenv("UAAMG_PDL");
         g_use_pdl = !(e && e[0] == '0');
+        e = getenv("UAAMG_SOLVE_GRAPH_CACHE");
+        g_solve_graph_cache = !(e && e[0] == '0');
     }
     if (!out) { set_error("out is NULL"); return UAAMG_ERR_INVALID_ARGUMENT; }
     *out = nullptr;

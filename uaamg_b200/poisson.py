@@ -226,6 +226,15 @@ class LaplacianWithLevel:
         return out
 
 
+def solve_graph_cache_stats() -> tuple[int, int]:
+    """(hits, captures) of the process's solve-graph cache: first solves that
+    replayed a graph captured for an earlier handle with the same launch
+    sequence, and graphs captured into the cache (uaamg_solve_graph_cache_stats)."""
+    hits, caps = C.c_int64(0), C.c_int64(0)
+    _lib.check(_lib.lib().uaamg_solve_graph_cache_stats(C.byref(hits), C.byref(caps)), "solve_graph_cache_stats")
+    return int(hits.value), int(caps.value)
+
+
 class PoissonSolver:
     """PCG with the unsmoothed-aggregation mu-cycle (mu = 2) as preconditioner."""
 
