@@ -27,7 +27,32 @@ u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 def build() -> str:
     path = os.path.join(_HERE, "liboracle.so")
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    if os.path.isdir(REFERENCE_ROOT):  # the reference's own helpers, where its sources are present
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={REFERENCE_ROOT}"], check=True)
     return path
+
+
+# Where build() finds the reference's sources; the built _ref/ libraries travel
+# without them.
+REFERENCE_ROOT = os.environ.get("UAAMG_REFERENCE_ROOT", "/root/reference")
+REF_LIB = os.path.join(_HERE, "_ref", "libuaamg_ref.so")
+REF_LIB_NATIVE = os.path.join(_HERE, "_ref", "libuaamg_ref_native.so")
+
+
+def ref_lib(native: bool = False):
+    """The reference's scalar helpers built from its own sources (None when
+    oracle/_ref was not built)."""
+    path = REF_LIB_NATIVE if native else REF_LIB
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    L.ref_fraction_inside2.argtypes = [C.c_float] * 2
+    L.ref_fraction_inside4.argtypes = [C.c_float] * 4
+    L.ref_volume_fraction_tet.argtypes = [C.c_float] * 4
+    L.ref_volume_fraction_cube.argtypes = [C.c_float] * 8
+    for f in ("ref_fraction_inside2", "ref_fraction_inside4", "ref_volume_fraction_tet", "ref_volume_fraction_cube"):
+        getattr(L, f).restype = C.c_float
+    return L
 
 
 def lib():
@@ -104,6 +129,12 @@ def lib():
         L.orc_visc_dot.restype = C.c_float
         L.orc_fraction_inside4.argtypes = [C.c_float] * 4
         L.orc_fraction_inside4.restype = C.c_float
+        L.orc_fraction_inside2.argtypes = [C.c_float] * 2
+        L.orc_fraction_inside2.restype = C.c_float
+        L.orc_tet_fraction.argtypes = [C.c_float] * 4
+        L.orc_tet_fraction.restype = C.c_float
+        L.orc_cube_fraction.argtypes = [C.c_float] * 8
+        L.orc_cube_fraction.restype = C.c_float
         L.orc_face_weights.argtypes = [C.c_int64, i32p, f32p, C.c_float, C.c_int64, i32p, vp, f32p]
         L.orc_pressure_gradient.argtypes = [C.c_int64, i32p, f32p, C.c_float, C.c_int64, i32p, f32p, f32p,
                                             C.c_int64, i32p, f32p, f32p, C.c_int64, i32p, u64p, f32p,

@@ -168,6 +168,7 @@ static inline float fraction_inside1(float l, float r) {
     if (l >= 0 && r < 0) return r / (r - l);
     return 0;
 }
+float orc_fraction_inside2(float l, float r) { return fraction_inside1(l, r); }
 
 /* ------------------------------------------------------------------------ */
 /* Level 0: BuildFinestMatrix (simd_vdb_poisson.cpp:474-597) + initializeFinest (:600-635) */

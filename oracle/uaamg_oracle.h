@@ -192,6 +192,12 @@ float orc_visc_dot(const orc_visc* h, int level, const float* a, const float* b)
 /* ------------------------------------------------------------------------ */
 /* The steps either side of the pressure solve (projection_oracle.c). */
 float orc_fraction_inside4(float phi_bl, float phi_br, float phi_tl, float phi_tr);
+/* the restated scalar helpers, for the tests that pin them against the
+ * reference's own build (oracle/_ref) */
+float orc_fraction_inside2(float l, float r);
+float orc_tet_fraction(float p0, float p1, float p2, float p3);
+float orc_cube_fraction(float p000, float p100, float p010, float p110, float p001, float p101, float p011,
+                        float p111);
 void orc_face_weights(int64_t solid_n, const int32_t* solid_origins, const float* solid_values, float solid_bg,
                       int64_t n, const int32_t* origins, const uint64_t* masks, float* out);
 void orc_pressure_gradient(int64_t phi_n, const int32_t* phi_origins, const float* phi_values, float phi_bg,

@@ -157,6 +157,11 @@ static float cube_fraction(float p000, float p100, float p010, float p110, float
             tet_fraction(p001, p111, p011, p010) + 2 * tet_fraction(p100, p111, p001, p010)) /
            12;
 }
+float orc_tet_fraction(float p0, float p1, float p2, float p3) { return tet_fraction(p0, p1, p2, p3); }
+float orc_cube_fraction(float p000, float p100, float p010, float p110, float p001, float p101, float p011,
+                        float p111) {
+    return cube_fraction(p000, p100, p010, p110, p001, p101, p011, p111);
+}
 
 /* ------------------------------------------------------------------------ */
 /* a float field over a leaf set with getValue semantics */
