@@ -21,6 +21,31 @@ from .grids import LeafGrid
 
 
 def _as_c(grid: LeafGrid, keep: list) -> _lib.LeafGridC:
+    """The C view of a leaf grid (pointers into its arrays).  A grid passed
+    again with the same arrays (the same objects, the same tensor storage)
+    reuses the view built the first time: a FLIP loop hands the same input
+    grids to every substep."""
+    vals = grid.values
+    key = (id(grid.origins), id(grid.masks), id(vals), grid.leaf_count, grid.components,
+           vals.data_ptr() if hasattr(vals, "data_ptr") else None,
+           np.asarray(grid.background, np.float32).tobytes())
+    cached = getattr(grid, "_c_view", None)
+    if cached is not None and cached[0] == key:
+        keep.extend(cached[2])
+        return cached[1]
+    mine: list = []
+    g = _as_c_build(grid, mine)
+    keep.extend(mine)
+    # only a view of the grid's own arrays is kept: a converted copy would miss later in-place writes
+    if all(a is grid.origins or a is grid.masks or a is vals for a in mine):
+        try:
+            grid._c_view = (key, g, mine)
+        except AttributeError:  # a grid type without a writable __dict__
+            pass
+    return g
+
+
+def _as_c_build(grid: LeafGrid, keep: list) -> _lib.LeafGridC:
     g = _lib.LeafGridC()
     g.leaf_count = grid.leaf_count
     org = np.ascontiguousarray(grid.origins, dtype=np.int32)
