@@ -504,6 +504,40 @@ def test_bottom_cycle_cluster_kernel_identical(gpu, n):
         assert sum(v[1] for v in prof_on.values()) < sum(v[1] for v in prof_off.values())
 
 
+@pytest.mark.parametrize("n,bottom", [(64, "1"), (128, "1"), (96, "0")])
+def test_fused_jacobi_pairs_identical(gpu, monkeypatch, n, bottom):
+    """Two consecutive Jacobi sweeps of a mid-size level (64 to 1023 leaves)
+    run as one k_sweep2 launch, the first sweep recomputed on the face layers
+    of each leaf's neighbours.  Preconditioner and PCG (graph and host loop,
+    both Jacobi smoothers) are bit-identical to the separate sweeps
+    (UAAMG_SWEEP2=0 at handle creation), with and without the cluster bottom
+    kernel, and the profile shows the pairs in place of sweeps."""
+    torch = gpu
+    from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver
+    monkeypatch.setenv("UAAMG_BOTTOM", bottom)
+    sc = scenes.plain_poisson_scene(n=n, seed=3)
+    monkeypatch.setenv("UAAMG_SWEEP2", "0")
+    lap_off = LaplacianWithLevel.createPressurePoissonLaplacian(sc.phi, sc.face_weights, sc.dt, sc.dx)
+    monkeypatch.setenv("UAAMG_SWEEP2", "1")
+    lap_on = LaplacianWithLevel.createPressurePoissonLaplacian(sc.phi, sc.face_weights, sc.dt, sc.dx)
+    rhs = lap_on.createPressurePoissonRightHandSide(sc.face_weights, sc.vx, sc.vy, sc.vz, sc.solid_velocity, sc.dt)
+    for sm in (PoissonSolver.SmootherOption.ScheduledRelaxedJacobi, PoissonSolver.SmootherOption.WeightedJacobi):
+        s_off, s_on = PoissonSolver(lap_off), PoissonSolver(lap_on)
+        s_off.mSmoother = s_on.mSmoother = sm
+        assert np.array_equal(s_off.precondition(rhs), s_on.precondition(rhs))
+        for graph in (0, 2):
+            s_off.use_graph = s_on.use_graph = graph
+            p_off, p_on = lap_on.getZeroVectorGrid(), lap_on.getZeroVectorGrid()
+            st_off, st_on = s_off.solveMultigridPCG(p_off, rhs), s_on.solveMultigridPCG(p_on, rhs)
+            assert st_off == st_on == 0 and s_off.mIterationTaken == s_on.mIterationTaken
+            assert np.array_equal(p_off, p_on)
+        d = torch.from_numpy(rhs).cuda()
+        prof_on = s_on.profile_pcg(torch.zeros_like(d), d)
+        prof_off = s_off.profile_pcg(torch.zeros_like(d), d)
+        assert any("jacobi pair" in k for k in prof_on) and not any("jacobi pair" in k for k in prof_off)
+        assert sum(v[1] for v in prof_on.values()) < sum(v[1] for v in prof_off.values())
+
+
 def test_torch_stream_ordering(gpu):
     """Device inputs that torch's current stream is still writing when a call
     is made: the Python classes order the handle's stream after torch's and

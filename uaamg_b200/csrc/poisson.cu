@@ -370,6 +370,7 @@ struct LevelDev {
     float* lhs = nullptr;
     float* rhs = nullptr;
     float* tmp = nullptr;
+    float* tmp2 = nullptr;  // second scratch vector: the intermediate of a fused sweep pair (k_sweep2)
     float* spai0 = nullptr;
     uint32_t* flags = nullptr;
     int* spai0_ready = nullptr;
@@ -417,6 +418,7 @@ struct uaamg_poisson {
     cudaGraph_t graph = nullptr;
     int graph_key = -1;
     std::shared_ptr<struct SolveGraph> shared_graph;  // set when graph / graph_exec belong to the solve-graph cache
+    bool use_sweep2 = true;  // fused Jacobi sweep pairs (Enq::pair), fixed at creation
     int64_t body_launches = 0, setup_launches = 0, finish_launches = 0;
     int64_t launches = 0;
     int64_t last_launches = 0;
@@ -739,7 +741,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             size_t n = (size_t)H.nl;
             bytes += carve_size(n * 8, 8) + carve_size(n * 6, 4) + carve_size(n * 8, 4) + carve_size(n, 4) +
                      carve_size(n, 1) + carve_size(n, 4) + carve_size(n * 3, 4) + carve_size(n, 4) + carve_size(1, 4);
-            bytes += 10 * carve_size(n * UAAMG_LEAF, 4);  // diag cx cy cz invdiag spai0 lhs rhs tmp (+1 spare)
+            bytes += 10 * carve_size(n * UAAMG_LEAF, 4);  // diag cx cy cz invdiag spai0 lhs rhs tmp tmp2
         }
         const HostLevel& HC = h->host.back();
         size_t nc = (size_t)HC.ndof;
@@ -806,7 +808,7 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             D.lhs = carve<float>(cur2, n * UAAMG_LEAF);
             D.rhs = carve<float>(cur2, n * UAAMG_LEAF);
             D.tmp = carve<float>(cur2, n * UAAMG_LEAF);
-            carve<float>(cur2, n * UAAMG_LEAF);
+            D.tmp2 = carve<float>(cur2, n * UAAMG_LEAF);
             const float t = H.dt / (H.dx * H.dx);  // LaplacianApplySIMD ctor (.cpp:1045-1065)
             DLevel& L = D.L;
             const Tab& T = tabs[l];
@@ -918,6 +920,7 @@ static bool g_use_pdl = true;
 // Level sweeps with SrcPlain on levels of at least STAGED_MIN_LEAVES leaves run
 // the bulk-async staged kernels (UAAMG_STAGED=0 turns them off).
 static bool g_use_staged = true;
+static bool g_use_sweep2 = true;  // fused Jacobi sweep pairs (Enq::pair)
 // Kernel shapes by level size (uaamg_set_tuning): the defaults below, or the
 // table an autotuner wrote.  Every choice gives the same results; only the
 // speed differs.  g_tune_gen is part of every graph's key, so a change rebuilds
@@ -1121,6 +1124,22 @@ struct Enq {
         count++;
     }
     bool split(int l) const { return g_use_staged && h->lv[l].L.nl >= SPLIT_MIN_LEAVES; }
+    // whether two consecutive Jacobi sweeps of level l run as one k_sweep2:
+    // latency-bound levels of about one wave at 2 CTAs per SM (from the staged
+    // size on); on larger levels the face-layer recomputation costs more than
+    // the launch it saves (measured: 776 and 784 leaves slower, 120-284 faster)
+    bool pair(int l) const {
+        const int nl = h->lv[l].L.nl;
+        return h->use_sweep2 && !split(l) && nl >= STAGED_MIN_LEAVES && nl <= 2 * g_sms;
+    }
+    template <class Src>
+    void sweep2(int l, const Src& src, const float* b, float* out, float wa, float wb) {
+        LevelDev& D = h->lv[l];
+        if (prof) pb("L" + std::to_string(l) + " jacobi pair" + SrcName<Src>::get());
+        launch(k_sweep2<Src>, (unsigned)D.L.nl, SW2_THREADS, s, D.L, src, b, out, wa, wb);
+        pe();
+        count++;
+    }
     template <class Src>
     void materialize(int l, const Src& src, float* out) {
         LevelDev& D = h->lv[l];
@@ -1346,16 +1365,21 @@ static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool sk
             else E.sweep<M_JACOBI>(l, SrcPlain{T}, rhs, lhs, wpre(1));
         } else if (spai) {
             E.sweep<M_SPAI0>(l, SrcFirstSpai0{rhs, D.spai0_ready}, rhs, lhs, 0.f);
+        } else if (E.pair(l)) {  // first sweep from zero + second + third in one launch, into T
+            E.sweep2(l, SrcFirstJacobi{rhs, wpre(0)}, rhs, T, wpre(1), wpre(2));
         } else {
             E.sweep<M_JACOBI>(l, SrcFirstJacobi{rhs, wpre(0)}, rhs, lhs, wpre(1));
         }
         if (spai) E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f, DotOut{nullptr, nullptr, nullptr}, true);
-        else E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(2));
+        else if (E.split(l) || !E.pair(l)) E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(2));
     } else {
         if (spai) {
             E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f, DotOut{nullptr, nullptr, nullptr}, true);
             E.sweep<M_SPAI0>(l, SrcPlain{T}, rhs, lhs, 0.f);
             E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f);
+        } else if (E.pair(l)) {  // the first two sweeps in one launch through tmp2
+            E.sweep2(l, SrcPlain{lhs}, rhs, D.tmp2, wpre(0), wpre(1));
+            E.sweep<M_JACOBI>(l, SrcPlain{D.tmp2}, rhs, T, wpre(2));
         } else {
             E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(0));
             E.sweep<M_JACOBI>(l, SrcPlain{T}, rhs, lhs, wpre(1));
@@ -1389,6 +1413,9 @@ static void enqueue_precond(Enq& E, int l, float* lhs, const float* rhs, bool sk
         E.sweep<M_SPAI0>(l, SrcProlong{T, P.lhs, 1.0f}, rhs, lhs, 0.f);
         E.sweep<M_SPAI0>(l, SrcPlain{lhs}, rhs, T, 0.f);
         E.sweep<M_SPAI0>(l, SrcPlain{T}, rhs, lhs, 0.f, dot);
+    } else if (E.pair(l)) {  // prolongation + the first two sweeps in one launch through tmp2
+        E.sweep2(l, SrcProlong{T, P.lhs, 1.0f}, rhs, D.tmp2, wpre(2), wpre(1));
+        E.sweep<M_JACOBI>(l, SrcPlain{D.tmp2}, rhs, lhs, wpre(0), dot);
     } else {
         E.sweep<M_JACOBI>(l, SrcProlong{T, P.lhs, 1.0f}, rhs, lhs, wpre(2));
         E.sweep<M_JACOBI>(l, SrcPlain{lhs}, rhs, T, wpre(1));
@@ -1850,6 +1877,8 @@ static int create_impl(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid*
         g_use_bottom = !(e && e[0] == '0');
         e = getenv("UAAMG_SOLVE_GRAPH_CACHE");
         g_solve_graph_cache = !(e && e[0] == '0');
+        e = getenv("UAAMG_SWEEP2");
+        g_use_sweep2 = !(e && e[0] == '0');
     }
     if (!out) { set_error("out is NULL"); return UAAMG_ERR_INVALID_ARGUMENT; }
     *out = nullptr;
@@ -1872,6 +1901,7 @@ static int create_impl(const uaamg_leaf_grid* liquid_phi, const uaamg_leaf_grid*
         h->scalar_host = reinterpret_cast<float*>((char*)h->pin_state + ((sizeof(PcgState) + 63) & ~size_t(63)));
         noalloc_resolve(h);
         h->bot_state = (g_use_bottom && g_tune.bottom_cycle) ? -1 : 0;
+        h->use_sweep2 = g_use_sweep2;
         {
             int sms = 0;
             if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->ctx->device) == cudaSuccess && sms > 0)

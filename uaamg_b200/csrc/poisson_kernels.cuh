@@ -188,7 +188,10 @@ __device__ __forceinline__ void stencil_static(const DLevel& L, int leaf, int t,
 // The 6-neighbour off-diagonal sum of one float4 (4 z-consecutive voxels):
 // off = ((x+ c_x+ + x- c_x-) + (y+ c_y+ + y- c_y-)) + (z+ c_z+ + z- c_z-)
 // with c_k- this voxel's minus-face entry and c_k+ the +k neighbour's.
-template <class Src>
+// SHFL: the partner half of the thread's z-line (thread t ^ 1, same warp)
+// supplies x and c_z at z = 4 / 3 by shuffle; without it they are loaded
+// (the same values), for threads whose partner computes something else.
+template <class Src, bool SHFL = true>
 __device__ __forceinline__ void stencil_dyn(const DLevel& L, int leaf, int t, const Src& src, const PStatic& S,
                                             float4& xc, float4& off) {
     const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1;
@@ -202,10 +205,20 @@ __device__ __forceinline__ void stencil_dyn(const DLevel& L, int leaf, int t, co
     else yp = S.nyp >= 0 ? src.get4(L, S.nyp, t - 14) : f4zero();
     if (Y > 0) ym = src.get4(L, leaf, t - 2);
     else ym = S.nym >= 0 ? src.get4(L, S.nym, t + 14) : f4zero();
-    const float px = __shfl_xor_sync(FULLMASK, xc.x, 1);
-    const float pw = __shfl_xor_sync(FULLMASK, xc.w, 1);
-    const float pcz = __shfl_xor_sync(FULLMASK, S.czo.x, 1);
     const int base = 4 * t;
+    float px, pw, pcz;
+    if constexpr (SHFL) {
+        px = __shfl_xor_sync(FULLMASK, xc.x, 1);
+        pw = __shfl_xor_sync(FULLMASK, xc.w, 1);
+        pcz = __shfl_xor_sync(FULLMASK, S.czo.x, 1);
+    } else if (zh == 0) {  // partner t + 1: z = 4..7
+        px = src.get1(L, leaf, base + 4);
+        pcz = (S.fl & TRIM_Z) ? L.def_face : L.cz[(long long)leaf * UAAMG_LEAF + base + 4];
+        pw = 0.f;
+    } else {  // partner t - 1: z = 0..3
+        pw = src.get1(L, leaf, base - 1);
+        px = pcz = 0.f;
+    }
     float zp3, zm0, czp3;
     if (zh == 0) {
         zp3 = px;
@@ -400,12 +413,12 @@ __device__ __forceinline__ void sweep_static(const DLevel& L, int leaf, int t, S
     if (MODE == M_SPAI0) S.sp = (fl & TRIM_SPAI0) ? f4splat(L.def_spai0) : ld4(L.spai0, leaf, t);
 }
 
-template <int MODE, class Src>
+template <int MODE, class Src, bool SHFL = true>
 __device__ __forceinline__ float4 sweep_value_s(const DLevel& L, int leaf, int t, const Src& src, const float* b,
                                                 float w, float wsor, float one_minus_wsor, const SStatic& S,
                                                 float4& xc, unsigned& m) {
     float4 off;
-    stencil_dyn(L, leaf, t, src, S.P, xc, off);
+    stencil_dyn<Src, SHFL>(L, leaf, t, src, S.P, xc, off);
     m = S.m;
     float4 res = f4zero();
     if (MODE == M_RED || MODE == M_BLACK) {
@@ -515,6 +528,110 @@ template <int MODE, class Src>
 __global__ void __launch_bounds__(128) k_sweep(DLevel L, Src src, const float* b, float* out, float w, float wsor,
                                                float one_minus_wsor, DotOut dot, int* spai0_ready) {
     sweep_leaf<MODE, Src, true>(L, blockIdx.x, gridDim.x, src, b, out, w, wsor, one_minus_wsor, dot, spai0_ready);
+}
+
+// ---------------------------------------------------------------------------
+// Two Jacobi sweeps in one launch: out = J_wb(J_wa(src)).  The second sweep at a
+// voxel reads the first sweep's result at its six neighbours, so a CTA computes
+// the first sweep for its leaf and for the face layers of its six neighbours
+// (the values the neighbouring CTAs compute too, from the same inputs with the
+// same operations: bit-identical), keeps them in a 10^3 shared cube and then
+// does the second sweep on its leaf.  Results are those of two k_sweep
+// launches.  src must not read `out` (neighbouring CTAs still read src).
+// Threads: 0-127 the leaf's 4-voxel groups; 128-191 the groups of the -x, +x,
+// -y, +y neighbours' face planes (x or y = 7 or 0 in that leaf); 192-319 one
+// group of the -z / +z neighbours per (x, y) of the face, holding the voxel at
+// z = 7 / 0.  The face groups compute without warp shuffles (their partner
+// thread is not their z-line's other half).
+#define SW2_THREADS 320
+__device__ __forceinline__ int sw2_idx(int X, int Y, int Z) { return ((X + 1) * 10 + (Y + 1)) * 10 + (Z + 1); }
+template <class Src>
+__global__ void __launch_bounds__(SW2_THREADS, 2) k_sweep2(DLevel L, Src src, const float* b, float* out, float wa,
+                                                           float wb) {
+    __shared__ float cube[1000];
+    const int t = threadIdx.x;
+    const int leaf = blockIdx.x;
+    const int* nb = L.nbr + (long long)leaf * 6;
+    // the group this thread computes in the first sweep: leaf gl, group gt; cube origin (cX, cY, cZ0)
+    int gl = leaf, gt = t, cX = t >> 4, cY = (t >> 1) & 7, cZ0 = 4 * (t & 1), zlane = -1;
+    if (t >= 128 && t < 192) {
+        const int h = t - 128, face = h >> 4, u = (h >> 1) & 7, zh = h & 1;
+        gl = nb[face];
+        cZ0 = 4 * zh;
+        if (face < 2) {
+            const int Xn = face == 0 ? 7 : 0;
+            gt = (Xn << 4) | (u << 1) | zh;
+            cX = face == 0 ? -1 : 8;
+            cY = u;
+        } else {
+            const int Yn = face == 2 ? 7 : 0;
+            gt = (u << 4) | (Yn << 1) | zh;
+            cX = u;
+            cY = face == 2 ? -1 : 8;
+        }
+    } else if (t >= 192) {
+        const int h = t - 192, zf = h >> 6, X = (h >> 3) & 7, Y = h & 7;
+        gl = nb[4 + zf];             // -z neighbour (its z = 4..7 group), then +z (its z = 0..3 group)
+        gt = (X << 4) | (Y << 1) | (zf ? 0 : 1);
+        cX = X;
+        cY = Y;
+        zlane = zf ? 0 : 3;          // the voxel at cube z = 8 / -1
+        cZ0 = zf ? 8 : -4;
+    }
+    SStatic S;
+    if (gl >= 0) sweep_static<M_JACOBI>(L, gl, gt, S);
+    griddep_wait();
+    griddep_launch();
+    float4 T = f4zero(), xc;
+    unsigned m = 0;
+    if (t < 128) T = sweep_value_s<M_JACOBI, Src, true>(L, leaf, t, src, b, wa, 0.f, 1.f, S, xc, m);
+    else if (gl >= 0) T = sweep_value_s<M_JACOBI, Src, false>(L, gl, gt, src, b, wa, 0.f, 1.f, S, xc, m);
+    if (zlane < 0) {
+        const int base = sw2_idx(cX, cY, cZ0);
+        cube[base] = T.x;
+        cube[base + 1] = T.y;
+        cube[base + 2] = T.z;
+        cube[base + 3] = T.w;
+    } else {
+        cube[sw2_idx(cX, cY, cZ0 + zlane)] = f4get(T, zlane);
+    }
+    __syncthreads();
+    if (t >= 128) return;
+    // second sweep on the leaf: stencil_dyn's operations with the first sweep's values from the cube
+    const int X = t >> 4, Y = (t >> 1) & 7, zh = t & 1, Z0 = 4 * zh;
+    const float pcz = __shfl_xor_sync(FULLMASK, S.P.czo.x, 1);
+    const float czp3 = zh == 0 ? pcz : S.P.czp3;
+    const float czp[4] = {S.P.czo.y, S.P.czo.z, S.P.czo.w, czp3};
+    float4 off;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int Z = Z0 + j;
+        float f1 = __fmul_rn(cube[sw2_idx(X + 1, Y, Z)], f4get(S.P.cxp, j));
+        float f2 = __fmul_rn(cube[sw2_idx(X - 1, Y, Z)], f4get(S.P.cxm, j));
+        float f3 = __fmul_rn(cube[sw2_idx(X, Y + 1, Z)], f4get(S.P.cyp, j));
+        float f4 = __fmul_rn(cube[sw2_idx(X, Y - 1, Z)], f4get(S.P.cym, j));
+        float f5 = __fmul_rn(cube[sw2_idx(X, Y, Z + 1)], czp[j]);
+        float f6 = __fmul_rn(cube[sw2_idx(X, Y, Z - 1)], f4get(S.P.czo, j));
+        f1 = __fadd_rn(f1, f2);
+        f3 = __fadd_rn(f3, f4);
+        f5 = __fadd_rn(f5, f6);
+        f1 = __fadd_rn(f1, f3);
+        f1 = __fadd_rn(f1, f5);
+        f4set(off, j, f1);
+    }
+    const float4 bb = ld4(b, leaf, t);
+    float4 res;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float r = __fsub_rn(f4get(bb, j), __fmaf_rn(f4get(T, j), f4get(S.dg, j), f4get(off, j)));
+        r = __fmul_rn(r, f4get(S.iv, j));
+        f4set(res, j, __fmaf_rn(wb, r, f4get(T, j)));
+    }
+    if (!(m & 1)) res.x = 0.f;
+    if (!(m & 2)) res.y = 0.f;
+    if (!(m & 4)) res.z = 0.f;
+    if (!(m & 8)) res.w = 0.f;
+    st4(out, leaf, t, res);
 }
 
 // out = value of a source (materialise a first sweep or a prolongation)
