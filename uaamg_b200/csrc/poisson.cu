@@ -335,6 +335,12 @@ struct PinStage {
         off = (off + bytes + 15) & ~size_t(15);
         return p;
     }
+    void* reserve(size_t bytes) {  // pinned space for a download, or nullptr
+        if (!base || off + bytes > cap) return nullptr;
+        char* p = base + off;
+        off = (off + bytes + 15) & ~size_t(15);
+        return p;
+    }
 };
 
 struct DevGrid {  // device copy of an input grid + its leaf map
@@ -697,8 +703,22 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         k_finest_mask<<<(unsigned)nphi, 128, 0, s>>>(dphi.g, pm, dphiorg, dfw.g, dtOverDxSqr, ddofmask);
         CHECK_LAUNCH();
         h->launches++;
-        std::vector<uint64_t> dofmask((size_t)nphi * 8);
-        CK(cudaMemcpyAsync(dofmask.data(), ddofmask, (size_t)nphi * 64, cudaMemcpyDeviceToHost, s));
+        // the DOF masks come back into pinned memory, so the copy does not hold the host
+        std::vector<uint64_t> dofmask_pageable;
+        uint64_t* dofmask = static_cast<uint64_t*>(stage.reserve((size_t)nphi * 64));
+        if (!dofmask) {
+            dofmask_pageable.resize((size_t)nphi * 8);
+            dofmask = dofmask_pageable.data();
+        }
+        CK(cudaMemcpyAsync(dofmask, ddofmask, (size_t)nphi * 64, cudaMemcpyDeviceToHost, s));
+        // while the mask kernel and its copy run: the tree-order key of every liquid-SDF leaf, and whether
+        // the leaves are in tree order already (as an OpenVDB leaf iteration gives them)
+        std::vector<unsigned __int128> pkey((size_t)nphi);
+        bool phi_sorted = true;
+        for (int64_t i = 0; i < nphi; ++i) {
+            pkey[i] = vdb_key128(&phi->origins[3 * i]);
+            if (i > 0 && pkey[i] < pkey[i - 1]) phi_sorted = false;
+        }
         CK(cudaStreamSynchronize(s));
         TRACE("DOF mask kernel + D2H");
         // ---- level-0 DOF leaves in tree order
@@ -707,10 +727,9 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         for (int64_t i = 0; i < nphi; ++i) {
             uint64_t any = 0;
             for (int w = 0; w < 8; ++w) any |= dofmask[8 * i + w];
-            if (any) keys.push_back({vdb_key128(&phi->origins[3 * i]), (int)i});
+            if (any) keys.push_back({pkey[i], (int)i});
         }
-        // inputs from an OpenVDB leaf iteration are in tree order already
-        if (!std::is_sorted(keys.begin(), keys.end())) std::sort(keys.begin(), keys.end());
+        if (!phi_sorted) std::sort(keys.begin(), keys.end());  // a subset of sorted leaves is sorted
         TRACE("  level-0 leaves ordered");
         std::vector<int32_t> src(keys.size());
         L0.org.resize(keys.size() * 3);
