@@ -265,7 +265,11 @@ def torch_ordered(kind: str, h, *objs):
         return
     import torch
     cur = torch.cuda.current_stream()
-    ext = torch.cuda.ExternalStream(handle_stream(kind, h))
+    hs = handle_stream(kind, h)
+    if hs == cur.cuda_stream:  # the handle runs on torch's stream: ordered already
+        yield
+        return
+    ext = torch.cuda.ExternalStream(hs)
     ext.wait_stream(cur)
     try:
         yield
@@ -287,4 +291,7 @@ def torch_after(kind: str, h, *objs) -> None:
     waits for the new handle's stream (kernels still reading the inputs)."""
     if is_cuda(*objs):
         import torch
-        torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(handle_stream(kind, h)))
+        cur = torch.cuda.current_stream()
+        hs = handle_stream(kind, h)
+        if hs != cur.cuda_stream:
+            cur.wait_stream(torch.cuda.ExternalStream(hs))

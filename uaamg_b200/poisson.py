@@ -83,6 +83,9 @@ class LaplacianWithLevel:
         self.mDt = dt
         self.mDxThisLevel = dx
         self.mLevel = 0
+        # solver settings last applied to the handle (smoother, max iterations,
+        # relative tolerance, graph mode): a new handle holds these defaults
+        self._applied = (0, 100, 1e-7, 1)
 
     @staticmethod
     def createPressurePoissonLaplacian(liquid_phi: LeafGrid, face_weights: LeafGrid, dt: float,
@@ -282,13 +285,17 @@ class PoissonSolver:
 
     def _configure(self):
         L = _lib.lib()
-        h = self.mMultigridHierarchy._h
-        _lib.check(L.uaamg_poisson_set_smoother(h, int(self.mSmoother)), "set_smoother")
-        _lib.check(L.uaamg_poisson_set_max_iterations(h, int(self.mMaxIteration)), "set_max_iterations")
-        _lib.check(L.uaamg_poisson_set_relative_tolerance(h, float(self.mRelativeTolerance)), "set_tolerance")
+        lvl = self.mMultigridHierarchy
+        h = lvl._h
         mode = self.use_graph if isinstance(self.use_graph, int) and not isinstance(self.use_graph, bool) \
             else (1 if self.use_graph else 0)
-        _lib.check(L.uaamg_poisson_set_graph_mode(h, mode), "set_graph_mode")
+        want = (int(self.mSmoother), int(self.mMaxIteration), float(self.mRelativeTolerance), int(mode))
+        if getattr(lvl, "_applied", None) != want:  # the handle keeps its settings between solves
+            _lib.check(L.uaamg_poisson_set_smoother(h, want[0]), "set_smoother")
+            _lib.check(L.uaamg_poisson_set_max_iterations(h, want[1]), "set_max_iterations")
+            _lib.check(L.uaamg_poisson_set_relative_tolerance(h, want[2]), "set_tolerance")
+            _lib.check(L.uaamg_poisson_set_graph_mode(h, want[3]), "set_graph_mode")
+            lvl._applied = want
         return L, h
 
     def _solve(self, host_fn, dev_fn, pressure, rhs) -> int:
