@@ -48,6 +48,53 @@ static void sort_unique_vdb(std::vector<int32_t>& org) {
     }
     org.swap(out);
 }
+// Tree order of distinct leaves listed by a dense x-major scan of their cells:
+// inside one 128^3 node the tree order is the x-major order of the node's
+// leaf cells (vdb_key's last field), which the scan already follows, so only
+// the nodes need ordering -- a counting pass by node rank, with the few nodes
+// sorted by key, instead of a sort of every leaf's 128-bit key.
+static void order_dense_scan(std::vector<int32_t>& org) {
+    const size_t n = org.size() / 3;
+    if (n < 2) return;
+    int lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    for (size_t i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) {
+            const int v = org[3 * i + c] >> 7;
+            lo[c] = std::min(lo[c], v);
+            hi[c] = std::max(hi[c], v);
+        }
+    const int64_t d1 = hi[1] - lo[1] + 1, d2 = hi[2] - lo[2] + 1;
+    const int64_t ncell = (hi[0] - lo[0] + 1) * d1 * d2;
+    if (ncell == 1) return;
+    std::vector<uint32_t> cnt((size_t)ncell, 0), cell(n);
+    for (size_t i = 0; i < n; ++i) {
+        cell[i] = (uint32_t)(((int64_t)((org[3 * i] >> 7) - lo[0]) * d1 + ((org[3 * i + 1] >> 7) - lo[1])) * d2 +
+                             ((org[3 * i + 2] >> 7) - lo[2]));
+        cnt[cell[i]]++;
+    }
+    std::vector<std::pair<unsigned __int128, uint32_t>> nodes;
+    for (int64_t k = 0; k < ncell; ++k)
+        if (cnt[(size_t)k]) {
+            const int32_t o[3] = {(int32_t)((k / (d1 * d2) + lo[0]) * 128), (int32_t)(((k / d2) % d1 + lo[1]) * 128),
+                                  (int32_t)((k % d2 + lo[2]) * 128)};
+            nodes.push_back({vdb_key128(o), (uint32_t)k});
+        }
+    std::sort(nodes.begin(), nodes.end());
+    std::vector<uint32_t> start((size_t)ncell, 0);
+    uint32_t acc = 0;
+    for (const auto& nd : nodes) {
+        start[nd.second] = acc;
+        acc += cnt[nd.second];
+    }
+    std::vector<int32_t> out(org.size());
+    for (size_t i = 0; i < n; ++i) {
+        const size_t d = start[cell[i]]++;
+        out[3 * d] = org[3 * i];
+        out[3 * d + 1] = org[3 * i + 1];
+        out[3 * d + 2] = org[3 * i + 2];
+    }
+    org.swap(out);
+}
 static void dilate_leaves(const int32_t* org, int64_t n, const uint64_t* masks, int r, bool face_only,
                           std::vector<int32_t>& out, bool vdb_order) {
     out.clear();
@@ -98,7 +145,7 @@ static void dilate_leaves(const int32_t* org, int64_t n, const uint64_t* masks, 
                     out.push_back((int32_t)((b + mn[1] - 1) * 8));
                     out.push_back((int32_t)((c + mn[2] - 1) * 8));
                 }
-    if (vdb_order) sort_unique_vdb(out);
+    if (vdb_order) order_dense_scan(out);  // the scan lists each leaf once
 }
 
 struct VHostLevel {
