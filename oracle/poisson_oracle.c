@@ -3,8 +3,10 @@
  * Poisson solver (SIMD_UAAMG/simd_vdb_poisson.cpp) on flattened 8^3 leaves.
  *
  * TEST INFRASTRUCTURE ONLY: the checker for the CUDA library and the timed CPU
- * baseline.  Parity is UNPINNED (the reference cannot be built here: it needs
- * OpenVDB, TBB and Eigen; it ships no golden vectors).
+ * baseline.  Parity is UNPINNED except for fraction_inside (the solver cannot
+ * be built here: it needs OpenVDB, TBB and Eigen, and it ships no golden
+ * vectors; its levelset_util.cpp is plain C++, and tests/test_oracle_ref_pin.py
+ * checks this file's fraction_inside against it bit for bit).
  *
  * Float arithmetic follows the reference operation by operation (the AVX
  * intrinsics in LightWeightApplier are mul/add/fmadd/sub in a fixed order);

@@ -4,8 +4,11 @@
  * on flattened 8^3 leaves.
  *
  * TEST INFRASTRUCTURE ONLY: the checker for the CUDA library and the timed CPU
- * baseline.  Parity is UNPINNED (the reference needs OpenVDB, TBB and Eigen,
- * none of which exist here, and ships no golden vectors).
+ * baseline.  Parity is UNPINNED except for volume_fraction (the solver needs
+ * OpenVDB, TBB and Eigen, none of which exist here, and ships no golden
+ * vectors; its volume_fractions.cpp is plain C++, and
+ * tests/test_oracle_ref_pin.py checks this file's tetrahedron and cube
+ * fractions against it bit for bit).
  *
  * Float arithmetic follows the reference operation by operation; compile with
  * -ffp-contract=off.  Deliberate, documented deviations:
