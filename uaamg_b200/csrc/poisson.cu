@@ -392,8 +392,10 @@ struct uaamg_poisson {
     DeviceCtx* ctx = nullptr;
     void* pin_state = nullptr;  // pinned block holding st_host and scalar_host
     size_t pin_state_cap = 0;
-    void* pin_stage = nullptr;  // pinned staging of the topology upload
+    void* pin_stage = nullptr;  // pinned staging of the level-0 table upload
     size_t pin_stage_cap = 0;
+    void* pin_stage2 = nullptr;  // pinned staging of the coarse levels' table upload
+    size_t pin_stage2_cap = 0;
     void* pin_in = nullptr;  // pinned staging of the small input tables (leaf maps, origins, masks)
     size_t pin_in_cap = 0;
     cudaStream_t own_stream = nullptr;
@@ -403,8 +405,9 @@ struct uaamg_poisson {
     std::vector<LevelDev> lv;
     int nlev = 0;
     // hierarchy memory (one allocation)
-    char* dmem = nullptr;
+    char* dmem = nullptr;   // level 0 and the PCG's vectors
     size_t dmem_bytes = 0;
+    char* dmem2 = nullptr;  // the coarse levels and the coarsest system
     // coarsest
     DCoarsest C{};
     // PCG
@@ -743,6 +746,118 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         L0.nl = (int)keys.size();
         finalize_host_level(L0);
         TRACE("  level-0 tables");
+        // ---- level 0 goes to the device first: its tables go up and its
+        // coefficients (and the rhs) are computed while the host coarsens the
+        // topology.  Two device blocks: level 0 with the PCG's vectors, then the
+        // coarse levels, level 0's parent / octant tables (which coarsening
+        // makes) and the coarsest system.  Each block's host-built tables lie
+        // contiguous at its start, so their pinned image goes up in one copy;
+        // the rest of the block is zeroed on the device.
+        const size_t n0 = (size_t)L0.nl * UAAMG_LEAF;
+        h->lv.assign(1, LevelDev());
+        // the arrays of one level (coefficients, flags, vectors) and its DLevel fields
+        auto carve_arrays = [&](const HostLevel& H, LevelDev& D, char*& cur) {
+            const size_t n = (size_t)H.nl;
+            D.dt = H.dt;
+            D.dx = H.dx;
+            D.flags = carve<uint32_t>(cur, n);
+            D.spai0_ready = carve<int>(cur, 1);
+            float* dg = carve<float>(cur, n * UAAMG_LEAF);
+            float* cx = carve<float>(cur, n * UAAMG_LEAF);
+            float* cy = carve<float>(cur, n * UAAMG_LEAF);
+            float* cz = carve<float>(cur, n * UAAMG_LEAF);
+            float* iv = carve<float>(cur, n * UAAMG_LEAF);
+            D.spai0 = carve<float>(cur, n * UAAMG_LEAF);
+            D.lhs = carve<float>(cur, n * UAAMG_LEAF);
+            D.rhs = carve<float>(cur, n * UAAMG_LEAF);
+            D.tmp = carve<float>(cur, n * UAAMG_LEAF);
+            D.tmp2 = carve<float>(cur, n * UAAMG_LEAF);
+            const float t = H.dt / (H.dx * H.dx);  // LaplacianApplySIMD ctor (.cpp:1045-1065)
+            DLevel& L = D.L;
+            L.nl = (int)n;
+            L.diag = dg; L.cx = cx; L.cy = cy; L.cz = cz; L.invdiag = iv; L.spai0 = D.spai0; L.flags = D.flags;
+            L.def_face = -t;
+            L.def_diag = 6.f * t;
+            L.def_invdiag = 1.0f / (6.f * t);
+            L.def_spai0 = 1.0f / (7.f * t);
+        };
+        auto arrays_bytes = [](size_t n) {
+            return carve_size(n, 4) + carve_size(1, 4) + 10 * carve_size(n * UAAMG_LEAF, 4);  // flags ... tmp2
+        };
+        using Up = std::pair<void*, std::pair<const void*, size_t>>;
+        // a block's table image through pinned memory the handle keeps until destroy (create() need not wait for
+        // the copy); the arrays not uploaded and the alignment gaps are zero, as the device memset made them
+        auto upload_tables = [&](char* block, size_t table_bytes, const std::vector<Up>& ups, void** pin,
+                                 size_t* cap) {
+            CK(ctx_pinned_acquire(h->ctx, table_bytes + 512, pin, cap));
+            char* img = (char*)*pin;
+            memset(img, 0, table_bytes);
+            for (const Up& u : ups) memcpy(img + ((char*)u.first - block), u.second.first, u.second.second);
+            CK(cudaMemcpyAsync(block, img, table_bytes, cudaMemcpyHostToDevice, s));
+        };
+        int* dsrc = nullptr;
+        {
+            const size_t n = (size_t)L0.nl;
+            size_t bytes = carve_size(n * 8, 8) + carve_size(n * 6, 4) + carve_size(n * 8, 4) + carve_size(n, 4) +
+                           carve_size(n * 3, 4) + carve_size(src.size(), 4) + arrays_bytes(n);
+            bytes += (ri ? 7 : 6) * carve_size(n0, 4);  // x b r z p q (+ the built rhs)
+            bytes += carve_size(red_buffer_doubles(std::max<size_t>(n, 1)), 8);
+            bytes += carve_size(sizeof(PcgState), 1) + carve_size(64, 4);
+            CK(ctx_dev_alloc(h->ctx, (void**)&h->dmem, bytes, s));
+            h->dmem_bytes = bytes;
+            char* cur = h->dmem;
+            LevelDev& D0 = h->lv[0];
+            std::vector<Up> ups;
+            uint64_t* m = carve<uint64_t>(cur, n * 8);
+            int* nb = carve<int>(cur, n * 6);
+            int* ch = carve<int>(cur, n * 8);
+            D0.dof_base = carve<int>(cur, n);
+            D0.org = carve<int>(cur, n * 3);
+            dsrc = carve<int>(cur, src.size());
+            ups.push_back({m, {L0.mask.data(), n * 64}});
+            ups.push_back({nb, {L0.nbr.data(), n * 24}});
+            ups.push_back({D0.dof_base, {L0.dof_base.data(), n * 4}});
+            ups.push_back({D0.org, {L0.org.data(), n * 12}});
+            ups.push_back({dsrc, {src.data(), src.size() * 4}});
+            const size_t table_bytes = (size_t)(cur - h->dmem);
+            CK(cudaMemsetAsync(cur, 0, bytes - table_bytes, s));
+            carve_arrays(L0, D0, cur);
+            D0.L.mask = m;
+            D0.L.nbr = nb;
+            D0.L.child = ch;
+            h->x = carve<float>(cur, n0);
+            h->b = carve<float>(cur, n0);
+            h->r = carve<float>(cur, n0);
+            h->z = carve<float>(cur, n0);
+            h->p = carve<float>(cur, n0);
+            h->q = carve<float>(cur, n0);
+            if (ri) h->rhs0 = carve<float>(cur, n0);
+            h->partials = carve<double>(cur, red_buffer_doubles(std::max<size_t>(n, 1)));
+            h->st = reinterpret_cast<PcgState*>(carve<char>(cur, sizeof(PcgState)));
+            h->scalar_dev = carve<float>(cur, 64);
+            upload_tables(h->dmem, table_bytes, ups, &h->pin_stage, &h->pin_stage_cap);
+        }
+        if (L0.nl > 0) {
+            LevelDev& D0 = h->lv[0];
+            k_finest_coef<<<(unsigned)L0.nl, 128, 0, s>>>(dphi.g, dphiorg, dfw.g, dtOverDxSqr, dsrc, D0.L.mask,
+                                                          level_out(D0));
+            CHECK_LAUNCH();
+            h->launches++;
+        }
+        if (ri) {
+            // createPressurePoissonRightHandSide into the PCG's b (the face
+            // weights uploaded once serve the matrix and the rhs)
+            CK(cudaStreamWaitEvent(s, ev_vel.e, 0));
+            LevelDev& D0 = h->lv[0];
+            if (D0.L.nl > 0) {
+                k_build_rhs<<<(unsigned)D0.L.nl, 128, 0, s>>>(D0.L.mask, D0.org, dfw.g, dvel[0].g, dvel[1].g,
+                                                              dvel[2].g, dvel[3].g, 1.0f / dx, h->rhs0);
+                CHECK_LAUNCH();
+                h->launches++;
+            }
+            h->rhs_resident = true;
+        }
+        TRACE("level 0 up, its kernels enqueued");
         // ---- coarse topology: constructMultigridHierarchy (.cpp:1813-1842)
         while (h->host.back().ndof > 4000 && h->host.size() < 32) {
             h->host.emplace_back();
@@ -752,126 +867,67 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             TRACE("  coarse level");
         }
         const int nlev = (int)h->host.size();
-        TRACE("host topology");
-        // ---- device memory for the whole hierarchy
-        size_t bytes = 0;
-        for (int l = 0; l < nlev; ++l) {
-            const HostLevel& H = h->host[l];
-            size_t n = (size_t)H.nl;
-            bytes += carve_size(n * 8, 8) + carve_size(n * 6, 4) + carve_size(n * 8, 4) + carve_size(n, 4) +
-                     carve_size(n, 1) + carve_size(n, 4) + carve_size(n * 3, 4) + carve_size(n, 4) + carve_size(1, 4);
-            bytes += 10 * carve_size(n * UAAMG_LEAF, 4);  // diag cx cy cz invdiag spai0 lhs rhs tmp tmp2
-        }
         const HostLevel& HC = h->host.back();
         size_t nc = (size_t)HC.ndof;
         if (nc > (size_t)CG_MAX_DOF) {
             set_error("coarsening stalled: %zu DOF on the coarsest level (max %d)", nc, CG_MAX_DOF);
             throw UaamgError{UAAMG_ERR_DOMAIN_TOO_LARGE};
         }
-        bytes += carve_size(nc, 4) * 3 + carve_size(nc * 6, 4) * 2;
-        size_t n0 = (size_t)L0.nl * UAAMG_LEAF;
-        bytes += (ri ? 7 : 6) * carve_size(n0, 4);  // x b r z p q (+ the built rhs)
-        bytes += carve_size(red_buffer_doubles(std::max<size_t>((size_t)L0.nl, 1)), 8);
-        bytes += carve_size(sizeof(PcgState), 1) + carve_size(64, 4) + carve_size(src.size(), 4);
-        CK(ctx_dev_alloc(h->ctx, (void**)&h->dmem, bytes, s));
-        h->dmem_bytes = bytes;
-        char* cur2 = h->dmem;
-        h->lv.assign(nlev, LevelDev());
-        // The tables the host built lie contiguous at the start of the block, so their pinned staging image goes up
-        // in one copy; the rest of the block (coefficients, vectors, reduction tickets, flags) is zeroed on the device.
-        struct Tab {
-            uint64_t* m;
-            int *nb, *ch, *par;
-            uint8_t* oc;
-        };
-        std::vector<Tab> tabs(nlev);
-        std::vector<std::pair<void*, std::pair<const void*, size_t>>> ups;
-        for (int l = 0; l < nlev; ++l) {
-            HostLevel& H = h->host[l];
-            LevelDev& D = h->lv[l];
-            const size_t n = (size_t)H.nl;
-            Tab& T = tabs[l];
-            T.m = carve<uint64_t>(cur2, n * 8);
-            T.nb = carve<int>(cur2, n * 6);
-            T.ch = carve<int>(cur2, n * 8);
-            T.par = carve<int>(cur2, n);
-            T.oc = carve<uint8_t>(cur2, n);
-            D.dof_base = carve<int>(cur2, n);
-            D.org = carve<int>(cur2, n * 3);
-            ups.push_back({T.m, {H.mask.data(), n * 64}});
-            ups.push_back({T.nb, {H.nbr.data(), n * 24}});
-            if (!H.child.empty()) ups.push_back({T.ch, {H.child.data(), n * 32}});
-            if (!H.parent.empty()) ups.push_back({T.par, {H.parent.data(), n * 4}});
-            if (!H.octant.empty()) ups.push_back({T.oc, {H.octant.data(), n}});
-            ups.push_back({D.dof_base, {H.dof_base.data(), n * 4}});
-            ups.push_back({D.org, {H.org.data(), n * 12}});
+        h->lv.resize(nlev);
+        int *dslot = nullptr, *ccol = nullptr;
+        float *cdiag = nullptr, *cinvd = nullptr, *cval = nullptr;
+        // ---- the coarse block
+        {
+            const size_t nl0 = (size_t)L0.nl;
+            size_t bytes = carve_size(nl0, 4) + carve_size(nl0, 1);  // level 0's parent, octant
+            for (int l = 1; l < nlev; ++l) {
+                const size_t n = (size_t)h->host[l].nl;
+                bytes += carve_size(n * 8, 8) + carve_size(n * 6, 4) + carve_size(n * 8, 4) + carve_size(n, 4) +
+                         carve_size(n, 1) + carve_size(n, 4) + carve_size(n * 3, 4) + arrays_bytes(n);
+            }
+            bytes += carve_size(nc, 4) * 3 + carve_size(nc * 6, 4) * 2;
+            CK(ctx_dev_alloc(h->ctx, (void**)&h->dmem2, bytes, s));
+            char* cur = h->dmem2;
+            std::vector<Up> ups;
+            int* par0 = carve<int>(cur, nl0);
+            uint8_t* oc0 = carve<uint8_t>(cur, nl0);
+            if (!L0.parent.empty()) ups.push_back({par0, {L0.parent.data(), nl0 * 4}});
+            if (!L0.octant.empty()) ups.push_back({oc0, {L0.octant.data(), nl0}});
+            h->lv[0].L.parent = par0;
+            h->lv[0].L.octant = oc0;
+            for (int l = 1; l < nlev; ++l) {
+                HostLevel& H = h->host[l];
+                LevelDev& D = h->lv[l];
+                const size_t n = (size_t)H.nl;
+                uint64_t* m = carve<uint64_t>(cur, n * 8);
+                int* nb = carve<int>(cur, n * 6);
+                int* ch = carve<int>(cur, n * 8);
+                int* par = carve<int>(cur, n);
+                uint8_t* oc = carve<uint8_t>(cur, n);
+                D.dof_base = carve<int>(cur, n);
+                D.org = carve<int>(cur, n * 3);
+                ups.push_back({m, {H.mask.data(), n * 64}});
+                ups.push_back({nb, {H.nbr.data(), n * 24}});
+                if (!H.child.empty()) ups.push_back({ch, {H.child.data(), n * 32}});
+                if (!H.parent.empty()) ups.push_back({par, {H.parent.data(), n * 4}});
+                if (!H.octant.empty()) ups.push_back({oc, {H.octant.data(), n}});
+                ups.push_back({D.dof_base, {H.dof_base.data(), n * 4}});
+                ups.push_back({D.org, {H.org.data(), n * 12}});
+                D.L.mask = m; D.L.nbr = nb; D.L.child = ch; D.L.parent = par; D.L.octant = oc;
+            }
+            const size_t table_bytes = (size_t)(cur - h->dmem2);
+            CK(cudaMemsetAsync(cur, 0, bytes - table_bytes, s));
+            for (int l = 1; l < nlev; ++l) carve_arrays(h->host[l], h->lv[l], cur);
+            h->C.n = (int)nc;
+            dslot = carve<int>(cur, nc);
+            cdiag = carve<float>(cur, nc);
+            cinvd = carve<float>(cur, nc);
+            ccol = carve<int>(cur, nc * 6);
+            cval = carve<float>(cur, nc * 6);
+            h->C.dof_slot = dslot; h->C.diag = cdiag; h->C.invd = cinvd; h->C.col = ccol; h->C.val = cval;
+            upload_tables(h->dmem2, table_bytes, ups, &h->pin_stage2, &h->pin_stage2_cap);
         }
-        int* dsrc = carve<int>(cur2, src.size());
-        ups.push_back({dsrc, {src.data(), src.size() * 4}});
-        const size_t table_bytes = (size_t)(cur2 - h->dmem);
-        CK(cudaMemsetAsync(cur2, 0, bytes - table_bytes, s));
-        for (int l = 0; l < nlev; ++l) {
-            HostLevel& H = h->host[l];
-            LevelDev& D = h->lv[l];
-            const size_t n = (size_t)H.nl;
-            D.dt = H.dt;
-            D.dx = H.dx;
-            D.flags = carve<uint32_t>(cur2, n);
-            D.spai0_ready = carve<int>(cur2, 1);
-            float* dg = carve<float>(cur2, n * UAAMG_LEAF);
-            float* cx = carve<float>(cur2, n * UAAMG_LEAF);
-            float* cy = carve<float>(cur2, n * UAAMG_LEAF);
-            float* cz = carve<float>(cur2, n * UAAMG_LEAF);
-            float* iv = carve<float>(cur2, n * UAAMG_LEAF);
-            D.spai0 = carve<float>(cur2, n * UAAMG_LEAF);
-            D.lhs = carve<float>(cur2, n * UAAMG_LEAF);
-            D.rhs = carve<float>(cur2, n * UAAMG_LEAF);
-            D.tmp = carve<float>(cur2, n * UAAMG_LEAF);
-            D.tmp2 = carve<float>(cur2, n * UAAMG_LEAF);
-            const float t = H.dt / (H.dx * H.dx);  // LaplacianApplySIMD ctor (.cpp:1045-1065)
-            DLevel& L = D.L;
-            const Tab& T = tabs[l];
-            L.nl = (int)n;
-            L.mask = T.m; L.nbr = T.nb; L.child = T.ch; L.parent = T.par; L.octant = T.oc;
-            L.diag = dg; L.cx = cx; L.cy = cy; L.cz = cz; L.invdiag = iv; L.spai0 = D.spai0; L.flags = D.flags;
-            L.def_face = -t;
-            L.def_diag = 6.f * t;
-            L.def_invdiag = 1.0f / (6.f * t);
-            L.def_spai0 = 1.0f / (7.f * t);
-        }
-        h->C.n = (int)nc;
-        int* dslot = carve<int>(cur2, nc);
-        float* cdiag = carve<float>(cur2, nc);
-        float* cinvd = carve<float>(cur2, nc);
-        int* ccol = carve<int>(cur2, nc * 6);
-        float* cval = carve<float>(cur2, nc * 6);
-        h->C.dof_slot = dslot; h->C.diag = cdiag; h->C.invd = cinvd; h->C.col = ccol; h->C.val = cval;
-        h->x = carve<float>(cur2, n0);
-        h->b = carve<float>(cur2, n0);
-        h->r = carve<float>(cur2, n0);
-        h->z = carve<float>(cur2, n0);
-        h->p = carve<float>(cur2, n0);
-        h->q = carve<float>(cur2, n0);
-        if (ri) h->rhs0 = carve<float>(cur2, n0);
-        h->partials = carve<double>(cur2, red_buffer_doubles(std::max<size_t>((size_t)L0.nl, 1)));
-        h->st = reinterpret_cast<PcgState*>(carve<char>(cur2, sizeof(PcgState)));
-        h->scalar_dev = carve<float>(cur2, 64);
-        // the table region's image in pinned memory (kept by the handle until destroy, so create() need not wait
-        // for the copy); the arrays not uploaded and the alignment gaps are zero, as the device memset made them
-        CK(ctx_pinned_acquire(h->ctx, table_bytes + 512, &h->pin_stage, &h->pin_stage_cap));
-        char* pin = (char*)h->pin_stage;
-        memset(pin, 0, table_bytes);
-        for (auto& u : ups) memcpy(pin + ((char*)u.first - h->dmem), u.second.first, u.second.second);
-        CK(cudaMemcpyAsync(h->dmem, pin, table_bytes, cudaMemcpyHostToDevice, s));
-        TRACE("alloc + table upload");
-        // ---- numeric construction on the device
-        if (L0.nl > 0) {
-            LevelDev& D0 = h->lv[0];
-            k_finest_coef<<<(unsigned)L0.nl, 128, 0, s>>>(dphi.g, dphiorg, dfw.g, dtOverDxSqr, dsrc, D0.L.mask,
-                                                          level_out(D0));
-            CHECK_LAUNCH();
-            h->launches++;
-        }
+        TRACE("coarse levels up");
         for (int l = 1; l < nlev; ++l) {
             LevelDev& D = h->lv[l];
             if (D.L.nl == 0) continue;
@@ -889,19 +945,6 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             k_coarsest_ell<<<(unsigned)D.L.nl, 128, 0, s>>>(D.L, D.dof_base, dslot, cdiag, cinvd, ccol, cval);
             CHECK_LAUNCH();
             h->launches++;
-        }
-        if (ri) {
-            // createPressurePoissonRightHandSide into the PCG's b (the face
-            // weights uploaded once serve the matrix and the rhs)
-            CK(cudaStreamWaitEvent(s, ev_vel.e, 0));
-            LevelDev& D0 = h->lv[0];
-            if (D0.L.nl > 0) {
-                k_build_rhs<<<(unsigned)D0.L.nl, 128, 0, s>>>(D0.L.mask, D0.org, dfw.g, dvel[0].g, dvel[1].g,
-                                                              dvel[2].g, dvel[3].g, 1.0f / dx, h->rhs0);
-                CHECK_LAUNCH();
-                h->launches++;
-            }
-            h->rhs_resident = true;
         }
         for (void* pmem : tofree) CK(cudaFreeAsync(pmem, s));
         tofree.clear();
@@ -1961,9 +2004,11 @@ int uaamg_poisson_destroy(uaamg_poisson* h) {
     if (h->ctx) mixed_free(h);
     if (h->ctx) {
         if (h->dmem) cudaFreeAsync(h->dmem, h->stream);
+        if (h->dmem2) cudaFreeAsync(h->dmem2, h->stream);
         if (h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
         ctx_pinned_release(h->ctx, h->pin_state, h->pin_state_cap);
         ctx_pinned_release(h->ctx, h->pin_stage, h->pin_stage_cap);
+        ctx_pinned_release(h->ctx, h->pin_stage2, h->pin_stage2_cap);
         ctx_pinned_release(h->ctx, h->pin_in, h->pin_in_cap);
         ctx_stream_release(h->ctx, h->body_stream);
         ctx_stream_release(h->ctx, h->own_stream);
