@@ -517,8 +517,10 @@ static void upload_grid_cs(DeviceCtx* ctx, cudaStream_t stream, const uaamg_leaf
                 ++*fg->launches;
                 read = rd;
             }
-            k_gather_host_leaves<<<(unsigned)n, 128, 0, stream>>>(static_cast<const float4*>(mapped), gr->components,
-                                                                  read, reinterpret_cast<float4*>(dv));
+            const int gctas = (int)std::min<int64_t>(n, std::max(1, ctx->sms));
+            k_gather_host_leaves<<<(unsigned)gctas, 128, 0, stream>>>(static_cast<const float4*>(mapped),
+                                                                      gr->components, (int)n, read,
+                                                                      reinterpret_cast<float4*>(dv));
             CHECK_LAUNCH();
             ++*fg->launches;
             dg.read = read;
@@ -687,11 +689,12 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
         // mask kernel, the host topology and the coefficient kernels.
         HostMap vmap[4];
         DevGrid dvel[4];
-        EventGuard ev_in, ev_vel;
+        EventGuard ev_in, ev_vel, ev_l0;
         if (ri) {
             cudaStream_t s2 = h->body_stream;
             CK(cudaEventCreateWithFlags(&ev_in.e, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&ev_vel.e, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ev_l0.e, cudaEventDisableTiming));
             CK(cudaEventRecord(ev_in.e, s));
             CK(cudaStreamWaitEvent(s2, ev_in.e, 0));
             const uaamg_leaf_grid* vg[4] = {ri->vx, ri->vy, ri->vz, ri->sv};
@@ -699,7 +702,6 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             // was uploaded on the first stream, which the second stream waits for)
             for (int k = 0; k < 4; ++k)
                 upload_grid_cs(h->ctx, s2, vg[k], dvel[k], vmap[k], tofree, fw, &dfw, &stage, fgp);
-            CK(cudaEventRecord(ev_vel.e, s2));
         }
         TRACE("upload inputs");
         const float dtOverDxSqr = dt / (dx * dx);
@@ -837,25 +839,31 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             h->scalar_dev = carve<float>(cur, 64);
             upload_tables(h->dmem, table_bytes, ups, &h->pin_stage, &h->pin_stage_cap);
         }
+        if (ri) {
+            // createPressurePoissonRightHandSide into the PCG's b (the face
+            // weights uploaded once serve the matrix and the rhs), on the
+            // velocities' stream once they and level 0's tables are up: the
+            // coarse levels' kernels that follow on the first stream do not
+            // wait for the velocities, which the first stream joins at the end
+            cudaStream_t s2 = h->body_stream;
+            LevelDev& D0 = h->lv[0];
+            if (D0.L.nl > 0) {
+                CK(cudaEventRecord(ev_l0.e, s));
+                CK(cudaStreamWaitEvent(s2, ev_l0.e, 0));
+                k_build_rhs<<<(unsigned)D0.L.nl, 128, 0, s2>>>(D0.L.mask, D0.org, dfw.g, dvel[0].g, dvel[1].g,
+                                                               dvel[2].g, dvel[3].g, 1.0f / dx, h->rhs0);
+                CHECK_LAUNCH();
+                h->launches++;
+            }
+            CK(cudaEventRecord(ev_vel.e, s2));
+            h->rhs_resident = true;
+        }
         if (L0.nl > 0) {
             LevelDev& D0 = h->lv[0];
             k_finest_coef<<<(unsigned)L0.nl, 128, 0, s>>>(dphi.g, dphiorg, dfw.g, dtOverDxSqr, dsrc, D0.L.mask,
                                                           level_out(D0));
             CHECK_LAUNCH();
             h->launches++;
-        }
-        if (ri) {
-            // createPressurePoissonRightHandSide into the PCG's b (the face
-            // weights uploaded once serve the matrix and the rhs)
-            CK(cudaStreamWaitEvent(s, ev_vel.e, 0));
-            LevelDev& D0 = h->lv[0];
-            if (D0.L.nl > 0) {
-                k_build_rhs<<<(unsigned)D0.L.nl, 128, 0, s>>>(D0.L.mask, D0.org, dfw.g, dvel[0].g, dvel[1].g,
-                                                              dvel[2].g, dvel[3].g, 1.0f / dx, h->rhs0);
-                CHECK_LAUNCH();
-                h->launches++;
-            }
-            h->rhs_resident = true;
         }
         TRACE("level 0 up, its kernels enqueued");
         // ---- coarse topology: constructMultigridHierarchy (.cpp:1813-1842)
@@ -946,6 +954,8 @@ static void build_hierarchy(uaamg_poisson* h, const uaamg_leaf_grid* phi, const 
             CHECK_LAUNCH();
             h->launches++;
         }
+        // the rhs and the velocities' buffers: done before the inputs are freed and the handle is used
+        if (ri) CK(cudaStreamWaitEvent(s, ev_vel.e, 0));
         for (void* pmem : tofree) CK(cudaFreeAsync(pmem, s));
         tofree.clear();
         TRACE("coefficient kernels enqueued");

@@ -146,22 +146,37 @@ __global__ void k_face_leaves_read(const int* org, int n, DGrid phi, const uint8
 }
 // A face grid's values [n][512][comps] from pinned host memory (read by the
 // kernel through its device mapping): the leaves the construction reads are
-// copied, the others hold NaN, which no result may depend on.
-__global__ void __launch_bounds__(128) k_gather_host_leaves(const float4* __restrict__ src, int comps,
-                                                            const uint8_t* need, float4* __restrict__ dst) {
-    const int leaf = blockIdx.x, t = threadIdx.x;
-    const long long base = (long long)leaf * comps * (UAAMG_LEAF / 4);
-    if (need[leaf]) {
-        float4 v[3];
+// copied, the others hold NaN, which no result may depend on.  A few CTAs
+// (one per SM) walk the leaves, each thread with the loads of GATHER_LEAVES
+// leaves in flight: that keeps the bus busy while leaving the SMs to the
+// kernels that run beside the copy (one CTA per leaf filled every SM with
+// CTAs waiting on the bus, and the construction's kernels queued behind them).
+constexpr int GATHER_LEAVES = 4;
+__global__ void __launch_bounds__(128) k_gather_host_leaves(const float4* __restrict__ src, int comps, int n,
+                                                            const uint8_t* __restrict__ need,
+                                                            float4* __restrict__ dst) {
+    const int t = threadIdx.x;
+    const float q = __int_as_float(0x7fffffff);
+    const float4 nan4 = make_float4(q, q, q, q);
+    for (int l0 = blockIdx.x; l0 < n; l0 += gridDim.x * GATHER_LEAVES) {
+        float4 v[GATHER_LEAVES][3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            if (c < comps) v[c] = src[base + c * 128 + t];
+        for (int u = 0; u < GATHER_LEAVES; ++u) {
+            const int leaf = l0 + u * (int)gridDim.x;
+            const bool rd = leaf < n && need[leaf];
+            const long long base = (long long)leaf * comps * (UAAMG_LEAF / 4);
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            if (c < comps) dst[base + c * 128 + t] = v[c];
-    } else {
-        const float q = __int_as_float(0x7fffffff);
-        for (int c = 0; c < comps; ++c) dst[base + c * 128 + t] = make_float4(q, q, q, q);
+            for (int c = 0; c < 3; ++c) v[u][c] = (rd && c < comps) ? src[base + c * 128 + t] : nan4;
+        }
+#pragma unroll
+        for (int u = 0; u < GATHER_LEAVES; ++u) {
+            const int leaf = l0 + u * (int)gridDim.x;
+            if (leaf >= n) break;
+            const long long base = (long long)leaf * comps * (UAAMG_LEAF / 4);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                if (c < comps) dst[base + c * 128 + t] = v[u][c];
+        }
     }
 }
 

@@ -20,6 +20,7 @@ namespace uaamg {
 
 struct DeviceCtx {
     int device = -1;
+    int sms = 0;  // streaming multiprocessors of the device
     cudaMemPool_t pool = nullptr;
     std::mutex mu;
     std::vector<cudaStream_t> streams;
@@ -50,6 +51,8 @@ inline DeviceCtx* device_ctx(cudaError_t* err) {
         if (*err != cudaSuccess) { delete c; return nullptr; }
         uint64_t thr = UINT64_MAX;
         *err = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        if (*err != cudaSuccess) { delete c; return nullptr; }
+        *err = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev);
         if (*err != cudaSuccess) { delete c; return nullptr; }
         ctxs[dev] = c;
     }
