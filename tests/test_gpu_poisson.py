@@ -463,6 +463,48 @@ def test_create_with_rhs_one_call_identical(scene64, gpu):
         PoissonSolver(lap).solveMultigridPCGResident(lap.getZeroVectorGrid())
 
 
+@pytest.mark.parametrize("n", [16, 40])
+def test_pinned_inputs_small_domains_identical(gpu, n):
+    """The gather of pinned face grids runs at most one CTA per SM, each
+    walking the leaves four at a time: 16^3 has fewer face-grid leaves (27)
+    than the GPU has SMs, and 40^3 (216) leaves a last partial pass.  The
+    one-call create from pinned host memory gives the same hierarchy, rhs,
+    pressure, iterations and status as from device-resident grids."""
+    torch = gpu
+    from uaamg_b200.poisson import LaplacianWithLevel, PoissonSolver
+    sc = scenes.plain_poisson_scene(n=n, seed=3)
+    keys = ("phi", "face_weights", "vx", "vy", "vz", "solid_velocity")
+    keep = []
+
+    def pinned(g):
+        t = torch.from_numpy(np.ascontiguousarray(g.values)).pin_memory()
+        keep.append(t)
+        return LeafGrid(origins=g.origins, values=t.numpy(), background=g.background, masks=g.masks)
+
+    def on_device(g):
+        d = LeafGrid(origins=g.origins, values=g.values, background=g.background, masks=g.masks)
+        d.values = torch.from_numpy(g.values).cuda()
+        return d
+
+    out = {}
+    for mode, conv in (("device", on_device), ("pinned", pinned)):
+        lap = LaplacianWithLevel.createPressurePoissonLaplacianWithRhs(*[conv(getattr(sc, k)) for k in keys],
+                                                                      sc.dt, sc.dx)
+        solver = PoissonSolver(lap)
+        p = lap.getZeroVectorGrid()
+        st = solver.solveMultigridPCGResident(p)
+        out[mode] = (lap, st, solver.mIterationTaken, p)
+    (l0, st0, it0, p0), (l1, st1, it1, p1) = out["device"], out["pinned"]
+    assert l1.num_levels() == l0.num_levels()
+    for l in range(l0.num_levels()):
+        assert np.array_equal(l1.dof_index(l), l0.dof_index(l))
+        (a1, f1), (a0, f0) = l1.coefficients(l), l0.coefficients(l)
+        assert all(np.array_equal(x, y) for x, y in zip(a1, a0)) and np.array_equal(f1, f0), l
+    assert np.array_equal(l1.copy_rhs(), l0.copy_rhs())
+    assert st0 == st1 == 0 and it0 == it1
+    assert np.array_equal(p1, p0)
+
+
 @pytest.mark.parametrize("n", [64, 128])
 def test_bottom_cycle_cluster_kernel_identical(gpu, n):
     """The two visits of the level next to the coarsest and their coarsest
