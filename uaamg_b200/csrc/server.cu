@@ -12,7 +12,11 @@
 //  * runs pressure rounds: every resident pressure request with a pending
 //    substep gets its right-hand side built on the device, and all of them
 //    are solved in one batched CUDA graph (uaamg_batch, kept while the set
-//    of requests is unchanged), or one after another when batching is off;
+//    of requests is unchanged), or one after another when batching is off.
+//    A set seen for the first time is also solved one request after another
+//    (each handle replays its own solve graph); the batch is built when the
+//    same set comes back in the next round, since a batch's first solve runs
+//    host-driven and pays off only over the rounds that reuse it;
 //    requests admitted meanwhile join the next round;
 //  * runs each viscosity request on a lane of its own (a host thread and a
 //    CUDA stream) that solves its substeps as their velocities arrive, in
@@ -162,6 +166,7 @@ struct uaamg_server {
     std::mutex copy_mu;              // one submission copy at a time on cstream
     uaamg_batch* batch = nullptr;
     std::vector<int64_t> batch_key;
+    std::vector<int64_t> last_key;  // the previous pressure round's set of requests
     std::string loop_error;
     double now() const { return std::chrono::duration<double>(srv_clock::now() - t0).count(); }
 };
@@ -310,9 +315,11 @@ static void srv_pressure_round(uaamg_server* s, std::vector<SrvReq*>& act_in,
     const size_t n = act.size();
     if (n == 0) return;
     std::vector<int> iters(n, 0), status(n, 0);
-    if (s->opt.batching) {
-        std::vector<int64_t> key(n);
-        for (size_t i = 0; i < n; ++i) key[i] = act[i]->id;
+    std::vector<int64_t> key(n);
+    for (size_t i = 0; i < n; ++i) key[i] = act[i]->id;
+    const bool repeat = key == s->last_key;
+    s->last_key = key;
+    if (s->opt.batching && ((s->batch && key == s->batch_key) || repeat)) {
         if (!s->batch || key != s->batch_key) {
             if (s->batch) uaamg_batch_destroy(s->batch);
             s->batch = nullptr;
@@ -461,6 +468,7 @@ static void srv_loop(uaamg_server* s) {
                     if (s->batch) uaamg_batch_destroy(s->batch);
                     s->batch = nullptr;
                     s->batch_key.clear();
+                    s->last_key.clear();
                     for (SrvReq* r : act) srv_fail(s, *r, ("pressure round: " + msg).c_str());
                 }
             }
